@@ -1,0 +1,181 @@
+"""ctypes front end of the CPU FP64 oracle (libeddy_oracle.so).
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg as the checker; the product never imports it.
+The library is built by oracle/Makefile into oracle/_build/.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libeddy_oracle.so")
+
+FIELDS = ["uo", "vo", "wo", "p", "dp", "dens", "tv", "us", "vs", "ws", "ua",
+          "va", "wa", "ub", "vb", "wb", "rha", "rhb", "rs", "planeU", "planeV",
+          "planeW", "planeD"]
+FID = {n: i for i, n in enumerate(FIELDS)}
+GRID_ARRAYS = ["xu", "xc", "ap", "au", "av", "aw", "yv", "yc", "bp", "bu", "bv",
+               "bw", "zw", "zc", "cp", "cu", "cv", "cw", "whx", "why", "whz",
+               "dfxu", "dfxw", "dfxul", "dfxwl", "dfxd", "dfxdl", "dens_bg"]
+
+
+class Params(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("itype", C.c_int * 7), ("ischm", C.c_int), ("isgs", C.c_int),
+                ("idens", C.c_int), ("ru1", C.c_double), ("prn", C.c_double),
+                ("denP1", C.c_double), ("grav", C.c_double), ("dpdx", C.c_double),
+                ("dpdy", C.c_double), ("dpdz", C.c_double), ("eps", C.c_double),
+                ("css", C.c_double), ("vspngx1", C.c_int), ("dspngx1", C.c_int),
+                ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
+                ("dspngx3in", C.c_int), ("dspngx3out", C.c_int)]
+
+
+def make_params(d: dict) -> Params:
+    p = Params()
+    for k, v in d.items():
+        if k == "itype":
+            arr = (C.c_int * 7)(0, *v)
+            p.itype = arr
+        else:
+            setattr(p, k, v)
+    return p
+
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        L.eo_grid_create.restype = C.c_void_p
+        L.eo_grid_create.argtypes = [C.POINTER(Params), dp, C.c_double, C.c_double, dp]
+        L.eo_grid_free.argtypes = [C.c_void_p]
+        L.eo_grid_get.argtypes = [C.c_void_p, C.c_int, dp, C.c_int]
+        L.eo_state_create.restype = C.c_void_p
+        L.eo_state_create.argtypes = [C.POINTER(Params), C.c_void_p]
+        L.eo_state_free.argtypes = [C.c_void_p]
+        L.eo_set.argtypes = [C.c_void_p, C.c_int, dp]
+        L.eo_get.argtypes = [C.c_void_p, C.c_int, dp]
+        L.eo_initialize.argtypes = [C.c_void_p, C.c_double]
+        L.eo_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
+        L.eo_substep.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.eo_direct.argtypes = [C.c_void_p, C.c_int]
+        L.eo_direct.restype = C.c_int
+        L.eo_apply_laplacian.argtypes = [C.c_void_p, dp, dp]
+        L.eo_rfftf.argtypes = [C.c_int, dp]
+        L.eo_rfftb.argtypes = [C.c_int, dp]
+        L.eo_turvis.argtypes = [C.c_void_p]
+        L.eo_filtersize.argtypes = [C.c_void_p]
+        L.eo_set_threads.argtypes = [C.c_int]
+        for name in ("eo_predictord", "eo_density"):
+            getattr(L, name).argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.eo_correct.argtypes = [C.c_void_p, C.c_double]
+        L.eo_pressure_update.argtypes = [C.c_void_p]
+        L.eo_rhs_density.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim == 1)
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def rfftf(x: np.ndarray) -> np.ndarray:
+    r = np.ascontiguousarray(x, dtype=np.float64).copy()
+    lib().eo_rfftf(len(r), _ptr(r))
+    return r
+
+
+def rfftb(x: np.ndarray) -> np.ndarray:
+    r = np.ascontiguousarray(x, dtype=np.float64).copy()
+    lib().eo_rfftb(len(r), _ptr(r))
+    return r
+
+
+class OracleGrid:
+    def __init__(self, params: dict, xfaces, ymin, ymax, zfaces):
+        self.params = params
+        self._p = make_params(params)
+        xf = np.ascontiguousarray(xfaces[:params["nx"] - 1], dtype=np.float64)
+        zf = np.ascontiguousarray(zfaces[:params["nz"] - 1], dtype=np.float64)
+        self.h = lib().eo_grid_create(C.byref(self._p), _ptr(xf), ymin, ymax, _ptr(zf))
+
+    def get(self, name: str) -> np.ndarray:
+        which = GRID_ARRAYS.index(name)
+        n = 3 * (max(self.params["nx"], self.params["ny"], self.params["nz"]) + 2)
+        n = max(n, self.params["nx"] * self.params["ny"])
+        out = np.zeros(n)
+        m = lib().eo_grid_get(self.h, which, _ptr(out), n)
+        return out[:m].copy()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().eo_grid_free(self.h)
+            self.h = None
+
+
+class OracleSolver:
+    """Whole-state oracle of the reference driver's time advance."""
+
+    def __init__(self, workload, threads: int = 0):
+        self.w = workload
+        params = workload.params()
+        xf, zf = workload.faces()
+        self.grid = OracleGrid(params, xf, workload.ylim[0], workload.ylim[1], zf)
+        self._p = make_params(params)
+        self.h = lib().eo_state_create(C.byref(self._p), self.grid.h)
+        if threads:
+            lib().eo_set_threads(threads)
+        self.shape = (params["nx"], params["ny"], params["nz"])
+
+    def set(self, name: str, a: np.ndarray):
+        a = np.asfortranarray(a, dtype=np.float64)
+        lib().eo_set(self.h, FID[name], _ptr(a))
+
+    def get(self, name: str) -> np.ndarray:
+        shape = self.shape[:2] if name.startswith("plane") else self.shape
+        a = np.zeros(shape, order="F")
+        lib().eo_get(self.h, FID[name], _ptr(a))
+        return a
+
+    def load_initial(self, fields: dict):
+        for k, v in fields.items():
+            self.set(k, v)
+
+    def initialize(self):
+        lib().eo_initialize(self.h, self.w.dt)
+
+    def step(self, nsteps: int = 1, poisson_method: int = 0):
+        lib().eo_step(self.h, self.w.dt, nsteps, poisson_method)
+
+    def direct(self, method: int = 0) -> int:
+        return lib().eo_direct(self.h, method)
+
+    def apply_laplacian(self, x: np.ndarray) -> np.ndarray:
+        x = np.asfortranarray(x, dtype=np.float64)
+        out = np.zeros(self.shape, order="F")
+        lib().eo_apply_laplacian(self.h, _ptr(x), _ptr(out))
+        return out
+
+    def turvis(self):
+        lib().eo_turvis(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().eo_state_free(self.h)
+            self.h = None

@@ -1,0 +1,723 @@
+/*
+ * eo_core.c -- oracle restatement of the pointwise/stencil parts of the
+ * fractional step.  TEST INFRASTRUCTURE ONLY.  Compiled with
+ * -ffp-contract=off so every expression keeps the reference's operation order.
+ *
+ * Cartesian branch only (icyl=0, ru=rp=1), explicit viscous/convective terms
+ * (implx=imply=implcx=implcy=0: the Crank-Nicolson parts ut,vt,wt are zero).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "eddy_oracle.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NX (g->nx)
+#define NY (g->ny)
+#define NZ (g->nz)
+#define IX(i, j, k) ((size_t)((i) - 1) + (size_t)NX * ((size_t)((j) - 1) + (size_t)NY * (size_t)((k) - 1)))
+#define A(a, i, j, k) (a)[IX(i, j, k)]
+#define DBG(i, j) g->dens_bg[(size_t)((i) - 1) + (size_t)NX * (size_t)((j) - 1)]
+
+void eo_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+uint64_t eo_splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+double eo_uniform(uint64_t seed, uint64_t counter) {
+  uint64_t h = eo_splitmix64(eo_splitmix64(seed) ^ counter);
+  return (double)(h >> 11) * (1.0 / 9007199254740992.0);
+}
+
+static double *zalloc(long n) { return (double *)calloc((size_t)n, sizeof(double)); }
+
+eo_state *eo_state_create(const eo_params *p, const eo_grid *g) {
+  eo_state *s = (eo_state *)calloc(1, sizeof(eo_state));
+  s->prm = *p;
+  s->g = (eo_grid *)g;
+  long n = (long)p->nx * p->ny * p->nz;
+  s->ncell = n;
+  double **f3[] = {&s->uo, &s->vo, &s->wo, &s->p, &s->dp, &s->dens, &s->tv,
+                   &s->us, &s->vs, &s->ws, &s->ua, &s->va, &s->wa, &s->ub,
+                   &s->vb, &s->wb, &s->rha, &s->rhb, &s->rs, &s->g_s, &s->sxx,
+                   &s->syy, &s->szz, &s->sxy, &s->syz, &s->sxz, &s->ilm,
+                   &s->imm, &s->lm, &s->mm, &s->uc, &s->vc, &s->wc, &s->dxdydz,
+                   &s->cles};
+  for (size_t i = 0; i < sizeof(f3) / sizeof(f3[0]); i++) *f3[i] = zalloc(n);
+  long n2 = (long)p->nx * p->ny;
+  s->planeU = zalloc(n2); s->planeV = zalloc(n2); s->planeW = zalloc(n2);
+  s->planeD = zalloc(n2);
+  return s;
+}
+
+void eo_state_free(eo_state *s) {
+  if (!s) return;
+  double *f3[] = {s->uo, s->vo, s->wo, s->p, s->dp, s->dens, s->tv, s->us,
+                  s->vs, s->ws, s->ua, s->va, s->wa, s->ub, s->vb, s->wb,
+                  s->rha, s->rhb, s->rs, s->g_s, s->sxx, s->syy, s->szz,
+                  s->sxy, s->syz, s->sxz, s->ilm, s->imm, s->lm, s->mm, s->uc,
+                  s->vc, s->wc, s->dxdydz, s->cles, s->planeU, s->planeV,
+                  s->planeW, s->planeD};
+  for (size_t i = 0; i < sizeof(f3) / sizeof(f3[0]); i++) free(f3[i]);
+  free(s);
+}
+
+double *eo_field(eo_state *s, int id) {
+  switch (id) {
+    case EO_UO: return s->uo; case EO_VO: return s->vo; case EO_WO: return s->wo;
+    case EO_P: return s->p; case EO_DP: return s->dp; case EO_DENS: return s->dens;
+    case EO_TV: return s->tv; case EO_US: return s->us; case EO_VS: return s->vs;
+    case EO_WS: return s->ws; case EO_UA: return s->ua; case EO_VA: return s->va;
+    case EO_WA: return s->wa; case EO_UB: return s->ub; case EO_VB: return s->vb;
+    case EO_WB: return s->wb; case EO_RHA: return s->rha; case EO_RHB: return s->rhb;
+    case EO_RS: return s->rs; case EO_PLANEU: return s->planeU;
+    case EO_PLANEV: return s->planeV; case EO_PLANEW: return s->planeW;
+    case EO_PLANED: return s->planeD;
+    default: return NULL;
+  }
+}
+
+static long field_len(eo_state *s, int id) {
+  if (id >= EO_PLANEU && id <= EO_PLANED) return (long)s->prm.nx * s->prm.ny;
+  return s->ncell;
+}
+int eo_set(eo_state *s, int id, const double *src) {
+  double *d = eo_field(s, id);
+  if (!d) return -1;
+  memcpy(d, src, sizeof(double) * (size_t)field_len(s, id));
+  return 0;
+}
+int eo_get(eo_state *s, int id, double *dst) {
+  double *d = eo_field(s, id);
+  if (!d) return -1;
+  memcpy(dst, d, sizeof(double) * (size_t)field_len(s, id));
+  return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * RHS: src/rhs.f:4-438 (icyl=0, all rflag* = 0 so the C.N. parts vanish).
+ * ut,vt,wt and ur,vr,wr are zeroed over the whole array first (rhs.f:65-70);
+ * qr = uo (rhs.f:58).
+ * ---------------------------------------------------------------------- */
+void eo_rhs(eo_state *s, const double *uo, const double *vo, const double *wo,
+            const double *tv, double *ut, double *vt, double *wt, double *ur,
+            double *vr, double *wr, double *qr) {
+  const eo_grid *g = s->g;
+  const double ru1 = s->prm.ru1;
+  const double *ap = g->ap, *au = g->au, *av = g->av, *aw = g->aw;
+  const double *bp = g->bp, *bu = g->bu, *bv = g->bv, *bw = g->bw;
+  const double *cp = g->cp, *cu = g->cu, *cv = g->cv, *cw = g->cw;
+  long n = s->ncell;
+  memcpy(qr, uo, sizeof(double) * (size_t)n);
+  memset(ut, 0, sizeof(double) * (size_t)n); memset(ur, 0, sizeof(double) * (size_t)n);
+  memset(vt, 0, sizeof(double) * (size_t)n); memset(vr, 0, sizeof(double) * (size_t)n);
+  memset(wt, 0, sizeof(double) * (size_t)n); memset(wr, 0, sizeof(double) * (size_t)n);
+  /* u component (rhs.f:77-205) */
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ibu; i <= g->ieu; i++) {
+        double qxp = (A(qr, i + 1, j, k) + A(qr, i, j, k)) * 0.5;
+        double qxm = (A(qr, i, j, k) + A(qr, i - 1, j, k)) * 0.5;
+        double uxp = (A(uo, i + 1, j, k) + A(uo, i, j, k)) * 0.5;
+        double uxm = (A(uo, i, j, k) + A(uo, i - 1, j, k)) * 0.5;
+        double uyp = (A(uo, i, j + 1, k) + A(uo, i, j, k)) * 0.5;
+        double uym = (A(uo, i, j, k) + A(uo, i, j - 1, k)) * 0.5;
+        double uzp = (A(uo, i, j, k + 1) + A(uo, i, j, k)) * 0.5;
+        double uzm = (A(uo, i, j, k) + A(uo, i, j, k - 1)) * 0.5;
+        double vxp = (A(vo, i + 1, j, k) + A(vo, i, j, k)) * 0.5;
+        double vxm = (A(vo, i + 1, j - 1, k) + A(vo, i, j - 1, k)) * 0.5;
+        double wxp = (A(wo, i + 1, j, k) + A(wo, i, j, k)) * 0.5;
+        double wxm = (A(wo, i + 1, j, k - 1) + A(wo, i, j, k - 1)) * 0.5;
+        double dqdxp = ap[i + 1] * (A(qr, i + 1, j, k) - A(qr, i, j, k));
+        double dqdxm = ap[i] * (A(qr, i, j, k) - A(qr, i - 1, j, k));
+        double dudyp = bv[j] * (A(uo, i, j + 1, k) - A(uo, i, j, k));
+        double dudym = bv[j - 1] * (A(uo, i, j, k) - A(uo, i, j - 1, k));
+        double dudzp = cw[k] * (A(uo, i, j, k + 1) - A(uo, i, j, k));
+        double dudzm = cw[k - 1] * (A(uo, i, j, k) - A(uo, i, j, k - 1));
+        double dvdxp = au[i] * (A(vo, i + 1, j, k) - A(vo, i, j, k));
+        double dvdxm = au[i] * (A(vo, i + 1, j - 1, k) - A(vo, i, j - 1, k));
+        double dwdxp = au[i] * (A(wo, i + 1, j, k) - A(wo, i, j, k));
+        double dwdxm = au[i] * (A(wo, i + 1, j, k - 1) - A(wo, i, j, k - 1));
+        double tvjp = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j + 1, k) + A(tv, i, j + 1, k));
+        double tvjm = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j - 1, k) + A(tv, i, j - 1, k));
+        double tvkp = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j, k + 1) + A(tv, i, j, k + 1));
+        double tvkm = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j, k - 1) + A(tv, i, j, k - 1));
+        double txxp = (ru1 + 2. * A(tv, i + 1, j, k)) * dqdxp;
+        double txxm = (ru1 + 2. * A(tv, i, j, k)) * dqdxm;
+        double tyyp = (ru1 + tvjp) * dudyp;
+        double tyym = (ru1 + tvjm) * dudym;
+        double tzzp = (ru1 + tvkp) * dudzp;
+        double tzzm = (ru1 + tvkm) * dudzm;
+        double txyp = tvjp * dvdxp;
+        double txym = tvjm * dvdxm;
+        double txzp = tvkp * dwdxp;
+        double txzm = tvkm * dwdxm;
+        double h11 = -au[i] * (qxp * uxp - qxm * uxm);
+        double h22 = -bu[j] * (vxp * uyp - vxm * uym);
+        double h33 = -cu[k] * (wxp * uzp - wxm * uzm);
+        double t11 = au[i] * (txxp - txxm);
+        double t22 = bu[j] * (tyyp - tyym);
+        double t33 = cu[k] * (tzzp - tzzm);
+        double s22 = bu[j] * (txyp - txym);
+        double s33 = cu[k] * (txzp - txzm);
+        A(ur, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33 + s22 + s33;
+      }
+  /* v component (rhs.f:219-335) */
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jbv; j <= g->jev; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        double vxp = (A(vo, i + 1, j, k) + A(vo, i, j, k)) * 0.5;
+        double vxm = (A(vo, i, j, k) + A(vo, i - 1, j, k)) * 0.5;
+        double vyp = (A(vo, i, j + 1, k) + A(vo, i, j, k)) * 0.5;
+        double vym = (A(vo, i, j, k) + A(vo, i, j - 1, k)) * 0.5;
+        double vzp = (A(vo, i, j, k + 1) + A(vo, i, j, k)) * 0.5;
+        double vzm = (A(vo, i, j, k) + A(vo, i, j, k - 1)) * 0.5;
+        double qyp = (A(qr, i, j + 1, k) + A(qr, i, j, k)) * 0.5;
+        double qym = (A(qr, i - 1, j + 1, k) + A(qr, i - 1, j, k)) * 0.5;
+        double wyp = (A(wo, i, j + 1, k) + A(wo, i, j, k)) * 0.5;
+        double wym = (A(wo, i, j + 1, k - 1) + A(wo, i, j, k - 1)) * 0.5;
+        double dvdxp = au[i] * (A(vo, i + 1, j, k) - A(vo, i, j, k));
+        double dvdxm = au[i - 1] * (A(vo, i, j, k) - A(vo, i - 1, j, k));
+        double dvdyp = bp[j + 1] * (A(vo, i, j + 1, k) - A(vo, i, j, k));
+        double dvdym = bp[j] * (A(vo, i, j, k) - A(vo, i, j - 1, k));
+        double dvdzp = cw[k] * (A(vo, i, j, k + 1) - A(vo, i, j, k));
+        double dvdzm = cw[k - 1] * (A(vo, i, j, k) - A(vo, i, j, k - 1));
+        double dudyp = bv[j] * (A(uo, i, j + 1, k) - A(uo, i, j, k));
+        double dudym = bv[j] * (A(uo, i - 1, j + 1, k) - A(uo, i - 1, j, k));
+        double dwdyp = bv[j] * (A(wo, i, j + 1, k) - A(wo, i, j, k));
+        double dwdym = bv[j] * (A(wo, i, j + 1, k - 1) - A(wo, i, j, k - 1));
+        double tvip = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i + 1, j + 1, k) + A(tv, i + 1, j, k));
+        double tvim = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i - 1, j + 1, k) + A(tv, i - 1, j, k));
+        double tvkp = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i, j + 1, k + 1) + A(tv, i, j, k + 1));
+        double tvkm = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i, j + 1, k - 1) + A(tv, i, j, k - 1));
+        double txxp = (ru1 + tvip) * dvdxp;
+        double txxm = (ru1 + tvim) * dvdxm;
+        double tyyp = (ru1 + 2. * A(tv, i, j + 1, k)) * dvdyp;
+        double tyym = (ru1 + 2. * A(tv, i, j, k)) * dvdym;
+        double tzzp = (ru1 + tvkp) * dvdzp;
+        double tzzm = (ru1 + tvkm) * dvdzm;
+        double txyp = tvip * dudyp;
+        double txym = tvim * dudym;
+        double tyzp = tvkp * dwdyp;
+        double tyzm = tvkm * dwdym;
+        double h11 = -av[i] * (qyp * vxp - qym * vxm);
+        double h22 = -bv[j] * (vyp * vyp - vym * vym);
+        double h33 = -cv[k] * (wyp * vzp - wym * vzm);
+        double t11 = av[i] * (txxp - txxm);
+        double t22 = bv[j] * (tyyp - tyym);
+        double t33 = cv[k] * (tzzp - tzzm);
+        double s11 = av[i] * (txyp - txym);
+        double s33 = cv[k] * (tyzp - tyzm);
+        A(vr, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33 + s11 + s33;
+      }
+  /* w component (rhs.f:347-428) */
+#pragma omp parallel for schedule(static)
+  for (int k = g->kbw; k <= g->kew; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        double wxp = (A(wo, i + 1, j, k) + A(wo, i, j, k)) * 0.5;
+        double wxm = (A(wo, i, j, k) + A(wo, i - 1, j, k)) * 0.5;
+        double wyp = (A(wo, i, j + 1, k) + A(wo, i, j, k)) * 0.5;
+        double wym = (A(wo, i, j, k) + A(wo, i, j - 1, k)) * 0.5;
+        double wzp = (A(wo, i, j, k + 1) + A(wo, i, j, k)) * 0.5;
+        double wzm = (A(wo, i, j, k) + A(wo, i, j, k - 1)) * 0.5;
+        double qzp = (A(qr, i, j, k + 1) + A(qr, i, j, k)) * 0.5;
+        double qzm = (A(qr, i - 1, j, k + 1) + A(qr, i - 1, j, k)) * 0.5;
+        double vzp = (A(vo, i, j, k + 1) + A(vo, i, j, k)) * 0.5;
+        double vzm = (A(vo, i, j - 1, k + 1) + A(vo, i, j - 1, k)) * 0.5;
+        double dwdxp = au[i] * (A(wo, i + 1, j, k) - A(wo, i, j, k));
+        double dwdxm = au[i - 1] * (A(wo, i, j, k) - A(wo, i - 1, j, k));
+        double dwdyp = bv[j] * (A(wo, i, j + 1, k) - A(wo, i, j, k));
+        double dwdym = bv[j - 1] * (A(wo, i, j, k) - A(wo, i, j - 1, k));
+        double dwdzp = cp[k + 1] * (A(wo, i, j, k + 1) - A(wo, i, j, k));
+        double dwdzm = cp[k] * (A(wo, i, j, k) - A(wo, i, j, k - 1));
+        double dudzp = cw[k] * (A(uo, i, j, k + 1) - A(uo, i, j, k));
+        double dudzm = cw[k] * (A(uo, i - 1, j, k + 1) - A(uo, i - 1, j, k));
+        double dvdzp = cw[k] * (A(vo, i, j, k + 1) - A(vo, i, j, k));
+        double dvdzm = cw[k] * (A(vo, i, j - 1, k + 1) - A(vo, i, j - 1, k));
+        double tvip = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i + 1, j, k + 1) + A(tv, i + 1, j, k));
+        double tvim = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i - 1, j, k + 1) + A(tv, i - 1, j, k));
+        double tvjp = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i, j + 1, k + 1) + A(tv, i, j + 1, k));
+        double tvjm = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i, j - 1, k + 1) + A(tv, i, j - 1, k));
+        double txxp = (ru1 + tvip) * dwdxp;
+        double txxm = (ru1 + tvim) * dwdxm;
+        double tyyp = (ru1 + tvjp) * dwdyp;
+        double tyym = (ru1 + tvjm) * dwdym;
+        double tzzp = (ru1 + 2. * A(tv, i, j, k + 1)) * dwdzp;
+        double tzzm = (ru1 + 2. * A(tv, i, j, k)) * dwdzm;
+        double txzp = tvip * dudzp;
+        double txzm = tvim * dudzm;
+        double tyzp = tvjp * dvdzp;
+        double tyzm = tvjm * dvdzm;
+        double h11 = -aw[i] * (qzp * wxp - qzm * wxm);
+        double h22 = -bw[j] * (vzp * wyp - vzm * wym);
+        double h33 = -cw[k] * (wzp * wzp - wzm * wzm);
+        double t11 = aw[i] * (txxp - txxm);
+        double t22 = bw[j] * (tyyp - tyym);
+        double t33 = cw[k] * (tzzp - tzzm);
+        double s11 = aw[i] * (txzp - txzm);
+        double s22 = bw[j] * (tyzp - tyzm);
+        A(wr, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33 + s11 + s22;
+      }
+}
+
+/* ------------------------------------------------------------------------
+ * PREDICTORD: src/timeindeg.f:1041-1265.  Cartesian buoyancy: gravity acts
+ * along x (the sin(yc) factor of the cylindrical form is 1, the cos(yv) factor
+ * on v is 0).  Sponges: timeindeg.f:1117-1143,1185-1211,1245-1263.
+ * ---------------------------------------------------------------------- */
+void eo_predictord(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
+  const eo_grid *g = s->g;
+  const eo_params *pr = &s->prm;
+  double coef = 0.5 * alfxdt, coefd = alfxdt;
+  double *uo = s->uo, *vo = s->vo, *wo = s->wo, *p = s->p, *dens = s->dens;
+  double *ua = s->ua, *va = s->va, *wa = s->wa, *ub = s->ub, *vb = s->vb,
+         *wb = s->wb, *us = s->us, *vs = s->vs, *ws = s->ws;
+  const double *au = g->au, *bv = g->bv, *cw = g->cw;
+  int vx1 = pr->vspngx1;
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ibu; i <= g->ieu; i++) {
+        double ustar = A(uo, i, j, k) + gamxdt * A(ub, i, j, k) + rhoxdt * A(ua, i, j, k) -
+                       alfxdt * au[i] * (A(p, i + 1, j, k) - A(p, i, j, k)) + coef * A(us, i, j, k) -
+                       alfxdt * pr->dpdx;
+        if (pr->idens == 1)
+          ustar = ustar - coefd * 0.50 * pr->grav *
+                              ((A(dens, i + 1, j, k) - DBG(i + 1, j)) + (A(dens, i, j, k) - DBG(i, j)));
+        A(ua, i, j, k) = A(ub, i, j, k);
+        A(ub, i, j, k) = A(us, i, j, k);
+        A(us, i, j, k) = ustar;
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ieu - vx1; i <= g->ieu; i++)
+        A(us, i, j, k) = A(us, i, j, k) + g->dfxu[i] * (0. - A(us, i, j, k)) * alfxdt * 1.0;
+  if (g->ivspngl == 1) {
+#pragma omp parallel for schedule(static)
+    for (int k = g->kz1; k <= g->kz2; k++)
+      for (int j = g->jy1; j <= g->jy2; j++)
+        for (int i = g->ibu; i <= g->ieu; i++)
+          A(us, i, j, k) = A(us, i, j, k) + g->dfxul[k] * (0. - A(us, i, j, k)) * alfxdt * 1.0;
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jbv; j <= g->jev; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        double vstar = A(vo, i, j, k) + gamxdt * A(vb, i, j, k) + rhoxdt * A(va, i, j, k) -
+                       alfxdt * bv[j] * (A(p, i, j + 1, k) - A(p, i, j, k)) + coef * A(vs, i, j, k) -
+                       alfxdt * pr->dpdy;
+        A(va, i, j, k) = A(vb, i, j, k);
+        A(vb, i, j, k) = A(vs, i, j, k);
+        A(vs, i, j, k) = vstar;
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jbv; j <= g->jev; j++)
+      for (int i = g->ix2 - vx1; i <= g->ix2; i++)
+        A(vs, i, j, k) = A(vs, i, j, k) + g->dfxw[i] * (0. - A(vs, i, j, k)) * alfxdt * 1.0;
+  if (g->ivspngl == 1) {
+#pragma omp parallel for schedule(static)
+    for (int k = g->kz1; k <= g->kz2; k++)
+      for (int j = g->jy1; j <= g->jy2; j++)
+        for (int i = g->ibu; i <= g->ieu; i++)
+          A(vs, i, j, k) = A(vs, i, j, k) + g->dfxwl[k] * (0. - A(vs, i, j, k)) * alfxdt * 1.0;
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = g->kbw; k <= g->kew; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        double wstar = A(wo, i, j, k) + gamxdt * A(wb, i, j, k) + rhoxdt * A(wa, i, j, k) -
+                       alfxdt * cw[k] * (A(p, i, j, k + 1) - A(p, i, j, k)) + coef * A(ws, i, j, k) -
+                       alfxdt * pr->dpdz;
+        A(wa, i, j, k) = A(wb, i, j, k);
+        A(wb, i, j, k) = A(ws, i, j, k);
+        A(ws, i, j, k) = wstar;
+      }
+#pragma omp parallel for schedule(static)
+  for (int k = g->kbw; k <= g->kew; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix2 - vx1; i <= g->ix2; i++)
+        A(ws, i, j, k) = A(ws, i, j, k) + g->dfxw[i] * (1. - A(ws, i, j, k)) * alfxdt * 1.0;
+  if (g->ivspngl == 1) {
+#pragma omp parallel for schedule(static)
+    for (int k = g->kbw; k <= g->kew; k++)
+      for (int j = g->jy1; j <= g->jy2; j++)
+        for (int i = g->ix1; i <= g->ix2; i++)
+          A(ws, i, j, k) = A(ws, i, j, k) + g->dfxwl[k] * (1. - A(ws, i, j, k)) * alfxdt * 1.0;
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * BOUNDARY: src/boundary.f:7-66 with BOUND050 (:69), BOUND060 (:125),
+ * BOUND082 (:372), BOUND500 (:409).  Whole-plane assignments as written.
+ * ---------------------------------------------------------------------- */
+static void fill_x_plane(const eo_grid *g, double *a, int idst, int isrc, double sgn, int zero) {
+  for (int k = 1; k <= NZ; k++)
+    for (int j = 1; j <= NY; j++) A(a, idst, j, k) = zero ? 0. : sgn * A(a, isrc, j, k);
+}
+static void fill_y_plane(const eo_grid *g, double *a, int jdst, int jsrc, double sgn, int zero) {
+  for (int k = 1; k <= NZ; k++)
+    for (int i = 1; i <= NX; i++) A(a, i, jdst, k) = zero ? 0. : sgn * A(a, i, jsrc, k);
+}
+static void fill_z_plane(const eo_grid *g, double *a, int kdst, int ksrc, double sgn, int zero) {
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) A(a, i, j, kdst) = zero ? 0. : sgn * A(a, i, j, ksrc);
+}
+
+void eo_boundary(eo_state *s, double *u, double *v, double *w) {
+  const eo_grid *g = s->g;
+  const int *it = s->prm.itype;
+  for (int ib = 1; ib <= 6; ib++) {
+    int t = it[ib];
+    if (t == 50 || t == 60) {
+      double sg = (t == 50) ? -1. : 1.;
+      switch (ib) {
+        case 1: fill_x_plane(g, u, g->ib1, 0, 0, 1); fill_x_plane(g, v, g->ib1, g->ix1, sg, 0);
+                fill_x_plane(g, w, g->ib1, g->ix1, sg, 0); break;
+        case 2: fill_x_plane(g, u, g->ix2, 0, 0, 1); fill_x_plane(g, v, g->ib2, g->ix2, sg, 0);
+                fill_x_plane(g, w, g->ib2, g->ix2, sg, 0); break;
+        case 3: fill_y_plane(g, u, g->jb1, g->jy1, sg, 0); fill_y_plane(g, v, g->jb1, 0, 0, 1);
+                fill_y_plane(g, w, g->jb1, g->jy1, sg, 0); break;
+        case 4: fill_y_plane(g, u, g->jb2, g->jy2, sg, 0); fill_y_plane(g, v, g->jy2, 0, 0, 1);
+                fill_y_plane(g, w, g->jb2, g->jy2, sg, 0); break;
+        case 5: fill_z_plane(g, u, g->kb1, g->kz1, sg, 0); fill_z_plane(g, v, g->kb1, g->kz1, sg, 0);
+                fill_z_plane(g, w, g->kb1, 0, 0, 1); break;
+        case 6: fill_z_plane(g, u, g->kb2, g->kz2, sg, 0); fill_z_plane(g, v, g->kb2, g->kz2, sg, 0);
+                fill_z_plane(g, w, g->kz2, 0, 0, 1); break;
+      }
+    } else if (t == 82) {
+      if (ib == 1) {
+        fill_x_plane(g, u, g->ib1, g->ix1, 1., 0); fill_x_plane(g, v, g->ib1, g->ix1, -1., 0);
+        fill_x_plane(g, w, g->ib1, g->ix1, -1., 0);
+      } else if (ib == 2) {
+        fill_x_plane(g, u, g->ib2, g->ix2, 1., 0); fill_x_plane(g, v, g->ib2, g->ix2, 1., 0);
+        fill_x_plane(g, w, g->ib2, g->ix2, 1., 0);
+      }
+    }
+  }
+  for (int ib = 1; ib <= 3; ib += 2) {
+    if (it[ib] != 500) continue;
+    if (ib == 1) {
+      fill_x_plane(g, u, g->ib1, g->ix2, 1., 0); fill_x_plane(g, v, g->ib1, g->ix2, 1., 0);
+      fill_x_plane(g, w, g->ib1, g->ix2, 1., 0);
+      fill_x_plane(g, u, g->ib2, g->ix1, 1., 0); fill_x_plane(g, v, g->ib2, g->ix1, 1., 0);
+      fill_x_plane(g, w, g->ib2, g->ix1, 1., 0);
+    } else {
+      fill_y_plane(g, u, g->jb1, g->jy2, 1., 0); fill_y_plane(g, v, g->jb1, g->jy2, 1., 0);
+      fill_y_plane(g, w, g->jb1, g->jy2, 1., 0);
+      fill_y_plane(g, u, g->jb2, g->jy1, 1., 0); fill_y_plane(g, v, g->jb2, g->jy1, 1., 0);
+      fill_y_plane(g, w, g->jb2, g->jy1, 1., 0);
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * BOUNDINOUT: src/boundary.f:505-994, inlet 305 (hybrid plane, :694) and
+ * outlets 710/720/730 (:806-958).  x-boundary mass correction (types 80-82)
+ * is not part of the restated configurations.
+ * ---------------------------------------------------------------------- */
+void eo_boundinout(eo_state *s, double *ubc, double *vbc, double *wbc,
+                   const double *uof, const double *vof, const double *wof,
+                   double alfxdt, int idiv) {
+  const eo_grid *g = s->g;
+  const int *it = s->prm.itype;
+  int iinq = idiv, iouq = idiv;
+  double qin1 = 0., qin2 = 0., area = 0., qinxg = 0.;
+  if (it[5] == 305) {
+    for (int j = 1; j <= NY; j++)
+      for (int i = 1; i <= NX; i++) {
+        size_t q = (size_t)(i - 1) + (size_t)NX * (j - 1);
+        A(ubc, i, j, g->kb1) = s->planeU[q];
+        A(vbc, i, j, g->kb1) = s->planeV[q];
+        A(wbc, i, j, g->kb1) = s->planeW[q];
+      }
+  } else {
+    iinq = 0;
+  }
+  if (iinq == 1) {
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        double areaij = 1.0 / (g->ap[i] * g->bp[j]);
+        qin1 = qin1 + A(wbc, i, j, g->kb1) * areaij;
+        area = area + areaij;
+      }
+    qin2 = qin1 / area;
+  }
+  if (idiv == 1) {
+    int t6 = it[6];
+    if (t6 == 710) {
+      for (int j = 1; j <= NY; j++)
+        for (int i = 1; i <= NX; i++) A(wbc, i, j, g->kz2) = A(wbc, i, j, g->kz2 - 1);
+    } else if (t6 == 720) {
+      double c = g->cp[g->kz2 - 1] / g->cp[g->kz2];
+      for (int j = 1; j <= NY; j++)
+        for (int i = 1; i <= NX; i++)
+          A(wbc, i, j, g->kz2) = (1 + c) * A(wbc, i, j, g->kz2 - 1) - c * A(wbc, i, j, g->kz2 - 2);
+    } else if (t6 == 730) {
+    } else {
+      iouq = 0;
+    }
+    if (iouq == 1) {
+      qin1 = qin1 + qinxg;
+      if (t6 == 730) {
+        double coef = qin2 * alfxdt * g->cp[g->kz2];
+        int kz2 = g->kz2;
+        for (int j = g->jy1; j <= g->jy2; j++)
+          for (int i = g->ix1; i <= g->ix2; i++) {
+            A(ubc, i, j, NZ) = A(uof, i, j, NZ) - coef * (A(uof, i, j, NZ) - A(uof, i, j, kz2));
+            A(vbc, i, j, NZ) = A(vof, i, j, NZ) - coef * (A(vof, i, j, NZ) - A(vof, i, j, kz2));
+            A(wbc, i, j, kz2) = A(wof, i, j, kz2) - coef * (A(wof, i, j, kz2) - A(wof, i, j, kz2 - 1));
+          }
+        fill_y_plane(g, ubc, 1, NY - 1, 1., 0); fill_y_plane(g, ubc, NY, 2, 1., 0);
+        fill_y_plane(g, vbc, 1, NY - 1, 1., 0); fill_y_plane(g, vbc, NY, 2, 1., 0);
+        fill_y_plane(g, wbc, 1, NY - 1, 1., 0); fill_y_plane(g, wbc, NY, 2, 1., 0);
+      }
+      double a2 = 0., qout = 0.;
+      for (int j = g->jy1; j <= g->jy2; j++)
+        for (int i = g->ix1; i <= g->ix2; i++) {
+          double areaij = 1.0 / (g->ap[i] * g->bp[j]);
+          qout = qout + A(wbc, i, j, g->kz2) * areaij;
+          a2 = a2 + areaij;
+        }
+      s->qin_last = qin1;
+      s->qout_last = qout;
+      if (qout != 0.) {
+        double c = qin1 / qout;
+        for (int j = g->jy1; j <= g->jy2; j++)
+          for (int i = g->ix1; i <= g->ix2; i++) A(wbc, i, j, g->kz2) = A(wbc, i, j, g->kz2) * c;
+      } else {
+        for (int j = g->jy1; j <= g->jy2; j++)
+          for (int i = g->ix1; i <= g->ix2; i++) A(wbc, i, j, g->kz2) = qin1 / a2;
+      }
+    }
+  } else {
+    int t6 = it[6];
+    if (t6 == 710) {
+      for (int j = 1; j <= NY; j++)
+        for (int i = 1; i <= NX; i++) {
+          A(ubc, i, j, NZ) = A(uof, i, j, g->kz2);
+          A(vbc, i, j, NZ) = A(vof, i, j, g->kz2);
+          A(wbc, i, j, g->kz2) = A(wof, i, j, g->kz2);
+        }
+    } else if (t6 == 720) {
+      double c = g->cw[g->kz2 - 1] / g->cw[g->kz2];
+      for (int j = 1; j <= NY; j++)
+        for (int i = 1; i <= NX; i++) {
+          A(ubc, i, j, NZ) = (1 + c) * A(uof, i, j, g->kz2) - c * A(uof, i, j, g->kz2 - 1);
+          A(vbc, i, j, NZ) = (1 + c) * A(vof, i, j, g->kz2) - c * A(vof, i, j, g->kz2 - 1);
+          A(wbc, i, j, g->kz2) = A(wof, i, j, g->kz2);
+        }
+    } else if (t6 == 730 || t6 == 731) {
+      for (int j = 1; j <= NY; j++)
+        for (int i = 1; i <= NX; i++) {
+          A(ubc, i, j, NZ) = A(uof, i, j, NZ);
+          A(vbc, i, j, NZ) = A(vof, i, j, NZ);
+          A(wbc, i, j, g->kz2) = A(wof, i, j, g->kz2);
+        }
+    }
+  }
+}
+
+/* DIVERGENCE: src/timeindeg.f:908-977 (rp=ru=1) */
+void eo_divergence(eo_state *s, const double *us, const double *vs, const double *ws, double *div) {
+  const eo_grid *g = s->g;
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++)
+        A(div, i, j, k) = (g->ap[i] * (A(us, i, j, k) - A(us, i - 1, j, k)) +
+                           g->bp[j] * (A(vs, i, j, k) - A(vs, i, j - 1, k)) +
+                           g->cp[k] * (A(ws, i, j, k) - A(ws, i, j, k - 1)));
+}
+
+/* CORRECT: src/timeindeg.f:981-1028: (us,vs,ws,dp) -> (uo,vo,wo) */
+void eo_correct(eo_state *s, double alfxdt) {
+  const eo_grid *g = s->g;
+  double *uo = s->uo, *vo = s->vo, *wo = s->wo, *us = s->us, *vs = s->vs, *ws = s->ws, *dp = s->dp;
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ibu; i <= g->ieu; i++)
+        A(uo, i, j, k) = A(us, i, j, k) - g->au[i] * (A(dp, i + 1, j, k) - A(dp, i, j, k)) * alfxdt;
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jbv; j <= g->jev; j++)
+      for (int i = g->ix1; i <= g->ix2; i++)
+        A(vo, i, j, k) = A(vs, i, j, k) - g->bv[j] * (A(dp, i, j + 1, k) - A(dp, i, j, k)) * alfxdt;
+#pragma omp parallel for schedule(static)
+  for (int k = g->kbw; k <= g->kew; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++)
+        A(wo, i, j, k) = A(ws, i, j, k) - g->cw[k] * (A(dp, i, j, k + 1) - A(dp, i, j, k)) * alfxdt;
+}
+
+/* Pressure update, reference value and ghost fills: src/Eddy6.f:2772-2853
+ * followed by :2911-2953 (explicit scheme, ibm=0). */
+void eo_pressure_update(eo_state *s) {
+  const eo_grid *g = s->g;
+  const int *it = s->prm.itype;
+  double *p = s->p, *dp = s->dp;
+  for (long q = 0; q < s->ncell; q++) p[q] = p[q] + dp[q];
+  double pref = 0.;
+  for (int j = g->jy1; j <= g->jy2; j++) pref += A(p, g->ix1, j, 2);
+  pref = pref / (double)(NY - 2);
+  s->pref_last = pref;
+  for (long q = 0; q < s->ncell; q++) p[q] = p[q] - pref;
+  /* first ghost pass (:2814-2853) */
+  if (g->mp == 0) { fill_x_plane(g, p, 1, g->ix2, 1., 0); fill_x_plane(g, p, NX, g->ix1, 1., 0); }
+  else { fill_x_plane(g, p, 1, g->ix1, -1., 0); fill_x_plane(g, p, NX, g->ix2, -1., 0); }
+  if (g->lp == 0) { fill_y_plane(g, p, 1, g->jy2, 1., 0); fill_y_plane(g, p, NY, g->jy1, 1., 0); }
+  else { fill_y_plane(g, p, 1, g->jy1, 1., 0); fill_y_plane(g, p, NY, g->jy2, 1., 0); }
+  if (it[5] == 500) fill_z_plane(g, p, 1, g->kz2, 1., 0);
+  if (it[6] == 500) fill_z_plane(g, p, NZ, g->kz1, 1., 0);
+  if (it[5] != 0 && it[5] != 500) fill_z_plane(g, p, 1, g->kz1, 1., 0);
+  if (it[6] != 0 && it[6] != 500) fill_z_plane(g, p, NZ, g->kz2, 1., 0);
+  /* second ghost pass (:2911-2953) */
+  if (it[5] != 0 && it[5] != 500) fill_z_plane(g, p, 1, g->kz1, 1., 0);
+  if (it[6] != 0 && it[6] != 500) fill_z_plane(g, p, NZ, g->kz2, 1., 0);
+  if (g->mp == 0) { fill_x_plane(g, p, 1, g->ix2, 1., 0); fill_x_plane(g, p, NX, g->ix1, 1., 0); }
+  else { fill_x_plane(g, p, 1, g->ix1, 1., 0); fill_x_plane(g, p, NX, g->ix2, 1., 0); }
+  if (g->lp == 0) { fill_y_plane(g, p, 1, g->jy2, 1., 0); fill_y_plane(g, p, NY, g->jy1, 1., 0); }
+  else { fill_y_plane(g, p, 1, g->jy1, 1., 0); fill_y_plane(g, p, NY, g->jy2, 1., 0); }
+}
+
+/* RHS_DENSITY: src/rhs_density.f:4-175 (rr -> rhb, rt -> rs; explicit) */
+void eo_rhs_density(eo_state *s) {
+  const eo_grid *g = s->g;
+  double *uo = s->uo, *vo = s->vo, *wo = s->wo, *dens = s->dens, *kv = s->tv;
+  double *rr = s->rhb, *rt = s->rs;
+  double repr1 = s->prm.ru1 / s->prm.prn;
+  memset(rr, 0, sizeof(double) * (size_t)s->ncell);
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        double qxp = A(uo, i, j, k), qxm = A(uo, i - 1, j, k);
+        double rxp = (A(dens, i + 1, j, k) + A(dens, i, j, k)) * 0.5;
+        double rxm = (A(dens, i, j, k) + A(dens, i - 1, j, k)) * 0.5;
+        double vyp = A(vo, i, j, k), vym = A(vo, i, j - 1, k);
+        double ryp = (A(dens, i, j + 1, k) + A(dens, i, j, k)) * 0.5;
+        double rym = (A(dens, i, j, k) + A(dens, i, j - 1, k)) * 0.5;
+        double wzp = A(wo, i, j, k), wzm = A(wo, i, j, k - 1);
+        double rzp = (A(dens, i, j, k + 1) + A(dens, i, j, k)) * 0.5;
+        double rzm = (A(dens, i, j, k) + A(dens, i, j, k - 1)) * 0.5;
+        double drdxp = g->au[i] * (A(dens, i + 1, j, k) - A(dens, i, j, k));
+        double drdxm = g->au[i - 1] * (A(dens, i, j, k) - A(dens, i - 1, j, k));
+        double drdyp = g->bv[j] * (A(dens, i, j + 1, k) - A(dens, i, j, k));
+        double drdym = g->bv[j - 1] * (A(dens, i, j, k) - A(dens, i, j - 1, k));
+        double drdzp = g->cw[k] * (A(dens, i, j, k + 1) - A(dens, i, j, k));
+        double drdzm = g->cw[k - 1] * (A(dens, i, j, k) - A(dens, i, j, k - 1));
+        double kvip = 0.5 * (A(kv, i + 1, j, k) + A(kv, i, j, k));
+        double kvim = 0.5 * (A(kv, i - 1, j, k) + A(kv, i, j, k));
+        double kvjp = 0.5 * (A(kv, i, j + 1, k) + A(kv, i, j, k));
+        double kvjm = 0.5 * (A(kv, i, j - 1, k) + A(kv, i, j, k));
+        double kvkp = 0.5 * (A(kv, i, j, k + 1) + A(kv, i, j, k));
+        double kvkm = 0.5 * (A(kv, i, j, k - 1) + A(kv, i, j, k));
+        double txxp = (repr1 + kvip) * drdxp;
+        double txxm = (repr1 + kvim) * drdxm;
+        double tyyp = (repr1 + kvjp) * drdyp;
+        double tyym = (repr1 + kvjm) * drdym;
+        double tzzp = (repr1 + kvkp) * drdzp;
+        double tzzm = (repr1 + kvkm) * drdzm;
+        double h11 = -g->ap[i] * (rxp * qxp - rxm * qxm);
+        double h22 = -g->bp[j] * (ryp * vyp - rym * vym);
+        double h33 = -g->cp[k] * (rzp * wzp - rzm * wzm);
+        double t11 = g->ap[i] * (txxp - txxm);
+        double t22 = g->bp[j] * (tyyp - tyym);
+        double t33 = g->cp[k] * (tzzp - tzzm);
+        A(rr, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33;
+        A(rt, i, j, k) = 0.;
+      }
+}
+
+/* BOUNDARY_DENS: src/boundary.f:2001-2197 (types 50, 82, 500) */
+void eo_boundary_dens(eo_state *s, double *d) {
+  const eo_grid *g = s->g;
+  const int *it = s->prm.itype;
+  for (int ib = 1; ib <= 6; ib++) {
+    int t = it[ib];
+    if (t == 50) {
+      if (ib == 1) for (int k = 1; k <= NZ; k++) for (int j = 1; j <= NY; j++)
+            A(d, g->ib1, j, k) = 2.0 * (0.5) - A(d, g->ib1 + 1, j, k);
+      if (ib == 2) for (int k = 1; k <= NZ; k++) for (int j = 1; j <= NY; j++)
+            A(d, g->ib2, j, k) = 2.0 * (-0.5) - A(d, g->ib2 - 1, j, k);
+    } else if (t == 80 || t == 82) {
+      if (ib == 1) fill_x_plane(g, d, g->ib1, g->ix1, 1., 0);
+      if (ib == 2) {
+        /* cylindrical background-gradient term vanishes for rp = 1 */
+        fill_x_plane(g, d, g->ix2, g->ix2 - 1, 1., 0);
+        fill_x_plane(g, d, g->ib2, g->ix2, 1., 0);
+      }
+    }
+  }
+  for (int ib = 1; ib <= 5; ib += 2) {
+    if (it[ib] != 500) continue;
+    if (ib == 1) { fill_x_plane(g, d, g->ib1, g->ix2, 1., 0); fill_x_plane(g, d, g->ib2, g->ix1, 1., 0); }
+    if (ib == 3) { fill_y_plane(g, d, g->jb1, g->jy2, 1., 0); fill_y_plane(g, d, g->jb2, g->jy1, 1., 0); }
+    if (ib == 5) { fill_z_plane(g, d, g->kb1, g->kz2, 1., 0); fill_z_plane(g, d, g->kb2, g->kz1, 1., 0); }
+  }
+}
+
+/* BOUNDINOUTD: src/boundary.f:2241-2281 */
+void eo_boundinoutd(eo_state *s, double *d) {
+  const eo_grid *g = s->g;
+  const int *it = s->prm.itype;
+  if (it[5] == 305) {
+    for (int j = 1; j <= NY; j++)
+      for (int i = 1; i <= NX; i++) A(d, i, j, g->kb1) = s->planeD[(size_t)(i - 1) + (size_t)NX * (j - 1)];
+    fill_z_plane(g, d, 2, 1, 1., 0);
+  }
+  if (it[6] == 730) {
+    fill_z_plane(g, d, g->kz2, g->kz2 - 1, 1., 0);
+    fill_z_plane(g, d, NZ, g->kz2, 1., 0);
+  }
+  if (it[6] == 710) fill_z_plane(g, d, g->kz2, g->kz2 - 1, 1., 0);
+}
+
+/* DENSITY: src/density.f:6-127 (explicit: no INVERSEYD/INVERSEXD) */
+void eo_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
+  const eo_grid *g = s->g;
+  double *dens = s->dens, *rha = s->rha, *rhb = s->rhb, *rs = s->rs;
+  double coef = 0.5 * alfxdt;
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        A(dens, i, j, k) = A(dens, i, j, k) + gamxdt * A(rhb, i, j, k) + rhoxdt * A(rha, i, j, k) +
+                           coef * A(rs, i, j, k);
+        A(rha, i, j, k) = A(rhb, i, j, k);
+        A(rhb, i, j, k) = A(rs, i, j, k);
+        A(rs, i, j, k) = A(dens, i, j, k);
+      }
+  for (long q = 0; q < s->ncell; q++) rhb[q] = rs[q] + 0.5 * alfxdt * rhb[q];
+  eo_boundary_dens(s, rhb);
+  if (g->idspngl == 1) {
+#pragma omp parallel for schedule(static)
+    for (int k = g->kz1; k <= g->kz2; k++)
+      for (int j = g->jy1; j <= g->jy2; j++)
+        for (int i = g->ix1; i <= g->ix2; i++)
+          A(dens, i, j, k) = A(dens, i, j, k) + g->dfxdl[k] * (DBG(i, j) - A(dens, i, j, k)) * alfxdt * 1.0;
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix2 - s->prm.dspngx1; i <= g->ix2; i++)
+        A(dens, i, j, k) = A(dens, i, j, k) + g->dfxd[i] * (DBG(i, j) - A(dens, i, j, k)) * alfxdt * 1.0;
+}

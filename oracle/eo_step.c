@@ -1,0 +1,121 @@
+/*
+ * eo_step.c -- oracle restatement of the driver's time-advance sequence,
+ * src/Eddy6.f:2095-3049 for ibm=0, explicit viscous terms, single rank.
+ * TEST INFRASTRUCTURE ONLY.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "eddy_oracle.h"
+
+/* RK3 / AB2 coefficients, src/inpall.f:218-235 */
+static void scheme(int ischm, double gam[3], double rho[3], double alf[3]) {
+  if (ischm == 1) {
+    gam[0] = 1.5; gam[1] = 0.; gam[2] = 0.;
+    rho[0] = -0.5; rho[1] = 0.; rho[2] = 0.;
+  } else {
+    gam[0] = 8. / 15.; gam[1] = 5. / 12.; gam[2] = 3. / 4.;
+    rho[0] = 0.; rho[1] = -17. / 60.; rho[2] = -5. / 12.;
+  }
+  for (int q = 0; q < 3; q++) alf[q] = gam[q] + rho[q];
+}
+
+static int g_poisson_method = 0;
+
+void eo_substep(eo_state *s, int is, double dtm1) {
+  double gam[3], rho[3], alf[3];
+  scheme(s->prm.ischm, gam, rho, alf);
+  double alfxdt = alf[is] * dtm1, gamxdt = gam[is] * dtm1, rhoxdt = rho[is] * dtm1;
+  /* Eddy6.f:2453 */
+  eo_rhs(s, s->uo, s->vo, s->wo, s->tv, s->us, s->vs, s->ws, s->ub, s->vb, s->wb, s->dp);
+  /* :2484 */
+  eo_predictord(s, alfxdt, gamxdt, rhoxdt);
+  /* :2689-2704 */
+  eo_boundary(s, s->us, s->vs, s->ws);
+  eo_boundinout(s, s->us, s->vs, s->ws, s->uo, s->vo, s->wo, alfxdt, 1);
+  eo_boundary(s, s->us, s->vs, s->ws);
+  /* :2712-2715 */
+  eo_divergence(s, s->us, s->vs, s->ws, s->dp);
+  for (long q = 0; q < s->ncell; q++) s->dp[q] = s->dp[q] / alfxdt;
+  /* :2722 */
+  eo_direct(s, g_poisson_method);
+  /* :2738-2761 */
+  eo_correct(s, alfxdt);
+  eo_boundary(s, s->uo, s->vo, s->wo);
+  eo_boundinout(s, s->uo, s->vo, s->wo, s->us, s->vs, s->ws, alfxdt, 0);
+  eo_boundary(s, s->uo, s->vo, s->wo);
+  /* :2772-2853, :2911-2953 */
+  eo_pressure_update(s);
+  /* :2957-2969 */
+  if (s->prm.idens == 1) {
+    eo_boundinoutd(s, s->dens);
+    eo_boundary_dens(s, s->dens);
+    eo_rhs_density(s);
+    eo_boundary_dens(s, s->rhb);
+    eo_boundary_dens(s, s->rs);
+    eo_density(s, alfxdt, gamxdt, rhoxdt);
+    eo_boundinoutd(s, s->dens);
+    eo_boundary_dens(s, s->dens);
+  }
+}
+
+void eo_step(eo_state *s, double dtm1, int nsteps, int poisson_method) {
+  double gam[3], rho[3], alf[3];
+  scheme(s->prm.ischm, gam, rho, alf);
+  g_poisson_method = poisson_method;
+  int nsub = (s->prm.ischm == 1) ? 1 : 3;
+  for (int n = 0; n < nsteps; n++) {
+    double tlevel = s->time;
+    for (int is = 0; is < nsub; is++) {
+      eo_substep(s, is, dtm1);
+      double sa = 0.;
+      for (int q = 0; q <= is; q++) sa += alf[q];
+      tlevel = s->time + sa * dtm1;
+    }
+    s->time = tlevel;
+    /* :3008-3019 */
+    if (s->prm.isgs != 0) eo_turvis(s);
+  }
+}
+
+/* Start-from-scratch initialisation after the fields are set (src/Eddy6.f
+ * :582-617 ghost fills, :620 sponge set-up (in eo_grid_create), :752-756
+ * inflow/outflow, :1718-1726 filter size and initial TURVIS). */
+void eo_initialize(eo_state *s, double dtm1) {
+  double gam[3], rho[3], alf[3];
+  scheme(s->prm.ischm, gam, rho, alf);
+  const eo_grid *g = s->g;
+  eo_boundary(s, s->uo, s->vo, s->wo);
+  eo_boundary_dens(s, s->dens);
+  /* pressure ghosts (:585-617) */
+  int nx = g->nx, ny = g->ny, nz = g->nz;
+  double *p = s->p;
+#define PA(i, j, k) p[(size_t)((i)-1) + (size_t)nx * ((size_t)((j)-1) + (size_t)ny * (size_t)((k)-1))]
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) {
+      if (g->mp == 0) { PA(1, j, k) = PA(g->ix2, j, k); PA(nx, j, k) = PA(g->ix1, j, k); }
+      else { PA(1, j, k) = -PA(g->ix1, j, k); PA(nx, j, k) = -PA(g->ix2, j, k); }
+    }
+  for (int k = 1; k <= nz; k++)
+    for (int i = 1; i <= nx; i++) {
+      if (g->lp == 0) { PA(i, 1, k) = PA(i, g->jy2, k); PA(i, ny, k) = PA(i, g->jy1, k); }
+      else { PA(i, 1, k) = PA(i, g->jy1, k); PA(i, ny, k) = PA(i, g->jy2, k); }
+    }
+  const int *it = s->prm.itype;
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++) {
+      if (it[5] == 500) PA(i, j, 1) = PA(i, j, g->kz2);
+      if (it[6] == 500) PA(i, j, nz) = PA(i, j, g->kz1);
+      if (it[5] != 0 && it[5] != 500) PA(i, j, 1) = PA(i, j, g->kz1);
+      if (it[6] != 0 && it[6] != 500) PA(i, j, nz) = PA(i, j, g->kz2);
+    }
+#undef PA
+  double alfxdt = alf[0] * dtm1;
+  eo_boundinout(s, s->uo, s->vo, s->wo, s->uo, s->vo, s->wo, alfxdt, 1);
+  eo_boundary(s, s->uo, s->vo, s->wo);
+  if (s->prm.idens == 1) eo_boundinoutd(s, s->dens);
+  if (s->prm.isgs != 0) {
+    eo_filtersize(s);
+    eo_turvis(s);
+  }
+}
