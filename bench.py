@@ -1,0 +1,305 @@
+"""Throughput of the fractional-step time advance on B200.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = 3 RK substeps (RHS+predictor, boundary fills, divergence + FFT
+Poisson solve + projection, pressure update, density) + the dynamic eddy
+viscosity update, on the 512x384x256 wake grid (streamwise x vertical x
+periodic), FP64, fields resident on the GPU.  Prints one JSON line.
+N > 1 runs N independent replicas (the solver does not shard; one GPU holds
+the whole domain): value = all ranks' cell-steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s at 512x384x256: plain FP64 vs FP32-refined+MLP closure, equal accuracy"
+UNIT = "Mcell-steps/s"
+
+# algorithmic HBM bytes per interior cell, per launch of each kernel category
+# (compulsory reads + writes of 8-byte fields)
+ALG_BYTES = {
+    "rhs_predictor": 15 * 8,   # R u,v,w,p,rho,nu_t,ua,va,wa  W u*,v*,w*,ua,va,wa
+    "div_fft_fwd": 4 * 8,      # R u*,v*,w*  W spectrum
+    "transform_fwd": 2 * 8,    # R spectrum W spectrum (plus 2*M flops/cell)
+    "z_line_solve": 2 * 8,     # R/W spectrum in place
+    "transform_bwd": 2 * 8,
+    "fft_bwd": 2 * 8,          # R spectrum W dp
+    "correct": 7 * 8,          # R u*,v*,w*,dp  W u,v,w
+    "pressure_update": 3 * 8,  # R p,dp W p
+    "density": 8 * 8,          # R rho,u,v,w,nu_t,rha  W rho,rha
+    "eddy_viscosity": 4 * 8,   # R u,v,w  W nu_t
+}
+OWN = [k for k in ALG_BYTES if not k.startswith("transform")]  # cuBLAS does the transforms
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true", help="tiny grid (profiling / smoke)")
+    return ap.parse_args()
+
+
+def workload(small=False):
+    from eddy_hybrid_b200 import config
+    if small:
+        return config.Workload("wake_64x48x32", mx=48, ly=32, nz_=64, re=1e4, fr=1.0, dt=5e-4,
+                               sphere=False)
+    w = config.wake_512x384x256()
+    w.sphere = False
+    return w
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                smax = float(c[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_baseline(steps=1):
+    """The CPU oracle (restatement of the reference CPU path, FP64, OpenMP
+    over the host cores) on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import eddy_oracle
+    from eddy_hybrid_b200 import config
+    cores = len(os.sched_getaffinity(0))
+    w = config.Workload("wake_sample_256x192x128", mx=192, ly=128, nz_=256, re=1e4, fr=1.0,
+                        dt=5e-4, sphere=False)
+    s = eddy_oracle.OracleSolver(w, threads=cores)
+    s.load_initial(config.initial_fields(w, s.grid.get("dens_bg")[: w.nx]))
+    s.initialize()
+    t0 = time.perf_counter()
+    s.step(steps)
+    dt = time.perf_counter() - t0
+    return {"value": w.ncell * steps / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} full step(s) of a 256x192x128 grid (1/8 of the cells, same "
+                      f"equations and parameters) after initialisation; {dt:.2f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from eddy_hybrid_b200 import config  # noqa: F401
+    for _ in range(args.warmup):
+        cpu_baseline(1)
+    vals = [cpu_baseline(1) for _ in range(args.steps)]
+    v = statistics.mean(x["value"] for x in vals)
+    cb = dict(vals[0])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "wake_512x384x256 (CPU sample, see cpu_baseline)",
+                       "form": "plain FP64 (CPU oracle port of the reference loops)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local, dist = dist_init(args.gpus)
+    import numpy as np
+
+    import eddy_hybrid_b200 as eb
+    from eddy_hybrid_b200 import config
+
+    w = workload(args.small)
+    g = eb.Solver(w, device=local if world > 1 else 0)
+    fields = config.initial_fields(w, g.metric("dens_bg")[: w.nx])
+    g.load_initial(fields)
+    g.initialize()
+    for _ in range(args.warmup):
+        g.step(1)
+    g.sync()
+
+    import torch
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.ExternalStream(g.stream, device=dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local if world > 1 else 0)
+    g.profile_enable(0x7FF)
+    launches0 = g.launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        g.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    launches = g.launches - launches0
+    ms = e0.elapsed_time(e1)
+    prof = g.profile_read()
+    g.profile_enable(0)
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ncell = w.ncell
+    value = world * ncell * args.steps / (ms / 1e3) / 1e6
+
+    # end to end through the public API with host buffers: per step upload the
+    # state from pinned host memory, step, read the state back
+    io = ["uo", "vo", "wo", "p", "dens", "tv"]
+    pinned = {}
+    for n in io:
+        t = torch.empty(w.nx * w.ny * w.nz, dtype=torch.float64, pin_memory=True)
+        a = t.numpy().reshape((w.nx, w.ny, w.nz), order="F")
+        a[...] = g.download(n)
+        pinned[n] = (t, a)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e2.record(stream)
+    for _ in range(args.e2e_steps):
+        for n in io:
+            g.upload(n, pinned[n][1])
+        g.step(1)
+        for n in io:
+            pinned[n][1][...] = g.download(n)
+    e3.record(stream)
+    e3.synchronize()
+    ems = e2.elapsed_time(e3)
+    if dist:
+        t = torch.tensor([ems], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e = world * ncell * args.e2e_steps / (ems / 1e3) / 1e6
+    fbytes = 8 * w.nx * w.ny * w.nz
+
+    # roofline of the dominant kernel among our own
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    dom = max(OWN, key=lambda c: prof[c][0])
+    dms, dn = prof[dom]
+    achieved = ALG_BYTES[dom] * ncell / (dms / dn / 1e3) / 1e9 if dn else None
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(dom)
+    total_ms = sum(v[0] for v in prof.values())
+    kernels = {c: {"ms_per_step": prof[c][0] / args.steps, "launches": prof[c][1],
+                   "share": prof[c][0] / total_ms if total_ms else None,
+                   **({"gbs": ALG_BYTES[c] * ncell / (prof[c][0] / prof[c][1] / 1e3) / 1e9}
+                      if prof[c][1] else {})}
+               for c in prof}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name + " (NZ-2=512 streamwise, NX-2=384 vertical, NY-2=256 periodic)",
+                   "form": "plain FP64", "global_batch": world * ncell, "steps_per_rank": args.steps,
+                   "re": w.re, "fr": w.fr, "dt": w.dt, "sgs": "dynamic (y average)",
+                   "immersed_body": "none (IB forcing not yet on the step)",
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (~15 GB state)"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": len(io) * fbytes,
+                "d2h_bytes_per_step": len(io) * fbytes},
+        "gpu_launches": launches,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_src,
+                     "algorithmic_bytes_per_cell": ALG_BYTES[dom]},
+        "kernels": kernels,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.small:
+        line["cpu_baseline"] = cpu_baseline(1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,240 @@
+"""B200-native fractional-step time advance of the eddy-hybrid LES solver.
+
+Host-side mirror of the reference's Fortran driver over the C ABI in
+include/eddy_b200.h (libeddy_b200.so, built in-tree by
+``eddy_hybrid_b200.build``).  The CUDA library is the only compute path: if
+it cannot be loaded every call raises; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import config  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libeddy_b200.so")
+
+FIELDS = ["uo", "vo", "wo", "p", "dp", "dens", "tv", "us", "vs", "ws", "ua",
+          "va", "wa", "ub", "vb", "wb", "rha", "rhb", "rs", "planeU", "planeV",
+          "planeW", "planeD"]
+FID = {n: i for i, n in enumerate(FIELDS)}
+METRICS = ["xu", "xc", "ap", "au", "av", "aw", "yv", "yc", "bp", "bu", "bv",
+           "bw", "zw", "zc", "cp", "cu", "cv", "cw", "whx", "why", "whz",
+           "dfxu", "dfxw", "dfxul", "dfxwl", "dfxd", "dfxdl", "dens_bg"]
+ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite value",
+          4: "singular system", 5: "refinement did not converge", 6: "timeout",
+          7: "out of memory"}
+PLAIN_FP64, MIXED = 0, 1
+
+
+class EddyError(RuntimeError):
+    pass
+
+
+class Params(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("itype", C.c_int * 7), ("ischm", C.c_int), ("isgs", C.c_int),
+                ("idens", C.c_int), ("ru1", C.c_double), ("prn", C.c_double),
+                ("denP1", C.c_double), ("grav", C.c_double), ("dpdx", C.c_double),
+                ("dpdy", C.c_double), ("dpdz", C.c_double), ("eps", C.c_double),
+                ("css", C.c_double), ("vspngx1", C.c_int), ("dspngx1", C.c_int),
+                ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
+                ("dspngx3in", C.c_int), ("dspngx3out", C.c_int),
+                ("precision", C.c_int), ("refine_sweeps", C.c_int),
+                ("closure", C.c_int)]
+
+
+def make_params(d: dict, precision: int = PLAIN_FP64, refine_sweeps: int = 2,
+                closure: int = 0) -> Params:
+    p = Params()
+    for k, v in d.items():
+        if k == "itype":
+            p.itype = (C.c_int * 7)(0, *v)
+        else:
+            setattr(p, k, v)
+    p.precision = precision
+    p.refine_sweeps = refine_sweeps
+    p.closure = closure
+    return p
+
+
+_lib = None
+_DP = C.POINTER(C.c_double)
+
+# exported symbols and their argument types (must match include/eddy_b200.h)
+SIGNATURES = {
+    "eddy_create": ([C.POINTER(C.c_void_p), C.POINTER(Params), _DP, C.c_double, C.c_double, _DP, C.c_int], C.c_int),
+    "eddy_destroy": ([C.c_void_p], C.c_int),
+    "eddy_upload": ([C.c_void_p, C.c_int, _DP], C.c_int),
+    "eddy_download": ([C.c_void_p, C.c_int, _DP], C.c_int),
+    "eddy_get_metric": ([C.c_void_p, C.c_int, _DP, C.c_int], C.c_int),
+    "eddy_grid_metric": ([C.POINTER(Params), _DP, C.c_double, C.c_double, _DP, C.c_int, _DP, C.c_int], C.c_int),
+    "eddy_rhs_predictord": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
+    "eddy_boundary": ([C.c_void_p, C.c_int], C.c_int),
+    "eddy_boundinout": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
+    "eddy_direct": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_correct": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_pressure_update": ([C.c_void_p], C.c_int),
+    "eddy_density": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
+    "eddy_turvis": ([C.c_void_p], C.c_int),
+    "eddy_initialize": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_substep": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
+    "eddy_step": ([C.c_void_p, C.c_double, C.c_int], C.c_int),
+    "eddy_poisson_solve": ([C.c_void_p, _DP, _DP, C.c_int], C.c_int),
+    "eddy_max_divergence": ([C.c_void_p, _DP], C.c_int),
+    "eddy_profile_enable": ([C.c_void_p, C.c_uint], C.c_int),
+    "eddy_profile_read": ([C.c_void_p, _DP, C.POINTER(C.c_longlong)], C.c_int),
+    "eddy_sync": ([C.c_void_p], C.c_int),
+    "eddy_last_error": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
+    "eddy_launch_count": ([C.c_void_p], C.c_int64),
+    "eddy_stream": ([C.c_void_p], C.c_void_p),
+}
+
+
+def lib():
+    """Load libeddy_b200.so (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EddyError(f"CUDA library not built: {LIB_PATH} (run python -m eddy_hybrid_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    if a.dtype != np.float64:
+        raise TypeError("float64 arrays required")
+    if not (a.flags.f_contiguous or a.ndim == 1):
+        raise ValueError("Fortran-ordered arrays required")
+    return a.ctypes.data_as(_DP)
+
+
+def grid_metric(workload, name: str) -> np.ndarray:
+    """Metric array built by the library's host code (no GPU needed)."""
+    p = make_params(workload.params())
+    xf, zf = workload.faces()
+    xf = np.ascontiguousarray(xf, dtype=np.float64)
+    zf = np.ascontiguousarray(zf, dtype=np.float64)
+    n = 3 * (max(workload.nx, workload.ny, workload.nz) + 2) + workload.nx * workload.ny
+    out = np.zeros(n)
+    m = lib().eddy_grid_metric(C.byref(p), _ptr(xf), workload.ylim[0], workload.ylim[1], _ptr(zf),
+                               METRICS.index(name), _ptr(out), n)
+    if m < 0:
+        raise EddyError("eddy_grid_metric failed")
+    return out[:m].copy()
+
+
+class Solver:
+    """One device-resident solver context (one CUDA stream)."""
+
+    def __init__(self, workload, device: int = 0, precision: int = PLAIN_FP64,
+                 refine_sweeps: int = 2, closure: int = 0):
+        self.w = workload
+        self.params = workload.params()
+        self._p = make_params(self.params, precision, refine_sweeps, closure)
+        xf, zf = workload.faces()
+        xf = np.ascontiguousarray(xf, dtype=np.float64)
+        zf = np.ascontiguousarray(zf, dtype=np.float64)
+        h = C.c_void_p()
+        rc = lib().eddy_create(C.byref(h), C.byref(self._p), _ptr(xf), workload.ylim[0],
+                               workload.ylim[1], _ptr(zf), device)
+        self.h = h
+        self._check(rc, "eddy_create")
+        self.shape = (self.params["nx"], self.params["ny"], self.params["nz"])
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = ""
+            if self.h:
+                buf = C.create_string_buffer(512)
+                lib().eddy_last_error(self.h, buf, 512)
+                msg = buf.value.decode(errors="replace")
+            raise EddyError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")
+
+    def metric(self, name: str) -> np.ndarray:
+        n = 3 * (max(self.shape) + 2) + self.shape[0] * self.shape[1]
+        out = np.zeros(n)
+        m = lib().eddy_get_metric(self.h, METRICS.index(name), _ptr(out), n)
+        if m < 0:
+            raise EddyError("eddy_get_metric failed")
+        return out[:m].copy()
+
+    def upload(self, name: str, a: np.ndarray):
+        a = np.asfortranarray(a, dtype=np.float64)
+        self._check(lib().eddy_upload(self.h, FID[name], _ptr(a)), "eddy_upload")
+
+    def download(self, name: str) -> np.ndarray:
+        shape = self.shape[:2] if name.startswith("plane") else self.shape
+        a = np.zeros(shape, order="F")
+        self._check(lib().eddy_download(self.h, FID[name], _ptr(a)), "eddy_download")
+        return a
+
+    def load_initial(self, fields: dict):
+        for k, v in fields.items():
+            self.upload(k, v)
+
+    def initialize(self):
+        self._check(lib().eddy_initialize(self.h, self.w.dt), "eddy_initialize")
+
+    def step(self, nsteps: int = 1, dt: float | None = None):
+        self._check(lib().eddy_step(self.h, self.w.dt if dt is None else dt, nsteps), "eddy_step")
+
+    def substep(self, is_: int, dt: float | None = None):
+        self._check(lib().eddy_substep(self.h, is_, self.w.dt if dt is None else dt), "eddy_substep")
+
+    def call(self, name: str, *args):
+        self._check(getattr(lib(), name)(self.h, *args), name)
+
+    def poisson_solve(self, rhs: np.ndarray) -> np.ndarray:
+        rhs = np.asfortranarray(rhs, dtype=np.float64)
+        out = np.zeros(self.shape, order="F")
+        self._check(lib().eddy_poisson_solve(self.h, _ptr(rhs), _ptr(out), 0), "eddy_poisson_solve")
+        return out
+
+    def max_divergence(self) -> float:
+        v = C.c_double(0.0)
+        self._check(lib().eddy_max_divergence(self.h, C.byref(v)), "eddy_max_divergence")
+        return v.value
+
+    PROFILE_CATEGORIES = ["rhs_predictor", "boundary", "div_fft_fwd", "transform_fwd",
+                          "z_line_solve", "transform_bwd", "fft_bwd", "correct",
+                          "pressure_update", "density", "eddy_viscosity"]
+
+    def profile_enable(self, mask: int = 0x7FF):
+        self._check(lib().eddy_profile_enable(self.h, mask), "eddy_profile_enable")
+
+    def profile_read(self) -> dict:
+        ms = (C.c_double * 11)()
+        n = (C.c_longlong * 11)()
+        self._check(lib().eddy_profile_read(self.h, ms, n), "eddy_profile_read")
+        return {c: (ms[i], n[i]) for i, c in enumerate(self.PROFILE_CATEGORIES)}
+
+    def sync(self):
+        self._check(lib().eddy_sync(self.h), "eddy_sync")
+
+    @property
+    def launches(self) -> int:
+        return int(lib().eddy_launch_count(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().eddy_stream(self.h) or 0)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().eddy_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

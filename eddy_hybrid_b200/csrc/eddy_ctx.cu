@@ -1,0 +1,574 @@
+// eddy_ctx.cu -- context, metrics, field storage, and the C ABI entry points
+// (include/eddy_b200.h).  The driver sequence in eddy_substep/eddy_step is
+// the time loop of src/Eddy6.f:2095-3049 (ibm=0, explicit viscous terms).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "eddy_internal.h"
+
+int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, double sgn, int zero);
+
+namespace {
+
+// Metric arrays from face coordinates, src/grid.f:21-173 (igrid=1, uniform y,
+// kgrid=1); index bounds src/setup.f:2-75; sponge src/Initialize.f:129-271.
+void build_metrics(eddy_ctx *ctx, const double *xf, double ymin, double ymax, const double *zf) {
+  const eddy_params &p = ctx->prm;
+  int nx = p.nx, ny = p.ny, nz = p.nz;
+  for (int a = 0; a < 28; a++) ctx->h[a].clear();
+  auto arr = [&](int id, int n) -> std::vector<double> & {
+    ctx->h[id].assign((size_t)n + 2, 0.0);
+    return ctx->h[id];
+  };
+  auto &xu = arr(0, nx), &xc = arr(1, nx), &ap = arr(2, nx), &au = arr(3, nx), &av = arr(4, nx), &aw = arr(5, nx);
+  auto &yv = arr(6, ny), &yc = arr(7, ny), &bp = arr(8, ny), &bu = arr(9, ny), &bv = arr(10, ny), &bw = arr(11, ny);
+  auto &zw = arr(12, nz), &zc = arr(13, nz), &cp = arr(14, nz), &cu = arr(15, nz), &cv = arr(16, nz),
+       &cw = arr(17, nz);
+  int ix1 = 2, ix2 = nx - 1;
+  for (int i = 1; i <= ix2; i++) xu[i] = xf[i - 1];
+  xu[nx] = 2. * xu[ix2] - xu[ix2 - 1];
+  for (int i = ix1; i <= ix2; i++) xc[i] = .5 * (xu[i - 1] + xu[i]);
+  xc[1] = 2. * xu[1] - xc[2];
+  xc[nx] = 2. * xu[ix2] - xc[ix2];
+  for (int i = ix1; i <= ix2; i++) au[i] = 2. / (xu[i + 1] - xu[i - 1]);
+  au[1] = 2. / (-3. * xu[1] + 4. * xu[2] - xu[3]);
+  au[ix2] = 2. / (3. * xu[ix2] - 4. * xu[ix2 - 1] + xu[ix2 - 2]);
+  au[nx] = au[ix2];
+  for (int i = ix1; i <= ix2; i++) ap[i] = 1. / (xu[i] - xu[i - 1]);
+  ap[1] = ap[ix1];
+  ap[nx] = ap[ix2];
+  for (int i = ix1; i <= ix2; i++) av[i] = 2. / (xc[i + 1] - xc[i - 1]);
+  av[1] = 2. / (-3. * xc[1] + 4. * xc[2] - xc[3]);
+  av[nx] = 2. / (3. * xc[nx] - 4. * xc[nx - 1] + xc[nx - 2]);
+  for (int i = 1; i <= nx; i++) aw[i] = av[i];
+  int jy1 = 2, jy2 = ny - 1;
+  double dely = (ymax - ymin) / (double)(ny - 2), rdely = 1. / dely;
+  for (int j = 1; j <= ny; j++) {
+    yv[j] = (double)(j - 1) * dely + ymin;
+    bp[j] = bu[j] = bv[j] = bw[j] = rdely;
+  }
+  ctx->dely = dely;
+  ctx->delysq = dely * dely;
+  for (int j = jy1; j <= jy2; j++) yc[j] = 0.5 * (yv[j] + yv[j - 1]);
+  yc[1] = 2. * yv[1] - yc[jy1];
+  yc[jy2 + 1] = 2. * yv[jy2] - yc[jy2];
+  int kz1 = 2, kz2 = nz - 1;
+  for (int k = 1; k <= kz2; k++) zw[k] = zf[k - 1];
+  zw[nz] = 2. * zw[kz2] - zw[kz2 - 1];
+  for (int k = kz1; k <= kz2; k++) zc[k] = .5 * (zw[k - 1] + zw[k]);
+  zc[1] = 2. * zw[1] - zc[2];
+  zc[nz] = 2. * zw[kz2] - zc[kz2];
+  for (int k = kz1; k <= kz2; k++) cw[k] = 2. / (zw[k + 1] - zw[k - 1]);
+  cw[1] = 2. / (-3. * zw[1] + 4. * zw[2] - zw[3]);
+  cw[kz2] = 2. / (3. * zw[kz2] - 4. * zw[kz2 - 1] + zw[kz2 - 2]);
+  cw[nz] = 0.;  // grid.f:112 copies the not yet filled COMMON cw(kz2)
+  for (int k = kz1; k <= kz2; k++) cp[k] = 1. / (zw[k] - zw[k - 1]);
+  cp[1] = cp[kz1];
+  cp[nz] = cp[kz2];
+  for (int k = kz1; k <= kz2; k++) cv[k] = 2. / (zc[k + 1] - zc[k - 1]);
+  cv[1] = 2. / (-3. * zc[1] + 4. * zc[2] - zc[3]);
+  cv[nz] = 2. / (3. * zc[nz] - 4. * zc[nz - 1] + zc[nz - 2]);
+  for (int k = 1; k <= nz; k++) cu[k] = cv[k];
+
+  Dims &d = ctx->d;
+  d.nx = nx; d.ny = ny; d.nz = nz;
+  d.ix1 = ix1; d.ix2 = ix2; d.jy1 = jy1; d.jy2 = jy2; d.kz1 = kz1; d.kz2 = kz2;
+  for (int b = 0; b < 7; b++) d.itype[b] = p.itype[b];
+  d.ibu = ix1;
+  d.ieu = p.itype[2] == 500 ? ix2 : ix2 - 1;
+  d.jbv = jy1;
+  d.jev = p.itype[4] == 500 ? jy2 : jy2 - 1;
+  d.kbw = kz1;
+  d.kew = (p.itype[6] == 500 || p.itype[6] == 0) ? kz2 : kz2 - 1;
+  d.mp = p.itype[2] == 500 ? 0 : 1;
+  d.lp = p.itype[4] == 500 ? 0 : 1;
+  d.np = p.itype[6] == 500 ? 0 : 1;
+  d.ncell = (long long)nx * ny * nz;
+
+  // filter weights (vt.f:1374-1434)
+  auto &whx = ctx->h[18], &why = ctx->h[19], &whz = ctx->h[20];
+  whx.assign((size_t)3 * (nx + 1), 0.0);
+  why.assign((size_t)3 * (ny + 1), 0.0);
+  whz.assign((size_t)3 * (nz + 1), 0.0);
+#define WH(a, i, dd) a[(size_t)((i)*3 + (dd) + 1)]
+  for (int i = ix1; i <= ix2; i++) WH(whx, i, 0) = 0.50;
+  for (int i = ix1 + 1; i <= ix2 - 1; i++) {
+    WH(whx, i, -1) = 0.25 * av[i] / au[i];
+    WH(whx, i, 1) = 0.25 * av[i] / au[i - 1];
+  }
+  WH(whx, ix1, -1) = 0.50 * av[ix1 + 1] / au[ix1] + 0.25 * av[ix1 + 1] / au[ix1 + 1];
+  WH(whx, ix1, 1) = -0.25 * av[ix1 + 1] / au[ix1];
+  WH(whx, ix2, -1) = 0.50 * av[ix2 - 1] / au[ix2 - 1] + 0.25 * av[ix2 - 1] / au[ix2 - 2];
+  WH(whx, ix2, 1) = -0.25 * av[ix2 - 1] / au[ix2 - 1];
+  for (int j = jy1; j <= jy2; j++) WH(why, j, 0) = 0.50;
+  for (int j = jy1 + 1; j <= jy2 - 1; j++) {
+    WH(why, j, -1) = 0.25 * bw[j] / bv[j];
+    WH(why, j, 1) = 0.25 * bw[j] / bv[j - 1];
+  }
+  WH(why, jy1, -1) = 0.50 * bw[jy1 + 1] / bv[jy1] + 0.25 * bw[jy1 + 1] / bv[jy1 + 1];
+  WH(why, jy1, 1) = -0.25 * bw[jy1 + 1] / bv[jy1];
+  WH(why, jy2, -1) = 0.50 * bw[jy2 - 1] / bv[jy2 - 1] + 0.25 * bw[jy2 - 1] / bv[jy2 - 2];
+  WH(why, jy2, 1) = -0.25 * bw[jy2 - 1] / bv[jy2 - 1];
+  for (int k = kz1; k <= kz2; k++) {
+    WH(whz, k, 0) = 0.50;
+    WH(whz, k, -1) = 0.25 * cu[k] / cw[k];
+    WH(whz, k, 1) = 0.25 * cu[k] / cw[k - 1];
+  }
+  if (p.itype[5] != 0) {
+    WH(whz, kz1, -1) = 0.50 * cu[kz1 + 1] / cw[kz1] + 0.25 * cu[kz1 + 1] / cw[kz1 + 1];
+    WH(whz, kz1, 1) = -0.25 * cu[kz1 + 1] / cw[kz1];
+  }
+  if (p.itype[6] != 0) {
+    WH(whz, kz2, -1) = 0.50 * cu[kz2 - 1] / cw[kz2 - 1] + 0.25 * cu[kz2 - 1] / cw[kz2 - 2];
+    WH(whz, kz2, 1) = -0.25 * cu[kz2 - 1] / cw[kz2 - 1];
+  }
+#undef WH
+  // sponges
+  auto &dfxu = arr(21, nx), &dfxw = arr(22, nx), &dfxul = arr(23, nz), &dfxwl = arr(24, nz), &dfxd = arr(25, nx),
+       &dfxdl = arr(26, nz);
+  int ibu = d.ibu, ieu = d.ieu, nzg = nz;
+  int vx1 = p.vspngx1, vin = p.vspngx3in, vout = p.vspngx3out, dx1 = p.dspngx1, din = p.dspngx3in,
+      dout = p.dspngx3out;
+  for (int i = ibu; i <= ieu; i++) {
+    dfxu[i] = 0.0;
+    if (i >= ieu - vx1 && vx1 > 0) {
+      double r = (xu[i] - xu[ieu - vx1]) / (xu[ieu] - xu[ieu - vx1]);
+      dfxu[i] = 5.0 * (r * r);
+    }
+  }
+  for (int i = ix1; i <= ix2; i++) {
+    dfxw[i] = 0.0;
+    if (i >= ix2 - vx1 && vx1 > 0) {
+      double r = (xc[i] - xc[ix2 - vx1]) / (xc[ix2] - xc[ix2 - vx1]);
+      dfxw[i] = 5.0 * (r * r);
+    }
+  }
+  std::vector<double> dfxug(nzg + 2, 0.), dfxwg(nzg + 2, 0.), dfxdg(nzg + 2, 0.);
+  for (int k = nzg; k >= 1; k--) {
+    if (k <= vin + 1 && vin > 0) {
+      double r = (zc[k] - zc[vin + 1]) / (zc[2] - zc[vin + 1]);
+      dfxug[k] = 20.0 * (r * r);
+      double r2 = (zw[k] - zw[vin + 1]) / (zw[2] - zw[vin + 1]);
+      dfxwg[k] = 20.0 * (r2 * r2);
+    }
+  }
+  for (int k = 1; k <= nzg; k++) {
+    if (k >= nzg - vout && vout > 0) {
+      double r = (zc[k - 2] - zc[nzg - vout]) / (zc[nzg - 2] - zc[nzg - dout]);
+      dfxug[k] = 10.0 * (r * r);
+      double r2 = (zw[k - 2] - zw[nzg - dout]) / (zw[nzg - 2] - zw[nzg - dout]);
+      dfxwg[k] = 10.0 * (r2 * r2);
+    }
+  }
+  int ivs = 0;
+  for (int k = kz1; k <= kz2; k++) {
+    dfxul[k] = dfxug[k];
+    dfxwl[k] = dfxwg[k];
+    if (dfxwl[k] > 0.0) ivs = 1;
+  }
+  for (int k = 1; k <= nzg; k++)
+    if (k >= nzg - dout && dout > 0) {
+      double r = (zc[k - 2] - zc[nzg - dout]) / (zc[nzg - 2] - zc[nzg - dout]);
+      dfxdg[k] = 100.0 * (r * r);
+    }
+  for (int k = nzg; k >= 1; k--)
+    if (k <= din + 1 && din > 0) {
+      double r = (zc[k] - zc[din + 1]) / (zc[2] - zc[din + 1]);
+      dfxdg[k] = 100.0 * (r * r);
+    }
+  int ids = 0;
+  for (int k = kz1; k <= kz2; k++) {
+    dfxdl[k] = dfxdg[k];
+    if (dfxdl[k] > 0.0) ids = 1;
+  }
+  for (int i = ibu; i <= ieu; i++)
+    if (i >= ieu - dx1 && dx1 > 0) {
+      double r = (xc[i] - xc[ieu - dx1]) / (xc[ieu] - xc[ieu - dx1]);
+      dfxd[i] = 5.0 * (r * r);
+    }
+  // background density (Cartesian vertical = x)
+  auto &dbg = ctx->h[27];
+  dbg.assign((size_t)nx * ny, 0.0);
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++) dbg[(size_t)(i - 1) + (size_t)nx * (j - 1)] = p.denP1 * xc[i];
+
+  Scalars &s = ctx->sc;
+  s.ru1 = p.ru1; s.prn = p.prn; s.grav = p.grav; s.dpdx = p.dpdx; s.dpdy = p.dpdy; s.dpdz = p.dpdz;
+  s.eps = p.eps; s.css = p.css; s.vspngx1 = p.vspngx1; s.dspngx1 = p.dspngx1;
+  s.ivspngl = ivs; s.idspngl = ids; s.idens = p.idens; s.isgs = p.isgs;
+}
+
+int upload_metrics(eddy_ctx *ctx) {
+  double **dst[] = {nullptr, nullptr, &ctx->m.ap, &ctx->m.au, &ctx->m.av, &ctx->m.aw, nullptr, nullptr,
+                    &ctx->m.bp, &ctx->m.bu, &ctx->m.bv, &ctx->m.bw, nullptr, nullptr, &ctx->m.cp, &ctx->m.cu,
+                    &ctx->m.cv, &ctx->m.cw, &ctx->m.whx, &ctx->m.why, &ctx->m.whz, &ctx->m.dfxu, &ctx->m.dfxw,
+                    &ctx->m.dfxul, &ctx->m.dfxwl, &ctx->m.dfxd, &ctx->m.dfxdl, &ctx->m.dens_bg};
+  for (int a = 0; a < 28; a++) {
+    if (!dst[a]) continue;
+    size_t b = sizeof(double) * ctx->h[a].size();
+    EDDY_CUDA(cudaMalloc(dst[a], b));
+    EDDY_CUDA(cudaMemcpy(*dst[a], ctx->h[a].data(), b, cudaMemcpyHostToDevice));
+  }
+  return EDDY_OK;
+}
+
+void free_all(eddy_ctx *ctx) {
+  DevMetrics &m = ctx->m;
+  double *mp[] = {m.ap, m.au, m.av, m.aw, m.bp, m.bu, m.bv, m.bw, m.cp, m.cu, m.cv, m.cw, m.whx, m.why, m.whz,
+                  m.dfxu, m.dfxw, m.dfxul, m.dfxwl, m.dfxd, m.dfxdl, m.dens_bg};
+  for (double *p : mp) if (p) cudaFree(p);
+  for (int f = 0; f < EDDY_NFIELDS; f++) if (ctx->f[f]) cudaFree(ctx->f[f]);
+  double *o[] = {ctx->dens_alt, ctx->uc, ctx->vc, ctx->wc, ctx->sij, ctx->gs, ctx->mm, ctx->lm, ctx->dxdydz,
+                 ctx->ilm2, ctx->imm2, ctx->scal};
+  for (double *p : o) if (p) cudaFree(p);
+  poisson_plan_destroy(ctx);
+  for (ProfEvent &e : ctx->prof_ev) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  for (ProfEvent &e : ctx->prof_pool) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  if (ctx->blas) cublasDestroy(ctx->blas);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+}
+
+int check_ctx(eddy_ctx *ctx) { return ctx ? EDDY_OK : EDDY_EINVAL; }
+
+void scheme(int ischm, double gam[3], double rho[3], double alf[3]) {
+  if (ischm == 1) {
+    gam[0] = 1.5; gam[1] = 0.; gam[2] = 0.;
+    rho[0] = -0.5; rho[1] = 0.; rho[2] = 0.;
+  } else {
+    gam[0] = 8. / 15.; gam[1] = 5. / 12.; gam[2] = 3. / 4.;
+    rho[0] = 0.; rho[1] = -17. / 60.; rho[2] = -5. / 12.;
+  }
+  for (int q = 0; q < 3; q++) alf[q] = gam[q] + rho[q];
+}
+
+}  // namespace
+
+extern "C" {
+
+int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, double ymin, double ymax,
+                const double *zw_faces, int device) {
+  if (!out || !prm || !xu_faces || !zw_faces) return EDDY_EINVAL;
+  *out = nullptr;
+  eddy_ctx *ctx = new (std::nothrow) eddy_ctx();
+  if (!ctx) return EDDY_ENOMEM;
+  ctx->prm = *prm;
+  const eddy_params &p = *prm;
+  auto fail = [&](int rc, const char *msg) {
+    if (msg) ctx->err = msg;
+    *out = ctx;  // keep the context so the caller can read the message
+    return rc;
+  };
+  if (p.nx < 6 || p.ny < 4 || p.nz < 6) return fail(EDDY_EINVAL, "grid too small (need NX,NZ >= 6, NY >= 4)");
+  if (p.ischm != 3 && p.ischm != 1) return fail(EDDY_EINVAL, "ischm must be 1 or 3");
+  if (p.isgs != 0 && p.isgs != 1 && p.isgs != 2)
+    return fail(EDDY_EINVAL, "only isgs 0 (none), 1 (Smagorinsky), 2 (dynamic, y average) are supported");
+  if (p.itype[3] != 500 || p.itype[4] != 500) return fail(EDDY_EINVAL, "y (ITYPE 3/4) must be periodic (500)");
+  for (int b = 1; b <= 2; b++)
+    if (p.itype[b] != 60 && p.itype[b] != 82) return fail(EDDY_EINVAL, "x boundaries must be type 60 or 82");
+  if (p.itype[5] != 305 || (p.itype[6] != 730))
+    return fail(EDDY_EINVAL, "z boundaries must be the hybrid inlet 305 and the convective outlet 730");
+  if (p.precision != EDDY_PLAIN_FP64) return fail(EDDY_EINVAL, "mixed precision form not available in this build");
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(EDDY_ECUDA, "cudaStreamCreate failed");
+  if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(EDDY_ECUDA, "cublasCreate failed");
+  cublasSetStream(ctx->blas, ctx->stream);
+  cublasSetMathMode(ctx->blas, CUBLAS_DEFAULT_MATH);
+  build_metrics(ctx, xu_faces, ymin, ymax, zw_faces);
+  int rc = upload_metrics(ctx);
+  if (rc) return fail(rc, nullptr);
+  size_t n3 = sizeof(double) * (size_t)ctx->d.ncell, n2 = sizeof(double) * (size_t)p.nx * p.ny;
+  for (int f = 0; f < EDDY_NFIELDS; f++) {
+    size_t b = (f >= EDDY_PLANEU) ? n2 : n3;
+    if (cudaMalloc(&ctx->f[f], b) != cudaSuccess) return fail(EDDY_ENOMEM, "device allocation failed");
+    cudaMemset(ctx->f[f], 0, b);
+  }
+  double **o[] = {&ctx->dens_alt, &ctx->uc, &ctx->vc, &ctx->wc, &ctx->gs, &ctx->mm, &ctx->lm, &ctx->dxdydz};
+  for (double **pp : o) {
+    if (cudaMalloc(pp, n3) != cudaSuccess) return fail(EDDY_ENOMEM, "device allocation failed");
+    cudaMemset(*pp, 0, n3);
+  }
+  if (cudaMalloc(&ctx->sij, 6 * n3) != cudaSuccess) return fail(EDDY_ENOMEM, "device allocation failed");
+  cudaMemset(ctx->sij, 0, 6 * n3);
+  size_t n2xz = sizeof(double) * (size_t)p.nx * p.nz;
+  if (cudaMalloc(&ctx->ilm2, n2xz) != cudaSuccess || cudaMalloc(&ctx->imm2, n2xz) != cudaSuccess)
+    return fail(EDDY_ENOMEM, "device allocation failed");
+  cudaMemset(ctx->ilm2, 0, n2xz);
+  cudaMemset(ctx->imm2, 0, n2xz);
+  if (cudaMalloc(&ctx->scal, sizeof(double) * 32) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
+  cudaMemset(ctx->scal, 0, sizeof(double) * 32);
+  rc = poisson_plan_create(ctx);
+  if (rc) return fail(rc, nullptr);
+  if (p.isgs != 0) {
+    rc = launch_filtersize(ctx);
+    if (rc) return fail(rc, nullptr);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(EDDY_ECUDA, "device error during set-up");
+  *out = ctx;
+  return EDDY_OK;
+}
+
+int eddy_destroy(eddy_ctx *ctx) {
+  if (!ctx) return EDDY_OK;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+  return EDDY_OK;
+}
+
+int eddy_upload(eddy_ctx *ctx, int field, const double *host) {
+  if (check_ctx(ctx) || field < 0 || field >= EDDY_NFIELDS || !host) return EDDY_EINVAL;
+  size_t b = sizeof(double) * (field >= EDDY_PLANEU ? (size_t)ctx->d.nx * ctx->d.ny : (size_t)ctx->d.ncell);
+  EDDY_CUDA(cudaMemcpyAsync(ctx->f[field], host, b, cudaMemcpyHostToDevice, ctx->stream));
+  if (field == EDDY_DENS) EDDY_CUDA(cudaMemcpyAsync(ctx->dens_alt, host, b, cudaMemcpyHostToDevice, ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EDDY_OK;
+}
+
+int eddy_download(eddy_ctx *ctx, int field, double *host) {
+  if (check_ctx(ctx) || field < 0 || field >= EDDY_NFIELDS || !host) return EDDY_EINVAL;
+  size_t b = sizeof(double) * (field >= EDDY_PLANEU ? (size_t)ctx->d.nx * ctx->d.ny : (size_t)ctx->d.ncell);
+  EDDY_CUDA(cudaMemcpyAsync(host, ctx->f[field], b, cudaMemcpyDeviceToHost, ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EDDY_OK;
+}
+
+int eddy_get_metric(eddy_ctx *ctx, int which, double *out, int n) {
+  if (check_ctx(ctx) || which < 0 || which >= 28 || !out) return -1;
+  const std::vector<double> &h = ctx->h[which];
+  int off = (which >= 18 && which <= 20) || which == 27 ? 0 : 1;
+  int len = (int)h.size() - (off ? 2 : 0);
+  if (which >= 18 && which <= 20) len = (int)h.size();
+  if (n < len) return -2;
+  std::memcpy(out, h.data() + off, sizeof(double) * (size_t)len);
+  return len;
+}
+
+int eddy_grid_metric(const eddy_params *prm, const double *xu_faces, double ymin, double ymax,
+                     const double *zw_faces, int which, double *out, int n) {
+  if (!prm || !xu_faces || !zw_faces || !out || which < 0 || which >= 28) return -1;
+  if (prm->nx < 6 || prm->ny < 4 || prm->nz < 6) return -1;
+  eddy_ctx tmp;
+  tmp.prm = *prm;
+  build_metrics(&tmp, xu_faces, ymin, ymax, zw_faces);
+  return eddy_get_metric(&tmp, which, out, n);
+}
+
+int eddy_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  return launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt);
+}
+
+int eddy_boundary(eddy_ctx *ctx, int set) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  double **f = ctx->f;
+  if (set == 0) return launch_boundary(ctx, f[EDDY_US], f[EDDY_VS], f[EDDY_WS]);
+  return launch_boundary(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO]);
+}
+
+int eddy_boundinout(eddy_ctx *ctx, int idiv, double alfxdt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  double **f = ctx->f;
+  if (idiv == 1)
+    return launch_boundinout(ctx, f[EDDY_US], f[EDDY_VS], f[EDDY_WS], f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], alfxdt, 1);
+  return launch_boundinout(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_US], f[EDDY_VS], f[EDDY_WS], alfxdt, 0);
+}
+
+int eddy_direct(eddy_ctx *ctx, double alfxdt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  return launch_direct(ctx, ctx->f[EDDY_US], ctx->f[EDDY_VS], ctx->f[EDDY_WS], alfxdt);
+}
+
+int eddy_correct(eddy_ctx *ctx, double alfxdt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  return launch_correct(ctx, alfxdt);
+}
+
+int eddy_pressure_update(eddy_ctx *ctx) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  return launch_pressure_update(ctx);
+}
+
+int eddy_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  if (ctx->prm.idens != 1) return EDDY_OK;
+  return launch_density(ctx, alfxdt, gamxdt, rhoxdt);
+}
+
+int eddy_turvis(eddy_ctx *ctx) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  if (ctx->prm.isgs == 0) return EDDY_OK;
+  return launch_turvis(ctx);
+}
+
+int eddy_initialize(eddy_ctx *ctx, double dt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  const Dims &d = ctx->d;
+  double **f = ctx->f;
+  int rc;
+  if ((rc = launch_boundary(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO]))) return rc;
+  // BOUNDARY_DENS alone (the inlet plane is applied after BOUNDINOUT below)
+  double *dn = f[EDDY_DENS];
+  if (d.itype[3] == 500) {
+    if ((rc = launch_fill_plane(ctx, dn, 1, 1, d.jy2, 1., 0))) return rc;
+    if ((rc = launch_fill_plane(ctx, dn, 1, d.ny, d.jy1, 1., 0))) return rc;
+  }
+  // pressure ghosts (src/Eddy6.f:585-617)
+  double *p = f[EDDY_P];
+  double sx = d.mp == 0 ? 1. : -1.;
+  if ((rc = launch_fill_plane(ctx, p, 0, 1, d.mp == 0 ? d.ix2 : d.ix1, sx, 0))) return rc;
+  if ((rc = launch_fill_plane(ctx, p, 0, d.nx, d.mp == 0 ? d.ix1 : d.ix2, sx, 0))) return rc;
+  if ((rc = launch_fill_plane(ctx, p, 1, 1, d.lp == 0 ? d.jy2 : d.jy1, 1., 0))) return rc;
+  if ((rc = launch_fill_plane(ctx, p, 1, d.ny, d.lp == 0 ? d.jy1 : d.jy2, 1., 0))) return rc;
+  if ((rc = launch_fill_plane(ctx, p, 2, 1, d.kz1, 1., 0))) return rc;
+  if ((rc = launch_fill_plane(ctx, p, 2, d.nz, d.kz2, 1., 0))) return rc;
+  double gam[3], rho[3], alf[3];
+  scheme(ctx->prm.ischm, gam, rho, alf);
+  if ((rc = launch_boundinout(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_UO], f[EDDY_VO], f[EDDY_WO],
+                              alf[0] * dt, 1)))
+    return rc;
+  if ((rc = launch_boundary(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO]))) return rc;
+  if (ctx->prm.idens == 1) {
+    // BOUNDINOUTD only (src/Eddy6.f:757)
+    if (d.itype[5] == 305) {
+      EDDY_CUDA(cudaMemcpyAsync(dn, f[EDDY_PLANED], sizeof(double) * d.nx * d.ny, cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+      if ((rc = launch_fill_plane(ctx, dn, 2, 2, 1, 1., 0))) return rc;
+    }
+    if (d.itype[6] == 730) {
+      if ((rc = launch_fill_plane(ctx, dn, 2, d.kz2, d.kz2 - 1, 1., 0))) return rc;
+      if ((rc = launch_fill_plane(ctx, dn, 2, d.nz, d.kz2, 1., 0))) return rc;
+    }
+    EDDY_CUDA(cudaMemcpyAsync(ctx->dens_alt, dn, sizeof(double) * d.ncell, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  if (ctx->prm.isgs != 0 && (rc = launch_turvis(ctx))) return rc;
+  return EDDY_OK;
+}
+
+int eddy_substep(eddy_ctx *ctx, int is, double dt) {
+  if (check_ctx(ctx) || is < 0 || is > 2) return EDDY_EINVAL;
+  double gam[3], rho[3], alf[3];
+  scheme(ctx->prm.ischm, gam, rho, alf);
+  double alfxdt = alf[is] * dt, gamxdt = gam[is] * dt, rhoxdt = rho[is] * dt;
+  double **f = ctx->f;
+  int rc;
+  {
+    ProfScope ps(ctx, PROF_RHS_PRED);
+    if ((rc = launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt))) return rc;
+  }
+  {
+    ProfScope ps(ctx, PROF_BC);
+    if ((rc = launch_boundary(ctx, f[EDDY_US], f[EDDY_VS], f[EDDY_WS]))) return rc;
+    if ((rc = launch_boundinout(ctx, f[EDDY_US], f[EDDY_VS], f[EDDY_WS], f[EDDY_UO], f[EDDY_VO], f[EDDY_WO],
+                                alfxdt, 1)))
+      return rc;
+    if ((rc = launch_boundary(ctx, f[EDDY_US], f[EDDY_VS], f[EDDY_WS]))) return rc;
+  }
+  if ((rc = launch_direct(ctx, f[EDDY_US], f[EDDY_VS], f[EDDY_WS], alfxdt))) return rc;
+  {
+    ProfScope ps(ctx, PROF_CORRECT);
+    if ((rc = launch_correct(ctx, alfxdt))) return rc;
+  }
+  {
+    ProfScope ps(ctx, PROF_BC);
+    if ((rc = launch_boundary(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO]))) return rc;
+    if ((rc = launch_boundinout(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_US], f[EDDY_VS], f[EDDY_WS],
+                                alfxdt, 0)))
+      return rc;
+    if ((rc = launch_boundary(ctx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO]))) return rc;
+  }
+  {
+    ProfScope ps(ctx, PROF_PUPDATE);
+    if ((rc = launch_pressure_update(ctx))) return rc;
+  }
+  if (ctx->prm.idens == 1) {
+    ProfScope ps(ctx, PROF_DENSITY);
+    if ((rc = launch_density(ctx, alfxdt, gamxdt, rhoxdt))) return rc;
+  }
+  return EDDY_OK;
+}
+
+int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
+  if (check_ctx(ctx) || nsteps < 0) return EDDY_EINVAL;
+  int nsub = ctx->prm.ischm == 1 ? 1 : 3;
+  for (int n = 0; n < nsteps; n++) {
+    for (int is = 0; is < nsub; is++) {
+      int rc = eddy_substep(ctx, is, dt);
+      if (rc) return rc;
+    }
+    if (ctx->prm.isgs != 0) {
+      ProfScope ps(ctx, PROF_TURVIS);
+      int rc = launch_turvis(ctx);
+      if (rc) return rc;
+    }
+  }
+  return EDDY_OK;
+}
+
+int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_device) {
+  if (check_ctx(ctx) || !rhs || !sol) return EDDY_EINVAL;
+  size_t b = sizeof(double) * (size_t)ctx->d.ncell;
+  if (on_device) return launch_poisson_rhs(ctx, rhs, sol);
+  // host arrays: stage through DP / US on the device
+  EDDY_CUDA(cudaMemcpyAsync(ctx->f[EDDY_US], rhs, b, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = launch_poisson_rhs(ctx, ctx->f[EDDY_US], ctx->f[EDDY_DP]);
+  if (rc) return rc;
+  EDDY_CUDA(cudaMemcpyAsync(sol, ctx->f[EDDY_DP], b, cudaMemcpyDeviceToHost, ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EDDY_OK;
+}
+
+int eddy_max_divergence(eddy_ctx *ctx, double *out) {
+  if (check_ctx(ctx) || !out) return EDDY_EINVAL;
+  return launch_max_divergence(ctx, out);
+}
+
+int eddy_profile_enable(eddy_ctx *ctx, unsigned mask) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (ProfEvent &e : ctx->prof_ev) ctx->prof_pool.push_back(e);
+  ctx->prof_ev.clear();
+  ctx->prof_mask = mask;
+  for (int c = 0; c < PROF_NCAT; c++) { ctx->prof_ms[c] = 0.; ctx->prof_n[c] = 0; }
+  return EDDY_OK;
+}
+
+int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (ProfEvent &e : ctx->prof_ev) {
+    float t = 0.f;
+    EDDY_CUDA(cudaEventElapsedTime(&t, e.a, e.b));
+    ctx->prof_ms[e.cat] += t;
+    ctx->prof_n[e.cat] += 1;
+    ctx->prof_pool.push_back(e);
+  }
+  ctx->prof_ev.clear();
+  for (int c = 0; c < PROF_NCAT; c++) {
+    if (ms) ms[c] = ctx->prof_ms[c];
+    if (counts) counts[c] = ctx->prof_n[c];
+  }
+  return EDDY_OK;
+}
+
+int eddy_sync(eddy_ctx *ctx) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EDDY_OK;
+}
+
+int eddy_last_error(eddy_ctx *ctx, char *buf, int len) {
+  if (!ctx || !buf || len <= 0) return EDDY_EINVAL;
+  std::snprintf(buf, (size_t)len, "%s", ctx->err.c_str());
+  return EDDY_OK;
+}
+
+int64_t eddy_launch_count(eddy_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+void *eddy_stream(eddy_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+// eddy_internal.h -- context layout and kernel launch declarations shared by
+// the CUDA translation units of libeddy_b200.so.
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/eddy_b200.h"
+
+// 1-D metric arrays on the device, indexed 1-based like the Fortran
+// (entry 0 unused), sizes nx+2 / ny+2 / nz+2.
+struct DevMetrics {
+  double *ap, *au, *av, *aw;
+  double *bp, *bu, *bv, *bw;
+  double *cp, *cu, *cv, *cw;
+  double *whx, *why, *whz;  // [i*3 + d+1]
+  double *dfxu, *dfxw, *dfxul, *dfxwl, *dfxd, *dfxdl;
+  double *dens_bg;  // (NX,NY)
+};
+
+// Integer bounds (src/setup.f, src/inpall.f:166-172) and scalars the kernels
+// read; passed by value.
+struct Dims {
+  int nx, ny, nz;
+  int ix1, ix2, jy1, jy2, kz1, kz2;
+  int ibu, ieu, jbv, jev, kbw, kew;
+  int mp, lp, np;
+  int itype[7];
+  long long ncell;  // nx*ny*nz
+};
+
+struct Scalars {
+  double ru1, prn, grav, dpdx, dpdy, dpdz, eps, css;
+  int vspngx1, dspngx1, ivspngl, idspngl, idens, isgs;
+};
+
+// Poisson plan (src/direct.f SAVE state): eigen-transform of the x operator.
+struct PoissonPlan {
+  int M, L, N;          // interior sizes along x, y (FFT), z
+  int m0;               // index of the null x-mode
+  double *Af, *Ab;      // forward/backward transform matrices (M x M, col-major)
+  float *Af32, *Ab32;   // FP32 copies for the mixed form
+  double *lam;          // eigenvalues of the x operator (M)
+  double *ak;           // modified wavenumber AK(J/2+1) per packed index (L)
+  double *an, *bn, *cn; // z operator (N)
+  double *twr, *twi;    // FFT twiddles exp(-2 pi i q/L), q < L/2
+  double *spec, *spec2; // spectral work arrays, M*L*N each
+  double *cprime;       // Thomas scratch, M*L*N
+  double *red;          // reduction scratch
+};
+
+// kernel categories timed with CUDA events when profiling is enabled
+enum {
+  PROF_RHS_PRED = 0, PROF_BC, PROF_DIV_FFT, PROF_GEMM_FWD, PROF_TRIDIAG, PROF_GEMM_BWD, PROF_FFT_BWD,
+  PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_NCAT
+};
+
+struct ProfEvent {
+  int cat;
+  cudaEvent_t a, b;
+};
+
+struct eddy_ctx {
+  int device = 0;
+  eddy_params prm{};
+  Dims d{};
+  Scalars sc{};
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  DevMetrics m{};
+  // host copies of the 1-D arrays (1-based, size n+2)
+  std::vector<double> h[28];
+  // fields (device, FP64, Fortran layout)
+  double *f[EDDY_NFIELDS] = {};
+  double *dens_alt = nullptr;  // ping-pong partner of DENS
+  // SGS arrays
+  double *uc = nullptr, *vc = nullptr, *wc = nullptr, *sij = nullptr, *gs = nullptr,
+         *mm = nullptr, *lm = nullptr, *dxdydz = nullptr, *ilm2 = nullptr, *imm2 = nullptr;
+  double *scal = nullptr;  // device scalars: [0] pref [1] qin1 [2] qin2 [3] dpm [4] maxdiv
+  PoissonPlan pp{};
+  std::string err;
+  int64_t launches = 0;
+  double dely = 0., delysq = 0.;
+  // profiling (CUDA events on the context stream around each category)
+  unsigned prof_mask = 0;
+  std::vector<ProfEvent> prof_ev;   // recorded in this window
+  std::vector<ProfEvent> prof_pool; // reusable events
+  double prof_ms[PROF_NCAT] = {};
+  long long prof_n[PROF_NCAT] = {};
+};
+
+// RAII scope: records a start event now and a stop event at scope exit when
+// the category is enabled.
+struct ProfScope {
+  eddy_ctx *c;
+  int cat;
+  bool on;
+  ProfEvent ev{};
+  ProfScope(eddy_ctx *ctx, int category) : c(ctx), cat(category), on((ctx->prof_mask >> category) & 1u) {
+    if (!on) return;
+    if (!c->prof_pool.empty()) {
+      ev = c->prof_pool.back();
+      c->prof_pool.pop_back();
+    } else {
+      cudaEventCreate(&ev.a);
+      cudaEventCreate(&ev.b);
+    }
+    ev.cat = cat;
+    cudaEventRecord(ev.a, c->stream);
+  }
+  ~ProfScope() {
+    if (!on) return;
+    cudaEventRecord(ev.b, c->stream);
+    c->prof_ev.push_back(ev);
+  }
+};
+
+#define EDDY_CUDA(call)                                                     \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);        \
+      return EDDY_ECUDA;                                                    \
+    }                                                                       \
+  } while (0)
+
+#define EDDY_LAUNCHED(ctx)                                                  \
+  do {                                                                      \
+    cudaError_t e_ = cudaGetLastError();                                    \
+    (ctx)->launches++;                                                      \
+    if (e_ != cudaSuccess) {                                                \
+      (ctx)->err = std::string("kernel launch: ") + cudaGetErrorString(e_); \
+      return EDDY_ECUDA;                                                    \
+    }                                                                       \
+  } while (0)
+
+// Fortran (i,j,k) 1-based -> linear index
+__host__ __device__ inline long long fidx(const Dims &d, int i, int j, int k) {
+  return (long long)(i - 1) + (long long)d.nx * ((long long)(j - 1) + (long long)d.ny * (long long)(k - 1));
+}
+
+// kernel drivers (each returns EDDY_* status)
+int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
+int launch_boundary(eddy_ctx *ctx, double *u, double *v, double *w);
+int launch_boundinout(eddy_ctx *ctx, double *ubc, double *vbc, double *wbc, const double *uof,
+                      const double *vof, const double *wof, double alfxdt, int idiv);
+int launch_correct(eddy_ctx *ctx, double alfxdt);
+int launch_pressure_update(eddy_ctx *ctx);
+int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
+int launch_boundinoutd_dens(eddy_ctx *ctx, double *dens);
+int launch_turvis(eddy_ctx *ctx);
+int launch_filtersize(eddy_ctx *ctx);
+int poisson_plan_create(eddy_ctx *ctx);
+int poisson_plan_destroy(eddy_ctx *ctx);
+// divergence/alfxdt of (us,vs,ws) -> solve -> DP (device), DIRECT semantics
+int launch_direct(eddy_ctx *ctx, const double *us, const double *vs, const double *ws,
+                  double alfxdt);
+// solve from an explicit right-hand side array (interior of rhs) -> dp
+int launch_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp);
+int launch_max_divergence(eddy_ctx *ctx, double *out_host);
+
+// host-side symmetric tridiagonal eigensolver (implicit QL with Wilkinson shift)
+int tridiag_eigen(int n, std::vector<double> &d, std::vector<double> &e, std::vector<double> &q);

@@ -1,0 +1,153 @@
+/*
+ * eddy_b200.h -- C ABI of the B200 (sm_100a) fractional-step time advance.
+ *
+ * Drop-in boundary for the reference's Fortran driver (src/Eddy6.f).  Every
+ * entry point returns an int status (EDDY_OK = 0); none exits or traps.
+ * Fields live on the GPU inside an opaque context; host arrays are touched
+ * only by eddy_upload/eddy_download (Fortran column-major (NX,NY,NZ) FP64 with
+ * ghost layers, exactly the driver's ALLOCATEd arrays, src/Eddy6.f:428-454).
+ * All work is enqueued on the context's CUDA stream; eddy_sync and
+ * eddy_download are the only calls that block.  A context is used by one host
+ * thread at a time.
+ *
+ * Axes follow the reference: x = x_ref (stretched), y = y_ref (uniform,
+ * periodic, FFT axis), z = z_ref (stretched).  Boundary types supported on
+ * the hot path: 60 (slip wall) and 50 (no-slip) on x, 500 on y, 305 (hybrid
+ * inlet plane) and 710/720/730 (outlets) on z.
+ */
+#ifndef EDDY_B200_H
+#define EDDY_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  EDDY_OK = 0,
+  EDDY_EINVAL = 1,      /* bad argument / unsupported configuration */
+  EDDY_ECUDA = 2,       /* CUDA or cuBLAS error */
+  EDDY_ENAN = 3,        /* non-finite value detected */
+  EDDY_ESINGULAR = 4,   /* singular pivot in a line solve */
+  EDDY_ENOCONV = 5,     /* refinement did not converge */
+  EDDY_ETIMEOUT = 6,    /* a bounded device-side wait expired */
+  EDDY_ENOMEM = 7
+};
+
+/* Precision forms. */
+enum { EDDY_PLAIN_FP64 = 0, EDDY_MIXED = 1 };
+
+/* Field ids for upload/download; numbering matches the reference names. */
+enum {
+  EDDY_UO = 0, EDDY_VO, EDDY_WO, EDDY_P, EDDY_DP, EDDY_DENS, EDDY_TV,
+  EDDY_US, EDDY_VS, EDDY_WS, EDDY_UA, EDDY_VA, EDDY_WA, EDDY_UB, EDDY_VB,
+  EDDY_WB, EDDY_RHA, EDDY_RHB, EDDY_RS,
+  EDDY_PLANEU, EDDY_PLANEV, EDDY_PLANEW, EDDY_PLANED, /* (NX,NY) planes */
+  EDDY_NFIELDS
+};
+
+/* Run parameters.  Names follow the reference's COMMON blocks
+ * (src/common.h:77-112) and the sponge module (src/Initialize.f:139-153). */
+typedef struct {
+  int nx, ny, nz;            /* NX, NY, NZ including one ghost layer each side */
+  int itype[7];              /* ITYPE(1..6) in itype[1..6]; itype[0] unused */
+  int ischm;                 /* 3 = RK3, 1 = AB2 (src/inpall.f:218-235) */
+  int isgs;                  /* 0 none, 1 Smagorinsky, 2 dynamic (y average) */
+  int idens;                 /* 1 = Boussinesq density equation */
+  double ru1, prn, denP1, grav, dpdx, dpdy, dpdz, eps, css;
+  int vspngx1, dspngx1, vspngx3in, vspngx3out, dspngx3in, dspngx3out;
+  int precision;             /* EDDY_PLAIN_FP64 or EDDY_MIXED */
+  int refine_sweeps;         /* mixed form: FP64-residual refinement sweeps (1-3) */
+  int closure;               /* 0 = dynamic TURVIS, 1 = learned MLP closure */
+} eddy_params;
+
+typedef struct eddy_ctx eddy_ctx;
+
+/* Create a context on CUDA device `device`.  Builds the metric arrays the way
+ * src/grid.f:8-483 does from face coordinates (x: nx-1 faces, z: nz-1 faces,
+ * the contents of the reference's grid files; y uniform on [ymin,ymax]),
+ * the sponge profiles (src/Initialize.f:129-271) and the Poisson plan
+ * (src/direct.f:121-585).  Replaces the driver's Grid/SETUP/SPONGE_SETUP
+ * calls (src/Eddy6.f:463,531,620). */
+int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces,
+                double ymin, double ymax, const double *zw_faces, int device);
+int eddy_destroy(eddy_ctx *ctx);
+
+/* Copy a field between the host (Fortran-ordered FP64) and the device. */
+int eddy_upload(eddy_ctx *ctx, int field, const double *host);
+int eddy_download(eddy_ctx *ctx, int field, double *host);
+/* Read one of the 1-D metric arrays the context built (same numbering as the
+ * oracle: 0 xu 1 xc 2 ap 3 au 4 av 5 aw 6 yv 7 yc 8 bp 9 bu 10 bv 11 bw
+ * 12 zw 13 zc 14 cp 15 cu 16 cv 17 cw 18 whx 19 why 20 whz 21 dfxu 22 dfxw
+ * 23 dfxul 24 dfxwl 25 dfxd 26 dfxdl 27 dens_bg); returns length or <0. */
+int eddy_get_metric(eddy_ctx *ctx, int which, double *out, int n);
+/* Host-only: the same metric arrays without a context or a GPU (the
+ * reference's Grid subroutine, src/grid.f:8). */
+int eddy_grid_metric(const eddy_params *prm, const double *xu_faces, double ymin, double ymax,
+                     const double *zw_faces, int which, double *out, int n);
+
+/* ---- one entry per reference subroutine on the hot path ---- */
+/* RHS (src/rhs.f:4) fused with PREDICTORD (src/timeindeg.f:1041): uo,vo,wo,
+ * tv,p,dens,ua.. -> us,vs,ws (u*), ua,va,wa (new explicit RHS). */
+int eddy_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
+/* BOUNDARY (src/boundary.f:7) on the provisional (set=0: US,VS,WS) or the
+ * corrected (set=1: UO,VO,WO) velocity. */
+int eddy_boundary(eddy_ctx *ctx, int set);
+/* BOUNDINOUT (src/boundary.f:505); idiv=1 predictor on US.. (old UO..),
+ * idiv=0 corrector on UO.. (from US..). */
+int eddy_boundinout(eddy_ctx *ctx, int idiv, double alfxdt);
+/* DIVERGENCE (src/timeindeg.f:908) / alfxdt then DIRECT (src/direct.f:2):
+ * solves for DP on the device. */
+int eddy_direct(eddy_ctx *ctx, double alfxdt);
+/* CORRECT (src/timeindeg.f:981). */
+int eddy_correct(eddy_ctx *ctx, double alfxdt);
+/* P=P+DP, reference value, ghost fills (src/Eddy6.f:2772-2853,2911-2953). */
+int eddy_pressure_update(eddy_ctx *ctx);
+/* BOUNDINOUTD/BOUNDARY_DENS/RHS_DENSITY/DENSITY sequence (src/Eddy6.f
+ * :2957-2969; src/rhs_density.f:4; src/density.f:6). */
+int eddy_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
+/* TURVIS dynamic procedure (src/vt.f:16) incl. FILTERSIZE (src/vt.f:1096). */
+int eddy_turvis(eddy_ctx *ctx);
+
+/* ---- driver twin (src/Eddy6.f:2095-3049) ---- */
+/* Start-from-scratch initialisation after uploading the initial fields
+ * (src/Eddy6.f:582-765, 1718-1726). */
+int eddy_initialize(eddy_ctx *ctx, double dt);
+/* One RK substep is (0-based) of the step, time step dt. */
+int eddy_substep(eddy_ctx *ctx, int is, double dt);
+/* nsteps full steps (3 RK substeps + eddy viscosity update each). */
+int eddy_step(eddy_ctx *ctx, double dt, int nsteps);
+
+/* Standalone Poisson solve of the operator DIRECT inverts: rhs is an
+ * (NX,NY,NZ) device or host array (interior used); the solution is written to
+ * sol (same shape, DIRECT's ghost convention).  `on_device` selects pointer
+ * space.  In the mixed form the solve is FP32 transforms wrapped in
+ * refine_sweeps FP64-residual iterative-refinement sweeps. */
+int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_device);
+
+/* Diagnostics: max |div u| of (UO,VO,WO) over the interior (src/info.f:32). */
+int eddy_max_divergence(eddy_ctx *ctx, double *out);
+
+/* Kernel-category timing with CUDA events on the context stream (the
+ * device-side counterpart of the reference's CLOCK array, src/info.f:350 and
+ * src/Eddy6.f:2104-2990).  Categories: 0 RHS+predictor, 1 boundary fills,
+ * 2 divergence+forward FFT, 3 forward transform, 4 z line solves,
+ * 5 backward transform, 6 backward FFT, 7 CORRECT, 8 pressure update,
+ * 9 density, 10 eddy viscosity.  eddy_profile_read synchronises, adds the
+ * window's elapsed times per category to ms[11] / counts[11] (cumulative
+ * since the mask was set) and starts a new window. */
+int eddy_profile_enable(eddy_ctx *ctx, unsigned mask);
+int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts);
+
+int eddy_sync(eddy_ctx *ctx);
+/* Copy the last error message (NUL-terminated, truncated to len). */
+int eddy_last_error(eddy_ctx *ctx, char *buf, int len);
+/* Number of kernels this context has launched since creation. */
+int64_t eddy_launch_count(eddy_ctx *ctx);
+/* The context's CUDA stream (cudaStream_t) for callers that synchronise. */
+void *eddy_stream(eddy_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

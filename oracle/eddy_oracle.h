@@ -144,6 +144,13 @@ void eo_substep(eo_state *s, int is, double dtm1);
 void eo_step(eo_state *s, double dtm1, int nsteps, int poisson_method);
 void eo_set_threads(int n);
 void eo_initialize(eo_state *s, double dtm1);
+/* one call per product C-ABI entry point (kernel-level parity tests) */
+void eo_call_rhs_predictord(eo_state *s, double alfxdt, double gamxdt, double rhoxdt);
+void eo_call_boundary(eo_state *s, int set);
+void eo_call_boundinout(eo_state *s, int idiv, double alfxdt);
+int eo_call_direct(eo_state *s, double alfxdt, int method);
+void eo_call_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt);
+double eo_max_divergence(eo_state *s);
 
 /* ---- deterministic noise: SplitMix64 counter generator ---- */
 uint64_t eo_splitmix64(uint64_t x);

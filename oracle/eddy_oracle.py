@@ -86,6 +86,14 @@ def lib():
         L.eo_correct.argtypes = [C.c_void_p, C.c_double]
         L.eo_pressure_update.argtypes = [C.c_void_p]
         L.eo_rhs_density.argtypes = [C.c_void_p]
+        L.eo_call_rhs_predictord.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.eo_call_density.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.eo_call_boundary.argtypes = [C.c_void_p, C.c_int]
+        L.eo_call_boundinout.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.eo_call_direct.argtypes = [C.c_void_p, C.c_double, C.c_int]
+        L.eo_call_direct.restype = C.c_int
+        L.eo_max_divergence.argtypes = [C.c_void_p]
+        L.eo_max_divergence.restype = C.c_double
         _lib = L
     return _lib
 
@@ -174,6 +182,34 @@ class OracleSolver:
 
     def turvis(self):
         lib().eo_turvis(self.h)
+
+    # one method per product C-ABI entry point
+    def rhs_predictord(self, alf, gam, rho):
+        lib().eo_call_rhs_predictord(self.h, alf, gam, rho)
+
+    def boundary(self, set_):
+        lib().eo_call_boundary(self.h, set_)
+
+    def boundinout(self, idiv, alf):
+        lib().eo_call_boundinout(self.h, idiv, alf)
+
+    def direct_from_velocity(self, alf, method=0):
+        return lib().eo_call_direct(self.h, alf, method)
+
+    def correct(self, alf):
+        lib().eo_correct(self.h, alf)
+
+    def pressure_update(self):
+        lib().eo_pressure_update(self.h)
+
+    def density(self, alf, gam, rho):
+        lib().eo_call_density(self.h, alf, gam, rho)
+
+    def substep(self, is_):
+        lib().eo_substep(self.h, is_, self.w.dt)
+
+    def max_divergence(self):
+        return lib().eo_max_divergence(self.h)
 
     def __del__(self):
         if getattr(self, "h", None):

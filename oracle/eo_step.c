@@ -119,3 +119,49 @@ void eo_initialize(eo_state *s, double dtm1) {
     eo_turvis(s);
   }
 }
+
+/* ---- one call per C-ABI entry point of the product, for kernel-level parity
+ * tests (same sequences as include/eddy_b200.h documents) ---- */
+void eo_call_rhs_predictord(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
+  eo_rhs(s, s->uo, s->vo, s->wo, s->tv, s->us, s->vs, s->ws, s->ub, s->vb, s->wb, s->dp);
+  eo_predictord(s, alfxdt, gamxdt, rhoxdt);
+}
+void eo_call_boundary(eo_state *s, int set) {
+  if (set == 0) eo_boundary(s, s->us, s->vs, s->ws);
+  else eo_boundary(s, s->uo, s->vo, s->wo);
+}
+void eo_call_boundinout(eo_state *s, int idiv, double alfxdt) {
+  if (idiv == 1) eo_boundinout(s, s->us, s->vs, s->ws, s->uo, s->vo, s->wo, alfxdt, 1);
+  else eo_boundinout(s, s->uo, s->vo, s->wo, s->us, s->vs, s->ws, alfxdt, 0);
+}
+int eo_call_direct(eo_state *s, double alfxdt, int method) {
+  eo_divergence(s, s->us, s->vs, s->ws, s->dp);
+  for (long q = 0; q < s->ncell; q++) s->dp[q] = s->dp[q] / alfxdt;
+  return eo_direct(s, method);
+}
+void eo_call_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
+  eo_boundinoutd(s, s->dens);
+  eo_boundary_dens(s, s->dens);
+  eo_rhs_density(s);
+  eo_boundary_dens(s, s->rhb);
+  eo_boundary_dens(s, s->rs);
+  eo_density(s, alfxdt, gamxdt, rhoxdt);
+  eo_boundinoutd(s, s->dens);
+  eo_boundary_dens(s, s->dens);
+}
+double eo_max_divergence(eo_state *s) {
+  const eo_grid *g = s->g;
+  double mx = 0.;
+  int nx = g->nx, ny = g->ny;
+#define OA(a, i, j, k) (a)[(size_t)((i)-1) + (size_t)nx * ((size_t)((j)-1) + (size_t)ny * (size_t)((k)-1))]
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        double dv = (g->ap[i] * (OA(s->uo, i, j, k) - OA(s->uo, i - 1, j, k)) +
+                     g->bp[j] * (OA(s->vo, i, j, k) - OA(s->vo, i, j - 1, k)) +
+                     g->cp[k] * (OA(s->wo, i, j, k) - OA(s->wo, i, j, k - 1)));
+        if (fabs(dv) > mx) mx = fabs(dv);
+      }
+#undef OA
+  return mx;
+}

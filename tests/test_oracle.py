@@ -1,0 +1,103 @@
+"""The CPU oracle against FFTPACK golden vectors, manufactured Poisson
+solutions and step invariants (no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from eddy_hybrid_b200 import config
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "fftpack_rfft.npz")
+
+
+@pytest.mark.parametrize("n", [2, 4, 8, 16, 32, 64, 256, 6, 12, 30, 384])
+def test_fft_matches_fftpack_golden(oracle, n):
+    g = np.load(GOLD)
+    f = oracle.rfftf(g[f"x{n}"])
+    assert np.max(np.abs(f - g[f"f{n}"])) <= 1e-13 * max(1.0, np.max(np.abs(g[f"f{n}"])))
+    b = oracle.rfftb(f)
+    assert np.max(np.abs(b - g[f"b{n}"])) <= 1e-12 * n
+    rb = oracle.rfftb(g[f"r{n}"])
+    assert np.max(np.abs(rb - g[f"rb{n}"])) <= 1e-12 * n
+
+
+def _compatible_rhs(s, w, seed=7):
+    rng = np.random.RandomState(seed)
+    d = np.zeros((w.nx, w.ny, w.nz), order="F")
+    d[1:-1, 1:-1, 1:-1] = rng.randn(w.mx, w.ly, w.nz_)
+    ap = s.grid.get("ap")
+    cp = s.grid.get("cp")
+    vol = (1 / ap[1:-1])[:, None, None] * np.ones((1, w.ly, 1)) * (1 / cp[1:-1])[None, None, :]
+    inner = d[1:-1, 1:-1, 1:-1]
+    inner -= (inner * vol).sum() / vol.sum()
+    return d
+
+
+@pytest.mark.parametrize("shape", [(8, 4, 10), (12, 8, 16), (20, 16, 14)])
+def test_poisson_manufactured_and_two_methods(oracle, shape):
+    mx, ly, nz_ = shape
+    w = config.small(mx=mx, ly=ly, nz_=nz_, beta=2.5)
+    s = oracle.OracleSolver(w)
+    d = _compatible_rhs(s, w)
+    sols = []
+    for method in (0, 1):
+        s.set("dp", d)
+        assert s.direct(method) == 0
+        x = s.get("dp")
+        r = s.apply_laplacian(x)
+        res = np.max(np.abs(r[1:-1, 1:-1, 1:-1] - d[1:-1, 1:-1, 1:-1])) / np.max(np.abs(d))
+        assert res < 1e-12, (method, res)
+        # zero-mean k=0 plane convention (direct.f:895-898)
+        assert abs(x[1:-1, 1:-1, 1:-1].mean()) < 1e-12 * np.abs(x).max()
+        sols.append(x)
+    assert rel_err(sols[0], sols[1]) < 1e-12
+
+
+def test_poisson_ghost_convention(oracle):
+    w = config.small(mx=8, ly=8, nz_=8)
+    s = oracle.OracleSolver(w)
+    s.set("dp", _compatible_rhs(s, w))
+    s.direct(0)
+    x = s.get("dp")
+    assert np.all(x[:, :, 0] == 0) and np.all(x[:, :, -1] == 0)
+    np.testing.assert_array_equal(x[0, 1:-1, 1:-1], x[1, 1:-1, 1:-1])
+    np.testing.assert_array_equal(x[:, 0, 1:-1], x[:, -2, 1:-1])
+    np.testing.assert_array_equal(x[:, -1, 1:-1], x[:, 1, 1:-1])
+
+
+def _run(oracle, w, steps):
+    s = oracle.OracleSolver(w)
+    f = config.initial_fields(w, s.grid.get("dens_bg")[: w.nx])
+    s.load_initial(f)
+    s.initialize()
+    s.step(steps)
+    return s
+
+
+def test_step_projection_is_divergence_free(oracle):
+    w = config.small(mx=16, ly=8, nz_=24, noise=0.2)
+    s = _run(oracle, w, 3)
+    for n in ("uo", "vo", "wo", "p", "dens", "tv"):
+        assert np.isfinite(s.get(n)).all()
+    # post-projection divergence (the src/info.f:32 quantity)
+    assert s.max_divergence() < 1e-11
+
+
+def test_step_dynamic_viscosity_active(oracle):
+    w = config.small(mx=16, ly=16, nz_=24, noise=0.5, re=1e4)
+    s = _run(oracle, w, 2)
+    tv = s.get("tv")
+    assert tv[1:-1, 1:-1, 1:-1].max() > 0.0
+    assert (tv[1:-1, 1:-1, 1:-1] >= 0).all()
+
+
+def test_mass_balance_outflow(oracle):
+    w = config.small(mx=12, ly=8, nz_=16, noise=0.1)
+    s = _run(oracle, w, 2)
+    wo = s.get("wo")
+    ap = s.grid.get("ap")
+    area = (1.0 / ap[1:-1])[:, None] * np.ones((1, w.ly)) * ((w.ylim[1] - w.ylim[0]) / w.ly)
+    qin = (wo[1:-1, 1:-1, 0] * area).sum()
+    qout = (wo[1:-1, 1:-1, -2] * area).sum()
+    assert abs(qin - qout) < 1e-10 * abs(qin)
