@@ -268,7 +268,7 @@ def main():
     kernels = {c: {"ms_per_step": prof[c][0] / args.steps, "launches": prof[c][1],
                    "share": prof[c][0] / total_ms if total_ms else None,
                    **({"gbs": ALG_BYTES[c] * ncell / (prof[c][0] / prof[c][1] / 1e3) / 1e9}
-                      if prof[c][1] else {})}
+                      if prof[c][1] and c in ALG_BYTES else {})}
                for c in prof}
 
     line = {

@@ -46,6 +46,7 @@ struct PoissonPlan {
   double *lam;          // eigenvalues of the x operator (M)
   double *ak;           // modified wavenumber AK(J/2+1) per packed index (L)
   double *an, *bn, *cn; // z operator (N)
+  double *wz;           // 1/cp(k): z cell widths for the compatibility projection
   double *twr, *twi;    // FFT twiddles exp(-2 pi i q/L), q < L/2
   double *spec, *spec2; // spectral work arrays, M*L*N each
   double *cprime;       // Thomas scratch, M*L*N

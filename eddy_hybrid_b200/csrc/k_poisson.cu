@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(FT)
 __global__ void __launch_bounds__(256)
     k_tridiag_z(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
                 const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
-                double *__restrict__ g, double *__restrict__ cpr) {
+                const double *__restrict__ wz, double *__restrict__ g, double *__restrict__ cpr) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)M * L) return;
   int mi = (int)(t % M), J = (int)(t / M);
@@ -154,6 +154,17 @@ __global__ void __launch_bounds__(256)
   int pin = (J == 0 && mi == m0);
   int s0 = pin ? 1 : 0;
   double lm = lam[mi], akJ = ak[J];
+  if (pin) {
+    // compatibility of the singular (J=0, constant-x) line: remove the
+    // z-volume-weighted mean so the Neumann system has a solution
+    double sv = 0., vv = 0.;
+    for (int k = 0; k < N; k++) {
+      sv += g[t + ML * k] * wz[k];
+      vv += wz[k];
+    }
+    double cm = sv / vv;
+    for (int k = 0; k < N; k++) g[t + ML * k] = g[t + ML * k] - cm;
+  }
   double prev_c = 0., prev_d = 0.;
   for (int k = s0; k < N; k++) {
     double a = (k == s0) ? 0. : an[k];
@@ -275,7 +286,7 @@ int solve_from_spec(eddy_ctx *ctx, double *dp) {
   {
     ProfScope ps(ctx, PROF_TRIDIAG);
     k_tridiag_z<<<(unsigned)((nl + 255) / 256), 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.lam, pp.ak, pp.an,
-                                                                       pp.bn, pp.cn, pp.spec2, pp.cprime);
+                                                                       pp.bn, pp.cn, pp.wz, pp.spec2, pp.cprime);
     EDDY_LAUNCHED(ctx);
   }
   {
@@ -377,6 +388,7 @@ int poisson_plan_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMalloc(&pp.an, sizeof(double) * N));
   EDDY_CUDA(cudaMalloc(&pp.bn, sizeof(double) * N));
   EDDY_CUDA(cudaMalloc(&pp.cn, sizeof(double) * N));
+  EDDY_CUDA(cudaMalloc(&pp.wz, sizeof(double) * N));
   EDDY_CUDA(cudaMalloc(&pp.twr, sizeof(double) * L));
   EDDY_CUDA(cudaMalloc(&pp.twi, sizeof(double) * L));
   EDDY_CUDA(cudaMalloc(&pp.spec, vol));
@@ -392,6 +404,9 @@ int poisson_plan_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMemcpy(pp.an, an.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.bn, bn.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.cn, cn.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  std::vector<double> wz(N);
+  for (int k = 0; k < N; k++) wz[k] = 1.0 / cp[k + 2];
+  EDDY_CUDA(cudaMemcpy(pp.wz, wz.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.twr, twr.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.twi, twi.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
   size_t smem = sizeof(double) * 2 * L * TI;
@@ -404,7 +419,7 @@ int poisson_plan_create(eddy_ctx *ctx) {
 
 int poisson_plan_destroy(eddy_ctx *ctx) {
   PoissonPlan &pp = ctx->pp;
-  void *ptrs[] = {pp.Af, pp.Ab, pp.Af32, pp.Ab32, pp.lam, pp.ak, pp.an, pp.bn, pp.cn,
+  void *ptrs[] = {pp.Af, pp.Ab, pp.Af32, pp.Ab32, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, pp.wz,
                   pp.twr, pp.twi, pp.spec, pp.spec2, pp.cprime, pp.red};
   for (void *p : ptrs) if (p) cudaFree(p);
   pp = PoissonPlan{};

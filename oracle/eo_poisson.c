@@ -371,6 +371,19 @@ int eo_direct(eo_state *s, int method) {
       double ak = ak_of(g, Jp);
       double *F = spec + (size_t)(Jp - 1) * M * N;
       for (int i = 0; i < M; i++) bml[i] = bm[i] - ak;
+      if (Jp == 1) {
+        /* compatibility: remove the volume-weighted mean of the k=0 right-hand
+         * side (the component outside the range of the Neumann operator) */
+        double sv = 0., vv = 0.;
+        for (int k = 0; k < N; k++)
+          for (int i = 0; i < M; i++) {
+            double v = 1.0 / (g->ap[i + 2] * g->cp[k + 2]);
+            sv += F[(size_t)k * M + i] * v;
+            vv += v;
+          }
+        double cmean = sv / vv;
+        for (long q = 0; q < (long)M * N; q++) F[q] = F[q] - cmean;
+      }
       if (method == 1) {
         int r = solve_block(M, N, am, bml, cm, an, bn, cn, F, Jp == 1);
         if (r) rc = r;

@@ -137,8 +137,14 @@ def test_full_step_parity(oracle, product, shape):
     assert rel_err(g.download("tv"), o.get("tv")) < 1e-12
     o.step(10)
     g.step(10)
-    for n in ("uo", "vo", "wo", "p", "dens", "tv"):
+    for n in ("uo", "vo", "wo", "dens", "tv"):
         e = rel_err(g.download(n), o.get(n))
         assert e < 1e-11, (n, e)
+    # Pressure: two exact FP64 solvers of the same Neumann system differ by
+    # up to cond(L)*eps in the solution (the oracle's own eigen and block
+    # solvers differ by ~3e-11 on these grids), so its bar is 1e-10 relative;
+    # the velocities it projects agree to ~1e-14.
+    e = rel_err(g.download("p"), o.get("p"))
+    assert e < 1e-10, ("p", e)
     assert g.max_divergence() < 1e-12
     assert o.max_divergence() < 1e-12
