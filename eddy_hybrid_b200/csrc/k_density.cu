@@ -27,27 +27,29 @@ __global__ void __launch_bounds__(BX *BY *BZ)
     dn[q] = dens[q];
     return;
   }
-  double qxp = A(uo, i, j, k), qxm = A(uo, i - 1, j, k);
-  double rxp = (A(dens, i + 1, j, k) + A(dens, i, j, k)) * 0.5;
-  double rxm = (A(dens, i, j, k) + A(dens, i - 1, j, k)) * 0.5;
-  double vyp = A(vo, i, j, k), vym = A(vo, i, j - 1, k);
-  double ryp = (A(dens, i, j + 1, k) + A(dens, i, j, k)) * 0.5;
-  double rym = (A(dens, i, j, k) + A(dens, i, j - 1, k)) * 0.5;
-  double wzp = A(wo, i, j, k), wzm = A(wo, i, j, k - 1);
-  double rzp = (A(dens, i, j, k + 1) + A(dens, i, j, k)) * 0.5;
-  double rzm = (A(dens, i, j, k) + A(dens, i, j, k - 1)) * 0.5;
-  double drdxp = m.au[i] * (A(dens, i + 1, j, k) - A(dens, i, j, k));
-  double drdxm = m.au[i - 1] * (A(dens, i, j, k) - A(dens, i - 1, j, k));
-  double drdyp = m.bv[j] * (A(dens, i, j + 1, k) - A(dens, i, j, k));
-  double drdym = m.bv[j - 1] * (A(dens, i, j, k) - A(dens, i, j - 1, k));
-  double drdzp = m.cw[k] * (A(dens, i, j, k + 1) - A(dens, i, j, k));
-  double drdzm = m.cw[k - 1] * (A(dens, i, j, k) - A(dens, i, j, k - 1));
-  double kvip = 0.5 * (A(kv, i + 1, j, k) + A(kv, i, j, k));
-  double kvim = 0.5 * (A(kv, i - 1, j, k) + A(kv, i, j, k));
-  double kvjp = 0.5 * (A(kv, i, j + 1, k) + A(kv, i, j, k));
-  double kvjm = 0.5 * (A(kv, i, j - 1, k) + A(kv, i, j, k));
-  double kvkp = 0.5 * (A(kv, i, j, k + 1) + A(kv, i, j, k));
-  double kvkm = 0.5 * (A(kv, i, j, k - 1) + A(kv, i, j, k));
+  const int sy = d.nx;
+  const long long sz = (long long)d.nx * d.ny;
+  double qxp = uo[q], qxm = uo[q-1];
+  double rxp = (dens[q+1] + dens[q]) * 0.5;
+  double rxm = (dens[q] + dens[q-1]) * 0.5;
+  double vyp = vo[q], vym = vo[q-sy];
+  double ryp = (dens[q+sy] + dens[q]) * 0.5;
+  double rym = (dens[q] + dens[q-sy]) * 0.5;
+  double wzp = wo[q], wzm = wo[q-sz];
+  double rzp = (dens[q+sz] + dens[q]) * 0.5;
+  double rzm = (dens[q] + dens[q-sz]) * 0.5;
+  double drdxp = m.au[i] * (dens[q+1] - dens[q]);
+  double drdxm = m.au[i - 1] * (dens[q] - dens[q-1]);
+  double drdyp = m.bv[j] * (dens[q+sy] - dens[q]);
+  double drdym = m.bv[j - 1] * (dens[q] - dens[q-sy]);
+  double drdzp = m.cw[k] * (dens[q+sz] - dens[q]);
+  double drdzm = m.cw[k - 1] * (dens[q] - dens[q-sz]);
+  double kvip = 0.5 * (kv[q+1] + kv[q]);
+  double kvim = 0.5 * (kv[q-1] + kv[q]);
+  double kvjp = 0.5 * (kv[q+sy] + kv[q]);
+  double kvjm = 0.5 * (kv[q-sy] + kv[q]);
+  double kvkp = 0.5 * (kv[q+sz] + kv[q]);
+  double kvkm = 0.5 * (kv[q-sz] + kv[q]);
   double txxp = (repr1 + kvip) * drdxp;
   double txxm = (repr1 + kvim) * drdxm;
   double tyyp = (repr1 + kvjp) * drdyp;

@@ -17,36 +17,36 @@ constexpr int BX = 32, BY = 4, BZ = 2;
 __device__ __forceinline__ double rhs_u(const Dims &d, const DevMetrics &m, double ru1,
                                         const double *__restrict__ uo, const double *__restrict__ vo,
                                         const double *__restrict__ wo, const double *__restrict__ tv,
-                                        int i, int j, int k) {
+                                        int i, int j, int k, long long q, int sy, long long sz) {
   const double *qr = uo;
-  double qxp = (A(qr, i + 1, j, k) + A(qr, i, j, k)) * 0.5;
-  double qxm = (A(qr, i, j, k) + A(qr, i - 1, j, k)) * 0.5;
-  double uxp = (A(uo, i + 1, j, k) + A(uo, i, j, k)) * 0.5;
-  double uxm = (A(uo, i, j, k) + A(uo, i - 1, j, k)) * 0.5;
-  double uyp = (A(uo, i, j + 1, k) + A(uo, i, j, k)) * 0.5;
-  double uym = (A(uo, i, j, k) + A(uo, i, j - 1, k)) * 0.5;
-  double uzp = (A(uo, i, j, k + 1) + A(uo, i, j, k)) * 0.5;
-  double uzm = (A(uo, i, j, k) + A(uo, i, j, k - 1)) * 0.5;
-  double vxp = (A(vo, i + 1, j, k) + A(vo, i, j, k)) * 0.5;
-  double vxm = (A(vo, i + 1, j - 1, k) + A(vo, i, j - 1, k)) * 0.5;
-  double wxp = (A(wo, i + 1, j, k) + A(wo, i, j, k)) * 0.5;
-  double wxm = (A(wo, i + 1, j, k - 1) + A(wo, i, j, k - 1)) * 0.5;
-  double dqdxp = m.ap[i + 1] * (A(qr, i + 1, j, k) - A(qr, i, j, k));
-  double dqdxm = m.ap[i] * (A(qr, i, j, k) - A(qr, i - 1, j, k));
-  double dudyp = m.bv[j] * (A(uo, i, j + 1, k) - A(uo, i, j, k));
-  double dudym = m.bv[j - 1] * (A(uo, i, j, k) - A(uo, i, j - 1, k));
-  double dudzp = m.cw[k] * (A(uo, i, j, k + 1) - A(uo, i, j, k));
-  double dudzm = m.cw[k - 1] * (A(uo, i, j, k) - A(uo, i, j, k - 1));
-  double dvdxp = m.au[i] * (A(vo, i + 1, j, k) - A(vo, i, j, k));
-  double dvdxm = m.au[i] * (A(vo, i + 1, j - 1, k) - A(vo, i, j - 1, k));
-  double dwdxp = m.au[i] * (A(wo, i + 1, j, k) - A(wo, i, j, k));
-  double dwdxm = m.au[i] * (A(wo, i + 1, j, k - 1) - A(wo, i, j, k - 1));
-  double tvjp = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j + 1, k) + A(tv, i, j + 1, k));
-  double tvjm = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j - 1, k) + A(tv, i, j - 1, k));
-  double tvkp = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j, k + 1) + A(tv, i, j, k + 1));
-  double tvkm = 0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j, k - 1) + A(tv, i, j, k - 1));
-  double txxp = (ru1 + 2. * A(tv, i + 1, j, k)) * dqdxp;
-  double txxm = (ru1 + 2. * A(tv, i, j, k)) * dqdxm;
+  double qxp = (qr[q+1] + qr[q]) * 0.5;
+  double qxm = (qr[q] + qr[q-1]) * 0.5;
+  double uxp = (uo[q+1] + uo[q]) * 0.5;
+  double uxm = (uo[q] + uo[q-1]) * 0.5;
+  double uyp = (uo[q+sy] + uo[q]) * 0.5;
+  double uym = (uo[q] + uo[q-sy]) * 0.5;
+  double uzp = (uo[q+sz] + uo[q]) * 0.5;
+  double uzm = (uo[q] + uo[q-sz]) * 0.5;
+  double vxp = (vo[q+1] + vo[q]) * 0.5;
+  double vxm = (vo[q+1-sy] + vo[q-sy]) * 0.5;
+  double wxp = (wo[q+1] + wo[q]) * 0.5;
+  double wxm = (wo[q+1-sz] + wo[q-sz]) * 0.5;
+  double dqdxp = m.ap[i + 1] * (qr[q+1] - qr[q]);
+  double dqdxm = m.ap[i] * (qr[q] - qr[q-1]);
+  double dudyp = m.bv[j] * (uo[q+sy] - uo[q]);
+  double dudym = m.bv[j - 1] * (uo[q] - uo[q-sy]);
+  double dudzp = m.cw[k] * (uo[q+sz] - uo[q]);
+  double dudzm = m.cw[k - 1] * (uo[q] - uo[q-sz]);
+  double dvdxp = m.au[i] * (vo[q+1] - vo[q]);
+  double dvdxm = m.au[i] * (vo[q+1-sy] - vo[q-sy]);
+  double dwdxp = m.au[i] * (wo[q+1] - wo[q]);
+  double dwdxm = m.au[i] * (wo[q+1-sz] - wo[q-sz]);
+  double tvjp = 0.25 * (tv[q+1] + tv[q] + tv[q+1+sy] + tv[q+sy]);
+  double tvjm = 0.25 * (tv[q+1] + tv[q] + tv[q+1-sy] + tv[q-sy]);
+  double tvkp = 0.25 * (tv[q+1] + tv[q] + tv[q+1+sz] + tv[q+sz]);
+  double tvkm = 0.25 * (tv[q+1] + tv[q] + tv[q+1-sz] + tv[q-sz]);
+  double txxp = (ru1 + 2. * tv[q+1]) * dqdxp;
+  double txxm = (ru1 + 2. * tv[q]) * dqdxm;
   double tyyp = (ru1 + tvjp) * dudyp;
   double tyym = (ru1 + tvjm) * dudym;
   double tzzp = (ru1 + tvkp) * dudzp;
@@ -70,36 +70,36 @@ __device__ __forceinline__ double rhs_u(const Dims &d, const DevMetrics &m, doub
 __device__ __forceinline__ double rhs_v(const Dims &d, const DevMetrics &m, double ru1,
                                         const double *__restrict__ uo, const double *__restrict__ vo,
                                         const double *__restrict__ wo, const double *__restrict__ tv,
-                                        int i, int j, int k) {
+                                        int i, int j, int k, long long q, int sy, long long sz) {
   const double *qr = uo;
-  double vxp = (A(vo, i + 1, j, k) + A(vo, i, j, k)) * 0.5;
-  double vxm = (A(vo, i, j, k) + A(vo, i - 1, j, k)) * 0.5;
-  double vyp = (A(vo, i, j + 1, k) + A(vo, i, j, k)) * 0.5;
-  double vym = (A(vo, i, j, k) + A(vo, i, j - 1, k)) * 0.5;
-  double vzp = (A(vo, i, j, k + 1) + A(vo, i, j, k)) * 0.5;
-  double vzm = (A(vo, i, j, k) + A(vo, i, j, k - 1)) * 0.5;
-  double qyp = (A(qr, i, j + 1, k) + A(qr, i, j, k)) * 0.5;
-  double qym = (A(qr, i - 1, j + 1, k) + A(qr, i - 1, j, k)) * 0.5;
-  double wyp = (A(wo, i, j + 1, k) + A(wo, i, j, k)) * 0.5;
-  double wym = (A(wo, i, j + 1, k - 1) + A(wo, i, j, k - 1)) * 0.5;
-  double dvdxp = m.au[i] * (A(vo, i + 1, j, k) - A(vo, i, j, k));
-  double dvdxm = m.au[i - 1] * (A(vo, i, j, k) - A(vo, i - 1, j, k));
-  double dvdyp = m.bp[j + 1] * (A(vo, i, j + 1, k) - A(vo, i, j, k));
-  double dvdym = m.bp[j] * (A(vo, i, j, k) - A(vo, i, j - 1, k));
-  double dvdzp = m.cw[k] * (A(vo, i, j, k + 1) - A(vo, i, j, k));
-  double dvdzm = m.cw[k - 1] * (A(vo, i, j, k) - A(vo, i, j, k - 1));
-  double dudyp = m.bv[j] * (A(uo, i, j + 1, k) - A(uo, i, j, k));
-  double dudym = m.bv[j] * (A(uo, i - 1, j + 1, k) - A(uo, i - 1, j, k));
-  double dwdyp = m.bv[j] * (A(wo, i, j + 1, k) - A(wo, i, j, k));
-  double dwdym = m.bv[j] * (A(wo, i, j + 1, k - 1) - A(wo, i, j, k - 1));
-  double tvip = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i + 1, j + 1, k) + A(tv, i + 1, j, k));
-  double tvim = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i - 1, j + 1, k) + A(tv, i - 1, j, k));
-  double tvkp = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i, j + 1, k + 1) + A(tv, i, j, k + 1));
-  double tvkm = 0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i, j + 1, k - 1) + A(tv, i, j, k - 1));
+  double vxp = (vo[q+1] + vo[q]) * 0.5;
+  double vxm = (vo[q] + vo[q-1]) * 0.5;
+  double vyp = (vo[q+sy] + vo[q]) * 0.5;
+  double vym = (vo[q] + vo[q-sy]) * 0.5;
+  double vzp = (vo[q+sz] + vo[q]) * 0.5;
+  double vzm = (vo[q] + vo[q-sz]) * 0.5;
+  double qyp = (qr[q+sy] + qr[q]) * 0.5;
+  double qym = (qr[q-1+sy] + qr[q-1]) * 0.5;
+  double wyp = (wo[q+sy] + wo[q]) * 0.5;
+  double wym = (wo[q+sy-sz] + wo[q-sz]) * 0.5;
+  double dvdxp = m.au[i] * (vo[q+1] - vo[q]);
+  double dvdxm = m.au[i - 1] * (vo[q] - vo[q-1]);
+  double dvdyp = m.bp[j + 1] * (vo[q+sy] - vo[q]);
+  double dvdym = m.bp[j] * (vo[q] - vo[q-sy]);
+  double dvdzp = m.cw[k] * (vo[q+sz] - vo[q]);
+  double dvdzm = m.cw[k - 1] * (vo[q] - vo[q-sz]);
+  double dudyp = m.bv[j] * (uo[q+sy] - uo[q]);
+  double dudym = m.bv[j] * (uo[q-1+sy] - uo[q-1]);
+  double dwdyp = m.bv[j] * (wo[q+sy] - wo[q]);
+  double dwdym = m.bv[j] * (wo[q+sy-sz] - wo[q-sz]);
+  double tvip = 0.25 * (tv[q+sy] + tv[q] + tv[q+1+sy] + tv[q+1]);
+  double tvim = 0.25 * (tv[q+sy] + tv[q] + tv[q-1+sy] + tv[q-1]);
+  double tvkp = 0.25 * (tv[q+sy] + tv[q] + tv[q+sy+sz] + tv[q+sz]);
+  double tvkm = 0.25 * (tv[q+sy] + tv[q] + tv[q+sy-sz] + tv[q-sz]);
   double txxp = (ru1 + tvip) * dvdxp;
   double txxm = (ru1 + tvim) * dvdxm;
-  double tyyp = (ru1 + 2. * A(tv, i, j + 1, k)) * dvdyp;
-  double tyym = (ru1 + 2. * A(tv, i, j, k)) * dvdym;
+  double tyyp = (ru1 + 2. * tv[q+sy]) * dvdyp;
+  double tyym = (ru1 + 2. * tv[q]) * dvdym;
   double tzzp = (ru1 + tvkp) * dvdzp;
   double tzzm = (ru1 + tvkm) * dvdzm;
   double txyp = tvip * dudyp;
@@ -121,38 +121,38 @@ __device__ __forceinline__ double rhs_v(const Dims &d, const DevMetrics &m, doub
 __device__ __forceinline__ double rhs_w(const Dims &d, const DevMetrics &m, double ru1,
                                         const double *__restrict__ uo, const double *__restrict__ vo,
                                         const double *__restrict__ wo, const double *__restrict__ tv,
-                                        int i, int j, int k) {
+                                        int i, int j, int k, long long q, int sy, long long sz) {
   const double *qr = uo;
-  double wxp = (A(wo, i + 1, j, k) + A(wo, i, j, k)) * 0.5;
-  double wxm = (A(wo, i, j, k) + A(wo, i - 1, j, k)) * 0.5;
-  double wyp = (A(wo, i, j + 1, k) + A(wo, i, j, k)) * 0.5;
-  double wym = (A(wo, i, j, k) + A(wo, i, j - 1, k)) * 0.5;
-  double wzp = (A(wo, i, j, k + 1) + A(wo, i, j, k)) * 0.5;
-  double wzm = (A(wo, i, j, k) + A(wo, i, j, k - 1)) * 0.5;
-  double qzp = (A(qr, i, j, k + 1) + A(qr, i, j, k)) * 0.5;
-  double qzm = (A(qr, i - 1, j, k + 1) + A(qr, i - 1, j, k)) * 0.5;
-  double vzp = (A(vo, i, j, k + 1) + A(vo, i, j, k)) * 0.5;
-  double vzm = (A(vo, i, j - 1, k + 1) + A(vo, i, j - 1, k)) * 0.5;
-  double dwdxp = m.au[i] * (A(wo, i + 1, j, k) - A(wo, i, j, k));
-  double dwdxm = m.au[i - 1] * (A(wo, i, j, k) - A(wo, i - 1, j, k));
-  double dwdyp = m.bv[j] * (A(wo, i, j + 1, k) - A(wo, i, j, k));
-  double dwdym = m.bv[j - 1] * (A(wo, i, j, k) - A(wo, i, j - 1, k));
-  double dwdzp = m.cp[k + 1] * (A(wo, i, j, k + 1) - A(wo, i, j, k));
-  double dwdzm = m.cp[k] * (A(wo, i, j, k) - A(wo, i, j, k - 1));
-  double dudzp = m.cw[k] * (A(uo, i, j, k + 1) - A(uo, i, j, k));
-  double dudzm = m.cw[k] * (A(uo, i - 1, j, k + 1) - A(uo, i - 1, j, k));
-  double dvdzp = m.cw[k] * (A(vo, i, j, k + 1) - A(vo, i, j, k));
-  double dvdzm = m.cw[k] * (A(vo, i, j - 1, k + 1) - A(vo, i, j - 1, k));
-  double tvip = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i + 1, j, k + 1) + A(tv, i + 1, j, k));
-  double tvim = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i - 1, j, k + 1) + A(tv, i - 1, j, k));
-  double tvjp = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i, j + 1, k + 1) + A(tv, i, j + 1, k));
-  double tvjm = 0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i, j - 1, k + 1) + A(tv, i, j - 1, k));
+  double wxp = (wo[q+1] + wo[q]) * 0.5;
+  double wxm = (wo[q] + wo[q-1]) * 0.5;
+  double wyp = (wo[q+sy] + wo[q]) * 0.5;
+  double wym = (wo[q] + wo[q-sy]) * 0.5;
+  double wzp = (wo[q+sz] + wo[q]) * 0.5;
+  double wzm = (wo[q] + wo[q-sz]) * 0.5;
+  double qzp = (qr[q+sz] + qr[q]) * 0.5;
+  double qzm = (qr[q-1+sz] + qr[q-1]) * 0.5;
+  double vzp = (vo[q+sz] + vo[q]) * 0.5;
+  double vzm = (vo[q-sy+sz] + vo[q-sy]) * 0.5;
+  double dwdxp = m.au[i] * (wo[q+1] - wo[q]);
+  double dwdxm = m.au[i - 1] * (wo[q] - wo[q-1]);
+  double dwdyp = m.bv[j] * (wo[q+sy] - wo[q]);
+  double dwdym = m.bv[j - 1] * (wo[q] - wo[q-sy]);
+  double dwdzp = m.cp[k + 1] * (wo[q+sz] - wo[q]);
+  double dwdzm = m.cp[k] * (wo[q] - wo[q-sz]);
+  double dudzp = m.cw[k] * (uo[q+sz] - uo[q]);
+  double dudzm = m.cw[k] * (uo[q-1+sz] - uo[q-1]);
+  double dvdzp = m.cw[k] * (vo[q+sz] - vo[q]);
+  double dvdzm = m.cw[k] * (vo[q-sy+sz] - vo[q-sy]);
+  double tvip = 0.25 * (tv[q+sz] + tv[q] + tv[q+1+sz] + tv[q+1]);
+  double tvim = 0.25 * (tv[q+sz] + tv[q] + tv[q-1+sz] + tv[q-1]);
+  double tvjp = 0.25 * (tv[q+sz] + tv[q] + tv[q+sy+sz] + tv[q+sy]);
+  double tvjm = 0.25 * (tv[q+sz] + tv[q] + tv[q-sy+sz] + tv[q-sy]);
   double txxp = (ru1 + tvip) * dwdxp;
   double txxm = (ru1 + tvim) * dwdxm;
   double tyyp = (ru1 + tvjp) * dwdyp;
   double tyym = (ru1 + tvjm) * dwdym;
-  double tzzp = (ru1 + 2. * A(tv, i, j, k + 1)) * dwdzp;
-  double tzzm = (ru1 + 2. * A(tv, i, j, k)) * dwdzm;
+  double tzzp = (ru1 + 2. * tv[q+sz]) * dwdzp;
+  double tzzm = (ru1 + 2. * tv[q]) * dwdzm;
   double txzp = tvip * dudzp;
   double txzm = tvim * dudzm;
   double tyzp = tvjp * dvdzp;
@@ -182,17 +182,19 @@ __global__ void __launch_bounds__(BX *BY *BZ)
   int k = 1 + threadIdx.z + blockIdx.z * BZ;
   if (i > d.nx || j > d.ny || k > d.nz) return;
   long long q = fidx(d, i, j, k);
+  const int sy = d.nx;
+  const long long sz = (long long)d.nx * d.ny;
   const double coef = 0.5 * alfxdt, coefd = alfxdt;
   const bool kin = (k >= d.kz1 && k <= d.kz2), jin = (j >= d.jy1 && j <= d.jy2);
   // ---- u ----
   double uval = 0.0;
   if (kin && jin && i >= d.ibu && i <= d.ieu) {
-    double ur = rhs_u(d, m, s.ru1, uo, vo, wo, tv, i, j, k);
-    double ustar = uo[q] + gamxdt * ur + rhoxdt * ua[q] - alfxdt * m.au[i] * (A(p, i + 1, j, k) - p[q]) +
+    double ur = rhs_u(d, m, s.ru1, uo, vo, wo, tv, i, j, k, q, sy, sz);
+    double ustar = uo[q] + gamxdt * ur + rhoxdt * ua[q] - alfxdt * m.au[i] * (p[q + 1] - p[q]) +
                    coef * 0.0 - alfxdt * s.dpdx;
     if (s.idens == 1)
       ustar = ustar - coefd * 0.50 * s.grav *
-                          ((A(dens, i + 1, j, k) - m.dens_bg[i + d.nx * (j - 1)]) +
+                          ((dens[q + 1] - m.dens_bg[i + d.nx * (j - 1)]) +
                            (dens[q] - m.dens_bg[(i - 1) + d.nx * (j - 1)]));
     ua[q] = ur;
     if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0. - ustar) * alfxdt * 1.0;
@@ -203,8 +205,8 @@ __global__ void __launch_bounds__(BX *BY *BZ)
   // ---- v ----
   double vval = 0.0;
   if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
-    double vr = rhs_v(d, m, s.ru1, uo, vo, wo, tv, i, j, k);
-    double vstar = vo[q] + gamxdt * vr + rhoxdt * va[q] - alfxdt * m.bv[j] * (A(p, i, j + 1, k) - p[q]) +
+    double vr = rhs_v(d, m, s.ru1, uo, vo, wo, tv, i, j, k, q, sy, sz);
+    double vstar = vo[q] + gamxdt * vr + rhoxdt * va[q] - alfxdt * m.bv[j] * (p[q + sy] - p[q]) +
                    coef * 0.0 - alfxdt * s.dpdy;
     va[q] = vr;
     if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0. - vstar) * alfxdt * 1.0;
@@ -215,8 +217,8 @@ __global__ void __launch_bounds__(BX *BY *BZ)
   // ---- w ----
   double wval = 0.0;
   if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
-    double wr = rhs_w(d, m, s.ru1, uo, vo, wo, tv, i, j, k);
-    double wstar = wo[q] + gamxdt * wr + rhoxdt * wa[q] - alfxdt * m.cw[k] * (A(p, i, j, k + 1) - p[q]) +
+    double wr = rhs_w(d, m, s.ru1, uo, vo, wo, tv, i, j, k, q, sy, sz);
+    double wstar = wo[q] + gamxdt * wr + rhoxdt * wa[q] - alfxdt * m.cw[k] * (p[q + sz] - p[q]) +
                    coef * 0.0 - alfxdt * s.dpdz;
     wa[q] = wr;
     if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1. - wstar) * alfxdt * 1.0;
@@ -353,13 +355,15 @@ __global__ void __launch_bounds__(BX *BY *BZ)
   int k = 1 + threadIdx.z + blockIdx.z * BZ;
   if (i > d.nx || j > d.ny || k > d.nz) return;
   long long q = fidx(d, i, j, k);
+  const int sy = d.nx;
+  const long long sz = (long long)d.nx * d.ny;
   bool kin = k >= d.kz1 && k <= d.kz2, jin = j >= d.jy1 && j <= d.jy2;
   if (kin && jin && i >= d.ibu && i <= d.ieu)
-    uo[q] = us[q] - m.au[i] * (A(dp, i + 1, j, k) - dp[q]) * alfxdt;
+    uo[q] = us[q] - m.au[i] * (dp[q + 1] - dp[q]) * alfxdt;
   if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2)
-    vo[q] = vs[q] - m.bv[j] * (A(dp, i, j + 1, k) - dp[q]) * alfxdt;
+    vo[q] = vs[q] - m.bv[j] * (dp[q + sy] - dp[q]) * alfxdt;
   if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2)
-    wo[q] = ws[q] - m.cw[k] * (A(dp, i, j, k + 1) - dp[q]) * alfxdt;
+    wo[q] = ws[q] - m.cw[k] * (dp[q + sz] - dp[q]) * alfxdt;
 }
 
 // pref = sum_j (p+dp)(ix1,j,2) / (NY-2), summed in order (src/Eddy6.f:2802)

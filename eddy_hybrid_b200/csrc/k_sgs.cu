@@ -56,35 +56,38 @@ __global__ void __launch_bounds__(BX *BY *BZ)
   if (i < d.ix1 || i > d.ix2 || jj > d.ny || k < d.kz1 || k > d.kz2) return;
   // periodic y-ghost rows take the value of the mapped interior row
   int j = jj == 1 ? d.jy2 : (jj == d.ny ? 2 : jj);
+  const int sy = d.nx;
+  const long long sz = (long long)d.nx * d.ny;
+  long long q = fidx(d, i, j, k);
   const double *au = m.au, *bv = m.bv, *cw = m.cw;
-  double dudxp = au[i] * (A(uc, i + 1, j, k) - A(uc, i, j, k));
-  double dudxm = au[i - 1] * (A(uc, i, j, k) - A(uc, i - 1, j, k));
-  double dudyp = bv[j] * (A(uc, i, j + 1, k) - A(uc, i, j, k));
-  double dudym = bv[j - 1] * (A(uc, i, j, k) - A(uc, i, j - 1, k));
-  double dudzp = cw[k] * (A(uc, i, j, k + 1) - A(uc, i, j, k));
-  double dudzm = cw[k - 1] * (A(uc, i, j, k) - A(uc, i, j, k - 1));
-  double dvdxp = au[i] * (A(vc, i + 1, j, k) - A(vc, i, j, k));
-  double dvdxm = au[i - 1] * (A(vc, i, j, k) - A(vc, i - 1, j, k));
-  double dvdyp = bv[j] * (A(vc, i, j + 1, k) - A(vc, i, j, k));
-  double dvdym = bv[j - 1] * (A(vc, i, j, k) - A(vc, i, j - 1, k));
-  double dvdzp = cw[k] * (A(vc, i, j, k + 1) - A(vc, i, j, k));
-  double dvdzm = cw[k - 1] * (A(vc, i, j, k) - A(vc, i, j, k - 1));
-  double dwdxp = au[i] * (A(wc, i + 1, j, k) - A(wc, i, j, k));
-  double dwdxm = au[i - 1] * (A(wc, i, j, k) - A(wc, i - 1, j, k));
-  double dwdyp = bv[j] * (A(wc, i, j + 1, k) - A(wc, i, j, k));
-  double dwdym = bv[j - 1] * (A(wc, i, j, k) - A(wc, i, j - 1, k));
-  double dwdzp = cw[k] * (A(wc, i, j, k + 1) - A(wc, i, j, k));
-  double dwdzm = cw[k - 1] * (A(wc, i, j, k) - A(wc, i, j, k - 1));
+  double dudxp = au[i] * (uc[q+1] - uc[q]);
+  double dudxm = au[i - 1] * (uc[q] - uc[q-1]);
+  double dudyp = bv[j] * (uc[q+sy] - uc[q]);
+  double dudym = bv[j - 1] * (uc[q] - uc[q-sy]);
+  double dudzp = cw[k] * (uc[q+sz] - uc[q]);
+  double dudzm = cw[k - 1] * (uc[q] - uc[q-sz]);
+  double dvdxp = au[i] * (vc[q+1] - vc[q]);
+  double dvdxm = au[i - 1] * (vc[q] - vc[q-1]);
+  double dvdyp = bv[j] * (vc[q+sy] - vc[q]);
+  double dvdym = bv[j - 1] * (vc[q] - vc[q-sy]);
+  double dvdzp = cw[k] * (vc[q+sz] - vc[q]);
+  double dvdzm = cw[k - 1] * (vc[q] - vc[q-sz]);
+  double dwdxp = au[i] * (wc[q+1] - wc[q]);
+  double dwdxm = au[i - 1] * (wc[q] - wc[q-1]);
+  double dwdyp = bv[j] * (wc[q+sy] - wc[q]);
+  double dwdym = bv[j - 1] * (wc[q] - wc[q-sy]);
+  double dwdzp = cw[k] * (wc[q+sz] - wc[q]);
+  double dwdzm = cw[k - 1] * (wc[q] - wc[q-sz]);
   double sxx = 0.5 * (dudxp + dudxm);
   double syy = 0.5 * (dvdyp + dvdym);
   double szz = 0.5 * (dwdzp + dwdzm);
   double sxy = 0.25 * (dudyp + dudym + dvdxp + dvdxm);
   double sxz = 0.25 * (dudzp + dudzm + dwdxp + dwdxm);
   double syz = 0.25 * (dwdyp + dwdym + dvdzp + dvdzm);
-  long long q = fidx(d, i, jj, k), n = d.ncell;
-  sij[q] = sxx; sij[q + n] = syy; sij[q + 2 * n] = szz;
-  sij[q + 3 * n] = sxy; sij[q + 4 * n] = sxz; sij[q + 5 * n] = syz;
-  gs[q] = sqrt(2. * (sxx * sxx + syy * syy + szz * szz) + 4. * (sxy * sxy + syz * syz + sxz * sxz));
+  long long qo = fidx(d, i, jj, k), n = d.ncell;
+  sij[qo] = sxx; sij[qo + n] = syy; sij[qo + 2 * n] = szz;
+  sij[qo + 3 * n] = sxy; sij[qo + 4 * n] = sxz; sij[qo + 5 * n] = syz;
+  gs[qo] = sqrt(2. * (sxx * sxx + syy * syy + szz * szz) + 4. * (sxy * sxy + syz * syz + sxz * sxz));
 }
 
 // the 22 filtered quantities at one point from the base fields
@@ -147,6 +150,7 @@ __global__ void __launch_bounds__(128)
   else if (k == d.kz2 && top_onesided) { zk[0] = d.kz2; zk[1] = d.kz2 - 1; zk[2] = d.kz2 - 2; }
   else { zk[0] = k - 1; zk[1] = k; zk[2] = k + 1; }
   const double wy[3] = {0.25, 0.50, 0.25};
+  const long long q0 = fidx(d, i, j, k), nxy = (long long)d.nx * d.ny;
   double Z[NQ];
 #pragma unroll
   for (int c = 0; c < NQ; c++) Z[c] = 0.;
@@ -161,7 +165,8 @@ __global__ void __launch_bounds__(128)
       for (int c = 0; c < NQ; c++) X[c] = 0.;
       for (int e = 0; e < 3; e++) {
         Base bs;
-        load_base(d, fidx(d, xi[e], jj, zk[a]), uc, vc, wc, gs, sij, bs);
+        load_base(d, q0 + (xi[e] - i) + (long long)(jj - j) * d.nx + (long long)(zk[a] - k) * nxy, uc, vc, wc, gs,
+                  sij, bs);
 #pragma unroll
         for (int c = 0; c < NQ; c++) {
           double t = wx[e] * quant(bs, c);
