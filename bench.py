@@ -51,12 +51,17 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--small", action="store_true", help="tiny grid (profiling / smoke)")
+    ap.add_argument("--small", action="store_true", help="tiny grid (smoke)")
+    ap.add_argument("--medium", action="store_true",
+                    help="128x192x128 grid (~3M cells, ~1 GB on the device) for ncu captures")
     return ap.parse_args()
 
 
-def workload(small=False):
+def workload(small=False, medium=False):
     from eddy_hybrid_b200 import config
+    if medium:
+        return config.Workload("wake_128x192x128", mx=192, ly=128, nz_=128, re=1e4, fr=1.0, dt=5e-4,
+                               sphere=False)
     if small:
         return config.Workload("wake_64x48x32", mx=48, ly=32, nz_=64, re=1e4, fr=1.0, dt=5e-4,
                                sphere=False)
@@ -178,7 +183,7 @@ def main():
     import eddy_hybrid_b200 as eb
     from eddy_hybrid_b200 import config
 
-    w = workload(args.small)
+    w = workload(args.small, args.medium)
     g = eb.Solver(w, device=local if world > 1 else 0)
     fields = config.initial_fields(w, g.metric("dens_bg")[: w.nx])
     g.load_initial(fields)
@@ -290,7 +295,7 @@ def main():
         "kernels": kernels,
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.small:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not (args.small or args.medium):
         line["cpu_baseline"] = cpu_baseline(1)
     if rank == 0:
         print(json.dumps(line), flush=True)
