@@ -87,6 +87,8 @@ SIGNATURES = {
     "eddy_max_divergence": ([C.c_void_p, _DP], C.c_int),
     "eddy_profile_enable": ([C.c_void_p, C.c_uint], C.c_int),
     "eddy_profile_read": ([C.c_void_p, _DP, C.POINTER(C.c_longlong)], C.c_int),
+    "eddy_max_divergence_noalloc": ([C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "eddy_sync": ([C.c_void_p], C.c_int),
     "eddy_last_error": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
     "eddy_launch_count": ([C.c_void_p], C.c_int64),

@@ -24,6 +24,7 @@ UNITS = {
     "k_poisson.cu": ["-fmad=false"],
     "k_density.cu": ["-fmad=false"],
     "k_sgs.cu": ["-fmad=false"],
+    "k_noalloc.cu": ["-fmad=false"],
     "host_eigen.cpp": [],
 }
 

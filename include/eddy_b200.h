@@ -139,6 +139,29 @@ int eddy_max_divergence(eddy_ctx *ctx, double *out);
 int eddy_profile_enable(eddy_ctx *ctx, unsigned mask);
 int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts);
 
+/* Largest grid (NX*NY*NZ, ghost layers included) eddy_max_divergence_noalloc
+ * accepts: the size its fixed device scratch array was built for. */
+#define EDDY_NOALLOC_MAX_CELLS (1 << 28)
+
+/* No counterpart in the reference.  max |div u| over the interior, like
+ * eddy_max_divergence, for callers that cannot call cudaMalloc (memory owned
+ * by another allocator, code where allocation is not allowed, or no solver
+ * context at all).  Allocates nothing: its scratch is a fixed 512 KiB
+ * file-scope device array that every GPU loading this library holds until
+ * the process exits.  u, v, w: device arrays (NX,NY,NZ), Fortran order;
+ * ap, bp, cp: device copies of the 1-D metric arrays AP(1:NX), BP(1:NY),
+ * CP(1:NZ); out: device pointer to one double that receives the result;
+ * stream: cudaStream_t (NULL = default stream).  Asynchronous: read out after
+ * synchronising the stream.  Returns EDDY_EINVAL when NX*NY*NZ exceeds
+ * EDDY_NOALLOC_MAX_CELLS.  The first call on a device looks up the scratch
+ * array's device address for that device, so make that first call before any
+ * stream capture.  All calls share the one scratch array (each call writes
+ * every slot it reads, so nothing needs clearing): calls that overlap on the
+ * GPU race and must be ordered by the caller. */
+int eddy_max_divergence_noalloc(int nx, int ny, int nz, const double *u, const double *v,
+                                const double *w, const double *ap, const double *bp,
+                                const double *cp, double *out, void *stream);
+
 int eddy_sync(eddy_ctx *ctx);
 /* Copy the last error message (NUL-terminated, truncated to len). */
 int eddy_last_error(eddy_ctx *ctx, char *buf, int len);
