@@ -5,9 +5,11 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "eddy_internal.h"
+#include "tma_ring.cuh"
 
 int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, double sgn, int zero);
 
@@ -224,6 +226,7 @@ void free_all(eddy_ctx *ctx) {
   double *o[] = {ctx->dens_alt, ctx->uc, ctx->vc, ctx->wc, ctx->sij, ctx->gs, ctx->mm, ctx->lm, ctx->dxdydz,
                  ctx->ilm2, ctx->imm2, ctx->scal};
   for (double *p : o) if (p) cudaFree(p);
+  if (ctx->err_flag) cudaFree(ctx->err_flag);
   poisson_plan_destroy(ctx);
   for (ProfEvent &e : ctx->prof_ev) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (ProfEvent &e : ctx->prof_pool) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -232,6 +235,22 @@ void free_all(eddy_ctx *ctx) {
 }
 
 int check_ctx(eddy_ctx *ctx) { return ctx ? EDDY_OK : EDDY_EINVAL; }
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
 
 void scheme(int ischm, double gam[3], double rho[3], double alf[3]) {
   if (ischm == 1) {
@@ -245,6 +264,35 @@ void scheme(int ischm, double gam[3], double rho[3], double alf[3]) {
 }
 
 }  // namespace
+
+int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int nz, int bx, int by, int esize) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return -1;
+  cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  cuuint64_t gstr[2] = {(cuuint64_t)nx * esize, (cuuint64_t)nx * ny * esize};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  cuuint32_t est[3] = {1, 1, 1};
+  CUtensorMapDataType dt = esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  CUresult r = fn(map, dt, 3, const_cast<void *>(base), gdim, gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : (int)r;
+}
+
+const CUtensorMap *ctx_tensor_map(eddy_ctx *ctx, const double *ptr, int bx, int by) {
+  for (TmaEntry &e : ctx->tmaps)
+    if (e.ptr == ptr && e.bx == bx && e.by == by) return &e.map;
+  TmaEntry e;
+  e.ptr = ptr;
+  e.bx = bx;
+  e.by = by;
+  int r = make_tensor_map_3d(&e.map, ptr, ctx->d.nx, ctx->d.ny, ctx->d.nz, bx, by, 8);
+  if (r != 0) {
+    ctx->err = "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")";
+    return nullptr;
+  }
+  ctx->tmaps.push_back(e);
+  return &ctx->tmaps.back().map;
+}
 
 extern "C" {
 
@@ -262,6 +310,8 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
     return rc;
   };
   if (p.nx < 6 || p.ny < 4 || p.nz < 6) return fail(EDDY_EINVAL, "grid too small (need NX,NZ >= 6, NY >= 4)");
+  if (p.nx % 2 != 0)
+    return fail(EDDY_EINVAL, "NX must be even (TMA rows of FP64 need 16-byte strides)");
   if (p.ischm != 3 && p.ischm != 1) return fail(EDDY_EINVAL, "ischm must be 1 or 3");
   if (p.isgs != 0 && p.isgs != 1 && p.isgs != 2)
     return fail(EDDY_EINVAL, "only isgs 0 (none), 1 (Smagorinsky), 2 (dynamic, y average) are supported");
@@ -301,6 +351,8 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   cudaMemset(ctx->imm2, 0, n2xz);
   if (cudaMalloc(&ctx->scal, sizeof(double) * 32) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
   cudaMemset(ctx->scal, 0, sizeof(double) * 32);
+  if (cudaMalloc(&ctx->err_flag, sizeof(int)) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
+  cudaMemset(ctx->err_flag, 0, sizeof(int));
   rc = poisson_plan_create(ctx);
   if (rc) return fail(rc, nullptr);
   if (p.isgs != 0) {
@@ -558,6 +610,13 @@ int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts) {
 int eddy_sync(eddy_ctx *ctx) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  int e = 0;
+  EDDY_CUDA(cudaMemcpy(&e, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    cudaMemset(ctx->err_flag, 0, sizeof(int));
+    ctx->err = "a device-side bounded wait expired (TMA plane pipeline)";
+    return EDDY_ETIMEOUT;
+  }
   return EDDY_OK;
 }
 

@@ -2,6 +2,7 @@
 // the CUDA translation units of libeddy_b200.so.
 #pragma once
 #include <cublas_v2.h>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -59,6 +60,17 @@ enum {
   PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_NCAT
 };
 
+// tensor maps of nine fields, passed by value to TMA kernels
+struct alignas(64) TmaMaps9 {
+  CUtensorMap m[9];
+};
+
+struct TmaEntry {
+  const void *ptr;
+  int bx, by;
+  alignas(64) CUtensorMap map;
+};
+
 struct ProfEvent {
   int cat;
   cudaEvent_t a, b;
@@ -90,6 +102,8 @@ struct eddy_ctx {
   std::vector<ProfEvent> prof_ev;   // recorded in this window
   std::vector<ProfEvent> prof_pool; // reusable events
   double prof_ms[PROF_NCAT] = {};
+  int *err_flag = nullptr;            // device word set by kernels whose bounded waits expire
+  std::vector<TmaEntry> tmaps;        // cached tensor maps per (field pointer, box)
   long long prof_n[PROF_NCAT] = {};
 };
 
@@ -142,6 +156,10 @@ struct ProfScope {
 __host__ __device__ inline long long fidx(const Dims &d, int i, int j, int k) {
   return (long long)(i - 1) + (long long)d.nx * ((long long)(j - 1) + (long long)d.ny * (long long)(k - 1));
 }
+
+// tensor map over an (NX,NY,NZ) FP64 field with a (bx,by,1) box, cached per
+// pointer; nullptr on failure (message in ctx->err)
+const CUtensorMap *ctx_tensor_map(eddy_ctx *ctx, const double *ptr, int bx, int by);
 
 // kernel drivers (each returns EDDY_* status)
 int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);

@@ -5,6 +5,7 @@
 // reference's operation order (src/rhs.f, src/timeindeg.f); the explicit
 // (non Crank-Nicolson) branch of the Cartesian equations.
 #include "eddy_internal.h"
+#include "tma_ring.cuh"
 
 #define A(a, i, j, k) (a)[fidx(d, (i), (j), (k))]
 
@@ -14,39 +15,36 @@ constexpr int BX = 32, BY = 4, BZ = 2;
 
 // ---------------------------------------------------------------------------
 // u-momentum explicit RHS at a u point (src/rhs.f:77-172)
-__device__ __forceinline__ double rhs_u(const Dims &d, const DevMetrics &m, double ru1,
-                                        const double *__restrict__ uo, const double *__restrict__ vo,
-                                        const double *__restrict__ wo, const double *__restrict__ tv,
-                                        int i, int j, int k, long long q, int sy, long long sz) {
-  const double *qr = uo;
-  double qxp = (qr[q+1] + qr[q]) * 0.5;
-  double qxm = (qr[q] + qr[q-1]) * 0.5;
-  double uxp = (uo[q+1] + uo[q]) * 0.5;
-  double uxm = (uo[q] + uo[q-1]) * 0.5;
-  double uyp = (uo[q+sy] + uo[q]) * 0.5;
-  double uym = (uo[q] + uo[q-sy]) * 0.5;
-  double uzp = (uo[q+sz] + uo[q]) * 0.5;
-  double uzm = (uo[q] + uo[q-sz]) * 0.5;
-  double vxp = (vo[q+1] + vo[q]) * 0.5;
-  double vxm = (vo[q+1-sy] + vo[q-sy]) * 0.5;
-  double wxp = (wo[q+1] + wo[q]) * 0.5;
-  double wxm = (wo[q+1-sz] + wo[q-sz]) * 0.5;
-  double dqdxp = m.ap[i + 1] * (qr[q+1] - qr[q]);
-  double dqdxm = m.ap[i] * (qr[q] - qr[q-1]);
-  double dudyp = m.bv[j] * (uo[q+sy] - uo[q]);
-  double dudym = m.bv[j - 1] * (uo[q] - uo[q-sy]);
-  double dudzp = m.cw[k] * (uo[q+sz] - uo[q]);
-  double dudzm = m.cw[k - 1] * (uo[q] - uo[q-sz]);
-  double dvdxp = m.au[i] * (vo[q+1] - vo[q]);
-  double dvdxm = m.au[i] * (vo[q+1-sy] - vo[q-sy]);
-  double dwdxp = m.au[i] * (wo[q+1] - wo[q]);
-  double dwdxm = m.au[i] * (wo[q+1-sz] - wo[q-sz]);
-  double tvjp = 0.25 * (tv[q+1] + tv[q] + tv[q+1+sy] + tv[q+sy]);
-  double tvjm = 0.25 * (tv[q+1] + tv[q] + tv[q+1-sy] + tv[q-sy]);
-  double tvkp = 0.25 * (tv[q+1] + tv[q] + tv[q+1+sz] + tv[q+sz]);
-  double tvkm = 0.25 * (tv[q+1] + tv[q] + tv[q+1-sz] + tv[q-sz]);
-  double txxp = (ru1 + 2. * tv[q+1]) * dqdxp;
-  double txxm = (ru1 + 2. * tv[q]) * dqdxm;
+template <class Acc>
+__device__ __forceinline__ double rhs_u(const Acc &S, const DevMetrics &m, double ru1, int i, int j, int k) {
+  double qxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * 0.5;
+  double qxm = (S.u(0, 0, 0) + S.u(-1, 0, 0)) * 0.5;
+  double uxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * 0.5;
+  double uxm = (S.u(0, 0, 0) + S.u(-1, 0, 0)) * 0.5;
+  double uyp = (S.u(0, 1, 0) + S.u(0, 0, 0)) * 0.5;
+  double uym = (S.u(0, 0, 0) + S.u(0, -1, 0)) * 0.5;
+  double uzp = (S.u(0, 0, 1) + S.u(0, 0, 0)) * 0.5;
+  double uzm = (S.u(0, 0, 0) + S.u(0, 0, -1)) * 0.5;
+  double vxp = (S.v(1, 0, 0) + S.v(0, 0, 0)) * 0.5;
+  double vxm = (S.v(1, -1, 0) + S.v(0, -1, 0)) * 0.5;
+  double wxp = (S.w(1, 0, 0) + S.w(0, 0, 0)) * 0.5;
+  double wxm = (S.w(1, 0, -1) + S.w(0, 0, -1)) * 0.5;
+  double dqdxp = m.ap[i + 1] * (S.u(1, 0, 0) - S.u(0, 0, 0));
+  double dqdxm = m.ap[i] * (S.u(0, 0, 0) - S.u(-1, 0, 0));
+  double dudyp = m.bv[j] * (S.u(0, 1, 0) - S.u(0, 0, 0));
+  double dudym = m.bv[j - 1] * (S.u(0, 0, 0) - S.u(0, -1, 0));
+  double dudzp = m.cw[k] * (S.u(0, 0, 1) - S.u(0, 0, 0));
+  double dudzm = m.cw[k - 1] * (S.u(0, 0, 0) - S.u(0, 0, -1));
+  double dvdxp = m.au[i] * (S.v(1, 0, 0) - S.v(0, 0, 0));
+  double dvdxm = m.au[i] * (S.v(1, -1, 0) - S.v(0, -1, 0));
+  double dwdxp = m.au[i] * (S.w(1, 0, 0) - S.w(0, 0, 0));
+  double dwdxm = m.au[i] * (S.w(1, 0, -1) - S.w(0, 0, -1));
+  double tvjp = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, 1, 0) + S.t(0, 1, 0));
+  double tvjm = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, -1, 0) + S.t(0, -1, 0));
+  double tvkp = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, 0, 1) + S.t(0, 0, 1));
+  double tvkm = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, 0, -1) + S.t(0, 0, -1));
+  double txxp = (ru1 + 2. * S.t(1, 0, 0)) * dqdxp;
+  double txxm = (ru1 + 2. * S.t(0, 0, 0)) * dqdxm;
   double tyyp = (ru1 + tvjp) * dudyp;
   double tyym = (ru1 + tvjm) * dudym;
   double tzzp = (ru1 + tvkp) * dudzp;
@@ -67,39 +65,36 @@ __device__ __forceinline__ double rhs_u(const Dims &d, const DevMetrics &m, doub
 }
 
 // v-momentum (src/rhs.f:219-321)
-__device__ __forceinline__ double rhs_v(const Dims &d, const DevMetrics &m, double ru1,
-                                        const double *__restrict__ uo, const double *__restrict__ vo,
-                                        const double *__restrict__ wo, const double *__restrict__ tv,
-                                        int i, int j, int k, long long q, int sy, long long sz) {
-  const double *qr = uo;
-  double vxp = (vo[q+1] + vo[q]) * 0.5;
-  double vxm = (vo[q] + vo[q-1]) * 0.5;
-  double vyp = (vo[q+sy] + vo[q]) * 0.5;
-  double vym = (vo[q] + vo[q-sy]) * 0.5;
-  double vzp = (vo[q+sz] + vo[q]) * 0.5;
-  double vzm = (vo[q] + vo[q-sz]) * 0.5;
-  double qyp = (qr[q+sy] + qr[q]) * 0.5;
-  double qym = (qr[q-1+sy] + qr[q-1]) * 0.5;
-  double wyp = (wo[q+sy] + wo[q]) * 0.5;
-  double wym = (wo[q+sy-sz] + wo[q-sz]) * 0.5;
-  double dvdxp = m.au[i] * (vo[q+1] - vo[q]);
-  double dvdxm = m.au[i - 1] * (vo[q] - vo[q-1]);
-  double dvdyp = m.bp[j + 1] * (vo[q+sy] - vo[q]);
-  double dvdym = m.bp[j] * (vo[q] - vo[q-sy]);
-  double dvdzp = m.cw[k] * (vo[q+sz] - vo[q]);
-  double dvdzm = m.cw[k - 1] * (vo[q] - vo[q-sz]);
-  double dudyp = m.bv[j] * (uo[q+sy] - uo[q]);
-  double dudym = m.bv[j] * (uo[q-1+sy] - uo[q-1]);
-  double dwdyp = m.bv[j] * (wo[q+sy] - wo[q]);
-  double dwdym = m.bv[j] * (wo[q+sy-sz] - wo[q-sz]);
-  double tvip = 0.25 * (tv[q+sy] + tv[q] + tv[q+1+sy] + tv[q+1]);
-  double tvim = 0.25 * (tv[q+sy] + tv[q] + tv[q-1+sy] + tv[q-1]);
-  double tvkp = 0.25 * (tv[q+sy] + tv[q] + tv[q+sy+sz] + tv[q+sz]);
-  double tvkm = 0.25 * (tv[q+sy] + tv[q] + tv[q+sy-sz] + tv[q-sz]);
+template <class Acc>
+__device__ __forceinline__ double rhs_v(const Acc &S, const DevMetrics &m, double ru1, int i, int j, int k) {
+  double vxp = (S.v(1, 0, 0) + S.v(0, 0, 0)) * 0.5;
+  double vxm = (S.v(0, 0, 0) + S.v(-1, 0, 0)) * 0.5;
+  double vyp = (S.v(0, 1, 0) + S.v(0, 0, 0)) * 0.5;
+  double vym = (S.v(0, 0, 0) + S.v(0, -1, 0)) * 0.5;
+  double vzp = (S.v(0, 0, 1) + S.v(0, 0, 0)) * 0.5;
+  double vzm = (S.v(0, 0, 0) + S.v(0, 0, -1)) * 0.5;
+  double qyp = (S.u(0, 1, 0) + S.u(0, 0, 0)) * 0.5;
+  double qym = (S.u(-1, 1, 0) + S.u(-1, 0, 0)) * 0.5;
+  double wyp = (S.w(0, 1, 0) + S.w(0, 0, 0)) * 0.5;
+  double wym = (S.w(0, 1, -1) + S.w(0, 0, -1)) * 0.5;
+  double dvdxp = m.au[i] * (S.v(1, 0, 0) - S.v(0, 0, 0));
+  double dvdxm = m.au[i - 1] * (S.v(0, 0, 0) - S.v(-1, 0, 0));
+  double dvdyp = m.bp[j + 1] * (S.v(0, 1, 0) - S.v(0, 0, 0));
+  double dvdym = m.bp[j] * (S.v(0, 0, 0) - S.v(0, -1, 0));
+  double dvdzp = m.cw[k] * (S.v(0, 0, 1) - S.v(0, 0, 0));
+  double dvdzm = m.cw[k - 1] * (S.v(0, 0, 0) - S.v(0, 0, -1));
+  double dudyp = m.bv[j] * (S.u(0, 1, 0) - S.u(0, 0, 0));
+  double dudym = m.bv[j] * (S.u(-1, 1, 0) - S.u(-1, 0, 0));
+  double dwdyp = m.bv[j] * (S.w(0, 1, 0) - S.w(0, 0, 0));
+  double dwdym = m.bv[j] * (S.w(0, 1, -1) - S.w(0, 0, -1));
+  double tvip = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(1, 1, 0) + S.t(1, 0, 0));
+  double tvim = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(-1, 1, 0) + S.t(-1, 0, 0));
+  double tvkp = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(0, 1, 1) + S.t(0, 0, 1));
+  double tvkm = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(0, 1, -1) + S.t(0, 0, -1));
   double txxp = (ru1 + tvip) * dvdxp;
   double txxm = (ru1 + tvim) * dvdxm;
-  double tyyp = (ru1 + 2. * tv[q+sy]) * dvdyp;
-  double tyym = (ru1 + 2. * tv[q]) * dvdym;
+  double tyyp = (ru1 + 2. * S.t(0, 1, 0)) * dvdyp;
+  double tyym = (ru1 + 2. * S.t(0, 0, 0)) * dvdym;
   double tzzp = (ru1 + tvkp) * dvdzp;
   double tzzm = (ru1 + tvkm) * dvdzm;
   double txyp = tvip * dudyp;
@@ -118,41 +113,38 @@ __device__ __forceinline__ double rhs_v(const Dims &d, const DevMetrics &m, doub
 }
 
 // w-momentum (src/rhs.f:347-422)
-__device__ __forceinline__ double rhs_w(const Dims &d, const DevMetrics &m, double ru1,
-                                        const double *__restrict__ uo, const double *__restrict__ vo,
-                                        const double *__restrict__ wo, const double *__restrict__ tv,
-                                        int i, int j, int k, long long q, int sy, long long sz) {
-  const double *qr = uo;
-  double wxp = (wo[q+1] + wo[q]) * 0.5;
-  double wxm = (wo[q] + wo[q-1]) * 0.5;
-  double wyp = (wo[q+sy] + wo[q]) * 0.5;
-  double wym = (wo[q] + wo[q-sy]) * 0.5;
-  double wzp = (wo[q+sz] + wo[q]) * 0.5;
-  double wzm = (wo[q] + wo[q-sz]) * 0.5;
-  double qzp = (qr[q+sz] + qr[q]) * 0.5;
-  double qzm = (qr[q-1+sz] + qr[q-1]) * 0.5;
-  double vzp = (vo[q+sz] + vo[q]) * 0.5;
-  double vzm = (vo[q-sy+sz] + vo[q-sy]) * 0.5;
-  double dwdxp = m.au[i] * (wo[q+1] - wo[q]);
-  double dwdxm = m.au[i - 1] * (wo[q] - wo[q-1]);
-  double dwdyp = m.bv[j] * (wo[q+sy] - wo[q]);
-  double dwdym = m.bv[j - 1] * (wo[q] - wo[q-sy]);
-  double dwdzp = m.cp[k + 1] * (wo[q+sz] - wo[q]);
-  double dwdzm = m.cp[k] * (wo[q] - wo[q-sz]);
-  double dudzp = m.cw[k] * (uo[q+sz] - uo[q]);
-  double dudzm = m.cw[k] * (uo[q-1+sz] - uo[q-1]);
-  double dvdzp = m.cw[k] * (vo[q+sz] - vo[q]);
-  double dvdzm = m.cw[k] * (vo[q-sy+sz] - vo[q-sy]);
-  double tvip = 0.25 * (tv[q+sz] + tv[q] + tv[q+1+sz] + tv[q+1]);
-  double tvim = 0.25 * (tv[q+sz] + tv[q] + tv[q-1+sz] + tv[q-1]);
-  double tvjp = 0.25 * (tv[q+sz] + tv[q] + tv[q+sy+sz] + tv[q+sy]);
-  double tvjm = 0.25 * (tv[q+sz] + tv[q] + tv[q-sy+sz] + tv[q-sy]);
+template <class Acc>
+__device__ __forceinline__ double rhs_w(const Acc &S, const DevMetrics &m, double ru1, int i, int j, int k) {
+  double wxp = (S.w(1, 0, 0) + S.w(0, 0, 0)) * 0.5;
+  double wxm = (S.w(0, 0, 0) + S.w(-1, 0, 0)) * 0.5;
+  double wyp = (S.w(0, 1, 0) + S.w(0, 0, 0)) * 0.5;
+  double wym = (S.w(0, 0, 0) + S.w(0, -1, 0)) * 0.5;
+  double wzp = (S.w(0, 0, 1) + S.w(0, 0, 0)) * 0.5;
+  double wzm = (S.w(0, 0, 0) + S.w(0, 0, -1)) * 0.5;
+  double qzp = (S.u(0, 0, 1) + S.u(0, 0, 0)) * 0.5;
+  double qzm = (S.u(-1, 0, 1) + S.u(-1, 0, 0)) * 0.5;
+  double vzp = (S.v(0, 0, 1) + S.v(0, 0, 0)) * 0.5;
+  double vzm = (S.v(0, -1, 1) + S.v(0, -1, 0)) * 0.5;
+  double dwdxp = m.au[i] * (S.w(1, 0, 0) - S.w(0, 0, 0));
+  double dwdxm = m.au[i - 1] * (S.w(0, 0, 0) - S.w(-1, 0, 0));
+  double dwdyp = m.bv[j] * (S.w(0, 1, 0) - S.w(0, 0, 0));
+  double dwdym = m.bv[j - 1] * (S.w(0, 0, 0) - S.w(0, -1, 0));
+  double dwdzp = m.cp[k + 1] * (S.w(0, 0, 1) - S.w(0, 0, 0));
+  double dwdzm = m.cp[k] * (S.w(0, 0, 0) - S.w(0, 0, -1));
+  double dudzp = m.cw[k] * (S.u(0, 0, 1) - S.u(0, 0, 0));
+  double dudzm = m.cw[k] * (S.u(-1, 0, 1) - S.u(-1, 0, 0));
+  double dvdzp = m.cw[k] * (S.v(0, 0, 1) - S.v(0, 0, 0));
+  double dvdzm = m.cw[k] * (S.v(0, -1, 1) - S.v(0, -1, 0));
+  double tvip = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(1, 0, 1) + S.t(1, 0, 0));
+  double tvim = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(-1, 0, 1) + S.t(-1, 0, 0));
+  double tvjp = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(0, 1, 1) + S.t(0, 1, 0));
+  double tvjm = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(0, -1, 1) + S.t(0, -1, 0));
   double txxp = (ru1 + tvip) * dwdxp;
   double txxm = (ru1 + tvim) * dwdxm;
   double tyyp = (ru1 + tvjp) * dwdyp;
   double tyym = (ru1 + tvjm) * dwdym;
-  double tzzp = (ru1 + 2. * tv[q+sz]) * dwdzp;
-  double tzzm = (ru1 + 2. * tv[q]) * dwdzm;
+  double tzzp = (ru1 + 2. * S.t(0, 0, 1)) * dwdzp;
+  double tzzm = (ru1 + 2. * S.t(0, 0, 0)) * dwdzm;
   double txzp = tvip * dudzp;
   double txzm = tvim * dudzm;
   double tyzp = tvjp * dvdzp;
@@ -168,64 +160,162 @@ __device__ __forceinline__ double rhs_w(const Dims &d, const DevMetrics &m, doub
   return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s22;
 }
 
-// RHS + PREDICTORD + sponges over the whole array (ghost cells of u*,v*,w*
-// are zero, as RHS leaves them, src/rhs.f:65-70).
-__global__ void __launch_bounds__(BX *BY *BZ)
-    k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const double *__restrict__ uo,
-                     const double *__restrict__ vo, const double *__restrict__ wo,
-                     const double *__restrict__ tv, const double *__restrict__ p,
-                     const double *__restrict__ dens, double *__restrict__ us, double *__restrict__ vs,
-                     double *__restrict__ ws, double *__restrict__ ua, double *__restrict__ va,
-                     double *__restrict__ wa, double alfxdt, double gamxdt, double rhoxdt) {
-  int i = 1 + threadIdx.x + blockIdx.x * BX;
-  int j = 1 + threadIdx.y + blockIdx.y * BY;
-  int k = 1 + threadIdx.z + blockIdx.z * BZ;
-  if (i > d.nx || j > d.ny || k > d.nz) return;
-  long long q = fidx(d, i, j, k);
+// RHS + PREDICTORD + sponges (src/rhs.f:4-438, src/timeindeg.f:1041-1265).
+// A block owns a 32x8 tile of (i,j) columns and marches along k over a chunk
+// of planes.  Planes of uo,vo,wo,tv,p,dens,ua,va,wa (with a one-cell halo in i
+// and j) stream into a 4-slot shared-memory ring by TMA, three planes ahead
+// of use; the three planes k-1,k,k+1 the stencil needs are always resident.
+constexpr int TX = 32, TY = 8, PX = TX + 2, PY = TY + 2;
+constexpr int NFLD = 9;                          // uo vo wo tv p dens ua va wa
+constexpr int PLANE = ((PX * PY + 15) / 16) * 16;  // doubles per field-plane (128-byte multiple)
+constexpr int SLOT = NFLD * PLANE;
+constexpr int NSLOT = 4;
+constexpr uint32_t BOX_BYTES = PX * PY * 8;
+constexpr int KCHUNK = 32;
+
+struct SmemAcc {
+  const double *sm;
+  int s0, s1, s2;  // slot offsets of planes k-1, k, k+1
+  int c;           // local cell index
+  __device__ __forceinline__ double at(int f, int di, int dj, int dk) const {
+    int so = dk < 0 ? s0 : (dk == 0 ? s1 : s2);
+    return sm[so + f * PLANE + c + dj * PX + di];
+  }
+  __device__ __forceinline__ double u(int di, int dj, int dk) const { return at(0, di, dj, dk); }
+  __device__ __forceinline__ double v(int di, int dj, int dk) const { return at(1, di, dj, dk); }
+  __device__ __forceinline__ double w(int di, int dj, int dk) const { return at(2, di, dj, dk); }
+  __device__ __forceinline__ double t(int di, int dj, int dk) const { return at(3, di, dj, dk); }
+};
+
+__global__ void __launch_bounds__(TX *TY)
+    k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const __grid_constant__ TmaMaps9 maps,
+                     double *__restrict__ us, double *__restrict__ vs, double *__restrict__ ws,
+                     double *__restrict__ ua, double *__restrict__ va, double *__restrict__ wa, double alfxdt,
+                     double gamxdt, double rhoxdt, int *err) {
+  extern __shared__ unsigned char smraw[];
+  __shared__ __align__(8) uint64_t bar[NSLOT];
+  double *sm = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = d.ix1 + blockIdx.x * TX, j0 = d.jy1 + blockIdx.y * TY;
+  const int k0 = d.kz1 + blockIdx.z * KCHUNK;
+  const int k1 = min(k0 + KCHUNK, d.kz2 + 1);  // exclusive
+  const int pfirst = k0 - 1, plast = k1;        // planes streamed
+  // TMA box origin (0-based): halo starts one cell before the tile
+  const int bx = i0 - 2, by = j0 - 2;
+  if (tid == 0) {
+    for (int q = 0; q < NSLOT; q++) tma::mbar_init(&bar[q], 1);
+    tma::fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int p) {
+    int u = p - pfirst, sl = u & (NSLOT - 1);
+    tma::mbar_expect_tx(&bar[sl], NFLD * BOX_BYTES);
+    for (int f = 0; f < NFLD; f++) tma::load_3d(sm + sl * SLOT + f * PLANE, &maps.m[f], bx, by, p - 1, &bar[sl]);
+  };
+  if (tid == 0)
+    for (int p = pfirst; p <= min(pfirst + NSLOT - 1, plast); p++) issue(p);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool active = (i <= d.ix2 && j <= d.jy2);
+  const int c = (ty + 1) * PX + (tx + 1);
   const int sy = d.nx;
   const long long sz = (long long)d.nx * d.ny;
   const double coef = 0.5 * alfxdt, coefd = alfxdt;
-  const bool kin = (k >= d.kz1 && k <= d.kz2), jin = (j >= d.jy1 && j <= d.jy2);
-  // ---- u ----
-  double uval = 0.0;
-  if (kin && jin && i >= d.ibu && i <= d.ieu) {
-    double ur = rhs_u(d, m, s.ru1, uo, vo, wo, tv, i, j, k, q, sy, sz);
-    double ustar = uo[q] + gamxdt * ur + rhoxdt * ua[q] - alfxdt * m.au[i] * (p[q + 1] - p[q]) +
-                   coef * 0.0 - alfxdt * s.dpdx;
-    if (s.idens == 1)
-      ustar = ustar - coefd * 0.50 * s.grav *
-                          ((dens[q + 1] - m.dens_bg[i + d.nx * (j - 1)]) +
-                           (dens[q] - m.dens_bg[(i - 1) + d.nx * (j - 1)]));
-    ua[q] = ur;
-    if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0. - ustar) * alfxdt * 1.0;
-    if (s.ivspngl == 1) ustar = ustar + m.dfxul[k] * (0. - ustar) * alfxdt * 1.0;
-    uval = ustar;
+  const bool jin = j >= d.jy1 && j <= d.jy2;
+  for (int k = k0; k < k1; k++) {
+    bool ok = true;
+    for (int p = k - 1; p <= k + 1; p++) {
+      int u = p - pfirst;
+      ok = ok && tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1);
+    }
+    if (ok && active) {
+      SmemAcc S{sm, ((k - 1 - pfirst) & 3) * SLOT, ((k - pfirst) & 3) * SLOT, ((k + 1 - pfirst) & 3) * SLOT, c};
+      long long q = fidx(d, i, j, k);
+      const bool kin = (k >= d.kz1 && k <= d.kz2);
+      // ---- u ----
+      double uval = 0.0;
+      if (kin && jin && i >= d.ibu && i <= d.ieu) {
+        double ur = rhs_u(S, m, s.ru1, i, j, k);
+        double ustar = S.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * S.at(6, 0, 0, 0) -
+                       alfxdt * m.au[i] * (S.at(4, 1, 0, 0) - S.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdx;
+        if (s.idens == 1)
+          ustar = ustar - coefd * 0.50 * s.grav *
+                              ((S.at(5, 1, 0, 0) - m.dens_bg[i + d.nx * (j - 1)]) +
+                               (S.at(5, 0, 0, 0) - m.dens_bg[(i - 1) + d.nx * (j - 1)]));
+        ua[q] = ur;
+        if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0. - ustar) * alfxdt * 1.0;
+        if (s.ivspngl == 1) ustar = ustar + m.dfxul[k] * (0. - ustar) * alfxdt * 1.0;
+        uval = ustar;
+      }
+      us[q] = uval;
+      // ---- v ----
+      double vval = 0.0;
+      if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
+        double vr = rhs_v(S, m, s.ru1, i, j, k);
+        double vstar = S.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * S.at(7, 0, 0, 0) -
+                       alfxdt * m.bv[j] * (S.at(4, 0, 1, 0) - S.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdy;
+        va[q] = vr;
+        if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0. - vstar) * alfxdt * 1.0;
+        if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin)
+          vstar = vstar + m.dfxwl[k] * (0. - vstar) * alfxdt * 1.0;
+        vval = vstar;
+      }
+      vs[q] = vval;
+      // ---- w ----
+      double wval = 0.0;
+      if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
+        double wr = rhs_w(S, m, s.ru1, i, j, k);
+        double wstar = S.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * S.at(8, 0, 0, 0) -
+                       alfxdt * m.cw[k] * (S.at(4, 0, 0, 1) - S.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdz;
+        wa[q] = wr;
+        if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1. - wstar) * alfxdt * 1.0;
+        if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1. - wstar) * alfxdt * 1.0;
+        wval = wstar;
+      }
+      ws[q] = wval;
+    }
+    // every thread is done with plane k-1 before its slot is refilled
+    int failed = __syncthreads_or(ok ? 0 : 1);
+    if (failed) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        // let copies already in flight land before the block's smem goes away
+        for (int p = k + 2; p <= min(k + NSLOT - 1, plast); p++) {
+          int u = p - pfirst;
+          tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1, 1u << 20);
+        }
+      }
+      return;
+    }
+    if (tid == 0 && k + NSLOT - 1 <= plast) {
+      tma::fence_proxy_async();
+      issue(k + NSLOT - 1);
+    }
   }
-  us[q] = uval;
-  // ---- v ----
-  double vval = 0.0;
-  if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
-    double vr = rhs_v(d, m, s.ru1, uo, vo, wo, tv, i, j, k, q, sy, sz);
-    double vstar = vo[q] + gamxdt * vr + rhoxdt * va[q] - alfxdt * m.bv[j] * (p[q + sy] - p[q]) +
-                   coef * 0.0 - alfxdt * s.dpdy;
-    va[q] = vr;
-    if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0. - vstar) * alfxdt * 1.0;
-    if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin) vstar = vstar + m.dfxwl[k] * (0. - vstar) * alfxdt * 1.0;
-    vval = vstar;
+  (void)sy;
+  (void)sz;
+}
+
+// ghost faces of u*,v*,w* are zero (RHS zeroes the whole arrays, src/rhs.f:65-70)
+__global__ void k_zero_faces3(Dims d, double *a, double *b, double *c3) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long sxy = (long long)d.nx * d.ny, sxz = (long long)d.nx * d.nz, syz = (long long)d.ny * d.nz;
+  int i, j, k;
+  if (t < 2 * sxy) {
+    long long r = t % sxy;
+    i = 1 + (int)(r % d.nx); j = 1 + (int)(r / d.nx); k = (t / sxy) ? d.nz : 1;
+  } else if (t < 2 * sxy + 2 * sxz) {
+    long long u = t - 2 * sxy, r = u % sxz;
+    i = 1 + (int)(r % d.nx); k = 1 + (int)(r / d.nx); j = (u / sxz) ? d.ny : 1;
+  } else if (t < 2 * sxy + 2 * sxz + 2 * syz) {
+    long long u = t - 2 * sxy - 2 * sxz, r = u % syz;
+    j = 1 + (int)(r % d.ny); k = 1 + (int)(r / d.ny); i = (u / syz) ? d.nx : 1;
+  } else {
+    return;
   }
-  vs[q] = vval;
-  // ---- w ----
-  double wval = 0.0;
-  if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
-    double wr = rhs_w(d, m, s.ru1, uo, vo, wo, tv, i, j, k, q, sy, sz);
-    double wstar = wo[q] + gamxdt * wr + rhoxdt * wa[q] - alfxdt * m.cw[k] * (p[q + sz] - p[q]) +
-                   coef * 0.0 - alfxdt * s.dpdz;
-    wa[q] = wr;
-    if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1. - wstar) * alfxdt * 1.0;
-    if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1. - wstar) * alfxdt * 1.0;
-    wval = wstar;
-  }
-  ws[q] = wval;
+  long long q = fidx(d, i, j, k);
+  a[q] = 0.;
+  b[q] = 0.;
+  c3[q] = 0.;
 }
 
 // ---------------------------------------------------------------------------
@@ -444,9 +534,24 @@ int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, doub
 int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   const Dims &d = ctx->d;
   double **f = ctx->f;
-  k_rhs_predictord<<<grid3(d), dim3(BX, BY, BZ), 0, ctx->stream>>>(
-      d, ctx->m, ctx->sc, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_TV], f[EDDY_P], f[EDDY_DENS],
-      f[EDDY_US], f[EDDY_VS], f[EDDY_WS], f[EDDY_UA], f[EDDY_VA], f[EDDY_WA], alfxdt, gamxdt, rhoxdt);
+  TmaMaps9 maps;
+  const double *src[NFLD] = {f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_TV], f[EDDY_P], f[EDDY_DENS],
+                             f[EDDY_UA], f[EDDY_VA], f[EDDY_WA]};
+  for (int q = 0; q < NFLD; q++) {
+    const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], PX, PY);
+    if (!mp) return EDDY_ECUDA;
+    maps.m[q] = *mp;
+  }
+  size_t smem = (size_t)NSLOT * SLOT * sizeof(double) + 128;
+  EDDY_CUDA(cudaFuncSetAttribute(k_rhs_predictord, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 g((d.ix2 - d.ix1 + TX) / TX, (d.jy2 - d.jy1 + TY) / TY, (d.kz2 - d.kz1 + KCHUNK) / KCHUNK);
+  k_rhs_predictord<<<g, dim3(TX, TY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, f[EDDY_US], f[EDDY_VS],
+                                                          f[EDDY_WS], f[EDDY_UA], f[EDDY_VA], f[EDDY_WA], alfxdt,
+                                                          gamxdt, rhoxdt, ctx->err_flag);
+  EDDY_LAUNCHED(ctx);
+  long long nghost = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
+  k_zero_faces3<<<(unsigned)((nghost + 255) / 256), 256, 0, ctx->stream>>>(d, f[EDDY_US], f[EDDY_VS],
+                                                                            f[EDDY_WS]);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
