@@ -60,11 +60,6 @@ enum {
   PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_NCAT
 };
 
-// tensor maps of nine fields, passed by value to TMA kernels
-struct alignas(64) TmaMaps9 {
-  CUtensorMap m[9];
-};
-
 struct TmaEntry {
   const void *ptr;
   int bx, by;

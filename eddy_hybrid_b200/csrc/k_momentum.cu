@@ -162,137 +162,74 @@ __device__ __forceinline__ double rhs_w(const Acc &S, const DevMetrics &m, doubl
 
 // RHS + PREDICTORD + sponges (src/rhs.f:4-438, src/timeindeg.f:1041-1265).
 // A block owns a 32x8 tile of (i,j) columns and marches along k over a chunk
-// of planes.  Planes of uo,vo,wo,tv,p,dens,ua,va,wa (with a one-cell halo in i
-// and j) stream into a 4-slot shared-memory ring by TMA, three planes ahead
-// of use; the three planes k-1,k,k+1 the stencil needs are always resident.
-constexpr int TX = 32, TY = 8, PX = TX + 2, PY = TY + 2;
-constexpr int NFLD = 9;                          // uo vo wo tv p dens ua va wa
-constexpr int PLANE = ((PX * PY + 15) / 16) * 16;  // doubles per field-plane (128-byte multiple)
-constexpr int SLOT = NFLD * PLANE;
-constexpr int NSLOT = 4;
-constexpr uint32_t BOX_BYTES = PX * PY * 8;
-constexpr int KCHUNK = 32;
+// of planes; planes of uo,vo,wo,tv,p,dens,ua,va,wa (one-cell halo in i and j)
+// stream into the shared-memory ring of tma_ring.cuh.
+constexpr int TX = 32, TY = 8, NFLD = 9, KCHUNK = 32;  // uo vo wo tv p dens ua va wa
+using Acc9 = RingAcc<TX, TY, NFLD>;
 
-struct SmemAcc {
-  const double *sm;
-  int s0, s1, s2;  // slot offsets of planes k-1, k, k+1
-  int c;           // local cell index
-  __device__ __forceinline__ double at(int f, int di, int dj, int dk) const {
-    int so = dk < 0 ? s0 : (dk == 0 ? s1 : s2);
-    return sm[so + f * PLANE + c + dj * PX + di];
-  }
-  __device__ __forceinline__ double u(int di, int dj, int dk) const { return at(0, di, dj, dk); }
-  __device__ __forceinline__ double v(int di, int dj, int dk) const { return at(1, di, dj, dk); }
-  __device__ __forceinline__ double w(int di, int dj, int dk) const { return at(2, di, dj, dk); }
-  __device__ __forceinline__ double t(int di, int dj, int dk) const { return at(3, di, dj, dk); }
+struct MomAcc {
+  const Acc9 &r;
+  __device__ __forceinline__ double u(int di, int dj, int dk) const { return r.at(0, di, dj, dk); }
+  __device__ __forceinline__ double v(int di, int dj, int dk) const { return r.at(1, di, dj, dk); }
+  __device__ __forceinline__ double w(int di, int dj, int dk) const { return r.at(2, di, dj, dk); }
+  __device__ __forceinline__ double t(int di, int dj, int dk) const { return r.at(3, di, dj, dk); }
 };
 
 __global__ void __launch_bounds__(TX *TY)
-    k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const __grid_constant__ TmaMaps9 maps,
+    k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const __grid_constant__ TmaMaps<NFLD> maps,
                      double *__restrict__ us, double *__restrict__ vs, double *__restrict__ ws,
                      double *__restrict__ ua, double *__restrict__ va, double *__restrict__ wa, double alfxdt,
                      double gamxdt, double rhoxdt, int *err) {
-  extern __shared__ unsigned char smraw[];
-  __shared__ __align__(8) uint64_t bar[NSLOT];
-  double *sm = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i0 = d.ix1 + blockIdx.x * TX, j0 = d.jy1 + blockIdx.y * TY;
-  const int k0 = d.kz1 + blockIdx.z * KCHUNK;
-  const int k1 = min(k0 + KCHUNK, d.kz2 + 1);  // exclusive
-  const int pfirst = k0 - 1, plast = k1;        // planes streamed
-  // TMA box origin (0-based): halo starts one cell before the tile
-  const int bx = i0 - 2, by = j0 - 2;
-  if (tid == 0) {
-    for (int q = 0; q < NSLOT; q++) tma::mbar_init(&bar[q], 1);
-    tma::fence_mbar_init();
-  }
-  __syncthreads();
-  auto issue = [&](int p) {
-    int u = p - pfirst, sl = u & (NSLOT - 1);
-    tma::mbar_expect_tx(&bar[sl], NFLD * BOX_BYTES);
-    for (int f = 0; f < NFLD; f++) tma::load_3d(sm + sl * SLOT + f * PLANE, &maps.m[f], bx, by, p - 1, &bar[sl]);
-  };
-  if (tid == 0)
-    for (int p = pfirst; p <= min(pfirst + NSLOT - 1, plast); p++) issue(p);
-  const int i = i0 + tx, j = j0 + ty;
-  const bool active = (i <= d.ix2 && j <= d.jy2);
-  const int c = (ty + 1) * PX + (tx + 1);
-  const int sy = d.nx;
-  const long long sz = (long long)d.nx * d.ny;
   const double coef = 0.5 * alfxdt, coefd = alfxdt;
-  const bool jin = j >= d.jy1 && j <= d.jy2;
-  for (int k = k0; k < k1; k++) {
-    bool ok = true;
-    for (int p = k - 1; p <= k + 1; p++) {
-      int u = p - pfirst;
-      ok = ok && tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1);
-    }
-    if (ok && active) {
-      SmemAcc S{sm, ((k - 1 - pfirst) & 3) * SLOT, ((k - pfirst) & 3) * SLOT, ((k + 1 - pfirst) & 3) * SLOT, c};
-      long long q = fidx(d, i, j, k);
-      const bool kin = (k >= d.kz1 && k <= d.kz2);
-      // ---- u ----
-      double uval = 0.0;
-      if (kin && jin && i >= d.ibu && i <= d.ieu) {
-        double ur = rhs_u(S, m, s.ru1, i, j, k);
-        double ustar = S.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * S.at(6, 0, 0, 0) -
-                       alfxdt * m.au[i] * (S.at(4, 1, 0, 0) - S.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdx;
-        if (s.idens == 1)
-          ustar = ustar - coefd * 0.50 * s.grav *
-                              ((S.at(5, 1, 0, 0) - m.dens_bg[i + d.nx * (j - 1)]) +
-                               (S.at(5, 0, 0, 0) - m.dens_bg[(i - 1) + d.nx * (j - 1)]));
-        ua[q] = ur;
-        if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0. - ustar) * alfxdt * 1.0;
-        if (s.ivspngl == 1) ustar = ustar + m.dfxul[k] * (0. - ustar) * alfxdt * 1.0;
-        uval = ustar;
-      }
-      us[q] = uval;
-      // ---- v ----
-      double vval = 0.0;
-      if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
-        double vr = rhs_v(S, m, s.ru1, i, j, k);
-        double vstar = S.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * S.at(7, 0, 0, 0) -
-                       alfxdt * m.bv[j] * (S.at(4, 0, 1, 0) - S.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdy;
-        va[q] = vr;
-        if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0. - vstar) * alfxdt * 1.0;
-        if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin)
-          vstar = vstar + m.dfxwl[k] * (0. - vstar) * alfxdt * 1.0;
-        vval = vstar;
-      }
-      vs[q] = vval;
-      // ---- w ----
-      double wval = 0.0;
-      if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
-        double wr = rhs_w(S, m, s.ru1, i, j, k);
-        double wstar = S.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * S.at(8, 0, 0, 0) -
-                       alfxdt * m.cw[k] * (S.at(4, 0, 0, 1) - S.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdz;
-        wa[q] = wr;
-        if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1. - wstar) * alfxdt * 1.0;
-        if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1. - wstar) * alfxdt * 1.0;
-        wval = wstar;
-      }
-      ws[q] = wval;
-    }
-    // every thread is done with plane k-1 before its slot is refilled
-    int failed = __syncthreads_or(ok ? 0 : 1);
-    if (failed) {
-      if (tid == 0) {
-        atomicExch(err, 1);
-        // let copies already in flight land before the block's smem goes away
-        for (int p = k + 2; p <= min(k + NSLOT - 1, plast); p++) {
-          int u = p - pfirst;
-          tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1, 1u << 20);
+  tma_march<NFLD, TX, TY, KCHUNK>(
+      d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err, [&](int i, int j, int k, bool active, const Acc9 &R) {
+        if (!active) return;
+        MomAcc S{R};
+        long long q = fidx(d, i, j, k);
+        const bool jin = j >= d.jy1 && j <= d.jy2;
+        const bool kin = (k >= d.kz1 && k <= d.kz2);
+        // ---- u ----
+        double uval = 0.0;
+        if (kin && jin && i >= d.ibu && i <= d.ieu) {
+          double ur = rhs_u(S, m, s.ru1, i, j, k);
+          double ustar = R.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * R.at(6, 0, 0, 0) -
+                         alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdx;
+          if (s.idens == 1)
+            ustar = ustar - coefd * 0.50 * s.grav *
+                                ((R.at(5, 1, 0, 0) - m.dens_bg[i + d.nx * (j - 1)]) +
+                                 (R.at(5, 0, 0, 0) - m.dens_bg[(i - 1) + d.nx * (j - 1)]));
+          ua[q] = ur;
+          if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0. - ustar) * alfxdt * 1.0;
+          if (s.ivspngl == 1) ustar = ustar + m.dfxul[k] * (0. - ustar) * alfxdt * 1.0;
+          uval = ustar;
         }
-      }
-      return;
-    }
-    if (tid == 0 && k + NSLOT - 1 <= plast) {
-      tma::fence_proxy_async();
-      issue(k + NSLOT - 1);
-    }
-  }
-  (void)sy;
-  (void)sz;
+        us[q] = uval;
+        // ---- v ----
+        double vval = 0.0;
+        if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
+          double vr = rhs_v(S, m, s.ru1, i, j, k);
+          double vstar = R.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * R.at(7, 0, 0, 0) -
+                         alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdy;
+          va[q] = vr;
+          if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0. - vstar) * alfxdt * 1.0;
+          if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin)
+            vstar = vstar + m.dfxwl[k] * (0. - vstar) * alfxdt * 1.0;
+          vval = vstar;
+        }
+        vs[q] = vval;
+        // ---- w ----
+        double wval = 0.0;
+        if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
+          double wr = rhs_w(S, m, s.ru1, i, j, k);
+          double wstar = R.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * R.at(8, 0, 0, 0) -
+                         alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdz;
+          wa[q] = wr;
+          if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1. - wstar) * alfxdt * 1.0;
+          if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1. - wstar) * alfxdt * 1.0;
+          wval = wstar;
+        }
+        ws[q] = wval;
+      });
 }
 
 // ghost faces of u*,v*,w* are zero (RHS zeroes the whole arrays, src/rhs.f:65-70)
@@ -534,15 +471,15 @@ int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, doub
 int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   const Dims &d = ctx->d;
   double **f = ctx->f;
-  TmaMaps9 maps;
+  TmaMaps<NFLD> maps;
   const double *src[NFLD] = {f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_TV], f[EDDY_P], f[EDDY_DENS],
                              f[EDDY_UA], f[EDDY_VA], f[EDDY_WA]};
   for (int q = 0; q < NFLD; q++) {
-    const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], PX, PY);
+    const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], TX + 2, TY + 2);
     if (!mp) return EDDY_ECUDA;
     maps.m[q] = *mp;
   }
-  size_t smem = (size_t)NSLOT * SLOT * sizeof(double) + 128;
+  size_t smem = ring_smem_bytes<NFLD, TX, TY>();
   EDDY_CUDA(cudaFuncSetAttribute(k_rhs_predictord, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 g((d.ix2 - d.ix1 + TX) / TX, (d.jy2 - d.jy1 + TY) / TY, (d.kz2 - d.kz1 + KCHUNK) / KCHUNK);
   k_rhs_predictord<<<g, dim3(TX, TY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, f[EDDY_US], f[EDDY_VS],

@@ -67,3 +67,95 @@ __device__ __forceinline__ void load_3d(void *dst, const CUtensorMap *map, int x
 // Host: encode a 3-D tiled tensor map over an (nx,ny,nz) Fortran array of
 // `esize`-byte elements with a (bx,by,1) box.  Returns 0 on success.
 int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int nz, int bx, int by, int esize);
+
+// ---------------------------------------------------------------------------
+// Generic k-marching driver over a 4-slot ring of halo planes of NF fields.
+// Block = TX x TY threads, tile = TX x TY (i,j) columns starting at the
+// interior origin (ix1, jy1) + block offset; k runs over a chunk of KC planes.
+// body(i, j, k, active, acc) is called once per plane per thread after planes
+// k-1, k, k+1 are resident; acc.at(f, di, dj, dk) reads field f at the offset.
+template <int NF>
+struct alignas(64) TmaMaps {
+  CUtensorMap m[NF];
+};
+
+template <int TX, int TY>
+struct RingGeom {
+  static constexpr int PX = TX + 2, PY = TY + 2;
+  static constexpr int PLANE = ((PX * PY + 15) / 16) * 16;  // doubles, 128-byte multiple
+  static constexpr unsigned BOX_BYTES = PX * PY * 8;
+};
+
+template <int TX, int TY, int NF>
+struct RingAcc {
+  using G = RingGeom<TX, TY>;
+  const double *sm;
+  int s0, s1, s2, c;
+  __device__ __forceinline__ double at(int f, int di, int dj, int dk) const {
+    int so = dk < 0 ? s0 : (dk == 0 ? s1 : s2);
+    return sm[so + f * G::PLANE + c + dj * G::PX + di];
+  }
+};
+
+template <int NF, int TX, int TY>
+constexpr size_t ring_smem_bytes() {
+  return (size_t)4 * NF * RingGeom<TX, TY>::PLANE * sizeof(double) + 128;
+}
+
+template <int NF, int TX, int TY, int KC, class Body>
+__device__ __forceinline__ void tma_march(int ix1, int ix2, int jy1, int jy2, int kz1, int kz2,
+                                          const TmaMaps<NF> &maps, int *err, Body &&body) {
+  using G = RingGeom<TX, TY>;
+  constexpr int NSLOT = 4, SLOT = NF * G::PLANE;
+  extern __shared__ unsigned char smraw_[];
+  __shared__ __align__(8) uint64_t bar[NSLOT];
+  double *sm = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smraw_) + 127) & ~uintptr_t(127));
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = ix1 + blockIdx.x * TX, j0 = jy1 + blockIdx.y * TY;
+  const int k0 = kz1 + blockIdx.z * KC;
+  const int k1 = min(k0 + KC, kz2 + 1);
+  const int pfirst = k0 - 1, plast = k1;
+  const int bx = i0 - 2, by = j0 - 2;
+  if (tid == 0) {
+    for (int q = 0; q < NSLOT; q++) tma::mbar_init(&bar[q], 1);
+    tma::fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int p) {
+    int u = p - pfirst, sl = u & (NSLOT - 1);
+    tma::mbar_expect_tx(&bar[sl], NF * G::BOX_BYTES);
+    for (int f = 0; f < NF; f++) tma::load_3d(sm + sl * SLOT + f * G::PLANE, &maps.m[f], bx, by, p - 1, &bar[sl]);
+  };
+  if (tid == 0)
+    for (int p = pfirst; p <= min(pfirst + NSLOT - 1, plast); p++) issue(p);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool active = (i <= ix2 && j <= jy2);
+  const int c = (ty + 1) * G::PX + (tx + 1);
+  for (int k = k0; k < k1; k++) {
+    bool ok = true;
+    for (int p = k - 1; p <= k + 1; p++) {
+      int u = p - pfirst;
+      ok = ok && tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1);
+    }
+    if (ok) {
+      RingAcc<TX, TY, NF> S{sm, ((k - 1 - pfirst) & 3) * SLOT, ((k - pfirst) & 3) * SLOT,
+                            ((k + 1 - pfirst) & 3) * SLOT, c};
+      body(i, j, k, active, S);
+    }
+    int failed = __syncthreads_or(ok ? 0 : 1);
+    if (failed) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        for (int p = k + 2; p <= min(k + NSLOT - 1, plast); p++) {
+          int u = p - pfirst;
+          tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1, 1u << 20);
+        }
+      }
+      return;
+    }
+    if (tid == 0 && k + NSLOT - 1 <= plast) {
+      tma::fence_proxy_async();
+      issue(k + NSLOT - 1);
+    }
+  }
+}
