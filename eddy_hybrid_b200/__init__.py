@@ -63,6 +63,7 @@ def make_params(d: dict, precision: int = PLAIN_FP64, refine_sweeps: int = 2,
 
 _lib = None
 _DP = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
 
 # exported symbols and their argument types (must match include/eddy_b200.h)
 SIGNATURES = {
@@ -89,6 +90,7 @@ SIGNATURES = {
     "eddy_profile_read": ([C.c_void_p, _DP, C.POINTER(C.c_longlong)], C.c_int),
     "eddy_max_divergence_noalloc": ([C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "eddy_umma_gemm_bf16": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, _FP, C.c_int], C.c_int),
     "eddy_sync": ([C.c_void_p], C.c_int),
     "eddy_last_error": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
     "eddy_launch_count": ([C.c_void_p], C.c_int64),

@@ -25,6 +25,7 @@ UNITS = {
     "k_density.cu": ["-fmad=false"],
     "k_sgs.cu": ["-fmad=false"],
     "k_noalloc.cu": ["-fmad=false"],
+    "k_mlp.cu": [],
     "host_eigen.cpp": [],
 }
 

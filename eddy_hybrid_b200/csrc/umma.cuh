@@ -1,0 +1,128 @@
+// umma.cuh -- 5th-generation tensor core (tcgen05) helpers for sm_100a:
+// TMEM allocation, shared-memory matrix descriptors for the no-swizzle
+// K-major canonical layout, the kind::f16 (BF16 in, FP32 accumulate)
+// instruction descriptor, MMA issue, commit to an mbarrier, TMEM loads.
+//
+// Canonical K-major layout without swizzle: the operand (rows x K) is tiled in
+// core matrices of 8 rows x 16 bytes (8 bf16); a core matrix is 128 contiguous
+// bytes (row r at byte 16*r).  Core matrices adjacent along K are LBO bytes
+// apart, adjacent along rows SBO bytes apart.  We store each row group's core
+// matrices contiguously along K: LBO = 128, SBO = 128 * (K / 8).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace umma {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// byte offset of element (row r, column k) of a rows x K bf16 operand in the
+// canonical layout above
+__host__ __device__ __forceinline__ uint32_t kmajor_offset(int r, int k, int K) {
+  return (uint32_t)((r >> 3) * (128 * (K >> 3)) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// shared-memory matrix descriptor (tcgen05 "matrix descriptor" format)
+__device__ __forceinline__ uint64_t make_desc(const void *smem_base, uint32_t lbo, uint32_t sbo) {
+  uint64_t addr = smem_u32(smem_base);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;               // bits 0-13 start address >> 4
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;  // bits 16-29 leading byte offset >> 4
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;  // bits 32-45 stride byte offset >> 4
+  d |= (uint64_t)1 << 46;                      // bits 46-48 fixed 0b001
+  // base offset 0, lbo mode 0, swizzle none (bits 61-63 = 0)
+  return d;
+}
+
+// instruction descriptor, kind::f16: D f32, A/B bf16, both K-major
+__host__ __device__ __forceinline__ uint32_t make_idesc_bf16(int M, int N) {
+  uint32_t d = 0;
+  d |= 1u << 4;                    // D format: f32
+  d |= 1u << 7;                    // A format: bf16
+  d |= 1u << 10;                   // B format: bf16
+  d |= (uint32_t)(N >> 3) << 17;   // N / 8
+  d |= (uint32_t)(M >> 4) << 24;   // M / 16
+  return d;
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *smem_result, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem_result)),
+               "r"(ncols)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// arrive on an mbarrier once all previously issued MMAs of this thread complete
+__device__ __forceinline__ void commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// make generic-proxy shared-memory writes visible to the tensor core (async proxy)
+__device__ __forceinline__ void fence_smem_to_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 32 lanes x 32 bit, 16 consecutive columns -> 16 registers per thread
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = (1u << 24)) {
+  for (uint32_t it = 0; it < limit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+}  // namespace umma

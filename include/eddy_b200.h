@@ -162,6 +162,13 @@ int eddy_max_divergence_noalloc(int nx, int ny, int nz, const double *u, const d
                                 const double *w, const double *ap, const double *bp,
                                 const double *cp, double *out, void *stream);
 
+/* ---- learned closure (tensor-core MLP), no counterpart in the reference's
+ * code: it stands in for the dynamic procedure of src/vt.f:172-431 ---- */
+/* Self-test of the BF16 tensor-core GEMM used by the closure's training:
+ * D[MxN] (+)= A[MxK] * B[NxK]^T, host arrays (bf16 bit patterns, f32 D). */
+int eddy_umma_gemm_bf16(eddy_ctx *ctx, int M, int N, int K, const uint16_t *A, const uint16_t *B,
+                        float *D, int acc);
+
 int eddy_sync(eddy_ctx *ctx);
 /* Copy the last error message (NUL-terminated, truncated to len). */
 int eddy_last_error(eddy_ctx *ctx, char *buf, int len);
