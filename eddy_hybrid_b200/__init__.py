@@ -91,6 +91,15 @@ SIGNATURES = {
     "eddy_max_divergence_noalloc": ([C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "eddy_umma_gemm_bf16": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, _FP, C.c_int], C.c_int),
+    "eddy_closure_set": ([C.c_void_p, _FP, _FP], C.c_int),
+    "eddy_closure_get": ([C.c_void_p, _FP, _FP], C.c_int),
+    "eddy_closure_harvest": ([C.c_void_p, C.c_void_p, C.c_int, _FP, _FP], C.c_int),
+    "eddy_closure_grad": ([C.c_void_p, _FP, _FP, C.c_int, _FP, _DP], C.c_int),
+    "eddy_closure_train": ([C.c_void_p, _FP, _FP, C.c_longlong, C.c_int, C.c_int, C.c_float, C.c_ulonglong, _DP],
+                           C.c_int),
+    "eddy_closure_apply": ([C.c_void_p, C.POINTER(C.c_longlong)], C.c_int),
+    "eddy_closure_refresh_fallback": ([C.c_void_p], C.c_int),
+    "eddy_download_kappa": ([C.c_void_p, _DP], C.c_int),
     "eddy_sync": ([C.c_void_p], C.c_int),
     "eddy_last_error": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
     "eddy_launch_count": ([C.c_void_p], C.c_int64),

@@ -228,6 +228,9 @@ void free_all(eddy_ctx *ctx) {
   for (double *p : o) if (p) cudaFree(p);
   if (ctx->err_flag) cudaFree(ctx->err_flag);
   poisson_plan_destroy(ctx);
+  mlp_release(ctx);
+  double *o2[] = {ctx->xc_dev, ctx->kappa, ctx->tv_dyn};
+  for (double *p : o2) if (p) cudaFree(p);
   for (ProfEvent &e : ctx->prof_ev) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (ProfEvent &e : ctx->prof_pool) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   if (ctx->blas) cublasDestroy(ctx->blas);
@@ -321,6 +324,7 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   if (p.itype[5] != 305 || (p.itype[6] != 730))
     return fail(EDDY_EINVAL, "z boundaries must be the hybrid inlet 305 and the convective outlet 730");
   if (p.precision != EDDY_PLAIN_FP64) return fail(EDDY_EINVAL, "mixed precision form not available in this build");
+  if (p.closure != 0 && p.closure != 1) return fail(EDDY_EINVAL, "closure must be 0 (dynamic) or 1 (learned)");
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -355,6 +359,15 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   cudaMemset(ctx->err_flag, 0, sizeof(int));
   rc = poisson_plan_create(ctx);
   if (rc) return fail(rc, nullptr);
+  {
+    size_t bx = sizeof(double) * ctx->h[1].size();
+    if (cudaMalloc(&ctx->xc_dev, bx) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
+    cudaMemcpy(ctx->xc_dev, ctx->h[1].data(), bx, cudaMemcpyHostToDevice);
+    if (cudaMalloc(&ctx->kappa, n3) != cudaSuccess || cudaMalloc(&ctx->tv_dyn, n3) != cudaSuccess)
+      return fail(EDDY_ENOMEM, "allocation failed");
+    cudaMemset(ctx->kappa, 0, n3);
+    cudaMemset(ctx->tv_dyn, 0, n3);
+  }
   if (p.isgs != 0) {
     rc = launch_filtersize(ctx);
     if (rc) return fail(rc, nullptr);
@@ -498,6 +511,8 @@ int eddy_initialize(eddy_ctx *ctx, double dt) {
     EDDY_CUDA(cudaMemcpyAsync(ctx->dens_alt, dn, sizeof(double) * d.ncell, cudaMemcpyDeviceToDevice, ctx->stream));
   }
   if (ctx->prm.isgs != 0 && (rc = launch_turvis(ctx))) return rc;
+  EDDY_CUDA(cudaMemcpyAsync(ctx->tv_dyn, f[EDDY_TV], sizeof(double) * d.ncell, cudaMemcpyDeviceToDevice, ctx->stream));
+  EDDY_CUDA(cudaMemcpyAsync(ctx->kappa, f[EDDY_TV], sizeof(double) * d.ncell, cudaMemcpyDeviceToDevice, ctx->stream));
   return EDDY_OK;
 }
 
@@ -554,11 +569,22 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
     }
     if (ctx->prm.isgs != 0) {
       ProfScope ps(ctx, PROF_TURVIS);
-      int rc = launch_turvis(ctx);
+      int rc;
+      if (ctx->prm.closure == 1) {
+        rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, nullptr);
+      } else {
+        rc = launch_turvis(ctx);
+      }
       if (rc) return rc;
     }
   }
   return EDDY_OK;
+}
+
+// the learned closure's fallback bookkeeping: fraction of cells outside the
+// training envelope in the last closure evaluation
+int closure_envelope_check(eddy_ctx *ctx, unsigned long long *nout) {
+  return launch_closure(ctx, ctx->tv_dyn, ctx->kappa, nout);
 }
 
 int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_device) {
@@ -570,6 +596,33 @@ int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_dev
   int rc = launch_poisson_rhs(ctx, ctx->f[EDDY_US], ctx->f[EDDY_DP]);
   if (rc) return rc;
   EDDY_CUDA(cudaMemcpyAsync(sol, ctx->f[EDDY_DP], b, cudaMemcpyDeviceToHost, ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EDDY_OK;
+}
+
+int eddy_closure_apply(eddy_ctx *ctx, long long *out_of_envelope) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  unsigned long long n = 0;
+  int rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, &n);
+  if (rc) return rc;
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (out_of_envelope) *out_of_envelope = (long long)n;
+  return EDDY_OK;
+}
+
+int eddy_closure_refresh_fallback(eddy_ctx *ctx) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  int rc = launch_turvis(ctx);
+  if (rc) return rc;
+  EDDY_CUDA(cudaMemcpyAsync(ctx->tv_dyn, ctx->f[EDDY_TV], sizeof(double) * ctx->d.ncell, cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+  ctx->closure_refresh++;
+  return EDDY_OK;
+}
+
+int eddy_download_kappa(eddy_ctx *ctx, double *host) {
+  if (check_ctx(ctx) || !host) return EDDY_EINVAL;
+  EDDY_CUDA(cudaMemcpyAsync(host, ctx->kappa, sizeof(double) * ctx->d.ncell, cudaMemcpyDeviceToHost, ctx->stream));
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
   return EDDY_OK;
 }

@@ -92,6 +92,11 @@ struct eddy_ctx {
   std::string err;
   int64_t launches = 0;
   double dely = 0., delysq = 0.;
+  double *xc_dev = nullptr;     // x cell centres (1-based, NX+2)
+  double *kappa = nullptr;      // eddy diffusivity of the learned closure (NX,NY,NZ)
+  double *tv_dyn = nullptr;     // last dynamic-model nu_t: closure fallback (NX,NY,NZ)
+  void *mlp = nullptr;          // closure network state (k_mlp.cu)
+  long long closure_out = 0, closure_cells = 0, closure_refresh = 0;
   // profiling (CUDA events on the context stream around each category)
   unsigned prof_mask = 0;
   std::vector<ProfEvent> prof_ev;   // recorded in this window
@@ -175,6 +180,8 @@ int launch_direct(eddy_ctx *ctx, const double *us, const double *vs, const doubl
 // solve from an explicit right-hand side array (interior of rhs) -> dp
 int launch_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp);
 int launch_max_divergence(eddy_ctx *ctx, double *out_host);
+int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigned long long *out_of_envelope);
+void mlp_release(eddy_ctx *ctx);
 
 // host-side symmetric tridiagonal eigensolver (implicit QL with Wilkinson shift)
 int tridiag_eigen(int n, std::vector<double> &d, std::vector<double> &e, std::vector<double> &q);

@@ -135,7 +135,10 @@ int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   if (rc) return rc;
   double repr1 = ctx->sc.ru1 / ctx->sc.prn;
   TmaMaps<DNF> maps;
-  const double *src[DNF] = {ctx->f[EDDY_DENS], ctx->f[EDDY_TV], ctx->f[EDDY_UO], ctx->f[EDDY_VO], ctx->f[EDDY_WO],
+  // eddy diffusivity: the dynamic model's nu_t (kappa_t = nu_t, src/Eddy6.f:2959)
+  // or the learned closure's kappa_t
+  const double *kv = ctx->prm.closure == 1 ? ctx->kappa : ctx->f[EDDY_TV];
+  const double *src[DNF] = {ctx->f[EDDY_DENS], kv, ctx->f[EDDY_UO], ctx->f[EDDY_VO], ctx->f[EDDY_WO],
                             ctx->f[EDDY_RHA]};
   for (int q = 0; q < DNF; q++) {
     const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], DTX + 2, DTY + 2);

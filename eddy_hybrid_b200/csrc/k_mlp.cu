@@ -28,7 +28,7 @@ constexpr int GKC = 64;  // K chunk per smem stage
 // K multiple of 16.  Rows of A beyond M read as zero.
 __global__ void __launch_bounds__(GT)
     k_umma_gemm(int M, int N, int K, const __nv_bfloat16 *__restrict__ A, const __nv_bfloat16 *__restrict__ B,
-                float *__restrict__ D, int acc, int *err) {
+                float *__restrict__ D, int acc, int kper, int *err) {
   extern __shared__ __align__(1024) unsigned char sm_[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
@@ -53,8 +53,9 @@ __global__ void __launch_bounds__(GT)
   const uint32_t idesc = umma::make_idesc_bf16(128, N);
   bool ok = true;
   int phase = 0;
-  for (int k0 = 0; k0 < K; k0 += GKC) {
-    int kc = min(GKC, K - k0);
+  const int kbeg = blockIdx.y * kper, kend = min(K, kbeg + kper);
+  for (int k0 = kbeg; k0 < kend; k0 += GKC) {
+    int kc = min(GKC, kend - k0);
     // stage A (128 x kc) and B (N x kc) into the canonical K-major layout
     for (int e = tid; e < 128 * (kc / 8); e += GT) {
       int r = e / (kc / 8), c8 = (e % (kc / 8)) * 8;
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(GT)
         // K step of 16 = two core matrices along K: byte offset 2 * LBO
         uint64_t ad = umma::make_desc(sa + (ks / 8) * 128, 128, 128 * (kc / 8));
         uint64_t bd = umma::make_desc(sb + (ks / 8) * 128, 128, 128 * (kc / 8));
-        umma::mma_bf16(tm, ad, bd, idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+        umma::mma_bf16(tm, ad, bd, idesc, (k0 > kbeg || ks > 0) ? 1u : 0u);
       }
       umma::commit(&bar);
     }
@@ -93,8 +94,13 @@ __global__ void __launch_bounds__(GT)
     umma::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
     if (ok && row < M) {
       float *dst = D + (size_t)row * N + c0;
+      if (gridDim.y > 1) {
 #pragma unroll
-      for (int q = 0; q < 16; q++) dst[q] = acc ? dst[q] + v[q] : v[q];
+        for (int q = 0; q < 16; q++) atomicAdd(dst + q, v[q]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; q++) dst[q] = acc ? dst[q] + v[q] : v[q];
+      }
     }
   }
   umma::fence_before_sync();
@@ -105,15 +111,21 @@ __global__ void __launch_bounds__(GT)
 }  // namespace
 
 // host launcher for the generic GEMM; A, B, D device pointers
-int launch_umma_gemm(eddy_ctx *ctx, int M, int N, int K, const void *A, const void *B, float *D, int acc) {
-  if (M % 128 || N % 16 || N < 16 || N > 256 || K % 16 || K < 16) {
-    ctx->err = "umma gemm: M%128, N%16 (16..256), K%16 required";
+// splitk > 1: K is split over that many CTAs whose partial products are
+// atomically added into D (which then always accumulates).
+int launch_umma_gemm(eddy_ctx *ctx, int M, int N, int K, const void *A, const void *B, float *D, int acc,
+                     int splitk = 1) {
+  if (M < 1 || N % 16 || N < 16 || N > 256 || K % 16 || K < 16 || splitk < 1) {
+    ctx->err = "umma gemm: N%16 (16..256), K%16 required";
     return EDDY_EINVAL;
   }
+  int kper = ((K + splitk - 1) / splitk + GKC - 1) / GKC * GKC;
+  int ns = (K + kper - 1) / kper;
   size_t smem = (size_t)(128 + N) * GKC * 2 + 1024;
   EDDY_CUDA(cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_umma_gemm<<<M / 128, GT, smem, ctx->stream>>>(M, N, K, static_cast<const __nv_bfloat16 *>(A),
-                                                  static_cast<const __nv_bfloat16 *>(B), D, acc, ctx->err_flag);
+  k_umma_gemm<<<dim3((M + 127) / 128, ns), GT, smem, ctx->stream>>>(
+      M, N, K, static_cast<const __nv_bfloat16 *>(A), static_cast<const __nv_bfloat16 *>(B), D, acc, kper,
+      ctx->err_flag);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
@@ -140,4 +152,675 @@ extern "C" int eddy_umma_gemm_bf16(eddy_ctx *ctx, int M, int N, int K, const uin
   cudaFree(dB);
   cudaFree(dD);
   return rc;
+}
+
+// ===========================================================================
+// Closure network: parameters, features, fused inference, training.
+// theta layout (FP32): W1[64][16] b1[64] W2[64][64] b2[64] W3[64][64] b3[64]
+// W4[16][64] b4[16]; W[n][k] is output n, input k (K-major rows).  Inputs 12..15
+// of layer 1 and outputs 2..15 of layer 4 are padding (zero weights).
+// meta (FP32): feat_mean[12] feat_istd[12] env_lo[12] env_hi[12] s_nu s_kappa.
+// ===========================================================================
+namespace {
+
+constexpr int NFEAT = 12, KIN = 16, HID = 64, NOUT = 16;
+constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + HID * KIN, OFF_W2 = OFF_B1 + HID, OFF_B2 = OFF_W2 + HID * HID,
+              OFF_W3 = OFF_B2 + HID, OFF_B3 = OFF_W3 + HID * HID, OFF_W4 = OFF_B3 + HID,
+              OFF_B4 = OFF_W4 + NOUT * HID, NTHETA = OFF_B4 + NOUT;
+constexpr int NMETA = 4 * NFEAT + 2;
+
+struct MlpMeta {
+  float mean[NFEAT], istd[NFEAT], lo[NFEAT], hi[NFEAT], s_nu, s_kappa;
+};
+
+__device__ __forceinline__ float silu(float x) { return x / (1.f + __expf(-x)); }
+__device__ __forceinline__ float sigm(float x) { return 1.f / (1.f + __expf(-x)); }
+__device__ __forceinline__ float softplus(float x) { return x > 20.f ? x : log1pf(__expf(x)); }
+
+// raw features of interior cell (i,j,k) and its filter width Delta
+// (9 velocity-gradient components * Delta, |grad rho| * Delta, N^2 = -g drho/dx,
+// distance to the nearest x wall)
+__device__ __forceinline__ void cell_features(const Dims &d, const DevMetrics &m, double grav, double xwall_lo,
+                                              double xwall_hi, const double *__restrict__ uo,
+                                              const double *__restrict__ vo, const double *__restrict__ wo,
+                                              const double *__restrict__ dens, const double *__restrict__ xc,
+                                              int i, int j, int k, float *f, float &delta) {
+  const long long q = fidx(d, i, j, k);
+  const long long sy = d.nx, sz = (long long)d.nx * d.ny;
+  auto UC = [&](long long o) { return 0.5 * (uo[q + o - 1] + uo[q + o]); };
+  auto VC = [&](long long o) { return 0.5 * (vo[q + o - sy] + vo[q + o]); };
+  auto WC = [&](long long o) { return 0.5 * (wo[q + o - sz] + wo[q + o]); };
+  double dudx = m.ap[i] * (uo[q] - uo[q - 1]);
+  double dudy = 0.5 * (m.bv[j] * (UC(sy) - UC(0)) + m.bv[j - 1] * (UC(0) - UC(-sy)));
+  double dudz = 0.5 * (m.cw[k] * (UC(sz) - UC(0)) + m.cw[k - 1] * (UC(0) - UC(-sz)));
+  double dvdx = 0.5 * (m.au[i] * (VC(1) - VC(0)) + m.au[i - 1] * (VC(0) - VC(-1)));
+  double dvdy = m.bp[j] * (vo[q] - vo[q - sy]);
+  double dvdz = 0.5 * (m.cw[k] * (VC(sz) - VC(0)) + m.cw[k - 1] * (VC(0) - VC(-sz)));
+  double dwdx = 0.5 * (m.au[i] * (WC(1) - WC(0)) + m.au[i - 1] * (WC(0) - WC(-1)));
+  double dwdy = 0.5 * (m.bv[j] * (WC(sy) - WC(0)) + m.bv[j - 1] * (WC(0) - WC(-sy)));
+  double dwdz = m.cp[k] * (wo[q] - wo[q - sz]);
+  double drx = 0.5 * (m.au[i] * (dens[q + 1] - dens[q]) + m.au[i - 1] * (dens[q] - dens[q - 1]));
+  double dry = 0.5 * (m.bv[j] * (dens[q + sy] - dens[q]) + m.bv[j - 1] * (dens[q] - dens[q - sy]));
+  double drz = 0.5 * (m.cw[k] * (dens[q + sz] - dens[q]) + m.cw[k - 1] * (dens[q] - dens[q - sz]));
+  double del = cbrt(1.0 / (m.ap[i] * m.bp[j] * m.cp[k]));
+  delta = (float)del;
+  f[0] = (float)(del * dudx); f[1] = (float)(del * dudy); f[2] = (float)(del * dudz);
+  f[3] = (float)(del * dvdx); f[4] = (float)(del * dvdy); f[5] = (float)(del * dvdz);
+  f[6] = (float)(del * dwdx); f[7] = (float)(del * dwdy); f[8] = (float)(del * dwdz);
+  f[9] = (float)(del * sqrt(drx * drx + dry * dry + drz * drz));
+  f[10] = (float)(-grav * drx);
+  double x = xc[i];
+  f[11] = (float)fmin(x - xwall_lo, xwall_hi - x);
+}
+
+__device__ __forceinline__ void interior_ijk(const Dims &d, long long t, int &i, int &j, int &k) {
+  long long mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
+  i = d.ix1 + (int)(t % mi);
+  j = d.jy1 + (int)((t / mi) % mj);
+  k = d.kz1 + (int)(t / (mi * mj));
+}
+
+// raw features (n x 12) and dynamic-model targets nu_t/Delta for a list of
+// interior cell indices
+__global__ void k_harvest(Dims d, DevMetrics m, double grav, double xlo, double xhi, const double *uo,
+                          const double *vo, const double *wo, const double *dens, const double *xc, const double *tv,
+                          const long long *cells, int n, float *X, float *T) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int i, j, k;
+  interior_ijk(d, cells[s], i, j, k);
+  float f[NFEAT], del;
+  cell_features(d, m, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
+  for (int c = 0; c < NFEAT; c++) X[(size_t)s * NFEAT + c] = f[c];
+  T[s] = (float)(tv[fidx(d, i, j, k)] / del);
+}
+
+// ---- fused inference ------------------------------------------------------
+constexpr int IT = 128;
+struct InferSmem {
+  unsigned char w1[HID * KIN * 2], w2[HID * HID * 2], w3[HID * HID * 2], w4[NOUT * HID * 2];
+  unsigned char a0[128 * KIN * 2], h[128 * HID * 2];
+  float b1[HID], b2[HID], b3[HID], b4[NOUT];
+  MlpMeta meta;
+  uint64_t bar;
+  uint32_t tmem;
+  int nout;
+};
+
+__device__ __forceinline__ void stage_weights(unsigned char *dst, const __nv_bfloat16 *src, int rows, int K) {
+  for (int e = threadIdx.x; e < rows * K / 8; e += blockDim.x) {
+    int r = e / (K / 8), c8 = (e % (K / 8)) * 8;
+    *reinterpret_cast<uint4 *>(dst + umma::kmajor_offset(r, c8, K)) =
+        *reinterpret_cast<const uint4 *>(src + (size_t)r * K + c8);
+  }
+}
+
+__device__ __forceinline__ void mma_layer(uint32_t tm, const unsigned char *a, const unsigned char *b, int N, int K) {
+  uint32_t idesc = umma::make_idesc_bf16(128, N);
+  for (int ks = 0; ks < K; ks += 16) {
+    uint64_t ad = umma::make_desc(a + (ks / 8) * 128, 128, 128 * (K / 8));
+    uint64_t bd = umma::make_desc(b + (ks / 8) * 128, 128, 128 * (K / 8));
+    umma::mma_bf16(tm, ad, bd, idesc, ks > 0 ? 1u : 0u);
+  }
+}
+
+// hidden epilogue: TMEM (64 cols of this thread's row) + bias -> SiLU -> bf16 row
+__device__ __forceinline__ void hidden_epilogue(uint32_t tm, int warp, int row, const float *bias,
+                                                unsigned char *h) {
+#pragma unroll
+  for (int c0 = 0; c0 < HID; c0 += 16) {
+    float v[16];
+    umma::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+    for (int q = 0; q < 16; q += 8) {
+      __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) o[e] = __float2bfloat16_rn(silu(v[q + e] + bias[c0 + q + e]));
+      *reinterpret_cast<uint4 *>(h + umma::kmajor_offset(row, c0 + q, HID)) = *reinterpret_cast<uint4 *>(o);
+    }
+  }
+}
+
+__device__ __forceinline__ bool sync_and_wait(uint64_t *bar, int &phase) {
+  bool ok = umma::mbar_wait(bar, phase);
+  phase ^= 1;
+  umma::fence_after_sync();
+  return ok;
+}
+
+__device__ __forceinline__ void publish_smem() {
+  umma::fence_smem_to_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+}
+
+// nu_t -> tv, kappa_t -> kappa for every interior cell; cells whose
+// normalised features leave [lo, hi] take the fallback (last dynamic-model
+// value).  counts[0] += out-of-envelope cells.
+__global__ void __launch_bounds__(IT)
+    k_mlp_infer(Dims d, DevMetrics m, double grav, double xlo, double xhi, const double *__restrict__ uo,
+                const double *__restrict__ vo, const double *__restrict__ wo, const double *__restrict__ dens,
+                const double *__restrict__ xc, const __nv_bfloat16 *__restrict__ wbf, const float *__restrict__ theta,
+                const float *__restrict__ meta, const double *__restrict__ fallback, double *__restrict__ tv,
+                double *__restrict__ kappa, unsigned long long *counts, int *err) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  InferSmem &S = *reinterpret_cast<InferSmem *>(smraw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    umma::tmem_alloc(&S.tmem, 64);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    umma::mbar_init(&S.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    S.nout = 0;
+  }
+  stage_weights(S.w1, wbf + OFF_W1, HID, KIN);
+  stage_weights(S.w2, wbf + OFF_W2, HID, HID);
+  stage_weights(S.w3, wbf + OFF_W3, HID, HID);
+  stage_weights(S.w4, wbf + OFF_W4, NOUT, HID);
+  for (int e = tid; e < HID; e += IT) {
+    S.b1[e] = theta[OFF_B1 + e];
+    S.b2[e] = theta[OFF_B2 + e];
+    S.b3[e] = theta[OFF_B3 + e];
+  }
+  if (tid < NOUT) S.b4[tid] = theta[OFF_B4 + tid];
+  for (int e = tid; e < NMETA; e += IT) reinterpret_cast<float *>(&S.meta)[e] = meta[e];
+  publish_smem();
+  const uint32_t tm = S.tmem;
+  const long long ninner = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
+  const long long ntiles = (ninner + 127) / 128;
+  int phase = 0;
+  bool ok = true;
+  int nout = 0;
+  for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    long long t = tile * 128 + tid;
+    bool valid = t < ninner;
+    int i = d.ix1, j = d.jy1, k = d.kz1;
+    float f[NFEAT], del = 1.f;
+    bool outside = false;
+    if (valid) {
+      interior_ijk(d, t, i, j, k);
+      cell_features(d, m, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
+      for (int c = 0; c < NFEAT; c++) {
+        f[c] = (f[c] - S.meta.mean[c]) * S.meta.istd[c];
+        outside = outside || !(f[c] >= S.meta.lo[c] && f[c] <= S.meta.hi[c]);
+      }
+    } else {
+      for (int c = 0; c < NFEAT; c++) f[c] = 0.f;
+    }
+    __align__(16) __nv_bfloat16 o[16];
+    for (int c = 0; c < 16; c++) o[c] = __float2bfloat16_rn(c < NFEAT ? f[c] : 0.f);
+    *reinterpret_cast<uint4 *>(S.a0 + umma::kmajor_offset(tid, 0, KIN)) = *reinterpret_cast<uint4 *>(o);
+    *reinterpret_cast<uint4 *>(S.a0 + umma::kmajor_offset(tid, 8, KIN)) = *reinterpret_cast<uint4 *>(o + 8);
+    publish_smem();
+    if (tid == 0) { mma_layer(tm, S.a0, S.w1, HID, KIN); umma::commit(&S.bar); }
+    ok = sync_and_wait(&S.bar, phase) && ok;
+    hidden_epilogue(tm, warp, tid, S.b1, S.h);
+    publish_smem();
+    if (tid == 0) { mma_layer(tm, S.h, S.w2, HID, HID); umma::commit(&S.bar); }
+    ok = sync_and_wait(&S.bar, phase) && ok;
+    __syncthreads();  // every row has read layer-1 activations into the MMA
+    hidden_epilogue(tm, warp, tid, S.b2, S.h);
+    publish_smem();
+    if (tid == 0) { mma_layer(tm, S.h, S.w3, HID, HID); umma::commit(&S.bar); }
+    ok = sync_and_wait(&S.bar, phase) && ok;
+    __syncthreads();
+    hidden_epilogue(tm, warp, tid, S.b3, S.h);
+    publish_smem();
+    if (tid == 0) { mma_layer(tm, S.h, S.w4, NOUT, HID); umma::commit(&S.bar); }
+    ok = sync_and_wait(&S.bar, phase) && ok;
+    float v[16];
+    umma::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16), v);
+    if (valid && ok) {
+      long long q = fidx(d, i, j, k);
+      double nu, ka;
+      if (outside) {
+        nu = fallback[q];
+        ka = fallback[q];
+        nout++;
+      } else {
+        nu = (double)del * S.meta.s_nu * softplus(v[0] + S.b4[0]);
+        ka = (double)del * S.meta.s_kappa * softplus(v[1] + S.b4[1]);
+      }
+      tv[q] = nu;
+      kappa[q] = ka;
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  atomicAdd(&S.nout, nout);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (tid == 0 && S.nout) atomicAdd(counts, (unsigned long long)S.nout);
+  if (warp == 0) umma::tmem_dealloc(tm, 64);
+}
+
+// ---- training -------------------------------------------------------------
+// Z (B x n, f32, pre-bias) += bias; A = bf16(SiLU(Z)) in both B x n and n x B
+__global__ void k_fwd_act(int B, int n, float *Z, const float *bias, __nv_bfloat16 *A, __nv_bfloat16 *AT) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)B * n) return;
+  int b = (int)(t / n), c = (int)(t % n);
+  float z = Z[t] + bias[c];
+  Z[t] = z;
+  __nv_bfloat16 a = __float2bfloat16_rn(silu(z));
+  A[t] = a;
+  AT[(size_t)c * B + b] = a;
+}
+
+// output layer: P = softplus(Z4 + b4) on columns 0,1; loss and dZ4
+__global__ void k_out_grad(int B, float *Z4, const float *b4, const float *Y, __nv_bfloat16 *dZ, __nv_bfloat16 *dZT,
+                           float *db, double *loss) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ float sdb[2];
+  __shared__ double sl;
+  if (threadIdx.x < 2) sdb[threadIdx.x] = 0.f;
+  if (threadIdx.x == 0) sl = 0.;
+  __syncthreads();
+  if (b < B) {
+    for (int c = 0; c < NOUT; c++) {
+      float g = 0.f;
+      if (c < 2) {
+        float z = Z4[(size_t)b * NOUT + c] + b4[c];
+        float p = softplus(z), r = p - Y[(size_t)b * 2 + c];
+        atomicAdd(&sl, (double)(r * r) / B);
+        g = 2.f * r * sigm(z) / B;
+        atomicAdd(&sdb[c], g);
+      }
+      __nv_bfloat16 gb = __float2bfloat16_rn(g);
+      dZ[(size_t)b * NOUT + c] = gb;
+      dZT[(size_t)c * B + b] = gb;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) atomicAdd(&db[threadIdx.x], sdb[threadIdx.x]);
+  if (threadIdx.x == 0) atomicAdd(loss, sl);
+}
+
+// hidden backward: dZ = dA * SiLU'(Z) (bf16, both layouts), db += column sums
+__global__ void k_bwd_act(int B, int n, const float *dA, const float *Z, __nv_bfloat16 *dZ, __nv_bfloat16 *dZT,
+                          float *db) {
+  __shared__ float sdb[HID];
+  for (int c = threadIdx.x; c < n; c += blockDim.x) sdb[c] = 0.f;
+  __syncthreads();
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (long long)B * n) {
+    int b = (int)(t / n), c = (int)(t % n);
+    float z = Z[t], s = sigm(z);
+    float g = dA[t] * (s * (1.f + z * (1.f - s)));
+    __nv_bfloat16 gb = __float2bfloat16_rn(g);
+    dZ[t] = gb;
+    dZT[(size_t)c * B + b] = gb;
+    atomicAdd(&sdb[c], g);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < n; c += blockDim.x) atomicAdd(&db[c], sdb[c]);
+}
+
+// gather a batch: X (bf16 n x 16 normalised features), Y (f32 n x 2)
+__global__ void k_gather(int B, const long long *perm, long long off, const __nv_bfloat16 *X, const float *Y,
+                         __nv_bfloat16 *Xb, __nv_bfloat16 *XbT, float *Yb) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  long long s = perm[off + b];
+  for (int c = 0; c < KIN; c++) {
+    __nv_bfloat16 v = X[s * KIN + c];
+    Xb[(size_t)b * KIN + c] = v;
+    XbT[(size_t)c * B + b] = v;
+  }
+  Yb[2 * b] = Y[2 * s];
+  Yb[2 * b + 1] = Y[2 * s + 1];
+}
+
+// Adam on theta, then refresh the bf16 weights (W and W^T)
+__global__ void k_adam(int n, float *theta, const float *grad, float *m1, float *m2, float lr, float b1, float b2,
+                       float eps, float c1, float c2) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  float g = grad[t];
+  float a = b1 * m1[t] + (1.f - b1) * g, v = b2 * m2[t] + (1.f - b2) * g * g;
+  m1[t] = a;
+  m2[t] = v;
+  theta[t] -= lr * (a / c1) / (sqrtf(v / c2) + eps);
+}
+
+__global__ void k_weights_bf16(const float *theta, __nv_bfloat16 *w, __nv_bfloat16 *wt) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NTHETA) return;
+  w[t] = __float2bfloat16_rn(theta[t]);
+  // transposed copies of the four weight matrices at the same offsets
+  int off = 0, rows = 0, cols = 0;
+  if (t < OFF_B1) { off = OFF_W1; rows = HID; cols = KIN; }
+  else if (t >= OFF_W2 && t < OFF_B2) { off = OFF_W2; rows = HID; cols = HID; }
+  else if (t >= OFF_W3 && t < OFF_B3) { off = OFF_W3; rows = HID; cols = HID; }
+  else if (t >= OFF_W4 && t < OFF_B4) { off = OFF_W4; rows = NOUT; cols = HID; }
+  else return;
+  int r = (t - off) / cols, c = (t - off) % cols;
+  wt[off + c * rows + r] = __float2bfloat16_rn(theta[t]);
+}
+
+__global__ void k_normalise(long long n, const float *raw, const float *meta, __nv_bfloat16 *X) {
+  long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  for (int c = 0; c < KIN; c++)
+    X[s * KIN + c] = __float2bfloat16_rn(c < NFEAT ? (raw[s * NFEAT + c] - meta[c]) * meta[NFEAT + c] : 0.f);
+}
+
+}  // namespace
+
+// ---- host side ---------------------------------------------------------------
+struct MlpTrainBuffers {
+  int B = 0;
+  __nv_bfloat16 *Xb = nullptr, *XbT = nullptr, *A1 = nullptr, *A1T = nullptr, *A2 = nullptr, *A2T = nullptr,
+                *A3 = nullptr, *A3T = nullptr, *dZ4 = nullptr, *dZ4T = nullptr, *dZ = nullptr, *dZT = nullptr;
+  float *Yb = nullptr, *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *Z4 = nullptr, *dA = nullptr;
+  void release() {
+    void *p[] = {Xb, XbT, A1, A1T, A2, A2T, A3, A3T, dZ4, dZ4T, dZ, dZT, Yb, Z1, Z2, Z3, Z4, dA};
+    for (void *q : p) if (q) cudaFree(q);
+    *this = MlpTrainBuffers{};
+  }
+};
+
+struct MlpState {
+  float *theta = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr, *meta = nullptr;
+  __nv_bfloat16 *w = nullptr, *wt = nullptr;
+  double *loss = nullptr;
+  unsigned long long *counts = nullptr;
+  double *fallback = nullptr;  // last dynamic-model nu_t
+  int adam_t = 0;
+  bool ready = false;
+  MlpTrainBuffers tb;
+};
+
+static MlpState *mlp_state(eddy_ctx *ctx) {
+  if (!ctx->mlp) {
+    MlpState *s = new MlpState();
+    ctx->mlp = s;
+  }
+  return static_cast<MlpState *>(ctx->mlp);
+}
+
+void mlp_release(eddy_ctx *ctx) {
+  MlpState *s = static_cast<MlpState *>(ctx->mlp);
+  if (!s) return;
+  void *p[] = {s->theta, s->grad, s->m1, s->m2, s->meta, s->w, s->wt, s->loss, s->counts, s->fallback};
+  for (void *q : p) if (q) cudaFree(q);
+  s->tb.release();
+  delete s;
+  ctx->mlp = nullptr;
+}
+
+static int mlp_alloc(eddy_ctx *ctx, MlpState *s) {
+  if (s->theta) return EDDY_OK;
+  EDDY_CUDA(cudaMalloc(&s->theta, sizeof(float) * NTHETA));
+  EDDY_CUDA(cudaMalloc(&s->grad, sizeof(float) * NTHETA));
+  EDDY_CUDA(cudaMalloc(&s->m1, sizeof(float) * NTHETA));
+  EDDY_CUDA(cudaMalloc(&s->m2, sizeof(float) * NTHETA));
+  EDDY_CUDA(cudaMalloc(&s->meta, sizeof(float) * NMETA));
+  EDDY_CUDA(cudaMalloc(&s->w, sizeof(__nv_bfloat16) * NTHETA));
+  EDDY_CUDA(cudaMalloc(&s->wt, sizeof(__nv_bfloat16) * NTHETA));
+  EDDY_CUDA(cudaMalloc(&s->loss, sizeof(double)));
+  EDDY_CUDA(cudaMalloc(&s->counts, sizeof(unsigned long long)));
+  EDDY_CUDA(cudaMemset(s->m1, 0, sizeof(float) * NTHETA));
+  EDDY_CUDA(cudaMemset(s->m2, 0, sizeof(float) * NTHETA));
+  EDDY_CUDA(cudaMemset(s->wt, 0, sizeof(__nv_bfloat16) * NTHETA));
+  return EDDY_OK;
+}
+
+static int tb_alloc(eddy_ctx *ctx, MlpTrainBuffers &t, int B) {
+  if (t.B == B) return EDDY_OK;
+  t.release();
+  t.B = B;
+  auto bf = [&](__nv_bfloat16 **p, size_t n) { return cudaMalloc(p, n * sizeof(__nv_bfloat16)); };
+  auto fl = [&](float **p, size_t n) { return cudaMalloc(p, n * sizeof(float)); };
+  size_t b = (size_t)B;
+  if (bf(&t.Xb, b * KIN) || bf(&t.XbT, b * KIN) || bf(&t.A1, b * HID) || bf(&t.A1T, b * HID) ||
+      bf(&t.A2, b * HID) || bf(&t.A2T, b * HID) || bf(&t.A3, b * HID) || bf(&t.A3T, b * HID) ||
+      bf(&t.dZ4, b * NOUT) || bf(&t.dZ4T, b * NOUT) || bf(&t.dZ, b * HID) || bf(&t.dZT, b * HID) ||
+      fl(&t.Yb, b * 2) || fl(&t.Z1, b * HID) || fl(&t.Z2, b * HID) || fl(&t.Z3, b * HID) || fl(&t.Z4, b * NOUT) ||
+      fl(&t.dA, b * HID)) {
+    ctx->err = "closure training buffers: allocation failed";
+    return EDDY_ENOMEM;
+  }
+  return EDDY_OK;
+}
+
+int launch_umma_gemm(eddy_ctx *ctx, int M, int N, int K, const void *A, const void *B, float *D, int acc,
+                     int splitk);
+
+// one forward + backward pass over the batch staged in tb (Xb, XbT, Yb);
+// gradients into s->grad, loss into s->loss (added)
+static int fwd_bwd(eddy_ctx *ctx, MlpState *s) {
+  MlpTrainBuffers &t = s->tb;
+  const int B = t.B;
+  cudaStream_t st = ctx->stream;
+  int rc;
+  const int nt = 256;
+  auto blocks = [&](long long n) { return (unsigned)((n + nt - 1) / nt); };
+  const __nv_bfloat16 *w = s->w, *wt = s->wt;
+  float *th = s->theta, *g = s->grad;
+  int splitk = B >= 4096 ? B / 1024 : 1;
+  // forward
+  if ((rc = launch_umma_gemm(ctx, B, HID, KIN, t.Xb, w + OFF_W1, t.Z1, 0, 1))) return rc;
+  k_fwd_act<<<blocks((long long)B * HID), nt, 0, st>>>(B, HID, t.Z1, th + OFF_B1, t.A1, t.A1T);
+  EDDY_LAUNCHED(ctx);
+  if ((rc = launch_umma_gemm(ctx, B, HID, HID, t.A1, w + OFF_W2, t.Z2, 0, 1))) return rc;
+  k_fwd_act<<<blocks((long long)B * HID), nt, 0, st>>>(B, HID, t.Z2, th + OFF_B2, t.A2, t.A2T);
+  EDDY_LAUNCHED(ctx);
+  if ((rc = launch_umma_gemm(ctx, B, HID, HID, t.A2, w + OFF_W3, t.Z3, 0, 1))) return rc;
+  k_fwd_act<<<blocks((long long)B * HID), nt, 0, st>>>(B, HID, t.Z3, th + OFF_B3, t.A3, t.A3T);
+  EDDY_LAUNCHED(ctx);
+  if ((rc = launch_umma_gemm(ctx, B, NOUT, HID, t.A3, w + OFF_W4, t.Z4, 0, 1))) return rc;
+  // backward
+  EDDY_CUDA(cudaMemsetAsync(g, 0, sizeof(float) * NTHETA, st));
+  k_out_grad<<<blocks(B), nt, 0, st>>>(B, t.Z4, th + OFF_B4, t.Yb, t.dZ4, t.dZ4T, g + OFF_B4, s->loss);
+  EDDY_LAUNCHED(ctx);
+  // layer 4: dW4 = dZ4^T A3 ; dA3 = dZ4 W4
+  if ((rc = launch_umma_gemm(ctx, NOUT, HID, B, t.dZ4T, t.A3T, g + OFF_W4, 1, splitk))) return rc;
+  if ((rc = launch_umma_gemm(ctx, B, HID, NOUT, t.dZ4, wt + OFF_W4, t.dA, 0, 1))) return rc;
+  k_bwd_act<<<blocks((long long)B * HID), nt, 0, st>>>(B, HID, t.dA, t.Z3, t.dZ, t.dZT, g + OFF_B3);
+  EDDY_LAUNCHED(ctx);
+  // layer 3
+  if ((rc = launch_umma_gemm(ctx, HID, HID, B, t.dZT, t.A2T, g + OFF_W3, 1, splitk))) return rc;
+  if ((rc = launch_umma_gemm(ctx, B, HID, HID, t.dZ, wt + OFF_W3, t.dA, 0, 1))) return rc;
+  k_bwd_act<<<blocks((long long)B * HID), nt, 0, st>>>(B, HID, t.dA, t.Z2, t.dZ, t.dZT, g + OFF_B2);
+  EDDY_LAUNCHED(ctx);
+  // layer 2
+  if ((rc = launch_umma_gemm(ctx, HID, HID, B, t.dZT, t.A1T, g + OFF_W2, 1, splitk))) return rc;
+  if ((rc = launch_umma_gemm(ctx, B, HID, HID, t.dZ, wt + OFF_W2, t.dA, 0, 1))) return rc;
+  k_bwd_act<<<blocks((long long)B * HID), nt, 0, st>>>(B, HID, t.dA, t.Z1, t.dZ, t.dZT, g + OFF_B1);
+  EDDY_LAUNCHED(ctx);
+  // layer 1
+  if ((rc = launch_umma_gemm(ctx, HID, KIN, B, t.dZT, t.XbT, g + OFF_W1, 1, splitk))) return rc;
+  return EDDY_OK;
+}
+
+static int refresh_bf16(eddy_ctx *ctx, MlpState *s) {
+  k_weights_bf16<<<(NTHETA + 255) / 256, 256, 0, ctx->stream>>>(s->theta, s->w, s->wt);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+extern "C" {
+
+int eddy_closure_set(eddy_ctx *ctx, const float *meta, const float *theta) {
+  if (!ctx || !meta || !theta) return EDDY_EINVAL;
+  MlpState *s = mlp_state(ctx);
+  int rc = mlp_alloc(ctx, s);
+  if (rc) return rc;
+  EDDY_CUDA(cudaMemcpyAsync(s->meta, meta, sizeof(float) * NMETA, cudaMemcpyHostToDevice, ctx->stream));
+  EDDY_CUDA(cudaMemcpyAsync(s->theta, theta, sizeof(float) * NTHETA, cudaMemcpyHostToDevice, ctx->stream));
+  EDDY_CUDA(cudaMemsetAsync(s->m1, 0, sizeof(float) * NTHETA, ctx->stream));
+  EDDY_CUDA(cudaMemsetAsync(s->m2, 0, sizeof(float) * NTHETA, ctx->stream));
+  s->adam_t = 0;
+  if ((rc = refresh_bf16(ctx, s))) return rc;
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  s->ready = true;
+  return EDDY_OK;
+}
+
+int eddy_closure_get(eddy_ctx *ctx, float *meta, float *theta) {
+  if (!ctx || !ctx->mlp) return EDDY_EINVAL;
+  MlpState *s = mlp_state(ctx);
+  if (meta) EDDY_CUDA(cudaMemcpy(meta, s->meta, sizeof(float) * NMETA, cudaMemcpyDeviceToHost));
+  if (theta) EDDY_CUDA(cudaMemcpy(theta, s->theta, sizeof(float) * NTHETA, cudaMemcpyDeviceToHost));
+  return EDDY_OK;
+}
+
+// features (raw) and targets nu_t/Delta of the given interior cells from the
+// current fields (TV holds the dynamic model's viscosity)
+int eddy_closure_harvest(eddy_ctx *ctx, const long long *cells, int n, float *X, float *T) {
+  if (!ctx || !cells || !X || !T || n <= 0) return EDDY_EINVAL;
+  long long *dc = nullptr;
+  float *dX = nullptr, *dT = nullptr;
+  EDDY_CUDA(cudaMalloc(&dc, sizeof(long long) * n));
+  EDDY_CUDA(cudaMalloc(&dX, sizeof(float) * (size_t)n * NFEAT));
+  EDDY_CUDA(cudaMalloc(&dT, sizeof(float) * n));
+  EDDY_CUDA(cudaMemcpyAsync(dc, cells, sizeof(long long) * n, cudaMemcpyHostToDevice, ctx->stream));
+  const std::vector<double> &xu = ctx->h[0];
+  k_harvest<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->d, ctx->m, ctx->sc.grav, xu[1], xu[ctx->d.ix2],
+                                                      ctx->f[EDDY_UO], ctx->f[EDDY_VO], ctx->f[EDDY_WO],
+                                                      ctx->f[EDDY_DENS], ctx->xc_dev, ctx->f[EDDY_TV], dc, n, dX, dT);
+  EDDY_LAUNCHED(ctx);
+  EDDY_CUDA(cudaMemcpyAsync(X, dX, sizeof(float) * (size_t)n * NFEAT, cudaMemcpyDeviceToHost, ctx->stream));
+  EDDY_CUDA(cudaMemcpyAsync(T, dT, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  cudaFree(dc);
+  cudaFree(dX);
+  cudaFree(dT);
+  return EDDY_OK;
+}
+
+// gradients of the mean-squared loss over one batch (n multiple of 128) of
+// raw features X (n x 12) and targets Y (n x 2), at the current parameters
+int eddy_closure_grad(eddy_ctx *ctx, const float *X, const float *Y, int n, float *grad, double *loss) {
+  if (!ctx || !ctx->mlp || !X || !Y || !grad || n <= 0 || n % 128) return EDDY_EINVAL;
+  MlpState *s = mlp_state(ctx);
+  int rc = tb_alloc(ctx, s->tb, n);
+  if (rc) return rc;
+  float *draw = nullptr, *dY = nullptr;
+  __nv_bfloat16 *dXn = nullptr;
+  long long *perm = nullptr;
+  EDDY_CUDA(cudaMalloc(&draw, sizeof(float) * (size_t)n * NFEAT));
+  EDDY_CUDA(cudaMalloc(&dY, sizeof(float) * (size_t)n * 2));
+  EDDY_CUDA(cudaMalloc(&dXn, sizeof(__nv_bfloat16) * (size_t)n * KIN));
+  EDDY_CUDA(cudaMalloc(&perm, sizeof(long long) * n));
+  std::vector<long long> id(n);
+  for (int q = 0; q < n; q++) id[q] = q;
+  EDDY_CUDA(cudaMemcpyAsync(perm, id.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, ctx->stream));
+  EDDY_CUDA(cudaMemcpyAsync(draw, X, sizeof(float) * (size_t)n * NFEAT, cudaMemcpyHostToDevice, ctx->stream));
+  EDDY_CUDA(cudaMemcpyAsync(dY, Y, sizeof(float) * (size_t)n * 2, cudaMemcpyHostToDevice, ctx->stream));
+  k_normalise<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, draw, s->meta, dXn);
+  EDDY_LAUNCHED(ctx);
+  k_gather<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, perm, 0, dXn, dY, s->tb.Xb, s->tb.XbT, s->tb.Yb);
+  EDDY_LAUNCHED(ctx);
+  EDDY_CUDA(cudaMemsetAsync(s->loss, 0, sizeof(double), ctx->stream));
+  rc = fwd_bwd(ctx, s);
+  if (rc == EDDY_OK) {
+    EDDY_CUDA(cudaMemcpyAsync(grad, s->grad, sizeof(float) * NTHETA, cudaMemcpyDeviceToHost, ctx->stream));
+    if (loss) EDDY_CUDA(cudaMemcpyAsync(loss, s->loss, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  cudaFree(draw);
+  cudaFree(dY);
+  cudaFree(dXn);
+  cudaFree(perm);
+  return rc;
+}
+
+// Adam training on the GPU: raw features X (n x 12), targets Y (n x 2),
+// minibatches of `batch` (multiple of 128) drawn from a seeded permutation
+// per epoch; loss_hist[e] = mean batch loss of epoch e.
+int eddy_closure_train(eddy_ctx *ctx, const float *X, const float *Y, long long n, int epochs, int batch, float lr,
+                       unsigned long long seed, double *loss_hist) {
+  if (!ctx || !ctx->mlp || !X || !Y || n < batch || batch <= 0 || batch % 128 || epochs < 1) return EDDY_EINVAL;
+  MlpState *s = mlp_state(ctx);
+  int rc = tb_alloc(ctx, s->tb, batch);
+  if (rc) return rc;
+  float *draw = nullptr, *dY = nullptr;
+  __nv_bfloat16 *dXn = nullptr;
+  long long *perm = nullptr;
+  EDDY_CUDA(cudaMalloc(&draw, sizeof(float) * (size_t)n * NFEAT));
+  EDDY_CUDA(cudaMalloc(&dY, sizeof(float) * (size_t)n * 2));
+  EDDY_CUDA(cudaMalloc(&dXn, sizeof(__nv_bfloat16) * (size_t)n * KIN));
+  EDDY_CUDA(cudaMalloc(&perm, sizeof(long long) * n));
+  EDDY_CUDA(cudaMemcpyAsync(draw, X, sizeof(float) * (size_t)n * NFEAT, cudaMemcpyHostToDevice, ctx->stream));
+  EDDY_CUDA(cudaMemcpyAsync(dY, Y, sizeof(float) * (size_t)n * 2, cudaMemcpyHostToDevice, ctx->stream));
+  k_normalise<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, draw, s->meta, dXn);
+  EDDY_LAUNCHED(ctx);
+  std::vector<long long> p((size_t)n);
+  uint64_t state = seed ^ 0x9E3779B97F4A7C15ull;
+  auto rnd = [&]() {
+    state += 0x9E3779B97F4A7C15ull;
+    uint64_t z = state;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  long long nb = n / batch;
+  for (int e = 0; e < epochs && rc == EDDY_OK; e++) {
+    for (long long q = 0; q < n; q++) p[(size_t)q] = q;
+    for (long long q = n - 1; q > 0; q--) std::swap(p[(size_t)q], p[(size_t)(rnd() % (uint64_t)(q + 1))]);
+    EDDY_CUDA(cudaMemcpyAsync(perm, p.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, ctx->stream));
+    EDDY_CUDA(cudaMemsetAsync(s->loss, 0, sizeof(double), ctx->stream));
+    for (long long b = 0; b < nb && rc == EDDY_OK; b++) {
+      k_gather<<<(batch + 255) / 256, 256, 0, ctx->stream>>>(batch, perm, b * batch, dXn, dY, s->tb.Xb, s->tb.XbT,
+                                                             s->tb.Yb);
+      EDDY_LAUNCHED(ctx);
+      rc = fwd_bwd(ctx, s);
+      if (rc) break;
+      s->adam_t++;
+      const float b1 = 0.9f, b2 = 0.999f;
+      float c1 = 1.f - powf(b1, (float)s->adam_t), c2 = 1.f - powf(b2, (float)s->adam_t);
+      k_adam<<<(NTHETA + 255) / 256, 256, 0, ctx->stream>>>(NTHETA, s->theta, s->grad, s->m1, s->m2, lr, b1, b2,
+                                                            1e-8f, c1, c2);
+      EDDY_LAUNCHED(ctx);
+      rc = refresh_bf16(ctx, s);
+    }
+    double l = 0.;
+    EDDY_CUDA(cudaMemcpyAsync(&l, s->loss, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (loss_hist) loss_hist[e] = l / (double)nb;
+  }
+  cudaFree(draw);
+  cudaFree(dY);
+  cudaFree(dXn);
+  cudaFree(perm);
+  return rc;
+}
+
+}  // extern "C"
+
+// nu_t, kappa_t over the whole field from the fused tensor-core kernel;
+// cells out of the training envelope take `fallback` (the last dynamic
+// nu_t).  out_of_envelope receives the count.
+int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigned long long *out_of_envelope) {
+  MlpState *s = static_cast<MlpState *>(ctx->mlp);
+  if (!s || !s->ready) {
+    ctx->err = "learned closure requested but no network is loaded";
+    return EDDY_EINVAL;
+  }
+  const Dims &d = ctx->d;
+  const std::vector<double> &xu = ctx->h[0];
+  EDDY_CUDA(cudaMemsetAsync(s->counts, 0, sizeof(unsigned long long), ctx->stream));
+  size_t smem = sizeof(InferSmem) + 1024;
+  EDDY_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+  long long ninner = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
+  long long ntiles = (ninner + 127) / 128;
+  int grid = (int)std::min<long long>(ntiles, (long long)nsm * 8);
+  k_mlp_infer<<<grid, IT, smem, ctx->stream>>>(d, ctx->m, ctx->sc.grav, xu[1], xu[d.ix2], ctx->f[EDDY_UO],
+                                              ctx->f[EDDY_VO], ctx->f[EDDY_WO], ctx->f[EDDY_DENS], ctx->xc_dev, s->w,
+                                              s->theta, s->meta, fallback, ctx->f[EDDY_TV], kappa, s->counts,
+                                              ctx->err_flag);
+  EDDY_LAUNCHED(ctx);
+  if (out_of_envelope)
+    EDDY_CUDA(cudaMemcpyAsync(out_of_envelope, s->counts, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+  return EDDY_OK;
 }

@@ -169,6 +169,29 @@ int eddy_max_divergence_noalloc(int nx, int ny, int nz, const double *u, const d
 int eddy_umma_gemm_bf16(eddy_ctx *ctx, int M, int N, int K, const uint16_t *A, const uint16_t *B,
                         float *D, int acc);
 
+/* Network parameters.  meta (50 floats): feature mean[12], 1/std[12], the
+ * training envelope lo[12], hi[12] in normalised units, output scales s_nu,
+ * s_kappa.  theta (10448 floats): W1[64][16] b1[64] W2[64][64] b2[64]
+ * W3[64][64] b3[64] W4[16][64] b4[16] (inputs 12-15 and outputs 2-15 pad). */
+int eddy_closure_set(eddy_ctx *ctx, const float *meta, const float *theta);
+int eddy_closure_get(eddy_ctx *ctx, float *meta, float *theta);
+/* Raw features (n x 12: 9 velocity gradients * Delta, |grad rho| * Delta,
+ * N^2, wall distance) and targets nu_t/Delta (from the current TV) of the
+ * given 0-based interior cell indices (i fastest). */
+int eddy_closure_harvest(eddy_ctx *ctx, const long long *cells, int n, float *X, float *T);
+/* Gradient of the batch loss (n multiple of 128) at the current parameters. */
+int eddy_closure_grad(eddy_ctx *ctx, const float *X, const float *Y, int n, float *grad, double *loss);
+/* Adam training on the GPU (own tensor-core forward/backward kernels). */
+int eddy_closure_train(eddy_ctx *ctx, const float *X, const float *Y, long long n, int epochs, int batch,
+                       float lr, unsigned long long seed, double *loss_hist);
+/* nu_t -> TV and kappa_t over the field with the fused tensor-core MLP;
+ * returns the number of cells outside the training envelope (they take the
+ * last dynamic-model value). */
+int eddy_closure_apply(eddy_ctx *ctx, long long *out_of_envelope);
+/* Recompute the dynamic model (TURVIS) and keep it as the fallback. */
+int eddy_closure_refresh_fallback(eddy_ctx *ctx);
+int eddy_download_kappa(eddy_ctx *ctx, double *host);
+
 int eddy_sync(eddy_ctx *ctx);
 /* Copy the last error message (NUL-terminated, truncated to len). */
 int eddy_last_error(eddy_ctx *ctx, char *buf, int len);
