@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(IT)
       kappa[q] = ka;
     }
     umma::fence_before_sync();
-    __syncthreads();
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;  // block-uniform loop exit
     umma::fence_after_sync();
   }
   if (!ok && tid == 0) atomicExch(err, 1);
