@@ -86,6 +86,7 @@ SIGNATURES = {
     "eddy_step": ([C.c_void_p, C.c_double, C.c_int], C.c_int),
     "eddy_poisson_solve": ([C.c_void_p, _DP, _DP, C.c_int], C.c_int),
     "eddy_max_divergence": ([C.c_void_p, _DP], C.c_int),
+    "eddy_refine_residuals": ([C.c_void_p, _DP, C.c_int], C.c_int),
     "eddy_profile_enable": ([C.c_void_p, C.c_uint], C.c_int),
     "eddy_profile_read": ([C.c_void_p, _DP, C.POINTER(C.c_longlong)], C.c_int),
     "eddy_max_divergence_noalloc": ([C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -217,16 +218,23 @@ class Solver:
         self._check(lib().eddy_max_divergence(self.h, C.byref(v)), "eddy_max_divergence")
         return v.value
 
+    def refine_residuals(self) -> np.ndarray:
+        """max |d - L phi| before each refinement sweep of the last mixed solve."""
+        out = np.zeros(4)
+        self._check(lib().eddy_refine_residuals(self.h, _ptr(out), 4), "eddy_refine_residuals")
+        return out
+
     PROFILE_CATEGORIES = ["rhs_predictor", "boundary", "div_fft_fwd", "transform_fwd",
                           "z_line_solve", "transform_bwd", "fft_bwd", "correct",
-                          "pressure_update", "density", "eddy_viscosity"]
+                          "pressure_update", "density", "eddy_viscosity", "refine_residual",
+                          "precision_copy"]
 
-    def profile_enable(self, mask: int = 0x7FF):
+    def profile_enable(self, mask: int = 0x1FFF):
         self._check(lib().eddy_profile_enable(self.h, mask), "eddy_profile_enable")
 
     def profile_read(self) -> dict:
-        ms = (C.c_double * 11)()
-        n = (C.c_longlong * 11)()
+        ms = (C.c_double * 13)()
+        n = (C.c_longlong * 13)()
         self._check(lib().eddy_profile_read(self.h, ms, n), "eddy_profile_read")
         return {c: (ms[i], n[i]) for i, c in enumerate(self.PROFILE_CATEGORIES)}
 

@@ -26,6 +26,7 @@ UNITS = {
     "k_sgs.cu": ["-fmad=false"],
     "k_noalloc.cu": ["-fmad=false"],
     "k_mlp.cu": [],
+    "k_mixed.cu": [],
     "host_eigen.cpp": [],
 }
 
@@ -39,7 +40,7 @@ def _newer(src_list, out):
 
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    hdrs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    hdrs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     hdrs.append(os.path.join(HERE, "..", "include", "eddy_b200.h"))
     objs = []
     for unit, extra in UNITS.items():

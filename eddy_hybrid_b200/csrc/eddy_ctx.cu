@@ -229,6 +229,7 @@ void free_all(eddy_ctx *ctx) {
   if (ctx->err_flag) cudaFree(ctx->err_flag);
   poisson_plan_destroy(ctx);
   mlp_release(ctx);
+  mixed_release(ctx);
   double *o2[] = {ctx->xc_dev, ctx->kappa, ctx->tv_dyn};
   for (double *p : o2) if (p) cudaFree(p);
   for (ProfEvent &e : ctx->prof_ev) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -268,11 +269,13 @@ void scheme(int ischm, double gam[3], double rho[3], double alf[3]) {
 
 }  // namespace
 
-int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int nz, int bx, int by, int esize) {
+int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int nz, int bx, int by, int esize,
+                       int pitch) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return -1;
+  if (pitch <= 0) pitch = nx;
   cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-  cuuint64_t gstr[2] = {(cuuint64_t)nx * esize, (cuuint64_t)nx * ny * esize};
+  cuuint64_t gstr[2] = {(cuuint64_t)pitch * esize, (cuuint64_t)pitch * ny * esize};
   cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   cuuint32_t est[3] = {1, 1, 1};
   CUtensorMapDataType dt = esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -323,7 +326,8 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
     if (p.itype[b] != 60 && p.itype[b] != 82) return fail(EDDY_EINVAL, "x boundaries must be type 60 or 82");
   if (p.itype[5] != 305 || (p.itype[6] != 730))
     return fail(EDDY_EINVAL, "z boundaries must be the hybrid inlet 305 and the convective outlet 730");
-  if (p.precision != EDDY_PLAIN_FP64) return fail(EDDY_EINVAL, "mixed precision form not available in this build");
+  if (p.precision != EDDY_PLAIN_FP64 && p.precision != EDDY_MIXED)
+    return fail(EDDY_EINVAL, "precision must be EDDY_PLAIN_FP64 or EDDY_MIXED");
   if (p.closure != 0 && p.closure != 1) return fail(EDDY_EINVAL, "closure must be 0 (dynamic) or 1 (learned)");
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
@@ -359,6 +363,7 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   cudaMemset(ctx->err_flag, 0, sizeof(int));
   rc = poisson_plan_create(ctx);
   if (rc) return fail(rc, nullptr);
+  if (p.precision == EDDY_MIXED && (rc = mixed_create(ctx))) return fail(rc, nullptr);
   {
     size_t bx = sizeof(double) * ctx->h[1].size();
     if (cudaMalloc(&ctx->xc_dev, bx) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
@@ -390,6 +395,8 @@ int eddy_upload(eddy_ctx *ctx, int field, const double *host) {
   size_t b = sizeof(double) * (field >= EDDY_PLANEU ? (size_t)ctx->d.nx * ctx->d.ny : (size_t)ctx->d.ncell);
   EDDY_CUDA(cudaMemcpyAsync(ctx->f[field], host, b, cudaMemcpyHostToDevice, ctx->stream));
   if (field == EDDY_DENS) EDDY_CUDA(cudaMemcpyAsync(ctx->dens_alt, host, b, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = mixed_from64(ctx, field);
+  if (rc) return rc;
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
   return EDDY_OK;
 }
@@ -397,6 +404,8 @@ int eddy_upload(eddy_ctx *ctx, int field, const double *host) {
 int eddy_download(eddy_ctx *ctx, int field, double *host) {
   if (check_ctx(ctx) || field < 0 || field >= EDDY_NFIELDS || !host) return EDDY_EINVAL;
   size_t b = sizeof(double) * (field >= EDDY_PLANEU ? (size_t)ctx->d.nx * ctx->d.ny : (size_t)ctx->d.ncell);
+  int rc = mixed_to64(ctx, field);
+  if (rc) return rc;
   EDDY_CUDA(cudaMemcpyAsync(host, ctx->f[field], b, cudaMemcpyDeviceToHost, ctx->stream));
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
   return EDDY_OK;
@@ -467,7 +476,18 @@ int eddy_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
 int eddy_turvis(eddy_ctx *ctx) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   if (ctx->prm.isgs == 0) return EDDY_OK;
-  return launch_turvis(ctx);
+  int rc = launch_turvis(ctx);
+  if (rc == EDDY_OK && ctx->mixed) rc = mixed_after_sgs(ctx);
+  return rc;
+}
+
+int eddy_refine_residuals(eddy_ctx *ctx, double *out, int n) {
+  if (check_ctx(ctx) || !out || n < 1) return EDDY_EINVAL;
+  if (!ctx->mixed) {
+    ctx->err = "refinement residuals exist only in the mixed-precision form";
+    return EDDY_EINVAL;
+  }
+  return mixed_residuals(ctx, out, n);
 }
 
 int eddy_initialize(eddy_ctx *ctx, double dt) {
@@ -513,6 +533,12 @@ int eddy_initialize(eddy_ctx *ctx, double dt) {
   if (ctx->prm.isgs != 0 && (rc = launch_turvis(ctx))) return rc;
   EDDY_CUDA(cudaMemcpyAsync(ctx->tv_dyn, f[EDDY_TV], sizeof(double) * d.ncell, cudaMemcpyDeviceToDevice, ctx->stream));
   EDDY_CUDA(cudaMemcpyAsync(ctx->kappa, f[EDDY_TV], sizeof(double) * d.ncell, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (ctx->mixed) {
+    // FP32 copies of every field the mixed form reads
+    const int fl[] = {EDDY_UO, EDDY_VO, EDDY_WO, EDDY_P, EDDY_DENS, EDDY_TV, EDDY_UA, EDDY_VA, EDDY_WA, EDDY_RHA};
+    for (int q : fl)
+      if ((rc = mixed_from64(ctx, q))) return rc;
+  }
   return EDDY_OK;
 }
 
@@ -521,6 +547,7 @@ int eddy_substep(eddy_ctx *ctx, int is, double dt) {
   double gam[3], rho[3], alf[3];
   scheme(ctx->prm.ischm, gam, rho, alf);
   double alfxdt = alf[is] * dt, gamxdt = gam[is] * dt, rhoxdt = rho[is] * dt;
+  if (ctx->mixed) return mixed_substep(ctx, alfxdt, gamxdt, rhoxdt);
   double **f = ctx->f;
   int rc;
   {
@@ -568,14 +595,18 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
       if (rc) return rc;
     }
     if (ctx->prm.isgs != 0) {
-      ProfScope ps(ctx, PROF_TURVIS);
       int rc;
-      if (ctx->prm.closure == 1) {
-        rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, nullptr);
-      } else {
-        rc = launch_turvis(ctx);
+      if (ctx->mixed && (rc = mixed_before_sgs(ctx))) return rc;
+      {
+        ProfScope ps(ctx, PROF_TURVIS);
+        if (ctx->prm.closure == 1) {
+          rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, nullptr);
+        } else {
+          rc = launch_turvis(ctx);
+        }
+        if (rc) return rc;
       }
-      if (rc) return rc;
+      if (ctx->mixed && (rc = mixed_after_sgs(ctx))) return rc;
     }
   }
   return EDDY_OK;
@@ -590,10 +621,11 @@ int closure_envelope_check(eddy_ctx *ctx, unsigned long long *nout) {
 int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_device) {
   if (check_ctx(ctx) || !rhs || !sol) return EDDY_EINVAL;
   size_t b = sizeof(double) * (size_t)ctx->d.ncell;
-  if (on_device) return launch_poisson_rhs(ctx, rhs, sol);
+  if (on_device) return ctx->mixed ? mixed_poisson_rhs(ctx, rhs, sol) : launch_poisson_rhs(ctx, rhs, sol);
   // host arrays: stage through DP / US on the device
   EDDY_CUDA(cudaMemcpyAsync(ctx->f[EDDY_US], rhs, b, cudaMemcpyHostToDevice, ctx->stream));
-  int rc = launch_poisson_rhs(ctx, ctx->f[EDDY_US], ctx->f[EDDY_DP]);
+  int rc = ctx->mixed ? mixed_poisson_rhs(ctx, ctx->f[EDDY_US], ctx->f[EDDY_DP])
+                      : launch_poisson_rhs(ctx, ctx->f[EDDY_US], ctx->f[EDDY_DP]);
   if (rc) return rc;
   EDDY_CUDA(cudaMemcpyAsync(sol, ctx->f[EDDY_DP], b, cudaMemcpyDeviceToHost, ctx->stream));
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -603,8 +635,10 @@ int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_dev
 int eddy_closure_apply(eddy_ctx *ctx, long long *out_of_envelope) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   unsigned long long n = 0;
-  int rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, &n);
-  if (rc) return rc;
+  int rc;
+  if (ctx->mixed && (rc = mixed_before_sgs(ctx))) return rc;
+  if ((rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, &n))) return rc;
+  if (ctx->mixed && (rc = mixed_after_sgs(ctx))) return rc;
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
   if (out_of_envelope) *out_of_envelope = (long long)n;
   return EDDY_OK;
@@ -614,6 +648,7 @@ int eddy_closure_refresh_fallback(eddy_ctx *ctx) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   int rc = launch_turvis(ctx);
   if (rc) return rc;
+  if (ctx->mixed && (rc = mixed_after_sgs(ctx))) return rc;
   EDDY_CUDA(cudaMemcpyAsync(ctx->tv_dyn, ctx->f[EDDY_TV], sizeof(double) * ctx->d.ncell, cudaMemcpyDeviceToDevice,
                             ctx->stream));
   ctx->closure_refresh++;

@@ -57,7 +57,7 @@ struct PoissonPlan {
 // kernel categories timed with CUDA events when profiling is enabled
 enum {
   PROF_RHS_PRED = 0, PROF_BC, PROF_DIV_FFT, PROF_GEMM_FWD, PROF_TRIDIAG, PROF_GEMM_BWD, PROF_FFT_BWD,
-  PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_NCAT
+  PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_REFINE, PROF_CONVERT, PROF_NCAT
 };
 
 struct TmaEntry {
@@ -96,6 +96,7 @@ struct eddy_ctx {
   double *kappa = nullptr;      // eddy diffusivity of the learned closure (NX,NY,NZ)
   double *tv_dyn = nullptr;     // last dynamic-model nu_t: closure fallback (NX,NY,NZ)
   void *mlp = nullptr;          // closure network state (k_mlp.cu)
+  void *mixed = nullptr;        // FP32 field set of the mixed-precision form (k_mixed.cu)
   long long closure_out = 0, closure_cells = 0, closure_refresh = 0;
   // profiling (CUDA events on the context stream around each category)
   unsigned prof_mask = 0;
@@ -180,6 +181,26 @@ int launch_direct(eddy_ctx *ctx, const double *us, const double *vs, const doubl
 // solve from an explicit right-hand side array (interior of rhs) -> dp
 int launch_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp);
 int launch_max_divergence(eddy_ctx *ctx, double *out_host);
+// DIRECT's ghost convention on a solution array (z planes zero, x Neumann, y periodic)
+int launch_dp_ghost(eddy_ctx *ctx, double *dp);
+
+// mixed-precision form (k_mixed.cu): FP32 stencils and FFTs, FP64 line solves,
+// FP64-residual iterative refinement, FP64 projection onto FP64 master velocities
+int mixed_create(eddy_ctx *ctx);
+void mixed_release(eddy_ctx *ctx);
+// refresh the FP32 copy of `field` from its FP64 array (after an upload)
+int mixed_from64(eddy_ctx *ctx, int field);
+// write the FP64 array of `field` from its FP32 master (before a download)
+int mixed_to64(eddy_ctx *ctx, int field);
+int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
+// mixed Poisson solve of L dp = rhs (rhs, dp FP64 device arrays)
+int mixed_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp);
+// max |residual| before each refinement sweep of the last mixed solve (host copy)
+int mixed_residuals(eddy_ctx *ctx, double *out, int n);
+// around an eddy-viscosity update: FP64 density for the closure features
+// before, FP32 copies of nu_t / kappa_t after
+int mixed_before_sgs(eddy_ctx *ctx);
+int mixed_after_sgs(eddy_ctx *ctx);
 int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigned long long *out_of_envelope);
 void mlp_release(eddy_ctx *ctx);
 

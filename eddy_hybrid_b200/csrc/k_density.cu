@@ -4,9 +4,9 @@
 // Explicit form: the Crank-Nicolson part RS is zero in the interior.
 #include "eddy_internal.h"
 #include "tma_ring.cuh"
+#include "bc_templates.cuh"
+#include "stencil_density.cuh"
 
-
-int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, double sgn, int zero);
 
 namespace {
 
@@ -23,44 +23,9 @@ __global__ void __launch_bounds__(DTX *DTY)
       d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err,
       [&](int i, int j, int k, bool active, const RingAcc<DTX, DTY, DNF> &S) {
         if (!active) return;
-        auto dens = [&](int a, int b, int c) { return S.at(0, a, b, c); };
-        auto kv = [&](int a, int b, int c) { return S.at(1, a, b, c); };
-        double qxp = S.at(2, 0, 0, 0), qxm = S.at(2, -1, 0, 0);
-        double rxp = (dens(1, 0, 0) + dens(0, 0, 0)) * 0.5;
-        double rxm = (dens(0, 0, 0) + dens(-1, 0, 0)) * 0.5;
-        double vyp = S.at(3, 0, 0, 0), vym = S.at(3, 0, -1, 0);
-        double ryp = (dens(0, 1, 0) + dens(0, 0, 0)) * 0.5;
-        double rym = (dens(0, 0, 0) + dens(0, -1, 0)) * 0.5;
-        double wzp = S.at(4, 0, 0, 0), wzm = S.at(4, 0, 0, -1);
-        double rzp = (dens(0, 0, 1) + dens(0, 0, 0)) * 0.5;
-        double rzm = (dens(0, 0, 0) + dens(0, 0, -1)) * 0.5;
-        double drdxp = m.au[i] * (dens(1, 0, 0) - dens(0, 0, 0));
-        double drdxm = m.au[i - 1] * (dens(0, 0, 0) - dens(-1, 0, 0));
-        double drdyp = m.bv[j] * (dens(0, 1, 0) - dens(0, 0, 0));
-        double drdym = m.bv[j - 1] * (dens(0, 0, 0) - dens(0, -1, 0));
-        double drdzp = m.cw[k] * (dens(0, 0, 1) - dens(0, 0, 0));
-        double drdzm = m.cw[k - 1] * (dens(0, 0, 0) - dens(0, 0, -1));
-        double kvip = 0.5 * (kv(1, 0, 0) + kv(0, 0, 0));
-        double kvim = 0.5 * (kv(-1, 0, 0) + kv(0, 0, 0));
-        double kvjp = 0.5 * (kv(0, 1, 0) + kv(0, 0, 0));
-        double kvjm = 0.5 * (kv(0, -1, 0) + kv(0, 0, 0));
-        double kvkp = 0.5 * (kv(0, 0, 1) + kv(0, 0, 0));
-        double kvkm = 0.5 * (kv(0, 0, -1) + kv(0, 0, 0));
-        double txxp = (repr1 + kvip) * drdxp;
-        double txxm = (repr1 + kvim) * drdxm;
-        double tyyp = (repr1 + kvjp) * drdyp;
-        double tyym = (repr1 + kvjm) * drdym;
-        double tzzp = (repr1 + kvkp) * drdzp;
-        double tzzm = (repr1 + kvkm) * drdzm;
-        double h11 = -m.ap[i] * (rxp * qxp - rxm * qxm);
-        double h22 = -m.bp[j] * (ryp * vyp - rym * vym);
-        double h33 = -m.cp[k] * (rzp * wzp - rzm * wzm);
-        double t11 = m.ap[i] * (txxp - txxm);
-        double t22 = m.bp[j] * (tyyp - tyym);
-        double t33 = m.cp[k] * (tzzp - tzzm);
-        double rr = h11 + h22 + h33 + t11 + t22 + t33;
+        double rr = rhs_dens<double>(S, m, repr1, i, j, k);
         double coef = 0.5 * alfxdt;
-        double dnew = dens(0, 0, 0) + gamxdt * rr + rhoxdt * S.at(5, 0, 0, 0) + coef * 0.0;
+        double dnew = S.at(0, 0, 0, 0) + gamxdt * rr + rhoxdt * S.at(5, 0, 0, 0) + coef * 0.0;
         long long q = fidx(d, i, j, k);
         rha[q] = rr;
         double bg = m.dens_bg[(i - 1) + d.nx * (j - 1)];
@@ -90,43 +55,11 @@ __global__ void k_dens_ghost_copy(Dims d, const double *__restrict__ dens, doubl
   dn[q] = dens[q];
 }
 
-__global__ void k_dens_inlet(Dims d, double *dens, const double *plane) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.nx * d.ny) return;
-  dens[t] = plane[t];
-}
-
 }  // namespace
 
 // BOUNDINOUTD (src/boundary.f:2241-2281) then BOUNDARY_DENS (:2001-2044)
 int launch_boundinoutd_dens(eddy_ctx *ctx, double *dens) {
-  const Dims &d = ctx->d;
-  int rc;
-#define F(...) \
-  if ((rc = launch_fill_plane(ctx, __VA_ARGS__)) != EDDY_OK) return rc
-  if (d.itype[5] == 305) {
-    k_dens_inlet<<<(d.nx * d.ny + 255) / 256, 256, 0, ctx->stream>>>(d, dens, ctx->f[EDDY_PLANED]);
-    EDDY_LAUNCHED(ctx);
-    F(dens, 2, 2, 1, 1., 0);
-  }
-  if (d.itype[6] == 730) { F(dens, 2, d.kz2, d.kz2 - 1, 1., 0); F(dens, 2, d.nz, d.kz2, 1., 0); }
-  if (d.itype[6] == 710) F(dens, 2, d.kz2, d.kz2 - 1, 1., 0);
-  // BOUNDARY_DENS
-  for (int ib = 1; ib <= 6; ib++) {
-    int t = d.itype[ib];
-    if (t == 50) {
-      ctx->err = "density wall type 50 is not on the restated hot path";
-      return EDDY_EINVAL;
-    } else if (t == 80 || t == 82) {
-      if (ib == 1) F(dens, 0, 1, d.ix1, 1., 0);
-      if (ib == 2) { F(dens, 0, d.ix2, d.ix2 - 1, 1., 0); F(dens, 0, d.nx, d.ix2, 1., 0); }
-    }
-  }
-  if (d.itype[1] == 500) { F(dens, 0, 1, d.ix2, 1., 0); F(dens, 0, d.nx, d.ix1, 1., 0); }
-  if (d.itype[3] == 500) { F(dens, 1, 1, d.jy2, 1., 0); F(dens, 1, d.ny, d.jy1, 1., 0); }
-  if (d.itype[5] == 500) { F(dens, 2, 1, d.kz2, 1., 0); F(dens, 2, d.nz, d.kz1, 1., 0); }
-#undef F
-  return EDDY_OK;
+  return bc_boundinoutd_dens<double>(ctx, ctx->d.nx, dens);
 }
 
 int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
@@ -141,7 +74,7 @@ int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   const double *src[DNF] = {ctx->f[EDDY_DENS], kv, ctx->f[EDDY_UO], ctx->f[EDDY_VO], ctx->f[EDDY_WO],
                             ctx->f[EDDY_RHA]};
   for (int q = 0; q < DNF; q++) {
-    const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], DTX + 2, DTY + 2);
+    const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], RingGeom<DTX, DTY>::PX, DTY + 2);
     if (!mp) return EDDY_ECUDA;
     maps.m[q] = *mp;
   }

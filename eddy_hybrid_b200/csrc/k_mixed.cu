@@ -1,0 +1,973 @@
+// k_mixed.cu -- the mixed-precision form of the time advance.
+//
+// Storage: FP32 copies of u, v, w, p, nu_t, kappa_t feed the stencils; the
+// predictor outputs u*, v*, w*, the RHS history and the density live in FP32
+// only.  FP64 is kept for
+//   * the master velocities written by the projection (max|div u| is a
+//     difference of nearly equal face fluxes and needs FP64 storage),
+//   * the pressure and the Poisson solution,
+//   * the per-wavenumber z-line elimination, the residual and the divergence.
+// FP32 arrays are (NX,NY,NZ) with the row pitch rounded up to 4 elements so
+// every row starts on a 16-byte boundary (TMA row strides).
+//
+// Poisson solve (src/direct.f:2-1118 semantics): the FP32 path (divergence in
+// FP64 -> FP32 FFT along y -> FP32 eigen-transform GEMM -> FP64 Thomas along z
+// on FP32 storage -> FP32 GEMM -> FP32 inverse FFT) is wrapped in FP64-residual
+// iterative refinement: phi_0 = S(d); r_s = d - L phi_s (FP64); phi_{s+1} =
+// phi_s + S(r_s).
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bc_templates.cuh"
+#include "eddy_internal.h"
+#include "tma_ring.cuh"
+
+namespace {
+
+#include "stencil_density.cuh"
+#include "stencil_rhs.cuh"
+
+// 1-D metric arrays in FP32 (same indexing as DevMetrics)
+struct DevMetrics32 {
+  float *ap, *au, *av, *aw;
+  float *bp, *bu, *bv, *bw;
+  float *cp, *cu, *cv, *cw;
+  float *whx, *why, *whz;
+  float *dfxu, *dfxw, *dfxul, *dfxwl, *dfxd, *dfxdl;
+  float *dens_bg;
+};
+
+struct MixedState {
+  int px = 0;      // row pitch (elements) of the FP32 arrays
+  size_t n32 = 0;  // px * ny * nz
+  float *uo = nullptr, *vo = nullptr, *wo = nullptr, *p = nullptr, *tv = nullptr, *kv = nullptr;
+  float *us = nullptr, *vs = nullptr, *ws = nullptr, *ua = nullptr, *va = nullptr, *wa = nullptr;
+  float *dens = nullptr, *dens_alt = nullptr, *rha = nullptr;
+  float *mbuf = nullptr;
+  DevMetrics32 m{};
+  float *twr = nullptr, *twi = nullptr;  // FFT twiddles: forward table then backward table
+  double *resid = nullptr;               // max |r| before each sweep (device, 4 entries)
+  double *wout = nullptr;                // outlet-face w (NX,NY) in FP64: exact mass balance
+};
+
+MixedState *ms(eddy_ctx *ctx) { return static_cast<MixedState *>(ctx->mixed); }
+
+// ---------------------------------------------------------------------------
+// precision copies over the whole (NX,NY,NZ) array
+__global__ void k_to32(Dims d, int px, const double *__restrict__ a, float *__restrict__ b) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.ncell) return;
+  int i = 1 + (int)(t % d.nx);
+  long long r = t / d.nx;
+  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
+  b[pidx(d, px, i, j, k)] = (float)a[t];
+}
+
+__global__ void k_to64(Dims d, int px, const float *__restrict__ b, double *__restrict__ a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.ncell) return;
+  int i = 1 + (int)(t % d.nx);
+  long long r = t / d.nx;
+  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
+  a[t] = (double)b[pidx(d, px, i, j, k)];
+}
+
+// ---------------------------------------------------------------------------
+// RHS + PREDICTORD in FP32 (src/rhs.f:4-438, src/timeindeg.f:1041-1265) on the
+// TMA plane ring; same structure as the FP64 kernel.
+constexpr int TX = 32, TY = 8, NFLD = 9, KCHUNK = 32;  // uo vo wo tv p dens ua va wa
+using Acc9 = RingAcc<TX, TY, NFLD, float>;
+
+struct MomAcc32 {
+  const Acc9 &r;
+  __device__ __forceinline__ float u(int di, int dj, int dk) const { return r.at(0, di, dj, dk); }
+  __device__ __forceinline__ float v(int di, int dj, int dk) const { return r.at(1, di, dj, dk); }
+  __device__ __forceinline__ float w(int di, int dj, int dk) const { return r.at(2, di, dj, dk); }
+  __device__ __forceinline__ float t(int di, int dj, int dk) const { return r.at(3, di, dj, dk); }
+};
+
+__global__ void __launch_bounds__(TX *TY)
+    k_rhs32(Dims d, DevMetrics32 m, Scalars s, int px, const __grid_constant__ TmaMaps<NFLD> maps,
+            float *__restrict__ us, float *__restrict__ vs, float *__restrict__ ws, float *__restrict__ ua,
+            float *__restrict__ va, float *__restrict__ wa, float alfxdt, float gamxdt, float rhoxdt, int *err) {
+  const float ru1 = (float)s.ru1, grav = (float)s.grav;
+  const float dpdx = (float)s.dpdx, dpdy = (float)s.dpdy, dpdz = (float)s.dpdz;
+  tma_march<NFLD, TX, TY, KCHUNK, float>(
+      d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err, [&](int i, int j, int k, bool active, const Acc9 &R) {
+        if (!active) return;
+        MomAcc32 S{R};
+        long long q = pidx(d, px, i, j, k);
+        const bool jin = j >= d.jy1 && j <= d.jy2;
+        const bool kin = (k >= d.kz1 && k <= d.kz2);
+        float uval = 0.f;
+        if (kin && jin && i >= d.ibu && i <= d.ieu) {
+          float ur = rhs_u<float>(S, m, ru1, i, j, k);
+          float ustar = R.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * R.at(6, 0, 0, 0) -
+                        alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) - alfxdt * dpdx;
+          if (s.idens == 1)
+            ustar = ustar - alfxdt * 0.5f * grav *
+                                ((R.at(5, 1, 0, 0) - m.dens_bg[i + d.nx * (j - 1)]) +
+                                 (R.at(5, 0, 0, 0) - m.dens_bg[(i - 1) + d.nx * (j - 1)]));
+          ua[q] = ur;
+          if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0.f - ustar) * alfxdt;
+          if (s.ivspngl == 1) ustar = ustar + m.dfxul[k] * (0.f - ustar) * alfxdt;
+          uval = ustar;
+        }
+        us[q] = uval;
+        float vval = 0.f;
+        if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
+          float vr = rhs_v<float>(S, m, ru1, i, j, k);
+          float vstar = R.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * R.at(7, 0, 0, 0) -
+                        alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) - alfxdt * dpdy;
+          va[q] = vr;
+          if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0.f - vstar) * alfxdt;
+          if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin) vstar = vstar + m.dfxwl[k] * (0.f - vstar) * alfxdt;
+          vval = vstar;
+        }
+        vs[q] = vval;
+        float wval = 0.f;
+        if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
+          float wr = rhs_w<float>(S, m, ru1, i, j, k);
+          float wstar = R.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * R.at(8, 0, 0, 0) -
+                        alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) - alfxdt * dpdz;
+          wa[q] = wr;
+          if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1.f - wstar) * alfxdt;
+          if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1.f - wstar) * alfxdt;
+          wval = wstar;
+        }
+        ws[q] = wval;
+      });
+}
+
+// ghost faces of u*,v*,w* are zero (src/rhs.f:65-70)
+__global__ void k_zero_faces32(Dims d, int px, float *a, float *b, float *c3) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long sxy = (long long)d.nx * d.ny, sxz = (long long)d.nx * d.nz, syz = (long long)d.ny * d.nz;
+  int i, j, k;
+  if (t < 2 * sxy) {
+    long long r = t % sxy;
+    i = 1 + (int)(r % d.nx); j = 1 + (int)(r / d.nx); k = (t / sxy) ? d.nz : 1;
+  } else if (t < 2 * sxy + 2 * sxz) {
+    long long u = t - 2 * sxy, r = u % sxz;
+    i = 1 + (int)(r % d.nx); k = 1 + (int)(r / d.nx); j = (u / sxz) ? d.ny : 1;
+  } else if (t < 2 * sxy + 2 * sxz + 2 * syz) {
+    long long u = t - 2 * sxy - 2 * sxz, r = u % syz;
+    j = 1 + (int)(r % d.ny); k = 1 + (int)(r / d.ny); i = (u / syz) ? d.nx : 1;
+  } else {
+    return;
+  }
+  long long q = pidx(d, px, i, j, k);
+  a[q] = 0.f;
+  b[q] = 0.f;
+  c3[q] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 FFT along y on TI32 consecutive x lines per block (one k plane)
+constexpr int TI32 = 32, FT32 = 256;
+
+__device__ __forceinline__ int bitrev(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
+
+__device__ void fft_lines32(float *re, float *im, int L, const float *__restrict__ twr,
+                            const float *__restrict__ twi) {
+  for (int len = 2; len <= L; len <<= 1) {
+    int h = len >> 1, stride = L / len;
+    for (int bf = threadIdx.x; bf < TI32 * (L >> 1); bf += blockDim.x) {
+      int ii = bf % TI32, pq = bf / TI32;
+      int grp = pq / h, qq = pq % h;
+      int a = grp * len + qq, b = a + h;
+      float wr = twr[qq * stride], wi = twi[qq * stride];
+      float xr = re[b * TI32 + ii], xi = im[b * TI32 + ii];
+      float tr = wr * xr - wi * xi;
+      float ti = wr * xi + wi * xr;
+      float ar = re[a * TI32 + ii], ai = im[a * TI32 + ii];
+      re[b * TI32 + ii] = ar - tr;
+      im[b * TI32 + ii] = ai - ti;
+      re[a * TI32 + ii] = ar + tr;
+      im[a * TI32 + ii] = ai + ti;
+    }
+    __syncthreads();
+  }
+}
+
+// Forward transform of the right-hand side.  mode 0: d = div(u*)/alfxdt in
+// FP64 from the FP32 predictor velocities (src/timeindeg.f:941-949), stored
+// to dvec; mode 1: d = dvec; mode 2: r = dvec - L phi (FP64 residual of the
+// DIRECT operator: Neumann x and z, periodic y), max|r| -> rmax.
+__global__ void __launch_bounds__(FT32)
+    k_fwd32(Dims d, DevMetrics m, int px, const float *__restrict__ us, const float *__restrict__ vs,
+            const float *__restrict__ ws, const double *__restrict__ win, const double *__restrict__ wout,
+            const double *__restrict__ phi, double *__restrict__ dvec, int mode, double alfxdt, double rdy2,
+            int logL, const float *__restrict__ twr, const float *__restrict__ twi, float *__restrict__ spec,
+            unsigned long long *rmax) {
+  extern __shared__ float smf[];
+  __shared__ double red[FT32 / 32];
+  const int L = 1 << logL, M = d.nx - 2;
+  float *re = smf, *im = smf + L * TI32;
+  const int i0 = d.ix1 + blockIdx.x * TI32;
+  const int k = d.kz1 + blockIdx.y;
+  const long long sz = (long long)d.nx * d.ny;
+  double amax = 0.;
+  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
+    int ii = t % TI32, jj = t / TI32;
+    int i = i0 + ii, j = d.jy1 + jj;
+    double v = 0.;
+    if (i <= d.ix2) {
+      long long q = fidx(d, i, j, k);
+      if (mode == 0) {
+        long long p = pidx(d, px, i, j, k);
+        // inlet and outlet faces from their FP64 planes (the mass balance of
+        // the convective outlet holds in FP64, so the right-hand side stays
+        // compatible with the Neumann operator)
+        int pl = (i - 1) + d.nx * (j - 1);
+        double wk = k == d.kz2 ? wout[pl] : (double)ws[p];
+        double wkm = k == d.kz1 ? win[pl] : (double)ws[p - (long long)px * d.ny];
+        v = (m.ap[i] * ((double)us[p] - (double)us[p - 1]) + m.bp[j] * ((double)vs[p] - (double)vs[p - px]) +
+             m.cp[k] * (wk - wkm));
+        v = v / alfxdt;
+        dvec[q] = v;
+      } else if (mode == 1) {
+        v = dvec[q];
+      } else {
+        double c = phi[q];
+        double lx = 0., lz = 0.;
+        if (i < d.ix2) lx += m.ap[i] * m.au[i] * (phi[q + 1] - c);
+        if (i > d.ix1) lx += m.ap[i] * m.au[i - 1] * (phi[q - 1] - c);
+        int jp = j < d.jy2 ? j + 1 : d.jy1, jm = j > d.jy1 ? j - 1 : d.jy2;
+        double ly = (phi[fidx(d, i, jp, k)] - 2. * c + phi[fidx(d, i, jm, k)]) * rdy2;
+        if (k < d.kz2) lz += m.cp[k] * m.cw[k] * (phi[q + sz] - c);
+        if (k > d.kz1) lz += m.cp[k] * m.cw[k - 1] * (phi[q - sz] - c);
+        v = dvec[q] - (lx + ly + lz);
+        amax = fmax(amax, fabs(v));
+      }
+    }
+    int r = bitrev(jj, logL);
+    re[r * TI32 + ii] = (float)v;
+    im[r * TI32 + ii] = 0.f;
+  }
+  if (mode == 2) {
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
+  }
+  __syncthreads();
+  if (mode == 2 && threadIdx.x == 0) {
+    double b = 0.;
+    for (int w = 0; w < FT32 / 32; w++) b = fmax(b, red[w]);
+    atomicMax(rmax, (unsigned long long)__double_as_longlong(b));
+  }
+  fft_lines32(re, im, L, twr, twi);
+  const long long lineK = (long long)(k - d.kz1) * L;
+  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
+    int ii = t % TI32, J = t / TI32;
+    int i = i0 + ii;
+    if (i > d.ix2) continue;
+    float v;
+    if (J == 0) v = re[ii];
+    else if (J == L - 1) v = re[(L / 2) * TI32 + ii];
+    else {
+      int qq = (J + 1) / 2;
+      v = (J & 1) ? re[qq * TI32 + ii] : im[qq * TI32 + ii];
+    }
+    spec[(long long)(i - d.ix1) + (long long)M * (J + lineK)] = v;
+  }
+}
+
+// (S - mean[J==0]) / L, Hermitian extension, inverse FFT; phi = or += result
+__global__ void __launch_bounds__(FT32)
+    k_bwd32(Dims d, const float *__restrict__ spec, const double *__restrict__ dpm, int logL,
+            const float *__restrict__ twr, const float *__restrict__ twi, double *__restrict__ phi, int accumulate) {
+  extern __shared__ float smf[];
+  const int L = 1 << logL, M = d.nx - 2;
+  float *re = smf, *im = smf + L * TI32;
+  const int i0 = d.ix1 + blockIdx.x * TI32;
+  const int k = d.kz1 + blockIdx.y;
+  const long long lineK = (long long)(k - d.kz1) * L;
+  const float mean = (float)dpm[0], rl = 1.f / (float)L;
+  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
+    int ii = t % TI32, q = t / TI32;
+    int i = i0 + ii;
+    float xr = 0.f, xi = 0.f;
+    if (i <= d.ix2) {
+      const float *S = spec + (long long)(i - d.ix1);
+      auto get = [&](int J) {
+        float v = S[(long long)M * (J + lineK)];
+        if (J == 0) v = v - mean;
+        return v * rl;
+      };
+      if (q == 0) xr = get(0);
+      else if (q == L / 2) xr = get(L - 1);
+      else if (q < L / 2) { xr = get(2 * q - 1); xi = get(2 * q); }
+      else { int qq = L - q; xr = get(2 * qq - 1); xi = -get(2 * qq); }
+    }
+    int r = bitrev(q, logL);
+    re[r * TI32 + ii] = xr;
+    im[r * TI32 + ii] = xi;
+  }
+  __syncthreads();
+  fft_lines32(re, im, L, twr, twi);
+  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
+    int ii = t % TI32, jj = t / TI32;
+    int i = i0 + ii;
+    if (i > d.ix2) continue;
+    long long q = fidx(d, i, d.jy1 + jj, k);
+    double v = (double)re[jj * TI32 + ii];
+    phi[q] = accumulate ? phi[q] + v : v;
+  }
+}
+
+// Thomas along z per (m,J) line in FP64 arithmetic on FP32 storage
+// (same elimination and singular-line treatment as the FP64 solve)
+__global__ void __launch_bounds__(256)
+    k_tridiag32(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
+                const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
+                const double *__restrict__ wz, float *__restrict__ g, double *__restrict__ cpr) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)M * L) return;
+  int mi = (int)(t % M), J = (int)(t / M);
+  long long ML = (long long)M * L;
+  int pin = (J == 0 && mi == m0);
+  int s0 = pin ? 1 : 0;
+  double lm = lam[mi], akJ = ak[J];
+  double cm = 0.;
+  if (pin) {
+    double sv = 0., vv = 0.;
+    for (int k = 0; k < N; k++) {
+      sv += (double)g[t + ML * k] * wz[k];
+      vv += wz[k];
+    }
+    cm = sv / vv;
+  }
+  double prev_c = 0., prev_d = 0.;
+  for (int k = s0; k < N; k++) {
+    double a = (k == s0) ? 0. : an[k];
+    double b = (bn[k] + lm) - akJ;
+    double den = b - a * prev_c;
+    double c = cn[k] / den;
+    double f = (double)g[t + ML * k] - cm;
+    double dd = (f - a * prev_d) / den;
+    cpr[t + ML * k] = c;
+    cpr[t + ML * k + ML * N] = dd;
+    prev_c = c;
+    prev_d = dd;
+  }
+  double x = prev_d;
+  g[t + ML * (N - 1)] = (float)x;
+  for (int k = N - 2; k >= s0; k--) {
+    x = cpr[t + ML * k + ML * N] - cpr[t + ML * k] * x;
+    g[t + ML * k] = (float)x;
+  }
+  if (pin) g[t] = 0.f;
+}
+
+__global__ void k_plane_sum32(int M, int L, int N, const float *__restrict__ s, double *part) {
+  __shared__ double sh[256];
+  double acc = 0.;
+  long long n = (long long)M * N;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    long long k = t / M, i = t % M;
+    acc += (double)s[i + (long long)M * L * k];
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sum_final(int nparts, long long count, const double *part, double *out) {
+  if (threadIdx.x != 0) return;
+  double s = 0.;
+  for (int b = 0; b < nparts; b++) s += part[b];
+  out[0] = s / (double)count;
+}
+
+// ---------------------------------------------------------------------------
+// CORRECT (src/timeindeg.f:981-1028) in FP64 onto the FP64 masters, with the
+// FP32 copies written alongside
+constexpr int BX = 32, BY = 4, BZ = 2;
+
+__global__ void __launch_bounds__(BX *BY *BZ)
+    k_correct_mixed(Dims d, DevMetrics m, int px, const float *__restrict__ us, const float *__restrict__ vs,
+                    const float *__restrict__ ws, const double *__restrict__ dp, double *__restrict__ uo,
+                    double *__restrict__ vo, double *__restrict__ wo, float *__restrict__ uo32,
+                    float *__restrict__ vo32, float *__restrict__ wo32, double alfxdt) {
+  int i = 1 + threadIdx.x + blockIdx.x * BX;
+  int j = 1 + threadIdx.y + blockIdx.y * BY;
+  int k = 1 + threadIdx.z + blockIdx.z * BZ;
+  if (i > d.nx || j > d.ny || k > d.nz) return;
+  long long q = fidx(d, i, j, k), p = pidx(d, px, i, j, k);
+  const int sy = d.nx;
+  const long long sz = (long long)d.nx * d.ny;
+  bool kin = k >= d.kz1 && k <= d.kz2, jin = j >= d.jy1 && j <= d.jy2;
+  if (kin && jin && i >= d.ibu && i <= d.ieu) {
+    double u = (double)us[p] - m.au[i] * (dp[q + 1] - dp[q]) * alfxdt;
+    uo[q] = u;
+    uo32[p] = (float)u;
+  }
+  if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
+    double v = (double)vs[p] - m.bv[j] * (dp[q + sy] - dp[q]) * alfxdt;
+    vo[q] = v;
+    vo32[p] = (float)v;
+  }
+  if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
+    double w = (double)ws[p] - m.cw[k] * (dp[q + sz] - dp[q]) * alfxdt;
+    wo[q] = w;
+    wo32[p] = (float)w;
+  }
+}
+
+// FP32 copies of the planes the velocity boundary conditions write:
+// x planes 1, IX2, NX; y planes 1, NY; z planes 1, KZ2, NZ
+__global__ void k_sync_planes(Dims d, int px, const double *__restrict__ u, const double *__restrict__ v,
+                              const double *__restrict__ w, float *__restrict__ u32, float *__restrict__ v32,
+                              float *__restrict__ w32) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long syz = (long long)d.ny * d.nz, sxz = (long long)d.nx * d.nz, sxy = (long long)d.nx * d.ny;
+  int i, j, k;
+  if (t < 3 * syz) {
+    int f = (int)(t / syz);
+    long long r = t % syz;
+    j = 1 + (int)(r % d.ny); k = 1 + (int)(r / d.ny);
+    i = f == 0 ? 1 : (f == 1 ? d.ix2 : d.nx);
+  } else if (t < 3 * syz + 2 * sxz) {
+    long long u2 = t - 3 * syz, r = u2 % sxz;
+    i = 1 + (int)(r % d.nx); k = 1 + (int)(r / d.nx);
+    j = (u2 / sxz) ? d.ny : 1;
+  } else if (t < 3 * syz + 2 * sxz + 3 * sxy) {
+    long long u2 = t - 3 * syz - 2 * sxz;
+    int f = (int)(u2 / sxy);
+    long long r = u2 % sxy;
+    i = 1 + (int)(r % d.nx); j = 1 + (int)(r / d.nx);
+    k = f == 0 ? 1 : (f == 1 ? d.kz2 : d.nz);
+  } else {
+    return;
+  }
+  long long q = fidx(d, i, j, k), p = pidx(d, px, i, j, k);
+  u32[p] = (float)u[q];
+  v32[p] = (float)v[q];
+  w32[p] = (float)w[q];
+}
+
+// pressure update (src/Eddy6.f:2772-2806, 2911-2953) in FP64, FP32 copy alongside
+__global__ void k_pref_m(Dims d, const double *p, const double *dp, double *out) {
+  double s = 0.;
+  for (int j = d.jy1; j <= d.jy2; j++) {
+    long long q = fidx(d, d.ix1, j, 2);
+    s += p[q] + dp[q];
+  }
+  out[0] = s / (double)(d.ny - 2);
+}
+
+__global__ void __launch_bounds__(256)
+    k_pupdate_m(Dims d, int px, double *__restrict__ p, const double *__restrict__ dp,
+                const double *__restrict__ pref, float *__restrict__ p32) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.ncell) return;
+  double v = (p[t] + dp[t]) - pref[0];
+  p[t] = v;
+  int i = 1 + (int)(t % d.nx);
+  long long r = t / d.nx;
+  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
+  p32[pidx(d, px, i, j, k)] = (float)v;
+}
+
+__device__ __forceinline__ int map_axis(int a, int n, int lo, int hi, int periodic, int active) {
+  if (!active) return a;
+  if (a == 1) return periodic ? hi : lo;
+  if (a == n) return periodic ? lo : hi;
+  return a;
+}
+
+__global__ void k_pghost_m(Dims d, int px, double *p, float *p32) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long sxy = (long long)d.nx * d.ny, sxz = (long long)d.nx * d.nz, syz = (long long)d.ny * d.nz;
+  int i, j, k;
+  if (t < 2 * sxy) {
+    long long r = t % sxy;
+    i = 1 + (int)(r % d.nx); j = 1 + (int)(r / d.nx); k = (t / sxy) ? d.nz : 1;
+  } else if (t < 2 * sxy + 2 * sxz) {
+    long long u = t - 2 * sxy, r = u % sxz;
+    i = 1 + (int)(r % d.nx); k = 1 + (int)(r / d.nx); j = (u / sxz) ? d.ny : 1;
+  } else if (t < 2 * sxy + 2 * sxz + 2 * syz) {
+    long long u = t - 2 * sxy - 2 * sxz, r = u % syz;
+    j = 1 + (int)(r % d.ny); k = 1 + (int)(r / d.ny); i = (u / syz) ? d.nx : 1;
+  } else {
+    return;
+  }
+  int zact = d.itype[5] != 0 || d.itype[6] != 0;
+  int zper = d.itype[5] == 500;
+  int si = map_axis(i, d.nx, d.ix1, d.ix2, d.mp == 0, 1);
+  int sj = map_axis(j, d.ny, d.jy1, d.jy2, d.lp == 0, 1);
+  int sk = map_axis(k, d.nz, d.kz1, d.kz2, zper, zact);
+  if (si == i && sj == j && sk == k) return;
+  double v = p[fidx(d, si, sj, sk)];
+  p[fidx(d, i, j, k)] = v;
+  p32[pidx(d, px, i, j, k)] = (float)v;
+}
+
+// ---------------------------------------------------------------------------
+// density in FP32 (src/rhs_density.f + src/density.f:6-99) on the plane ring
+constexpr int DTX = 32, DTY = 8, DKC = 32, DNF = 6;  // dens kv uo vo wo rha
+using Acc6 = RingAcc<DTX, DTY, DNF, float>;
+
+__global__ void __launch_bounds__(DTX *DTY)
+    k_density32(Dims d, DevMetrics32 m, Scalars s, int px, const __grid_constant__ TmaMaps<DNF> maps,
+                float *__restrict__ rha, float *__restrict__ dn, float repr1, float alfxdt, float gamxdt,
+                float rhoxdt, int *err) {
+  tma_march<DNF, DTX, DTY, DKC, float>(d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err,
+                                       [&](int i, int j, int k, bool active, const Acc6 &S) {
+                                         if (!active) return;
+                                         float rr = rhs_dens<float>(S, m, repr1, i, j, k);
+                                         float dnew = S.at(0, 0, 0, 0) + gamxdt * rr + rhoxdt * S.at(5, 0, 0, 0);
+                                         long long q = pidx(d, px, i, j, k);
+                                         rha[q] = rr;
+                                         float bg = m.dens_bg[(i - 1) + d.nx * (j - 1)];
+                                         if (s.idspngl == 1) dnew = dnew + m.dfxdl[k] * (bg - dnew) * alfxdt;
+                                         if (i >= d.ix2 - s.dspngx1) dnew = dnew + m.dfxd[i] * (bg - dnew) * alfxdt;
+                                         dn[q] = dnew;
+                                       });
+}
+
+__global__ void k_dens_ghost32(Dims d, int px, const float *__restrict__ dens, float *__restrict__ dn) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long sxy = (long long)d.nx * d.ny, sxz = (long long)d.nx * d.nz, syz = (long long)d.ny * d.nz;
+  int i, j, k;
+  if (t < 2 * sxy) {
+    long long r = t % sxy;
+    i = 1 + (int)(r % d.nx); j = 1 + (int)(r / d.nx); k = (t / sxy) ? d.nz : 1;
+  } else if (t < 2 * sxy + 2 * sxz) {
+    long long u = t - 2 * sxy, r = u % sxz;
+    i = 1 + (int)(r % d.nx); k = 1 + (int)(r / d.nx); j = (u / sxz) ? d.ny : 1;
+  } else if (t < 2 * sxy + 2 * sxz + 2 * syz) {
+    long long u = t - 2 * sxy - 2 * sxz, r = u % syz;
+    j = 1 + (int)(r % d.ny); k = 1 + (int)(r / d.ny); i = (u / syz) ? d.nx : 1;
+  } else {
+    return;
+  }
+  long long q = pidx(d, px, i, j, k);
+  dn[q] = dens[q];
+}
+
+// ---------------------------------------------------------------------------
+// outlet-face plane in FP64 (BOUNDINOUT 730 mass balance, src/boundary.f:920-944)
+__global__ void k_plane_from32(Dims d, int px, const float *__restrict__ w32, int k, double *__restrict__ plane) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.nx * d.ny) return;
+  int i = 1 + t % d.nx, j = 1 + t / d.nx;
+  plane[t] = (double)w32[pidx(d, px, i, j, k)];
+}
+
+__global__ void k_rescale_plane(Dims d, int px, double *__restrict__ plane, float *__restrict__ w32,
+                                const double *flux_in, const double *flux_out) {
+  int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= mi * mj) return;
+  int i = d.ix1 + t % mi, j = d.jy1 + t / mi;
+  int q = (i - 1) + d.nx * (j - 1);
+  double qin1 = flux_in[0], qout = flux_out[0];
+  double v = qout != 0. ? plane[q] * (qin1 / qout) : qin1 / flux_out[1];
+  plane[q] = v;
+  w32[pidx(d, px, i, j, d.kz2)] = (float)v;
+}
+
+__global__ void k_plane_to64(Dims d, const double *__restrict__ plane, double *__restrict__ w, int k) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.nx * d.ny) return;
+  w[(long long)t + (long long)d.nx * d.ny * (k - 1)] = plane[t];
+}
+
+// ---------------------------------------------------------------------------
+const CUtensorMap *tmap32(eddy_ctx *ctx, const float *ptr, int bx, int by) {
+  for (TmaEntry &e : ctx->tmaps)
+    if (e.ptr == ptr && e.bx == bx && e.by == by) return &e.map;
+  TmaEntry e;
+  e.ptr = ptr;
+  e.bx = bx;
+  e.by = by;
+  int r = make_tensor_map_3d(&e.map, ptr, ctx->d.nx, ctx->d.ny, ctx->d.nz, bx, by, 4, ms(ctx)->px);
+  if (r != 0) {
+    ctx->err = "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")";
+    return nullptr;
+  }
+  ctx->tmaps.push_back(e);
+  return &ctx->tmaps.back().map;
+}
+
+constexpr int NPART = 296;
+
+inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
+
+int to32(eddy_ctx *ctx, const double *a, float *b) {
+  k_to32<<<nblk(ctx->d.ncell), 256, 0, ctx->stream>>>(ctx->d, ms(ctx)->px, a, b);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+int to64(eddy_ctx *ctx, const float *b, double *a) {
+  k_to64<<<nblk(ctx->d.ncell), 256, 0, ctx->stream>>>(ctx->d, ms(ctx)->px, b, a);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+int log2i(int L) {
+  int l = 0;
+  while ((1 << l) < L) l++;
+  return l;
+}
+
+// FP32 spectral solve of the transformed right-hand side in pp.spec (as
+// float) -> phi (set or accumulate)
+int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
+  MixedState *x = ms(ctx);
+  PoissonPlan &pp = ctx->pp;
+  const Dims &d = ctx->d;
+  int M = pp.M, L = pp.L, N = pp.N;
+  long long lines = (long long)L * N;
+  float *s1 = reinterpret_cast<float *>(pp.spec), *s2 = reinterpret_cast<float *>(pp.spec2);
+  const float one = 1.f, zero = 0.f;
+  cublasStatus_t bs;
+  {
+    ProfScope ps(ctx, PROF_GEMM_FWD);
+    bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Af32, M, s1, M, &zero, s2, M);
+    if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (forward transform) failed"; return EDDY_ECUDA; }
+    ctx->launches++;
+  }
+  {
+    ProfScope ps(ctx, PROF_TRIDIAG);
+    long long nl = (long long)M * L;
+    k_tridiag32<<<nblk(nl), 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, pp.wz, s2,
+                                                  pp.cprime);
+    EDDY_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, PROF_GEMM_BWD);
+    bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Ab32, M, s2, M, &zero, s1, M);
+    if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (backward transform) failed"; return EDDY_ECUDA; }
+    ctx->launches++;
+  }
+  ProfScope ps(ctx, PROF_FFT_BWD);
+  k_plane_sum32<<<NPART, 256, 0, ctx->stream>>>(M, L, N, s1, pp.red);
+  EDDY_LAUNCHED(ctx);
+  k_sum_final<<<1, 32, 0, ctx->stream>>>(NPART, (long long)M * N, pp.red, ctx->scal + 3);
+  EDDY_LAUNCHED(ctx);
+  size_t smem = sizeof(float) * 2 * L * TI32;
+  dim3 g((M + TI32 - 1) / TI32, N);
+  k_bwd32<<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi,
+                                          accumulate);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+// forward pass (mode as in k_fwd32) into pp.spec (as float)
+int fwd32(eddy_ctx *ctx, int mode, double alfxdt, const double *phi, double *dvec, int sweep) {
+  MixedState *x = ms(ctx);
+  PoissonPlan &pp = ctx->pp;
+  const Dims &d = ctx->d;
+  size_t smem = sizeof(float) * 2 * pp.L * TI32;
+  dim3 g((pp.M + TI32 - 1) / TI32, pp.N);
+  ProfScope ps(ctx, mode == 2 ? PROF_REFINE : PROF_DIV_FFT);
+  k_fwd32<<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
+                                          phi, dvec, mode, alfxdt,
+                                          1.0 / ctx->delysq, log2i(pp.L), x->twr, x->twi,
+                                          reinterpret_cast<float *>(pp.spec),
+                                          reinterpret_cast<unsigned long long *>(x->resid + sweep));
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+// the refined solve: mode 0 (divergence of the FP32 predictor velocities) or
+// mode 1 (dvec given); solution into phi with DIRECT's ghosts
+int refined_solve(eddy_ctx *ctx, int mode, double alfxdt, double *dvec, double *phi) {
+  MixedState *x = ms(ctx);
+  int sweeps = ctx->prm.refine_sweeps;
+  int rc;
+  EDDY_CUDA(cudaMemsetAsync(x->resid, 0, 4 * sizeof(double), ctx->stream));
+  if ((rc = fwd32(ctx, mode, alfxdt, nullptr, dvec, 0))) return rc;
+  if ((rc = solve32(ctx, phi, 0))) return rc;
+  for (int s = 0; s < sweeps; s++) {
+    if ((rc = fwd32(ctx, 2, alfxdt, phi, dvec, s))) return rc;
+    if ((rc = solve32(ctx, phi, 1))) return rc;
+  }
+  return launch_dp_ghost(ctx, phi);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+int mixed_create(eddy_ctx *ctx) {
+  const Dims &d = ctx->d;
+  if (ctx->prm.refine_sweeps < 1 || ctx->prm.refine_sweeps > 3) {
+    ctx->err = "refine_sweeps must be 1, 2 or 3 in the mixed form";
+    return EDDY_EINVAL;
+  }
+  MixedState *x = new (std::nothrow) MixedState();
+  if (!x) return EDDY_ENOMEM;
+  ctx->mixed = x;
+  x->px = (d.nx + 3) / 4 * 4;
+  x->n32 = (size_t)x->px * d.ny * d.nz;
+  float **fl[] = {&x->uo, &x->vo, &x->wo, &x->p, &x->tv, &x->kv, &x->us, &x->vs,
+                  &x->ws, &x->ua, &x->va, &x->wa, &x->dens, &x->dens_alt, &x->rha};
+  for (float **p : fl) {
+    EDDY_CUDA(cudaMalloc(p, sizeof(float) * x->n32));
+    EDDY_CUDA(cudaMemset(*p, 0, sizeof(float) * x->n32));
+  }
+  // metrics in FP32, one buffer
+  float **dst[] = {nullptr, nullptr, &x->m.ap, &x->m.au, &x->m.av, &x->m.aw, nullptr, nullptr,
+                   &x->m.bp, &x->m.bu, &x->m.bv, &x->m.bw, nullptr, nullptr, &x->m.cp, &x->m.cu,
+                   &x->m.cv, &x->m.cw, &x->m.whx, &x->m.why, &x->m.whz, &x->m.dfxu, &x->m.dfxw,
+                   &x->m.dfxul, &x->m.dfxwl, &x->m.dfxd, &x->m.dfxdl, &x->m.dens_bg};
+  size_t tot = 0;
+  for (int a = 0; a < 28; a++)
+    if (dst[a]) tot += (ctx->h[a].size() + 31) / 32 * 32;
+  std::vector<float> hb(tot, 0.f);
+  EDDY_CUDA(cudaMalloc(&x->mbuf, sizeof(float) * tot));
+  size_t off = 0;
+  for (int a = 0; a < 28; a++) {
+    if (!dst[a]) continue;
+    for (size_t e = 0; e < ctx->h[a].size(); e++) hb[off + e] = (float)ctx->h[a][e];
+    *dst[a] = x->mbuf + off;
+    off += (ctx->h[a].size() + 31) / 32 * 32;
+  }
+  EDDY_CUDA(cudaMemcpy(x->mbuf, hb.data(), sizeof(float) * tot, cudaMemcpyHostToDevice));
+  int L = ctx->pp.L;
+  std::vector<float> twr(L), twi(L);
+  for (int r = 0; r < L / 2; r++) {
+    double angf = -2.0 * M_PI * (double)r / (double)L, angb = 2.0 * M_PI * (double)r / (double)L;
+    twr[r] = (float)std::cos(angf);
+    twi[r] = (float)std::sin(angf);
+    twr[L / 2 + r] = (float)std::cos(angb);
+    twi[L / 2 + r] = (float)std::sin(angb);
+  }
+  EDDY_CUDA(cudaMalloc(&x->twr, sizeof(float) * L));
+  EDDY_CUDA(cudaMalloc(&x->twi, sizeof(float) * L));
+  EDDY_CUDA(cudaMemcpy(x->twr, twr.data(), sizeof(float) * L, cudaMemcpyHostToDevice));
+  EDDY_CUDA(cudaMemcpy(x->twi, twi.data(), sizeof(float) * L, cudaMemcpyHostToDevice));
+  EDDY_CUDA(cudaMalloc(&x->wout, sizeof(double) * (size_t)d.nx * d.ny));
+  EDDY_CUDA(cudaMemset(x->wout, 0, sizeof(double) * (size_t)d.nx * d.ny));
+  EDDY_CUDA(cudaMalloc(&x->resid, 4 * sizeof(double)));
+  EDDY_CUDA(cudaMemset(x->resid, 0, 4 * sizeof(double)));
+  // the refined solve keeps c' and the forward-eliminated right-hand side in FP64
+  EDDY_CUDA(cudaFree(ctx->pp.cprime));
+  ctx->pp.cprime = nullptr;
+  EDDY_CUDA(cudaMalloc(&ctx->pp.cprime, 2 * sizeof(double) * (size_t)ctx->pp.M * ctx->pp.L * ctx->pp.N));
+  size_t smem = sizeof(float) * 2 * L * TI32;
+  if (smem > 48 * 1024) {
+    EDDY_CUDA(cudaFuncSetAttribute(k_fwd32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EDDY_CUDA(cudaFuncSetAttribute(k_bwd32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  EDDY_CUDA(cudaFuncSetAttribute(k_rhs32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ring_smem_bytes<NFLD, TX, TY, float>()));
+  EDDY_CUDA(cudaFuncSetAttribute(k_density32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ring_smem_bytes<DNF, DTX, DTY, float>()));
+  return EDDY_OK;
+}
+
+void mixed_release(eddy_ctx *ctx) {
+  MixedState *x = ms(ctx);
+  if (!x) return;
+  float *fl[] = {x->uo, x->vo, x->wo, x->p, x->tv, x->kv, x->us, x->vs,
+                 x->ws, x->ua, x->va, x->wa, x->dens, x->dens_alt, x->rha, x->mbuf, x->twr, x->twi};
+  for (float *p : fl) if (p) cudaFree(p);
+  if (x->resid) cudaFree(x->resid);
+  if (x->wout) cudaFree(x->wout);
+  delete x;
+  ctx->mixed = nullptr;
+}
+
+// FP32 array that mirrors (or, for the FP32-master fields, holds) `field`
+static float *mirror(MixedState *x, int field) {
+  switch (field) {
+    case EDDY_UO: return x->uo;
+    case EDDY_VO: return x->vo;
+    case EDDY_WO: return x->wo;
+    case EDDY_P: return x->p;
+    case EDDY_TV: return x->tv;
+    case EDDY_DENS: return x->dens;
+    case EDDY_US: return x->us;
+    case EDDY_VS: return x->vs;
+    case EDDY_WS: return x->ws;
+    case EDDY_UA: return x->ua;
+    case EDDY_VA: return x->va;
+    case EDDY_WA: return x->wa;
+    case EDDY_RHA: return x->rha;
+    default: return nullptr;
+  }
+}
+
+int mixed_from64(eddy_ctx *ctx, int field) {
+  MixedState *x = ms(ctx);
+  if (!x) return EDDY_OK;
+  float *b = mirror(x, field);
+  if (!b) return EDDY_OK;
+  int rc = to32(ctx, ctx->f[field], b);
+  if (rc) return rc;
+  if (field == EDDY_DENS) return to32(ctx, ctx->f[field], x->dens_alt);
+  if (field == EDDY_TV) return to32(ctx, ctx->f[field], x->kv);
+  return EDDY_OK;
+}
+
+int mixed_to64(eddy_ctx *ctx, int field) {
+  MixedState *x = ms(ctx);
+  if (!x) return EDDY_OK;
+  switch (field) {
+    case EDDY_DENS: case EDDY_US: case EDDY_VS: case EDDY_WS:
+    case EDDY_UA: case EDDY_VA: case EDDY_WA: case EDDY_RHA:
+      return to64(ctx, mirror(x, field), ctx->f[field]);
+    default:
+      return EDDY_OK;
+  }
+}
+
+// after the eddy viscosity (dynamic model or learned closure) is updated in
+// FP64: FP32 copies for the stencils
+int mixed_after_sgs(eddy_ctx *ctx) {
+  MixedState *x = ms(ctx);
+  ProfScope ps(ctx, PROF_CONVERT);
+  int rc = to32(ctx, ctx->f[EDDY_TV], x->tv);
+  if (rc) return rc;
+  return to32(ctx, ctx->prm.closure == 1 ? ctx->kappa : ctx->f[EDDY_TV], x->kv);
+}
+
+// before the eddy viscosity: the FP64 density the closure features read
+int mixed_before_sgs(eddy_ctx *ctx) {
+  if (ctx->prm.closure != 1 || ctx->prm.idens != 1) return EDDY_OK;
+  ProfScope ps(ctx, PROF_CONVERT);
+  return to64(ctx, ms(ctx)->dens, ctx->f[EDDY_DENS]);
+}
+
+// BOUNDINOUT predictor (src/boundary.f:694-944) on the FP32 u*: inlet plane,
+// convective 730 outlet, then the outlet mass balance in FP64 on the outlet
+// plane (inflow flux from the FP64 inlet plane)
+static int boundinout_pred(eddy_ctx *ctx, double alfxdt) {
+  MixedState *x = ms(ctx);
+  const Dims &d = ctx->d;
+  const int px = x->px;
+  cudaStream_t st = ctx->stream;
+  double *fin = ctx->scal + 8, *fout = ctx->scal + 10;
+  int n2 = d.nx * d.ny, nin = (d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1);
+  bct::k_inlet_plane<float><<<nblk(n2), 256, 0, st>>>(d, px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEU],
+                                                      ctx->f[EDDY_PLANEV], ctx->f[EDDY_PLANEW]);
+  EDDY_LAUNCHED(ctx);
+  bct::k_plane_flux<double><<<1, 1024, 0, st>>>(d, d.nx, ctx->m, ctx->f[EDDY_PLANEW], 1, fin);
+  EDDY_LAUNCHED(ctx);
+  bct::k_outlet_convective<float, float><<<nblk(nin), 256, 0, st>>>(d, px, ctx->m, x->us, x->vs, x->ws, x->uo, x->vo,
+                                                                    x->wo, fin, alfxdt);
+  EDDY_LAUNCHED(ctx);
+  bct::k_yper3<float><<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, px, x->us, x->vs, x->ws);
+  EDDY_LAUNCHED(ctx);
+  k_plane_from32<<<nblk(n2), 256, 0, st>>>(d, px, x->ws, d.kz2, x->wout);
+  EDDY_LAUNCHED(ctx);
+  bct::k_plane_flux<double><<<1, 1024, 0, st>>>(d, d.nx, ctx->m, x->wout, 1, fout);
+  EDDY_LAUNCHED(ctx);
+  k_rescale_plane<<<nblk(nin), 256, 0, st>>>(d, px, x->wout, x->ws, fin, fout);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
+  MixedState *x = ms(ctx);
+  const Dims &d = ctx->d;
+  const int px = x->px;
+  double **f = ctx->f;
+  int rc;
+  {
+    ProfScope ps(ctx, PROF_RHS_PRED);
+    TmaMaps<NFLD> maps;
+    const float *src[NFLD] = {x->uo, x->vo, x->wo, x->tv, x->p, x->dens, x->ua, x->va, x->wa};
+    for (int q = 0; q < NFLD; q++) {
+      const CUtensorMap *mp = tmap32(ctx, src[q], RingGeom<TX, TY, float>::PX, TY + 2);
+      if (!mp) return EDDY_ECUDA;
+      maps.m[q] = *mp;
+    }
+    dim3 g((d.ix2 - d.ix1 + TX) / TX, (d.jy2 - d.jy1 + TY) / TY, (d.kz2 - d.kz1 + KCHUNK) / KCHUNK);
+    k_rhs32<<<g, dim3(TX, TY), ring_smem_bytes<NFLD, TX, TY, float>(), ctx->stream>>>(
+        d, x->m, ctx->sc, px, maps, x->us, x->vs, x->ws, x->ua, x->va, x->wa, (float)alfxdt, (float)gamxdt,
+        (float)rhoxdt, ctx->err_flag);
+    EDDY_LAUNCHED(ctx);
+    long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
+    k_zero_faces32<<<nblk(ng), 256, 0, ctx->stream>>>(d, px, x->us, x->vs, x->ws);
+    EDDY_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, PROF_BC);
+    if ((rc = bc_boundary<float>(ctx, px, x->us, x->vs, x->ws))) return rc;
+    if ((rc = boundinout_pred(ctx, alfxdt))) return rc;
+    if ((rc = bc_boundary<float>(ctx, px, x->us, x->vs, x->ws))) return rc;
+  }
+  // FP64 divergence right-hand side kept in the (unused in this form) FP64 u* array
+  if ((rc = refined_solve(ctx, 0, alfxdt, f[EDDY_US], f[EDDY_DP]))) return rc;
+  {
+    ProfScope ps(ctx, PROF_CORRECT);
+    dim3 g((d.nx + BX - 1) / BX, (d.ny + BY - 1) / BY, (d.nz + BZ - 1) / BZ);
+    k_correct_mixed<<<g, dim3(BX, BY, BZ), 0, ctx->stream>>>(d, ctx->m, px, x->us, x->vs, x->ws, f[EDDY_DP],
+                                                             f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], x->uo, x->vo, x->wo,
+                                                             alfxdt);
+    EDDY_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, PROF_BC);
+    if ((rc = bc_boundary<double>(ctx, d.nx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO]))) return rc;
+    if ((rc = bc_boundinout<double, float>(ctx, d.nx, px, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], x->us, x->vs, x->ws,
+                                           alfxdt, 0)))
+      return rc;
+    k_plane_to64<<<nblk((long long)d.nx * d.ny), 256, 0, ctx->stream>>>(d, x->wout, f[EDDY_WO], d.kz2);
+    EDDY_LAUNCHED(ctx);
+    if ((rc = bc_boundary<double>(ctx, d.nx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO]))) return rc;
+    long long np = 3LL * d.ny * d.nz + 2LL * d.nx * d.nz + 3LL * d.nx * d.ny;
+    k_sync_planes<<<nblk(np), 256, 0, ctx->stream>>>(d, px, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], x->uo, x->vo, x->wo);
+    EDDY_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, PROF_PUPDATE);
+    k_pref_m<<<1, 1, 0, ctx->stream>>>(d, f[EDDY_P], f[EDDY_DP], ctx->scal);
+    EDDY_LAUNCHED(ctx);
+    k_pupdate_m<<<nblk(d.ncell), 256, 0, ctx->stream>>>(d, px, f[EDDY_P], f[EDDY_DP], ctx->scal, x->p);
+    EDDY_LAUNCHED(ctx);
+    long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
+    k_pghost_m<<<nblk(ng), 256, 0, ctx->stream>>>(d, px, f[EDDY_P], x->p);
+    EDDY_LAUNCHED(ctx);
+  }
+  if (ctx->prm.idens == 1) {
+    ProfScope ps(ctx, PROF_DENSITY);
+    if ((rc = bc_boundinoutd_dens<float>(ctx, px, x->dens))) return rc;
+    TmaMaps<DNF> maps;
+    const float *src[DNF] = {x->dens, x->kv, x->uo, x->vo, x->wo, x->rha};
+    for (int q = 0; q < DNF; q++) {
+      const CUtensorMap *mp = tmap32(ctx, src[q], RingGeom<DTX, DTY, float>::PX, DTY + 2);
+      if (!mp) return EDDY_ECUDA;
+      maps.m[q] = *mp;
+    }
+    dim3 g((d.ix2 - d.ix1 + DTX) / DTX, (d.jy2 - d.jy1 + DTY) / DTY, (d.kz2 - d.kz1 + DKC) / DKC);
+    k_density32<<<g, dim3(DTX, DTY), ring_smem_bytes<DNF, DTX, DTY, float>(), ctx->stream>>>(
+        d, x->m, ctx->sc, px, maps, x->rha, x->dens_alt, (float)(ctx->sc.ru1 / ctx->sc.prn), (float)alfxdt,
+        (float)gamxdt, (float)rhoxdt, ctx->err_flag);
+    EDDY_LAUNCHED(ctx);
+    long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
+    k_dens_ghost32<<<nblk(ng), 256, 0, ctx->stream>>>(d, px, x->dens, x->dens_alt);
+    EDDY_LAUNCHED(ctx);
+    float *t = x->dens;
+    x->dens = x->dens_alt;
+    x->dens_alt = t;
+    if ((rc = bc_boundinoutd_dens<float>(ctx, px, x->dens))) return rc;
+  }
+  return EDDY_OK;
+}
+
+int mixed_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp) {
+  // mode 1 reads the right-hand side from dvec; refinement reads it again
+  return refined_solve(ctx, 1, 1.0, const_cast<double *>(rhs), dp);
+}
+
+int mixed_residuals(eddy_ctx *ctx, double *out, int n) {
+  MixedState *x = ms(ctx);
+  if (!x || n < 1) return EDDY_EINVAL;
+  double h[4];
+  EDDY_CUDA(cudaMemcpyAsync(h, x->resid, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int s = 0; s < n && s < 4; s++) out[s] = h[s];
+  return EDDY_OK;
+}

@@ -6,6 +6,7 @@
 // (non Crank-Nicolson) branch of the Cartesian equations.
 #include "eddy_internal.h"
 #include "tma_ring.cuh"
+#include "bc_templates.cuh"
 
 #define A(a, i, j, k) (a)[fidx(d, (i), (j), (k))]
 
@@ -13,152 +14,7 @@ namespace {
 
 constexpr int BX = 32, BY = 4, BZ = 2;
 
-// ---------------------------------------------------------------------------
-// u-momentum explicit RHS at a u point (src/rhs.f:77-172)
-template <class Acc>
-__device__ __forceinline__ double rhs_u(const Acc &S, const DevMetrics &m, double ru1, int i, int j, int k) {
-  double qxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * 0.5;
-  double qxm = (S.u(0, 0, 0) + S.u(-1, 0, 0)) * 0.5;
-  double uxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * 0.5;
-  double uxm = (S.u(0, 0, 0) + S.u(-1, 0, 0)) * 0.5;
-  double uyp = (S.u(0, 1, 0) + S.u(0, 0, 0)) * 0.5;
-  double uym = (S.u(0, 0, 0) + S.u(0, -1, 0)) * 0.5;
-  double uzp = (S.u(0, 0, 1) + S.u(0, 0, 0)) * 0.5;
-  double uzm = (S.u(0, 0, 0) + S.u(0, 0, -1)) * 0.5;
-  double vxp = (S.v(1, 0, 0) + S.v(0, 0, 0)) * 0.5;
-  double vxm = (S.v(1, -1, 0) + S.v(0, -1, 0)) * 0.5;
-  double wxp = (S.w(1, 0, 0) + S.w(0, 0, 0)) * 0.5;
-  double wxm = (S.w(1, 0, -1) + S.w(0, 0, -1)) * 0.5;
-  double dqdxp = m.ap[i + 1] * (S.u(1, 0, 0) - S.u(0, 0, 0));
-  double dqdxm = m.ap[i] * (S.u(0, 0, 0) - S.u(-1, 0, 0));
-  double dudyp = m.bv[j] * (S.u(0, 1, 0) - S.u(0, 0, 0));
-  double dudym = m.bv[j - 1] * (S.u(0, 0, 0) - S.u(0, -1, 0));
-  double dudzp = m.cw[k] * (S.u(0, 0, 1) - S.u(0, 0, 0));
-  double dudzm = m.cw[k - 1] * (S.u(0, 0, 0) - S.u(0, 0, -1));
-  double dvdxp = m.au[i] * (S.v(1, 0, 0) - S.v(0, 0, 0));
-  double dvdxm = m.au[i] * (S.v(1, -1, 0) - S.v(0, -1, 0));
-  double dwdxp = m.au[i] * (S.w(1, 0, 0) - S.w(0, 0, 0));
-  double dwdxm = m.au[i] * (S.w(1, 0, -1) - S.w(0, 0, -1));
-  double tvjp = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, 1, 0) + S.t(0, 1, 0));
-  double tvjm = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, -1, 0) + S.t(0, -1, 0));
-  double tvkp = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, 0, 1) + S.t(0, 0, 1));
-  double tvkm = 0.25 * (S.t(1, 0, 0) + S.t(0, 0, 0) + S.t(1, 0, -1) + S.t(0, 0, -1));
-  double txxp = (ru1 + 2. * S.t(1, 0, 0)) * dqdxp;
-  double txxm = (ru1 + 2. * S.t(0, 0, 0)) * dqdxm;
-  double tyyp = (ru1 + tvjp) * dudyp;
-  double tyym = (ru1 + tvjm) * dudym;
-  double tzzp = (ru1 + tvkp) * dudzp;
-  double tzzm = (ru1 + tvkm) * dudzm;
-  double txyp = tvjp * dvdxp;
-  double txym = tvjm * dvdxm;
-  double txzp = tvkp * dwdxp;
-  double txzm = tvkm * dwdxm;
-  double h11 = -m.au[i] * (qxp * uxp - qxm * uxm);
-  double h22 = -m.bu[j] * (vxp * uyp - vxm * uym);
-  double h33 = -m.cu[k] * (wxp * uzp - wxm * uzm);
-  double t11 = m.au[i] * (txxp - txxm);
-  double t22 = m.bu[j] * (tyyp - tyym);
-  double t33 = m.cu[k] * (tzzp - tzzm);
-  double s22 = m.bu[j] * (txyp - txym);
-  double s33 = m.cu[k] * (txzp - txzm);
-  return h11 + h22 + h33 + t11 + t22 + t33 + s22 + s33;
-}
-
-// v-momentum (src/rhs.f:219-321)
-template <class Acc>
-__device__ __forceinline__ double rhs_v(const Acc &S, const DevMetrics &m, double ru1, int i, int j, int k) {
-  double vxp = (S.v(1, 0, 0) + S.v(0, 0, 0)) * 0.5;
-  double vxm = (S.v(0, 0, 0) + S.v(-1, 0, 0)) * 0.5;
-  double vyp = (S.v(0, 1, 0) + S.v(0, 0, 0)) * 0.5;
-  double vym = (S.v(0, 0, 0) + S.v(0, -1, 0)) * 0.5;
-  double vzp = (S.v(0, 0, 1) + S.v(0, 0, 0)) * 0.5;
-  double vzm = (S.v(0, 0, 0) + S.v(0, 0, -1)) * 0.5;
-  double qyp = (S.u(0, 1, 0) + S.u(0, 0, 0)) * 0.5;
-  double qym = (S.u(-1, 1, 0) + S.u(-1, 0, 0)) * 0.5;
-  double wyp = (S.w(0, 1, 0) + S.w(0, 0, 0)) * 0.5;
-  double wym = (S.w(0, 1, -1) + S.w(0, 0, -1)) * 0.5;
-  double dvdxp = m.au[i] * (S.v(1, 0, 0) - S.v(0, 0, 0));
-  double dvdxm = m.au[i - 1] * (S.v(0, 0, 0) - S.v(-1, 0, 0));
-  double dvdyp = m.bp[j + 1] * (S.v(0, 1, 0) - S.v(0, 0, 0));
-  double dvdym = m.bp[j] * (S.v(0, 0, 0) - S.v(0, -1, 0));
-  double dvdzp = m.cw[k] * (S.v(0, 0, 1) - S.v(0, 0, 0));
-  double dvdzm = m.cw[k - 1] * (S.v(0, 0, 0) - S.v(0, 0, -1));
-  double dudyp = m.bv[j] * (S.u(0, 1, 0) - S.u(0, 0, 0));
-  double dudym = m.bv[j] * (S.u(-1, 1, 0) - S.u(-1, 0, 0));
-  double dwdyp = m.bv[j] * (S.w(0, 1, 0) - S.w(0, 0, 0));
-  double dwdym = m.bv[j] * (S.w(0, 1, -1) - S.w(0, 0, -1));
-  double tvip = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(1, 1, 0) + S.t(1, 0, 0));
-  double tvim = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(-1, 1, 0) + S.t(-1, 0, 0));
-  double tvkp = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(0, 1, 1) + S.t(0, 0, 1));
-  double tvkm = 0.25 * (S.t(0, 1, 0) + S.t(0, 0, 0) + S.t(0, 1, -1) + S.t(0, 0, -1));
-  double txxp = (ru1 + tvip) * dvdxp;
-  double txxm = (ru1 + tvim) * dvdxm;
-  double tyyp = (ru1 + 2. * S.t(0, 1, 0)) * dvdyp;
-  double tyym = (ru1 + 2. * S.t(0, 0, 0)) * dvdym;
-  double tzzp = (ru1 + tvkp) * dvdzp;
-  double tzzm = (ru1 + tvkm) * dvdzm;
-  double txyp = tvip * dudyp;
-  double txym = tvim * dudym;
-  double tyzp = tvkp * dwdyp;
-  double tyzm = tvkm * dwdym;
-  double h11 = -m.av[i] * (qyp * vxp - qym * vxm);
-  double h22 = -m.bv[j] * (vyp * vyp - vym * vym);
-  double h33 = -m.cv[k] * (wyp * vzp - wym * vzm);
-  double t11 = m.av[i] * (txxp - txxm);
-  double t22 = m.bv[j] * (tyyp - tyym);
-  double t33 = m.cv[k] * (tzzp - tzzm);
-  double s11 = m.av[i] * (txyp - txym);
-  double s33 = m.cv[k] * (tyzp - tyzm);
-  return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s33;
-}
-
-// w-momentum (src/rhs.f:347-422)
-template <class Acc>
-__device__ __forceinline__ double rhs_w(const Acc &S, const DevMetrics &m, double ru1, int i, int j, int k) {
-  double wxp = (S.w(1, 0, 0) + S.w(0, 0, 0)) * 0.5;
-  double wxm = (S.w(0, 0, 0) + S.w(-1, 0, 0)) * 0.5;
-  double wyp = (S.w(0, 1, 0) + S.w(0, 0, 0)) * 0.5;
-  double wym = (S.w(0, 0, 0) + S.w(0, -1, 0)) * 0.5;
-  double wzp = (S.w(0, 0, 1) + S.w(0, 0, 0)) * 0.5;
-  double wzm = (S.w(0, 0, 0) + S.w(0, 0, -1)) * 0.5;
-  double qzp = (S.u(0, 0, 1) + S.u(0, 0, 0)) * 0.5;
-  double qzm = (S.u(-1, 0, 1) + S.u(-1, 0, 0)) * 0.5;
-  double vzp = (S.v(0, 0, 1) + S.v(0, 0, 0)) * 0.5;
-  double vzm = (S.v(0, -1, 1) + S.v(0, -1, 0)) * 0.5;
-  double dwdxp = m.au[i] * (S.w(1, 0, 0) - S.w(0, 0, 0));
-  double dwdxm = m.au[i - 1] * (S.w(0, 0, 0) - S.w(-1, 0, 0));
-  double dwdyp = m.bv[j] * (S.w(0, 1, 0) - S.w(0, 0, 0));
-  double dwdym = m.bv[j - 1] * (S.w(0, 0, 0) - S.w(0, -1, 0));
-  double dwdzp = m.cp[k + 1] * (S.w(0, 0, 1) - S.w(0, 0, 0));
-  double dwdzm = m.cp[k] * (S.w(0, 0, 0) - S.w(0, 0, -1));
-  double dudzp = m.cw[k] * (S.u(0, 0, 1) - S.u(0, 0, 0));
-  double dudzm = m.cw[k] * (S.u(-1, 0, 1) - S.u(-1, 0, 0));
-  double dvdzp = m.cw[k] * (S.v(0, 0, 1) - S.v(0, 0, 0));
-  double dvdzm = m.cw[k] * (S.v(0, -1, 1) - S.v(0, -1, 0));
-  double tvip = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(1, 0, 1) + S.t(1, 0, 0));
-  double tvim = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(-1, 0, 1) + S.t(-1, 0, 0));
-  double tvjp = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(0, 1, 1) + S.t(0, 1, 0));
-  double tvjm = 0.25 * (S.t(0, 0, 1) + S.t(0, 0, 0) + S.t(0, -1, 1) + S.t(0, -1, 0));
-  double txxp = (ru1 + tvip) * dwdxp;
-  double txxm = (ru1 + tvim) * dwdxm;
-  double tyyp = (ru1 + tvjp) * dwdyp;
-  double tyym = (ru1 + tvjm) * dwdym;
-  double tzzp = (ru1 + 2. * S.t(0, 0, 1)) * dwdzp;
-  double tzzm = (ru1 + 2. * S.t(0, 0, 0)) * dwdzm;
-  double txzp = tvip * dudzp;
-  double txzm = tvim * dudzm;
-  double tyzp = tvjp * dvdzp;
-  double tyzm = tvjm * dvdzm;
-  double h11 = -m.aw[i] * (qzp * wxp - qzm * wxm);
-  double h22 = -m.bw[j] * (vzp * wyp - vzm * wym);
-  double h33 = -m.cw[k] * (wzp * wzp - wzm * wzm);
-  double t11 = m.aw[i] * (txxp - txxm);
-  double t22 = m.bw[j] * (tyyp - tyym);
-  double t33 = m.cw[k] * (tzzp - tzzm);
-  double s11 = m.aw[i] * (txzp - txzm);
-  double s22 = m.bw[j] * (tyzp - tyzm);
-  return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s22;
-}
+#include "stencil_rhs.cuh"
 
 // RHS + PREDICTORD + sponges (src/rhs.f:4-438, src/timeindeg.f:1041-1265).
 // A block owns a 32x8 tile of (i,j) columns and marches along k over a chunk
@@ -191,7 +47,7 @@ __global__ void __launch_bounds__(TX *TY)
         // ---- u ----
         double uval = 0.0;
         if (kin && jin && i >= d.ibu && i <= d.ieu) {
-          double ur = rhs_u(S, m, s.ru1, i, j, k);
+          double ur = rhs_u<double>(S, m, s.ru1, i, j, k);
           double ustar = R.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * R.at(6, 0, 0, 0) -
                          alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdx;
           if (s.idens == 1)
@@ -207,7 +63,7 @@ __global__ void __launch_bounds__(TX *TY)
         // ---- v ----
         double vval = 0.0;
         if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
-          double vr = rhs_v(S, m, s.ru1, i, j, k);
+          double vr = rhs_v<double>(S, m, s.ru1, i, j, k);
           double vstar = R.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * R.at(7, 0, 0, 0) -
                          alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdy;
           va[q] = vr;
@@ -220,7 +76,7 @@ __global__ void __launch_bounds__(TX *TY)
         // ---- w ----
         double wval = 0.0;
         if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
-          double wr = rhs_w(S, m, s.ru1, i, j, k);
+          double wr = rhs_w<double>(S, m, s.ru1, i, j, k);
           double wstar = R.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * R.at(8, 0, 0, 0) -
                          alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdz;
           wa[q] = wr;
@@ -253,123 +109,6 @@ __global__ void k_zero_faces3(Dims d, double *a, double *b, double *c3) {
   a[q] = 0.;
   b[q] = 0.;
   c3[q] = 0.;
-}
-
-// ---------------------------------------------------------------------------
-// plane fill a(dst) = sgn*a(src) (or 0) over a whole plane of one axis.
-__global__ void k_fill_plane(Dims d, double *a, int axis, int dst, int src, double sgn, int zero) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int n1 = axis == 0 ? d.ny : d.nx;
-  int n2 = axis == 2 ? d.ny : d.nz;
-  if (t >= n1 * n2) return;
-  int a1 = 1 + t % n1, a2 = 1 + t / n1;
-  long long qd, qs;
-  if (axis == 0) { qd = fidx(d, dst, a1, a2); qs = fidx(d, src, a1, a2); }
-  else if (axis == 1) { qd = fidx(d, a1, dst, a2); qs = fidx(d, a1, src, a2); }
-  else { qd = fidx(d, a1, a2, dst); qs = fidx(d, a1, a2, src); }
-  a[qd] = zero ? 0. : sgn * a[qs];
-}
-
-// deterministic single-block sum over the interior (i,j) of plane k of
-// a(i,j,k)/(ap(i)bp(j)) (flux through a z plane, src/boundary.f:787-795)
-__global__ void k_plane_flux(Dims d, DevMetrics m, const double *a, int k, double *out) {
-  __shared__ double sf[1024], sa[1024];
-  int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
-  double f = 0., ar = 0.;
-  for (int t = threadIdx.x; t < mi * mj; t += blockDim.x) {
-    int i = d.ix1 + t % mi, j = d.jy1 + t / mi;
-    double areaij = 1.0 / (m.ap[i] * m.bp[j]);
-    f = f + a[fidx(d, i, j, k)] * areaij;
-    ar = ar + areaij;
-  }
-  sf[threadIdx.x] = f;
-  sa[threadIdx.x] = ar;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) {
-      sf[threadIdx.x] += sf[threadIdx.x + w];
-      sa[threadIdx.x] += sa[threadIdx.x + w];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    out[0] = sf[0];
-    out[1] = sa[0];
-  }
-}
-
-__global__ void k_inlet_plane(Dims d, double *ubc, double *vbc, double *wbc, const double *pu,
-                              const double *pv, const double *pw) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.nx * d.ny) return;
-  long long q = (long long)t;  // k = 1 plane
-  ubc[q] = pu[t];
-  vbc[q] = pv[t];
-  wbc[q] = pw[t];
-}
-
-// 730 convective outflow, predictor (src/boundary.f:853-870); flux[0..1] inlet
-__global__ void k_outlet_convective(Dims d, DevMetrics m, double *ubc, double *vbc, double *wbc,
-                                    const double *uof, const double *vof, const double *wof,
-                                    const double *flux_in, double alfxdt) {
-  int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= mi * mj) return;
-  int i = d.ix1 + t % mi, j = d.jy1 + t / mi;
-  double qin2 = flux_in[0] / flux_in[1];
-  double coef = qin2 * alfxdt * m.cp[d.kz2];
-  int NZ = d.nz, kz2 = d.kz2;
-  long long qn = fidx(d, i, j, NZ), qk = fidx(d, i, j, kz2), qkm = fidx(d, i, j, kz2 - 1);
-  ubc[qn] = uof[qn] - coef * (uof[qn] - uof[qk]);
-  vbc[qn] = vof[qn] - coef * (vof[qn] - vof[qk]);
-  wbc[qk] = wof[qk] - coef * (wof[qk] - wof[qkm]);
-}
-
-// y periodic ghost rows of three arrays over all i,k (src/boundary.f:862-867)
-__global__ void k_yper3(Dims d, double *a, double *b, double *c) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.nx * d.nz) return;
-  int i = 1 + t % d.nx, k = 1 + t / d.nx;
-  double *arr[3] = {a, b, c};
-  for (int s = 0; s < 3; s++) {
-    double *x = arr[s];
-    x[fidx(d, i, 1, k)] = x[fidx(d, i, d.ny - 1, k)];
-    x[fidx(d, i, d.ny, k)] = x[fidx(d, i, 2, k)];
-  }
-}
-
-// outflow mass balance (src/boundary.f:920-944)
-__global__ void k_outlet_rescale(Dims d, double *wbc, const double *flux_in, const double *flux_out) {
-  int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= mi * mj) return;
-  int i = d.ix1 + t % mi, j = d.jy1 + t / mi;
-  long long q = fidx(d, i, j, d.kz2);
-  double qin1 = flux_in[0], qout = flux_out[0];
-  if (qout != 0.) {
-    double c = qin1 / qout;
-    wbc[q] = wbc[q] * c;
-  } else {
-    wbc[q] = qin1 / flux_out[1];
-  }
-}
-
-// corrector 730/731 and 710 copies (src/boundary.f:947-980)
-__global__ void k_outlet_corrector(Dims d, double *ubc, double *vbc, double *wbc, const double *uof,
-                                   const double *vof, const double *wof, int t6) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.nx * d.ny) return;
-  int i = 1 + t % d.nx, j = 1 + t / d.nx;
-  long long qn = fidx(d, i, j, d.nz), qk = fidx(d, i, j, d.kz2);
-  if (t6 == 730 || t6 == 731) {
-    ubc[qn] = uof[qn];
-    vbc[qn] = vof[qn];
-    wbc[qk] = wof[qk];
-  } else if (t6 == 710) {
-    ubc[qn] = uof[qk];
-    vbc[qn] = vof[qk];
-    wbc[qk] = wof[qk];
-  }
 }
 
 // CORRECT (src/timeindeg.f:981-1028)
@@ -454,18 +193,10 @@ inline dim3 grid3(const Dims &d) {
   return dim3((d.nx + BX - 1) / BX, (d.ny + BY - 1) / BY, (d.nz + BZ - 1) / BZ);
 }
 
-int fill(eddy_ctx *ctx, double *a, int axis, int dst, int src, double sgn, int zero) {
-  const Dims &d = ctx->d;
-  int n = axis == 0 ? d.ny * d.nz : (axis == 1 ? d.nx * d.nz : d.nx * d.ny);
-  k_fill_plane<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d, a, axis, dst, src, sgn, zero);
-  EDDY_LAUNCHED(ctx);
-  return EDDY_OK;
-}
-
 }  // namespace
 
 int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, double sgn, int zero) {
-  return fill(ctx, a, axis, dst, src, sgn, zero);
+  return bc_fill<double>(ctx, ctx->d.nx, a, axis, dst, src, sgn, zero);
 }
 
 int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
@@ -475,7 +206,7 @@ int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rh
   const double *src[NFLD] = {f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_TV], f[EDDY_P], f[EDDY_DENS],
                              f[EDDY_UA], f[EDDY_VA], f[EDDY_WA]};
   for (int q = 0; q < NFLD; q++) {
-    const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], TX + 2, TY + 2);
+    const CUtensorMap *mp = ctx_tensor_map(ctx, src[q], RingGeom<TX, TY>::PX, TY + 2);
     if (!mp) return EDDY_ECUDA;
     maps.m[q] = *mp;
   }
@@ -493,87 +224,15 @@ int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rh
   return EDDY_OK;
 }
 
-// BOUNDARY (src/boundary.f:7-66): wall types first, then periodic x/y.
+// BOUNDARY (src/boundary.f:7-66)
 int launch_boundary(eddy_ctx *ctx, double *u, double *v, double *w) {
-  const Dims &d = ctx->d;
-  int rc;
-#define F(...) \
-  if ((rc = fill(ctx, __VA_ARGS__)) != EDDY_OK) return rc
-  for (int ib = 1; ib <= 6; ib++) {
-    int t = d.itype[ib];
-    if (t == 50 || t == 60) {
-      double sg = (t == 50) ? -1. : 1.;
-      switch (ib) {
-        case 1: F(u, 0, 1, 0, 0., 1); F(v, 0, 1, d.ix1, sg, 0); F(w, 0, 1, d.ix1, sg, 0); break;
-        case 2: F(u, 0, d.ix2, 0, 0., 1); F(v, 0, d.nx, d.ix2, sg, 0); F(w, 0, d.nx, d.ix2, sg, 0); break;
-        case 3: F(u, 1, 1, d.jy1, sg, 0); F(v, 1, 1, 0, 0., 1); F(w, 1, 1, d.jy1, sg, 0); break;
-        case 4: F(u, 1, d.ny, d.jy2, sg, 0); F(v, 1, d.jy2, 0, 0., 1); F(w, 1, d.ny, d.jy2, sg, 0); break;
-        case 5: F(u, 2, 1, d.kz1, sg, 0); F(v, 2, 1, d.kz1, sg, 0); F(w, 2, 1, 0, 0., 1); break;
-        case 6: F(u, 2, d.nz, d.kz2, sg, 0); F(v, 2, d.nz, d.kz2, sg, 0); F(w, 2, d.kz2, 0, 0., 1); break;
-      }
-    } else if (t == 82) {
-      if (ib == 1) { F(u, 0, 1, d.ix1, 1., 0); F(v, 0, 1, d.ix1, -1., 0); F(w, 0, 1, d.ix1, -1., 0); }
-      if (ib == 2) { F(u, 0, d.nx, d.ix2, 1., 0); F(v, 0, d.nx, d.ix2, 1., 0); F(w, 0, d.nx, d.ix2, 1., 0); }
-    }
-  }
-  if (d.itype[1] == 500) {
-    F(u, 0, 1, d.ix2, 1., 0); F(v, 0, 1, d.ix2, 1., 0); F(w, 0, 1, d.ix2, 1., 0);
-    F(u, 0, d.nx, d.ix1, 1., 0); F(v, 0, d.nx, d.ix1, 1., 0); F(w, 0, d.nx, d.ix1, 1., 0);
-  }
-  if (d.itype[3] == 500) {
-    F(u, 1, 1, d.jy2, 1., 0); F(v, 1, 1, d.jy2, 1., 0); F(w, 1, 1, d.jy2, 1., 0);
-    F(u, 1, d.ny, d.jy1, 1., 0); F(v, 1, d.ny, d.jy1, 1., 0); F(w, 1, d.ny, d.jy1, 1., 0);
-  }
-#undef F
-  return EDDY_OK;
+  return bc_boundary<double>(ctx, ctx->d.nx, u, v, w);
 }
 
-// BOUNDINOUT (src/boundary.f:505-994) for inlet 305 and outlets 710/720/730.
+// BOUNDINOUT (src/boundary.f:505-994)
 int launch_boundinout(eddy_ctx *ctx, double *ubc, double *vbc, double *wbc, const double *uof,
                       const double *vof, const double *wof, double alfxdt, int idiv) {
-  const Dims &d = ctx->d;
-  cudaStream_t st = ctx->stream;
-  double *fin = ctx->scal + 8, *fout = ctx->scal + 10;
-  int n2 = d.nx * d.ny, nin = (d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1);
-  int iinq = idiv;
-  if (d.itype[5] == 305) {
-    k_inlet_plane<<<(n2 + 255) / 256, 256, 0, st>>>(d, ubc, vbc, wbc, ctx->f[EDDY_PLANEU],
-                                                    ctx->f[EDDY_PLANEV], ctx->f[EDDY_PLANEW]);
-    EDDY_LAUNCHED(ctx);
-  } else {
-    iinq = 0;
-  }
-  int t6 = d.itype[6];
-  if (idiv == 1) {
-    if (t6 == 710 || t6 == 720) {
-      ctx->err = "outlet types 710/720 are not on the restated hot path";
-      return EDDY_EINVAL;
-    }
-    if (t6 != 730) return EDDY_OK;
-    if (iinq != 1) {
-      ctx->err = "convective outlet needs the 305 inlet flux";
-      return EDDY_EINVAL;
-    }
-    k_plane_flux<<<1, 1024, 0, st>>>(d, ctx->m, wbc, 1, fin);
-    EDDY_LAUNCHED(ctx);
-    k_outlet_convective<<<(nin + 255) / 256, 256, 0, st>>>(d, ctx->m, ubc, vbc, wbc, uof, vof, wof, fin,
-                                                           alfxdt);
-    EDDY_LAUNCHED(ctx);
-    k_yper3<<<(d.nx * d.nz + 255) / 256, 256, 0, st>>>(d, ubc, vbc, wbc);
-    EDDY_LAUNCHED(ctx);
-    k_plane_flux<<<1, 1024, 0, st>>>(d, ctx->m, wbc, d.kz2, fout);
-    EDDY_LAUNCHED(ctx);
-    k_outlet_rescale<<<(nin + 255) / 256, 256, 0, st>>>(d, wbc, fin, fout);
-    EDDY_LAUNCHED(ctx);
-  } else {
-    if (t6 == 720) {
-      ctx->err = "outlet type 720 is not on the restated hot path";
-      return EDDY_EINVAL;
-    }
-    k_outlet_corrector<<<(n2 + 255) / 256, 256, 0, st>>>(d, ubc, vbc, wbc, uof, vof, wof, t6);
-    EDDY_LAUNCHED(ctx);
-  }
-  return EDDY_OK;
+  return bc_boundinout<double, double>(ctx, ctx->d.nx, ctx->d.nx, ubc, vbc, wbc, uof, vof, wof, alfxdt, idiv);
 }
 
 int launch_correct(eddy_ctx *ctx, double alfxdt) {

@@ -453,6 +453,14 @@ int launch_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp) {
   return solve_from_spec(ctx, dp);
 }
 
+int launch_dp_ghost(eddy_ctx *ctx, double *dp) {
+  const Dims &d = ctx->d;
+  long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
+  k_dp_ghost<<<(unsigned)((ng + 255) / 256), 256, 0, ctx->stream>>>(d, dp);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
 int launch_max_divergence(eddy_ctx *ctx, double *out_host) {
   const Dims &d = ctx->d;
   k_maxdiv_partial<<<NPART, 256, 0, ctx->stream>>>(d, ctx->m, ctx->f[EDDY_UO], ctx->f[EDDY_VO], ctx->f[EDDY_WO],

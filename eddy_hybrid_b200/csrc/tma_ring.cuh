@@ -65,8 +65,10 @@ __device__ __forceinline__ void load_3d(void *dst, const CUtensorMap *map, int x
 }  // namespace tma
 
 // Host: encode a 3-D tiled tensor map over an (nx,ny,nz) Fortran array of
-// `esize`-byte elements with a (bx,by,1) box.  Returns 0 on success.
-int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int nz, int bx, int by, int esize);
+// `esize`-byte elements with row pitch `pitch` elements and a (bx,by,1) box.
+// Returns 0 on success.
+int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int nz, int bx, int by, int esize,
+                       int pitch = 0);
 
 // ---------------------------------------------------------------------------
 // Generic k-marching driver over a 4-slot ring of halo planes of NF fields.
@@ -79,37 +81,39 @@ struct alignas(64) TmaMaps {
   CUtensorMap m[NF];
 };
 
-template <int TX, int TY>
+template <int TX, int TY, class T = double>
 struct RingGeom {
-  static constexpr int PX = TX + 2, PY = TY + 2;
-  static constexpr int PLANE = ((PX * PY + 15) / 16) * 16;  // doubles, 128-byte multiple
-  static constexpr unsigned BOX_BYTES = PX * PY * 8;
+  // box rows must span a multiple of 16 bytes: TX + 2 halo columns rounded up
+  static constexpr int PX = (((TX + 2) * (int)sizeof(T) + 15) / 16) * 16 / (int)sizeof(T), PY = TY + 2;
+  static constexpr int EPL = 128 / (int)sizeof(T);                 // elements per 128 bytes
+  static constexpr int PLANE = ((PX * PY + EPL - 1) / EPL) * EPL;  // elements, 128-byte multiple
+  static constexpr unsigned BOX_BYTES = PX * PY * sizeof(T);
 };
 
-template <int TX, int TY, int NF>
+template <int TX, int TY, int NF, class T = double>
 struct RingAcc {
-  using G = RingGeom<TX, TY>;
-  const double *sm;
+  using G = RingGeom<TX, TY, T>;
+  const T *sm;
   int s0, s1, s2, c;
-  __device__ __forceinline__ double at(int f, int di, int dj, int dk) const {
+  __device__ __forceinline__ T at(int f, int di, int dj, int dk) const {
     int so = dk < 0 ? s0 : (dk == 0 ? s1 : s2);
     return sm[so + f * G::PLANE + c + dj * G::PX + di];
   }
 };
 
-template <int NF, int TX, int TY>
+template <int NF, int TX, int TY, class T = double>
 constexpr size_t ring_smem_bytes() {
-  return (size_t)4 * NF * RingGeom<TX, TY>::PLANE * sizeof(double) + 128;
+  return (size_t)4 * NF * RingGeom<TX, TY, T>::PLANE * sizeof(T) + 128;
 }
 
-template <int NF, int TX, int TY, int KC, class Body>
+template <int NF, int TX, int TY, int KC, class T = double, class Body>
 __device__ __forceinline__ void tma_march(int ix1, int ix2, int jy1, int jy2, int kz1, int kz2,
                                           const TmaMaps<NF> &maps, int *err, Body &&body) {
-  using G = RingGeom<TX, TY>;
+  using G = RingGeom<TX, TY, T>;
   constexpr int NSLOT = 4, SLOT = NF * G::PLANE;
   extern __shared__ unsigned char smraw_[];
   __shared__ __align__(8) uint64_t bar[NSLOT];
-  double *sm = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smraw_) + 127) & ~uintptr_t(127));
+  T *sm = reinterpret_cast<T *>((reinterpret_cast<uintptr_t>(smraw_) + 127) & ~uintptr_t(127));
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = ix1 + blockIdx.x * TX, j0 = jy1 + blockIdx.y * TY;
   const int k0 = kz1 + blockIdx.z * KC;
@@ -138,8 +142,8 @@ __device__ __forceinline__ void tma_march(int ix1, int ix2, int jy1, int jy2, in
       ok = ok && tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1);
     }
     if (ok) {
-      RingAcc<TX, TY, NF> S{sm, ((k - 1 - pfirst) & 3) * SLOT, ((k - pfirst) & 3) * SLOT,
-                            ((k + 1 - pfirst) & 3) * SLOT, c};
+      RingAcc<TX, TY, NF, T> S{sm, ((k - 1 - pfirst) & 3) * SLOT, ((k - pfirst) & 3) * SLOT,
+                               ((k + 1 - pfirst) & 3) * SLOT, c};
       body(i, j, k, active, S);
     }
     int failed = __syncthreads_or(ok ? 0 : 1);

@@ -125,6 +125,11 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps);
  * refine_sweeps FP64-residual iterative-refinement sweeps. */
 int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_device);
 
+/* Mixed form only (no counterpart in the reference): max |d - L phi| of the
+ * last refined Poisson solve before each sweep s, out[s] for s < min(n, 4);
+ * entries past refine_sweeps are 0.  EDDY_EINVAL in the plain form. */
+int eddy_refine_residuals(eddy_ctx *ctx, double *out, int n);
+
 /* Diagnostics: max |div u| of (UO,VO,WO) over the interior (src/info.f:32). */
 int eddy_max_divergence(eddy_ctx *ctx, double *out);
 
@@ -133,8 +138,9 @@ int eddy_max_divergence(eddy_ctx *ctx, double *out);
  * src/Eddy6.f:2104-2990).  Categories: 0 RHS+predictor, 1 boundary fills,
  * 2 divergence+forward FFT, 3 forward transform, 4 z line solves,
  * 5 backward transform, 6 backward FFT, 7 CORRECT, 8 pressure update,
- * 9 density, 10 eddy viscosity.  eddy_profile_read synchronises, adds the
- * window's elapsed times per category to ms[11] / counts[11] (cumulative
+ * 9 density, 10 eddy viscosity, 11 refinement residual + forward FFT,
+ * 12 FP64/FP32 copies (mixed form).  eddy_profile_read synchronises, adds the
+ * window's elapsed times per category to ms[13] / counts[13] (cumulative
  * since the mask was set) and starts a new window. */
 int eddy_profile_enable(eddy_ctx *ctx, unsigned mask);
 int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts);
