@@ -3,9 +3,13 @@
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = 3 RK substeps (RHS+predictor, boundary fills, divergence + FFT
-Poisson solve + projection, pressure update, density) + the dynamic eddy
-viscosity update, on the 512x384x256 wake grid (streamwise x vertical x
-periodic), FP64, fields resident on the GPU.  Prints one JSON line.
+Poisson solve + projection, pressure update, density) + the eddy viscosity
+update, on the 512x384x256 wake grid (streamwise x vertical x periodic),
+fields resident on the GPU.  Both forms run from the same state: the plain
+FP64 form (dynamic model) and the chosen form (FP32 stencils and FFTs, FP64
+residual refinement and projection, learned MLP closure); `value` is the
+chosen form, `plain` the FP64 form, `accuracy` the chosen form's error against
+the plain one.  Prints one JSON line.
 N > 1 runs N independent replicas (the solver does not shard; one GPU holds
 the whole domain): value = all ranks' cell-steps / max-over-ranks time.
 """
@@ -50,6 +54,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--sweeps", type=int, default=1, help="refinement sweeps of the mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="tiny grid (smoke)")
     ap.add_argument("--medium", action="store_true",
@@ -173,55 +178,170 @@ def run_reference(args):
     return 0
 
 
+# algorithmic bytes per interior cell per launch in the mixed form (FP32
+# stencil fields, FP64 masters, residual, solution and pressure)
+ALG_BYTES_MIXED = {
+    "rhs_predictor": 15 * 4,   # R 9 FP32 fields  W u*,v*,w*,ua,va,wa FP32
+    "div_fft_fwd": 3 * 4 + 8 + 4,  # R u*,v*,w* FP32  W d FP64, spectrum FP32
+    "refine_residual": 8 + 8 + 4,  # R phi, d FP64  W spectrum FP32
+    "transform_fwd": 2 * 4,
+    "z_line_solve": 2 * 4,
+    "transform_bwd": 2 * 4,
+    "correct": 3 * 4 + 8 + 3 * 8 + 3 * 4,  # R u*,v*,w* FP32, dp  W u,v,w FP64 + FP32 copies
+    "pressure_update": 8 + 8 + 8 + 4,      # R p,dp  W p FP64, p FP32
+    "density": 6 * 4 + 2 * 4,              # R rho,kappa,u,v,w,rha  W rho,rha (FP32)
+    "eddy_viscosity": 4 * 8 + 2 * 8,       # R u,v,w,rho FP64  W nu_t,kappa_t
+    "precision_copy": 4 + 8,               # one FP32<->FP64 copy
+}
+OWN_MIXED = ["rhs_predictor", "div_fft_fwd", "refine_residual", "z_line_solve", "fft_bwd", "correct",
+             "pressure_update", "density", "eddy_viscosity", "precision_copy"]
+MLP_FLOP_PER_CELL = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64 * 16)
+
+
+def timed_steps(g, steps, stream, torch):
+    """K steps bracketed by CUDA events on the solver's stream, profiled."""
+    g.sync()
+    torch.cuda.synchronize()
+    g.profile_enable(0x1FFF)
+    l0 = g.launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        g.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    prof = g.profile_read()
+    g.profile_enable(0)
+    return ms, prof, g.launches - l0
+
+
+def kernel_table(prof, steps, ncell, alg):
+    total = sum(v[0] for v in prof.values())
+    out = {}
+    for c, (ms, n) in prof.items():
+        if not n:
+            continue
+        e = {"ms_per_step": ms / steps, "launches": n, "share": ms / total if total else None}
+        if c in alg:
+            e["gbs"] = alg[c] * ncell / (ms / n / 1e3) / 1e9
+        out[c] = e
+    return out
+
+
+def field_errors(a, b, names):
+    import numpy as np
+    rep = {}
+    for n in names:
+        x, y = a.download(n)[1:-1, 1:-1, 1:-1], b.download(n)[1:-1, 1:-1, 1:-1]
+        d = x - y
+        rep[n] = {"rms": float(np.sqrt(np.mean(d * d))), "max": float(np.max(np.abs(d))),
+                  "rel_rms": float(np.sqrt(np.mean(d * d)) / max(np.sqrt(np.mean(y * y)), 1e-300))}
+    return rep
+
+
+def closure_weights(g_plain, w, log):
+    """Saved network, or one trained now on pairs harvested from the plain run."""
+    from eddy_hybrid_b200 import train_closure as tc
+    from eddy_hybrid_b200 import closure as cl
+    got = tc.load()
+    if got is not None:
+        meta, theta, rep = got
+        rep = dict(rep)
+        rep["source"] = "eddy_hybrid_b200/closure_weights.npz"
+        return meta, theta, rep
+    c = cl.Closure(g_plain)
+    X, T = c.harvest(cl.sample_cells(w, 2_000_000, 5))
+    meta, theta, hist = tc.train(g_plain, X, T, epochs=4, log=log)
+    rep = {"source": "trained in this run on 2e6 cells of the plain run's state", "loss_by_epoch":
+           [float(v) for v in hist]}
+    return meta, theta, rep
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     rank, world, local, dist = dist_init(args.gpus)
     import numpy as np
+    import torch
 
     import eddy_hybrid_b200 as eb
+    from eddy_hybrid_b200 import closure as cl
     from eddy_hybrid_b200 import config
 
-    w = workload(args.small, args.medium)
-    g = eb.Solver(w, device=local if world > 1 else 0)
-    fields = config.initial_fields(w, g.metric("dens_bg")[: w.nx])
-    g.load_initial(fields)
-    g.initialize()
-    for _ in range(args.warmup):
-        g.step(1)
-    g.sync()
-
-    import torch
-    dev = torch.device("cuda", local if world > 1 else 0)
+    log = (lambda *a: print(*a, file=sys.stderr, flush=True)) if rank == 0 else (lambda *a: None)
+    dev_i = local if world > 1 else 0
+    dev = torch.device("cuda", dev_i)
     torch.cuda.set_device(dev)
-    stream = torch.cuda.ExternalStream(g.stream, device=dev)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = Clocks(local if world > 1 else 0)
-    g.profile_enable(0x7FF)
-    launches0 = g.launches
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        g.step(1)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    launches = g.launches - launches0
-    ms = e0.elapsed_time(e1)
-    prof = g.profile_read()
-    g.profile_enable(0)
-    clk = clocks.stop()
-    if dist:
-        dist.barrier()
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    w = workload(args.small, args.medium)
     ncell = w.ncell
-    value = world * ncell * args.steps / (ms / 1e3) / 1e6
+    sweeps = args.sweeps
+
+    def make(precision, closure):
+        g = eb.Solver(w, device=dev_i, precision=precision, refine_sweeps=sweeps, closure=closure)
+        return g
+
+    # ---- plain FP64 form ----
+    g0 = make(eb.PLAIN_FP64, 0)
+    fields = config.initial_fields(w, g0.metric("dens_bg")[: w.nx])
+    g0.load_initial(fields)
+    g0.initialize()
+    for _ in range(args.warmup):
+        g0.step(1)
+    s0 = torch.cuda.ExternalStream(g0.stream, device=dev)
+    if dist:
+        dist.barrier()
+    ms0, prof0, _ = timed_steps(g0, args.steps, s0, torch)
+    log(f"plain FP64: {ms0 / args.steps:.2f} ms/step")
+
+    # ---- mixed precision with the dynamic model (precision error alone) ----
+    g1 = make(eb.MIXED, 0)
+    g1.load_initial(fields)
+    g1.initialize()
+    g1.step(args.warmup + args.steps)
+    g1.sync()
+    acc_mixed = field_errors(g1, g0, ["uo", "vo", "wo", "p", "dens", "tv"])
+    acc_mixed["max_div_u"] = g1.max_divergence()
+    acc_mixed["refine_residuals_last_solve"] = [float(v) for v in g1.refine_residuals()[:sweeps]]
+    g1.close()
+
+    # ---- chosen form: mixed precision + learned closure ----
+    meta, theta, wrep = closure_weights(g0, w, log)
+    g2 = make(eb.MIXED, 1)
+    cl.Closure(g2).set(meta, theta)
+    g2.load_initial(fields)
+    g2.initialize()
+    for _ in range(args.warmup):
+        g2.step(1)
+    s2 = torch.cuda.ExternalStream(g2.stream, device=dev)
+    if dist:
+        dist.barrier()
+    clocks = Clocks(dev_i)
+    ms2, prof2, launches = timed_steps(g2, args.steps, s2, torch)
+    clk = clocks.stop()
+    log(f"chosen form: {ms2 / args.steps:.2f} ms/step")
+    acc_chosen = field_errors(g2, g0, ["uo", "vo", "wo", "p", "dens"])
+    acc_chosen["max_div_u"] = g2.max_divergence()
+    nu_closure = g2.download("tv")[1:-1, 1:-1, 1:-1]
+    c2 = cl.Closure(g2)
+    nout = c2.apply()
+    nu_closure = g2.download("tv")[1:-1, 1:-1, 1:-1]
+    c2.refresh_fallback()                     # the dynamic model on the same state
+    nu_dyn = g2.download("tv")[1:-1, 1:-1, 1:-1]
+    acc_chosen["nu_t_rel_err_vs_dynamic"] = float(np.linalg.norm(nu_closure - nu_dyn) /
+                                                  max(np.linalg.norm(nu_dyn), 1e-300))
+    acc_chosen["cells_outside_envelope"] = nout
+    # restore the closure's viscosity before the end-to-end run
+    c2.apply()
+    if dist:
+        t = torch.tensor([ms0, ms2], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms0, ms2 = (float(v) for v in t.tolist())
+    value = world * ncell * args.steps / (ms2 / 1e3) / 1e6
+    value_plain = world * ncell * args.steps / (ms0 / 1e3) / 1e6
 
     # end to end through the public API with host buffers: per step upload the
     # state from pinned host memory, step, read the state back
@@ -230,21 +350,21 @@ def main():
     for n in io:
         t = torch.empty(w.nx * w.ny * w.nz, dtype=torch.float64, pin_memory=True)
         a = t.numpy().reshape((w.nx, w.ny, w.nz), order="F")
-        a[...] = g.download(n)
+        a[...] = g2.download(n)
         pinned[n] = (t, a)
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    e2.record(stream)
+    e2.record(s2)
     for _ in range(args.e2e_steps):
         for n in io:
-            g.upload(n, pinned[n][1])
-        g.step(1)
+            g2.upload(n, pinned[n][1])
+        g2.step(1)
         for n in io:
-            pinned[n][1][...] = g.download(n)
-    e3.record(stream)
+            pinned[n][1][...] = g2.download(n)
+    e3.record(s2)
     e3.synchronize()
     ems = e2.elapsed_time(e3)
     if dist:
@@ -254,7 +374,7 @@ def main():
     e2e = world * ncell * args.e2e_steps / (ems / 1e3) / 1e6
     fbytes = 8 * w.nx * w.ny * w.nz
 
-    # roofline of the dominant kernel among our own
+    # roofline of the dominant kernel among our own (chosen form)
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -262,44 +382,51 @@ def main():
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    dom = max(OWN, key=lambda c: prof[c][0])
-    dms, dn = prof[dom]
-    achieved = ALG_BYTES[dom] * ncell / (dms / dn / 1e3) / 1e9 if dn else None
+    k2 = kernel_table(prof2, args.steps, ncell, ALG_BYTES_MIXED)
+    dom = max((c for c in OWN_MIXED if c in k2 and c in ALG_BYTES_MIXED), key=lambda c: prof2[c][0])
+    dms, dn = prof2[dom]
+    achieved = ALG_BYTES_MIXED[dom] * ncell / (dms / dn / 1e3) / 1e9 if dn else None
     traffic = None
     tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tf):
         traffic = json.load(open(tf)).get(dom)
-    total_ms = sum(v[0] for v in prof.values())
-    kernels = {c: {"ms_per_step": prof[c][0] / args.steps, "launches": prof[c][1],
-                   "share": prof[c][0] / total_ms if total_ms else None,
-                   **({"gbs": ALG_BYTES[c] * ncell / (prof[c][0] / prof[c][1] / 1e3) / 1e9}
-                      if prof[c][1] and c in ALG_BYTES else {})}
-               for c in prof}
+    mlp_ms = prof2["eddy_viscosity"][0] / max(prof2["eddy_viscosity"][1], 1)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "warmup": args.warmup, "ms_per_step": ms2 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 stencils/FFTs + f64 solve/projection, bf16 MLP",
+        "data": "synthetic",
         "config": {"workload": w.name + " (NZ-2=512 streamwise, NX-2=384 vertical, NY-2=256 periodic)",
-                   "form": "plain FP64", "global_batch": world * ncell, "steps_per_rank": args.steps,
-                   "re": w.re, "fr": w.fr, "dt": w.dt, "sgs": "dynamic (y average)",
+                   "form": f"chosen: FP32 stencils+FFTs, FP64-residual refinement ({sweeps} sweeps), "
+                           "learned MLP closure",
+                   "global_batch": world * ncell, "steps_per_rank": args.steps,
+                   "re": w.re, "fr": w.fr, "dt": w.dt,
                    "immersed_body": "none (IB forcing not yet on the step)",
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (~15 GB state)"},
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (~20 GB state)"},
+        "plain": {"value": value_plain, "ms_per_step": ms0 / args.steps, "dtype": "f64",
+                  "kernels": kernel_table(prof0, args.steps, ncell, ALG_BYTES)},
+        "speedup_chosen_vs_plain": ms0 / ms2,
+        "accuracy": {"reference": "plain FP64 GPU form (bit-exact/1e-11 vs the CPU oracle) from the "
+                                  f"same state after {args.warmup + args.steps} steps",
+                     "mixed_dynamic": acc_mixed, "chosen": acc_chosen, "closure": wrep},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": len(io) * fbytes,
                 "d2h_bytes_per_step": len(io) * fbytes},
         "gpu_launches": launches,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
-                     "peak_source": peak_src,
-                     "algorithmic_bytes_per_cell": ALG_BYTES[dom]},
-        "kernels": kernels,
+                     "peak_source": peak_src, "algorithmic_bytes_per_cell": ALG_BYTES_MIXED[dom]},
+        "mlp_tensor": {"tflops": MLP_FLOP_PER_CELL * ncell / (mlp_ms / 1e3) / 1e12 if mlp_ms else None,
+                       "peak_tflops": peaks.get("bf16_tflops"), "flop_per_cell": MLP_FLOP_PER_CELL},
+        "kernels": k2,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not (args.small or args.medium):
         line["cpu_baseline"] = cpu_baseline(1)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    g.close()
+    g2.close()
+    g0.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

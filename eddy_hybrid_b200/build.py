@@ -27,6 +27,7 @@ UNITS = {
     "k_noalloc.cu": ["-fmad=false"],
     "k_mlp.cu": [],
     "k_mixed.cu": [],
+    "k_xform.cu": [],
     "host_eigen.cpp": [],
 }
 

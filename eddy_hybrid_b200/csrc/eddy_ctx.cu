@@ -284,6 +284,19 @@ int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int n
   return r == CUDA_SUCCESS ? 0 : (int)r;
 }
 
+int make_tensor_map_2d(CUtensorMap *map, const void *base, long long w, long long h, int bx, int by) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return -1;
+  cuuint64_t gdim[2] = {(cuuint64_t)w, (cuuint64_t)h};
+  cuuint64_t gstr[1] = {(cuuint64_t)w * 4};
+  cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
+  cuuint32_t est[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), gdim, gstr, box, est,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : (int)r;
+}
+
 const CUtensorMap *ctx_tensor_map(eddy_ctx *ctx, const double *ptr, int bx, int by) {
   for (TmaEntry &e : ctx->tmaps)
     if (e.ptr == ptr && e.bx == bx && e.by == by) return &e.map;

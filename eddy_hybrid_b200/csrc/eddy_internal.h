@@ -184,6 +184,12 @@ int launch_max_divergence(eddy_ctx *ctx, double *out_host);
 // DIRECT's ghost convention on a solution array (z planes zero, x Neumann, y periodic)
 int launch_dp_ghost(eddy_ctx *ctx, double *dp);
 
+// tensor-core (3xTF32) eigen-transforms of the mixed solve (k_xform.cu):
+// B matrices from a column-major FP64 M x M transform; out = in * B^T
+bool xform_supported(int M);
+int xform_prepare(eddy_ctx *ctx, const double *T_dev, float **bhi, float **blo);
+int launch_xform(eddy_ctx *ctx, const float *in, float *out, const float *bhi, const float *blo);
+
 // mixed-precision form (k_mixed.cu): FP32 stencils and FFTs, FP64 line solves,
 // FP64-residual iterative refinement, FP64 projection onto FP64 master velocities
 int mixed_create(eddy_ctx *ctx);

@@ -50,6 +50,8 @@ struct MixedState {
   float *twr = nullptr, *twi = nullptr;  // FFT twiddles: forward table then backward table
   double *resid = nullptr;               // max |r| before each sweep (device, 4 entries)
   double *wout = nullptr;                // outlet-face w (NX,NY) in FP64: exact mass balance
+  // 3xTF32 tensor-core transforms: forward (Af) and backward (Ab) matrices, hi/lo
+  float *fhi = nullptr, *flo = nullptr, *bhi = nullptr, *blo = nullptr;
 };
 
 MixedState *ms(eddy_ctx *ctx) { return static_cast<MixedState *>(ctx->mixed); }
@@ -170,196 +172,178 @@ constexpr int TI32 = 32, FT32 = 256;
 
 __device__ __forceinline__ int bitrev(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
 
-__device__ void fft_lines32(float *re, float *im, int L, const float *__restrict__ twr,
-                            const float *__restrict__ twi) {
-  for (int len = 2; len <= L; len <<= 1) {
-    int h = len >> 1, stride = L / len;
-    for (int bf = threadIdx.x; bf < TI32 * (L >> 1); bf += blockDim.x) {
-      int ii = bf % TI32, pq = bf / TI32;
-      int grp = pq / h, qq = pq % h;
-      int a = grp * len + qq, b = a + h;
-      float wr = twr[qq * stride], wi = twi[qq * stride];
-      float xr = re[b * TI32 + ii], xi = im[b * TI32 + ii];
-      float tr = wr * xr - wi * xi;
-      float ti = wr * xi + wi * xr;
-      float ar = re[a * TI32 + ii], ai = im[a * TI32 + ii];
-      re[b * TI32 + ii] = ar - tr;
-      im[b * TI32 + ii] = ai - ti;
-      re[a * TI32 + ii] = ar + tr;
-      im[a * TI32 + ii] = ai + ti;
-    }
-    __syncthreads();
-  }
-}
+#include "fft_lines.cuh"
 
-// Forward transform of the right-hand side.  mode 0: d = div(u*)/alfxdt in
+// Forward transform of the right-hand side.  MODE 0: d = div(u*)/alfxdt in
 // FP64 from the FP32 predictor velocities (src/timeindeg.f:941-949), stored
-// to dvec; mode 1: d = dvec; mode 2: r = dvec - L phi (FP64 residual of the
+// to dvec; MODE 1: d = dvec; MODE 2: r = dvec - L phi (FP64 residual of the
 // DIRECT operator: Neumann x and z, periodic y), max|r| -> rmax.
-__global__ void __launch_bounds__(FT32)
+// Each thread gathers U elements per pass with all loads issued before the
+// shared-memory stores, so several requests per thread are in flight.
+template <int MODE>
+__global__ void __launch_bounds__(FT32, 3)
     k_fwd32(Dims d, DevMetrics m, int px, const float *__restrict__ us, const float *__restrict__ vs,
             const float *__restrict__ ws, const double *__restrict__ win, const double *__restrict__ wout,
-            const double *__restrict__ phi, double *__restrict__ dvec, int mode, double alfxdt, double rdy2,
-            int logL, const float *__restrict__ twr, const float *__restrict__ twi, float *__restrict__ spec,
+            const double *__restrict__ phi, double *__restrict__ dvec, double alfxdt, double rdy2, int logL,
+            const float *__restrict__ twr, const float *__restrict__ twi, float *__restrict__ spec,
             unsigned long long *rmax) {
+  constexpr int U = MODE == 2 ? 4 : 8;
   extern __shared__ float smf[];
   __shared__ double red[FT32 / 32];
-  const int L = 1 << logL, M = d.nx - 2;
+  const int L = 1 << logL, M = d.nx - 2, NT = L * TI32;
   float *re = smf, *im = smf + L * TI32;
+  float *tsr = smf + 2 * L * TI32, *tsi = tsr + L / 2;
+  load_twiddles(tsr, tsi, twr, twi, L / 2);
   const int i0 = d.ix1 + blockIdx.x * TI32;
   const int k = d.kz1 + blockIdx.y;
   const long long sz = (long long)d.nx * d.ny;
   double amax = 0.;
-  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
-    int ii = t % TI32, jj = t / TI32;
-    int i = i0 + ii, j = d.jy1 + jj;
-    double v = 0.;
-    if (i <= d.ix2) {
-      long long q = fidx(d, i, j, k);
-      if (mode == 0) {
-        long long p = pidx(d, px, i, j, k);
-        // inlet and outlet faces from their FP64 planes (the mass balance of
-        // the convective outlet holds in FP64, so the right-hand side stays
-        // compatible with the Neumann operator)
-        int pl = (i - 1) + d.nx * (j - 1);
-        double wk = k == d.kz2 ? wout[pl] : (double)ws[p];
-        double wkm = k == d.kz1 ? win[pl] : (double)ws[p - (long long)px * d.ny];
-        v = (m.ap[i] * ((double)us[p] - (double)us[p - 1]) + m.bp[j] * ((double)vs[p] - (double)vs[p - px]) +
-             m.cp[k] * (wk - wkm));
-        v = v / alfxdt;
-        dvec[q] = v;
-      } else if (mode == 1) {
-        v = dvec[q];
-      } else {
-        double c = phi[q];
-        double lx = 0., lz = 0.;
-        if (i < d.ix2) lx += m.ap[i] * m.au[i] * (phi[q + 1] - c);
-        if (i > d.ix1) lx += m.ap[i] * m.au[i - 1] * (phi[q - 1] - c);
-        int jp = j < d.jy2 ? j + 1 : d.jy1, jm = j > d.jy1 ? j - 1 : d.jy2;
-        double ly = (phi[fidx(d, i, jp, k)] - 2. * c + phi[fidx(d, i, jm, k)]) * rdy2;
-        if (k < d.kz2) lz += m.cp[k] * m.cw[k] * (phi[q + sz] - c);
-        if (k > d.kz1) lz += m.cp[k] * m.cw[k - 1] * (phi[q - sz] - c);
-        v = dvec[q] - (lx + ly + lz);
-        amax = fmax(amax, fabs(v));
+  for (int t0 = threadIdx.x; t0 < NT; t0 += FT32 * U) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT32;
+      const int ii = t % TI32, jj = t / TI32;
+      const int i = i0 + ii, j = d.jy1 + jj;
+      v[u] = 0.;
+      if (t < NT && i <= d.ix2) {
+        const long long q = fidx(d, i, j, k);
+        if (MODE == 0) {
+          const long long p = pidx(d, px, i, j, k);
+          // inlet and outlet faces from their FP64 planes (the mass balance of
+          // the convective outlet holds in FP64, so the right-hand side stays
+          // compatible with the Neumann operator)
+          const int pl = (i - 1) + d.nx * (j - 1);
+          const double wk = k == d.kz2 ? wout[pl] : (double)ws[p];
+          const double wkm = k == d.kz1 ? win[pl] : (double)ws[p - (long long)px * d.ny];
+          double x = (m.ap[i] * ((double)us[p] - (double)us[p - 1]) + m.bp[j] * ((double)vs[p] - (double)vs[p - px]) +
+                      m.cp[k] * (wk - wkm));
+          x = x / alfxdt;
+          dvec[q] = x;
+          v[u] = x;
+        } else if (MODE == 1) {
+          v[u] = dvec[q];
+        } else {
+          const double c = phi[q];
+          const double pe = i < d.ix2 ? phi[q + 1] : c, pw = i > d.ix1 ? phi[q - 1] : c;
+          const int jp = j < d.jy2 ? j + 1 : d.jy1, jm = j > d.jy1 ? j - 1 : d.jy2;
+          const double pn = phi[fidx(d, i, jp, k)], ps = phi[fidx(d, i, jm, k)];
+          const double pt = k < d.kz2 ? phi[q + sz] : c, pb = k > d.kz1 ? phi[q - sz] : c;
+          const double lx = m.ap[i] * m.au[i] * (pe - c) + m.ap[i] * m.au[i - 1] * (pw - c);
+          const double ly = (pn - 2. * c + ps) * rdy2;
+          const double lz = m.cp[k] * m.cw[k] * (pt - c) + m.cp[k] * m.cw[k - 1] * (pb - c);
+          const double x = dvec[q] - (lx + ly + lz);
+          amax = fmax(amax, fabs(x));
+          v[u] = x;
+        }
       }
     }
-    int r = bitrev(jj, logL);
-    re[r * TI32 + ii] = (float)v;
-    im[r * TI32 + ii] = 0.f;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT32;
+      if (t < NT) {
+        const int ii = t % TI32, r = bitrev(t / TI32, logL);
+        re[r * TI32 + ii] = (float)v[u];
+        im[r * TI32 + ii] = 0.f;
+      }
+    }
   }
-  if (mode == 2) {
+  if (MODE == 2) {
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
   }
   __syncthreads();
-  if (mode == 2 && threadIdx.x == 0) {
+  if (MODE == 2 && threadIdx.x == 0) {
     double b = 0.;
     for (int w = 0; w < FT32 / 32; w++) b = fmax(b, red[w]);
     atomicMax(rmax, (unsigned long long)__double_as_longlong(b));
   }
-  fft_lines32(re, im, L, twr, twi);
+  fft_lines_r22<float, TI32>(re, im, logL, tsr, tsi);
   const long long lineK = (long long)(k - d.kz1) * L;
-  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
-    int ii = t % TI32, J = t / TI32;
-    int i = i0 + ii;
+  for (int t = threadIdx.x; t < NT; t += blockDim.x) {
+    const int ii = t % TI32, J = t / TI32;
+    const int i = i0 + ii;
     if (i > d.ix2) continue;
     float v;
     if (J == 0) v = re[ii];
     else if (J == L - 1) v = re[(L / 2) * TI32 + ii];
     else {
-      int qq = (J + 1) / 2;
+      const int qq = (J + 1) / 2;
       v = (J & 1) ? re[qq * TI32 + ii] : im[qq * TI32 + ii];
     }
     spec[(long long)(i - d.ix1) + (long long)M * (J + lineK)] = v;
   }
 }
 
-// (S - mean[J==0]) / L, Hermitian extension, inverse FFT; phi = or += result
-__global__ void __launch_bounds__(FT32)
+// (S - mean[J==0]) / L, Hermitian extension, inverse FFT; phi = (ACC ? phi +
+// : ) result.  Gathers and the accumulate reads are batched U per thread.
+template <int ACC>
+__global__ void __launch_bounds__(FT32, 3)
     k_bwd32(Dims d, const float *__restrict__ spec, const double *__restrict__ dpm, int logL,
-            const float *__restrict__ twr, const float *__restrict__ twi, double *__restrict__ phi, int accumulate) {
+            const float *__restrict__ twr, const float *__restrict__ twi, double *__restrict__ phi) {
+  constexpr int U = 8;
   extern __shared__ float smf[];
-  const int L = 1 << logL, M = d.nx - 2;
+  const int L = 1 << logL, M = d.nx - 2, NT = L * TI32;
   float *re = smf, *im = smf + L * TI32;
+  float *tsr = smf + 2 * L * TI32, *tsi = tsr + L / 2;
+  load_twiddles(tsr, tsi, twr, twi, L / 2);
   const int i0 = d.ix1 + blockIdx.x * TI32;
   const int k = d.kz1 + blockIdx.y;
   const long long lineK = (long long)(k - d.kz1) * L;
   const float mean = (float)dpm[0], rl = 1.f / (float)L;
-  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
-    int ii = t % TI32, q = t / TI32;
-    int i = i0 + ii;
-    float xr = 0.f, xi = 0.f;
-    if (i <= d.ix2) {
-      const float *S = spec + (long long)(i - d.ix1);
-      auto get = [&](int J) {
-        float v = S[(long long)M * (J + lineK)];
-        if (J == 0) v = v - mean;
-        return v * rl;
-      };
-      if (q == 0) xr = get(0);
-      else if (q == L / 2) xr = get(L - 1);
-      else if (q < L / 2) { xr = get(2 * q - 1); xi = get(2 * q); }
-      else { int qq = L - q; xr = get(2 * qq - 1); xi = -get(2 * qq); }
+  for (int t0 = threadIdx.x; t0 < NT; t0 += FT32 * U) {
+    float xr[U], xi[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT32;
+      const int ii = t % TI32, q = t / TI32;
+      const int i = i0 + ii;
+      xr[u] = 0.f;
+      xi[u] = 0.f;
+      if (t < NT && i <= d.ix2) {
+        const float *S = spec + (long long)(i - d.ix1);
+        auto get = [&](int J) {
+          float v = S[(long long)M * (J + lineK)];
+          if (J == 0) v = v - mean;
+          return v * rl;
+        };
+        if (q == 0) xr[u] = get(0);
+        else if (q == L / 2) xr[u] = get(L - 1);
+        else if (q < L / 2) { xr[u] = get(2 * q - 1); xi[u] = get(2 * q); }
+        else { const int qq = L - q; xr[u] = get(2 * qq - 1); xi[u] = -get(2 * qq); }
+      }
     }
-    int r = bitrev(q, logL);
-    re[r * TI32 + ii] = xr;
-    im[r * TI32 + ii] = xi;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT32;
+      if (t < NT) {
+        const int ii = t % TI32, r = bitrev(t / TI32, logL);
+        re[r * TI32 + ii] = xr[u];
+        im[r * TI32 + ii] = xi[u];
+      }
+    }
   }
   __syncthreads();
-  fft_lines32(re, im, L, twr, twi);
-  for (int t = threadIdx.x; t < L * TI32; t += blockDim.x) {
-    int ii = t % TI32, jj = t / TI32;
-    int i = i0 + ii;
-    if (i > d.ix2) continue;
-    long long q = fidx(d, i, d.jy1 + jj, k);
-    double v = (double)re[jj * TI32 + ii];
-    phi[q] = accumulate ? phi[q] + v : v;
+  fft_lines_r22<float, TI32>(re, im, logL, tsr, tsi);
+  for (int t0 = threadIdx.x; t0 < NT; t0 += FT32 * U) {
+    double old[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT32;
+      const int ii = t % TI32, jj = t / TI32, i = i0 + ii;
+      old[u] = 0.;
+      if (ACC && t < NT && i <= d.ix2) old[u] = phi[fidx(d, i, d.jy1 + jj, k)];
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT32;
+      const int ii = t % TI32, jj = t / TI32, i = i0 + ii;
+      if (t < NT && i <= d.ix2) phi[fidx(d, i, d.jy1 + jj, k)] = old[u] + (double)re[jj * TI32 + ii];
+    }
   }
 }
 
-// Thomas along z per (m,J) line in FP64 arithmetic on FP32 storage
-// (same elimination and singular-line treatment as the FP64 solve)
-__global__ void __launch_bounds__(256)
-    k_tridiag32(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
-                const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
-                const double *__restrict__ wz, float *__restrict__ g, double *__restrict__ cpr) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)M * L) return;
-  int mi = (int)(t % M), J = (int)(t / M);
-  long long ML = (long long)M * L;
-  int pin = (J == 0 && mi == m0);
-  int s0 = pin ? 1 : 0;
-  double lm = lam[mi], akJ = ak[J];
-  double cm = 0.;
-  if (pin) {
-    double sv = 0., vv = 0.;
-    for (int k = 0; k < N; k++) {
-      sv += (double)g[t + ML * k] * wz[k];
-      vv += wz[k];
-    }
-    cm = sv / vv;
-  }
-  double prev_c = 0., prev_d = 0.;
-  for (int k = s0; k < N; k++) {
-    double a = (k == s0) ? 0. : an[k];
-    double b = (bn[k] + lm) - akJ;
-    double den = b - a * prev_c;
-    double c = cn[k] / den;
-    double f = (double)g[t + ML * k] - cm;
-    double dd = (f - a * prev_d) / den;
-    cpr[t + ML * k] = c;
-    cpr[t + ML * k + ML * N] = dd;
-    prev_c = c;
-    prev_d = dd;
-  }
-  double x = prev_d;
-  g[t + ML * (N - 1)] = (float)x;
-  for (int k = N - 2; k >= s0; k--) {
-    x = cpr[t + ML * k + ML * N] - cpr[t + ML * k] * x;
-    g[t + ML * k] = (float)x;
-  }
-  if (pin) g[t] = 0.f;
-}
+#include "tridiag_z.cuh"
 
 __global__ void k_plane_sum32(int M, int L, int N, const float *__restrict__ s, double *part) {
   __shared__ double sh[256];
@@ -630,34 +614,50 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   float *s1 = reinterpret_cast<float *>(pp.spec), *s2 = reinterpret_cast<float *>(pp.spec2);
   const float one = 1.f, zero = 0.f;
   cublasStatus_t bs;
+  int rc;
   {
     ProfScope ps(ctx, PROF_GEMM_FWD);
-    bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Af32, M, s1, M, &zero, s2, M);
-    if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (forward transform) failed"; return EDDY_ECUDA; }
-    ctx->launches++;
+    if (x->fhi) {
+      if ((rc = launch_xform(ctx, s1, s2, x->fhi, x->flo))) return rc;
+    } else {
+      bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Af32, M, s1, M, &zero, s2,
+                       M);
+      if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (forward transform) failed"; return EDDY_ECUDA; }
+      ctx->launches++;
+    }
   }
   {
     ProfScope ps(ctx, PROF_TRIDIAG);
     long long nl = (long long)M * L;
-    k_tridiag32<<<nblk(nl), 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, pp.wz, s2,
-                                                  pp.cprime);
+    k_line_mean<float><<<1, 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.wz, s2, ctx->scal + 5);
+    EDDY_LAUNCHED(ctx);
+    k_tridiag_lines<float><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
+        M, L, N, pp.m0, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, s2, pp.cprime,
+        pp.cprime + (size_t)M * L * N);
     EDDY_LAUNCHED(ctx);
   }
   {
     ProfScope ps(ctx, PROF_GEMM_BWD);
-    bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Ab32, M, s2, M, &zero, s1, M);
-    if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (backward transform) failed"; return EDDY_ECUDA; }
-    ctx->launches++;
+    if (x->bhi) {
+      if ((rc = launch_xform(ctx, s2, s1, x->bhi, x->blo))) return rc;
+    } else {
+      bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Ab32, M, s2, M, &zero, s1,
+                       M);
+      if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (backward transform) failed"; return EDDY_ECUDA; }
+      ctx->launches++;
+    }
   }
   ProfScope ps(ctx, PROF_FFT_BWD);
   k_plane_sum32<<<NPART, 256, 0, ctx->stream>>>(M, L, N, s1, pp.red);
   EDDY_LAUNCHED(ctx);
   k_sum_final<<<1, 32, 0, ctx->stream>>>(NPART, (long long)M * N, pp.red, ctx->scal + 3);
   EDDY_LAUNCHED(ctx);
-  size_t smem = sizeof(float) * 2 * L * TI32;
+  size_t smem = sizeof(float) * (2 * L * TI32 + L);
   dim3 g((M + TI32 - 1) / TI32, N);
-  k_bwd32<<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi,
-                                          accumulate);
+  if (accumulate)
+    k_bwd32<1><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi);
+  else
+    k_bwd32<0><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
@@ -667,14 +667,22 @@ int fwd32(eddy_ctx *ctx, int mode, double alfxdt, const double *phi, double *dve
   MixedState *x = ms(ctx);
   PoissonPlan &pp = ctx->pp;
   const Dims &d = ctx->d;
-  size_t smem = sizeof(float) * 2 * pp.L * TI32;
+  size_t smem = sizeof(float) * (2 * pp.L * TI32 + pp.L);
   dim3 g((pp.M + TI32 - 1) / TI32, pp.N);
   ProfScope ps(ctx, mode == 2 ? PROF_REFINE : PROF_DIV_FFT);
-  k_fwd32<<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
-                                          phi, dvec, mode, alfxdt,
-                                          1.0 / ctx->delysq, log2i(pp.L), x->twr, x->twi,
-                                          reinterpret_cast<float *>(pp.spec),
-                                          reinterpret_cast<unsigned long long *>(x->resid + sweep));
+  auto *rm = reinterpret_cast<unsigned long long *>(x->resid + sweep);
+  float *sp = reinterpret_cast<float *>(pp.spec);
+  const int lg = log2i(pp.L);
+  const double rdy2 = 1.0 / ctx->delysq;
+  if (mode == 0)
+    k_fwd32<0><<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
+                                               phi, dvec, alfxdt, rdy2, lg, x->twr, x->twi, sp, rm);
+  else if (mode == 1)
+    k_fwd32<1><<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
+                                               phi, dvec, alfxdt, rdy2, lg, x->twr, x->twi, sp, rm);
+  else
+    k_fwd32<2><<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
+                                               phi, dvec, alfxdt, rdy2, lg, x->twr, x->twi, sp, rm);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
@@ -746,6 +754,11 @@ int mixed_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMalloc(&x->twi, sizeof(float) * L));
   EDDY_CUDA(cudaMemcpy(x->twr, twr.data(), sizeof(float) * L, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(x->twi, twi.data(), sizeof(float) * L, cudaMemcpyHostToDevice));
+  if (xform_supported(ctx->pp.M)) {
+    int rc = xform_prepare(ctx, ctx->pp.Af, &x->fhi, &x->flo);
+    if (rc == EDDY_OK) rc = xform_prepare(ctx, ctx->pp.Ab, &x->bhi, &x->blo);
+    if (rc) return rc;
+  }
   EDDY_CUDA(cudaMalloc(&x->wout, sizeof(double) * (size_t)d.nx * d.ny));
   EDDY_CUDA(cudaMemset(x->wout, 0, sizeof(double) * (size_t)d.nx * d.ny));
   EDDY_CUDA(cudaMalloc(&x->resid, 4 * sizeof(double)));
@@ -754,10 +767,13 @@ int mixed_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaFree(ctx->pp.cprime));
   ctx->pp.cprime = nullptr;
   EDDY_CUDA(cudaMalloc(&ctx->pp.cprime, 2 * sizeof(double) * (size_t)ctx->pp.M * ctx->pp.L * ctx->pp.N));
-  size_t smem = sizeof(float) * 2 * L * TI32;
+  size_t smem = sizeof(float) * (2 * L * TI32 + L);
   if (smem > 48 * 1024) {
-    EDDY_CUDA(cudaFuncSetAttribute(k_fwd32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    EDDY_CUDA(cudaFuncSetAttribute(k_bwd32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EDDY_CUDA(cudaFuncSetAttribute(k_fwd32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EDDY_CUDA(cudaFuncSetAttribute(k_fwd32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EDDY_CUDA(cudaFuncSetAttribute(k_fwd32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EDDY_CUDA(cudaFuncSetAttribute(k_bwd32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EDDY_CUDA(cudaFuncSetAttribute(k_bwd32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   EDDY_CUDA(cudaFuncSetAttribute(k_rhs32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ring_smem_bytes<NFLD, TX, TY, float>()));
@@ -774,6 +790,8 @@ void mixed_release(eddy_ctx *ctx) {
   for (float *p : fl) if (p) cudaFree(p);
   if (x->resid) cudaFree(x->resid);
   if (x->wout) cudaFree(x->wout);
+  float *tw[] = {x->fhi, x->flo, x->bhi, x->blo};
+  for (float *p : tw) if (p) cudaFree(p);
   delete x;
   ctx->mixed = nullptr;
 }

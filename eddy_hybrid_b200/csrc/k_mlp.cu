@@ -180,8 +180,13 @@ __device__ __forceinline__ float softplus(float x) { return x > 20.f ? x : log1p
 // raw features of interior cell (i,j,k) and its filter width Delta
 // (9 velocity-gradient components * Delta, |grad rho| * Delta, N^2 = -g drho/dx,
 // distance to the nearest x wall)
-__device__ __forceinline__ void cell_features(const Dims &d, const DevMetrics &m, double grav, double xwall_lo,
-                                              double xwall_hi, const double *__restrict__ uo,
+// cube roots of the cell widths along x, y, z: Delta = cx[i] cy[j] cz[k]
+struct CellGeom {
+  const double *cx, *cy, *cz;
+};
+
+__device__ __forceinline__ void cell_features(const Dims &d, const DevMetrics &m, const CellGeom &cg, double grav,
+                                              double xwall_lo, double xwall_hi, const double *__restrict__ uo,
                                               const double *__restrict__ vo, const double *__restrict__ wo,
                                               const double *__restrict__ dens, const double *__restrict__ xc,
                                               int i, int j, int k, float *f, float &delta) {
@@ -202,7 +207,7 @@ __device__ __forceinline__ void cell_features(const Dims &d, const DevMetrics &m
   double drx = 0.5 * (m.au[i] * (dens[q + 1] - dens[q]) + m.au[i - 1] * (dens[q] - dens[q - 1]));
   double dry = 0.5 * (m.bv[j] * (dens[q + sy] - dens[q]) + m.bv[j - 1] * (dens[q] - dens[q - sy]));
   double drz = 0.5 * (m.cw[k] * (dens[q + sz] - dens[q]) + m.cw[k - 1] * (dens[q] - dens[q - sz]));
-  double del = cbrt(1.0 / (m.ap[i] * m.bp[j] * m.cp[k]));
+  double del = cg.cx[i] * cg.cy[j] * cg.cz[k];
   delta = (float)del;
   f[0] = (float)(del * dudx); f[1] = (float)(del * dudy); f[2] = (float)(del * dudz);
   f[3] = (float)(del * dvdx); f[4] = (float)(del * dvdy); f[5] = (float)(del * dvdz);
@@ -213,24 +218,28 @@ __device__ __forceinline__ void cell_features(const Dims &d, const DevMetrics &m
   f[11] = (float)fmin(x - xwall_lo, xwall_hi - x);
 }
 
-__device__ __forceinline__ void interior_ijk(const Dims &d, long long t, int &i, int &j, int &k) {
-  long long mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
-  i = d.ix1 + (int)(t % mi);
-  j = d.jy1 + (int)((t / mi) % mj);
-  k = d.kz1 + (int)(t / (mi * mj));
+// interior cell number t (x fastest) -> (i,j,k); the interior has fewer
+// than 2^32 cells (checked at launch)
+__device__ __forceinline__ void interior_ijk(const Dims &d, unsigned t, int &i, int &j, int &k) {
+  unsigned mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
+  unsigned r = t / mi;
+  i = d.ix1 + (int)(t - r * mi);
+  unsigned kk = r / mj;
+  j = d.jy1 + (int)(r - kk * mj);
+  k = d.kz1 + (int)kk;
 }
 
 // raw features (n x 12) and dynamic-model targets nu_t/Delta for a list of
 // interior cell indices
-__global__ void k_harvest(Dims d, DevMetrics m, double grav, double xlo, double xhi, const double *uo,
+__global__ void k_harvest(Dims d, DevMetrics m, CellGeom cg, double grav, double xlo, double xhi, const double *uo,
                           const double *vo, const double *wo, const double *dens, const double *xc, const double *tv,
                           const long long *cells, int n, float *X, float *T) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   int i, j, k;
-  interior_ijk(d, cells[s], i, j, k);
+  interior_ijk(d, (unsigned)cells[s], i, j, k);
   float f[NFEAT], del;
-  cell_features(d, m, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
+  cell_features(d, m, cg, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
   for (int c = 0; c < NFEAT; c++) X[(size_t)s * NFEAT + c] = f[c];
   T[s] = (float)(tv[fidx(d, i, j, k)] / del);
 }
@@ -264,20 +273,31 @@ __device__ __forceinline__ void mma_layer(uint32_t tm, const unsigned char *a, c
   }
 }
 
-// hidden epilogue: TMEM (64 cols of this thread's row) + bias -> SiLU -> bf16 row
-__device__ __forceinline__ void hidden_epilogue(uint32_t tm, int warp, int row, const float *bias,
+// SiLU of two pre-activations given as halves h = x/2 (FP32), in BF16x2:
+// silu(x) = x sigmoid(x) = h + h tanh(h); one tanh.approx.bf16x2 per pair
+__device__ __forceinline__ uint32_t silu2_bf16(float h0, float h1) {
+  __nv_bfloat162 hb = __floats2bfloat162_rn(h0, h1);
+  uint32_t hv = *reinterpret_cast<uint32_t *>(&hb), tv, r;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tv) : "r"(hv));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(r) : "r"(hv), "r"(tv));
+  return r;
+}
+
+// hidden epilogue: TMEM (64 cols of this thread's row) + bias -> SiLU -> bf16
+// row of the next layer's A operand.  hbias = bias / 2.
+__device__ __forceinline__ void hidden_epilogue(uint32_t tm, int warp, int row, const float *hbias,
                                                 unsigned char *h) {
+  uint32_t r[HID];
+  umma::tmem_ld64(tm + ((uint32_t)(warp * 32) << 16), r);
+  auto x = [&](int c) { return fmaf(__uint_as_float(r[c]), 0.5f, hbias[c]); };
 #pragma unroll
-  for (int c0 = 0; c0 < HID; c0 += 16) {
-    float v[16];
-    umma::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-#pragma unroll
-    for (int q = 0; q < 16; q += 8) {
-      __align__(16) __nv_bfloat16 o[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) o[e] = __float2bfloat16_rn(silu(v[q + e] + bias[c0 + q + e]));
-      *reinterpret_cast<uint4 *>(h + umma::kmajor_offset(row, c0 + q, HID)) = *reinterpret_cast<uint4 *>(o);
-    }
+  for (int c0 = 0; c0 < HID; c0 += 8) {
+    uint4 o;
+    o.x = silu2_bf16(x(c0 + 0), x(c0 + 1));
+    o.y = silu2_bf16(x(c0 + 2), x(c0 + 3));
+    o.z = silu2_bf16(x(c0 + 4), x(c0 + 5));
+    o.w = silu2_bf16(x(c0 + 6), x(c0 + 7));
+    *reinterpret_cast<uint4 *>(h + umma::kmajor_offset(row, c0, HID)) = o;
   }
 }
 
@@ -299,7 +319,7 @@ __device__ __forceinline__ void publish_smem() {
 // normalised features leave [lo, hi] take the fallback (last dynamic-model
 // value).  counts[0] += out-of-envelope cells.
 __global__ void __launch_bounds__(IT)
-    k_mlp_infer(Dims d, DevMetrics m, double grav, double xlo, double xhi, const double *__restrict__ uo,
+    k_mlp_infer(Dims d, DevMetrics m, CellGeom cg, double grav, double xlo, double xhi, const double *__restrict__ uo,
                 const double *__restrict__ vo, const double *__restrict__ wo, const double *__restrict__ dens,
                 const double *__restrict__ xc, const __nv_bfloat16 *__restrict__ wbf, const float *__restrict__ theta,
                 const float *__restrict__ meta, const double *__restrict__ fallback, double *__restrict__ tv,
@@ -320,29 +340,29 @@ __global__ void __launch_bounds__(IT)
   stage_weights(S.w2, wbf + OFF_W2, HID, HID);
   stage_weights(S.w3, wbf + OFF_W3, HID, HID);
   stage_weights(S.w4, wbf + OFF_W4, NOUT, HID);
-  for (int e = tid; e < HID; e += IT) {
-    S.b1[e] = theta[OFF_B1 + e];
-    S.b2[e] = theta[OFF_B2 + e];
-    S.b3[e] = theta[OFF_B3 + e];
+  for (int e = tid; e < HID; e += IT) {  // hidden biases halved for the SiLU epilogue
+    S.b1[e] = 0.5f * theta[OFF_B1 + e];
+    S.b2[e] = 0.5f * theta[OFF_B2 + e];
+    S.b3[e] = 0.5f * theta[OFF_B3 + e];
   }
   if (tid < NOUT) S.b4[tid] = theta[OFF_B4 + tid];
   for (int e = tid; e < NMETA; e += IT) reinterpret_cast<float *>(&S.meta)[e] = meta[e];
   publish_smem();
   const uint32_t tm = S.tmem;
-  const long long ninner = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
-  const long long ntiles = (ninner + 127) / 128;
+  const unsigned ninner = (unsigned)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
+  const unsigned ntiles = (ninner + 127) / 128;
   int phase = 0;
   bool ok = true;
   int nout = 0;
-  for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    long long t = tile * 128 + tid;
+  for (unsigned tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    unsigned t = tile * 128 + tid;
     bool valid = t < ninner;
     int i = d.ix1, j = d.jy1, k = d.kz1;
     float f[NFEAT], del = 1.f;
     bool outside = false;
     if (valid) {
       interior_ijk(d, t, i, j, k);
-      cell_features(d, m, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
+      cell_features(d, m, cg, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
       for (int c = 0; c < NFEAT; c++) {
         f[c] = (f[c] - S.meta.mean[c]) * S.meta.istd[c];
         outside = outside || !(f[c] >= S.meta.lo[c] && f[c] <= S.meta.hi[c]);
@@ -531,6 +551,7 @@ struct MlpState {
   double *loss = nullptr;
   unsigned long long *counts = nullptr;
   double *fallback = nullptr;  // last dynamic-model nu_t
+  double *cbw = nullptr;       // cube roots of the cell widths (x, y, z blocks)
   int adam_t = 0;
   bool ready = false;
   MlpTrainBuffers tb;
@@ -547,11 +568,30 @@ static MlpState *mlp_state(eddy_ctx *ctx) {
 void mlp_release(eddy_ctx *ctx) {
   MlpState *s = static_cast<MlpState *>(ctx->mlp);
   if (!s) return;
-  void *p[] = {s->theta, s->grad, s->m1, s->m2, s->meta, s->w, s->wt, s->loss, s->counts, s->fallback};
+  void *p[] = {s->theta, s->grad, s->m1, s->m2, s->meta, s->w, s->wt, s->loss, s->counts, s->fallback, s->cbw};
   for (void *q : p) if (q) cudaFree(q);
   s->tb.release();
   delete s;
   ctx->mlp = nullptr;
+}
+
+// Delta = (cell volume)^(1/3) as a product of per-axis cube roots
+static int mlp_geom(eddy_ctx *ctx, MlpState *s, CellGeom &cg) {
+  const Dims &d = ctx->d;
+  size_t nx = d.nx + 2, ny = d.ny + 2, nz = d.nz + 2;
+  if (!s->cbw) {
+    std::vector<double> h(nx + ny + nz, 0.0);
+    const std::vector<double> &ap = ctx->h[2], &bp = ctx->h[8], &cp = ctx->h[14];
+    for (size_t i = 0; i < nx && i < ap.size(); i++) h[i] = ap[i] > 0 ? std::cbrt(1.0 / ap[i]) : 0.0;
+    for (size_t j = 0; j < ny && j < bp.size(); j++) h[nx + j] = bp[j] > 0 ? std::cbrt(1.0 / bp[j]) : 0.0;
+    for (size_t k = 0; k < nz && k < cp.size(); k++) h[nx + ny + k] = cp[k] > 0 ? std::cbrt(1.0 / cp[k]) : 0.0;
+    EDDY_CUDA(cudaMalloc(&s->cbw, sizeof(double) * h.size()));
+    EDDY_CUDA(cudaMemcpy(s->cbw, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  }
+  cg.cx = s->cbw;
+  cg.cy = s->cbw + nx;
+  cg.cz = s->cbw + nx + ny;
+  return EDDY_OK;
 }
 
 static int mlp_alloc(eddy_ctx *ctx, MlpState *s) {
@@ -675,6 +715,9 @@ int eddy_closure_get(eddy_ctx *ctx, float *meta, float *theta) {
 // current fields (TV holds the dynamic model's viscosity)
 int eddy_closure_harvest(eddy_ctx *ctx, const long long *cells, int n, float *X, float *T) {
   if (!ctx || !cells || !X || !T || n <= 0) return EDDY_EINVAL;
+  CellGeom cg;
+  int rc = mlp_geom(ctx, mlp_state(ctx), cg);
+  if (rc) return rc;
   long long *dc = nullptr;
   float *dX = nullptr, *dT = nullptr;
   EDDY_CUDA(cudaMalloc(&dc, sizeof(long long) * n));
@@ -682,7 +725,7 @@ int eddy_closure_harvest(eddy_ctx *ctx, const long long *cells, int n, float *X,
   EDDY_CUDA(cudaMalloc(&dT, sizeof(float) * n));
   EDDY_CUDA(cudaMemcpyAsync(dc, cells, sizeof(long long) * n, cudaMemcpyHostToDevice, ctx->stream));
   const std::vector<double> &xu = ctx->h[0];
-  k_harvest<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->d, ctx->m, ctx->sc.grav, xu[1], xu[ctx->d.ix2],
+  k_harvest<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->d, ctx->m, cg, ctx->sc.grav, xu[1], xu[ctx->d.ix2],
                                                       ctx->f[EDDY_UO], ctx->f[EDDY_VO], ctx->f[EDDY_WO],
                                                       ctx->f[EDDY_DENS], ctx->xc_dev, ctx->f[EDDY_TV], dc, n, dX, dT);
   EDDY_LAUNCHED(ctx);
@@ -806,6 +849,13 @@ int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigne
   }
   const Dims &d = ctx->d;
   const std::vector<double> &xu = ctx->h[0];
+  CellGeom cg;
+  int rc = mlp_geom(ctx, s, cg);
+  if (rc) return rc;
+  if ((long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1) >= (1LL << 32) - 256) {
+    ctx->err = "learned closure: interior larger than 2^32 cells";
+    return EDDY_EINVAL;
+  }
   EDDY_CUDA(cudaMemsetAsync(s->counts, 0, sizeof(unsigned long long), ctx->stream));
   size_t smem = sizeof(InferSmem) + 1024;
   EDDY_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -814,7 +864,7 @@ int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigne
   long long ninner = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
   long long ntiles = (ninner + 127) / 128;
   int grid = (int)std::min<long long>(ntiles, (long long)nsm * 8);
-  k_mlp_infer<<<grid, IT, smem, ctx->stream>>>(d, ctx->m, ctx->sc.grav, xu[1], xu[d.ix2], ctx->f[EDDY_UO],
+  k_mlp_infer<<<grid, IT, smem, ctx->stream>>>(d, ctx->m, cg, ctx->sc.grav, xu[1], xu[d.ix2], ctx->f[EDDY_UO],
                                               ctx->f[EDDY_VO], ctx->f[EDDY_WO], ctx->f[EDDY_DENS], ctx->xc_dev, s->w,
                                               s->theta, s->meta, fallback, ctx->f[EDDY_TV], kappa, s->counts,
                                               ctx->err_flag);

@@ -28,33 +28,11 @@ __device__ __forceinline__ int bitrev(int x, int logn) {
   return (int)(__brev((unsigned)x) >> (32 - logn));
 }
 
-// in-place radix-2 DIT on TI lines stored re[j*TI+ii], im[j*TI+ii] (input in
-// bit-reversed order).  tw*: table exp(s*2 pi i r/L), r < L/2.
-__device__ void fft_lines(double *re, double *im, int L, const double *__restrict__ twr,
-                          const double *__restrict__ twi) {
-  for (int len = 2; len <= L; len <<= 1) {
-    int h = len >> 1, stride = L / len;
-    for (int bf = threadIdx.x; bf < TI * (L >> 1); bf += blockDim.x) {
-      int ii = bf % TI, pidx = bf / TI;
-      int grp = pidx / h, qq = pidx % h;
-      int a = grp * len + qq, b = a + h;
-      double wr = twr[qq * stride], wi = twi[qq * stride];
-      double xr = re[b * TI + ii], xi = im[b * TI + ii];
-      double tr = wr * xr - wi * xi;
-      double ti = wr * xi + wi * xr;
-      double ar = re[a * TI + ii], ai = im[a * TI + ii];
-      re[b * TI + ii] = ar - tr;
-      im[b * TI + ii] = ai - ti;
-      re[a * TI + ii] = ar + tr;
-      im[a * TI + ii] = ai + ti;
-    }
-    __syncthreads();
-  }
-}
+#include "fft_lines.cuh"
 
 // Step 1.  mode 0: f = divergence(us,vs,ws)/alfxdt (src/timeindeg.f:941-949,
 // src/Eddy6.f:2715); mode 1: f = rhs interior.
-__global__ void __launch_bounds__(FT)
+__global__ void __launch_bounds__(FT, 3)
     k_div_fft_fwd(Dims d, DevMetrics m, const double *__restrict__ us, const double *__restrict__ vs,
                   const double *__restrict__ ws, const double *__restrict__ rhs, int mode, double alfxdt,
                   int logL, const double *__restrict__ twr, const double *__restrict__ twi,
@@ -62,28 +40,44 @@ __global__ void __launch_bounds__(FT)
   extern __shared__ double sm[];
   const int L = 1 << logL, M = d.nx - 2;
   double *re = sm, *im = sm + L * TI;
+  double *tsr = sm + 2 * L * TI, *tsi = tsr + L / 2;
+  load_twiddles(tsr, tsi, twr, twi, L / 2);
   int i0 = d.ix1 + blockIdx.x * TI;
   int k = d.kz1 + blockIdx.y;
-  for (int t = threadIdx.x; t < L * TI; t += blockDim.x) {
-    int ii = t % TI, jj = t / TI;
-    int i = i0 + ii, j = d.jy1 + jj;
-    double v = 0.;
-    if (i <= d.ix2) {
-      if (mode == 0) {
-        v = (m.ap[i] * (us[fidx(d, i, j, k)] - us[fidx(d, i - 1, j, k)]) +
-             m.bp[j] * (vs[fidx(d, i, j, k)] - vs[fidx(d, i, j - 1, k)]) +
-             m.cp[k] * (ws[fidx(d, i, j, k)] - ws[fidx(d, i, j, k - 1)]));
-        v = v / alfxdt;
-      } else {
-        v = rhs[fidx(d, i, j, k)];
+  // gathers batched U per thread (loads issued before the shared stores)
+  constexpr int U = 8;
+  const int NT = L * TI;
+  for (int t0 = threadIdx.x; t0 < NT; t0 += FT * U) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT;
+      const int ii = t % TI, jj = t / TI;
+      const int i = i0 + ii, j = d.jy1 + jj;
+      v[u] = 0.;
+      if (t < NT && i <= d.ix2) {
+        if (mode == 0) {
+          double x = (m.ap[i] * (us[fidx(d, i, j, k)] - us[fidx(d, i - 1, j, k)]) +
+                      m.bp[j] * (vs[fidx(d, i, j, k)] - vs[fidx(d, i, j - 1, k)]) +
+                      m.cp[k] * (ws[fidx(d, i, j, k)] - ws[fidx(d, i, j, k - 1)]));
+          v[u] = x / alfxdt;
+        } else {
+          v[u] = rhs[fidx(d, i, j, k)];
+        }
       }
     }
-    int r = bitrev(jj, logL);
-    re[r * TI + ii] = v;
-    im[r * TI + ii] = 0.;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT;
+      if (t < NT) {
+        const int ii = t % TI, r = bitrev(t / TI, logL);
+        re[r * TI + ii] = v[u];
+        im[r * TI + ii] = 0.;
+      }
+    }
   }
   __syncthreads();
-  fft_lines(re, im, L, twr, twi);
+  fft_lines_r22<double, TI>(re, im, logL, tsr, tsi);
   // packed order [a0, a1, b1, ..., a_{L/2}]
   long long lineK = (long long)(k - d.kz1) * L;
   for (int t = threadIdx.x; t < L * TI; t += blockDim.x) {
@@ -102,38 +96,54 @@ __global__ void __launch_bounds__(FT)
 }
 
 // Step 5: (S - dpm[J==0]) / L, Hermitian extension, inverse DIT, real part.
-__global__ void __launch_bounds__(FT)
+__global__ void __launch_bounds__(FT, 3)
     k_fft_bwd(Dims d, const double *__restrict__ spec, const double *__restrict__ dpm, int logL,
               const double *__restrict__ twr, const double *__restrict__ twi, double *__restrict__ dp) {
   extern __shared__ double sm[];
   const int L = 1 << logL, M = d.nx - 2;
   double *re = sm, *im = sm + L * TI;
+  double *tsr = sm + 2 * L * TI, *tsi = tsr + L / 2;
+  load_twiddles(tsr, tsi, twr, twi, L / 2);
   int i0 = d.ix1 + blockIdx.x * TI;
   int k = d.kz1 + blockIdx.y;
   long long lineK = (long long)(k - d.kz1) * L;
   double mean = dpm[0];
-  for (int t = threadIdx.x; t < L * TI; t += blockDim.x) {
-    int ii = t % TI, q = t / TI;  // q: complex index 0..L-1
-    int i = i0 + ii;
-    double xr = 0., xi = 0.;
-    if (i <= d.ix2) {
-      const double *S = spec + (long long)(i - d.ix1);
-      auto get = [&](int J) {
-        double v = S[(long long)M * (J + lineK)];
-        if (J == 0) v = v - mean;
-        return v / (double)L;
-      };
-      if (q == 0) xr = get(0);
-      else if (q == L / 2) xr = get(L - 1);
-      else if (q < L / 2) { xr = get(2 * q - 1); xi = get(2 * q); }
-      else { int qq = L - q; xr = get(2 * qq - 1); xi = -get(2 * qq); }
+  constexpr int U = 8;
+  const int NT = L * TI;
+  for (int t0 = threadIdx.x; t0 < NT; t0 += FT * U) {
+    double xr[U], xi[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT;
+      const int ii = t % TI, q = t / TI;  // q: complex index 0..L-1
+      const int i = i0 + ii;
+      xr[u] = 0.;
+      xi[u] = 0.;
+      if (t < NT && i <= d.ix2) {
+        const double *S = spec + (long long)(i - d.ix1);
+        auto get = [&](int J) {
+          double v = S[(long long)M * (J + lineK)];
+          if (J == 0) v = v - mean;
+          return v / (double)L;
+        };
+        if (q == 0) xr[u] = get(0);
+        else if (q == L / 2) xr[u] = get(L - 1);
+        else if (q < L / 2) { xr[u] = get(2 * q - 1); xi[u] = get(2 * q); }
+        else { const int qq = L - q; xr[u] = get(2 * qq - 1); xi[u] = -get(2 * qq); }
+      }
     }
-    int r = bitrev(q, logL);
-    re[r * TI + ii] = xr;
-    im[r * TI + ii] = xi;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * FT;
+      if (t < NT) {
+        const int ii = t % TI, r = bitrev(t / TI, logL);
+        re[r * TI + ii] = xr[u];
+        im[r * TI + ii] = xi[u];
+      }
+    }
   }
   __syncthreads();
-  fft_lines(re, im, L, twr, twi);
+  fft_lines_r22<double, TI>(re, im, logL, tsr, tsi);
   for (int t = threadIdx.x; t < L * TI; t += blockDim.x) {
     int ii = t % TI, jj = t / TI;
     int i = i0 + ii;
@@ -143,48 +153,7 @@ __global__ void __launch_bounds__(FT)
 }
 
 // Step 3: Thomas along z for each (m,J) line; S laid out [k][J][m].
-__global__ void __launch_bounds__(256)
-    k_tridiag_z(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
-                const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
-                const double *__restrict__ wz, double *__restrict__ g, double *__restrict__ cpr) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)M * L) return;
-  int mi = (int)(t % M), J = (int)(t / M);
-  long long ML = (long long)M * L;
-  int pin = (J == 0 && mi == m0);
-  int s0 = pin ? 1 : 0;
-  double lm = lam[mi], akJ = ak[J];
-  if (pin) {
-    // compatibility of the singular (J=0, constant-x) line: remove the
-    // z-volume-weighted mean so the Neumann system has a solution
-    double sv = 0., vv = 0.;
-    for (int k = 0; k < N; k++) {
-      sv += g[t + ML * k] * wz[k];
-      vv += wz[k];
-    }
-    double cm = sv / vv;
-    for (int k = 0; k < N; k++) g[t + ML * k] = g[t + ML * k] - cm;
-  }
-  double prev_c = 0., prev_d = 0.;
-  for (int k = s0; k < N; k++) {
-    double a = (k == s0) ? 0. : an[k];
-    double b = (bn[k] + lm) - akJ;
-    double den = b - a * prev_c;
-    double c = cn[k] / den;
-    double f = g[t + ML * k];
-    double dd = (f - a * prev_d) / den;
-    cpr[t + ML * k] = c;
-    g[t + ML * k] = dd;
-    prev_c = c;
-    prev_d = dd;
-  }
-  double x = prev_d;
-  for (int k = N - 2; k >= s0; k--) {
-    x = g[t + ML * k] - cpr[t + ML * k] * x;
-    g[t + ML * k] = x;
-  }
-  if (pin) g[t] = 0.;
-}
+#include "tridiag_z.cuh"
 
 // Step 4b: mean of the J = 0 plane (M*N values), deterministic two-stage.
 __global__ void k_plane_sum_partial(int M, int L, int N, const double *__restrict__ s, double *part) {
@@ -285,8 +254,11 @@ int solve_from_spec(eddy_ctx *ctx, double *dp) {
   long long nl = (long long)M * L;
   {
     ProfScope ps(ctx, PROF_TRIDIAG);
-    k_tridiag_z<<<(unsigned)((nl + 255) / 256), 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.lam, pp.ak, pp.an,
-                                                                       pp.bn, pp.cn, pp.wz, pp.spec2, pp.cprime);
+    k_line_mean<double><<<1, 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.wz, pp.spec2, ctx->scal + 5);
+    EDDY_LAUNCHED(ctx);
+    // the eliminated right-hand side overwrites the spectrum in place
+    k_tridiag_lines<double><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
+        M, L, N, pp.m0, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, pp.spec2, pp.cprime, pp.spec2);
     EDDY_LAUNCHED(ctx);
   }
   {
@@ -303,7 +275,7 @@ int solve_from_spec(eddy_ctx *ctx, double *dp) {
   EDDY_LAUNCHED(ctx);
   int logL = 0;
   while ((1 << logL) < L) logL++;
-  size_t smem = sizeof(double) * 2 * L * TI;
+  size_t smem = sizeof(double) * (2 * L * TI + L);
   dim3 g((M + TI - 1) / TI, N);
   k_fft_bwd<<<g, FT, smem, ctx->stream>>>(d, pp.spec, ctx->scal + 3, logL, pp.twr + L / 2, pp.twi + L / 2, dp);
   EDDY_LAUNCHED(ctx);
@@ -409,7 +381,7 @@ int poisson_plan_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMemcpy(pp.wz, wz.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.twr, twr.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.twi, twi.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
-  size_t smem = sizeof(double) * 2 * L * TI;
+  size_t smem = sizeof(double) * (2 * L * TI + L);
   if (smem > 48 * 1024) {
     EDDY_CUDA(cudaFuncSetAttribute(k_div_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     EDDY_CUDA(cudaFuncSetAttribute(k_fft_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -432,7 +404,7 @@ static int fwd(eddy_ctx *ctx, const double *us, const double *vs, const double *
   const Dims &d = ctx->d;
   int logL = 0;
   while ((1 << logL) < pp.L) logL++;
-  size_t smem = sizeof(double) * 2 * pp.L * TI;
+  size_t smem = sizeof(double) * (2 * pp.L * TI + pp.L);
   dim3 g((pp.M + TI - 1) / TI, pp.N);
   ProfScope ps(ctx, PROF_DIV_FFT);
   k_div_fft_fwd<<<g, FT, smem, ctx->stream>>>(d, ctx->m, us, vs, ws, rhs, mode, alfxdt, logL, pp.twr, pp.twi,

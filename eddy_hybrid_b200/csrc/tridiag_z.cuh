@@ -1,0 +1,94 @@
+// tridiag_z.cuh -- per-wavenumber line solves along the stretched z axis of
+// the Poisson solve (the z direction of src/direct.f's block-tridiagonal
+// systems after the x eigen-transform): for every (m, J) line
+//   an(k) x(k-1) + (bn(k) + lambda_m - AK(J)) x(k) + cn(k) x(k+1) = g(k).
+// Thomas elimination in FP64 arithmetic; the right-hand side and solution are
+// stored as G (double for the plain form, float for the mixed form's
+// correction solves), the eliminated right-hand side dd in FP64.
+// The singular line (J = 0, m = m0, the constant x mode) is made compatible by
+// removing its z-volume-weighted mean (computed by k_line_mean) and pinned by
+// dropping its first equation; its first entry is set to zero.
+// dd may alias g (plain form: in place).  Loads are issued in chunks of ZC planes ahead of the recurrence so each
+// thread keeps several memory requests in flight.
+#pragma once
+
+constexpr int ZC = 8;
+
+// weighted mean of the singular line: out = sum_k g(m0,0,k) wz(k) / sum_k wz(k)
+template <class G>
+__global__ void k_line_mean(int M, int L, int N, int m0, const double *__restrict__ wz, const G *__restrict__ g,
+                            double *out) {
+  __shared__ double s1[256], s2[256];
+  double a = 0., b = 0.;
+  long long ML = (long long)M * L;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    a += (double)g[m0 + ML * k] * wz[k];
+    b += wz[k];
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = s1[0] / s2[0];
+}
+
+template <class G>
+__global__ void __launch_bounds__(128)
+    k_tridiag_lines(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
+                    const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
+                    const double *__restrict__ cmean, G *g, double *__restrict__ cpr, double *dd) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)M * L) return;
+  const int mi = (int)(t % M), J = (int)(t / M);
+  const long long ML = (long long)M * L;
+  const bool pin = (J == 0 && mi == m0);
+  const int s0 = pin ? 1 : 0;
+  const double shift = lam[mi] - ak[J];
+  const double cm = pin ? cmean[0] : 0.;
+  double pc = 0., pd = 0.;
+  for (int k0 = s0; k0 < N; k0 += ZC) {
+    double fv[ZC];
+#pragma unroll
+    for (int q = 0; q < ZC; q++) fv[q] = (k0 + q < N) ? (double)g[t + ML * (k0 + q)] : 0.;
+#pragma unroll
+    for (int q = 0; q < ZC; q++) {
+      const int k = k0 + q;
+      if (k < N) {
+        const double a = (k == s0) ? 0. : an[k];
+        const double rden = 1.0 / ((bn[k] + shift) - a * pc);
+        const double c = cn[k] * rden;
+        const double e = ((fv[q] - cm) - a * pd) * rden;
+        cpr[t + ML * k] = c;
+        dd[t + ML * k] = e;
+        pc = c;
+        pd = e;
+      }
+    }
+  }
+  double x = pd;
+  g[t + ML * (N - 1)] = (G)x;
+  for (int k1 = N - 2; k1 >= s0; k1 -= ZC) {
+    double cv[ZC], ev[ZC];
+#pragma unroll
+    for (int q = 0; q < ZC; q++) {
+      const int k = k1 - q;
+      cv[q] = k >= s0 ? cpr[t + ML * k] : 0.;
+      ev[q] = k >= s0 ? dd[t + ML * k] : 0.;
+    }
+#pragma unroll
+    for (int q = 0; q < ZC; q++) {
+      const int k = k1 - q;
+      if (k >= s0) {
+        x = ev[q] - cv[q] * x;
+        g[t + ML * k] = (G)x;
+      }
+    }
+  }
+  if (pin) g[t] = (G)0.;
+}
