@@ -87,6 +87,16 @@ SIGNATURES = {
     "eddy_poisson_solve": ([C.c_void_p, _DP, _DP, C.c_int], C.c_int),
     "eddy_max_divergence": ([C.c_void_p, _DP], C.c_int),
     "eddy_refine_residuals": ([C.c_void_p, _DP, C.c_int], C.c_int),
+    "eddy_ib_set_body": ([C.c_void_p, C.c_int, _DP, _DP, _DP], C.c_int),
+    "eddy_ib_move": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_ib_set_cadence": ([C.c_void_p, C.c_int], C.c_int),
+    "eddy_ib_regen": ([C.c_void_p], C.c_int),
+    "eddy_ib_momforc": ([C.c_void_p], C.c_int),
+    "eddy_ib_correct": ([C.c_void_p, C.c_int], C.c_int),
+    "eddy_ib_flags": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
+    "eddy_ib_limits": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "eddy_ib_stencils": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
+                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "eddy_profile_enable": ([C.c_void_p, C.c_uint], C.c_int),
     "eddy_profile_read": ([C.c_void_p, _DP, C.POINTER(C.c_longlong)], C.c_int),
     "eddy_max_divergence_noalloc": ([C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -218,6 +228,43 @@ class Solver:
         self._check(lib().eddy_max_divergence(self.h, C.byref(v)), "eddy_max_divergence")
         return v.value
 
+    # ---- immersed body ----
+    def set_body(self, tri: np.ndarray, normals: np.ndarray, velocity=(0.0, 0.0, 0.0)):
+        # C order [triangle][vertex][x, y, z] and [triangle][x, y, z]
+        tri = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1)
+        nrm = np.ascontiguousarray(normals, dtype=np.float64).reshape(-1)
+        vel = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
+        self._check(lib().eddy_ib_set_body(self.h, len(tri) // 9, _ptr(tri), _ptr(nrm), _ptr(vel)),
+                    "eddy_ib_set_body")
+
+    def ib_flags(self, which: int) -> np.ndarray:
+        out = np.zeros(self.shape[0] * self.shape[1] * self.shape[2], dtype=np.int8)
+        self._check(lib().eddy_ib_flags(self.h, which, out.ctypes.data_as(C.c_void_p)), "eddy_ib_flags")
+        return out.reshape(self.shape, order="F")
+
+    def ib_limits(self):
+        lim = (C.c_int * 6)()
+        self._check(lib().eddy_ib_limits(self.h, lim), "eddy_ib_limits")
+        return tuple(lim)
+
+    def ib_stencils(self, q: int) -> dict:
+        n, nl = C.c_int(0), C.c_int(0)
+        self._check(lib().eddy_ib_stencils(self.h, q, C.byref(n), C.byref(nl), None, None, None, None, None, None),
+                    "eddy_ib_stencils")
+        m = n.value
+        ijk = np.zeros(3 * max(m, 1), np.int32)
+        dijk = np.zeros(3 * max(m, 1), np.int32)
+        lev = np.zeros(max(m, 1), np.int32)
+        xn = np.zeros(3 * max(m, 1))
+        lu = np.zeros(4 * max(m, 1))
+        indx = np.zeros(2 * max(m, 1), np.int32)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        self._check(lib().eddy_ib_stencils(self.h, q, C.byref(n), C.byref(nl), vp(ijk), vp(dijk), vp(lev), vp(xn),
+                                           vp(lu), vp(indx)), "eddy_ib_stencils")
+        return {"n": m, "nlev": nl.value, "ijk": ijk[:3 * m].reshape(m, 3), "dijk": dijk[:3 * m].reshape(m, 3),
+                "lev": lev[:m], "xn": xn[:3 * m].reshape(m, 3), "lu": lu[:4 * m].reshape(m, 4),
+                "indx": indx[:2 * m].reshape(m, 2)}
+
     def refine_residuals(self) -> np.ndarray:
         """max |d - L phi| before each refinement sweep of the last mixed solve."""
         out = np.zeros(4)
@@ -227,14 +274,14 @@ class Solver:
     PROFILE_CATEGORIES = ["rhs_predictor", "boundary", "div_fft_fwd", "transform_fwd",
                           "z_line_solve", "transform_bwd", "fft_bwd", "correct",
                           "pressure_update", "density", "eddy_viscosity", "refine_residual",
-                          "precision_copy"]
+                          "precision_copy", "ib_regen", "ib_force"]
 
-    def profile_enable(self, mask: int = 0x1FFF):
+    def profile_enable(self, mask: int = 0x7FFF):
         self._check(lib().eddy_profile_enable(self.h, mask), "eddy_profile_enable")
 
     def profile_read(self) -> dict:
-        ms = (C.c_double * 13)()
-        n = (C.c_longlong * 13)()
+        ms = (C.c_double * 15)()
+        n = (C.c_longlong * 15)()
         self._check(lib().eddy_profile_read(self.h, ms, n), "eddy_profile_read")
         return {c: (ms[i], n[i]) for i, c in enumerate(self.PROFILE_CATEGORIES)}
 

@@ -28,6 +28,7 @@ UNITS = {
     "k_mlp.cu": [],
     "k_mixed.cu": [],
     "k_xform.cu": [],
+    "k_ib.cu": ["-fmad=false"],
     "host_eigen.cpp": [],
 }
 

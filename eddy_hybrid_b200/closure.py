@@ -2,8 +2,11 @@
 training-data harvesting and training driver over the C ABI.
 
 The network (12 -> 64 -> 64 -> 64 -> 2, SiLU hidden, softplus outputs) maps
-local, filter-width-scaled velocity- and density-gradient features to
-nu_t/Delta and kappa_t/Delta.  It stands in for the test filtering and
+local, filter-width-scaled velocity- and density-gradient features to the
+eddy-viscosity and diffusivity coefficients C_nu, C_kappa of
+nu_t = C_nu Delta^2 |S| and kappa_t = C_kappa Delta^2 |S| (|S| from the same
+gradient features), the form of the dynamic procedure's result, so the
+closure scales with the local strain like the model it replaces.  It stands in for the test filtering and
 coefficient averaging of the dynamic procedure (src/vt.f:172-431); targets
 come from that procedure run by the plain solver itself, and kappa_t = nu_t
 as in the reference's build (src/Eddy6.f:2959 passes TV as the diffusivity).
@@ -52,23 +55,45 @@ def init_theta(seed: int = 0) -> np.ndarray:
     return th
 
 
+def strain_scale(X: np.ndarray) -> np.ndarray:
+    """Delta*|S| = Delta*sqrt(2 S_ij S_ij) from the nine Delta-scaled
+    velocity-gradient features (row a, column b: Delta du_a/dx_b)."""
+    g = X[:, :9].reshape(-1, 3, 3).astype(np.float64)
+    S = 0.5 * (g + np.transpose(g, (0, 2, 1)))
+    return np.sqrt(2.0 * np.sum(S * S, axis=(1, 2)))
+
+
+def coefficients(X: np.ndarray, T: np.ndarray):
+    """Dynamic coefficient C = (nu_t/Delta) / (Delta|S|) of each sample and a
+    mask of the samples where |S| is large enough to define it."""
+    q = strain_scale(X)
+    ok = q > 1e-8 * max(float(np.median(q)), 1e-30)
+    C = np.zeros_like(q)
+    C[ok] = T[ok].astype(np.float64) / q[ok]
+    return C, ok
+
+
 def make_meta(X: np.ndarray, T: np.ndarray, margin: float = 1.0) -> np.ndarray:
     """Feature mean/std, the training envelope (min/max of the normalised
-    features widened by `margin` standard deviations) and output scales."""
+    features widened by `margin` standard deviations) and coefficient scales."""
     mean = X.mean(axis=0)
     std = X.std(axis=0)
     std[std < 1e-12] = 1.0
     Z = (X - mean) / std
     lo = Z.min(axis=0) - margin
     hi = Z.max(axis=0) + margin
-    s = float(np.sqrt(np.mean(T.astype(np.float64) ** 2))) or 1.0
+    C, ok = coefficients(X, T)
+    s = float(np.sqrt(np.mean(C[ok] ** 2))) if ok.any() else 1.0
+    s = s or 1.0
     return np.concatenate([mean, 1.0 / std, lo, hi, [s, s]]).astype(np.float32)
 
 
-def targets(T: np.ndarray, meta: np.ndarray) -> np.ndarray:
-    """Network targets (nu_t/Delta, kappa_t/Delta) in output-scale units."""
+def targets(X: np.ndarray, T: np.ndarray, meta: np.ndarray):
+    """Network targets (C_nu, C_kappa in output-scale units) for the samples
+    where the coefficient is defined, and their mask."""
     s_nu, s_ka = meta[4 * NFEAT], meta[4 * NFEAT + 1]
-    return np.stack([T / s_nu, T / s_ka], axis=1).astype(np.float32)
+    C, ok = coefficients(X, T)
+    return np.stack([C / s_nu, C / s_ka], axis=1).astype(np.float32), ok
 
 
 def sample_cells(workload, n: int, seed: int) -> np.ndarray:

@@ -230,6 +230,7 @@ void free_all(eddy_ctx *ctx) {
   poisson_plan_destroy(ctx);
   mlp_release(ctx);
   mixed_release(ctx);
+  ib_release(ctx);
   double *o2[] = {ctx->xc_dev, ctx->kappa, ctx->tv_dyn};
   for (double *p : o2) if (p) cudaFree(p);
   for (ProfEvent &e : ctx->prof_ev) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -494,6 +495,59 @@ int eddy_turvis(eddy_ctx *ctx) {
   return rc;
 }
 
+int eddy_ib_set_body(eddy_ctx *ctx, int nb, const double *vertices, const double *normals,
+                     const double *velocity) {
+  if (check_ctx(ctx) || nb < 0 || (nb > 0 && (!vertices || !normals))) return EDDY_EINVAL;
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return ib_set_body(ctx, nb, vertices, normals, velocity);
+}
+
+int eddy_ib_set_cadence(eddy_ctx *ctx, int every_substep) {
+  if (check_ctx(ctx) || !ctx->ib) return EDDY_EINVAL;
+  return ib_set_cadence(ctx, every_substep);
+}
+
+int eddy_ib_move(eddy_ctx *ctx, double tmove) {
+  if (check_ctx(ctx) || !ctx->ib) return EDDY_EINVAL;
+  return ib_move(ctx, tmove);
+}
+
+int eddy_ib_regen(eddy_ctx *ctx) {
+  if (check_ctx(ctx) || !ctx->ib) return EDDY_EINVAL;
+  return ib_regen(ctx);
+}
+
+int eddy_ib_momforc(eddy_ctx *ctx) {
+  if (check_ctx(ctx) || !ctx->ib) return EDDY_EINVAL;
+  const double *vb = ib_velocity(ctx);
+  double **f = ctx->f;
+  int rc;
+  if ((rc = ib_force(ctx, 0, 0, f[EDDY_US], vb[0], vb[0], nullptr, 0))) return rc;
+  if ((rc = ib_force(ctx, 1, 1, f[EDDY_VS], vb[1], vb[1], nullptr, 0))) return rc;
+  return ib_force(ctx, 2, 2, f[EDDY_WS], vb[2], vb[2], nullptr, 0);
+}
+
+int eddy_ib_correct(eddy_ctx *ctx, int field) {
+  if (check_ctx(ctx) || !ctx->ib || (field != EDDY_P && field != EDDY_DENS)) return EDDY_EINVAL;
+  return ib_force(ctx, 3, 4, ctx->f[field], 0.0, 0.0, nullptr, 0);
+}
+
+int eddy_ib_flags(eddy_ctx *ctx, int which, signed char *out) {
+  if (check_ctx(ctx) || !ctx->ib || !out) return EDDY_EINVAL;
+  return ib_download(ctx, which, out);
+}
+
+int eddy_ib_limits(eddy_ctx *ctx, int *lim6) {
+  if (check_ctx(ctx) || !ctx->ib || !lim6) return EDDY_EINVAL;
+  return ib_limits(ctx, lim6);
+}
+
+int eddy_ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn,
+                     double *lu, int *indx) {
+  if (check_ctx(ctx) || !ctx->ib) return EDDY_EINVAL;
+  return ib_stencils(ctx, q, n, nlev, ijk, dijk, lev, xn, lu, indx);
+}
+
 int eddy_refine_residuals(eddy_ctx *ctx, double *out, int n) {
   if (check_ctx(ctx) || !out || n < 1) return EDDY_EINVAL;
   if (!ctx->mixed) {
@@ -560,12 +614,27 @@ int eddy_substep(eddy_ctx *ctx, int is, double dt) {
   double gam[3], rho[3], alf[3];
   scheme(ctx->prm.ischm, gam, rho, alf);
   double alfxdt = alf[is] * dt, gamxdt = gam[is] * dt, rhoxdt = rho[is] * dt;
+  int rc;
+  // moving body: RBM, then new tags and stencils (src/Eddy6.f:2163-2380), every
+  // substep over alfxdt, or at the first substep over the whole step
+  if (ctx->ib && (ib_every_substep(ctx) || is == 0)) {
+    ProfScope ps(ctx, PROF_IB_REGEN);
+    if ((rc = ib_move(ctx, ib_every_substep(ctx) ? alfxdt : dt))) return rc;
+    if ((rc = ib_regen(ctx))) return rc;
+  }
   if (ctx->mixed) return mixed_substep(ctx, alfxdt, gamxdt, rhoxdt);
   double **f = ctx->f;
-  int rc;
   {
     ProfScope ps(ctx, PROF_RHS_PRED);
     if ((rc = launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt))) return rc;
+  }
+  // momforc_mod2 + velinterior (src/Eddy6.f:2526-2575)
+  if (ctx->ib) {
+    ProfScope ps(ctx, PROF_IB_FORCE);
+    const double *vb = ib_velocity(ctx);
+    if ((rc = ib_force(ctx, 0, 0, f[EDDY_US], vb[0], vb[0], nullptr, 0))) return rc;
+    if ((rc = ib_force(ctx, 1, 1, f[EDDY_VS], vb[1], vb[1], nullptr, 0))) return rc;
+    if ((rc = ib_force(ctx, 2, 2, f[EDDY_WS], vb[2], vb[2], nullptr, 0))) return rc;
   }
   {
     ProfScope ps(ctx, PROF_BC);
@@ -619,6 +688,8 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
         }
         if (rc) return rc;
       }
+      // tvinterior (src/Eddy6.f:3040-3042)
+      if (ctx->ib && (rc = ib_interior(ctx, 3, ctx->f[EDDY_TV], 0.0))) return rc;
       if (ctx->mixed && (rc = mixed_after_sgs(ctx))) return rc;
     }
   }

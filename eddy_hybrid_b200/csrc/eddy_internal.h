@@ -57,7 +57,8 @@ struct PoissonPlan {
 // kernel categories timed with CUDA events when profiling is enabled
 enum {
   PROF_RHS_PRED = 0, PROF_BC, PROF_DIV_FFT, PROF_GEMM_FWD, PROF_TRIDIAG, PROF_GEMM_BWD, PROF_FFT_BWD,
-  PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_REFINE, PROF_CONVERT, PROF_NCAT
+  PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_REFINE, PROF_CONVERT, PROF_IB_REGEN,
+  PROF_IB_FORCE, PROF_NCAT
 };
 
 struct TmaEntry {
@@ -97,6 +98,8 @@ struct eddy_ctx {
   double *tv_dyn = nullptr;     // last dynamic-model nu_t: closure fallback (NX,NY,NZ)
   void *mlp = nullptr;          // closure network state (k_mlp.cu)
   void *mixed = nullptr;        // FP32 field set of the mixed-precision form (k_mixed.cu)
+  void *ib = nullptr;           // immersed body state (k_ib.cu)
+  double *ibax[6] = {};         // device xu, xc, yv, yc, zw, zc (1-based) for the body kernels
   long long closure_out = 0, closure_cells = 0, closure_refresh = 0;
   // profiling (CUDA events on the context stream around each category)
   unsigned prof_mask = 0;
@@ -183,6 +186,25 @@ int launch_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp);
 int launch_max_divergence(eddy_ctx *ctx, double *out_host);
 // DIRECT's ghost convention on a solution array (z planes zero, x Neumann, y periodic)
 int launch_dp_ghost(eddy_ctx *ctx, double *dp);
+
+// immersed boundary (k_ib.cu).  Stencil sets q: 0 u, 1 v, 2 w, 3 p; flag
+// arrays fq: 0 u, 1 v, 2 w, 3 tv (taguo), 4 p (flagp)
+int ib_set_body(eddy_ctx *ctx, int nb, const double *vert, const double *normals, const double *vel);
+int ib_release(eddy_ctx *ctx);
+int ib_move(eddy_ctx *ctx, double tmove);
+int ib_regen(eddy_ctx *ctx);
+// forcing of a by set q, then `interior` where flag fq == 1; mirror (FP32,
+// row pitch mpitch) receives every written value when non-null
+int ib_force(eddy_ctx *ctx, int q, int fq, double *a, double b0, double interior, float *mirror, int mpitch);
+int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, double interior);
+const double *ib_velocity(eddy_ctx *ctx);
+int ib_set_cadence(eddy_ctx *ctx, int every_substep);
+int ib_every_substep(eddy_ctx *ctx);
+int ib_interior(eddy_ctx *ctx, int fq, double *a, double value);
+int ib_download(eddy_ctx *ctx, int which, signed char *out);
+int ib_limits(eddy_ctx *ctx, int *lim6);
+int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
+                int *indx);
 
 // tensor-core (3xTF32) eigen-transforms of the mixed solve (k_xform.cu):
 // B matrices from a column-major FP64 M x M transform; out = in * B^T

@@ -90,5 +90,8 @@ int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   double *t = ctx->f[EDDY_DENS];
   ctx->f[EDDY_DENS] = ctx->dens_alt;
   ctx->dens_alt = t;
-  return launch_boundinoutd_dens(ctx, ctx->f[EDDY_DENS]);
+  if ((rc = launch_boundinoutd_dens(ctx, ctx->f[EDDY_DENS]))) return rc;
+  // immersed body: correctdens_mod2 + densinterior (src/Eddy6.f:2972-2983)
+  if (ctx->ib) return ib_force(ctx, 3, 4, ctx->f[EDDY_DENS], 0.0, 0.0, nullptr, 0);
+  return EDDY_OK;
 }

@@ -1,0 +1,1443 @@
+// k_ib.cu -- immersed boundary on the GPU: body motion, cell tagging by ray
+// casting, interior / forcing / fluid flags, forcing-point lists, grid-line
+// interpolation stencils with their 2x2 systems, and the forcing itself.
+//
+//   RBM (translation)      src/rbm.f:2-40
+//   LIMIMB                 src/object.f:713-800
+//   TAG3D_MOD, segtriint,  src/rt.f:2704-3020, 1179-1226, 1263-1330
+//   intersect_triangle
+//   taguo / flagp          src/devel.f:8-110, src/matint.f:135-260
+//   forcpts                src/matint.f:3388-3430 (k, j, i order)
+//   geom_mod / grid_intr   src/devel.f:9265-9800, src/matint.f:800-1160
+//   mtrx, ludcmp, lubksb   src/devel.f:1159-1290, src/numrec.f:22-118 (n = 2)
+//   momforc_mod2           src/momforc.f:1248-1485 (explicit)
+//   correctpres_mod2 /     src/momforc.f:1617-1900
+//   correctdens_mod2
+//   velinterior, presinterior, densinterior, tvinterior
+//
+// Restatement choices (shared with the CPU oracle): every triangle whose xy
+// box holds a column is tested by TAG3D (found through a 2-D bin grid instead
+// of the reference's kd-tree); every forcing point takes the grid-line
+// stencil (grid_intr) with exact 3/5/25-nearest-centroid candidate lists
+// (3-D bin grid; ties by triangle index); dependency loops resolve points
+// whose extension point is a forcing point; points without a stencil are
+// dropped.  The geometry kernels are compiled with -fmad=false so every
+// intersection, distance and LU factor matches the oracle bit for bit.
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bc_templates.cuh"
+#include "eddy_internal.h"
+
+namespace {
+
+constexpr int NCR = 16;     // crossings kept per column
+constexpr int NNTR3D = 25;  // largest candidate list of grid_intr
+constexpr int NFLU = 30;    // dependency loops
+constexpr int B2 = 256;     // 2-D bins per axis (tagging)
+constexpr int B3 = 64;      // 3-D bins per axis (nearest centroids)
+
+struct Box6 {
+  int imin, imax, jmin, jmax, kmin, kmax;
+};
+
+struct Bins {
+  double lo[3], hi[3], inv[3];  // bin grid over the box lo..hi
+  int nb[3];
+  int *start = nullptr, *items = nullptr, *cursor = nullptr;
+  int nitems = 0, cap = 0;
+};
+
+// stencils of one variable (device arrays) and host level offsets
+struct StencilSet {
+  int n = 0, nlev = 0, cap = 0;
+  int *ijk = nullptr, *dijk = nullptr, *lev = nullptr, *indx = nullptr;
+  double *xn = nullptr, *lu = nullptr;
+  std::vector<int> lev_start;
+};
+
+struct IbState {
+  int nb = 0;
+  double *v = nullptr, *c = nullptr, *n = nullptr;  // [nb*9], [nb*3], [nb*3]
+  double vel[3] = {0, 0, 0};
+  double *red = nullptr;                            // reduction scratch
+  int *dlim = nullptr;                              // device LIMIMB result
+  Box6 lim{};
+  signed char *tag[4] = {};   // TAG3D results u, v, w, p
+  signed char *flag[5] = {};  // taguo u, v, w, tv; flagp p
+  signed char *work = nullptr;
+  Bins b2, b3;
+  // per-point scratch of the geometry search
+  int *pts = nullptr, *status = nullptr, *ddx = nullptr, *order = nullptr, *cnt = nullptr;
+  double *xnp = nullptr, *lup = nullptr;
+  int *indxp = nullptr;
+  int pcap = 0;
+  StencilSet set[4];
+  int *hcnt = nullptr;  // pinned host counters
+  bool ready = false;
+  int every_substep = 0;  // 1: move + regenerate every substep (IBM > 1), 0: once per step
+  // persistent scratch (grown on demand, never freed during a run)
+  enum { S_BINCNT = 0, S_BCNT, S_BOFF, S_CUR, S_STATUS, S_LEV, S_DD, S_ORDER, S_CNT, S_BSUM, S_NI };
+  int *si[S_NI] = {};
+  size_t si_cap[S_NI] = {};
+  double *sxn = nullptr;
+  size_t sxn_cap = 0;
+};
+
+IbState *ibs(eddy_ctx *ctx) { return static_cast<IbState *>(ctx->ib); }
+
+__host__ __device__ inline long long lidx(int nx, int ny, int i, int j, int k) {
+  return (long long)(i - 1) + (long long)nx * ((long long)(j - 1) + (long long)ny * (long long)(k - 1));
+}
+
+// coordinate arrays of variable q: u (xu, yc, zc), v (xc, yv, zc), w (xc, yc, zw), p (xc, yc, zc)
+struct Axes {
+  const double *x, *y, *z;
+};
+
+// ---------------------------------------------------------------------------
+// geometry primitives (identical operations to the oracle)
+__device__ __forceinline__ void sub3(double *r, const double *a, const double *b) {
+  r[0] = a[0] - b[0];
+  r[1] = a[1] - b[1];
+  r[2] = a[2] - b[2];
+}
+__device__ __forceinline__ void cross3(double *r, const double *x, const double *y) {
+  r[0] = x[1] * y[2] - y[1] * x[2];
+  r[1] = x[2] * y[0] - y[2] * x[0];
+  r[2] = x[0] * y[1] - y[0] * x[1];
+}
+__device__ __forceinline__ double dot3(const double *x, const double *y) {
+  return x[0] * y[0] + x[1] * y[1] + x[2] * y[2];
+}
+
+__device__ int intersect_triangle(const double *orig, const double *dir, const double *v0, const double *v1,
+                                  const double *v2, double &t) {
+  double e1[3], e2[3], pv[3], tv[3], qv[3];
+  t = 0.;
+  sub3(e1, v1, v0);
+  sub3(e2, v2, v0);
+  cross3(pv, dir, e2);
+  double det = dot3(e1, pv);
+  if (det > -1.0e-18 && det < 1.0e-18) return 2;
+  double inv = 1.0 / det;
+  sub3(tv, orig, v0);
+  double u = dot3(tv, pv) * inv;
+  if (u < 0.0 || u > 1.0) return 3;
+  cross3(qv, tv, e1);
+  double v = dot3(dir, qv) * inv;
+  if (v < 0.0 || (u + v - 1.) > 1.e-07) return 3;
+  t = dot3(e2, qv) * inv;
+  return 1;
+}
+
+__device__ bool segtriint(const double *p1, const double *p2, const double *tri, double *xm) {
+  double q[3] = {p1[0], p1[1], p1[2]}, r[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
+  double t;
+  int code = intersect_triangle(q, r, tri, tri + 3, tri + 6, t);
+  if (code == 1 && (t > 1.0 || t < 0.0)) return false;
+  if (code == 2) code = intersect_triangle(q, r, tri, tri + 6, tri + 3, t);
+  xm[0] = q[0] + t * r[0];
+  xm[1] = q[1] + t * r[1];
+  xm[2] = q[2] + t * r[2];
+  return code == 1;
+}
+
+__device__ int locate(const double *xx1, int n, double x) {
+  int jl = 0, ju = n + 1;
+  if (xx1[1] == x) return 1;
+  const bool asc = xx1[n] > xx1[1];
+  while (ju - jl > 1) {
+    int jm = (ju + jl) / 2;
+    if (asc == (x > xx1[jm]))
+      jl = jm;
+    else
+      ju = jm;
+  }
+  return jl;
+}
+
+// ---------------------------------------------------------------------------
+// RBM: translate vertices, recompute centroids
+__global__ void k_move(int nb, double *v, double *c, double dx, double dy, double dz) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  double *tv = v + 9 * t;
+  const double d[3] = {dx, dy, dz};
+  for (int a = 0; a < 3; a++)
+    for (int q = 0; q < 3; q++) tv[3 * a + q] = tv[3 * a + q] + d[q];
+  for (int q = 0; q < 3; q++) c[3 * t + q] = ((tv[q] + tv[3 + q]) + tv[6 + q]) / 3.0;
+}
+
+__global__ void k_centroids(int nb, const double *v, double *c) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const double *tv = v + 9 * t;
+  for (int q = 0; q < 3; q++) c[3 * t + q] = ((tv[q] + tv[3 + q]) + tv[6 + q]) / 3.0;
+}
+
+// min/max of centroid x, z and of vertex x, y, z: exact, through order-
+// preserving 64-bit keys and integer atomics (any block order gives the same
+// result).  keys[0..9]: min cx, max cx, min cz, max cz, min/max vx, vy, vz.
+__device__ __forceinline__ long long okey(double x) {
+  long long b = __double_as_longlong(x);
+  return b >= 0 ? b : b ^ 0x7fffffffffffffffLL;
+}
+__device__ __forceinline__ double okey_inv(long long k) {
+  return __longlong_as_double(k >= 0 ? k : k ^ 0x7fffffffffffffffLL);
+}
+
+__global__ void k_bounds_init(long long *keys) {
+  if (threadIdx.x < 10) keys[threadIdx.x] = (threadIdx.x & 1) ? okey(-1e300) : okey(1e300);
+}
+
+__global__ void k_body_bounds(int nb, const double *v, const double *c, long long *keys) {
+  double r[10] = {1e300, -1e300, 1e300, -1e300, 1e300, -1e300, 1e300, -1e300, 1e300, -1e300};
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+    r[0] = fmin(r[0], c[3 * t]);
+    r[1] = fmax(r[1], c[3 * t]);
+    r[2] = fmin(r[2], c[3 * t + 2]);
+    r[3] = fmax(r[3], c[3 * t + 2]);
+    for (int a = 0; a < 3; a++)
+      for (int q = 0; q < 3; q++) {
+        r[4 + 2 * q] = fmin(r[4 + 2 * q], v[9 * t + 3 * a + q]);
+        r[5 + 2 * q] = fmax(r[5 + 2 * q], v[9 * t + 3 * a + q]);
+      }
+  }
+  for (int q = 0; q < 10; q++) {
+    double x = r[q];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_xor_sync(0xffffffffu, x, off);
+      x = (q & 1) ? fmax(x, o) : fmin(x, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      if (q & 1)
+        atomicMax(&keys[q], okey(x));
+      else
+        atomicMin(&keys[q], okey(x));
+    }
+  }
+}
+
+__global__ void k_bounds_decode(const long long *keys, double *out) {
+  if (threadIdx.x < 10) out[threadIdx.x] = okey_inv(keys[threadIdx.x]);
+}
+
+// LIMIMB (src/object.f:713-800): X = xu, Z = zw, Cartesian, one rank
+__global__ void k_limimb(Dims d, const double *xu, const double *zw, const double *zc, const double *bnd,
+                         int *lim) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double mnx = bnd[0], mxx = bnd[1], mnz = bnd[2], mxz = bnd[3];
+  int imin = locate(xu, d.nx, mnx), imax = locate(xu, d.nx, mxx);
+  int kmin = d.nz, kmax = 1;
+  if (mnz < zw[d.nz] && mxz >= zc[1]) {
+    kmin = locate(zw, d.nz, mnz);
+    kmax = locate(zw, d.nz, mxz);
+  }
+  imin -= 3;
+  imax += 3;
+  if (imin < 1) imin = 1;
+  if (imax > d.nx - 1) imax = d.nx - 1;
+  if (kmax >= kmin) {
+    kmin -= 3;
+    kmax += 3;
+  }
+  if (kmin < 1) kmin = 1;
+  if (kmax > d.nz) kmax = d.nz;
+  lim[0] = imin; lim[1] = imax; lim[2] = 2; lim[3] = d.ny - 1; lim[4] = kmin; lim[5] = kmax;
+}
+
+// ---------------------------------------------------------------------------
+// bin grids (triangle xy boxes in 2-D, centroids in 3-D)
+__global__ void k_bin2_count(int nb, const double *v, Bins b, int *cnt) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const double *tv = v + 9 * t;
+  double x0 = fmin(fmin(tv[0], tv[3]), tv[6]), x1 = fmax(fmax(tv[0], tv[3]), tv[6]);
+  double y0 = fmin(fmin(tv[1], tv[4]), tv[7]), y1 = fmax(fmax(tv[1], tv[4]), tv[7]);
+  int bx0 = min(max((int)((x0 - b.lo[0]) * b.inv[0]), 0), b.nb[0] - 1);
+  int bx1 = min(max((int)((x1 - b.lo[0]) * b.inv[0]), 0), b.nb[0] - 1);
+  int by0 = min(max((int)((y0 - b.lo[1]) * b.inv[1]), 0), b.nb[1] - 1);
+  int by1 = min(max((int)((y1 - b.lo[1]) * b.inv[1]), 0), b.nb[1] - 1);
+  for (int by = by0; by <= by1; by++)
+    for (int bx = bx0; bx <= bx1; bx++) atomicAdd(&cnt[bx + b.nb[0] * by], 1);
+}
+
+__global__ void k_bin2_fill(int nb, const double *v, Bins b, int *cursor, int *items) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const double *tv = v + 9 * t;
+  double x0 = fmin(fmin(tv[0], tv[3]), tv[6]), x1 = fmax(fmax(tv[0], tv[3]), tv[6]);
+  double y0 = fmin(fmin(tv[1], tv[4]), tv[7]), y1 = fmax(fmax(tv[1], tv[4]), tv[7]);
+  int bx0 = min(max((int)((x0 - b.lo[0]) * b.inv[0]), 0), b.nb[0] - 1);
+  int bx1 = min(max((int)((x1 - b.lo[0]) * b.inv[0]), 0), b.nb[0] - 1);
+  int by0 = min(max((int)((y0 - b.lo[1]) * b.inv[1]), 0), b.nb[1] - 1);
+  int by1 = min(max((int)((y1 - b.lo[1]) * b.inv[1]), 0), b.nb[1] - 1);
+  for (int by = by0; by <= by1; by++)
+    for (int bx = bx0; bx <= bx1; bx++) items[atomicAdd(&cursor[bx + b.nb[0] * by], 1)] = t;
+}
+
+__device__ __forceinline__ int bin3_of(const Bins &b, const double *p, int a) {
+  return min(max((int)((p[a] - b.lo[a]) * b.inv[a]), 0), b.nb[a] - 1);
+}
+
+__global__ void k_bin3_count(int nb, const double *c, Bins b, int *cnt) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const double *p = c + 3 * t;
+  atomicAdd(&cnt[bin3_of(b, p, 0) + b.nb[0] * (bin3_of(b, p, 1) + b.nb[1] * bin3_of(b, p, 2))], 1);
+}
+
+__global__ void k_bin3_fill(int nb, const double *c, Bins b, int *cursor, int *items) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const double *p = c + 3 * t;
+  int bin = bin3_of(b, p, 0) + b.nb[0] * (bin3_of(b, p, 1) + b.nb[1] * bin3_of(b, p, 2));
+  items[atomicAdd(&cursor[bin], 1)] = t;
+}
+
+// exclusive scan of n counts: start[q] = sum of cnt[0..q), start[n] = total,
+// cursor[q] = start[q].  Three launches: per-block sums, a one-block scan of
+// the block sums, per-block scans with the block offset.
+constexpr int SB = 1024;
+__global__ void k_scan_sums(int n, const int *cnt, int *bsum) {
+  __shared__ int w[SB / 32];
+  const int q = blockIdx.x * SB + threadIdx.x;
+  int v = q < n ? cnt[q] : 0;
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int a = 0; a < SB / 32; a++) t += w[a];
+    bsum[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_scan_top(int nb, int *bsum, int *total) {
+  if (threadIdx.x != 0) return;
+  int acc = 0;
+  for (int b = 0; b < nb; b++) {
+    int v = bsum[b];
+    bsum[b] = acc;
+    acc += v;
+  }
+  *total = acc;
+}
+
+__global__ void k_scan_apply(int n, const int *cnt, const int *bsum, int *start, int *cursor) {
+  __shared__ int w[SB / 32];
+  const int q = blockIdx.x * SB + threadIdx.x;
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int v = q < n ? cnt[q] : 0;
+  int x = v;  // inclusive warp scan
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) w[wi] = x;
+  __syncthreads();
+  if (wi == 0) {
+    int z = w[lane];
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, z, off);
+      if (lane >= off) z += y;
+    }
+    w[lane] = z;
+  }
+  __syncthreads();
+  const int excl = bsum[blockIdx.x] + (wi > 0 ? w[wi - 1] : 0) + x - v;
+  if (q < n) {
+    start[q] = excl;
+    if (cursor) cursor[q] = excl;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// TAG3D_MOD (src/rt.f:2704-3020): one thread per (i, j) column of the body box
+__global__ void k_tag(Dims d, Axes ax, const int *lim, const double *v, Bins b, const int *bstart,
+                      const int *bitems, double rzmin, double rzmax, signed char *ibs, int *err) {
+  const int imin = lim[0], imax = lim[1];
+  const int ni = imax - imin + 1, nj = d.ny - 2;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ni * nj) return;
+  const int i = imin + t % ni, j = 2 + t / ni;
+  const double xcc = ax.x[i], ycc = ax.y[j];
+  double zc_[NCR];
+  int nc = 0;
+  if (xcc >= b.lo[0] && xcc <= b.hi[0] && ycc >= b.lo[1] && ycc <= b.hi[1]) {
+    // same bin arithmetic as the triangle insertion (monotone in x, y)
+    const int bx = min(max((int)((xcc - b.lo[0]) * b.inv[0]), 0), b.nb[0] - 1);
+    const int by = min(max((int)((ycc - b.lo[1]) * b.inv[1]), 0), b.nb[1] - 1);
+    const int bin = bx + b.nb[0] * by;
+    for (int s = bstart[bin]; s < bstart[bin + 1]; s++) {
+      const double *tv = v + 9 * bitems[s];
+      if (ycc >= fmin(fmin(tv[1], tv[4]), tv[7]) && ycc <= fmax(fmax(tv[1], tv[4]), tv[7]) &&
+          xcc >= fmin(fmin(tv[0], tv[3]), tv[6]) && xcc <= fmax(fmax(tv[0], tv[3]), tv[6])) {
+        const double p1[3] = {xcc, ycc, rzmin}, p2[3] = {xcc, ycc, rzmax};
+        double xm[3];
+        if (segtriint(p1, p2, tv, xm)) {
+          if (nc < NCR) zc_[nc] = xm[2];
+          nc++;
+        }
+      }
+    }
+  }
+  if (nc > NCR) {
+    atomicExch(err, 2);
+    nc = NCR;
+  }
+  double zo[NCR];
+  for (int i1 = 0; i1 < nc; i1++) {
+    double ztmin = 1.0e10;
+    int isave = 0;
+    for (int i2 = 0; i2 < nc; i2++)
+      if (zc_[i2] <= ztmin) {
+        ztmin = zc_[i2];
+        isave = i2;
+      }
+    zo[i1] = ztmin;
+    zc_[isave] = 2.0e10;
+  }
+  double zz[NCR];
+  for (int i1 = 0; i1 < nc; i1++) zz[i1] = zo[i1];
+  int ncl = 0;
+  for (int i1 = 0; i1 < nc; i1++) {
+    int ndp = 0;
+    for (int i2 = 0; i2 < i1; i2++)
+      if (fabs(zz[i2] - zz[i1]) < 1.e-06) ndp++;
+    if (ndp == 0) zo[ncl++] = zz[i1];
+  }
+  if (ncl == 1) ncl = 0;
+  for (int ic = 0; ic + 1 < ncl; ic += 2) {
+    int k1 = locate(ax.z, d.nz, zo[ic]);
+    int k2 = locate(ax.z, d.nz, zo[ic + 1]);
+    if (k2 > k1)
+      for (int k = k1 + 1; k <= k2; k++) ibs[lidx(d.nx, d.ny, i, j, k)] = -1;
+  }
+}
+
+// y periodic copy of an int8 array over i in [i0,i1], k in [k0,k1]
+__global__ void k_yper_i8(Dims d, signed char *a, int i0, int i1, int k0, int k1) {
+  const int ni = i1 - i0 + 1, nk = k1 - k0 + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ni * nk) return;
+  const int i = i0 + t % ni, k = k0 + t / ni;
+  a[lidx(d.nx, d.ny, i, 1, k)] = a[lidx(d.nx, d.ny, i, d.ny - 1, k)];
+  a[lidx(d.nx, d.ny, i, d.ny, k)] = a[lidx(d.nx, d.ny, i, 2, k)];
+}
+
+// taguo (src/devel.f:8-110) over the body box: 1 interior, -1 forcing
+__global__ void k_taguo(Dims d, Box6 L, int itagy, const signed char *f, signed char *fo) {
+  const int ni = L.imax - L.imin + 1, nj = L.jmax - L.jmin + 1, nk = L.kmax - L.kmin + 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)ni * nj * nk) return;
+  const int i = L.imin + (int)(t % ni), j = L.jmin + (int)((t / ni) % nj), k = L.kmin + (int)(t / ((long long)ni * nj));
+  const long long q = lidx(d.nx, d.ny, i, j, k);
+  const int c = f[q];
+  signed char o = (c == -1) ? 1 : 0;
+  const int k1 = max(2, L.kmin), k2 = min(d.nz - 1, L.kmax);
+  if (k >= k1 && k <= k2 && i >= max(2, L.imin) && c == 1) {
+    const long long sy = d.nx, sz = (long long)d.nx * d.ny;
+    const int nn = itagy == 0 ? 2 : 0;
+    int nb[6] = {c + f[q + 1], c + f[q - 1], c + f[q + sz], c + f[q - sz], c + f[q - sy], c + f[q + sy]};
+    long long prod = 1;
+    for (int m = 0; m < 6 - nn; m++) prod *= nb[m];
+    if (prod == 0) o = -1;
+  }
+  fo[q] = o;
+}
+
+// flagp (src/matint.f:135-260) over the body box
+__global__ void k_flagp(Dims d, Box6 L, const signed char *fu, const signed char *fv, const signed char *fw,
+                        signed char *fp) {
+  const int i0 = max(2, L.imin);
+  const int ni = L.imax - i0 + 1, nj = L.jmax - L.jmin + 1, nk = L.kmax - L.kmin + 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ni <= 0 || t >= (long long)ni * nj * nk) return;
+  const int i = i0 + (int)(t % ni), j = L.jmin + (int)((t / ni) % nj), k = L.kmin + (int)(t / ((long long)ni * nj));
+  const bool pass0 = (k <= 1), pass1 = (k >= max(2, L.kmin) && k <= L.kmax);
+  if (!pass0 && !pass1) return;
+  const long long q = lidx(d.nx, d.ny, i, j, k), sy = d.nx, sz = (long long)d.nx * d.ny;
+  int it[6], n;
+  if (pass0) {
+    it[0] = fu[q]; it[1] = fu[q - 1]; it[2] = fw[q]; it[3] = fv[q]; it[4] = fv[q - sy];
+    n = 5;
+  } else {
+    it[0] = fu[q]; it[1] = fu[q - 1]; it[2] = fw[q]; it[3] = fw[q - sz]; it[4] = fv[q]; it[5] = fv[q - sy];
+    n = 6;
+  }
+  int ifld = 0, ibdy = 0, ibnd = 0;
+  for (int m = 0; m < n; m++) {
+    ifld += it[m] == 0;
+    ibdy += it[m] > 0;
+    ibnd += it[m] < 0;
+  }
+  signed char o = 0;
+  if ((ibdy + ibnd) != 0 && ifld != 0) o = -1;
+  if (ifld == 0 && ibnd != 0) o = -1;
+  if (ifld == 0 && ibnd == 0 && ibdy != 0) o = 1;
+  fp[q] = o;
+}
+
+// ---------------------------------------------------------------------------
+// forcpts (src/matint.f:3388-3430): stable compaction of flag == -1 cells of
+// the box i in [max(2,imin), imax], j in [jmin, jmax], k in [max(2,kmin),
+// min(nz-1,kmax)] in (k, j, i) order
+constexpr int CB = 256;
+__device__ __forceinline__ bool fp_cell(const Dims &d, const Box6 &L, const signed char *f, long long t, int &i,
+                                        int &j, int &k) {
+  const int i0 = max(2, L.imin), k0 = max(2, L.kmin), k1 = min(d.nz - 1, L.kmax);
+  const int ni = L.imax - i0 + 1, nj = L.jmax - L.jmin + 1, nk = k1 - k0 + 1;
+  if (ni <= 0 || nk <= 0 || t >= (long long)ni * nj * nk) return false;
+  i = i0 + (int)(t % ni);
+  j = L.jmin + (int)((t / ni) % nj);
+  k = k0 + (int)(t / ((long long)ni * nj));
+  return f[lidx(d.nx, d.ny, i, j, k)] == -1;
+}
+
+__global__ void k_compact_count(Dims d, Box6 L, const signed char *f, int *bcnt) {
+  int i, j, k;
+  const long long t = (long long)blockIdx.x * CB + threadIdx.x;
+  const bool on = fp_cell(d, L, f, t, i, j, k);
+  const int c = __syncthreads_count(on ? 1 : 0);
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = c;
+}
+
+__global__ void k_compact_write(Dims d, Box6 L, const signed char *f, const int *boff, int *ijk) {
+  __shared__ int wsum[CB / 32];
+  int i, j, k;
+  const long long t = (long long)blockIdx.x * CB + threadIdx.x;
+  const bool on = fp_cell(d, L, f, t, i, j, k);
+  const unsigned bal = __ballot_sync(0xffffffffu, on);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(bal);
+  __syncthreads();
+  int base = boff[blockIdx.x];
+  for (int q = 0; q < w; q++) base += wsum[q];
+  if (on) {
+    const int pos = base + __popc(bal & ((1u << lane) - 1u));
+    ijk[3 * pos] = i;
+    ijk[3 * pos + 1] = j;
+    ijk[3 * pos + 2] = k;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// exact k nearest centroids of q (ties by triangle index), one warp: the
+// lanes scan the bins of Chebyshev rings 0..R keeping their own k best, the
+// lists are merged in k rounds of a lexicographic (d2, index) warp arg-min;
+// the search widens until every unvisited centroid is provably farther than
+// the k-th found (R bins of the smallest width h).  Lane 0's result in out.
+__device__ int knn_warp(const Bins &b, const int *bstart, const int *bitems, const double *c, const double *q,
+                        int kk, int *out) {
+  const int lane = threadIdx.x & 31;
+  const int cx = bin3_of(b, q, 0), cy = bin3_of(b, q, 1), cz = bin3_of(b, q, 2);
+  const double h = fmin(fmin(1.0 / b.inv[0], 1.0 / b.inv[1]), 1.0 / b.inv[2]);
+  const int rmax = max(max(b.nb[0], b.nb[1]), b.nb[2]);
+  int R = 1, got = 0;
+  double bound = 1e300;  // squared distance within which the k nearest lie
+  for (int attempt = 0; attempt < 16; attempt++) {
+    double bd[NNTR3D];
+    int bi[NNTR3D];
+    int m = 0;
+    const int side = 2 * R + 1, nbins = side * side * side;
+    for (int bb = lane; bb < nbins; bb += 32) {
+      const int dx = bb % side - R, dy = (bb / side) % side - R, dz = bb / (side * side) - R;
+      const int x = cx + dx, y = cy + dy, z = cz + dz;
+      if (x < 0 || y < 0 || z < 0 || x >= b.nb[0] || y >= b.nb[1] || z >= b.nb[2]) continue;
+      const int bin = x + b.nb[0] * (y + b.nb[1] * z);
+      if (bstart[bin] == bstart[bin + 1]) continue;
+      // skip bins entirely farther than the k-th distance already established
+      if (bound < 1e300) {
+        const int xyz[3] = {x, y, z};
+        double md = 0.;
+        for (int a = 0; a < 3; a++) {
+          const double w = 1.0 / b.inv[a];
+          const double lo = b.lo[a] + w * xyz[a], hi = lo + w;
+          const double e = q[a] < lo ? lo - q[a] : (q[a] > hi ? q[a] - hi : 0.);
+          md += e * e;
+        }
+        if (md > bound) continue;
+      }
+      for (int s = bstart[bin]; s < bstart[bin + 1]; s++) {
+        const int tt = bitems[s];
+        const double *p = c + 3 * tt;
+        const double ex = p[0] - q[0], ey = p[1] - q[1], ez = p[2] - q[2];
+        const double d2 = ex * ex + ey * ey + ez * ez;
+        if (m == kk && !(d2 < bd[m - 1] || (d2 == bd[m - 1] && tt < bi[m - 1]))) continue;
+        int pp = m < kk ? m : kk - 1;
+        while (pp > 0 && (bd[pp - 1] > d2 || (bd[pp - 1] == d2 && bi[pp - 1] > tt))) {
+          bd[pp] = bd[pp - 1];
+          bi[pp] = bi[pp - 1];
+          pp--;
+        }
+        bd[pp] = d2;
+        bi[pp] = tt;
+        if (m < kk) m++;
+      }
+    }
+    // merge the lane lists
+    int ptr = 0;
+    double kth = 0.;
+    got = 0;
+    for (int r = 0; r < kk; r++) {
+      double hv = ptr < m ? bd[ptr] : 1e300;
+      int hi = ptr < m ? bi[ptr] : 0x7fffffff;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, hv, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, hi, off);
+        if (ov < hv || (ov == hv && oi < hi)) {
+          hv = ov;
+          hi = oi;
+        }
+      }
+      if (hi == 0x7fffffff) break;
+      if (lane == 0) out[r] = hi;
+      if (ptr < m && bi[ptr] == hi) ptr++;
+      got++;
+      kth = hv;
+    }
+    const double lim = (double)R * h;
+    if ((got == kk && kth < lim * lim) || R >= rmax || (got == kk && bound < 1e300)) break;
+    int Rn = R + 1;
+    if (got == kk) {
+      // the k nearest lie within sqrt(kth): one more pass over the bins that
+      // reach that ball gives the exact list
+      bound = kth;
+      const int need = (int)ceil(sqrt(kth) / h) + 1;
+      Rn = max(Rn, need);
+    } else {
+      Rn = 2 * R;
+    }
+    R = min(Rn, rmax);
+  }
+  if (lane == 0)
+    for (int r = got; r < kk; r++) out[r] = -1;
+  __syncwarp();
+  return got;
+}
+
+__constant__ int c_gind[26][3] = {
+    {1, 0, 0},  {-1, 0, 0}, {0, 0, 1},   {0, 0, -1},  {1, 0, 1},   {1, 0, -1},  {-1, 0, 1},
+    {-1, 0, -1}, {0, 1, 0},  {0, -1, 0},  {1, 1, 0},   {-1, 1, 0},  {0, 1, 1},   {0, 1, -1},
+    {1, 1, 1},  {1, 1, -1}, {-1, 1, 1},  {-1, 1, -1}, {1, -1, 0},  {-1, -1, 0}, {0, -1, 1},
+    {0, -1, -1}, {1, -1, 1}, {1, -1, -1}, {-1, -1, 1}, {-1, -1, -1}};
+
+__device__ double unitdot(const double *x, const double *xn, const double *nrm) {
+  double a[3] = {x[0] - xn[0], x[1] - xn[1], x[2] - xn[2]};
+  double ma = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  a[0] = a[0] / ma; a[1] = a[1] / ma; a[2] = a[2] / ma;
+  double b[3] = {nrm[0], nrm[1], nrm[2]};
+  double mb = sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+  b[0] = b[0] / mb; b[1] = b[1] / mb; b[2] = b[2] / mb;
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+// grid_intr (src/matint.f:800-1160), isrt = 0, igrdint = 1, one warp: lane
+// d < 26 takes grid direction d.  The physical directions (flag <= 0) are
+// the ones the reference visits, in the order of their criterion (fluid
+// first, then boundary, each by index); every direction's result (first
+// candidate triangle, in list order, crossed by the 10x extended grid segment
+// with the extension point on the outward side) is independent of the
+// others, so the lanes search concurrently and the recorded intersections are
+// then numbered in visiting order for the selection (dot product with the
+// normal + flag * number, first maximum).  Returns (to every lane) 1, -1
+// (extension point is a forcing point), 0 (no intersection), -2 (only
+// inward ones); lane 0 writes xn, dd.
+__device__ int grid_intr_warp(const Dims &d, const Axes &ax, const double *v, const double *nrm,
+                              const signed char *flag, int im, int jm, int km, const int *inn, int nn, double *xn,
+                              int *dd) {
+  const int lane = threadIdx.x & 31;
+  const bool dirl = lane < 26;
+  const int id = dirl ? c_gind[lane][0] : 0, jd = dirl ? c_gind[lane][1] : 0, kd = dirl ? c_gind[lane][2] : 0;
+  const int fext = dirl ? flag[lidx(d.nx, d.ny, im + id, jm + jd, km + kd)] : 1;
+  const double crit = !dirl ? -100.0 : (fext == 0 ? 1.0 : (fext < 0 ? 0.5 : -2.0));
+  // visiting slot: rank by (criterion descending, index ascending)
+  int rank = 0;
+  for (int e = 0; e < 26; e++) {
+    const double ce = __shfl_sync(0xffffffffu, crit, e);
+    if (ce > crit || (ce == crit && e < lane)) rank++;
+  }
+  const double p0[3] = {ax.x[im], ax.y[jm], ax.z[km]};
+  const double pe[3] = {ax.x[im + id], ax.y[jm + jd], ax.z[km + kd]};
+  // one scan of the candidate list serves the three list lengths: a
+  // direction's result for length k is its first valid crossing if that lies
+  // within the first k candidates; hits are counted up to it (or up to k)
+  int pos = 1 << 20, h3 = 0, h5 = 0, hall = 0, tri = -1;
+  double xm[3] = {0., 0., 0.};
+  if (dirl && fext <= 0) {
+    double r[3] = {pe[0] - p0[0], pe[1] - p0[1], pe[2] - p0[2]};
+    r[0] = r[0] * 10.0; r[1] = r[1] * 10.0; r[2] = r[2] * 10.0;
+    const double s1[3] = {p0[0] - r[0], p0[1] - r[1], p0[2] - r[2]};
+    const double s2[3] = {p0[0] + r[0], p0[1] + r[1], p0[2] + r[2]};
+    for (int in = 0; in < nn; in++) {
+      const int n = inn[in];
+      if (n < 0) continue;
+      double x3[3];
+      if (segtriint(s1, s2, v + 9 * n, x3)) {
+        hall++;
+        if (in < 3) h3++;
+        if (in < 5) h5++;
+        if (unitdot(pe, p0, nrm + 3 * n) > 0.0) {
+          tri = n;
+          pos = in;
+          xm[0] = x3[0]; xm[1] = x3[1]; xm[2] = x3[2];
+          break;
+        }
+      }
+    }
+  }
+  int gi = 0;
+  for (int lv = 0; lv < 3; lv++) {
+    const int kk = lv == 0 ? 3 : (lv == 1 ? 5 : nn);
+    const bool rec = pos < kk;
+    const int hits = rec ? hall : (lv == 0 ? h3 : (lv == 1 ? h5 : hall));
+    const unsigned smask = __reduce_or_sync(0xffffffffu, rec ? (1u << rank) : 0u);
+    int tot = hits;
+    for (int off = 16; off > 0; off >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, off);
+    if (smask == 0) {
+      gi = tot == 0 ? 0 : -2;
+      continue;
+    }
+    const int m = __popc(smask & ((1u << rank) - 1u));
+    double ds = -1e300;
+    int key = 0x7fffffff;
+    if (rec) {
+      ds = unitdot(pe, p0, nrm + 3 * tri);
+      ds = ds + (double)fext * (double)(m + 1);
+      key = m;
+    }
+    double bds = ds;
+    int bkey = key, blane = lane;
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ods = __shfl_xor_sync(0xffffffffu, bds, off);
+      const int okey = __shfl_xor_sync(0xffffffffu, bkey, off);
+      const int olane = __shfl_xor_sync(0xffffffffu, blane, off);
+      if (ods > bds || (ods == bds && okey < bkey)) {
+        bds = ods;
+        bkey = okey;
+        blane = olane;
+      }
+    }
+    if (lane == blane) {
+      xn[0] = xm[0]; xn[1] = xm[1]; xn[2] = xm[2];
+      dd[0] = id; dd[1] = jd; dd[2] = kd;
+    }
+    const int cand = __shfl_sync(0xffffffffu, fext < 0 ? 1 : 0, blane);
+    return cand ? -1 : 1;
+  }
+  return gi;
+}
+
+// ludcmp for n = 2 (implicit partial pivoting), column-major a11 a21 a12 a22
+__device__ void lu2(double *a, int *indx) {
+  double A[2][2] = {{a[0], a[2]}, {a[1], a[3]}};
+  double vv[2];
+  for (int i = 0; i < 2; i++) {
+    double aamax = 0.;
+    for (int j = 0; j < 2; j++)
+      if (fabs(A[i][j]) > aamax) aamax = fabs(A[i][j]);
+    vv[i] = 1. / aamax;
+  }
+  double aamax = 0.;
+  int imax = 0;
+  for (int i = 0; i < 2; i++) {
+    double dum = vv[i] * fabs(A[i][0]);
+    if (dum >= aamax) {
+      imax = i;
+      aamax = dum;
+    }
+  }
+  if (imax != 0) {
+    for (int k = 0; k < 2; k++) {
+      double dum = A[imax][k];
+      A[imax][k] = A[0][k];
+      A[0][k] = dum;
+    }
+    vv[imax] = vv[0];
+  }
+  indx[0] = imax;
+  if (A[0][0] == 0.) A[0][0] = 1.0e-20;
+  {
+    double dum = 1. / A[0][0];
+    A[1][0] = A[1][0] * dum;
+  }
+  {
+    double sum = A[1][1];
+    sum = sum - A[1][0] * A[0][1];
+    A[1][1] = sum;
+  }
+  indx[1] = 1;
+  if (A[1][1] == 0.) A[1][1] = 1.0e-20;
+  a[0] = A[0][0]; a[1] = A[1][0]; a[2] = A[0][1]; a[3] = A[1][1];
+}
+
+// lubksb for n = 2
+__device__ __forceinline__ void lusolve2(const double *a, const int *indx, double *b) {
+  const double A[2][2] = {{a[0], a[2]}, {a[1], a[3]}};
+  int ii = -1;
+  for (int i = 0; i < 2; i++) {
+    const int ll = indx[i];
+    double sum = b[ll];
+    b[ll] = b[i];
+    if (ii >= 0) {
+      for (int j = ii; j <= i - 1; j++) sum = sum - A[i][j] * b[j];
+    } else if (sum != 0.) {
+      ii = i;
+    }
+    b[i] = sum;
+  }
+  for (int i = 1; i >= 0; i--) {
+    double sum = b[i];
+    for (int j = i + 1; j < 2; j++) sum = sum - A[i][j] * b[j];
+    b[i] = sum / A[i][i];
+  }
+}
+
+// first dependency loop, one warp per forcing point: grid_intr with the
+// candidate lists of the 3, 5, 25 nearest centroids; status: 1 resolved, -2
+// waits for its extension point, 0 dropped
+constexpr int GW = 4;  // warps (points) per block
+__global__ void __launch_bounds__(GW * 32)
+    k_geom_first(Dims d, Axes ax, int n, const int *ijk, const double *v, const double *c, const double *nrm, Bins b,
+                 const int *bstart, const int *bitems, const signed char *fw, int *status, double *xn, int *dd) {
+  __shared__ int inn_s[GW][NNTR3D];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.x * GW + w;
+  if (p >= n) return;  // whole warp
+  const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
+  const double qv[3] = {ax.x[im], ax.y[jm], ax.z[km]};
+  // the exact nearest-centroid list is sorted, so the 3- and 5-lists are its
+  // prefixes; grid_intr_warp evaluates the three lengths in one scan
+  knn_warp(b, bstart, bitems, c, qv, NNTR3D, inn_s[w]);
+  const int gi = grid_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn_s[w], NNTR3D, xn + 3 * p, dd + 3 * p);
+  __syncwarp();
+  if (lane == 0) status[p] = gi == 1 ? 1 : (gi == -1 ? -2 : 0);
+}
+
+// later loops: a waiting point resolves once its extension point is no longer
+// a forcing point in the working flags
+__global__ void k_geom_recheck(Dims d, int n, const int *ijk, const int *dd, const signed char *fw, int *status,
+                               int *lev, int ilp, int last) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || status[p] != -2) return;
+  const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
+  if (fw[lidx(d.nx, d.ny, im + dd[3 * p], jm + dd[3 * p + 1], km + dd[3 * p + 2])] == 0) {
+    status[p] = 1;
+    lev[p] = ilp;
+  } else if (last) {
+    status[p] = 0;
+  }
+}
+
+// points resolved in loop ilp: working flag 0, level recorded, counter
+__global__ void k_geom_mark(Dims d, int n, const int *ijk, int *status, int *lev, int ilp, signed char *fw,
+                            int *cnt) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  if (status[p] == 1) {
+    if (ilp == 1) lev[p] = 1;
+    if (lev[p] == ilp) {
+      fw[lidx(d.nx, d.ny, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2])] = 0;
+      atomicAdd(&cnt[0], 1);
+    }
+  } else if (status[p] == -2) {
+    atomicAdd(&cnt[1], 1);
+  }
+}
+
+// dropped points: the variable's flag becomes fluid (velocity) or interior (pressure)
+__global__ void k_geom_drop(Dims d, int n, const int *ijk, int *status, signed char *flag, signed char value,
+                            int drop_waiting) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  if (status[p] == 0 || (drop_waiting && status[p] == -2)) {
+    status[p] = 0;
+    flag[lidx(d.nx, d.ny, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2])] = value;
+  }
+}
+
+// output order: by level, then forcpts order (position = level offset + rank)
+__global__ void k_geom_rank_count(int n, const int *status, const int *lev, int nlev, int *levcnt) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || status[p] != 1) return;
+  atomicAdd(&levcnt[lev[p] - 1], 1);
+}
+
+// mtrx (src/devel.f:1159-1290) for the resolved points, written at their
+// final position; pos computed by a stable per-level prefix over the list
+__global__ void k_geom_emit(Dims d, Axes ax, int n, const int *ijk, const int *status, const int *lev,
+                            const int *order, const double *xnp, const int *ddp, int imn, int *oijk, int *odd,
+                            int *olev, double *oxn, double *olu, int *oindx) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || status[p] != 1) return;
+  const int o = order[p];
+  const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
+  const int di = ddp[3 * p], dj = ddp[3 * p + 1], dk = ddp[3 * p + 2];
+  oijk[3 * o] = im; oijk[3 * o + 1] = jm; oijk[3 * o + 2] = km;
+  odd[3 * o] = di; odd[3 * o + 1] = dj; odd[3 * o + 2] = dk;
+  olev[o] = lev[p];
+  const double xnx = xnp[3 * p], xny = xnp[3 * p + 1], xnz = xnp[3 * p + 2];
+  oxn[3 * o] = xnx; oxn[3 * o + 1] = xny; oxn[3 * o + 2] = xnz;
+  const double xu = ax.x[im], yu = ax.y[jm], zu = ax.z[km];
+  const double x1 = ax.x[im + di], y1 = ax.y[jm + dj], z1 = ax.z[km + dk];
+  const double is1 = imn == 1 ? -1. : 1.;
+  const double so = sqrt(((xu - xnx) * (xu - xnx) + (yu - xny) * (yu - xny)) + (zu - xnz) * (zu - xnz)) * is1;
+  const double s1 = sqrt(((xu - x1) * (xu - x1) + (yu - y1) * (yu - y1)) + (zu - z1) * (zu - z1)) * 1.0;
+  double A[4];
+  if (imn != 0) {
+    A[0] = 1.; A[2] = so;
+  } else {
+    A[0] = 0.; A[2] = 1.0;
+  }
+  A[1] = 1.; A[3] = s1;
+  lu2(A, oindx + 2 * o);
+  for (int q = 0; q < 4; q++) olu[4 * o + q] = A[q];
+}
+
+// stable per-level ranks: order[p] = levstart[l] + (number of resolved
+// points of level l before p), computed per level by block counts + scan
+__global__ void k_level_count(int n, const int *status, const int *lev, int l, int *bcnt) {
+  const int p = blockIdx.x * CB + threadIdx.x;
+  const bool on = p < n && status[p] == 1 && lev[p] == l;
+  const int c = __syncthreads_count(on ? 1 : 0);
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = c;
+}
+
+__global__ void k_level_rank(int n, const int *status, const int *lev, int l, int base, const int *boff,
+                             int *order) {
+  __shared__ int wsum[CB / 32];
+  const int p = blockIdx.x * CB + threadIdx.x;
+  const bool on = p < n && status[p] == 1 && lev[p] == l;
+  const unsigned bal = __ballot_sync(0xffffffffu, on);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(bal);
+  __syncthreads();
+  int r = boff[blockIdx.x];
+  for (int q = 0; q < w; q++) r += wsum[q];
+  if (on) order[p] = base + r + __popc(bal & ((1u << lane) - 1u));
+}
+
+// ---------------------------------------------------------------------------
+// forcing (momforc_mod2 explicit / correctpres_mod2, correctdens_mod2 with a
+// zero normal gradient) for the points of one level; T storage with row pitch
+template <class T>
+__global__ void k_force(Dims d, int pitch, int o0, int o1, const int *ijk, const int *dd, const double *lu,
+                        const int *indx, T *a, double b0, float *mirror, int mpitch) {
+  const int o = o0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= o1) return;
+  const int im = ijk[3 * o], jm = ijk[3 * o + 1], km = ijk[3 * o + 2];
+  int i1 = im + dd[3 * o], j1 = jm + dd[3 * o + 1], k1 = km + dd[3 * o + 2];
+  if (j1 <= 1)
+    j1 = d.ny - 2 + j1;
+  else if (j1 >= d.ny)
+    j1 = j1 - d.ny + 2;
+  double b[2] = {b0, (double)a[pidx(d, pitch, i1, j1, k1)]};
+  lusolve2(lu + 4 * o, indx + 2 * o, b);
+  a[pidx(d, pitch, im, jm, km)] = (T)b[0];
+  if (mirror) mirror[pidx(d, mpitch, im, jm, km)] = (float)b[0];
+}
+
+// y periodic planes of a field (whole (i, k) range)
+template <class T>
+__global__ void k_yper_field(Dims d, int pitch, T *a, float *mirror, int mpitch) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.nx * d.nz) return;
+  const int i = 1 + t % d.nx, k = 1 + t / d.nx;
+  const T lo = a[pidx(d, pitch, i, d.ny - 1, k)], hi = a[pidx(d, pitch, i, 2, k)];
+  a[pidx(d, pitch, i, 1, k)] = lo;
+  a[pidx(d, pitch, i, d.ny, k)] = hi;
+  if (mirror) {
+    mirror[pidx(d, mpitch, i, 1, k)] = (float)lo;
+    mirror[pidx(d, mpitch, i, d.ny, k)] = (float)hi;
+  }
+}
+
+// interior value at flag == 1 over the body box
+template <class T>
+__global__ void k_interior(Dims d, int pitch, Box6 L, const signed char *flag, T *a, double value, float *mirror,
+                           int mpitch) {
+  const int ni = L.imax - L.imin + 1, nj = L.jmax - L.jmin + 1, nk = L.kmax - L.kmin + 1;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)ni * nj * nk) return;
+  const int i = L.imin + (int)(t % ni), j = L.jmin + (int)((t / ni) % nj), k = L.kmin + (int)(t / ((long long)ni * nj));
+  if (flag[lidx(d.nx, d.ny, i, j, k)] == 1) {
+    a[pidx(d, pitch, i, j, k)] = (T)value;
+    if (mirror) mirror[pidx(d, mpitch, i, j, k)] = (float)value;
+  }
+}
+
+inline unsigned nblk(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+// exclusive scan with start[n] = total (bsum: scratch of >= ceil(n/SB) ints)
+int scan_launch(eddy_ctx *ctx, int n, const int *cnt, int *start, int *cursor, int *bsum) {
+  cudaStream_t st = ctx->stream;
+  const int nb = (n + SB - 1) / SB;
+  k_scan_sums<<<nb, SB, 0, st>>>(n, cnt, bsum);
+  EDDY_LAUNCHED(ctx);
+  k_scan_top<<<1, 32, 0, st>>>(nb, bsum, start + n);
+  EDDY_LAUNCHED(ctx);
+  k_scan_apply<<<nb, SB, 0, st>>>(n, cnt, bsum, start, cursor);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+// a persistent int scratch buffer of at least `need` entries
+int *scratch(eddy_ctx *ctx, IbState *s, int which, size_t need) {
+  if (need > s->si_cap[which]) {
+    if (s->si[which]) cudaFree(s->si[which]);
+    s->si[which] = nullptr;
+    s->si_cap[which] = 0;
+    size_t cap = need + need / 2 + 64;
+    if (cudaMalloc(&s->si[which], sizeof(int) * cap) != cudaSuccess) {
+      ctx->err = "immersed-body scratch allocation failed";
+      return nullptr;
+    }
+    s->si_cap[which] = cap;
+  }
+  return s->si[which];
+}
+
+double *scratch_d(eddy_ctx *ctx, IbState *s, size_t need) {
+  if (need > s->sxn_cap) {
+    if (s->sxn) cudaFree(s->sxn);
+    s->sxn = nullptr;
+    s->sxn_cap = 0;
+    size_t cap = need + need / 2 + 64;
+    if (cudaMalloc(&s->sxn, sizeof(double) * cap) != cudaSuccess) {
+      ctx->err = "immersed-body scratch allocation failed";
+      return nullptr;
+    }
+    s->sxn_cap = cap;
+  }
+  return s->sxn;
+}
+
+int ensure(eddy_ctx *ctx, int **p, int &cap, int need) {
+  if (need <= cap) return EDDY_OK;
+  if (*p) cudaFree(*p);
+  EDDY_CUDA(cudaMalloc(p, sizeof(int) * need));
+  cap = need;
+  return EDDY_OK;
+}
+
+// bins over [lo, hi] with nb cells per axis (dims of the grid: 2 or 3)
+int build_bins(eddy_ctx *ctx, Bins &b, int dims, const double *lo, const double *hi, int nb_axis, int ntri,
+               const double *data, bool tri2d) {
+  int nbins = 1;
+  for (int a = 0; a < 3; a++) {
+    b.nb[a] = a < dims ? nb_axis : 1;
+    b.lo[a] = a < dims ? lo[a] : 0.;
+    b.hi[a] = a < dims ? hi[a] : 1.;
+    double w = (b.hi[a] - b.lo[a]) / b.nb[a];
+    if (!(w > 0)) w = 1e-30;
+    b.inv[a] = 1.0 / w;
+    nbins *= b.nb[a];
+  }
+  if (!b.start) {
+    EDDY_CUDA(cudaMalloc(&b.start, sizeof(int) * (nbins + 1)));
+    EDDY_CUDA(cudaMalloc(&b.cursor, sizeof(int) * nbins));
+  }
+  cudaStream_t st = ctx->stream;
+  EDDY_CUDA(cudaMemsetAsync(b.cursor, 0, sizeof(int) * nbins, st));
+  if (tri2d)
+    k_bin2_count<<<nblk(ntri), 256, 0, st>>>(ntri, data, b, b.cursor);
+  else
+    k_bin3_count<<<nblk(ntri), 256, 0, st>>>(ntri, data, b, b.cursor);
+  EDDY_LAUNCHED(ctx);
+  int *cnt = scratch(ctx, ibs(ctx), IbState::S_BINCNT, nbins);
+  if (!cnt) return EDDY_ENOMEM;
+  EDDY_CUDA(cudaMemcpyAsync(cnt, b.cursor, sizeof(int) * nbins, cudaMemcpyDeviceToDevice, st));
+  {
+    int *bsum = scratch(ctx, ibs(ctx), IbState::S_BSUM, (nbins + SB - 1) / SB + 1);
+    if (!bsum) return EDDY_ENOMEM;
+    int rc = scan_launch(ctx, nbins, cnt, b.start, b.cursor, bsum);
+    if (rc) return rc;
+  }
+  int total = 0;
+  EDDY_CUDA(cudaMemcpyAsync(&total, b.start + nbins, sizeof(int), cudaMemcpyDeviceToHost, st));
+  EDDY_CUDA(cudaStreamSynchronize(st));
+  if (total > b.cap) {
+    if (b.items) cudaFree(b.items);
+    EDDY_CUDA(cudaMalloc(&b.items, sizeof(int) * (size_t)(total + 1)));
+    b.cap = total;
+  }
+  b.nitems = total;
+  if (tri2d)
+    k_bin2_fill<<<nblk(ntri), 256, 0, st>>>(ntri, data, b, b.cursor, b.items);
+  else
+    k_bin3_fill<<<nblk(ntri), 256, 0, st>>>(ntri, data, b, b.cursor, b.items);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+Axes axes_of(eddy_ctx *ctx, int q) {
+  // 1-based device coordinate arrays kept in the IB scratch: xu, xc, yv, yc, zw, zc
+  double *const *a = ctx->ibax;
+  Axes ax;
+  ax.x = (q == 0) ? a[0] : a[1];
+  ax.y = (q == 1) ? a[2] : a[3];
+  ax.z = (q == 2) ? a[4] : a[5];
+  return ax;
+}
+
+// forcpts + geometry + mtrx for variable q with flag array fq
+int geom(eddy_ctx *ctx, int q, int fq, int imn) {
+  IbState *s = ibs(ctx);
+  const Dims &d = ctx->d;
+  cudaStream_t st = ctx->stream;
+  Box6 L = s->lim;
+  signed char *flag = s->flag[fq];
+  // forcpts
+  const int i0 = std::max(2, L.imin), k0 = std::max(2, L.kmin), k1 = std::min(d.nz - 1, L.kmax);
+  const long long nbox = (long long)std::max(0, L.imax - i0 + 1) * (L.jmax - L.jmin + 1) * std::max(0, k1 - k0 + 1);
+  const int nblocks = (int)std::max(1LL, (nbox + CB - 1) / CB);
+  int *bcnt = scratch(ctx, s, IbState::S_BCNT, nblocks), *boff = scratch(ctx, s, IbState::S_BOFF, nblocks + 1),
+      *cur = scratch(ctx, s, IbState::S_CUR, nblocks);
+  if (!bcnt || !boff || !cur) return EDDY_ENOMEM;
+  k_compact_count<<<nblocks, CB, 0, st>>>(d, L, flag, bcnt);
+  EDDY_LAUNCHED(ctx);
+  {
+    int *bsum = scratch(ctx, s, IbState::S_BSUM, (nblocks + SB - 1) / SB + 1);
+    if (!bsum) return EDDY_ENOMEM;
+    int rc0 = scan_launch(ctx, nblocks, bcnt, boff, cur, bsum);
+    if (rc0) return rc0;
+  }
+  EDDY_CUDA(cudaMemcpyAsync(s->hcnt, boff + nblocks, sizeof(int), cudaMemcpyDeviceToHost, st));
+  EDDY_CUDA(cudaStreamSynchronize(st));
+  const int n = s->hcnt[0];
+  int rc;
+  if ((rc = ensure(ctx, &s->pts, s->pcap, 3 * std::max(n, 1)))) return rc;
+  k_compact_write<<<nblocks, CB, 0, st>>>(d, L, flag, boff, s->pts);
+  EDDY_LAUNCHED(ctx);
+  StencilSet &S = s->set[q];
+  S.n = 0;
+  S.nlev = 0;
+  S.lev_start.assign(1, 0);
+  if (n == 0) return EDDY_OK;
+  // per-point scratch
+  int *status = scratch(ctx, s, IbState::S_STATUS, n), *lev = scratch(ctx, s, IbState::S_LEV, n),
+      *dd = scratch(ctx, s, IbState::S_DD, 3 * (size_t)n), *order = scratch(ctx, s, IbState::S_ORDER, n),
+      *cnt = scratch(ctx, s, IbState::S_CNT, NFLU + 2);
+  double *xn = scratch_d(ctx, s, 3 * (size_t)n);
+  if (!status || !lev || !dd || !order || !cnt || !xn) return EDDY_ENOMEM;
+  EDDY_CUDA(cudaMemsetAsync(lev, 0, sizeof(int) * n, st));
+  signed char *fw = s->work;
+  const size_t nc = (size_t)d.ncell;
+  EDDY_CUDA(cudaMemcpyAsync(fw, flag, nc, cudaMemcpyDeviceToDevice, st));
+  Axes ax = axes_of(ctx, q);
+  k_geom_first<<<(unsigned)((n + GW - 1) / GW), GW * 32, 0, st>>>(d, ax, n, s->pts, s->v, s->c, s->n, s->b3,
+                                                                   s->b3.start, s->b3.items, fw, status, xn, dd);
+  EDDY_LAUNCHED(ctx);
+  k_geom_drop<<<nblk(n), 256, 0, st>>>(d, n, s->pts, status, flag, (signed char)(imn == 0 ? 1 : 0), 0);
+  EDDY_LAUNCHED(ctx);
+  int nlev = 0;
+  for (int ilp = 1; ilp <= NFLU; ilp++) {
+    if (ilp > 1) {
+      k_geom_recheck<<<nblk(n), 256, 0, st>>>(d, n, s->pts, dd, fw, status, lev, ilp, ilp == NFLU);
+      EDDY_LAUNCHED(ctx);
+    }
+    EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, st));
+    k_geom_mark<<<nblk(n), 256, 0, st>>>(d, n, s->pts, status, lev, ilp, fw, cnt);
+    EDDY_LAUNCHED(ctx);
+    k_yper_i8<<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, fw, 1, d.nx, 1, d.nz);
+    EDDY_LAUNCHED(ctx);
+    EDDY_CUDA(cudaMemcpyAsync(s->hcnt, cnt, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+    EDDY_CUDA(cudaStreamSynchronize(st));
+    const int nres = s->hcnt[0], nwait = s->hcnt[1];
+    if (nres > 0) nlev = ilp;
+    // done, or no progress: points still waiting are dropped below
+    if (nwait == 0 || nres == 0) break;
+  }
+  k_geom_drop<<<nblk(n), 256, 0, st>>>(d, n, s->pts, status, flag, (signed char)(imn == 0 ? 1 : 0), 1);
+  EDDY_LAUNCHED(ctx);
+  // level sizes -> offsets
+  EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (NFLU + 2), st));
+  k_geom_rank_count<<<nblk(n), 256, 0, st>>>(n, status, lev, nlev, cnt + 1);
+  EDDY_LAUNCHED(ctx);
+  std::vector<int> lc(NFLU + 2, 0);
+  EDDY_CUDA(cudaMemcpyAsync(lc.data(), cnt + 1, sizeof(int) * (NFLU + 1), cudaMemcpyDeviceToHost, st));
+  EDDY_CUDA(cudaStreamSynchronize(st));
+  S.lev_start.assign(nlev + 1, 0);
+  for (int l = 0; l < nlev; l++) S.lev_start[l + 1] = S.lev_start[l] + lc[l];
+  const int nv = S.lev_start[nlev];
+  S.n = nv;
+  S.nlev = nlev;
+  if (nv > S.cap) {
+    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu};
+    for (void *p : ptrs) if (p) cudaFree(p);
+    EDDY_CUDA(cudaMalloc(&S.ijk, sizeof(int) * 3 * nv));
+    EDDY_CUDA(cudaMalloc(&S.dijk, sizeof(int) * 3 * nv));
+    EDDY_CUDA(cudaMalloc(&S.lev, sizeof(int) * nv));
+    EDDY_CUDA(cudaMalloc(&S.indx, sizeof(int) * 2 * nv));
+    EDDY_CUDA(cudaMalloc(&S.xn, sizeof(double) * 3 * nv));
+    EDDY_CUDA(cudaMalloc(&S.lu, sizeof(double) * 4 * nv));
+    S.cap = nv;
+  }
+  if (nv > 0) {
+    const int nbl = (n + CB - 1) / CB;
+    int *bcnt = scratch(ctx, s, IbState::S_BCNT, nbl), *boff = scratch(ctx, s, IbState::S_BOFF, nbl + 1),
+        *cur = scratch(ctx, s, IbState::S_CUR, nbl);
+    if (!bcnt || !boff || !cur) return EDDY_ENOMEM;
+    for (int l = 1; l <= nlev; l++) {
+      k_level_count<<<nbl, CB, 0, st>>>(n, status, lev, l, bcnt);
+      EDDY_LAUNCHED(ctx);
+      int *bsum = scratch(ctx, s, IbState::S_BSUM, (nbl + SB - 1) / SB + 1);
+      if (!bsum) return EDDY_ENOMEM;
+      int rc0 = scan_launch(ctx, nbl, bcnt, boff, cur, bsum);
+      if (rc0) return rc0;
+      k_level_rank<<<nbl, CB, 0, st>>>(n, status, lev, l, S.lev_start[l - 1], boff, order);
+      EDDY_LAUNCHED(ctx);
+    }
+    k_geom_emit<<<nblk(n), 256, 0, st>>>(d, ax, n, s->pts, status, lev, order, xn, dd, imn, S.ijk, S.dijk, S.lev,
+                                         S.xn, S.lu, S.indx);
+    EDDY_LAUNCHED(ctx);
+  }
+  return EDDY_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+int ib_release(eddy_ctx *ctx) {
+  IbState *s = ibs(ctx);
+  if (!s) return EDDY_OK;
+  void *p[] = {s->v, s->c, s->n, s->red, s->dlim, s->work, s->pts, s->b2.start, s->b2.items, s->b2.cursor,
+               s->b3.start, s->b3.items, s->b3.cursor};
+  for (void *q : p) if (q) cudaFree(q);
+  for (int q = 0; q < IbState::S_NI; q++) if (s->si[q]) cudaFree(s->si[q]);
+  if (s->sxn) cudaFree(s->sxn);
+  for (int q = 0; q < 4; q++) if (s->tag[q]) cudaFree(s->tag[q]);
+  for (int q = 0; q < 5; q++) if (s->flag[q]) cudaFree(s->flag[q]);
+  for (StencilSet &S : s->set) {
+    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu};
+    for (void *q : ptrs) if (q) cudaFree(q);
+  }
+  if (s->hcnt) cudaFreeHost(s->hcnt);
+  for (int a = 0; a < 6; a++)
+    if (ctx->ibax[a]) {
+      cudaFree(ctx->ibax[a]);
+      ctx->ibax[a] = nullptr;
+    }
+  delete s;
+  ctx->ib = nullptr;
+  return EDDY_OK;
+}
+
+int ib_set_body(eddy_ctx *ctx, int nb, const double *vert, const double *normals, const double *vel) {
+  ib_release(ctx);
+  if (nb <= 0) return EDDY_OK;
+  IbState *s = new (std::nothrow) IbState();
+  if (!s) return EDDY_ENOMEM;
+  ctx->ib = s;
+  s->nb = nb;
+  for (int q = 0; q < 3; q++) s->vel[q] = vel ? vel[q] : 0.0;
+  EDDY_CUDA(cudaMalloc(&s->v, sizeof(double) * 9 * nb));
+  EDDY_CUDA(cudaMalloc(&s->c, sizeof(double) * 3 * nb));
+  EDDY_CUDA(cudaMalloc(&s->n, sizeof(double) * 3 * nb));
+  EDDY_CUDA(cudaMemcpy(s->v, vert, sizeof(double) * 9 * nb, cudaMemcpyHostToDevice));
+  EDDY_CUDA(cudaMemcpy(s->n, normals, sizeof(double) * 3 * nb, cudaMemcpyHostToDevice));
+  EDDY_CUDA(cudaMalloc(&s->red, sizeof(double) * 24));
+  EDDY_CUDA(cudaMalloc(&s->dlim, sizeof(int) * 8));
+  EDDY_CUDA(cudaMallocHost(&s->hcnt, sizeof(int) * 64));
+  const size_t nc = (size_t)ctx->d.ncell;
+  for (int q = 0; q < 4; q++) EDDY_CUDA(cudaMalloc(&s->tag[q], nc));
+  for (int q = 0; q < 5; q++) {
+    EDDY_CUDA(cudaMalloc(&s->flag[q], nc));
+    EDDY_CUDA(cudaMemset(s->flag[q], 0, nc));
+  }
+  EDDY_CUDA(cudaMalloc(&s->work, nc));
+  // coordinate arrays (1-based, size n+1)
+  const int ids[6] = {0, 1, 6, 7, 12, 13};  // xu xc yv yc zw zc in ctx->h
+  for (int a = 0; a < 6; a++) {
+    const std::vector<double> &h = ctx->h[ids[a]];
+    EDDY_CUDA(cudaMalloc(&ctx->ibax[a], sizeof(double) * h.size()));
+    EDDY_CUDA(cudaMemcpy(ctx->ibax[a], h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  }
+  k_centroids<<<nblk(nb), 256, 0, ctx->stream>>>(nb, s->v, s->c);
+  EDDY_LAUNCHED(ctx);
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  s->ready = true;
+  return EDDY_OK;
+}
+
+int ib_move(eddy_ctx *ctx, double tmove) {
+  IbState *s = ibs(ctx);
+  if (!s) return EDDY_OK;
+  k_move<<<nblk(s->nb), 256, 0, ctx->stream>>>(s->nb, s->v, s->c, s->vel[0] * tmove, s->vel[1] * tmove,
+                                               s->vel[2] * tmove);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+// the regeneration of src/Eddy6.f:2184-2380 for the current body position
+int ib_regen(eddy_ctx *ctx) {
+  IbState *s = ibs(ctx);
+  if (!s) return EDDY_OK;
+  const Dims &d = ctx->d;
+  cudaStream_t st = ctx->stream;
+  int rc;
+  long long *keys = reinterpret_cast<long long *>(s->red + 10);
+  k_bounds_init<<<1, 32, 0, st>>>(keys);
+  EDDY_LAUNCHED(ctx);
+  k_body_bounds<<<std::min(1184, (int)nblk(s->nb)), 256, 0, st>>>(s->nb, s->v, s->c, keys);
+  EDDY_LAUNCHED(ctx);
+  k_bounds_decode<<<1, 32, 0, st>>>(keys, s->red);
+  EDDY_LAUNCHED(ctx);
+  k_limimb<<<1, 32, 0, st>>>(d, ctx->ibax[0], ctx->ibax[4], ctx->ibax[5], s->red, s->dlim);
+  EDDY_LAUNCHED(ctx);
+  double bnd[10];
+  EDDY_CUDA(cudaMemcpyAsync(bnd, s->red, sizeof(double) * 10, cudaMemcpyDeviceToHost, st));
+  EDDY_CUDA(cudaMemcpyAsync(s->hcnt, s->dlim, sizeof(int) * 6, cudaMemcpyDeviceToHost, st));
+  EDDY_CUDA(cudaStreamSynchronize(st));
+  s->lim = Box6{s->hcnt[0], s->hcnt[1], s->hcnt[2], s->hcnt[3], s->hcnt[4], s->hcnt[5]};
+  // bins: triangle xy boxes (2-D) and centroids (3-D)
+  {
+    double lo[3] = {bnd[4], bnd[6], bnd[8]}, hi[3] = {bnd[5], bnd[7], bnd[9]};
+    if ((rc = build_bins(ctx, s->b2, 2, lo, hi, B2, s->nb, s->v, true))) return rc;
+    if ((rc = build_bins(ctx, s->b3, 3, lo, hi, B3, s->nb, s->c, false))) return rc;
+  }
+  const double zmin = ctx->h[12][1], zmax = ctx->h[12][d.nz - 1], zlen = zmax - zmin;
+  const double rzmin = std::fmin(zmin - zlen, -1.0e8), rzmax = std::fmax(zmax + zlen, 1.0e8);
+  const Box6 L = s->lim;
+  const size_t nc = (size_t)d.ncell;
+  const int ni = L.imax - L.imin + 1, nj = d.ny - 2;
+  for (int q = 0; q < 4; q++) {
+    EDDY_CUDA(cudaMemsetAsync(s->tag[q], 1, nc, st));
+    k_tag<<<nblk((long long)ni * nj, 128), 128, 0, st>>>(d, axes_of(ctx, q), s->dlim, s->v, s->b2, s->b2.start,
+                                                          s->b2.items, rzmin, rzmax, s->tag[q], ctx->err_flag);
+    EDDY_LAUNCHED(ctx);
+    if (L.kmax >= L.kmin) {
+      k_yper_i8<<<nblk((long long)ni * (L.kmax - L.kmin + 1)), 256, 0, st>>>(d, s->tag[q], L.imin, L.imax, L.kmin,
+                                                                               L.kmax);
+      EDDY_LAUNCHED(ctx);
+    }
+    // taguo into flag q
+    EDDY_CUDA(cudaMemsetAsync(s->flag[q], 0, nc, st));
+    const long long nbx = (long long)ni * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
+    if (nbx > 0) {
+      k_taguo<<<nblk(nbx), 256, 0, st>>>(d, L, 0, s->tag[q], s->flag[q]);
+      EDDY_LAUNCHED(ctx);
+    }
+    k_yper_i8<<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, s->flag[q], 1, d.nx, 1, d.nz);
+    EDDY_LAUNCHED(ctx);
+  }
+  for (int q = 0; q < 3; q++)
+    if ((rc = geom(ctx, q, q, 1))) return rc;
+  EDDY_CUDA(cudaMemsetAsync(s->flag[4], 0, nc, st));
+  {
+    const int i0 = std::max(2, L.imin);
+    const long long nbx = (long long)std::max(0, L.imax - i0 + 1) * (L.jmax - L.jmin + 1) *
+                          std::max(0, L.kmax - L.kmin + 1);
+    if (nbx > 0) {
+      k_flagp<<<nblk(nbx), 256, 0, st>>>(d, L, s->flag[0], s->flag[1], s->flag[2], s->flag[4]);
+      EDDY_LAUNCHED(ctx);
+    }
+  }
+  return geom(ctx, 3, 4, 0);
+}
+
+// forcing of an array by stencil set q, then its interior value at flag fq
+template <class T>
+static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, double interior, float *mirror,
+                   int mpitch) {
+  IbState *s = ibs(ctx);
+  const Dims &d = ctx->d;
+  cudaStream_t st = ctx->stream;
+  StencilSet &S = s->set[q];
+  for (int l = 0; l < S.nlev; l++) {
+    const int o0 = S.lev_start[l], o1 = S.lev_start[l + 1];
+    if (o1 > o0) {
+      k_force<T><<<nblk(o1 - o0, 128), 128, 0, st>>>(d, pitch, o0, o1, S.ijk, S.dijk, S.lu, S.indx, a, b0, mirror,
+                                                     mpitch);
+      EDDY_LAUNCHED(ctx);
+    }
+    k_yper_field<T><<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, pitch, a, mirror, mpitch);
+    EDDY_LAUNCHED(ctx);
+  }
+  const Box6 L = s->lim;
+  const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
+  if (nbx > 0) {
+    k_interior<T><<<nblk(nbx), 256, 0, st>>>(d, pitch, L, s->flag[fq], a, interior, mirror, mpitch);
+    EDDY_LAUNCHED(ctx);
+  }
+  k_yper_field<T><<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, pitch, a, mirror, mpitch);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+int ib_force(eddy_ctx *ctx, int q, int fq, double *a, double b0, double interior, float *mirror, int mpitch) {
+  if (!ibs(ctx)) return EDDY_OK;
+  return force_t<double>(ctx, q, fq, a, ctx->d.nx, b0, interior, mirror, mpitch);
+}
+
+int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, double interior) {
+  if (!ibs(ctx)) return EDDY_OK;
+  return force_t<float>(ctx, q, fq, a, pitch, b0, interior, nullptr, 0);
+}
+
+const double *ib_velocity(eddy_ctx *ctx) { return ibs(ctx) ? ibs(ctx)->vel : nullptr; }
+
+int ib_set_cadence(eddy_ctx *ctx, int every_substep) {
+  if (!ibs(ctx)) return EDDY_EINVAL;
+  ibs(ctx)->every_substep = every_substep ? 1 : 0;
+  return EDDY_OK;
+}
+
+int ib_every_substep(eddy_ctx *ctx) { return ibs(ctx) ? ibs(ctx)->every_substep : 0; }
+
+// value where flag fq == 1 (tvinterior), then y periodic planes
+int ib_interior(eddy_ctx *ctx, int fq, double *a, double value) {
+  IbState *s = ibs(ctx);
+  if (!s) return EDDY_OK;
+  const Dims &d = ctx->d;
+  const Box6 L = s->lim;
+  const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
+  if (nbx > 0) {
+    k_interior<double><<<nblk(nbx), 256, 0, ctx->stream>>>(d, d.nx, L, s->flag[fq], a, value, nullptr, 0);
+    EDDY_LAUNCHED(ctx);
+  }
+  k_yper_field<double><<<nblk((long long)d.nx * d.nz), 256, 0, ctx->stream>>>(d, d.nx, a, nullptr, 0);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+int ib_download(eddy_ctx *ctx, int which, signed char *out) {
+  IbState *s = ibs(ctx);
+  if (!s || which < 0 || which > 8) return EDDY_EINVAL;
+  signed char *src = which < 4 ? s->tag[which] : s->flag[which - 4];
+  EDDY_CUDA(cudaMemcpyAsync(out, src, (size_t)ctx->d.ncell, cudaMemcpyDeviceToHost, ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EDDY_OK;
+}
+
+int ib_limits(eddy_ctx *ctx, int *lim6) {
+  IbState *s = ibs(ctx);
+  if (!s) return EDDY_EINVAL;
+  lim6[0] = s->lim.imin; lim6[1] = s->lim.imax; lim6[2] = s->lim.jmin;
+  lim6[3] = s->lim.jmax; lim6[4] = s->lim.kmin; lim6[5] = s->lim.kmax;
+  return EDDY_OK;
+}
+
+int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
+                int *indx) {
+  IbState *s = ibs(ctx);
+  if (!s || q < 0 || q > 3) return EDDY_EINVAL;
+  StencilSet &S = s->set[q];
+  if (n) *n = S.n;
+  if (nlev) *nlev = S.nlev;
+  cudaStream_t st = ctx->stream;
+  if (S.n > 0) {
+    if (ijk) EDDY_CUDA(cudaMemcpyAsync(ijk, S.ijk, sizeof(int) * 3 * S.n, cudaMemcpyDeviceToHost, st));
+    if (dijk) EDDY_CUDA(cudaMemcpyAsync(dijk, S.dijk, sizeof(int) * 3 * S.n, cudaMemcpyDeviceToHost, st));
+    if (lev) EDDY_CUDA(cudaMemcpyAsync(lev, S.lev, sizeof(int) * S.n, cudaMemcpyDeviceToHost, st));
+    if (xn) EDDY_CUDA(cudaMemcpyAsync(xn, S.xn, sizeof(double) * 3 * S.n, cudaMemcpyDeviceToHost, st));
+    if (lu) EDDY_CUDA(cudaMemcpyAsync(lu, S.lu, sizeof(double) * 4 * S.n, cudaMemcpyDeviceToHost, st));
+    if (indx) EDDY_CUDA(cudaMemcpyAsync(indx, S.indx, sizeof(int) * 2 * S.n, cudaMemcpyDeviceToHost, st));
+  }
+  EDDY_CUDA(cudaStreamSynchronize(st));
+  return EDDY_OK;
+}

@@ -910,6 +910,14 @@ int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
     k_zero_faces32<<<nblk(ng), 256, 0, ctx->stream>>>(d, px, x->us, x->vs, x->ws);
     EDDY_LAUNCHED(ctx);
   }
+  // immersed body: momforc_mod2 + velinterior on the FP32 predictor velocities
+  if (ctx->ib) {
+    ProfScope ps(ctx, PROF_IB_FORCE);
+    const double *vb = ib_velocity(ctx);
+    if ((rc = ib_force32(ctx, 0, 0, x->us, px, vb[0], vb[0]))) return rc;
+    if ((rc = ib_force32(ctx, 1, 1, x->vs, px, vb[1], vb[1]))) return rc;
+    if ((rc = ib_force32(ctx, 2, 2, x->ws, px, vb[2], vb[2]))) return rc;
+  }
   {
     ProfScope ps(ctx, PROF_BC);
     if ((rc = bc_boundary<float>(ctx, px, x->us, x->vs, x->ws))) return rc;
@@ -945,6 +953,7 @@ int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
     EDDY_LAUNCHED(ctx);
     k_pupdate_m<<<nblk(d.ncell), 256, 0, ctx->stream>>>(d, px, f[EDDY_P], f[EDDY_DP], ctx->scal, x->p);
     EDDY_LAUNCHED(ctx);
+    if (ctx->ib && (rc = ib_force(ctx, 3, 4, f[EDDY_P], 0.0, 0.0, x->p, px))) return rc;
     long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
     k_pghost_m<<<nblk(ng), 256, 0, ctx->stream>>>(d, px, f[EDDY_P], x->p);
     EDDY_LAUNCHED(ctx);
@@ -971,6 +980,7 @@ int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
     x->dens = x->dens_alt;
     x->dens_alt = t;
     if ((rc = bc_boundinoutd_dens<float>(ctx, px, x->dens))) return rc;
+    if (ctx->ib && (rc = ib_force32(ctx, 3, 4, x->dens, px, 0.0, 0.0))) return rc;
   }
   return EDDY_OK;
 }

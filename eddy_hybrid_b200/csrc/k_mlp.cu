@@ -7,7 +7,8 @@
 //                       gradient) all map onto it.
 //  * k_mlp_infer      : fused per-cell inference: features of a 128-cell tile
 //                       -> four MMA layers with bias/SiLU epilogues from TMEM
-//                       -> nu_t, kappa_t.
+//                       -> coefficients C_nu, C_kappa -> nu_t = C_nu Delta^2 |S|,
+//                       kappa_t = C_kappa Delta^2 |S|.
 // The closure stands in for the dynamic procedure's test filtering and
 // coefficient averaging (src/vt.f:172-431).
 #include <cuda_bf16.h>
@@ -358,11 +359,14 @@ __global__ void __launch_bounds__(IT)
     unsigned t = tile * 128 + tid;
     bool valid = t < ninner;
     int i = d.ix1, j = d.jy1, k = d.kz1;
-    float f[NFEAT], del = 1.f;
+    float f[NFEAT], del = 1.f, dsr = 0.f;
     bool outside = false;
     if (valid) {
       interior_ijk(d, t, i, j, k);
       cell_features(d, m, cg, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
+      // Delta |S| = Delta sqrt(2 S_ij S_ij) from the raw gradient features
+      const float s01 = 0.5f * (f[1] + f[3]), s02 = 0.5f * (f[2] + f[6]), s12 = 0.5f * (f[5] + f[7]);
+      dsr = sqrtf(2.f * (f[0] * f[0] + f[4] * f[4] + f[8] * f[8] + 2.f * (s01 * s01 + s02 * s02 + s12 * s12)));
       for (int c = 0; c < NFEAT; c++) {
         f[c] = (f[c] - S.meta.mean[c]) * S.meta.istd[c];
         outside = outside || !(f[c] >= S.meta.lo[c] && f[c] <= S.meta.hi[c]);
@@ -401,8 +405,9 @@ __global__ void __launch_bounds__(IT)
         ka = fallback[q];
         nout++;
       } else {
-        nu = (double)del * S.meta.s_nu * softplus(v[0] + S.b4[0]);
-        ka = (double)del * S.meta.s_kappa * softplus(v[1] + S.b4[1]);
+        // nu_t = C_nu Delta^2 |S|, kappa_t = C_kappa Delta^2 |S|
+        nu = (double)del * (double)dsr * S.meta.s_nu * softplus(v[0] + S.b4[0]);
+        ka = (double)del * (double)dsr * S.meta.s_kappa * softplus(v[1] + S.b4[1]);
       }
       tv[q] = nu;
       kappa[q] = ka;

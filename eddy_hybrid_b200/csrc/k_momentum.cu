@@ -252,6 +252,11 @@ int launch_pressure_update(eddy_ctx *ctx) {
   EDDY_LAUNCHED(ctx);
   k_pupdate<<<(unsigned)((d.ncell + 255) / 256), 256, 0, ctx->stream>>>(d, p, dp, ctx->scal);
   EDDY_LAUNCHED(ctx);
+  // immersed body: correctpres_mod2 + presinterior (src/Eddy6.f:2881-2897)
+  if (ctx->ib) {
+    int rc = ib_force(ctx, 3, 4, p, 0.0, 0.0, nullptr, 0);
+    if (rc) return rc;
+  }
   long long nghost = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
   k_pghost<<<(unsigned)((nghost + 255) / 256), 256, 0, ctx->stream>>>(d, p);
   EDDY_LAUNCHED(ctx);

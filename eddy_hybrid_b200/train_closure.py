@@ -31,11 +31,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "closure_weights.npz")
 
 
-def smag_scale(X: np.ndarray) -> np.ndarray:
-    """Delta*|S| from the nine Delta-scaled velocity-gradient features."""
-    g = X[:, :9].reshape(-1, 3, 3).astype(np.float64)
-    S = 0.5 * (g + np.transpose(g, (0, 2, 1)))
-    return np.sqrt(2.0 * np.sum(S * S, axis=(1, 2)))
+smag_scale = cl.strain_scale
 
 
 def rel(a, b) -> float:
@@ -43,7 +39,7 @@ def rel(a, b) -> float:
 
 
 def harvest(grid=(192, 128, 256), frs=(0.5, 1.0, 2.0), spin=20, snaps=4, every=5, per_snap=1_600_000,
-            re=1e4, noise=0.3, seed=0, log=print):
+            re=1e4, noise=0.3, sphere=True, seed=0, log=print):
     """Run the plain solver at each Froude number and harvest (X, T) samples.
     Returns the training and held-out sets and the last solver (for training)."""
     mx, ly, nz_ = grid
@@ -52,11 +48,16 @@ def harvest(grid=(192, 128, 256), frs=(0.5, 1.0, 2.0), spin=20, snaps=4, every=5
     for fi, fr in enumerate(frs):
         # velocity fluctuations strong enough for the dynamic procedure to
         # produce a non-zero eddy viscosity (its coefficient is clipped at 0)
-        w = config.Workload(f"train_fr{fr}", mx=mx, ly=ly, nz_=nz_, re=re, fr=fr, dt=5e-4, sphere=False,
-                            noise=noise)
+        w = config.Workload(f"train_fr{fr}", mx=mx, ly=ly, nz_=nz_, re=re, fr=fr, dt=5e-4, sphere=sphere,
+                            noise=noise, body_speed=1.0)
         if solver is not None:
             solver.close()
         s = Solver(w)
+        if sphere:
+            from . import body as bd
+            h = float(np.diff(w.faces()[0]).min())
+            tri, nrm = bd.icosphere(bd.level_for_spacing(max(h, 0.004)))
+            s.set_body(tri, nrm, bd.body_velocity(w))
         s.load_initial(config.initial_fields(w, s.metric("dens_bg")[: w.nx]))
         s.initialize()
         s.step(spin)
@@ -79,7 +80,8 @@ def train(solver, X, T, epochs=8, batch=8192, lr=2e-3, seed=1, log=print):
     meta = cl.make_meta(X, T)
     c = cl.Closure(solver)
     c.set(meta, cl.init_theta(seed))
-    hist = c.train(X, cl.targets(T, meta), epochs=epochs, batch=batch, lr=lr, seed=seed)
+    Y, ok = cl.targets(X, T, meta)
+    hist = c.train(X[ok], Y[ok], epochs=epochs, batch=batch, lr=lr, seed=seed)
     log(f"  training loss by epoch: {np.round(hist, 4).tolist()}")
     meta, theta = c.get()
     return meta, theta, hist
@@ -102,7 +104,7 @@ def evaluate(meta, theta, X, T):
     a = silu(a @ P["W2"].T.astype(np.float64) + P["b2"])
     a = silu(a @ P["W3"].T.astype(np.float64) + P["b3"])
     o = a @ P["W4"].T.astype(np.float64) + P["b4"]
-    nu = np.logaddexp(0.0, o[:, 0]) * meta[4 * cl.NFEAT]
+    nu = np.logaddexp(0.0, o[:, 0]) * meta[4 * cl.NFEAT] * smag_scale(X)
     outside = ((Z < meta[2 * cl.NFEAT:3 * cl.NFEAT]) | (Z > meta[3 * cl.NFEAT:4 * cl.NFEAT])).any(axis=1)
     q = smag_scale(X)
     C = float(np.dot(q, T) / np.dot(q, q))
@@ -121,6 +123,7 @@ def main():
     ap.add_argument("--per-snap", type=int, default=1_600_000)
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--noise", type=float, default=0.3, help="initial velocity noise amplitude")
+    ap.add_argument("--no-sphere", action="store_true", help="train on flows without the immersed sphere")
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=DEFAULT_OUT)
@@ -128,14 +131,15 @@ def main():
     grid = tuple(int(v) for v in a.grid.split("x"))
     frs = tuple(float(v) for v in a.frs.split(","))
     t0 = time.time()
-    X, T, Xt, Tt, s = harvest(grid, frs, a.spin, a.snaps, a.every, a.per_snap, noise=a.noise)
+    X, T, Xt, Tt, s = harvest(grid, frs, a.spin, a.snaps, a.every, a.per_snap, noise=a.noise,
+                              sphere=not a.no_sphere)
     t1 = time.time()
     print(f"harvested {len(X)} training / {len(Xt)} held-out samples in {t1 - t0:.1f} s")
     meta, theta, hist = train(s, X, T, a.epochs, a.batch, a.lr)
     t2 = time.time()
     rep = evaluate(meta, theta, Xt, Tt)
     rep.update({"train_samples": int(len(X)), "grid": list(grid), "frs": list(frs), "epochs": a.epochs,
-                "noise": a.noise, "mean_target": float(T.mean()),
+                "noise": a.noise, "sphere": not a.no_sphere, "mean_target": float(T.mean()),
                 "loss_by_epoch": [float(v) for v in hist], "harvest_s": t1 - t0, "train_s": t2 - t1})
     print(json.dumps(rep))
     np.savez(a.out, meta=meta, theta=theta, report=json.dumps(rep))

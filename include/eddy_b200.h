@@ -125,6 +125,44 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps);
  * refine_sweeps FP64-residual iterative-refinement sweeps. */
 int eddy_poisson_solve(eddy_ctx *ctx, const double *rhs, double *sol, int on_device);
 
+/* ---- immersed boundary (src/rt.f, src/devel.f, src/matint.f, src/momforc.f,
+ * src/rbm.f) ---- */
+/* Attach a triangulated body (replaces the STL read of src/object.f and the
+ * motion law of src/rbm.f): nb triangles, vertices [nb][3][3] (x,y,z of the
+ * three vertices), unit outward normals [nb][3], translation velocity [3].
+ * nb = 0 detaches.  With a body attached, eddy_substep moves it, regenerates
+ * tags and stencils and applies the forcing (the IBM > 1 path). */
+int eddy_ib_set_body(eddy_ctx *ctx, int nb, const double *vertices, const double *normals,
+                     const double *velocity);
+/* Regeneration cadence: every_substep = 1 moves the body over alfxdt and
+ * regenerates at every substep (the reference's IBM > 1 path,
+ * src/Eddy6.f:2163); 0 (the default) moves it over the whole step and
+ * regenerates once, at the first substep. */
+int eddy_ib_set_cadence(eddy_ctx *ctx, int every_substep);
+/* RBM (src/rbm.f:2): translate the body over tmove. */
+int eddy_ib_move(eddy_ctx *ctx, double tmove);
+/* LIMIMB, TAG3D_MOD, taguo, geom_mod + mtrx, flagp for the current body
+ * position (src/Eddy6.f:2184-2380). */
+int eddy_ib_regen(eddy_ctx *ctx);
+/* momforc_mod2 on US, VS, WS then velinterior (src/Eddy6.f:2526-2575). */
+int eddy_ib_momforc(eddy_ctx *ctx);
+/* field EDDY_P: correctpres_mod2 + presinterior (src/Eddy6.f:2881-2897);
+ * EDDY_DENS: correctdens_mod2 + densinterior (:2972-2983). */
+int eddy_ib_correct(eddy_ctx *ctx, int field);
+/* int8 (NX,NY,NZ): which 0..3 = TAG3D results on the u, v, w, p grids
+ * (-1 inside, 1 outside); 4..7 = taguo flags u, v, w, tv and 8 = flagp
+ * (1 interior, -1 forcing point, 0 fluid). */
+int eddy_ib_flags(eddy_ctx *ctx, int which, signed char *out);
+/* body index box (LIMIMB): imin imax jmin jmax kmin kmax */
+int eddy_ib_limits(eddy_ctx *ctx, int *lim6);
+/* Stencils of set q (0 u, 1 v, 2 w, 3 p), ordered by dependency loop: n, the
+ * number of loops, forcing points ijk[3n] (1-based), extension offsets
+ * dijk[3n], loop lev[n], body intersection xn[3n], LU factors lu[4n]
+ * (column-major a11 a21 a12 a22) and pivots indx[2n].  Null arrays are
+ * skipped (call once with nulls for n). */
+int eddy_ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn,
+                     double *lu, int *indx);
+
 /* Mixed form only (no counterpart in the reference): max |d - L phi| of the
  * last refined Poisson solve before each sweep s, out[s] for s < min(n, 4);
  * entries past refine_sweeps are 0.  EDDY_EINVAL in the plain form. */
@@ -139,8 +177,9 @@ int eddy_max_divergence(eddy_ctx *ctx, double *out);
  * 2 divergence+forward FFT, 3 forward transform, 4 z line solves,
  * 5 backward transform, 6 backward FFT, 7 CORRECT, 8 pressure update,
  * 9 density, 10 eddy viscosity, 11 refinement residual + forward FFT,
- * 12 FP64/FP32 copies (mixed form).  eddy_profile_read synchronises, adds the
- * window's elapsed times per category to ms[13] / counts[13] (cumulative
+ * 12 FP64/FP32 copies (mixed form), 13 immersed-body regeneration, 14
+ * immersed-body forcing.  eddy_profile_read synchronises, adds the window's
+ * elapsed times per category to ms[15] / counts[15] (cumulative
  * since the mask was set) and starts a new window. */
 int eddy_profile_enable(eddy_ctx *ctx, unsigned mask);
 int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts);

@@ -87,6 +87,7 @@ typedef struct {
   double time;
   double pref_last;
   double qin_last, qout_last;
+  struct eo_ib *ib;  /* immersed body (NULL: none) */
 } eo_state;
 
 eo_state *eo_state_create(const eo_params *p, const eo_grid *g);
@@ -151,6 +152,51 @@ void eo_call_boundinout(eo_state *s, int idiv, double alfxdt);
 int eo_call_direct(eo_state *s, double alfxdt, int method);
 void eo_call_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt);
 double eo_max_divergence(eo_state *s);
+
+/* ---- immersed boundary (eo_ib.c; src/rt.f, devel.f, matint.f, momforc.f) ---- */
+typedef struct eo_ib eo_ib;
+/* stencils of one variable, ordered by dependency level */
+typedef struct {
+  int n, nlev;
+  int *i, *j, *k;       /* forcing points (1-based) */
+  int *di, *dj, *dk;    /* extension point offsets (grid-line stencil) */
+  int *lev;             /* dependency loop (1-based) */
+  int *indx;            /* [n][2] LU pivots (0-based rows) */
+  double *xn, *yn, *zn; /* body intersection */
+  double *lu;           /* [n][4] LU factors, column-major a11 a21 a12 a22 */
+  int *lev_start;       /* [nlev+1] offsets of each level */
+} eo_ib_set;
+/* vert [nb][3][3] (x,y,z of vertices a,b,c), normals [nb][3], vel[3] */
+eo_ib *eo_ib_create(const eo_grid *g, int nb, const double *vert, const double *normals, const double *vel);
+void eo_ib_free(eo_ib *ib);
+void eo_ib_limimb(eo_ib *ib);
+void eo_ib_tag(eo_ib *ib, int q);
+void eo_ib_taguo(eo_ib *ib, int q, int fq);
+void eo_ib_flagp(eo_ib *ib);
+void eo_ib_geom(eo_ib *ib, int q, int fq, int imn);
+void eo_ib_regen(eo_ib *ib);
+void eo_ib_move(eo_ib *ib, double tmove);
+void eo_ib_force(eo_ib *ib, int q, double *a, double b0);
+void eo_ib_interior(eo_ib *ib, int fq, double *a, double value);
+const int *eo_ib_limits(const eo_ib *ib);
+const signed char *eo_ib_tags(const eo_ib *ib, int q);
+const signed char *eo_ib_flags(const eo_ib *ib, int fq);
+const eo_ib_set *eo_ib_stencils(const eo_ib *ib, int q);
+void eo_ib_body(const eo_ib *ib, double *v, double *c);
+const double *eo_ib_velocity(const eo_ib *ib);
+void eo_ib_set_cadence(eo_ib *ib, int every);
+int eo_ib_every(const eo_ib *ib);
+int eo_locate(const double *xx1, int n, double x);
+int eo_segtriint(const double *p1, const double *p2, const double *a, const double *b, const double *c,
+                 double *xm);
+void eo_lu2(double *a, int *indx);
+void eo_lusolve2(const double *a, const int *indx, double *b);
+int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int jm, int km, const int *inn,
+                    int nn, double *xn, int *dd);
+/* attach a body to the solver: the substep then moves it, regenerates the
+ * stencils and applies the forcing (src/Eddy6.f:2163-2380, 2526-2575,
+ * 2881-2897, 2972-2983) */
+void eo_state_set_ib(eo_state *s, eo_ib *ib);
 
 /* ---- deterministic noise: SplitMix64 counter generator ---- */
 uint64_t eo_splitmix64(uint64_t x);

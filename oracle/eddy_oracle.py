@@ -35,6 +35,12 @@ class Params(C.Structure):
                 ("dspngx3in", C.c_int), ("dspngx3out", C.c_int)]
 
 
+class IBSet(C.Structure):
+    _fields_ = [("n", C.c_int), ("nlev", C.c_int)] + \
+        [(f, C.POINTER(C.c_int)) for f in ("i", "j", "k", "di", "dj", "dk", "lev", "indx")] + \
+        [(f, C.POINTER(C.c_double)) for f in ("xn", "yn", "zn", "lu")] + [("lev_start", C.POINTER(C.c_int))]
+
+
 def make_params(d: dict) -> Params:
     p = Params()
     for k, v in d.items():
@@ -94,6 +100,31 @@ def lib():
         L.eo_call_direct.restype = C.c_int
         L.eo_max_divergence.argtypes = [C.c_void_p]
         L.eo_max_divergence.restype = C.c_double
+        vp = C.c_void_p
+        L.eo_ib_create.restype = vp
+        L.eo_ib_create.argtypes = [vp, C.c_int, dp, dp, dp]
+        L.eo_ib_free.argtypes = [vp]
+        for name in ("eo_ib_regen", "eo_ib_limimb", "eo_ib_flagp"):
+            getattr(L, name).argtypes = [vp]
+        L.eo_ib_tag.argtypes = [vp, C.c_int]
+        L.eo_ib_taguo.argtypes = [vp, C.c_int, C.c_int]
+        L.eo_ib_geom.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.eo_ib_move.argtypes = [vp, C.c_double]
+        L.eo_ib_set_cadence.argtypes = [vp, C.c_int]
+        L.eo_ib_force.argtypes = [vp, C.c_int, dp, C.c_double]
+        L.eo_ib_interior.argtypes = [vp, C.c_int, dp, C.c_double]
+        L.eo_ib_limits.restype = C.POINTER(C.c_int)
+        L.eo_ib_limits.argtypes = [vp]
+        L.eo_ib_tags.restype = C.POINTER(C.c_byte)
+        L.eo_ib_tags.argtypes = [vp, C.c_int]
+        L.eo_ib_flags.restype = C.POINTER(C.c_byte)
+        L.eo_ib_flags.argtypes = [vp, C.c_int]
+        L.eo_ib_stencils.restype = C.POINTER(IBSet)
+        L.eo_ib_stencils.argtypes = [vp, C.c_int]
+        L.eo_ib_body.argtypes = [vp, dp, dp]
+        L.eo_state_set_ib.argtypes = [vp, vp]
+        L.eo_locate.restype = C.c_int
+        L.eo_locate.argtypes = [dp, C.c_int, C.c_double]
         _lib = L
     return _lib
 
@@ -215,3 +246,75 @@ class OracleSolver:
         if getattr(self, "h", None):
             lib().eo_state_free(self.h)
             self.h = None
+
+
+class OracleIB:
+    """Immersed body attached to an OracleSolver (restated TAG3D_MOD, taguo,
+    flagp, grid-line geom/mtrx, momforc/correctpres, RBM translation)."""
+
+    VARS = ("u", "v", "w", "p")
+
+    def __init__(self, solver: "OracleSolver", tri: np.ndarray, normals: np.ndarray, vel=(0.0, 0.0, 0.0),
+                 attach: bool = True):
+        self.s = solver
+        tri = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1)
+        nrm = np.ascontiguousarray(normals, dtype=np.float64).reshape(-1)
+        v = np.ascontiguousarray(vel, dtype=np.float64)
+        self.nb = len(tri) // 9
+        self.h = lib().eo_ib_create(solver.grid.h, self.nb, _ptr(tri), _ptr(nrm), _ptr(v))
+        if attach:
+            lib().eo_state_set_ib(solver.h, self.h)
+
+    def regen(self):
+        lib().eo_ib_regen(self.h)
+
+    def set_cadence(self, every_substep: int):
+        lib().eo_ib_set_cadence(self.h, every_substep)
+
+    def move(self, t: float):
+        lib().eo_ib_move(self.h, t)
+
+    def limits(self):
+        p = lib().eo_ib_limits(self.h)
+        return tuple(p[a] for a in range(6))
+
+    def _grid3(self, ptr):
+        nx, ny, nz = self.s.shape
+        a = np.ctypeslib.as_array(ptr, shape=(nx * ny * nz,)).copy()
+        return a.reshape((nx, ny, nz), order="F")
+
+    def tags(self, q: int) -> np.ndarray:
+        return self._grid3(lib().eo_ib_tags(self.h, q))
+
+    def flags(self, fq: int) -> np.ndarray:
+        return self._grid3(lib().eo_ib_flags(self.h, fq))
+
+    def stencils(self, q: int) -> dict:
+        S = lib().eo_ib_stencils(self.h, q).contents
+        n = S.n
+        out = {"n": n, "nlev": S.nlev}
+        for f in ("i", "j", "k", "di", "dj", "dk", "lev"):
+            out[f] = np.ctypeslib.as_array(getattr(S, f), shape=(n,)).copy() if n else np.zeros(0, np.int32)
+        for f in ("xn", "yn", "zn"):
+            out[f] = np.ctypeslib.as_array(getattr(S, f), shape=(n,)).copy() if n else np.zeros(0)
+        out["lu"] = np.ctypeslib.as_array(S.lu, shape=(4 * n,)).copy().reshape(n, 4) if n else np.zeros((0, 4))
+        out["indx"] = np.ctypeslib.as_array(S.indx, shape=(2 * n,)).copy().reshape(n, 2) if n else \
+            np.zeros((0, 2), np.int32)
+        out["lev_start"] = np.ctypeslib.as_array(S.lev_start, shape=(S.nlev + 1,)).copy()
+        return out
+
+    def force(self, q: int, a: np.ndarray, b0: float) -> np.ndarray:
+        a = np.asfortranarray(a, dtype=np.float64).copy(order="F")
+        lib().eo_ib_force(self.h, q, _ptr(a), b0)
+        return a
+
+    def interior(self, fq: int, a: np.ndarray, value: float) -> np.ndarray:
+        a = np.asfortranarray(a, dtype=np.float64).copy(order="F")
+        lib().eo_ib_interior(self.h, fq, _ptr(a), value)
+        return a
+
+    def body(self):
+        v = np.zeros(9 * self.nb)
+        c = np.zeros(3 * self.nb)
+        lib().eo_ib_body(self.h, _ptr(v), _ptr(c))
+        return v.reshape(self.nb, 3, 3), c.reshape(self.nb, 3)

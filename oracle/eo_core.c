@@ -580,6 +580,13 @@ void eo_pressure_update(eo_state *s) {
   pref = pref / (double)(NY - 2);
   s->pref_last = pref;
   for (long q = 0; q < s->ncell; q++) p[q] = p[q] - pref;
+  /* immersed body: pressure at the pressure forcing points and inside
+   * (correctpres_mod2 + presinterior, :2881-2897; their effect on the ghost
+   * planes is recomputed by the passes below) */
+  if (s->ib) {
+    eo_ib_force(s->ib, 3, p, 0.0);
+    eo_ib_interior(s->ib, 4, p, 0.0);
+  }
   /* first ghost pass (:2814-2853) */
   if (g->mp == 0) { fill_x_plane(g, p, 1, g->ix2, 1., 0); fill_x_plane(g, p, NX, g->ix1, 1., 0); }
   else { fill_x_plane(g, p, 1, g->ix1, -1., 0); fill_x_plane(g, p, NX, g->ix2, -1., 0); }

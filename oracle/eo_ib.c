@@ -1,0 +1,745 @@
+/*
+ * eo_ib.c -- immersed-boundary restatement (TEST INFRASTRUCTURE ONLY: the
+ * checker for the CUDA immersed-boundary kernels).
+ *
+ * Follows, for one body in a Cartesian domain on a single rank:
+ *   LIMIMB            src/object.f:713-800   body index limits from centroids
+ *   TAG3D_MOD         src/rt.f:2704-3020     ray casting along z, IMBDCMP=0
+ *   segtriint         src/rt.f:1179-1226     segment/triangle
+ *   intersect_triangle src/rt.f:1263-1330    Moller-Trumbore, det eps 1e-18,
+ *                                            u+v-1 > 1e-7 edge tolerance
+ *   LOCATE            src/numrec.f:390-422   bisection (restated)
+ *   taguo             src/devel.f:8-110      interior / forcing / fluid flags
+ *   flagp             src/matint.f:135-260   pressure flags
+ *   forcpts           src/matint.f:3388-3430 forcing-point list (k, j, i order)
+ *   grid_intr         src/matint.f:800-1160  grid-line stencil (26 directions)
+ *   geom_mod          src/devel.f:9265-9800  dependency loops
+ *   mtrx              src/devel.f:1159-1290  2x2 systems
+ *   ludcmp / lubksb   src/numrec.f:22-118    LU with implicit partial pivoting
+ *                                            (the published Crout algorithm,
+ *                                            restated for n = 2)
+ *   momforc_mod2      src/momforc.f:1248-1485 explicit forcing
+ *   velinterior       src/momforc.f:186-300
+ *   correctpres_mod2  src/momforc.f:1617-1760, correctdens_mod2 :1762
+ *   presinterior      src/devel.f:1525, densinterior src/momforc.f:574
+ *   RBM, ubd/vbd/wbd  src/rbm.f:2-40,168-309 (translation at a constant velocity)
+ *
+ * Restatement choices (the same in the CUDA path):
+ *  * TAG3D's 2-D kd-tree (ANN committee4) only prunes the triangles tested
+ *    against a column; here every triangle whose xy bounding box contains the
+ *    column is tested, which is the set the reference's bounding-box test
+ *    accepts when the search radius covers the triangle.
+ *  * geom_mod's normal-direction and closest-point stencils (norm_intr,
+ *    closest_intr, ANN committee3 + recheckface) are not restated: every
+ *    forcing point takes the grid-line stencil of grid_intr (mrk = 2), with
+ *    the 3-D nearest-centroid candidate lists of sizes 3, 5, nntr3d computed
+ *    exactly (ties by triangle index).  A point whose extension point is a
+ *    forcing point waits for a later dependency loop; a loop that resolves no
+ *    point ends the search and the remaining points are dropped, as are
+ *    points with no valid grid-line stencil (the velocity flag becomes fluid,
+ *    the pressure flag interior, as geom_mod's "not valid" branch does).
+ *  * The body translates at a constant velocity: ubd/vbd/wbd are constants.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "eddy_oracle.h"
+
+#define NCR 16
+#define NNTR3D 25
+#define NFLU 30
+
+static long IDX(const eo_grid *g, int i, int j, int k) {
+  return (long)(i - 1) + (long)g->nx * ((long)(j - 1) + (long)g->ny * (long)(k - 1));
+}
+
+/* ---- LOCATE (src/numrec.f:390-422): jl with xx(jl) < x <= xx(jl+1), 1-based */
+int eo_locate(const double *xx1, int n, double x) {
+  /* xx1 is 1-based: xx1[1..n] */
+  int jl = 0, ju = n + 1;
+  if (xx1[1] == x) return 1;
+  int asc = xx1[n] > xx1[1];
+  while (ju - jl > 1) {
+    int jm = (ju + jl) / 2;
+    if (asc == (x > xx1[jm]))
+      jl = jm;
+    else
+      ju = jm;
+  }
+  return jl;
+}
+
+/* ---- intersect_triangle (src/rt.f:1263-1330) ---- */
+static void sub3(double *r, const double *a, const double *b) {
+  r[0] = a[0] - b[0];
+  r[1] = a[1] - b[1];
+  r[2] = a[2] - b[2];
+}
+static void cross3(double *r, const double *x, const double *y) {
+  r[0] = x[1] * y[2] - y[1] * x[2];
+  r[1] = x[2] * y[0] - y[2] * x[0];
+  r[2] = x[0] * y[1] - y[0] * x[1];
+}
+static double dot3(const double *x, const double *y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; }
+
+static int intersect_triangle(const double *orig, const double *dir, const double *v0, const double *v1,
+                              const double *v2, double *t, double *u, double *v) {
+  double e1[3], e2[3], pv[3], tv[3], qv[3];
+  *t = 0.;
+  *u = 0.;
+  *v = 0.;
+  sub3(e1, v1, v0);
+  sub3(e2, v2, v0);
+  cross3(pv, dir, e2);
+  double det = dot3(e1, pv);
+  if (det > -1.0e-18 && det < 1.0e-18) return 2;
+  double inv = 1.0 / det;
+  sub3(tv, orig, v0);
+  *u = dot3(tv, pv) * inv;
+  if (*u < 0.0 || *u > 1.0) return 3;
+  cross3(qv, tv, e1);
+  *v = dot3(dir, qv) * inv;
+  if (*v < 0.0 || (*u + *v - 1.) > 1.e-07) return 3;
+  *t = dot3(e2, qv) * inv;
+  return 1;
+}
+
+/* segtriint (src/rt.f:1179-1226): 1 and the point when segment p1->p2 meets
+ * triangle (a,b,c) */
+int eo_segtriint(const double *p1, const double *p2, const double *a, const double *b, const double *c,
+                 double *xm) {
+  double q[3] = {p1[0], p1[1], p1[2]}, r[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
+  double t, u, v;
+  int code = intersect_triangle(q, r, a, b, c, &t, &u, &v);
+  if (code == 1 && (t > 1.0 || t < 0.0)) return 0;
+  if (code == 2) code = intersect_triangle(q, r, a, c, b, &t, &u, &v);
+  xm[0] = q[0] + t * r[0];
+  xm[1] = q[1] + t * r[1];
+  xm[2] = q[2] + t * r[2];
+  return code == 1;
+}
+
+/* ---- state ---- */
+struct eo_ib {
+  const eo_grid *g;
+  int nb;
+  double *v, *c, *n;  /* vertices [nb][3][3], centroids [nb][3], normals [nb][3] */
+  double vel[3];
+  int lim[6];         /* imin imax jmin jmax kmin kmax */
+  signed char *tag[4];  /* TAG3D IBS per variable u, v, w, p */
+  signed char *flag[5]; /* taguo flags u, v, w, tv; flagp p */
+  eo_ib_set set[4];     /* stencils u, v, w, p */
+  int nntr3d, nflu, itagy;
+  int every; /* 1: move + regenerate every substep, 0: once per step */
+};
+
+eo_ib *eo_ib_create(const eo_grid *g, int nb, const double *vert, const double *normals, const double *vel) {
+  eo_ib *ib = (eo_ib *)calloc(1, sizeof(eo_ib));
+  ib->g = g;
+  ib->nb = nb;
+  ib->v = (double *)malloc(sizeof(double) * 9 * nb);
+  ib->c = (double *)malloc(sizeof(double) * 3 * nb);
+  ib->n = (double *)malloc(sizeof(double) * 3 * nb);
+  memcpy(ib->v, vert, sizeof(double) * 9 * nb);
+  memcpy(ib->n, normals, sizeof(double) * 3 * nb);
+  for (int t = 0; t < nb; t++)
+    for (int d = 0; d < 3; d++) {
+      const double *tv = ib->v + 9 * t;
+      ib->c[3 * t + d] = ((tv[d] + tv[3 + d]) + tv[6 + d]) / 3.0;
+    }
+  for (int d = 0; d < 3; d++) ib->vel[d] = vel[d];
+  long nc = (long)g->nx * g->ny * g->nz;
+  for (int q = 0; q < 4; q++) ib->tag[q] = (signed char *)calloc(nc, 1);
+  for (int q = 0; q < 5; q++) ib->flag[q] = (signed char *)calloc(nc, 1);
+  ib->nntr3d = NNTR3D;
+  ib->nflu = NFLU;
+  ib->itagy = 0;
+  return ib;
+}
+
+static void set_free(eo_ib_set *s) {
+  free(s->i); free(s->j); free(s->k); free(s->di); free(s->dj); free(s->dk);
+  free(s->lev); free(s->indx); free(s->xn); free(s->yn); free(s->zn); free(s->lu); free(s->lev_start);
+  memset(s, 0, sizeof(*s));
+}
+
+void eo_ib_free(eo_ib *ib) {
+  if (!ib) return;
+  free(ib->v); free(ib->c); free(ib->n);
+  for (int q = 0; q < 4; q++) { free(ib->tag[q]); set_free(&ib->set[q]); }
+  for (int q = 0; q < 5; q++) free(ib->flag[q]);
+  free(ib);
+}
+
+/* coordinates of variable q: 0 u (xu, yc, zc), 1 v (xc, yv, zc), 2 w (xc, yc, zw), 3 p (xc, yc, zc) */
+static void var_axes(const eo_grid *g, int q, const double **x, const double **y, const double **z) {
+  *x = (q == 0) ? g->xu : g->xc;
+  *y = (q == 1) ? g->yv : g->yc;
+  *z = (q == 2) ? g->zw : g->zc;
+}
+
+/* ---- LIMIMB (src/object.f:713-800), Cartesian, single rank ---- */
+void eo_ib_limimb(eo_ib *ib) {
+  const eo_grid *g = ib->g;
+  double mnx = 1e300, mxx = -1e300, mnz = 1e300, mxz = -1e300;
+  for (int t = 0; t < ib->nb; t++) {
+    mnx = fmin(mnx, ib->c[3 * t]);
+    mxx = fmax(mxx, ib->c[3 * t]);
+    mnz = fmin(mnz, ib->c[3 * t + 2]);
+    mxz = fmax(mxz, ib->c[3 * t + 2]);
+  }
+  int imin = eo_locate(g->xu, g->nx, mnx), imax = eo_locate(g->xu, g->nx, mxx);
+  int kmin = g->nz, kmax = 1;
+  if (mnz < g->zw[g->nz] && mxz >= g->zc[1]) {
+    kmin = eo_locate(g->zw, g->nz, mnz);
+    kmax = eo_locate(g->zw, g->nz, mxz);
+  }
+  imin -= 3;
+  imax += 3;
+  if (imin < 1) imin = 1;
+  if (imax > g->nx - 1) imax = g->nx - 1;
+  if (kmax >= kmin) {
+    kmin -= 3;
+    kmax += 3;
+  }
+  if (kmin < 1) kmin = 1; /* ITYPE(5) /= 500 */
+  if (kmax > g->nz) kmax = g->nz;
+  ib->lim[0] = imin; ib->lim[1] = imax;
+  ib->lim[2] = 2; ib->lim[3] = g->ny - 1;
+  ib->lim[4] = kmin; ib->lim[5] = kmax;
+}
+
+/* ---- TAG3D_MOD (src/rt.f:2704-3020) for variable q ---- */
+void eo_ib_tag(eo_ib *ib, int q) {
+  const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
+  signed char *ibs = ib->tag[q];
+  long nc = (long)g->nx * g->ny * g->nz;
+  for (long t = 0; t < nc; t++) ibs[t] = 1;
+  const double zmin = g->zw[1], zmax = g->zw[g->nz - 1], zlen = zmax - zmin;
+  const double rzmin = fmin(zmin - zlen, -1.0e8), rzmax = fmax(zmax + zlen, 1.0e8);
+  for (int i = ib->lim[0]; i <= ib->lim[1]; i++)
+    for (int j = 2; j <= g->ny - 1; j++) {
+      const double xcc = X[i], ycc = Y[j];
+      double zc_[NCR], zo[NCR];
+      int nc_ = 0;
+      for (int t = 0; t < ib->nb; t++) {
+        const double *a = ib->v + 9 * t, *b = a + 3, *c = a + 6;
+        if (ycc >= fmin(fmin(a[1], b[1]), c[1]) && ycc <= fmax(fmax(a[1], b[1]), c[1]) &&
+            xcc >= fmin(fmin(a[0], b[0]), c[0]) && xcc <= fmax(fmax(a[0], b[0]), c[0])) {
+          double p1[3] = {xcc, ycc, rzmin}, p2[3] = {xcc, ycc, rzmax}, xm[3];
+          if (eo_segtriint(p1, p2, a, b, c, xm)) {
+            if (nc_ < NCR) zc_[nc_] = xm[2];
+            nc_++;
+          }
+        }
+      }
+      if (nc_ > NCR) nc_ = NCR;
+      /* selection sort ascending; ties take the last minimum (.le.) */
+      for (int i1 = 0; i1 < nc_; i1++) {
+        double ztmin = 1.0e10;
+        int isave = 0;
+        for (int i2 = 0; i2 < nc_; i2++)
+          if (zc_[i2] <= ztmin) {
+            ztmin = zc_[i2];
+            isave = i2;
+          }
+        zo[i1] = ztmin;
+        zc_[isave] = 2.0e10;
+      }
+      /* drop crossings within 1e-6 of an earlier one */
+      double zz[NCR];
+      for (int i1 = 0; i1 < nc_; i1++) zz[i1] = zo[i1];
+      int ncl = 0;
+      for (int i1 = 0; i1 < nc_; i1++) {
+        int ndp = 0;
+        for (int i2 = 0; i2 < nc_; i2++)
+          if (fabs(zz[i2] - zz[i1]) < 1.e-06 && i1 > i2) ndp++;
+        if (ndp == 0) zo[ncl++] = zz[i1];
+      }
+      if (ncl == 1) ncl = 0;
+      for (int ic = 0; ic + 1 < ncl; ic += 2) {
+        int k1 = eo_locate(Z, g->nz, zo[ic]);
+        int k2 = eo_locate(Z, g->nz, zo[ic + 1]);
+        if (k2 > k1)
+          for (int k = k1 + 1; k <= k2; k++) ibs[IDX(g, i, j, k)] = -1;
+      }
+    }
+  /* y periodic ghosts over the body's k range */
+  for (int k = ib->lim[4]; k <= ib->lim[5]; k++)
+    for (int i = ib->lim[0]; i <= ib->lim[1]; i++) {
+      ibs[IDX(g, i, 1, k)] = ibs[IDX(g, i, g->ny - 1, k)];
+      ibs[IDX(g, i, g->ny, k)] = ibs[IDX(g, i, 2, k)];
+    }
+}
+
+/* ---- taguo (src/devel.f:8-110): flago 1 interior, -1 forcing, 0 fluid ---- */
+void eo_ib_taguo(eo_ib *ib, int q, int fq) {
+  const eo_grid *g = ib->g;
+  const signed char *f = ib->tag[q];
+  signed char *fo = ib->flag[fq];
+  long nc = (long)g->nx * g->ny * g->nz;
+  memset(fo, 0, nc);
+  const int *L = ib->lim;
+  for (int k = L[4]; k <= L[5]; k++)
+    for (int j = L[2]; j <= L[3]; j++)
+      for (int i = L[0]; i <= L[1]; i++)
+        if (f[IDX(g, i, j, k)] == -1) fo[IDX(g, i, j, k)] = 1;
+  for (int k = 1; k <= g->nz; k++)
+    for (int i = 1; i <= g->nx; i++) {
+      fo[IDX(g, i, 1, k)] = fo[IDX(g, i, g->ny - 1, k)];
+      fo[IDX(g, i, g->ny, k)] = fo[IDX(g, i, 2, k)];
+    }
+  const int nn = ib->itagy == 0 ? 2 : 0;
+  const int k1 = L[4] > 2 ? L[4] : 2, k2 = L[5] < g->nz - 1 ? L[5] : g->nz - 1;
+  for (int k = k1; k <= k2; k++)
+    for (int j = L[2]; j <= L[3]; j++)
+      for (int i = (L[0] > 2 ? L[0] : 2); i <= L[1]; i++) {
+        int c = f[IDX(g, i, j, k)];
+        int nb[6] = {c + f[IDX(g, i + 1, j, k)], c + f[IDX(g, i - 1, j, k)], c + f[IDX(g, i, j, k + 1)],
+                     c + f[IDX(g, i, j, k - 1)], c + f[IDX(g, i, j - 1, k)], c + f[IDX(g, i, j + 1, k)]};
+        long prod = 1;
+        for (int m = 0; m < 6 - nn; m++) prod *= nb[m];
+        if (prod == 0 && c == 1) fo[IDX(g, i, j, k)] = -1;
+      }
+  for (int k = 1; k <= g->nz; k++)
+    for (int i = 1; i <= g->nx; i++) {
+      fo[IDX(g, i, 1, k)] = fo[IDX(g, i, g->ny - 1, k)];
+      fo[IDX(g, i, g->ny, k)] = fo[IDX(g, i, 2, k)];
+    }
+}
+
+/* ---- flagp (src/matint.f:135-260) ---- */
+void eo_ib_flagp(eo_ib *ib) {
+  const eo_grid *g = ib->g;
+  const signed char *fu = ib->flag[0], *fv = ib->flag[1], *fw = ib->flag[2];
+  signed char *fp = ib->flag[4];
+  long nc = (long)g->nx * g->ny * g->nz;
+  memset(fp, 0, nc);
+  const int *L = ib->lim;
+  for (int pass = 0; pass < 2; pass++) {
+    int ka = pass == 0 ? L[4] : (L[4] > 2 ? L[4] : 2);
+    int kb = pass == 0 ? 1 : L[5];
+    for (int k = ka; k <= kb; k++)
+      for (int j = L[2]; j <= L[3]; j++)
+        for (int i = (L[0] > 2 ? L[0] : 2); i <= L[1]; i++) {
+          int it[6], n;
+          if (pass == 0) {
+            it[0] = fu[IDX(g, i, j, k)]; it[1] = fu[IDX(g, i - 1, j, k)]; it[2] = fw[IDX(g, i, j, k)];
+            it[3] = fv[IDX(g, i, j, k)]; it[4] = fv[IDX(g, i, j - 1, k)];
+            n = 5;
+          } else {
+            it[0] = fu[IDX(g, i, j, k)]; it[1] = fu[IDX(g, i - 1, j, k)]; it[2] = fw[IDX(g, i, j, k)];
+            it[3] = fw[IDX(g, i, j, k - 1)]; it[4] = fv[IDX(g, i, j, k)]; it[5] = fv[IDX(g, i, j - 1, k)];
+            n = 6;
+          }
+          int ifld = 0, ibdy = 0, ibnd = 0;
+          for (int m = 0; m < n; m++) {
+            ifld += it[m] == 0;
+            ibdy += it[m] > 0;
+            ibnd += it[m] < 0;
+          }
+          signed char *o = &fp[IDX(g, i, j, k)];
+          if ((ibdy + ibnd) != 0 && ifld != 0) *o = -1;
+          if (ifld == 0 && ibnd != 0) *o = -1;
+          if (ifld == 0 && ibnd == 0 && ibdy != 0) *o = 1;
+        }
+  }
+}
+
+/* ---- exact k nearest centroids (ties by triangle index) ---- */
+static void knn(const eo_ib *ib, const double *q, int k, int *out) {
+  double best[NNTR3D];
+  int bi[NNTR3D];
+  int m = 0;
+  for (int t = 0; t < ib->nb; t++) {
+    const double *c = ib->c + 3 * t;
+    double dx = c[0] - q[0], dy = c[1] - q[1], dz = c[2] - q[2];
+    double d2 = dx * dx + dy * dy + dz * dz;
+    if (m < k || d2 < best[m - 1]) {
+      int p = m < k ? m : k - 1;
+      while (p > 0 && best[p - 1] > d2) {
+        best[p] = best[p - 1];
+        bi[p] = bi[p - 1];
+        p--;
+      }
+      best[p] = d2;
+      bi[p] = t;
+      if (m < k) m++;
+    }
+  }
+  for (int a = 0; a < m; a++) out[a] = bi[a];
+  for (int a = m; a < k; a++) out[a] = -1;
+}
+
+static const int GIND[26][3] = {
+    {1, 0, 0},  {-1, 0, 0}, {0, 0, 1},   {0, 0, -1},  {1, 0, 1},   {1, 0, -1},  {-1, 0, 1},
+    {-1, 0, -1}, {0, 1, 0},  {0, -1, 0},  {1, 1, 0},   {-1, 1, 0},  {0, 1, 1},   {0, 1, -1},
+    {1, 1, 1},  {1, 1, -1}, {-1, 1, 1},  {-1, 1, -1}, {1, -1, 0},  {-1, -1, 0}, {0, -1, 1},
+    {0, -1, -1}, {1, -1, 1}, {1, -1, -1}, {-1, -1, 1}, {-1, -1, -1}};
+
+static double unitdot(const double *x, const double *xn, const double *nrm) {
+  double a[3] = {x[0] - xn[0], x[1] - xn[1], x[2] - xn[2]};
+  double ma = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  a[0] = a[0] / ma; a[1] = a[1] / ma; a[2] = a[2] / ma;
+  double b[3] = {nrm[0], nrm[1], nrm[2]};
+  double mb = sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+  b[0] = b[0] / mb; b[1] = b[1] / mb; b[2] = b[2] / mb;
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+/* grid_intr (src/matint.f:800-1160), isrt = 0, igrdint = 1: returns 1 (fluid
+ * extension point), -1 (extension point is a forcing point), 0 (no
+ * intersection), -2 (intersections only behind) */
+int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int jm, int km, const int *inn,
+                    int nn, double *xn, int *dd) {
+  const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
+  double crit[26];
+  int ord[26];
+  for (int i = 0; i < 26; i++) {
+    int f = flag[IDX(g, im + GIND[i][0], jm + GIND[i][1], km + GIND[i][2])];
+    crit[i] = -2.0;
+    if (f == 0)
+      crit[i] = 1.0;
+    else if (f < 0)
+      crit[i] = 0.5;
+  }
+  int nphy = 0;
+  for (int i = 0; i < 26; i++) {
+    int b = 0;
+    for (int m = 1; m < 26; m++)
+      if (crit[m] > crit[b]) b = m;
+    ord[i] = b;
+    crit[b] = -10.0;
+    if (flag[IDX(g, im + GIND[i][0], jm + GIND[i][1], km + GIND[i][2])] <= 0) nphy++;
+  }
+  int intrs = 0, ibint = 0;
+  double xint[26][3];
+  int tri[26], dir[26], icand[26];
+  const double p0[3] = {X[im], Y[jm], Z[km]};
+  for (int i = 0; i < nphy; i++) {
+    const int ii = ord[i];
+    const int id = GIND[ii][0], jd = GIND[ii][1], kd = GIND[ii][2];
+    const int fext = flag[IDX(g, im + id, jm + jd, km + kd)];
+    if (fext > 0) continue;
+    const double pe[3] = {X[im + id], Y[jm + jd], Z[km + kd]};
+    double r[3] = {pe[0] - p0[0], pe[1] - p0[1], pe[2] - p0[2]};
+    r[0] = r[0] * 10.0; r[1] = r[1] * 10.0; r[2] = r[2] * 10.0;
+    const double s1[3] = {p0[0] - r[0], p0[1] - r[1], p0[2] - r[2]};
+    const double s2[3] = {p0[0] + r[0], p0[1] + r[1], p0[2] + r[2]};
+    for (int in = 0; in < nn; in++) {
+      const int n = inn[in];
+      if (n < 0) continue;
+      const double *a = ib->v + 9 * n;
+      double xm[3];
+      if (eo_segtriint(s1, s2, a, a + 3, a + 6, xm)) {
+        ibint++;
+        double dp = unitdot(pe, p0, ib->n + 3 * n);
+        if (dp > 0.0) {
+          if (fext == 0 || fext < 0) {
+            xint[intrs][0] = xm[0]; xint[intrs][1] = xm[1]; xint[intrs][2] = xm[2];
+            tri[intrs] = n;
+            dir[intrs] = ii;
+            icand[intrs] = fext < 0;
+            intrs++;
+            break;
+          }
+        }
+      }
+    }
+  }
+  if (intrs == 0) return ibint == 0 ? 0 : -2;
+  double best = 0.;
+  int bsel = -1;
+  for (int m = 0; m < intrs; m++) {
+    const int ii = dir[m];
+    const double pe[3] = {X[im + GIND[ii][0]], Y[jm + GIND[ii][1]], Z[km + GIND[ii][2]]};
+    double ds = unitdot(pe, p0, ib->n + 3 * tri[m]);
+    ds = ds + (double)flag[IDX(g, im + GIND[ii][0], jm + GIND[ii][1], km + GIND[ii][2])] * (double)(m + 1);
+    if (bsel < 0 || ds > best) {
+      best = ds;
+      bsel = m;
+    }
+  }
+  xn[0] = xint[bsel][0]; xn[1] = xint[bsel][1]; xn[2] = xint[bsel][2];
+  dd[0] = GIND[dir[bsel]][0]; dd[1] = GIND[dir[bsel]][1]; dd[2] = GIND[dir[bsel]][2];
+  return icand[bsel] ? -1 : 1;
+}
+
+/* ---- ludcmp/lubksb for n = 2 (implicit partial pivoting, Crout) ---- */
+void eo_lu2(double *a /* column-major a11 a21 a12 a22 */, int *indx) {
+  double A[2][2] = {{a[0], a[2]}, {a[1], a[3]}};
+  double vv[2];
+  for (int i = 0; i < 2; i++) {
+    double aamax = 0.;
+    for (int j = 0; j < 2; j++)
+      if (fabs(A[i][j]) > aamax) aamax = fabs(A[i][j]);
+    vv[i] = 1. / aamax;
+  }
+  /* column 1 */
+  double aamax = 0.;
+  int imax = 0;
+  for (int i = 0; i < 2; i++) {
+    double sum = A[i][0];
+    double dum = vv[i] * fabs(sum);
+    if (dum >= aamax) {
+      imax = i;
+      aamax = dum;
+    }
+  }
+  if (imax != 0) {
+    for (int k = 0; k < 2; k++) {
+      double dum = A[imax][k];
+      A[imax][k] = A[0][k];
+      A[0][k] = dum;
+    }
+    vv[imax] = vv[0];
+  }
+  indx[0] = imax;
+  if (A[0][0] == 0.) A[0][0] = 1.0e-20;
+  {
+    double dum = 1. / A[0][0];
+    A[1][0] = A[1][0] * dum;
+  }
+  /* column 2 */
+  {
+    double sum = A[1][1];
+    sum = sum - A[1][0] * A[0][1];
+    A[1][1] = sum;
+  }
+  indx[1] = 1;
+  if (A[1][1] == 0.) A[1][1] = 1.0e-20;
+  a[0] = A[0][0]; a[1] = A[1][0]; a[2] = A[0][1]; a[3] = A[1][1];
+}
+
+void eo_lusolve2(const double *a, const int *indx, double *b) {
+  double A[2][2] = {{a[0], a[2]}, {a[1], a[3]}};
+  int ii = -1;
+  for (int i = 0; i < 2; i++) {
+    int ll = indx[i];
+    double sum = b[ll];
+    b[ll] = b[i];
+    if (ii >= 0) {
+      for (int j = ii; j <= i - 1; j++) sum = sum - A[i][j] * b[j];
+    } else if (sum != 0.) {
+      ii = i;
+    }
+    b[i] = sum;
+  }
+  for (int i = 1; i >= 0; i--) {
+    double sum = b[i];
+    for (int j = i + 1; j < 2; j++) sum = sum - A[i][j] * b[j];
+    b[i] = sum / A[i][i];
+  }
+}
+
+/* ---- forcpts + geom_mod (grid-line stencils) + mtrx, variable q (flag fq) ---- */
+void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
+  const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
+  eo_ib_set *S = &ib->set[q];
+  set_free(S);
+  signed char *flagu = ib->flag[fq];
+  const int *L = ib->lim;
+  const int k1 = L[4] > 2 ? L[4] : 2, k2 = L[5] < g->nz - 1 ? L[5] : g->nz - 1;
+  /* forcpts: (k, j, i) order */
+  int cap = 1024, n = 0;
+  int *pi = (int *)malloc(sizeof(int) * cap), *pj = (int *)malloc(sizeof(int) * cap),
+      *pk = (int *)malloc(sizeof(int) * cap);
+  for (int k = k1; k <= k2; k++)
+    for (int j = L[2]; j <= L[3]; j++)
+      for (int i = (L[0] > 2 ? L[0] : 2); i <= L[1]; i++)
+        if (flagu[IDX(g, i, j, k)] == -1) {
+          if (n == cap) {
+            cap *= 2;
+            pi = (int *)realloc(pi, sizeof(int) * cap);
+            pj = (int *)realloc(pj, sizeof(int) * cap);
+            pk = (int *)realloc(pk, sizeof(int) * cap);
+          }
+          pi[n] = i; pj[n] = j; pk[n] = k;
+          n++;
+        }
+  long nc = (long)g->nx * g->ny * g->nz;
+  signed char *fw = (signed char *)malloc(nc);
+  memcpy(fw, flagu, nc);
+  int *mrk = (int *)calloc(n > 0 ? n : 1, sizeof(int)), *lev = (int *)calloc(n > 0 ? n : 1, sizeof(int));
+  int *ddx = (int *)calloc(3 * (n > 0 ? n : 1), sizeof(int));
+  double *xnv = (double *)calloc(3 * (n > 0 ? n : 1), sizeof(double));
+  int *pend = (int *)malloc(sizeof(int) * (n > 0 ? n : 1)), *nxt = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+  int np = n;
+  for (int a = 0; a < n; a++) pend[a] = a;
+  const int sizes[3] = {3, 5, ib->nntr3d};
+  int nlev = 0;
+  for (int ilp = 1; ilp <= ib->nflu && np > 0; ilp++) {
+    int nn2 = 0, nres = 0;
+    int *res = (int *)malloc(sizeof(int) * np);
+    for (int a = 0; a < np; a++) {
+      const int p = pend[a];
+      const int im = pi[p], jm = pj[p], km = pk[p];
+      int gi;
+      if (mrk[p] == -2) {
+        gi = fw[IDX(g, im + ddx[3 * p], jm + ddx[3 * p + 1], km + ddx[3 * p + 2])] == 0 ? 1 : -1;
+      } else {
+        const double qv[3] = {X[im], Y[jm], Z[km]};
+        int inn[NNTR3D];
+        gi = 0;
+        for (int icm = 0; icm < 3; icm++) {
+          knn(ib, qv, sizes[icm], inn);
+          gi = eo_ib_grid_intr(ib, q, fw, im, jm, km, inn, sizes[icm], xnv + 3 * p, ddx + 3 * p);
+          if (gi != 0 && gi != -2) break;
+        }
+      }
+      if (gi == 1) {
+        mrk[p] = 2;
+        lev[p] = ilp;
+        res[nres++] = p;
+      } else if (gi == -1 && ilp < ib->nflu) {
+        mrk[p] = -2;
+        nxt[nn2++] = p;
+      } else {
+        mrk[p] = 0;
+        flagu[IDX(g, im, jm, km)] = (signed char)(imn == 0 ? 1 : 0);
+      }
+    }
+    if (nres > 0) nlev = ilp;
+    for (int a = 0; a < nres; a++) fw[IDX(g, pi[res[a]], pj[res[a]], pk[res[a]])] = 0;
+    for (int k = 1; k <= g->nz; k++)
+      for (int i = 1; i <= g->nx; i++) {
+        fw[IDX(g, i, 1, k)] = fw[IDX(g, i, g->ny - 1, k)];
+        fw[IDX(g, i, g->ny, k)] = fw[IDX(g, i, 2, k)];
+      }
+    free(res);
+    if (nres == 0) {
+      /* no progress: the remaining points are dropped */
+      for (int a = 0; a < nn2; a++) {
+        int p = nxt[a];
+        mrk[p] = 0;
+        flagu[IDX(g, pi[p], pj[p], pk[p])] = (signed char)(imn == 0 ? 1 : 0);
+      }
+      nn2 = 0;
+    }
+    int *t = pend; pend = nxt; nxt = t;
+    np = nn2;
+  }
+  /* outputs ordered by level, then forcpts order */
+  int nv = 0;
+  for (int a = 0; a < n; a++) nv += mrk[a] == 2;
+  S->n = nv;
+  S->nlev = nlev;
+  int m1 = nv > 0 ? nv : 1;
+  S->i = (int *)malloc(sizeof(int) * m1); S->j = (int *)malloc(sizeof(int) * m1); S->k = (int *)malloc(sizeof(int) * m1);
+  S->di = (int *)malloc(sizeof(int) * m1); S->dj = (int *)malloc(sizeof(int) * m1); S->dk = (int *)malloc(sizeof(int) * m1);
+  S->lev = (int *)malloc(sizeof(int) * m1); S->indx = (int *)malloc(sizeof(int) * 2 * m1);
+  S->xn = (double *)malloc(sizeof(double) * m1); S->yn = (double *)malloc(sizeof(double) * m1);
+  S->zn = (double *)malloc(sizeof(double) * m1); S->lu = (double *)malloc(sizeof(double) * 4 * m1);
+  S->lev_start = (int *)malloc(sizeof(int) * (nlev + 2));
+  int o = 0;
+  for (int l = 1; l <= nlev; l++) {
+    S->lev_start[l - 1] = o;
+    for (int a = 0; a < n; a++) {
+      if (mrk[a] != 2 || lev[a] != l) continue;
+      S->i[o] = pi[a]; S->j[o] = pj[a]; S->k[o] = pk[a];
+      S->di[o] = ddx[3 * a]; S->dj[o] = ddx[3 * a + 1]; S->dk[o] = ddx[3 * a + 2];
+      S->lev[o] = l;
+      S->xn[o] = xnv[3 * a]; S->yn[o] = xnv[3 * a + 1]; S->zn[o] = xnv[3 * a + 2];
+      /* mtrx (src/devel.f:1159-1290), Cartesian, mrk = 2 */
+      const double xu = X[pi[a]], yu = Y[pj[a]], zu = Z[pk[a]];
+      const double x1 = X[pi[a] + S->di[o]], y1 = Y[pj[a] + S->dj[o]], z1 = Z[pk[a] + S->dk[o]];
+      const double is1 = imn == 1 ? -1. : 1.;
+      double so = sqrt(((xu - S->xn[o]) * (xu - S->xn[o]) + (yu - S->yn[o]) * (yu - S->yn[o])) +
+                       (zu - S->zn[o]) * (zu - S->zn[o])) * is1;
+      double s1 = sqrt(((xu - x1) * (xu - x1) + (yu - y1) * (yu - y1)) + (zu - z1) * (zu - z1)) * 1.0;
+      double *A = S->lu + 4 * o;
+      if (imn != 0) {
+        A[0] = 1.; A[2] = so;
+      } else {
+        A[0] = 0.; A[2] = 1.0;
+      }
+      A[1] = 1.; A[3] = s1;
+      eo_lu2(A, S->indx + 2 * o);
+      o++;
+    }
+  }
+  S->lev_start[nlev] = o;
+  free(pi); free(pj); free(pk); free(fw); free(mrk); free(lev); free(ddx); free(xnv); free(pend); free(nxt);
+}
+
+/* the whole regeneration for the current body position (src/Eddy6.f:2163-2380) */
+void eo_ib_regen(eo_ib *ib) {
+  eo_ib_limimb(ib);
+  for (int q = 0; q < 4; q++) {
+    eo_ib_tag(ib, q);
+    eo_ib_taguo(ib, q, q);
+  }
+  for (int q = 0; q < 3; q++) eo_ib_geom(ib, q, q, 1);
+  eo_ib_flagp(ib);
+  eo_ib_geom(ib, 3, 4, 0);
+}
+
+/* RBM: translation over tmove (src/rbm.f:2-40 with a constant velocity) */
+void eo_ib_move(eo_ib *ib, double tmove) {
+  for (int t = 0; t < ib->nb; t++) {
+    double *tv = ib->v + 9 * t;
+    for (int a = 0; a < 3; a++)
+      for (int d = 0; d < 3; d++) tv[3 * a + d] = tv[3 * a + d] + ib->vel[d] * tmove;
+    for (int d = 0; d < 3; d++) ib->c[3 * t + d] = ((tv[d] + tv[3 + d]) + tv[6 + d]) / 3.0;
+  }
+}
+
+static void yper(const eo_grid *g, double *a) {
+  for (int k = 1; k <= g->nz; k++)
+    for (int i = 1; i <= g->nx; i++) {
+      a[IDX(g, i, 1, k)] = a[IDX(g, i, g->ny - 1, k)];
+      a[IDX(g, i, g->ny, k)] = a[IDX(g, i, 2, k)];
+    }
+}
+
+/* momforc_mod2 explicit (src/momforc.f:1400-1470) / correctpres_mod2 with a
+ * zero normal gradient: levels in order, y periodic planes after each */
+void eo_ib_force(eo_ib *ib, int q, double *a, double b0) {
+  const eo_grid *g = ib->g;
+  eo_ib_set *S = &ib->set[q];
+  for (int l = 0; l < S->nlev; l++) {
+    for (int o = S->lev_start[l]; o < S->lev_start[l + 1]; o++) {
+      int i1 = S->i[o] + S->di[o], j1 = S->j[o] + S->dj[o], k1 = S->k[o] + S->dk[o];
+      if (j1 <= 1)
+        j1 = g->ny - 2 + j1;
+      else if (j1 >= g->ny)
+        j1 = j1 - g->ny + 2;
+      double b[2] = {b0, a[IDX(g, i1, j1, k1)]};
+      eo_lusolve2(S->lu + 4 * o, S->indx + 2 * o, b);
+      a[IDX(g, S->i[o], S->j[o], S->k[o])] = b[0];
+    }
+    yper(g, a);
+  }
+}
+
+/* velinterior / presinterior / densinterior / tvinterior: value at flag == 1 */
+void eo_ib_interior(eo_ib *ib, int fq, double *a, double value) {
+  const eo_grid *g = ib->g;
+  const int *L = ib->lim;
+  const signed char *f = ib->flag[fq];
+  for (int k = L[4]; k <= L[5]; k++)
+    for (int j = L[2]; j <= L[3]; j++)
+      for (int i = L[0]; i <= L[1]; i++)
+        if (f[IDX(g, i, j, k)] == 1) a[IDX(g, i, j, k)] = value;
+  yper(g, a);
+}
+
+/* ---- accessors ---- */
+const int *eo_ib_limits(const eo_ib *ib) { return ib->lim; }
+const double *eo_ib_velocity(const eo_ib *ib) { return ib->vel; }
+void eo_ib_set_cadence(eo_ib *ib, int every) { ib->every = every ? 1 : 0; }
+int eo_ib_every(const eo_ib *ib) { return ib->every; }
+const signed char *eo_ib_tags(const eo_ib *ib, int q) { return ib->tag[q]; }
+const signed char *eo_ib_flags(const eo_ib *ib, int fq) { return ib->flag[fq]; }
+const eo_ib_set *eo_ib_stencils(const eo_ib *ib, int q) { return &ib->set[q]; }
+void eo_ib_body(const eo_ib *ib, double *v, double *c) {
+  if (v) memcpy(v, ib->v, sizeof(double) * 9 * ib->nb);
+  if (c) memcpy(c, ib->c, sizeof(double) * 3 * ib->nb);
+}

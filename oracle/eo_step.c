@@ -26,10 +26,26 @@ void eo_substep(eo_state *s, int is, double dtm1) {
   double gam[3], rho[3], alf[3];
   scheme(s->prm.ischm, gam, rho, alf);
   double alfxdt = alf[is] * dtm1, gamxdt = gam[is] * dtm1, rhoxdt = rho[is] * dtm1;
+  /* moving body: RBM, then new stencils (:2163-2380); every substep over
+   * alfxdt, or once per step (first substep) over the whole step */
+  if (s->ib && (eo_ib_every(s->ib) || is == 0)) {
+    eo_ib_move(s->ib, eo_ib_every(s->ib) ? alfxdt : dtm1);
+    eo_ib_regen(s->ib);
+  }
   /* Eddy6.f:2453 */
   eo_rhs(s, s->uo, s->vo, s->wo, s->tv, s->us, s->vs, s->ws, s->ub, s->vb, s->wb, s->dp);
   /* :2484 */
   eo_predictord(s, alfxdt, gamxdt, rhoxdt);
+  /* momentum forcing and body velocity inside (:2526-2575) */
+  if (s->ib) {
+    const double *vel = eo_ib_velocity(s->ib);
+    eo_ib_force(s->ib, 0, s->us, vel[0]);
+    eo_ib_force(s->ib, 1, s->vs, vel[1]);
+    eo_ib_force(s->ib, 2, s->ws, vel[2]);
+    eo_ib_interior(s->ib, 0, s->us, vel[0]);
+    eo_ib_interior(s->ib, 1, s->vs, vel[1]);
+    eo_ib_interior(s->ib, 2, s->ws, vel[2]);
+  }
   /* :2689-2704 */
   eo_boundary(s, s->us, s->vs, s->ws);
   eo_boundinout(s, s->us, s->vs, s->ws, s->uo, s->vo, s->wo, alfxdt, 1);
@@ -56,8 +72,15 @@ void eo_substep(eo_state *s, int is, double dtm1) {
     eo_density(s, alfxdt, gamxdt, rhoxdt);
     eo_boundinoutd(s, s->dens);
     eo_boundary_dens(s, s->dens);
+    /* correctdens_mod2 + densinterior (:2972-2983) */
+    if (s->ib) {
+      eo_ib_force(s->ib, 3, s->dens, 0.0);
+      eo_ib_interior(s->ib, 4, s->dens, 0.0);
+    }
   }
 }
+
+void eo_state_set_ib(eo_state *s, eo_ib *ib) { s->ib = ib; }
 
 void eo_step(eo_state *s, double dtm1, int nsteps, int poisson_method) {
   double gam[3], rho[3], alf[3];
@@ -75,6 +98,8 @@ void eo_step(eo_state *s, double dtm1, int nsteps, int poisson_method) {
     s->time = tlevel;
     /* :3008-3019 */
     if (s->prm.isgs != 0) eo_turvis(s);
+    /* tvinterior (:3040-3042) */
+    if (s->ib && s->prm.isgs != 0) eo_ib_interior(s->ib, 3, s->tv, 0.0);
   }
 }
 
