@@ -181,18 +181,19 @@ __device__ __forceinline__ int bitrev(int x, int logn) { return (int)(__brev((un
 // Each thread gathers U elements per pass with all loads issued before the
 // shared-memory stores, so several requests per thread are in flight.
 template <int MODE>
-__global__ void __launch_bounds__(FT32, 3)
+__global__ void __launch_bounds__(FT32, 4)
     k_fwd32(Dims d, DevMetrics m, int px, const float *__restrict__ us, const float *__restrict__ vs,
             const float *__restrict__ ws, const double *__restrict__ win, const double *__restrict__ wout,
             const double *__restrict__ phi, double *__restrict__ dvec, double alfxdt, double rdy2, int logL,
             const float *__restrict__ twr, const float *__restrict__ twi, float *__restrict__ spec,
             unsigned long long *rmax) {
   constexpr int U = MODE == 2 ? 4 : 8;
+  constexpr int HL = TI32 / 2;  // lines ii and ii + HL share one complex FFT (re, im)
   extern __shared__ float smf[];
   __shared__ double red[FT32 / 32];
   const int L = 1 << logL, M = d.nx - 2, NT = L * TI32;
-  float *re = smf, *im = smf + L * TI32;
-  float *tsr = smf + 2 * L * TI32, *tsi = tsr + L / 2;
+  float *re = smf, *im = smf + L * HL;
+  float *tsr = smf + 2 * L * HL, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
   const int i0 = d.ix1 + blockIdx.x * TI32;
   const int k = d.kz1 + blockIdx.y;
@@ -243,8 +244,10 @@ __global__ void __launch_bounds__(FT32, 3)
       const int t = t0 + u * FT32;
       if (t < NT) {
         const int ii = t % TI32, r = bitrev(t / TI32, logL);
-        re[r * TI32 + ii] = (float)v[u];
-        im[r * TI32 + ii] = 0.f;
+        if (ii < HL)
+          re[r * HL + ii] = (float)v[u];
+        else
+          im[r * HL + ii - HL] = (float)v[u];
       }
     }
   }
@@ -258,19 +261,29 @@ __global__ void __launch_bounds__(FT32, 3)
     for (int w = 0; w < FT32 / 32; w++) b = fmax(b, red[w]);
     atomicMax(rmax, (unsigned long long)__double_as_longlong(b));
   }
-  fft_lines_r22<float, TI32>(re, im, logL, tsr, tsi);
+  fft_lines_r22<float, HL>(re, im, logL, tsr, tsi);
+  // separate the two real transforms: A_q = (Z_q + conj Z_{L-q}) / 2,
+  // B_q = (Z_q - conj Z_{L-q}) / 2i; packed order [a0, a1, b1, ..., a_{L/2}]
   const long long lineK = (long long)(k - d.kz1) * L;
   for (int t = threadIdx.x; t < NT; t += blockDim.x) {
     const int ii = t % TI32, J = t / TI32;
     const int i = i0 + ii;
     if (i > d.ix2) continue;
-    float v;
-    if (J == 0) v = re[ii];
-    else if (J == L - 1) v = re[(L / 2) * TI32 + ii];
-    else {
-      const int qq = (J + 1) / 2;
-      v = (J & 1) ? re[qq * TI32 + ii] : im[qq * TI32 + ii];
+    const int pl = ii % HL;
+    const bool second = ii >= HL;
+    const int qq = (J == 0) ? 0 : (J == L - 1 ? L / 2 : (J + 1) / 2);
+    const int qm = (L - qq) & (L - 1);
+    const float zr = re[qq * HL + pl], zi = im[qq * HL + pl];
+    const float wr = re[qm * HL + pl], wi = im[qm * HL + pl];
+    float vr, vi;
+    if (!second) {
+      vr = 0.5f * (zr + wr);
+      vi = 0.5f * (zi - wi);
+    } else {
+      vr = 0.5f * (zi + wi);
+      vi = 0.5f * (wr - zr);
     }
+    const float v = (J == 0 || J == L - 1 || (J & 1)) ? vr : vi;
     spec[(long long)(i - d.ix1) + (long long)M * (J + lineK)] = v;
   }
 }
@@ -278,67 +291,81 @@ __global__ void __launch_bounds__(FT32, 3)
 // (S - mean[J==0]) / L, Hermitian extension, inverse FFT; phi = (ACC ? phi +
 // : ) result.  Gathers and the accumulate reads are batched U per thread.
 template <int ACC>
-__global__ void __launch_bounds__(FT32, 3)
+__global__ void __launch_bounds__(FT32, 4)
     k_bwd32(Dims d, const float *__restrict__ spec, const double *__restrict__ dpm, int logL,
             const float *__restrict__ twr, const float *__restrict__ twi, double *__restrict__ phi) {
   constexpr int U = 8;
+  constexpr int HL = TI32 / 2;  // lines ii and ii + HL share one complex inverse FFT
   extern __shared__ float smf[];
-  const int L = 1 << logL, M = d.nx - 2, NT = L * TI32;
-  float *re = smf, *im = smf + L * TI32;
-  float *tsr = smf + 2 * L * TI32, *tsi = tsr + L / 2;
+  const int L = 1 << logL, M = d.nx - 2, NT = L * HL;
+  float *re = smf, *im = smf + L * HL;
+  float *tsr = smf + 2 * L * HL, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
   const int i0 = d.ix1 + blockIdx.x * TI32;
   const int k = d.kz1 + blockIdx.y;
   const long long lineK = (long long)(k - d.kz1) * L;
   const float mean = (float)dpm[0], rl = 1.f / (float)L;
+  // Z_q = A_q + i B_q from the packed spectra of lines a = ii and b = ii + HL
   for (int t0 = threadIdx.x; t0 < NT; t0 += FT32 * U) {
     float xr[U], xi[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * FT32;
-      const int ii = t % TI32, q = t / TI32;
-      const int i = i0 + ii;
-      xr[u] = 0.f;
-      xi[u] = 0.f;
-      if (t < NT && i <= d.ix2) {
-        const float *S = spec + (long long)(i - d.ix1);
-        auto get = [&](int J) {
-          float v = S[(long long)M * (J + lineK)];
-          if (J == 0) v = v - mean;
-          return v * rl;
+      const int pl = t % HL, q = t / HL;
+      float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
+      if (t < NT) {
+        auto herm = [&](int i, float &hr, float &hi) {
+          hr = 0.f;
+          hi = 0.f;
+          if (i > d.ix2) return;
+          const float *S = spec + (long long)(i - d.ix1);
+          auto get = [&](int J) {
+            float v = S[(long long)M * (J + lineK)];
+            if (J == 0) v = v - mean;
+            return v * rl;
+          };
+          if (q == 0) hr = get(0);
+          else if (q == L / 2) hr = get(L - 1);
+          else if (q < L / 2) { hr = get(2 * q - 1); hi = get(2 * q); }
+          else { const int qq = L - q; hr = get(2 * qq - 1); hi = -get(2 * qq); }
         };
-        if (q == 0) xr[u] = get(0);
-        else if (q == L / 2) xr[u] = get(L - 1);
-        else if (q < L / 2) { xr[u] = get(2 * q - 1); xi[u] = get(2 * q); }
-        else { const int qq = L - q; xr[u] = get(2 * qq - 1); xi[u] = -get(2 * qq); }
+        herm(i0 + pl, ar, ai);
+        herm(i0 + pl + HL, br, bi);
       }
+      xr[u] = ar - bi;
+      xi[u] = ai + br;
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * FT32;
       if (t < NT) {
-        const int ii = t % TI32, r = bitrev(t / TI32, logL);
-        re[r * TI32 + ii] = xr[u];
-        im[r * TI32 + ii] = xi[u];
+        const int pl = t % HL, r = bitrev(t / HL, logL);
+        re[r * HL + pl] = xr[u];
+        im[r * HL + pl] = xi[u];
       }
     }
   }
   __syncthreads();
-  fft_lines_r22<float, TI32>(re, im, logL, tsr, tsi);
-  for (int t0 = threadIdx.x; t0 < NT; t0 += FT32 * U) {
+  fft_lines_r22<float, HL>(re, im, logL, tsr, tsi);
+  // real part -> line a, imaginary part -> line b
+  const int NO = L * TI32;
+  for (int t0 = threadIdx.x; t0 < NO; t0 += FT32 * U) {
     double old[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * FT32;
       const int ii = t % TI32, jj = t / TI32, i = i0 + ii;
       old[u] = 0.;
-      if (ACC && t < NT && i <= d.ix2) old[u] = phi[fidx(d, i, d.jy1 + jj, k)];
+      if (ACC && t < NO && i <= d.ix2) old[u] = phi[fidx(d, i, d.jy1 + jj, k)];
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * FT32;
       const int ii = t % TI32, jj = t / TI32, i = i0 + ii;
-      if (t < NT && i <= d.ix2) phi[fidx(d, i, d.jy1 + jj, k)] = old[u] + (double)re[jj * TI32 + ii];
+      if (t < NO && i <= d.ix2) {
+        const float z = ii < HL ? re[jj * HL + ii] : im[jj * HL + ii - HL];
+        phi[fidx(d, i, d.jy1 + jj, k)] = old[u] + (double)z;
+      }
     }
   }
 }
@@ -652,7 +679,7 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   EDDY_LAUNCHED(ctx);
   k_sum_final<<<1, 32, 0, ctx->stream>>>(NPART, (long long)M * N, pp.red, ctx->scal + 3);
   EDDY_LAUNCHED(ctx);
-  size_t smem = sizeof(float) * (2 * L * TI32 + L);
+  size_t smem = sizeof(float) * (2 * L * (TI32 / 2) + L);
   dim3 g((M + TI32 - 1) / TI32, N);
   if (accumulate)
     k_bwd32<1><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi);
@@ -667,7 +694,7 @@ int fwd32(eddy_ctx *ctx, int mode, double alfxdt, const double *phi, double *dve
   MixedState *x = ms(ctx);
   PoissonPlan &pp = ctx->pp;
   const Dims &d = ctx->d;
-  size_t smem = sizeof(float) * (2 * pp.L * TI32 + pp.L);
+  size_t smem = sizeof(float) * (2 * pp.L * (TI32 / 2) + pp.L);
   dim3 g((pp.M + TI32 - 1) / TI32, pp.N);
   ProfScope ps(ctx, mode == 2 ? PROF_REFINE : PROF_DIV_FFT);
   auto *rm = reinterpret_cast<unsigned long long *>(x->resid + sweep);
@@ -767,7 +794,7 @@ int mixed_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaFree(ctx->pp.cprime));
   ctx->pp.cprime = nullptr;
   EDDY_CUDA(cudaMalloc(&ctx->pp.cprime, 2 * sizeof(double) * (size_t)ctx->pp.M * ctx->pp.L * ctx->pp.N));
-  size_t smem = sizeof(float) * (2 * L * TI32 + L);
+  size_t smem = sizeof(float) * (2 * L * (TI32 / 2) + L);
   if (smem > 48 * 1024) {
     EDDY_CUDA(cudaFuncSetAttribute(k_fwd32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     EDDY_CUDA(cudaFuncSetAttribute(k_fwd32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
