@@ -1,7 +1,7 @@
 """Learned eddy-viscosity closure: parameter packing, feature normalisation,
 training-data harvesting and training driver over the C ABI.
 
-The network (12 -> 64 -> 64 -> 64 -> 2, SiLU hidden, softplus outputs) maps
+The network (12 -> 64 -> 64 -> 64 -> 2, hard-swish hidden, softplus outputs) maps
 local, filter-width-scaled velocity- and density-gradient features to the
 eddy-viscosity and diffusivity coefficients C_nu, C_kappa of
 nu_t = C_nu Delta^2 |S| and kappa_t = C_kappa Delta^2 |S| (|S| from the same

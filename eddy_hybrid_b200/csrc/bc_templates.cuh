@@ -11,10 +11,6 @@
 
 int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, double sgn, int zero);
 
-__host__ __device__ inline long long pidx(const Dims &d, int pitch, int i, int j, int k) {
-  return (long long)(i - 1) + (long long)pitch * ((long long)(j - 1) + (long long)d.ny * (long long)(k - 1));
-}
-
 namespace {
 namespace bct {
 

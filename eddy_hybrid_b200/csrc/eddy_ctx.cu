@@ -678,10 +678,11 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
     }
     if (ctx->prm.isgs != 0) {
       int rc;
-      if (ctx->mixed && (rc = mixed_before_sgs(ctx))) return rc;
+      // the learned closure writes the mixed form's FP32 copies itself
+      const bool closure = ctx->prm.closure == 1;
       {
         ProfScope ps(ctx, PROF_TURVIS);
-        if (ctx->prm.closure == 1) {
+        if (closure) {
           rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, nullptr);
         } else {
           rc = launch_turvis(ctx);
@@ -689,8 +690,10 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
         if (rc) return rc;
       }
       // tvinterior (src/Eddy6.f:3040-3042)
-      if (ctx->ib && (rc = ib_interior(ctx, 3, ctx->f[EDDY_TV], 0.0))) return rc;
-      if (ctx->mixed && (rc = mixed_after_sgs(ctx))) return rc;
+      MixedViews mv{};
+      const bool mirror = ctx->mixed && closure && mixed_views(ctx, &mv) == EDDY_OK;
+      if (ctx->ib && (rc = ib_interior(ctx, 3, ctx->f[EDDY_TV], 0.0, mirror ? mv.tv : nullptr, mv.px))) return rc;
+      if (ctx->mixed && !closure && (rc = mixed_after_sgs(ctx))) return rc;
     }
   }
   return EDDY_OK;
@@ -720,7 +723,6 @@ int eddy_closure_apply(eddy_ctx *ctx, long long *out_of_envelope) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   unsigned long long n = 0;
   int rc;
-  if (ctx->mixed && (rc = mixed_before_sgs(ctx))) return rc;
   if ((rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, &n))) return rc;
   if (ctx->mixed && (rc = mixed_after_sgs(ctx))) return rc;
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));

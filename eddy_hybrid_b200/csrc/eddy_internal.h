@@ -161,6 +161,11 @@ __host__ __device__ inline long long fidx(const Dims &d, int i, int j, int k) {
   return (long long)(i - 1) + (long long)d.nx * ((long long)(j - 1) + (long long)d.ny * (long long)(k - 1));
 }
 
+// the same for an array with row pitch `pitch` (the mixed form's FP32 arrays)
+__host__ __device__ inline long long pidx(const Dims &d, int pitch, int i, int j, int k) {
+  return (long long)(i - 1) + (long long)pitch * ((long long)(j - 1) + (long long)d.ny * (long long)(k - 1));
+}
+
 // tensor map over an (NX,NY,NZ) FP64 field with a (bx,by,1) box, cached per
 // pointer; nullptr on failure (message in ctx->err)
 const CUtensorMap *ctx_tensor_map(eddy_ctx *ctx, const double *ptr, int bx, int by);
@@ -200,17 +205,26 @@ int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, dou
 const double *ib_velocity(eddy_ctx *ctx);
 int ib_set_cadence(eddy_ctx *ctx, int every_substep);
 int ib_every_substep(eddy_ctx *ctx);
-int ib_interior(eddy_ctx *ctx, int fq, double *a, double value);
+int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror = nullptr, int mpitch = 0);
 int ib_download(eddy_ctx *ctx, int which, signed char *out);
 int ib_limits(eddy_ctx *ctx, int *lim6);
 int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
                 int *indx);
 
-// tensor-core (3xTF32) eigen-transforms of the mixed solve (k_xform.cu):
-// B matrices from a column-major FP64 M x M transform; out = in * B^T
+// tensor-core (3xTF32) eigen-transforms of the mixed solve (k_xform.cu).
+// sym: mirror-symmetric split form, modes ordered even then odd; lam and m0
+// are the eigenvalues and the null mode in the transform's mode order.
+struct XformPlan {
+  int sym = 0;
+  float *fhi = nullptr, *flo = nullptr, *bhi = nullptr, *blo = nullptr;
+  double *lam = nullptr;
+  int m0 = 0;
+};
 bool xform_supported(int M);
-int xform_prepare(eddy_ctx *ctx, const double *T_dev, float **bhi, float **blo);
-int launch_xform(eddy_ctx *ctx, const float *in, float *out, const float *bhi, const float *blo);
+int xform_prepare(eddy_ctx *ctx, XformPlan *xp);
+void xform_release(XformPlan *xp);
+// dir 0: x values -> mode coefficients; 1: back
+int launch_xform(eddy_ctx *ctx, const XformPlan *xp, int dir, const float *in, float *out);
 
 // mixed-precision form (k_mixed.cu): FP32 stencils and FFTs, FP64 line solves,
 // FP64-residual iterative refinement, FP64 projection onto FP64 master velocities
@@ -221,13 +235,19 @@ int mixed_from64(eddy_ctx *ctx, int field);
 // write the FP64 array of `field` from its FP32 master (before a download)
 int mixed_to64(eddy_ctx *ctx, int field);
 int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
+// FP32 arrays of the mixed form the learned closure reads and writes
+struct MixedViews {
+  const float *uo, *vo, *wo, *dens;
+  float *tv, *kv;
+  int px;
+};
+int mixed_views(eddy_ctx *ctx, MixedViews *v);
 // mixed Poisson solve of L dp = rhs (rhs, dp FP64 device arrays)
 int mixed_poisson_rhs(eddy_ctx *ctx, const double *rhs, double *dp);
 // max |residual| before each refinement sweep of the last mixed solve (host copy)
 int mixed_residuals(eddy_ctx *ctx, double *out, int n);
 // around an eddy-viscosity update: FP64 density for the closure features
 // before, FP32 copies of nu_t / kappa_t after
-int mixed_before_sgs(eddy_ctx *ctx);
 int mixed_after_sgs(eddy_ctx *ctx);
 int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigned long long *out_of_envelope);
 void mlp_release(eddy_ctx *ctx);

@@ -1390,17 +1390,17 @@ int ib_set_cadence(eddy_ctx *ctx, int every_substep) {
 int ib_every_substep(eddy_ctx *ctx) { return ibs(ctx) ? ibs(ctx)->every_substep : 0; }
 
 // value where flag fq == 1 (tvinterior), then y periodic planes
-int ib_interior(eddy_ctx *ctx, int fq, double *a, double value) {
+int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror, int mpitch) {
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
   const Dims &d = ctx->d;
   const Box6 L = s->lim;
   const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
   if (nbx > 0) {
-    k_interior<double><<<nblk(nbx), 256, 0, ctx->stream>>>(d, d.nx, L, s->flag[fq], a, value, nullptr, 0);
+    k_interior<double><<<nblk(nbx), 256, 0, ctx->stream>>>(d, d.nx, L, s->flag[fq], a, value, mirror, mpitch);
     EDDY_LAUNCHED(ctx);
   }
-  k_yper_field<double><<<nblk((long long)d.nx * d.nz), 256, 0, ctx->stream>>>(d, d.nx, a, nullptr, 0);
+  k_yper_field<double><<<nblk((long long)d.nx * d.nz), 256, 0, ctx->stream>>>(d, d.nx, a, mirror, mpitch);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }

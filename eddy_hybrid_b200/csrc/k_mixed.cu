@@ -50,8 +50,8 @@ struct MixedState {
   float *twr = nullptr, *twi = nullptr;  // FFT twiddles: forward table then backward table
   double *resid = nullptr;               // max |r| before each sweep (device, 4 entries)
   double *wout = nullptr;                // outlet-face w (NX,NY) in FP64: exact mass balance
-  // 3xTF32 tensor-core transforms: forward (Af) and backward (Ab) matrices, hi/lo
-  float *fhi = nullptr, *flo = nullptr, *bhi = nullptr, *blo = nullptr;
+  // 3xTF32 tensor-core transforms (null fhi: FP32 cuBLAS GEMMs with the plan's matrices)
+  XformPlan xp;
 };
 
 MixedState *ms(eddy_ctx *ctx) { return static_cast<MixedState *>(ctx->mixed); }
@@ -167,93 +167,156 @@ __global__ void k_zero_faces32(Dims d, int px, float *a, float *b, float *c3) {
 }
 
 // ---------------------------------------------------------------------------
-// FP32 FFT along y on TI32 consecutive x lines per block (one k plane)
-constexpr int TI32 = 32, FT32 = 256;
+// FP32 FFT along y on TI32 consecutive x lines per block (one k plane).
+// Lane l of every warp owns line i0 + l for the whole block, warp w owns a
+// contiguous run of JW = L/8 rows; lines l and l + 16 share one complex FFT
+// (re, im).  Neighbours along y come from the previous/next iteration's
+// registers and along x from the adjacent lanes (shuffles), so each element
+// is loaded once; offsets within a k plane are 32-bit.
+constexpr int TI32 = 32, FT32 = 256, HL32 = TI32 / 2;
+
+inline size_t fft32_smem(int L) { return sizeof(float) * (2 * (size_t)L * HL32 + HL32 + L); }
 
 __device__ __forceinline__ int bitrev(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
 
 #include "fft_lines.cuh"
 
+// shared-memory slot of line `lane` at row r (the second half of the lines is
+// the imaginary part; the im array is offset by 16 words so the two halves of
+// a warp hit different banks)
+__device__ __forceinline__ float &slot32(float *re, float *im, int r, int lane) {
+  return lane < HL32 ? re[r * HL32 + lane] : im[r * HL32 + lane - HL32];
+}
+
 // Forward transform of the right-hand side.  MODE 0: d = div(u*)/alfxdt in
 // FP64 from the FP32 predictor velocities (src/timeindeg.f:941-949), stored
 // to dvec; MODE 1: d = dvec; MODE 2: r = dvec - L phi (FP64 residual of the
 // DIRECT operator: Neumann x and z, periodic y), max|r| -> rmax.
-// Each thread gathers U elements per pass with all loads issued before the
-// shared-memory stores, so several requests per thread are in flight.
 template <int MODE>
-__global__ void __launch_bounds__(FT32, 4)
+__global__ void __launch_bounds__(FT32, 3)
     k_fwd32(Dims d, DevMetrics m, int px, const float *__restrict__ us, const float *__restrict__ vs,
             const float *__restrict__ ws, const double *__restrict__ win, const double *__restrict__ wout,
-            const double *__restrict__ phi, double *__restrict__ dvec, double alfxdt, double rdy2, int logL,
+            const double *__restrict__ phi, double *__restrict__ dvec, double ralf, double rdy2, int logL,
             const float *__restrict__ twr, const float *__restrict__ twi, float *__restrict__ spec,
             unsigned long long *rmax) {
-  constexpr int U = MODE == 2 ? 4 : 8;
-  constexpr int HL = TI32 / 2;  // lines ii and ii + HL share one complex FFT (re, im)
+  constexpr int U = 8;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ float smf[];
   __shared__ double red[FT32 / 32];
-  const int L = 1 << logL, M = d.nx - 2, NT = L * TI32;
-  float *re = smf, *im = smf + L * HL;
-  float *tsr = smf + 2 * L * HL, *tsi = tsr + L / 2;
+  const int L = 1 << logL, M = d.nx - 2;
+  float *re = smf, *im = smf + L * HL32 + HL32;
+  float *tsr = im + L * HL32, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
-  const int i0 = d.ix1 + blockIdx.x * TI32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i = d.ix1 + blockIdx.x * TI32 + lane;
+  const bool act = i <= d.ix2;
+  const int ic = act ? i : d.ix2;  // loads of idle lanes stay in bounds
   const int k = d.kz1 + blockIdx.y;
-  const long long sz = (long long)d.nx * d.ny;
+  const int JW = (L + 7) / 8, jb = min(L, warp * JW), je = min(L, jb + JW);
+  const int nx = d.nx;
+  double *D = dvec + fidx(d, ic, d.jy1, k);
   double amax = 0.;
-  for (int t0 = threadIdx.x; t0 < NT; t0 += FT32 * U) {
-    double v[U];
+  if (MODE == 0) {
+    constexpr int U0 = 4;
+    const long long pb = pidx(d, px, ic, d.jy1, k);
+    const float *Us = us + pb, *Vs = vs + pb, *Ws = ws + pb;
+    const int pz = px * d.ny;
+    const bool top = k == d.kz2, bot = k == d.kz1;
+    const double *Wo = wout + (ic - 1) + (long long)nx * (d.jy1 - 1);
+    const double *Wi = win + (ic - 1) + (long long)nx * (d.jy1 - 1);
+    const double api = m.ap[ic], cpk = m.cp[k];
+    const double *bp = m.bp + d.jy1;
+    double vprev = jb < je ? (double)Vs[(jb - 1) * px] : 0.;
+    for (int j0 = jb; j0 < je; j0 += U0) {
+      float uu[U0], ul[U0], vv[U0];
+      double wk[U0], wm[U0];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int t = t0 + u * FT32;
-      const int ii = t % TI32, jj = t / TI32;
-      const int i = i0 + ii, j = d.jy1 + jj;
-      v[u] = 0.;
-      if (t < NT && i <= d.ix2) {
-        const long long q = fidx(d, i, j, k);
-        if (MODE == 0) {
-          const long long p = pidx(d, px, i, j, k);
-          // inlet and outlet faces from their FP64 planes (the mass balance of
-          // the convective outlet holds in FP64, so the right-hand side stays
-          // compatible with the Neumann operator)
-          const int pl = (i - 1) + d.nx * (j - 1);
-          const double wk = k == d.kz2 ? wout[pl] : (double)ws[p];
-          const double wkm = k == d.kz1 ? win[pl] : (double)ws[p - (long long)px * d.ny];
-          double x = (m.ap[i] * ((double)us[p] - (double)us[p - 1]) + m.bp[j] * ((double)vs[p] - (double)vs[p - px]) +
-                      m.cp[k] * (wk - wkm));
-          x = x / alfxdt;
-          dvec[q] = x;
-          v[u] = x;
-        } else if (MODE == 1) {
-          v[u] = dvec[q];
-        } else {
-          const double c = phi[q];
-          const double pe = i < d.ix2 ? phi[q + 1] : c, pw = i > d.ix1 ? phi[q - 1] : c;
-          const int jp = j < d.jy2 ? j + 1 : d.jy1, jm = j > d.jy1 ? j - 1 : d.jy2;
-          const double pn = phi[fidx(d, i, jp, k)], ps = phi[fidx(d, i, jm, k)];
-          const double pt = k < d.kz2 ? phi[q + sz] : c, pb = k > d.kz1 ? phi[q - sz] : c;
-          const double lx = m.ap[i] * m.au[i] * (pe - c) + m.ap[i] * m.au[i - 1] * (pw - c);
-          const double ly = (pn - 2. * c + ps) * rdy2;
-          const double lz = m.cp[k] * m.cw[k] * (pt - c) + m.cp[k] * m.cw[k - 1] * (pb - c);
-          const double x = dvec[q] - (lx + ly + lz);
-          amax = fmax(amax, fabs(x));
-          v[u] = x;
+      for (int u = 0; u < U0; u++) {
+        const int jj = j0 + u;
+        if (jj < je) {
+          const int o = jj * px;
+          uu[u] = Us[o];
+          vv[u] = Vs[o];
+          ul[u] = lane == 0 ? Us[o - 1] : 0.f;
+          wk[u] = top ? Wo[jj * nx] : (double)Ws[o];
+          wm[u] = bot ? Wi[jj * nx] : (double)Ws[o - pz];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U0; u++) {
+        const int jj = j0 + u;
+        if (jj < je) {
+          float w = __shfl_up_sync(FULL, uu[u], 1);
+          if (lane == 0) w = ul[u];
+          const double vc = (double)vv[u];
+          double x = api * ((double)uu[u] - (double)w) + bp[jj] * (vc - vprev) + cpk * (wk[u] - wm[u]);
+          x = act ? x * ralf : 0.;
+          vprev = vc;
+          if (act) D[jj * nx] = x;
+          slot32(re, im, bitrev(jj, logL), lane) = (float)x;
         }
       }
     }
+  } else if (MODE == 1) {
+    for (int j0 = jb; j0 < je; j0 += U) {
+      double v[U];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int t = t0 + u * FT32;
-      if (t < NT) {
-        const int ii = t % TI32, r = bitrev(t / TI32, logL);
-        if (ii < HL)
-          re[r * HL + ii] = (float)v[u];
-        else
-          im[r * HL + ii - HL] = (float)v[u];
+      for (int u = 0; u < U; u++) v[u] = (j0 + u < je) ? D[(j0 + u) * nx] : 0.;
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        if (j0 + u < je) slot32(re, im, bitrev(j0 + u, logL), lane) = act ? (float)v[u] : 0.f;
+    }
+  } else {
+    constexpr int U2 = 3;
+    const double *P = phi + fidx(d, ic, d.jy1, k);
+    const int sz = nx * d.ny;
+    const bool has_e = act && i < d.ix2, has_w = act && i > d.ix1;
+    const bool kt = k < d.kz2, kb = k > d.kz1;
+    const double ae = m.ap[ic] * m.au[ic], aw = m.ap[ic] * m.au[ic - 1];
+    const double ct = m.cp[k] * m.cw[k], cb = m.cp[k] * m.cw[k - 1];
+    double cprev = 0., ccur = 0.;
+    if (jb < je) {
+      cprev = P[((jb - 1 + L) & (L - 1)) * nx];
+      ccur = P[jb * nx];
+    }
+    for (int j0 = jb; j0 < je; j0 += U2) {
+      // edge[u]: the east neighbour for lane 31, the west one for lane 0
+      double cn[U2], tt[U2], bb[U2], dd[U2], edge[U2];
+#pragma unroll
+      for (int u = 0; u < U2; u++) {
+        const int jj = j0 + u;
+        if (jj < je) {
+          const int o = jj * nx;
+          cn[u] = P[((jj + 1) & (L - 1)) * nx];
+          tt[u] = kt ? P[o + sz] : 0.;
+          bb[u] = kb ? P[o - sz] : 0.;
+          dd[u] = D[o];
+          edge[u] = (lane == 31 && has_e) ? P[o + 1] : ((lane == 0 && has_w) ? P[o - 1] : 0.);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U2; u++) {
+        const int jj = j0 + u;
+        if (jj < je) {
+          const double c = ccur;
+          double pe = __shfl_down_sync(FULL, c, 1), pw = __shfl_up_sync(FULL, c, 1);
+          if (lane == 31) pe = edge[u];
+          if (lane == 0) pw = edge[u];
+          if (!has_e) pe = c;
+          if (!has_w) pw = c;
+          const double pt = kt ? tt[u] : c, pbm = kb ? bb[u] : c;
+          const double lap = ae * (pe - c) + aw * (pw - c) + (cn[u] - 2. * c + cprev) * rdy2 + ct * (pt - c) +
+                             cb * (pbm - c);
+          const double x = act ? dd[u] - lap : 0.;
+          amax = fmax(amax, fabs(x));
+          slot32(re, im, bitrev(jj, logL), lane) = (float)x;
+          cprev = c;
+          ccur = cn[u];
+        }
       }
     }
-  }
-  if (MODE == 2) {
-    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(FULL, amax, o));
+    if (lane == 0) red[warp] = amax;
   }
   __syncthreads();
   if (MODE == 2 && threadIdx.x == 0) {
@@ -261,115 +324,108 @@ __global__ void __launch_bounds__(FT32, 4)
     for (int w = 0; w < FT32 / 32; w++) b = fmax(b, red[w]);
     atomicMax(rmax, (unsigned long long)__double_as_longlong(b));
   }
-  fft_lines_r22<float, HL>(re, im, logL, tsr, tsi);
+  fft_lines_r22<float, HL32>(re, im, logL, tsr, tsi);
   // separate the two real transforms: A_q = (Z_q + conj Z_{L-q}) / 2,
   // B_q = (Z_q - conj Z_{L-q}) / 2i; packed order [a0, a1, b1, ..., a_{L/2}]
-  const long long lineK = (long long)(k - d.kz1) * L;
-  for (int t = threadIdx.x; t < NT; t += blockDim.x) {
-    const int ii = t % TI32, J = t / TI32;
-    const int i = i0 + ii;
-    if (i > d.ix2) continue;
-    const int pl = ii % HL;
-    const bool second = ii >= HL;
-    const int qq = (J == 0) ? 0 : (J == L - 1 ? L / 2 : (J + 1) / 2);
-    const int qm = (L - qq) & (L - 1);
-    const float zr = re[qq * HL + pl], zi = im[qq * HL + pl];
-    const float wr = re[qm * HL + pl], wi = im[qm * HL + pl];
-    float vr, vi;
-    if (!second) {
-      vr = 0.5f * (zr + wr);
-      vi = 0.5f * (zi - wi);
-    } else {
-      vr = 0.5f * (zi + wi);
-      vi = 0.5f * (wr - zr);
+  const int pl = lane & (HL32 - 1);
+  const bool second = lane >= HL32;
+  float *S = spec + (long long)(ic - d.ix1) + (long long)M * L * (k - d.kz1);
+  for (int q = warp; q <= L / 2; q += FT32 / 32) {
+    const int qm = (L - q) & (L - 1);
+    const float zr = re[q * HL32 + pl], zi = im[q * HL32 + pl];
+    const float wr = re[qm * HL32 + pl], wi = im[qm * HL32 + pl];
+    const float vr = second ? 0.5f * (zi + wi) : 0.5f * (zr + wr);
+    const float vi = second ? 0.5f * (wr - zr) : 0.5f * (zi - wi);
+    if (act) {
+      if (q == 0) {
+        S[0] = vr;
+      } else if (q == L / 2) {
+        S[(long long)M * (L - 1)] = vr;
+      } else {
+        S[(long long)M * (2 * q - 1)] = vr;
+        S[(long long)M * (2 * q)] = vi;
+      }
     }
-    const float v = (J == 0 || J == L - 1 || (J & 1)) ? vr : vi;
-    spec[(long long)(i - d.ix1) + (long long)M * (J + lineK)] = v;
   }
 }
 
 // (S - mean[J==0]) / L, Hermitian extension, inverse FFT; phi = (ACC ? phi +
-// : ) result.  Gathers and the accumulate reads are batched U per thread.
+// : ) result.  Lanes l < 16 hold A_q of line l, lanes l + 16 B_q of line
+// l + 16; one shuffle gives each half the other's values to form Z_q (low
+// half) and Z_{L-q} (high half).
 template <int ACC>
 __global__ void __launch_bounds__(FT32, 4)
     k_bwd32(Dims d, const float *__restrict__ spec, const double *__restrict__ dpm, int logL,
             const float *__restrict__ twr, const float *__restrict__ twi, double *__restrict__ phi) {
-  constexpr int U = 8;
-  constexpr int HL = TI32 / 2;  // lines ii and ii + HL share one complex inverse FFT
+  constexpr int U = 4;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ float smf[];
-  const int L = 1 << logL, M = d.nx - 2, NT = L * HL;
-  float *re = smf, *im = smf + L * HL;
-  float *tsr = smf + 2 * L * HL, *tsi = tsr + L / 2;
+  const int L = 1 << logL, M = d.nx - 2;
+  float *re = smf, *im = smf + L * HL32 + HL32;
+  float *tsr = im + L * HL32, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
-  const int i0 = d.ix1 + blockIdx.x * TI32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i = d.ix1 + blockIdx.x * TI32 + lane;
+  const bool act = i <= d.ix2;
+  const int ic = act ? i : d.ix2;
   const int k = d.kz1 + blockIdx.y;
-  const long long lineK = (long long)(k - d.kz1) * L;
+  const int pl = lane & (HL32 - 1);
+  const bool low = lane < HL32;
+  const float *S = spec + (long long)(ic - d.ix1) + (long long)M * L * (k - d.kz1);
   const float mean = (float)dpm[0], rl = 1.f / (float)L;
-  // Z_q = A_q + i B_q from the packed spectra of lines a = ii and b = ii + HL
-  for (int t0 = threadIdx.x; t0 < NT; t0 += FT32 * U) {
-    float xr[U], xi[U];
+  for (int q0 = warp; q0 <= L / 2; q0 += U * (FT32 / 32)) {
+    float a[U], b[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const int t = t0 + u * FT32;
-      const int pl = t % HL, q = t / HL;
-      float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
-      if (t < NT) {
-        auto herm = [&](int i, float &hr, float &hi) {
-          hr = 0.f;
-          hi = 0.f;
-          if (i > d.ix2) return;
-          const float *S = spec + (long long)(i - d.ix1);
-          auto get = [&](int J) {
-            float v = S[(long long)M * (J + lineK)];
-            if (J == 0) v = v - mean;
-            return v * rl;
-          };
-          if (q == 0) hr = get(0);
-          else if (q == L / 2) hr = get(L - 1);
-          else if (q < L / 2) { hr = get(2 * q - 1); hi = get(2 * q); }
-          else { const int qq = L - q; hr = get(2 * qq - 1); hi = -get(2 * qq); }
-        };
-        herm(i0 + pl, ar, ai);
-        herm(i0 + pl + HL, br, bi);
+      const int q = q0 + u * (FT32 / 32);
+      a[u] = 0.f;
+      b[u] = 0.f;
+      if (q <= L / 2 && act) {
+        if (q == 0) {
+          a[u] = S[0] - mean;
+        } else if (q == L / 2) {
+          a[u] = S[(long long)M * (L - 1)];
+        } else {
+          a[u] = S[(long long)M * (2 * q - 1)];
+          b[u] = S[(long long)M * (2 * q)];
+        }
       }
-      xr[u] = ar - bi;
-      xi[u] = ai + br;
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const int t = t0 + u * FT32;
-      if (t < NT) {
-        const int pl = t % HL, r = bitrev(t / HL, logL);
-        re[r * HL + pl] = xr[u];
-        im[r * HL + pl] = xi[u];
+      const int q = q0 + u * (FT32 / 32);
+      if (q <= L / 2) {
+        const float ar = a[u] * rl, ai = b[u] * rl;
+        const float orr = __shfl_xor_sync(FULL, ar, HL32), oi = __shfl_xor_sync(FULL, ai, HL32);
+        if (low) {  // own A_q, other B_q: Z_q = (Ar - Bi) + i (Ai + Br)
+          const int r = bitrev(q, logL);
+          re[r * HL32 + pl] = ar - oi;
+          im[r * HL32 + pl] = ai + orr;
+        } else if (q != 0 && q != L / 2) {  // own B_q, other A_q: Z_{L-q} = (Ar + Bi) + i (Br - Ai)
+          const int r = bitrev(L - q, logL);
+          re[r * HL32 + pl] = orr + ai;
+          im[r * HL32 + pl] = ar - oi;
+        }
       }
     }
   }
   __syncthreads();
-  fft_lines_r22<float, HL>(re, im, logL, tsr, tsi);
-  // real part -> line a, imaginary part -> line b
-  const int NO = L * TI32;
-  for (int t0 = threadIdx.x; t0 < NO; t0 += FT32 * U) {
-    double old[U];
+  fft_lines_r22<float, HL32>(re, im, logL, tsr, tsi);
+  // real part -> line pl, imaginary part -> line pl + 16
+  const int JW = (L + 7) / 8, jb = min(L, warp * JW), je = min(L, jb + JW);
+  const int nx = d.nx;
+  double *P = phi + fidx(d, ic, d.jy1, k);
+  for (int j0 = jb; j0 < je; j0 += 8) {
+    double old[8];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int t = t0 + u * FT32;
-      const int ii = t % TI32, jj = t / TI32, i = i0 + ii;
-      old[u] = 0.;
-      if (ACC && t < NO && i <= d.ix2) old[u] = phi[fidx(d, i, d.jy1 + jj, k)];
-    }
+    for (int u = 0; u < 8; u++) old[u] = (ACC && act && j0 + u < je) ? P[(j0 + u) * nx] : 0.;
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int t = t0 + u * FT32;
-      const int ii = t % TI32, jj = t / TI32, i = i0 + ii;
-      if (t < NO && i <= d.ix2) {
-        const float z = ii < HL ? re[jj * HL + ii] : im[jj * HL + ii - HL];
-        phi[fidx(d, i, d.jy1 + jj, k)] = old[u] + (double)z;
-      }
+    for (int u = 0; u < 8; u++) {
+      const int jj = j0 + u;
+      if (jj < je && act) P[jj * nx] = old[u] + (double)slot32(re, im, jj, lane);
     }
   }
 }
-
 #include "tridiag_z.cuh"
 
 __global__ void k_plane_sum32(int M, int L, int N, const float *__restrict__ s, double *part) {
@@ -644,8 +700,8 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   int rc;
   {
     ProfScope ps(ctx, PROF_GEMM_FWD);
-    if (x->fhi) {
-      if ((rc = launch_xform(ctx, s1, s2, x->fhi, x->flo))) return rc;
+    if (x->xp.fhi) {
+      if ((rc = launch_xform(ctx, &x->xp, 0, s1, s2))) return rc;
     } else {
       bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Af32, M, s1, M, &zero, s2,
                        M);
@@ -656,17 +712,20 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   {
     ProfScope ps(ctx, PROF_TRIDIAG);
     long long nl = (long long)M * L;
-    k_line_mean<float><<<1, 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.wz, s2, ctx->scal + 5);
+    // mode order of the transforms: the split form orders even modes first
+    const double *lam = x->xp.fhi ? x->xp.lam : pp.lam;
+    const int m0 = x->xp.fhi ? x->xp.m0 : pp.m0;
+    k_line_mean<float><<<1, 256, 0, ctx->stream>>>(M, L, N, m0, pp.wz, s2, ctx->scal + 5);
     EDDY_LAUNCHED(ctx);
-    k_tridiag_lines<float><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
-        M, L, N, pp.m0, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, s2, pp.cprime,
-        pp.cprime + (size_t)M * L * N);
+    float *c32 = reinterpret_cast<float *>(pp.cprime);
+    k_tridiag_lines<float, float><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
+        M, L, N, m0, lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, s2, c32, c32 + (size_t)M * L * N);
     EDDY_LAUNCHED(ctx);
   }
   {
     ProfScope ps(ctx, PROF_GEMM_BWD);
-    if (x->bhi) {
-      if ((rc = launch_xform(ctx, s2, s1, x->bhi, x->blo))) return rc;
+    if (x->xp.bhi) {
+      if ((rc = launch_xform(ctx, &x->xp, 1, s2, s1))) return rc;
     } else {
       bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Ab32, M, s2, M, &zero, s1,
                        M);
@@ -679,7 +738,7 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   EDDY_LAUNCHED(ctx);
   k_sum_final<<<1, 32, 0, ctx->stream>>>(NPART, (long long)M * N, pp.red, ctx->scal + 3);
   EDDY_LAUNCHED(ctx);
-  size_t smem = sizeof(float) * (2 * L * (TI32 / 2) + L);
+  size_t smem = fft32_smem(L);
   dim3 g((M + TI32 - 1) / TI32, N);
   if (accumulate)
     k_bwd32<1><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi);
@@ -694,8 +753,9 @@ int fwd32(eddy_ctx *ctx, int mode, double alfxdt, const double *phi, double *dve
   MixedState *x = ms(ctx);
   PoissonPlan &pp = ctx->pp;
   const Dims &d = ctx->d;
-  size_t smem = sizeof(float) * (2 * pp.L * (TI32 / 2) + pp.L);
+  size_t smem = fft32_smem(pp.L);
   dim3 g((pp.M + TI32 - 1) / TI32, pp.N);
+  const double ralf = 1.0 / alfxdt;
   ProfScope ps(ctx, mode == 2 ? PROF_REFINE : PROF_DIV_FFT);
   auto *rm = reinterpret_cast<unsigned long long *>(x->resid + sweep);
   float *sp = reinterpret_cast<float *>(pp.spec);
@@ -703,13 +763,13 @@ int fwd32(eddy_ctx *ctx, int mode, double alfxdt, const double *phi, double *dve
   const double rdy2 = 1.0 / ctx->delysq;
   if (mode == 0)
     k_fwd32<0><<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
-                                               phi, dvec, alfxdt, rdy2, lg, x->twr, x->twi, sp, rm);
+                                               phi, dvec, ralf, rdy2, lg, x->twr, x->twi, sp, rm);
   else if (mode == 1)
     k_fwd32<1><<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
-                                               phi, dvec, alfxdt, rdy2, lg, x->twr, x->twi, sp, rm);
+                                               phi, dvec, ralf, rdy2, lg, x->twr, x->twi, sp, rm);
   else
     k_fwd32<2><<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,
-                                               phi, dvec, alfxdt, rdy2, lg, x->twr, x->twi, sp, rm);
+                                               phi, dvec, ralf, rdy2, lg, x->twr, x->twi, sp, rm);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
@@ -782,19 +842,20 @@ int mixed_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMemcpy(x->twr, twr.data(), sizeof(float) * L, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(x->twi, twi.data(), sizeof(float) * L, cudaMemcpyHostToDevice));
   if (xform_supported(ctx->pp.M)) {
-    int rc = xform_prepare(ctx, ctx->pp.Af, &x->fhi, &x->flo);
-    if (rc == EDDY_OK) rc = xform_prepare(ctx, ctx->pp.Ab, &x->bhi, &x->blo);
+    int rc = xform_prepare(ctx, &x->xp);
     if (rc) return rc;
   }
   EDDY_CUDA(cudaMalloc(&x->wout, sizeof(double) * (size_t)d.nx * d.ny));
   EDDY_CUDA(cudaMemset(x->wout, 0, sizeof(double) * (size_t)d.nx * d.ny));
   EDDY_CUDA(cudaMalloc(&x->resid, 4 * sizeof(double)));
   EDDY_CUDA(cudaMemset(x->resid, 0, 4 * sizeof(double)));
-  // the refined solve keeps c' and the forward-eliminated right-hand side in FP64
-  EDDY_CUDA(cudaFree(ctx->pp.cprime));
-  ctx->pp.cprime = nullptr;
-  EDDY_CUDA(cudaMalloc(&ctx->pp.cprime, 2 * sizeof(double) * (size_t)ctx->pp.M * ctx->pp.L * ctx->pp.N));
-  size_t smem = sizeof(float) * (2 * L * (TI32 / 2) + L);
+  // the correction solves keep c' and the forward-eliminated right-hand side
+  // in FP32, side by side in the (FP64-sized) c' buffer
+  if (L < 8) {
+    ctx->err = "the mixed form needs at least 8 cells along y";
+    return EDDY_EINVAL;
+  }
+  size_t smem = fft32_smem(L);
   if (smem > 48 * 1024) {
     EDDY_CUDA(cudaFuncSetAttribute(k_fwd32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     EDDY_CUDA(cudaFuncSetAttribute(k_fwd32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -817,8 +878,7 @@ void mixed_release(eddy_ctx *ctx) {
   for (float *p : fl) if (p) cudaFree(p);
   if (x->resid) cudaFree(x->resid);
   if (x->wout) cudaFree(x->wout);
-  float *tw[] = {x->fhi, x->flo, x->bhi, x->blo};
-  for (float *p : tw) if (p) cudaFree(p);
+  xform_release(&x->xp);
   delete x;
   ctx->mixed = nullptr;
 }
@@ -877,11 +937,11 @@ int mixed_after_sgs(eddy_ctx *ctx) {
   return to32(ctx, ctx->prm.closure == 1 ? ctx->kappa : ctx->f[EDDY_TV], x->kv);
 }
 
-// before the eddy viscosity: the FP64 density the closure features read
-int mixed_before_sgs(eddy_ctx *ctx) {
-  if (ctx->prm.closure != 1 || ctx->prm.idens != 1) return EDDY_OK;
-  ProfScope ps(ctx, PROF_CONVERT);
-  return to64(ctx, ms(ctx)->dens, ctx->f[EDDY_DENS]);
+int mixed_views(eddy_ctx *ctx, MixedViews *v) {
+  MixedState *x = ms(ctx);
+  if (!x) return EDDY_EINVAL;
+  *v = MixedViews{x->uo, x->vo, x->wo, x->dens, x->tv, x->kv, x->px};
+  return EDDY_OK;
 }
 
 // BOUNDINOUT predictor (src/boundary.f:694-944) on the FP32 u*: inlet plane,

@@ -1,12 +1,13 @@
 // k_mlp.cu -- learned eddy-viscosity closure on the 5th-generation tensor
-// cores: a per-cell MLP 12 -> 64 -> 64 -> 64 -> 2 (SiLU, softplus outputs),
+// cores: a per-cell MLP 12 -> 64 -> 64 -> 64 -> 2 (hard-swish hidden
+// activations, softplus outputs),
 // BF16 operands, FP32 accumulation in TMEM (tcgen05.mma kind::f16).
 //
 //  * k_umma_gemm      : D[M x N] (+)= A[M x K] * B[N x K]^T, BF16 in, FP32 out;
 //                       the training GEMMs (forward, input gradient, weight
 //                       gradient) all map onto it.
 //  * k_mlp_infer      : fused per-cell inference: features of a 128-cell tile
-//                       -> four MMA layers with bias/SiLU epilogues from TMEM
+//                       -> four MMA layers with bias/activation epilogues from TMEM
 //                       -> coefficients C_nu, C_kappa -> nu_t = C_nu Delta^2 |S|,
 //                       kappa_t = C_kappa Delta^2 |S|.
 // The closure stands in for the dynamic procedure's test filtering and
@@ -174,7 +175,11 @@ struct MlpMeta {
   float mean[NFEAT], istd[NFEAT], lo[NFEAT], hi[NFEAT], s_nu, s_kappa;
 };
 
-__device__ __forceinline__ float silu(float x) { return x / (1.f + __expf(-x)); }
+// hidden activation: hard-swish x * sat(x/6 + 1/2) (SiLU-shaped, FMA-pipe only)
+__device__ __forceinline__ float hswish(float x) { return x * __saturatef(fmaf(x, 1.f / 6.f, 0.5f)); }
+__device__ __forceinline__ float hswish_grad(float x) {
+  return x <= -3.f ? 0.f : (x >= 3.f ? 1.f : fmaf(x, 1.f / 3.f, 0.5f));
+}
 __device__ __forceinline__ float sigm(float x) { return 1.f / (1.f + __expf(-x)); }
 __device__ __forceinline__ float softplus(float x) { return x > 20.f ? x : log1pf(__expf(x)); }
 
@@ -186,35 +191,46 @@ struct CellGeom {
   const double *cx, *cy, *cz;
 };
 
+// T: storage of the fields (FP64 arrays of pitch NX, or the mixed form's
+// FP32 copies of pitch px); A: arithmetic of the gradients
+template <class T, class A>
 __device__ __forceinline__ void cell_features(const Dims &d, const DevMetrics &m, const CellGeom &cg, double grav,
-                                              double xwall_lo, double xwall_hi, const double *__restrict__ uo,
-                                              const double *__restrict__ vo, const double *__restrict__ wo,
-                                              const double *__restrict__ dens, const double *__restrict__ xc,
-                                              int i, int j, int k, float *f, float &delta) {
-  const long long q = fidx(d, i, j, k);
-  const long long sy = d.nx, sz = (long long)d.nx * d.ny;
-  auto UC = [&](long long o) { return 0.5 * (uo[q + o - 1] + uo[q + o]); };
-  auto VC = [&](long long o) { return 0.5 * (vo[q + o - sy] + vo[q + o]); };
-  auto WC = [&](long long o) { return 0.5 * (wo[q + o - sz] + wo[q + o]); };
-  double dudx = m.ap[i] * (uo[q] - uo[q - 1]);
-  double dudy = 0.5 * (m.bv[j] * (UC(sy) - UC(0)) + m.bv[j - 1] * (UC(0) - UC(-sy)));
-  double dudz = 0.5 * (m.cw[k] * (UC(sz) - UC(0)) + m.cw[k - 1] * (UC(0) - UC(-sz)));
-  double dvdx = 0.5 * (m.au[i] * (VC(1) - VC(0)) + m.au[i - 1] * (VC(0) - VC(-1)));
-  double dvdy = m.bp[j] * (vo[q] - vo[q - sy]);
-  double dvdz = 0.5 * (m.cw[k] * (VC(sz) - VC(0)) + m.cw[k - 1] * (VC(0) - VC(-sz)));
-  double dwdx = 0.5 * (m.au[i] * (WC(1) - WC(0)) + m.au[i - 1] * (WC(0) - WC(-1)));
-  double dwdy = 0.5 * (m.bv[j] * (WC(sy) - WC(0)) + m.bv[j - 1] * (WC(0) - WC(-sy)));
-  double dwdz = m.cp[k] * (wo[q] - wo[q - sz]);
-  double drx = 0.5 * (m.au[i] * (dens[q + 1] - dens[q]) + m.au[i - 1] * (dens[q] - dens[q - 1]));
-  double dry = 0.5 * (m.bv[j] * (dens[q + sy] - dens[q]) + m.bv[j - 1] * (dens[q] - dens[q - sy]));
-  double drz = 0.5 * (m.cw[k] * (dens[q + sz] - dens[q]) + m.cw[k - 1] * (dens[q] - dens[q - sz]));
-  double del = cg.cx[i] * cg.cy[j] * cg.cz[k];
+                                              double xwall_lo, double xwall_hi, int pitch, const T *__restrict__ uo,
+                                              const T *__restrict__ vo, const T *__restrict__ wo,
+                                              const T *__restrict__ dens, const double *__restrict__ xc, int i, int j,
+                                              int k, float *f, float &delta) {
+  const long long q = pidx(d, pitch, i, j, k);
+  const long long sy = pitch, sz = (long long)pitch * d.ny;
+  const A h = (A)0.5;
+  auto U = [&](long long o) { return (A)uo[q + o]; };
+  auto V = [&](long long o) { return (A)vo[q + o]; };
+  auto W = [&](long long o) { return (A)wo[q + o]; };
+  auto R = [&](long long o) { return (A)dens[q + o]; };
+  auto UC = [&](long long o) { return h * (U(o - 1) + U(o)); };
+  auto VC = [&](long long o) { return h * (V(o - sy) + V(o)); };
+  auto WC = [&](long long o) { return h * (W(o - sz) + W(o)); };
+  const A api = (A)m.ap[i], aui = (A)m.au[i], aum = (A)m.au[i - 1];
+  const A bpj = (A)m.bp[j], bvj = (A)m.bv[j], bvm = (A)m.bv[j - 1];
+  const A cpk = (A)m.cp[k], cwk = (A)m.cw[k], cwm = (A)m.cw[k - 1];
+  A dudx = api * (U(0) - U(-1));
+  A dudy = h * (bvj * (UC(sy) - UC(0)) + bvm * (UC(0) - UC(-sy)));
+  A dudz = h * (cwk * (UC(sz) - UC(0)) + cwm * (UC(0) - UC(-sz)));
+  A dvdx = h * (aui * (VC(1) - VC(0)) + aum * (VC(0) - VC(-1)));
+  A dvdy = bpj * (V(0) - V(-sy));
+  A dvdz = h * (cwk * (VC(sz) - VC(0)) + cwm * (VC(0) - VC(-sz)));
+  A dwdx = h * (aui * (WC(1) - WC(0)) + aum * (WC(0) - WC(-1)));
+  A dwdy = h * (bvj * (WC(sy) - WC(0)) + bvm * (WC(0) - WC(-sy)));
+  A dwdz = cpk * (W(0) - W(-sz));
+  A drx = h * (aui * (R(1) - R(0)) + aum * (R(0) - R(-1)));
+  A dry = h * (bvj * (R(sy) - R(0)) + bvm * (R(0) - R(-sy)));
+  A drz = h * (cwk * (R(sz) - R(0)) + cwm * (R(0) - R(-sz)));
+  A del = (A)(cg.cx[i] * cg.cy[j] * cg.cz[k]);
   delta = (float)del;
   f[0] = (float)(del * dudx); f[1] = (float)(del * dudy); f[2] = (float)(del * dudz);
   f[3] = (float)(del * dvdx); f[4] = (float)(del * dvdy); f[5] = (float)(del * dvdz);
   f[6] = (float)(del * dwdx); f[7] = (float)(del * dwdy); f[8] = (float)(del * dwdz);
   f[9] = (float)(del * sqrt(drx * drx + dry * dry + drz * drz));
-  f[10] = (float)(-grav * drx);
+  f[10] = (float)(-(A)grav * drx);
   double x = xc[i];
   f[11] = (float)fmin(x - xwall_lo, xwall_hi - x);
 }
@@ -240,19 +256,25 @@ __global__ void k_harvest(Dims d, DevMetrics m, CellGeom cg, double grav, double
   int i, j, k;
   interior_ijk(d, (unsigned)cells[s], i, j, k);
   float f[NFEAT], del;
-  cell_features(d, m, cg, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
+  cell_features<double, double>(d, m, cg, grav, xlo, xhi, d.nx, uo, vo, wo, dens, xc, i, j, k, f, del);
   for (int c = 0; c < NFEAT; c++) X[(size_t)s * NFEAT + c] = f[c];
   T[s] = (float)(tv[fidx(d, i, j, k)] / del);
 }
 
 // ---- fused inference ------------------------------------------------------
+// One CTA of 128 threads runs two 128-cell tiles at a time (thread t owns
+// cell t of each), with separate activation buffers and TMEM accumulators
+// (columns 0..63 and 64..127): while the tensor core runs one tile's layer,
+// the threads run the other tile's epilogue.
 constexpr int IT = 128;
 struct InferSmem {
   unsigned char w1[HID * KIN * 2], w2[HID * HID * 2], w3[HID * HID * 2], w4[NOUT * HID * 2];
-  unsigned char a0[128 * KIN * 2], h[128 * HID * 2];
+  // h[g]: layer input of tile g; the normalised features (layer 1's input,
+  // 128 x KIN) occupy its first 4 KB until layer 1's MMA has read them
+  unsigned char h[2][128 * HID * 2];
   float b1[HID], b2[HID], b3[HID], b4[NOUT];
   MlpMeta meta;
-  uint64_t bar;
+  uint64_t bar[2];
   uint32_t tmem;
   int nout;
 };
@@ -274,39 +296,39 @@ __device__ __forceinline__ void mma_layer(uint32_t tm, const unsigned char *a, c
   }
 }
 
-// SiLU of two pre-activations given as halves h = x/2 (FP32), in BF16x2:
-// silu(x) = x sigmoid(x) = h + h tanh(h); one tanh.approx.bf16x2 per pair
-__device__ __forceinline__ uint32_t silu2_bf16(float h0, float h1) {
-  __nv_bfloat162 hb = __floats2bfloat162_rn(h0, h1);
-  uint32_t hv = *reinterpret_cast<uint32_t *>(&hb), tv, r;
-  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tv) : "r"(hv));
-  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(r) : "r"(hv), "r"(tv));
-  return r;
+// two activations packed to BF16x2 (round to nearest)
+__device__ __forceinline__ uint32_t act2_bf16(float x0, float x1) {
+  __nv_bfloat162 hb = __floats2bfloat162_rn(hswish(x0), hswish(x1));
+  return *reinterpret_cast<uint32_t *>(&hb);
 }
 
-// hidden epilogue: TMEM (64 cols of this thread's row) + bias -> SiLU -> bf16
-// row of the next layer's A operand.  hbias = bias / 2.
-__device__ __forceinline__ void hidden_epilogue(uint32_t tm, int warp, int row, const float *hbias,
+// hidden epilogue: TMEM (64 cols of this thread's row) + bias -> hard-swish
+// -> bf16 row of the next layer's A operand
+__device__ __forceinline__ void hidden_epilogue(uint32_t tm, int warp, int row, const float *bias,
                                                 unsigned char *h) {
   uint32_t r[HID];
   umma::tmem_ld64(tm + ((uint32_t)(warp * 32) << 16), r);
-  auto x = [&](int c) { return fmaf(__uint_as_float(r[c]), 0.5f, hbias[c]); };
+  auto x = [&](int c) { return __uint_as_float(r[c]) + bias[c]; };
 #pragma unroll
   for (int c0 = 0; c0 < HID; c0 += 8) {
     uint4 o;
-    o.x = silu2_bf16(x(c0 + 0), x(c0 + 1));
-    o.y = silu2_bf16(x(c0 + 2), x(c0 + 3));
-    o.z = silu2_bf16(x(c0 + 4), x(c0 + 5));
-    o.w = silu2_bf16(x(c0 + 6), x(c0 + 7));
+    o.x = act2_bf16(x(c0 + 0), x(c0 + 1));
+    o.y = act2_bf16(x(c0 + 2), x(c0 + 3));
+    o.z = act2_bf16(x(c0 + 4), x(c0 + 5));
+    o.w = act2_bf16(x(c0 + 6), x(c0 + 7));
     *reinterpret_cast<uint4 *>(h + umma::kmajor_offset(row, c0, HID)) = o;
   }
 }
 
+// one thread waits on the MMA barrier, the block meets at a barrier (the
+// other warps sleep there instead of polling the mbarrier)
 __device__ __forceinline__ bool sync_and_wait(uint64_t *bar, int &phase) {
-  bool ok = umma::mbar_wait(bar, phase);
+  int ok = 1;
+  if (threadIdx.x == 0) ok = umma::mbar_wait(bar, phase) ? 1 : 0;
   phase ^= 1;
+  ok = __syncthreads_and(ok);
   umma::fence_after_sync();
-  return ok;
+  return ok != 0;
 }
 
 __device__ __forceinline__ void publish_smem() {
@@ -316,24 +338,36 @@ __device__ __forceinline__ void publish_smem() {
   umma::fence_after_sync();
 }
 
+// one cell of a tile: where it is and what the output needs
+struct CellIn {
+  bool valid, outside;
+  int i, j, k;
+  float del, dsr;
+};
+
 // nu_t -> tv, kappa_t -> kappa for every interior cell; cells whose
 // normalised features leave [lo, hi] take the fallback (last dynamic-model
-// value).  counts[0] += out-of-envelope cells.
+// value).  counts[0] += out-of-envelope cells.  T: storage of the input
+// fields (pitch `pitch`); tv32/kv32 (pitch px32, may be null): FP32 copies
+// of the outputs for the mixed form's stencils.
+template <class T>
 __global__ void __launch_bounds__(IT)
-    k_mlp_infer(Dims d, DevMetrics m, CellGeom cg, double grav, double xlo, double xhi, const double *__restrict__ uo,
-                const double *__restrict__ vo, const double *__restrict__ wo, const double *__restrict__ dens,
-                const double *__restrict__ xc, const __nv_bfloat16 *__restrict__ wbf, const float *__restrict__ theta,
-                const float *__restrict__ meta, const double *__restrict__ fallback, double *__restrict__ tv,
-                double *__restrict__ kappa, unsigned long long *counts, int *err) {
+    k_mlp_infer(Dims d, DevMetrics m, CellGeom cg, double grav, double xlo, double xhi, int pitch,
+                const T *__restrict__ uo, const T *__restrict__ vo, const T *__restrict__ wo,
+                const T *__restrict__ dens, const double *__restrict__ xc, const __nv_bfloat16 *__restrict__ wbf,
+                const float *__restrict__ theta, const float *__restrict__ meta, const double *__restrict__ fallback,
+                double *__restrict__ tv, double *__restrict__ kappa, float *__restrict__ tv32,
+                float *__restrict__ kv32, int px32, unsigned long long *counts, int *err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   InferSmem &S = *reinterpret_cast<InferSmem *>(smraw);
   const int tid = threadIdx.x, warp = tid >> 5;
   if (warp == 0) {
-    umma::tmem_alloc(&S.tmem, 64);
+    umma::tmem_alloc(&S.tmem, 128);
     umma::tmem_relinquish();
   }
   if (tid == 0) {
-    umma::mbar_init(&S.bar, 1);
+    umma::mbar_init(&S.bar[0], 1);
+    umma::mbar_init(&S.bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     S.nout = 0;
   }
@@ -341,76 +375,99 @@ __global__ void __launch_bounds__(IT)
   stage_weights(S.w2, wbf + OFF_W2, HID, HID);
   stage_weights(S.w3, wbf + OFF_W3, HID, HID);
   stage_weights(S.w4, wbf + OFF_W4, NOUT, HID);
-  for (int e = tid; e < HID; e += IT) {  // hidden biases halved for the SiLU epilogue
-    S.b1[e] = 0.5f * theta[OFF_B1 + e];
-    S.b2[e] = 0.5f * theta[OFF_B2 + e];
-    S.b3[e] = 0.5f * theta[OFF_B3 + e];
+  for (int e = tid; e < HID; e += IT) {
+    S.b1[e] = theta[OFF_B1 + e];
+    S.b2[e] = theta[OFF_B2 + e];
+    S.b3[e] = theta[OFF_B3 + e];
   }
   if (tid < NOUT) S.b4[tid] = theta[OFF_B4 + tid];
   for (int e = tid; e < NMETA; e += IT) reinterpret_cast<float *>(&S.meta)[e] = meta[e];
   publish_smem();
   const uint32_t tm = S.tmem;
   const unsigned ninner = (unsigned)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
-  const unsigned ntiles = (ninner + 127) / 128;
-  int phase = 0;
+  const unsigned ntiles = (ninner + 127) / 128, npairs = (ntiles + 1) / 2;
+  const unsigned char *wl[3] = {S.w2, S.w3, S.w4};
+  const float *bl[3] = {S.b1, S.b2, S.b3};
+  int phase[2] = {0, 0};
   bool ok = true;
   int nout = 0;
-  for (unsigned tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    unsigned t = tile * 128 + tid;
-    bool valid = t < ninner;
-    int i = d.ix1, j = d.jy1, k = d.kz1;
-    float f[NFEAT], del = 1.f, dsr = 0.f;
-    bool outside = false;
-    if (valid) {
-      interior_ijk(d, t, i, j, k);
-      cell_features(d, m, cg, grav, xlo, xhi, uo, vo, wo, dens, xc, i, j, k, f, del);
-      // Delta |S| = Delta sqrt(2 S_ij S_ij) from the raw gradient features
-      const float s01 = 0.5f * (f[1] + f[3]), s02 = 0.5f * (f[2] + f[6]), s12 = 0.5f * (f[5] + f[7]);
-      dsr = sqrtf(2.f * (f[0] * f[0] + f[4] * f[4] + f[8] * f[8] + 2.f * (s01 * s01 + s02 * s02 + s12 * s12)));
-      for (int c = 0; c < NFEAT; c++) {
-        f[c] = (f[c] - S.meta.mean[c]) * S.meta.istd[c];
-        outside = outside || !(f[c] >= S.meta.lo[c] && f[c] <= S.meta.hi[c]);
-      }
-    } else {
-      for (int c = 0; c < NFEAT; c++) f[c] = 0.f;
-    }
-    __align__(16) __nv_bfloat16 o[16];
-    for (int c = 0; c < 16; c++) o[c] = __float2bfloat16_rn(c < NFEAT ? f[c] : 0.f);
-    *reinterpret_cast<uint4 *>(S.a0 + umma::kmajor_offset(tid, 0, KIN)) = *reinterpret_cast<uint4 *>(o);
-    *reinterpret_cast<uint4 *>(S.a0 + umma::kmajor_offset(tid, 8, KIN)) = *reinterpret_cast<uint4 *>(o + 8);
-    publish_smem();
-    if (tid == 0) { mma_layer(tm, S.a0, S.w1, HID, KIN); umma::commit(&S.bar); }
-    ok = sync_and_wait(&S.bar, phase) && ok;
-    hidden_epilogue(tm, warp, tid, S.b1, S.h);
-    publish_smem();
-    if (tid == 0) { mma_layer(tm, S.h, S.w2, HID, HID); umma::commit(&S.bar); }
-    ok = sync_and_wait(&S.bar, phase) && ok;
-    __syncthreads();  // every row has read layer-1 activations into the MMA
-    hidden_epilogue(tm, warp, tid, S.b2, S.h);
-    publish_smem();
-    if (tid == 0) { mma_layer(tm, S.h, S.w3, HID, HID); umma::commit(&S.bar); }
-    ok = sync_and_wait(&S.bar, phase) && ok;
-    __syncthreads();
-    hidden_epilogue(tm, warp, tid, S.b3, S.h);
-    publish_smem();
-    if (tid == 0) { mma_layer(tm, S.h, S.w4, NOUT, HID); umma::commit(&S.bar); }
-    ok = sync_and_wait(&S.bar, phase) && ok;
-    float v[16];
-    umma::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16), v);
-    if (valid && ok) {
-      long long q = fidx(d, i, j, k);
-      double nu, ka;
-      if (outside) {
-        nu = fallback[q];
-        ka = fallback[q];
-        nout++;
+  for (unsigned pair = blockIdx.x; pair < npairs && ok; pair += gridDim.x) {
+    CellIn c[2];
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+      const unsigned t = (2 * pair + g) * 128 + tid;
+      CellIn &C = c[g];
+      C.valid = t < ninner;
+      C.outside = false;
+      C.i = d.ix1; C.j = d.jy1; C.k = d.kz1;
+      C.del = 1.f; C.dsr = 0.f;
+      float f[NFEAT];
+      if (C.valid) {
+        interior_ijk(d, t, C.i, C.j, C.k);
+        cell_features<T, T>(d, m, cg, grav, xlo, xhi, pitch, uo, vo, wo, dens, xc, C.i, C.j, C.k, f, C.del);
+        // Delta |S| = Delta sqrt(2 S_ij S_ij) from the raw gradient features
+        const float s01 = 0.5f * (f[1] + f[3]), s02 = 0.5f * (f[2] + f[6]), s12 = 0.5f * (f[5] + f[7]);
+        C.dsr = sqrtf(2.f * (f[0] * f[0] + f[4] * f[4] + f[8] * f[8] + 2.f * (s01 * s01 + s02 * s02 + s12 * s12)));
+        for (int q = 0; q < NFEAT; q++) {
+          f[q] = (f[q] - S.meta.mean[q]) * S.meta.istd[q];
+          C.outside = C.outside || !(f[q] >= S.meta.lo[q] && f[q] <= S.meta.hi[q]);
+        }
       } else {
-        // nu_t = C_nu Delta^2 |S|, kappa_t = C_kappa Delta^2 |S|
-        nu = (double)del * (double)dsr * S.meta.s_nu * softplus(v[0] + S.b4[0]);
-        ka = (double)del * (double)dsr * S.meta.s_kappa * softplus(v[1] + S.b4[1]);
+        for (int q = 0; q < NFEAT; q++) f[q] = 0.f;
       }
-      tv[q] = nu;
-      kappa[q] = ka;
+      __align__(16) __nv_bfloat16 o[16];
+      for (int q = 0; q < 16; q++) o[q] = __float2bfloat16_rn(q < NFEAT ? f[q] : 0.f);
+      *reinterpret_cast<uint4 *>(S.h[g] + umma::kmajor_offset(tid, 0, KIN)) = *reinterpret_cast<uint4 *>(o);
+      *reinterpret_cast<uint4 *>(S.h[g] + umma::kmajor_offset(tid, 8, KIN)) = *reinterpret_cast<uint4 *>(o + 8);
+    }
+    publish_smem();
+    if (tid == 0) {
+      mma_layer(tm, S.h[0], S.w1, HID, KIN);
+      umma::commit(&S.bar[0]);
+      mma_layer(tm + 64, S.h[1], S.w1, HID, KIN);
+      umma::commit(&S.bar[1]);
+    }
+    // layers 2..4: epilogue of layer L of one tile while the other tile's
+    // layer runs on the tensor core
+#pragma unroll
+    for (int L = 0; L < 3; L++) {
+#pragma unroll
+      for (int g = 0; g < 2; g++) {
+        ok = sync_and_wait(&S.bar[g], phase[g]) && ok;
+        hidden_epilogue(tm + 64 * g, warp, tid, bl[L], S.h[g]);
+        publish_smem();
+        if (tid == 0) {
+          mma_layer(tm + 64 * g, S.h[g], wl[L], L == 2 ? NOUT : HID, HID);
+          umma::commit(&S.bar[g]);
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+      ok = sync_and_wait(&S.bar[g], phase[g]) && ok;
+      float v[16];
+      umma::tmem_ld16(tm + 64 * g + ((uint32_t)(warp * 32) << 16), v);
+      const CellIn &C = c[g];
+      if (C.valid && ok) {
+        long long q = fidx(d, C.i, C.j, C.k);
+        double nu, ka;
+        if (C.outside) {
+          nu = fallback[q];
+          ka = fallback[q];
+          nout++;
+        } else {
+          // nu_t = C_nu Delta^2 |S|, kappa_t = C_kappa Delta^2 |S|
+          nu = (double)C.del * (double)C.dsr * S.meta.s_nu * softplus(v[0] + S.b4[0]);
+          ka = (double)C.del * (double)C.dsr * S.meta.s_kappa * softplus(v[1] + S.b4[1]);
+        }
+        tv[q] = nu;
+        kappa[q] = ka;
+        if (tv32) {
+          const long long p = pidx(d, px32, C.i, C.j, C.k);
+          tv32[p] = (float)nu;
+          kv32[p] = (float)ka;
+        }
+      }
     }
     umma::fence_before_sync();
     ok = __syncthreads_and(ok ? 1 : 0) != 0;  // block-uniform loop exit
@@ -421,18 +478,18 @@ __global__ void __launch_bounds__(IT)
   umma::fence_before_sync();
   __syncthreads();
   if (tid == 0 && S.nout) atomicAdd(counts, (unsigned long long)S.nout);
-  if (warp == 0) umma::tmem_dealloc(tm, 64);
+  if (warp == 0) umma::tmem_dealloc(tm, 128);
 }
 
 // ---- training -------------------------------------------------------------
-// Z (B x n, f32, pre-bias) += bias; A = bf16(SiLU(Z)) in both B x n and n x B
+// Z (B x n, f32, pre-bias) += bias; A = bf16(hswish(Z)) in both B x n and n x B
 __global__ void k_fwd_act(int B, int n, float *Z, const float *bias, __nv_bfloat16 *A, __nv_bfloat16 *AT) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)B * n) return;
   int b = (int)(t / n), c = (int)(t % n);
   float z = Z[t] + bias[c];
   Z[t] = z;
-  __nv_bfloat16 a = __float2bfloat16_rn(silu(z));
+  __nv_bfloat16 a = __float2bfloat16_rn(hswish(z));
   A[t] = a;
   AT[(size_t)c * B + b] = a;
 }
@@ -466,7 +523,7 @@ __global__ void k_out_grad(int B, float *Z4, const float *b4, const float *Y, __
   if (threadIdx.x == 0) atomicAdd(loss, sl);
 }
 
-// hidden backward: dZ = dA * SiLU'(Z) (bf16, both layouts), db += column sums
+// hidden backward: dZ = dA * act'(Z) (bf16, both layouts), db += column sums
 __global__ void k_bwd_act(int B, int n, const float *dA, const float *Z, __nv_bfloat16 *dZ, __nv_bfloat16 *dZT,
                           float *db) {
   __shared__ float sdb[HID];
@@ -475,8 +532,7 @@ __global__ void k_bwd_act(int B, int n, const float *dA, const float *Z, __nv_bf
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < (long long)B * n) {
     int b = (int)(t / n), c = (int)(t % n);
-    float z = Z[t], s = sigm(z);
-    float g = dA[t] * (s * (1.f + z * (1.f - s)));
+    float g = dA[t] * hswish_grad(Z[t]);
     __nv_bfloat16 gb = __float2bfloat16_rn(g);
     dZ[t] = gb;
     dZT[(size_t)c * B + b] = gb;
@@ -863,16 +919,27 @@ int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigne
   }
   EDDY_CUDA(cudaMemsetAsync(s->counts, 0, sizeof(unsigned long long), ctx->stream));
   size_t smem = sizeof(InferSmem) + 1024;
-  EDDY_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
   long long ninner = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
-  long long ntiles = (ninner + 127) / 128;
-  int grid = (int)std::min<long long>(ntiles, (long long)nsm * 8);
-  k_mlp_infer<<<grid, IT, smem, ctx->stream>>>(d, ctx->m, cg, ctx->sc.grav, xu[1], xu[d.ix2], ctx->f[EDDY_UO],
-                                              ctx->f[EDDY_VO], ctx->f[EDDY_WO], ctx->f[EDDY_DENS], ctx->xc_dev, s->w,
-                                              s->theta, s->meta, fallback, ctx->f[EDDY_TV], kappa, s->counts,
-                                              ctx->err_flag);
+  long long npairs = ((ninner + 127) / 128 + 1) / 2;
+  int grid = (int)std::min<long long>(npairs, (long long)nsm * 4);
+  MixedViews mv;
+  if (ctx->mixed && mixed_views(ctx, &mv) == EDDY_OK) {
+    // the mixed form: features from the FP32 copies, FP32 outputs alongside
+    EDDY_CUDA(cudaFuncSetAttribute(k_mlp_infer<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_mlp_infer<float><<<grid, IT, smem, ctx->stream>>>(d, ctx->m, cg, ctx->sc.grav, xu[1], xu[d.ix2], mv.px, mv.uo,
+                                                        mv.vo, mv.wo, mv.dens, ctx->xc_dev, s->w, s->theta, s->meta,
+                                                        fallback, ctx->f[EDDY_TV], kappa, mv.tv, mv.kv, mv.px,
+                                                        s->counts, ctx->err_flag);
+  } else {
+    EDDY_CUDA(cudaFuncSetAttribute(k_mlp_infer<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_mlp_infer<double><<<grid, IT, smem, ctx->stream>>>(d, ctx->m, cg, ctx->sc.grav, xu[1], xu[d.ix2], d.nx,
+                                                         ctx->f[EDDY_UO], ctx->f[EDDY_VO], ctx->f[EDDY_WO],
+                                                         ctx->f[EDDY_DENS], ctx->xc_dev, s->w, s->theta, s->meta,
+                                                         fallback, ctx->f[EDDY_TV], kappa, nullptr, nullptr, 0,
+                                                         s->counts, ctx->err_flag);
+  }
   EDDY_LAUNCHED(ctx);
   if (out_of_envelope)
     EDDY_CUDA(cudaMemcpyAsync(out_of_envelope, s->counts, sizeof(unsigned long long), cudaMemcpyDeviceToHost,

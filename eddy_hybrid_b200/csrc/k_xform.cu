@@ -8,14 +8,24 @@
 // tcgen05.mma kind::tf32, which keeps the transform at FP32 accuracy (the
 // refinement sweeps then see the same convergence as with an FP32 GEMM).
 //
-// One CTA per 128-line tile, all M outputs (TMEM columns 0..M-1, M <= 512).
-// K is streamed in chunks of 16 through a 3-stage shared-memory pipeline:
-// the A chunk arrives by four 2-D TMA boxes (16 bytes x 128 lines each) so
+// Mirror-symmetric x operators (a grid symmetric about its centre, the same
+// boundary type at both ends: the eigenvectors are even or odd about the
+// centre) take the split form with half the work: with H = M/2 and the modes
+// ordered even then odd,
+//   forward:  c_even = F_e (f[x] + f[M-1-x]),  c_odd = F_o (f[x] - f[M-1-x]),
+//   backward: e = B_e c_even, o = B_o c_odd, f[x] = e + o, f[M-1-x] = e - o,
+// all four matrices H x H.
+//
+// One CTA per 128-line tile, all M outputs in TMEM columns 0..M-1 (M <= 512).
+// K is streamed in chunks of 8 through a multi-stage shared-memory pipeline:
+// each A chunk arrives by two 2-D TMA boxes (16 bytes x 128 lines each) so
 // shared memory holds it in the canonical no-swizzle K-major layout
 // [k/4][line][4]; the B chunks (prepared on the host in that layout, hi and
-// lo) arrive by 1-D bulk copies.  The CTA splits A into hi/lo in shared
-// memory, one thread issues the MMAs and commits them to the stage's "empty"
-// barrier; the epilogue reads TMEM (lane = line) and stores rows.
+// lo) arrive by 1-D bulk copies.  Loading, splitting A into hi/lo (and, for
+// the symmetric forward transform, forming the mirror sums and differences)
+// and the MMAs run in separate warps so the three overlap across stages; the
+// epilogue reads TMEM (lane = line) and stores rows.
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -25,8 +35,9 @@
 
 namespace {
 
-constexpr int XT = 128;  // threads per CTA
-constexpr int KC = 16;   // K per pipeline stage
+constexpr int XT = 192;   // threads per CTA: loader warp, MMA warp, 4 splitter/epilogue warps
+constexpr int KC = 8;     // K per pipeline stage (one MMA k-step)
+constexpr int MAXST = 8;  // pipeline stages at most
 
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
@@ -64,191 +75,380 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint6
       : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tma::smem_u32(bar)) : "memory");
+}
+
+// 32 lanes x 32 bit, 32 consecutive columns, load and wait in one asm block
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ float4 tf32_hi(float4 v) {
+  float4 h;
+  h.x = __uint_as_float(__float_as_uint(v.x) & 0xFFFFE000u);
+  h.y = __uint_as_float(__float_as_uint(v.y) & 0xFFFFE000u);
+  h.z = __uint_as_float(__float_as_uint(v.z) & 0xFFFFE000u);
+  h.w = __uint_as_float(__float_as_uint(v.w) & 0xFFFFE000u);
+  return h;
+}
+
+__device__ __forceinline__ float4 sub4(float4 a, float4 b) {
+  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+
+// Per-stage layout.  mode 0 (plain): A, A_lo, B_hi, B_lo with B of M rows.
+// modes 1/2 (symmetric): A1, A1_lo, A2, A2_lo, B1_hi, B1_lo, B2_hi, B2_lo with
+// B1, B2 of H rows each.
 struct StageGeom {
-  int nn;             // outputs (= M)
+  int nb;             // rows of one B block (M or H)
+  int na;             // A blocks per stage (1 or 2)
   uint32_t a_bytes;   // 128 x KC floats
-  uint32_t b_bytes;   // nn x KC floats (one of hi / lo)
-  uint32_t stage;     // bytes per stage: A, A_lo, B_hi, B_lo
+  uint32_t b_bytes;   // nb x KC floats (one of hi / lo)
+  uint32_t stage;     // bytes per stage
 };
 
-__host__ __device__ inline StageGeom stage_geom(int nn) {
+__host__ __device__ inline StageGeom stage_geom(int mode, int M) {
   StageGeom g;
-  g.nn = nn;
+  g.na = mode ? 2 : 1;
+  g.nb = mode ? M / 2 : M;
   g.a_bytes = 128u * KC * 4u;
-  g.b_bytes = (uint32_t)nn * KC * 4u;
-  g.stage = 2u * g.a_bytes + 2u * g.b_bytes;
+  g.b_bytes = (uint32_t)g.nb * KC * 4u;
+  g.stage = g.na * (2u * g.a_bytes + 2u * g.b_bytes);
   return g;
 }
 
+// Warp roles: warp 0 loads (one lane issues the TMA and bulk copies of a
+// stage once the MMAs that read it have completed), warp 1 issues the MMAs
+// (one lane), warps 2-5 split each A chunk into hi/lo and, at the end, drain
+// TMEM (warp w reads lanes 32 (w % 4) .. +31).  Stage barriers: full (copies
+// landed), split (128 splitter arrivals), empty (MMAs done, tcgen05.commit),
+// and done after the last chunk.  Every wait is bounded; a timeout raises the
+// error flag, the roles stop issuing work and wait (bounded) for what they
+// already issued before TMEM is released.
 __global__ void __launch_bounds__(XT, 1)
     k_xform_tf32(const __grid_constant__ CUtensorMap amap, const float *__restrict__ bhi,
-                 const float *__restrict__ blo, float *__restrict__ out, long long P, int M, int nst, int *err) {
+                 const float *__restrict__ blo, float *__restrict__ out, long long P, int M, int mode, int nst,
+                 int *err) {
   extern __shared__ __align__(1024) unsigned char xsm[];
-  __shared__ __align__(8) uint64_t full[4], empty[4];
+  __shared__ __align__(8) uint64_t full[MAXST], split[MAXST], empty[MAXST], done;
   __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
   unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(xsm) + 1023) & ~uintptr_t(1023));
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const StageGeom G = stage_geom(M);
-  const int nch = M / KC;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const StageGeom G = stage_geom(mode, M);
+  const int H = M / 2;
+  const int nch = (mode ? H : M) / KC;
   const long long p0 = (long long)blockIdx.x * 128;
-  const int part0 = M < 256 ? M : 256, part1 = M - part0;
   uint32_t ncols = 64;
   while ((int)ncols < M) ncols <<= 1;
-  if (warp == 0) {
+  if (warp == 1) {
     umma::tmem_alloc(&tmem_base, ncols);
     umma::tmem_relinquish();
   }
   if (tid == 0) {
+    abort_flag = 0;
     for (int s = 0; s < nst; s++) {
       umma::mbar_init(&full[s], 1);
+      umma::mbar_init(&split[s], 128);
       umma::mbar_init(&empty[s], 1);
     }
+    umma::mbar_init(&done, 1);
     tma::fence_mbar_init();
   }
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tm = tmem_base;
-  auto st_a = [&](int s) { return base + (size_t)s * G.stage; };
-  auto st_alo = [&](int s) { return base + (size_t)s * G.stage + G.a_bytes; };
-  auto st_bhi = [&](int s) { return base + (size_t)s * G.stage + 2 * G.a_bytes; };
-  auto st_blo = [&](int s) { return base + (size_t)s * G.stage + 2 * G.a_bytes + G.b_bytes; };
-  auto issue = [&](int c) {
-    const int s = c % nst;
-    tma::mbar_expect_tx(&full[s], G.a_bytes + 2 * G.b_bytes);
-    for (int q = 0; q < KC / 4; q++)
-      load_2d(st_a(s) + q * 128 * 16, &amap, c * KC + 4 * q, (int)p0, &full[s]);
-    const size_t boff = (size_t)c * (KC / 4) * M * 4;  // floats
-    bulk_load(st_bhi(s), bhi + boff, G.b_bytes, &full[s]);
-    bulk_load(st_blo(s), blo + boff, G.b_bytes, &full[s]);
-  };
-  if (tid == 0)
-    for (int c = 0; c < nst && c < nch; c++) issue(c);
-  const uint32_t id0 = idesc_tf32(128, part0), id1 = part1 ? idesc_tf32(128, part1) : 0u;
-  const uint32_t lbo_a = 128 * 16, lbo_b = (uint32_t)M * 16;
-  bool ok = true;
-  int c = 0;
-  for (; c < nch; c++) {
-    const int s = c % nst;
-    ok = tma::mbar_wait(&full[s], (c / nst) & 1);
-    if (__syncthreads_or(ok ? 0 : 1)) { ok = false; break; }
-    // split A into TF32 hi (in place) and lo
-    float4 *a4 = reinterpret_cast<float4 *>(st_a(s));
-    float4 *l4 = reinterpret_cast<float4 *>(st_alo(s));
-    for (int e = tid; e < 128 * KC / 4; e += XT) {
-      float4 v = a4[e], h, l;
-      h.x = __uint_as_float(__float_as_uint(v.x) & 0xFFFFE000u); l.x = v.x - h.x;
-      h.y = __uint_as_float(__float_as_uint(v.y) & 0xFFFFE000u); l.y = v.y - h.y;
-      h.z = __uint_as_float(__float_as_uint(v.z) & 0xFFFFE000u); l.z = v.z - h.z;
-      h.w = __uint_as_float(__float_as_uint(v.w) & 0xFFFFE000u); l.w = v.w - h.w;
-      a4[e] = h;
-      l4[e] = l;
-    }
-    umma::fence_smem_to_async();
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (tid == 0) {
-      for (int ks = 0; ks < KC / 8; ks++) {
-        const uint32_t ko = ks * 2;  // two k-groups of 4 per MMA
-        uint64_t ah = umma::make_desc(st_a(s) + ko * lbo_a, lbo_a, 128);
-        uint64_t al = umma::make_desc(st_alo(s) + ko * lbo_a, lbo_a, 128);
-        const uint32_t first = (c == 0 && ks == 0) ? 0u : 1u;
-        for (int part = 0; part < (part1 ? 2 : 1); part++) {
-          const uint32_t boff = ko * lbo_b + (part ? part0 * 16 : 0);
-          uint64_t bh = umma::make_desc(st_bhi(s) + boff, lbo_b, 128);
-          uint64_t bl = umma::make_desc(st_blo(s) + boff, lbo_b, 128);
-          const uint32_t d = tm + (part ? (uint32_t)part0 : 0u);
-          const uint32_t id = part ? id1 : id0;
-          mma_tf32(d, ah, bh, id, first);
-          mma_tf32(d, ah, bl, id, 1u);
-          mma_tf32(d, al, bh, id, 1u);
-        }
-      }
-      umma::commit(&empty[s]);
-      // refill the stage the previous chunk used, once its MMAs are done
-      if (c >= 1 && c - 1 + nst < nch) {
-        const int sp = (c - 1) % nst;
-        if (!umma::mbar_wait(&empty[sp], ((c - 1) / nst) & 1)) {
-          atomicExch(err, 1);
-        } else {
-          issue(c - 1 + nst);
-        }
-      }
-    }
-  }
-  // all MMAs complete: the last chunk's commit covers every earlier MMA
-  bool done = false;
-  if (ok && c == nch) done = umma::mbar_wait(&empty[(nch - 1) % nst], ((nch - 1) / nst) & 1);
-  if (!done && tid == 0) {
+  // block h (0 or 1) of a stage: A_hi, A_lo, B_hi, B_lo
+  auto st_a = [&](int s, int h) { return base + (size_t)s * G.stage + h * (2 * G.a_bytes + 2 * G.b_bytes); };
+  auto st_alo = [&](int s, int h) { return st_a(s, h) + G.a_bytes; };
+  auto st_bhi = [&](int s, int h) { return st_a(s, h) + 2 * G.a_bytes; };
+  auto st_blo = [&](int s, int h) { return st_a(s, h) + 2 * G.a_bytes + G.b_bytes; };
+  auto fail = [&]() {
+    abort_flag = 1;
     atomicExch(err, 1);
-    // bounded waits for the copies and MMAs that may still be in flight
-    const int cf = c < nch ? c : nch - 1;
-    for (int q = cf; q < nch && q <= cf + nst - 2; q++) tma::mbar_wait(&full[q % nst], (q / nst) & 1, 1u << 20);
-    if (cf >= 1) umma::mbar_wait(&empty[(cf - 1) % nst], ((cf - 1) / nst) & 1, 1u << 20);
-  }
-  done = __syncthreads_and(done ? 1 : 0) != 0;
-  umma::fence_after_sync();
-  if (done) {
-    const long long row = p0 + warp * 32 + (tid & 31);
-    for (int c0 = 0; c0 < M; c0 += 64) {
-      uint32_t r[64];
-      umma::tmem_ld64(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-      if (row < P) {
-        float4 *dst = reinterpret_cast<float4 *>(out + row * M + c0);
-        const int nv = (M - c0 < 64 ? M - c0 : 64) / 4;
+  };
+  bool ok = true;
+  if (warp == 0) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int c = 0; c < nch && !abort_flag; c++) {
+        const int s = c % nst;
+        if (c >= nst && !umma::mbar_wait(&empty[s], ((c / nst) - 1) & 1)) { fail(); break; }
+        tma::mbar_expect_tx(&full[s], G.na * (G.a_bytes + 2 * G.b_bytes));
+        for (int h = 0; h < G.na; h++) {
+          // K offset of the A block: plain / first half at 8c; mirror block
+          // (forward) at M - 8(c+1); odd-mode block (backward) at H + 8c
+          const int k0 = h == 0 ? c * KC : (mode == 1 ? M - (c + 1) * KC : H + c * KC);
+          for (int q = 0; q < KC / 4; q++) load_2d(st_a(s, h) + q * 128 * 16, &amap, k0 + 4 * q, (int)p0, &full[s]);
+          const size_t boff = (size_t)h * G.nb * G.nb + (size_t)c * (KC / 4) * G.nb * 4;  // floats
+          bulk_load(st_bhi(s, h), bhi + boff, G.b_bytes, &full[s]);
+          bulk_load(st_blo(s, h), blo + boff, G.b_bytes, &full[s]);
+        }
+        issued = c + 1;
+      }
+      // copies still in flight land before the CTA may exit
+      for (int c = issued - nst < 0 ? 0 : issued - nst; c < issued; c++)
+        if (!umma::mbar_wait(&full[c % nst], (c / nst) & 1, 1u << 20)) atomicExch(err, 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t lbo_a = 128 * 16, lbo_b = (uint32_t)G.nb * 16;
+      for (int c = 0; c < nch; c++) {
+        const int s = c % nst;
+        if (abort_flag || !umma::mbar_wait(&split[s], (c / nst) & 1)) { fail(); break; }
+        umma::fence_after_sync();
+        const uint32_t acc = c == 0 ? 0u : 1u;
+        for (int h = 0; h < G.na; h++) {
+          const uint64_t ah = umma::make_desc(st_a(s, h), lbo_a, 128);
+          const uint64_t al = umma::make_desc(st_alo(s, h), lbo_a, 128);
+          // columns of this block: [h*H, h*H + nb) in the symmetric form; the
+          // plain form splits its M columns into MMAs of at most 256
+          for (int n0 = 0; n0 < G.nb; n0 += 256) {
+            const int nn = G.nb - n0 < 256 ? G.nb - n0 : 256;
+            const uint32_t id = idesc_tf32(128, nn);
+            const uint64_t bh = umma::make_desc(st_bhi(s, h) + n0 * 16, lbo_b, 128);
+            const uint64_t bl = umma::make_desc(st_blo(s, h) + n0 * 16, lbo_b, 128);
+            const uint32_t d = tm + (uint32_t)(h * H + n0);
+            mma_tf32(d, ah, bh, id, acc);
+            mma_tf32(d, ah, bl, id, 1u);
+            mma_tf32(d, al, bh, id, 1u);
+          }
+        }
+        umma::commit(&empty[s]);
+      }
+      // the commit after the last issued MMA completes once all of them have
+      umma::commit(&done);
+    }
+  } else {
+    const int t = tid - 64;
+    for (int c = 0; c < nch; c++) {
+      const int s = c % nst;
+      if (abort_flag) { ok = false; break; }
+      if (!umma::mbar_wait(&full[s], (c / nst) & 1)) { fail(); ok = false; break; }
+      // 128 rows x 2 k-groups = 256 float4 per A block; thread t handles
+      // (row t, both k-groups)
+      float4 *a1 = reinterpret_cast<float4 *>(st_a(s, 0));
+      float4 *l1 = reinterpret_cast<float4 *>(st_alo(s, 0));
+      if (mode == 1) {
+        // mirror sums and differences: local k of the mirror block is 7 - k
+        float4 *a2 = reinterpret_cast<float4 *>(st_a(s, 1));
+        float4 *l2 = reinterpret_cast<float4 *>(st_alo(s, 1));
+        const float4 x0 = a1[t], x1 = a1[128 + t], y0 = a2[t], y1 = a2[128 + t];
+        const float4 r0 = make_float4(y1.w, y1.z, y1.y, y1.x), r1 = make_float4(y0.w, y0.z, y0.y, y0.x);
+        const float4 s0 = make_float4(x0.x + r0.x, x0.y + r0.y, x0.z + r0.z, x0.w + r0.w);
+        const float4 s1 = make_float4(x1.x + r1.x, x1.y + r1.y, x1.z + r1.z, x1.w + r1.w);
+        const float4 d0 = sub4(x0, r0), d1 = sub4(x1, r1);
+        float4 h;
+        h = tf32_hi(s0); a1[t] = h; l1[t] = sub4(s0, h);
+        h = tf32_hi(s1); a1[128 + t] = h; l1[128 + t] = sub4(s1, h);
+        h = tf32_hi(d0); a2[t] = h; l2[t] = sub4(d0, h);
+        h = tf32_hi(d1); a2[128 + t] = h; l2[128 + t] = sub4(d1, h);
+      } else {
+        for (int hb = 0; hb < G.na; hb++) {
+          float4 *a = reinterpret_cast<float4 *>(st_a(s, hb));
+          float4 *l = reinterpret_cast<float4 *>(st_alo(s, hb));
 #pragma unroll
-        for (int q = 0; q < 16; q++)
-          if (q < nv)
-            dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
-                                 __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+          for (int e = 0; e < 2; e++) {
+            const float4 v = a[e * 128 + t], h = tf32_hi(v);
+            a[e * 128 + t] = h;
+            l[e * 128 + t] = sub4(v, h);
+          }
+        }
+      }
+      umma::fence_smem_to_async();
+      mbar_arrive(&split[s]);
+    }
+    // epilogue: all MMAs complete
+    if (ok && !umma::mbar_wait(&done, 0)) { fail(); ok = false; }
+    umma::fence_after_sync();
+    if (ok && !abort_flag) {
+      const int q4 = warp & 3;
+      const long long row = p0 + q4 * 32 + lane;
+      const uint32_t tl = tm + ((uint32_t)(q4 * 32) << 16);
+      float *orow = out + row * M;
+      if (mode == 2) {
+        // f[x] = e + o, f[M-1-x] = e - o
+        for (int c0 = 0; c0 < H; c0 += 32) {
+          uint32_t e[32], o[32];
+          tmem_ld32(tl + (uint32_t)c0, e);
+          tmem_ld32(tl + (uint32_t)(H + c0), o);
+          const int nv = (H - c0 < 32 ? H - c0 : 32) / 4;
+          if (row < P) {
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+              if (q < nv) {
+                float p[4], m[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                  const float ev = __uint_as_float(e[4 * q + u]), ov = __uint_as_float(o[4 * q + u]);
+                  p[u] = ev + ov;
+                  m[u] = ev - ov;
+                }
+                const int x = c0 + 4 * q;
+                *reinterpret_cast<float4 *>(orow + x) = make_float4(p[0], p[1], p[2], p[3]);
+                *reinterpret_cast<float4 *>(orow + (M - 4 - x)) = make_float4(m[3], m[2], m[1], m[0]);
+              }
+            }
+          }
+        }
+      } else {
+        for (int c0 = 0; c0 < M; c0 += 64) {
+          uint32_t r[64];
+          umma::tmem_ld64(tl + (uint32_t)c0, r);
+          if (row < P) {
+            float4 *dst = reinterpret_cast<float4 *>(orow + c0);
+            const int nv = (M - c0 < 64 ? M - c0 : 64) / 4;
+#pragma unroll
+            for (int q = 0; q < 16; q++)
+              if (q < nv)
+                dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                     __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+          }
+        }
       }
     }
   }
+  // on the error path the MMAs already issued may still run: wait (bounded)
+  // for their commit before TMEM is released
+  if (warp == 1 && lane == 0 && abort_flag) umma::mbar_wait(&done, 0, 1u << 20);
   umma::fence_before_sync();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tm, ncols);
+  if (warp == 1) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tm, ncols);
+  }
+}
+
+// hi/lo split of an FP64 value: hi the TF32 truncation of its FP32 rounding
+void split_tf32(double x, float &h, float &l) {
+  float f = (float)x;
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u &= 0xFFFFE000u;
+  std::memcpy(&h, &u, 4);
+  l = (float)(x - (double)h);
+}
+
+// append B[n][k] = T(n, k) (nb x nb, T given as a callable) in the [k/4][n][4]
+// layout to hi/lo
+template <class F>
+void append_block(int nb, F T, std::vector<float> &hi, std::vector<float> &lo) {
+  const size_t o0 = hi.size();
+  hi.resize(o0 + (size_t)nb * nb);
+  lo.resize(o0 + (size_t)nb * nb);
+  for (int n = 0; n < nb; n++)
+    for (int k = 0; k < nb; k++) {
+      const size_t o = o0 + ((size_t)(k / 4) * nb + n) * 4 + (k % 4);
+      split_tf32(T(n, k), hi[o], lo[o]);
+    }
+}
+
+int upload(eddy_ctx *ctx, const std::vector<float> &h, float **d) {
+  EDDY_CUDA(cudaMalloc(d, sizeof(float) * h.size()));
+  EDDY_CUDA(cudaMemcpy(*d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+  return EDDY_OK;
+}
+
+int xform_stages(int mode, int M) {
+  const size_t st = stage_geom(mode, M).stage;
+  int n = (int)((227 * 1024 - 2048) / st);
+  return n > MAXST ? MAXST : n;
 }
 
 }  // namespace
 
-// Device B matrices (hi, lo) in the [k/4][n][4] layout from a column-major
-// M x M FP64 matrix T with B[n][k] = T(n, k).
-int xform_prepare(eddy_ctx *ctx, const double *T_dev, float **bhi, float **blo) {
-  const int M = ctx->pp.M;
-  std::vector<double> T((size_t)M * M);
-  EDDY_CUDA(cudaMemcpy(T.data(), T_dev, sizeof(double) * T.size(), cudaMemcpyDeviceToHost));
-  std::vector<float> hi((size_t)M * M), lo((size_t)M * M);
-  for (int n = 0; n < M; n++)
-    for (int k = 0; k < M; k++) {
-      double x = T[(size_t)n + (size_t)M * k];
-      float f = (float)x;
-      uint32_t u;
-      std::memcpy(&u, &f, 4);
-      u &= 0xFFFFE000u;
-      float h;
-      std::memcpy(&h, &u, 4);
-      float l = (float)(x - (double)h);
-      size_t o = ((size_t)(k / 4) * M + n) * 4 + (k % 4);
-      hi[o] = h;
-      lo[o] = l;
+bool xform_supported(int M) { return M >= 16 && M <= 512 && M % 16 == 0; }
+
+// Transform matrices from the FP64 plan.  Af (col-major, Af(n, x)) maps
+// x values to mode coefficients, Ab (col-major, Ab(x, n)) back.  The split
+// form is used when every mode is even or odd about the centre to within
+// 1e-9 of its largest entry, H of each.
+int xform_prepare(eddy_ctx *ctx, XformPlan *xp) {
+  const PoissonPlan &pp = ctx->pp;
+  const int M = pp.M, H = M / 2;
+  std::vector<double> Af((size_t)M * M), Ab((size_t)M * M), lam(M);
+  EDDY_CUDA(cudaMemcpy(Af.data(), pp.Af, sizeof(double) * Af.size(), cudaMemcpyDeviceToHost));
+  EDDY_CUDA(cudaMemcpy(Ab.data(), pp.Ab, sizeof(double) * Ab.size(), cudaMemcpyDeviceToHost));
+  EDDY_CUDA(cudaMemcpy(lam.data(), pp.lam, sizeof(double) * M, cudaMemcpyDeviceToHost));
+  auto af = [&](int n, int x) { return Af[(size_t)n + (size_t)M * x]; };
+  auto ab = [&](int x, int n) { return Ab[(size_t)x + (size_t)M * n]; };
+  std::vector<int> even, odd;
+  bool sym = (M % 32 == 0) && H <= 256;
+  for (int n = 0; n < M && sym; n++) {
+    double dot = 0., mf = 0., mb = 0.;
+    for (int x = 0; x < M; x++) {
+      dot += af(n, x) * af(n, M - 1 - x);
+      mf = std::fmax(mf, std::fabs(af(n, x)));
+      mb = std::fmax(mb, std::fabs(ab(x, n)));
     }
-  EDDY_CUDA(cudaMalloc(bhi, sizeof(float) * hi.size()));
-  EDDY_CUDA(cudaMalloc(blo, sizeof(float) * lo.size()));
-  EDDY_CUDA(cudaMemcpy(*bhi, hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice));
-  EDDY_CUDA(cudaMemcpy(*blo, lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice));
+    const double sg = dot >= 0. ? 1. : -1.;
+    for (int x = 0; x < M && sym; x++) {
+      if (std::fabs(af(n, x) - sg * af(n, M - 1 - x)) > 1e-9 * mf) sym = false;
+      if (std::fabs(ab(x, n) - sg * ab(M - 1 - x, n)) > 1e-9 * mb) sym = false;
+    }
+    (sg > 0. ? even : odd).push_back(n);
+  }
+  if (sym && ((int)even.size() != H || (int)odd.size() != H)) sym = false;
+  std::vector<float> fh, fl, bh, bl;
+  std::vector<double> lp(M);
+  int m0 = pp.m0;
+  if (sym) {
+    std::vector<int> perm(even);
+    perm.insert(perm.end(), odd.begin(), odd.end());
+    for (int m = 0; m < M; m++) {
+      lp[m] = lam[perm[m]];
+      if (perm[m] == pp.m0) m0 = m;
+    }
+    // forward: B1[m][x] = Af(even[m], x), B2[m][x] = Af(odd[m], x), x < H
+    append_block(H, [&](int m, int x) { return af(even[m], x); }, fh, fl);
+    append_block(H, [&](int m, int x) { return af(odd[m], x); }, fh, fl);
+    // backward: B1[x][m] = Ab(x, even[m]), B2[x][m] = Ab(x, odd[m]), x < H
+    append_block(H, [&](int x, int m) { return ab(x, even[m]); }, bh, bl);
+    append_block(H, [&](int x, int m) { return ab(x, odd[m]); }, bh, bl);
+  } else {
+    lp = lam;
+    append_block(M, [&](int n, int x) { return af(n, x); }, fh, fl);
+    append_block(M, [&](int x, int n) { return ab(x, n); }, bh, bl);
+  }
+  xp->sym = sym ? 1 : 0;
+  xp->m0 = m0;
+  int rc;
+  if ((rc = upload(ctx, fh, &xp->fhi)) || (rc = upload(ctx, fl, &xp->flo)) || (rc = upload(ctx, bh, &xp->bhi)) ||
+      (rc = upload(ctx, bl, &xp->blo)))
+    return rc;
+  EDDY_CUDA(cudaMalloc(&xp->lam, sizeof(double) * M));
+  EDDY_CUDA(cudaMemcpy(xp->lam, lp.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+  size_t smax = 0;
+  for (int mode = sym ? 1 : 0; mode < (sym ? 3 : 1); mode++) {
+    const size_t smem = (size_t)xform_stages(mode, M) * stage_geom(mode, M).stage + 1024;
+    smax = smem > smax ? smem : smax;
+  }
+  EDDY_CUDA(cudaFuncSetAttribute(k_xform_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
   return EDDY_OK;
 }
 
-bool xform_supported(int M) { return M >= 16 && M <= 512 && M % 16 == 0; }
-
-static int xform_stages(int M) {
-  size_t st = stage_geom(M).stage;
-  return (3 * st + 2048 <= 227 * 1024) ? 3 : 2;
+void xform_release(XformPlan *xp) {
+  float *p[] = {xp->fhi, xp->flo, xp->bhi, xp->blo};
+  for (float *q : p)
+    if (q) cudaFree(q);
+  if (xp->lam) cudaFree(xp->lam);
+  *xp = XformPlan{};
 }
 
-// out (P x M) = in (P x M) * B^T on the tensor cores
-int launch_xform(eddy_ctx *ctx, const float *in, float *out, const float *bhi, const float *blo) {
+// out (P x M) = transform of in (P x M) on the tensor cores; dir 0 forward
+// (x values -> mode coefficients), 1 backward
+int launch_xform(eddy_ctx *ctx, const XformPlan *xp, int dir, const float *in, float *out) {
   const int M = ctx->pp.M;
   const long long P = (long long)ctx->pp.L * ctx->pp.N;
   const CUtensorMap *mp = nullptr;
@@ -267,11 +467,12 @@ int launch_xform(eddy_ctx *ctx, const float *in, float *out, const float *bhi, c
     ctx->tmaps.push_back(e);
     mp = &ctx->tmaps.back().map;
   }
-  const int nst = xform_stages(M);
-  const size_t smem = (size_t)nst * stage_geom(M).stage + 1024;
-  EDDY_CUDA(cudaFuncSetAttribute(k_xform_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int mode = xp->sym ? 1 + dir : 0;
+  const int nst = xform_stages(mode, M);
+  const size_t smem = (size_t)nst * stage_geom(mode, M).stage + 1024;
   const unsigned grid = (unsigned)((P + 127) / 128);
-  k_xform_tf32<<<grid, XT, smem, ctx->stream>>>(*mp, bhi, blo, out, P, M, nst, ctx->err_flag);
+  k_xform_tf32<<<grid, XT, smem, ctx->stream>>>(*mp, dir ? xp->bhi : xp->fhi, dir ? xp->blo : xp->flo, out, P, M,
+                                                mode, nst, ctx->err_flag);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }

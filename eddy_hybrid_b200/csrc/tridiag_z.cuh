@@ -4,7 +4,9 @@
 //   an(k) x(k-1) + (bn(k) + lambda_m - AK(J)) x(k) + cn(k) x(k+1) = g(k).
 // Thomas elimination in FP64 arithmetic; the right-hand side and solution are
 // stored as G (double for the plain form, float for the mixed form's
-// correction solves), the eliminated right-hand side dd in FP64.
+// correction solves); the eliminated coefficients c' and right-hand side dd
+// as C (FP64 in the plain form; FP32 in the mixed form, whose solves feed an
+// FP64-residual refinement and need only FP32 accuracy).
 // The singular line (J = 0, m = m0, the constant x mode) is made compatible by
 // removing its z-volume-weighted mean (computed by k_line_mean) and pinned by
 // dropping its first equation; its first entry is set to zero.
@@ -38,11 +40,11 @@ __global__ void k_line_mean(int M, int L, int N, int m0, const double *__restric
   if (threadIdx.x == 0) out[0] = s1[0] / s2[0];
 }
 
-template <class G>
+template <class G, class C = double>
 __global__ void __launch_bounds__(128)
     k_tridiag_lines(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
                     const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
-                    const double *__restrict__ cmean, G *g, double *__restrict__ cpr, double *dd) {
+                    const double *__restrict__ cmean, G *g, C *__restrict__ cpr, C *dd) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)M * L) return;
   const int mi = (int)(t % M), J = (int)(t / M);
@@ -64,8 +66,8 @@ __global__ void __launch_bounds__(128)
         const double rden = 1.0 / ((bn[k] + shift) - a * pc);
         const double c = cn[k] * rden;
         const double e = ((fv[q] - cm) - a * pd) * rden;
-        cpr[t + ML * k] = c;
-        dd[t + ML * k] = e;
+        cpr[t + ML * k] = (C)c;
+        dd[t + ML * k] = (C)e;
         pc = c;
         pd = e;
       }
@@ -78,8 +80,8 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
     for (int q = 0; q < ZC; q++) {
       const int k = k1 - q;
-      cv[q] = k >= s0 ? cpr[t + ML * k] : 0.;
-      ev[q] = k >= s0 ? dd[t + ML * k] : 0.;
+      cv[q] = k >= s0 ? (double)cpr[t + ML * k] : 0.;
+      ev[q] = k >= s0 ? (double)dd[t + ML * k] : 0.;
     }
 #pragma unroll
     for (int q = 0; q < ZC; q++) {

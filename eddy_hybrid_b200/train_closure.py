@@ -90,19 +90,17 @@ def train(solver, X, T, epochs=8, batch=8192, lr=2e-3, seed=1, log=print):
 def evaluate(meta, theta, X, T):
     """Held-out relative nu_t error of the network (FP32 numpy forward of the
     BF16 weights) and of the best constant coefficient fitted on the same set."""
-    import sys
-    sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
     P = cl.unpack(theta)
     Z = (X - meta[:cl.NFEAT]) * meta[cl.NFEAT:2 * cl.NFEAT]
     h = Z.astype(np.float64)
 
-    def silu(x):
-        return x / (1.0 + np.exp(-x))
+    def act(x):  # hard-swish
+        return x * np.clip(x / 6.0 + 0.5, 0.0, 1.0)
     pad = np.zeros((len(h), cl.KIN))
     pad[:, :cl.NFEAT] = h
-    a = silu(pad @ P["W1"].T.astype(np.float64) + P["b1"])
-    a = silu(a @ P["W2"].T.astype(np.float64) + P["b2"])
-    a = silu(a @ P["W3"].T.astype(np.float64) + P["b3"])
+    a = act(pad @ P["W1"].T.astype(np.float64) + P["b1"])
+    a = act(a @ P["W2"].T.astype(np.float64) + P["b2"])
+    a = act(a @ P["W3"].T.astype(np.float64) + P["b3"])
     o = a @ P["W4"].T.astype(np.float64) + P["b4"]
     nu = np.logaddexp(0.0, o[:, 0]) * meta[4 * cl.NFEAT] * smag_scale(X)
     outside = ((Z < meta[2 * cl.NFEAT:3 * cl.NFEAT]) | (Z > meta[3 * cl.NFEAT:4 * cl.NFEAT])).any(axis=1)

@@ -17,8 +17,16 @@ def bf16(x):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def silu(z):
-    return z / (1.0 + np.exp(-z))
+def hswish(z):
+    """Hidden activation: hard-swish z * clip(z/6 + 1/2, 0, 1) (the device
+    computes it in FP32 as z * sat(fma(z, 1/6, 1/2)))."""
+    z32 = np.asarray(z, dtype=np.float32)
+    t = np.clip(z32 * np.float32(1.0 / 6.0) + np.float32(0.5), 0.0, 1.0)
+    return (z32 * t).astype(np.float64)
+
+
+def hswish_grad(z):
+    return np.where(z <= -3.0, 0.0, np.where(z >= 3.0, 1.0, z / 3.0 + 0.5))
 
 
 def sigm(z):
@@ -40,11 +48,11 @@ def forward(P, X):
     W = {k: bf16(P[k]) for k in ("W1", "W2", "W3", "W4")}
     b = {k: P[k].astype(np.float64) for k in ("b1", "b2", "b3", "b4")}
     Z1 = X @ W["W1"].T + b["b1"]
-    A1 = bf16(silu(Z1).astype(np.float32))
+    A1 = bf16(hswish(Z1).astype(np.float32))
     Z2 = A1 @ W["W2"].T + b["b2"]
-    A2 = bf16(silu(Z2).astype(np.float32))
+    A2 = bf16(hswish(Z2).astype(np.float32))
     Z3 = A2 @ W["W3"].T + b["b3"]
-    A3 = bf16(silu(Z3).astype(np.float32))
+    A3 = bf16(hswish(Z3).astype(np.float32))
     Z4 = A3 @ W["W4"].T + b["b4"]
     return dict(X=X, W=W, Z1=Z1, A1=A1, Z2=Z2, A2=A2, Z3=Z3, A3=A3, Z4=Z4, out=softplus(Z4[:, :2]))
 
@@ -62,8 +70,7 @@ def backward(c, Y):
     dA = dZ4b @ c["W"]["W4"]
     for l, Aprev in ((3, c["A2"]), (2, c["A1"]), (1, c["X"])):
         z = c[f"Z{l}"]
-        s = sigm(z)
-        dZ = dA * (s * (1 + z * (1 - s)))
+        dZ = dA * hswish_grad(z)
         g[f"b{l}"] = dZ.sum(0)
         dZb = bf16(dZ.astype(np.float32))
         g[f"W{l}"] = dZb.T @ Aprev
