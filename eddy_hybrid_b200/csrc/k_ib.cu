@@ -620,6 +620,179 @@ __device__ int knn_warp(const Bins &b, const int *bstart, const int *bitems, con
   return got;
 }
 
+// Exact k nearest centroids by (d2, index), one warp, selection instead of
+// per-lane insertion lists: the candidate indices of the (2R+1)^3 bin cube
+// are written to shared memory, a 64-bucket histogram of d2 over
+// [0, 3 ((R+1) h)^2] (every candidate of the cube is closer than that) finds
+// the bucket holding the k-th smallest, every candidate at or below that
+// bucket (a superset of the k nearest, as the bucket index is monotone in d2)
+// is sorted by a warp bitonic network, and the cube is accepted once the k-th
+// distance is inside it (d_k < (R h)^2) or it spans the whole bin grid.
+// Returns the number found, or -1 when the candidates overflow the buffers
+// (the caller then uses knn_warp).
+constexpr int KCAP = 2048, KSEL = 128, NHB = 64;
+struct KnnSmem {
+  int id[KCAP];
+  double sd[KSEL];
+  int sid[KSEL];
+  int hist[NHB];
+  int nsel;
+};
+
+__device__ __forceinline__ bool key_less(double da, int ia, double db, int ib) {
+  return da < db || (da == db && ia < ib);
+}
+
+__device__ __forceinline__ double cdist2(const double *c, int tt, const double *q) {
+  const double *p = c + 3 * tt;
+  const double ex = p[0] - q[0], ey = p[1] - q[1], ez = p[2] - q[2];
+  return ex * ex + ey * ey + ez * ez;
+}
+
+__device__ int knn_warp2(const Bins &b, const int *bstart, const int *bitems, const double *c, const double *q,
+                         int kk, int *out, KnnSmem &S) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int cx = bin3_of(b, q, 0), cy = bin3_of(b, q, 1), cz = bin3_of(b, q, 2);
+  const double h = fmin(fmin(1.0 / b.inv[0], 1.0 / b.inv[1]), 1.0 / b.inv[2]);
+  const double hmax = fmax(fmax(1.0 / b.inv[0], 1.0 / b.inv[1]), 1.0 / b.inv[2]);
+  const int rmax = max(max(b.nb[0], b.nb[1]), b.nb[2]);
+  for (int R = 1; R <= rmax; R++) {
+    const int side = 2 * R + 1, nbins = side * side * side;
+    auto bin_at = [&](int bb) {
+      const int x = cx + bb % side - R, y = cy + (bb / side) % side - R, z = cz + bb / (side * side) - R;
+      if (x < 0 || y < 0 || z < 0 || x >= b.nb[0] || y >= b.nb[1] || z >= b.nb[2]) return -1;
+      return x + b.nb[0] * (y + b.nb[1] * z);
+    };
+    int cnt = 0;
+    for (int bb = lane; bb < nbins; bb += 32) {
+      const int bin = bin_at(bb);
+      if (bin >= 0) cnt += bstart[bin + 1] - bstart[bin];
+    }
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int C = __shfl_sync(FULL, incl, 31);
+    if (C > KCAP) return -1;
+    if (C < kk && R < rmax) continue;
+    int off = incl - cnt;
+    for (int bb = lane; bb < nbins; bb += 32) {
+      const int bin = bin_at(bb);
+      if (bin < 0) continue;
+      for (int t = bstart[bin]; t < bstart[bin + 1]; t++) S.id[off++] = bitems[t];
+    }
+    const int K = min(kk, C);
+    S.hist[lane] = 0;
+    S.hist[lane + 32] = 0;
+    __syncwarp();
+    // bucket index: monotone non-decreasing in d2, clamped to the last bucket
+    const double span = (double)(R + 1) * hmax;
+    const double scale = (double)NHB / (3.0 * span * span);
+    auto bucket = [&](double d2) { return min(NHB - 1, (int)(d2 * scale)); };
+    for (int e = lane; e < C; e += 32) atomicAdd(&S.hist[bucket(cdist2(c, S.id[e], q))], 1);
+    __syncwarp();
+    // smallest bucket whose cumulative count reaches K (lane owns 2 buckets)
+    const int h0 = S.hist[2 * lane], h1 = S.hist[2 * lane + 1];
+    int cum = h0 + h1;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, cum, o);
+      if (lane >= o) cum += y;
+    }
+    const int before = cum - h0 - h1;
+    const int bl = before + h0 >= K ? 2 * lane : 2 * lane + 1;
+    const bool mine = K > 0 && before < K && cum >= K;
+    const unsigned who = __ballot_sync(FULL, mine);
+    const int bstar = who ? __shfl_sync(FULL, bl, __ffs(who) - 1) : NHB - 1;
+    // gather the candidates at or below bstar
+    int nsel = 0;
+    for (int e0 = 0; e0 < C; e0 += 32) {
+      const int e = e0 + lane;
+      double d2 = 0.;
+      int tt = 0;
+      bool sel = false;
+      if (e < C) {
+        tt = S.id[e];
+        d2 = cdist2(c, tt, q);
+        sel = bucket(d2) <= bstar;
+      }
+      const unsigned m = __ballot_sync(FULL, sel);
+      const int pos = nsel + __popc(m & ((1u << lane) - 1u));
+      if (sel && pos < KSEL) {
+        S.sd[pos] = d2;
+        S.sid[pos] = tt;
+      }
+      nsel += __popc(m);
+    }
+    __syncwarp();
+    if (nsel > KSEL) return -1;
+    // warp bitonic sort of up to 128 slots (4 per lane, slot = r * 32 + lane)
+    double kd[4];
+    int ki[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int e = r * 32 + lane;
+      kd[r] = e < nsel ? S.sd[e] : 1e300;
+      ki[r] = e < nsel ? S.sid[e] : 0x7fffffff;
+    }
+    const int nsort = nsel <= 32 ? 32 : (nsel <= 64 ? 64 : 128);
+    for (int k2 = 2; k2 <= nsort; k2 <<= 1) {
+      for (int j = k2 >> 1; j > 0; j >>= 1) {
+        if (j >= 32) {
+          const int rj = j >> 5;
+#pragma unroll
+          for (int r = 0; r < 4; r++) {
+            const int pr = r ^ rj;
+            if (pr > r && r * 32 < nsort) {
+              const int e = r * 32 + lane;
+              const bool up = (e & k2) == 0;
+              const bool sw = up ? key_less(kd[pr], ki[pr], kd[r], ki[r]) : key_less(kd[r], ki[r], kd[pr], ki[pr]);
+              if (sw) {
+                const double td = kd[r]; kd[r] = kd[pr]; kd[pr] = td;
+                const int ti = ki[r]; ki[r] = ki[pr]; ki[pr] = ti;
+              }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < 4; r++) {
+            if (r * 32 < nsort) {
+              const int e = r * 32 + lane;
+              const double od = __shfl_xor_sync(FULL, kd[r], j);
+              const int oi = __shfl_xor_sync(FULL, ki[r], j);
+              const bool up = (e & k2) == 0, lower = (lane & j) == 0;
+              // the lower slot keeps the smaller key when ascending
+              const bool take_other = (lower == up) ? key_less(od, oi, kd[r], ki[r]) : key_less(kd[r], ki[r], od, oi);
+              if (take_other) {
+                kd[r] = od;
+                ki[r] = oi;
+              }
+            }
+          }
+        }
+      }
+    }
+    // k-th distance: slot K-1
+    double dk = 0.;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const double v = __shfl_sync(FULL, kd[r], (K - 1) & 31);
+      if (K > 0 && r == (K - 1) >> 5) dk = v;
+    }
+    const double lim = (double)R * h;
+    if (C >= kk && !(dk < lim * lim) && R < rmax) continue;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int e = r * 32 + lane;
+      if (e < kk) out[e] = e < K ? ki[r] : -1;
+    }
+    __syncwarp();
+    return K;
+  }
+  return -1;
+}
+
 __constant__ int c_gind[26][3] = {
     {1, 0, 0},  {-1, 0, 0}, {0, 0, 1},   {0, 0, -1},  {1, 0, 1},   {1, 0, -1},  {-1, 0, 1},
     {-1, 0, -1}, {0, 1, 0},  {0, -1, 0},  {1, 1, 0},   {-1, 1, 0},  {0, 1, 1},   {0, 1, -1},
@@ -805,6 +978,7 @@ __global__ void __launch_bounds__(GW * 32)
     k_geom_first(Dims d, Axes ax, int n, const int *ijk, const double *v, const double *c, const double *nrm, Bins b,
                  const int *bstart, const int *bitems, const signed char *fw, int *status, double *xn, int *dd) {
   __shared__ int inn_s[GW][NNTR3D];
+  __shared__ KnnSmem ks[GW];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.x * GW + w;
   if (p >= n) return;  // whole warp
@@ -812,7 +986,8 @@ __global__ void __launch_bounds__(GW * 32)
   const double qv[3] = {ax.x[im], ax.y[jm], ax.z[km]};
   // the exact nearest-centroid list is sorted, so the 3- and 5-lists are its
   // prefixes; grid_intr_warp evaluates the three lengths in one scan
-  knn_warp(b, bstart, bitems, c, qv, NNTR3D, inn_s[w]);
+  if (knn_warp2(b, bstart, bitems, c, qv, NNTR3D, inn_s[w], ks[w]) < 0)
+    knn_warp(b, bstart, bitems, c, qv, NNTR3D, inn_s[w]);
   const int gi = grid_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn_s[w], NNTR3D, xn + 3 * p, dd + 3 * p);
   __syncwarp();
   if (lane == 0) status[p] = gi == 1 ? 1 : (gi == -1 ? -2 : 0);

@@ -90,52 +90,77 @@ struct MomAcc32 {
   __device__ __forceinline__ float t(int di, int dj, int dk) const { return r.at(3, di, dj, dk); }
 };
 
+// metric values around one (i, j) column and one k plane, in registers: the
+// stencil templates read m.xx[i + o], m.xx[j + o], m.xx[k + o] with o in
+// {-1, 0, 1}, which fold to one of the three fields after inlining
+struct Reg3 {
+  float lo, mid, hi;
+  int base;
+  __device__ __forceinline__ float operator[](int idx) const {
+    const int o = idx - base;
+    return o < 0 ? lo : (o == 0 ? mid : hi);
+  }
+};
+
+__device__ __forceinline__ Reg3 reg3(const float *a, int c) { return Reg3{a[c - 1], a[c], a[c + 1], c}; }
+
+struct MetricCol32 {
+  Reg3 ap, au, av, aw, bp, bu, bv, bw, cp, cu, cv, cw;
+};
+
 __global__ void __launch_bounds__(TX *TY)
     k_rhs32(Dims d, DevMetrics32 m, Scalars s, int px, const __grid_constant__ TmaMaps<NFLD> maps,
             float *__restrict__ us, float *__restrict__ vs, float *__restrict__ ws, float *__restrict__ ua,
             float *__restrict__ va, float *__restrict__ wa, float alfxdt, float gamxdt, float rhoxdt, int *err) {
   const float ru1 = (float)s.ru1, grav = (float)s.grav;
   const float dpdx = (float)s.dpdx, dpdy = (float)s.dpdy, dpdz = (float)s.dpdz;
+  // this thread's column (the mapping of tma_march), clamped for idle threads
+  const int ic = min(d.ix1 + (int)(blockIdx.x * TX + threadIdx.x), d.ix2);
+  const int jc = min(d.jy1 + (int)(blockIdx.y * TY + threadIdx.y), d.jy2);
+  MetricCol32 mc;
+  mc.ap = reg3(m.ap, ic); mc.au = reg3(m.au, ic); mc.av = reg3(m.av, ic); mc.aw = reg3(m.aw, ic);
+  mc.bp = reg3(m.bp, jc); mc.bu = reg3(m.bu, jc); mc.bv = reg3(m.bv, jc); mc.bw = reg3(m.bw, jc);
+  const float dfxu_i = m.dfxu[ic], dfxw_i = m.dfxw[ic];
+  const float bg1 = m.dens_bg[ic + d.nx * (jc - 1)], bg0 = m.dens_bg[(ic - 1) + d.nx * (jc - 1)];
   tma_march<NFLD, TX, TY, KCHUNK, float>(
       d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err, [&](int i, int j, int k, bool active, const Acc9 &R) {
         if (!active) return;
+        mc.cp = reg3(m.cp, k); mc.cu = reg3(m.cu, k); mc.cv = reg3(m.cv, k); mc.cw = reg3(m.cw, k);
         MomAcc32 S{R};
         long long q = pidx(d, px, i, j, k);
         const bool jin = j >= d.jy1 && j <= d.jy2;
         const bool kin = (k >= d.kz1 && k <= d.kz2);
         float uval = 0.f;
         if (kin && jin && i >= d.ibu && i <= d.ieu) {
-          float ur = rhs_u<float>(S, m, ru1, i, j, k);
+          float ur = rhs_u<float>(S, mc, ru1, i, j, k);
           float ustar = R.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * R.at(6, 0, 0, 0) -
-                        alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) - alfxdt * dpdx;
+                        alfxdt * mc.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) - alfxdt * dpdx;
           if (s.idens == 1)
-            ustar = ustar - alfxdt * 0.5f * grav *
-                                ((R.at(5, 1, 0, 0) - m.dens_bg[i + d.nx * (j - 1)]) +
-                                 (R.at(5, 0, 0, 0) - m.dens_bg[(i - 1) + d.nx * (j - 1)]));
+            ustar = ustar - alfxdt * 0.5f * grav * ((R.at(5, 1, 0, 0) - bg1) + (R.at(5, 0, 0, 0) - bg0));
           ua[q] = ur;
-          if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0.f - ustar) * alfxdt;
+          if (i >= d.ieu - s.vspngx1) ustar = ustar + dfxu_i * (0.f - ustar) * alfxdt;
           if (s.ivspngl == 1) ustar = ustar + m.dfxul[k] * (0.f - ustar) * alfxdt;
           uval = ustar;
         }
         us[q] = uval;
         float vval = 0.f;
         if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
-          float vr = rhs_v<float>(S, m, ru1, i, j, k);
+          float vr = rhs_v<float>(S, mc, ru1, i, j, k);
           float vstar = R.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * R.at(7, 0, 0, 0) -
-                        alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) - alfxdt * dpdy;
+                        alfxdt * mc.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) - alfxdt * dpdy;
           va[q] = vr;
-          if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0.f - vstar) * alfxdt;
+          if (i >= d.ix2 - s.vspngx1) vstar = vstar + dfxw_i * (0.f - vstar) * alfxdt;
           if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin) vstar = vstar + m.dfxwl[k] * (0.f - vstar) * alfxdt;
           vval = vstar;
         }
         vs[q] = vval;
         float wval = 0.f;
         if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
-          float wr = rhs_w<float>(S, m, ru1, i, j, k);
+          float wr = rhs_w<float>(S, mc, ru1, i, j, k);
           float wstar = R.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * R.at(8, 0, 0, 0) -
-                        alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) - alfxdt * dpdz;
+                        alfxdt * mc.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) - alfxdt * dpdz;
           wa[q] = wr;
-          if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1.f - wstar) * alfxdt;
+          if (i >= d.ix2 - s.vspngx1) wstar = wstar + dfxw_i * (1.f - wstar) * alfxdt;
           if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1.f - wstar) * alfxdt;
           wval = wstar;
         }
@@ -520,13 +545,15 @@ __global__ void k_sync_planes(Dims d, int px, const double *__restrict__ u, cons
 }
 
 // pressure update (src/Eddy6.f:2772-2806, 2911-2953) in FP64, FP32 copy alongside
+// reference pressure: mean of p + dp over the row (ix1, :, 2); one warp
 __global__ void k_pref_m(Dims d, const double *p, const double *dp, double *out) {
   double s = 0.;
-  for (int j = d.jy1; j <= d.jy2; j++) {
+  for (int j = d.jy1 + (int)threadIdx.x; j <= d.jy2; j += 32) {
     long long q = fidx(d, d.ix1, j, 2);
     s += p[q] + dp[q];
   }
-  out[0] = s / (double)(d.ny - 2);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) out[0] = s / (double)(d.ny - 2);
 }
 
 __global__ void __launch_bounds__(256)
@@ -1036,7 +1063,7 @@ int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   }
   {
     ProfScope ps(ctx, PROF_PUPDATE);
-    k_pref_m<<<1, 1, 0, ctx->stream>>>(d, f[EDDY_P], f[EDDY_DP], ctx->scal);
+    k_pref_m<<<1, 32, 0, ctx->stream>>>(d, f[EDDY_P], f[EDDY_DP], ctx->scal);
     EDDY_LAUNCHED(ctx);
     k_pupdate_m<<<nblk(d.ncell), 256, 0, ctx->stream>>>(d, px, f[EDDY_P], f[EDDY_DP], ctx->scal, x->p);
     EDDY_LAUNCHED(ctx);

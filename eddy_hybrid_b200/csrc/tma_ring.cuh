@@ -138,8 +138,9 @@ __device__ __forceinline__ void tma_march(int ix1, int ix2, int jy1, int jy2, in
   const bool active = (i <= ix2 && j <= jy2);
   const int c = (ty + 1) * G::PX + (tx + 1);
   for (int k = k0; k < k1; k++) {
+    // planes k-1 and k were waited for in earlier iterations
     bool ok = true;
-    for (int p = k - 1; p <= k + 1; p++) {
+    for (int p = k == k0 ? k - 1 : k + 1; p <= k + 1; p++) {
       int u = p - pfirst;
       ok = ok && tma::mbar_wait(&bar[u & (NSLOT - 1)], (u >> 2) & 1);
     }

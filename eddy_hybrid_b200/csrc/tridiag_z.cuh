@@ -10,11 +10,10 @@
 // The singular line (J = 0, m = m0, the constant x mode) is made compatible by
 // removing its z-volume-weighted mean (computed by k_line_mean) and pinned by
 // dropping its first equation; its first entry is set to zero.
-// dd may alias g (plain form: in place).  Loads are issued in chunks of ZC planes ahead of the recurrence so each
-// thread keeps several memory requests in flight.
+// dd may alias g (plain form: in place).  Loads are issued in chunks of ZC
+// planes ahead of the recurrence so each thread keeps several memory
+// requests in flight.
 #pragma once
-
-constexpr int ZC = 8;
 
 // weighted mean of the singular line: out = sum_k g(m0,0,k) wz(k) / sum_k wz(k)
 template <class G>
@@ -40,7 +39,7 @@ __global__ void k_line_mean(int M, int L, int N, int m0, const double *__restric
   if (threadIdx.x == 0) out[0] = s1[0] / s2[0];
 }
 
-template <class G, class C = double>
+template <class G, class C = double, int ZC = 8>
 __global__ void __launch_bounds__(128)
     k_tridiag_lines(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
                     const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
@@ -54,10 +53,14 @@ __global__ void __launch_bounds__(128)
   const double shift = lam[mi] - ak[J];
   const double cm = pin ? cmean[0] : 0.;
   double pc = 0., pd = 0.;
-  for (int k0 = s0; k0 < N; k0 += ZC) {
-    double fv[ZC];
+  // forward elimination; the loads of the next chunk are issued before the
+  // recurrence over the current one (two register buffers)
+  G fa[ZC], fb[ZC];
+  auto load_f = [&](G (&f)[ZC], int k0) {
 #pragma unroll
-    for (int q = 0; q < ZC; q++) fv[q] = (k0 + q < N) ? (double)g[t + ML * (k0 + q)] : 0.;
+    for (int q = 0; q < ZC; q++) f[q] = (k0 + q < N) ? g[t + ML * (k0 + q)] : G(0);
+  };
+  auto elim = [&](const G (&f)[ZC], int k0) {
 #pragma unroll
     for (int q = 0; q < ZC; q++) {
       const int k = k0 + q;
@@ -65,31 +68,52 @@ __global__ void __launch_bounds__(128)
         const double a = (k == s0) ? 0. : an[k];
         const double rden = 1.0 / ((bn[k] + shift) - a * pc);
         const double c = cn[k] * rden;
-        const double e = ((fv[q] - cm) - a * pd) * rden;
+        const double e = (((double)f[q] - cm) - a * pd) * rden;
         cpr[t + ML * k] = (C)c;
         dd[t + ML * k] = (C)e;
         pc = c;
         pd = e;
       }
     }
+  };
+  load_f(fa, s0);
+  for (int k0 = s0; k0 < N; k0 += 2 * ZC) {
+    if (k0 + ZC < N) load_f(fb, k0 + ZC);
+    elim(fa, k0);
+    if (k0 + ZC < N) {
+      if (k0 + 2 * ZC < N) load_f(fa, k0 + 2 * ZC);
+      elim(fb, k0 + ZC);
+    }
   }
+  // back substitution, same double buffering (chunk k1, k1-1, ..., k1-ZC+1)
   double x = pd;
   g[t + ML * (N - 1)] = (G)x;
-  for (int k1 = N - 2; k1 >= s0; k1 -= ZC) {
-    double cv[ZC], ev[ZC];
+  C ca[ZC], ea[ZC], cb[ZC], eb[ZC];
+  auto load_b = [&](C (&cv)[ZC], C (&ev)[ZC], int k1) {
 #pragma unroll
     for (int q = 0; q < ZC; q++) {
       const int k = k1 - q;
-      cv[q] = k >= s0 ? (double)cpr[t + ML * k] : 0.;
-      ev[q] = k >= s0 ? (double)dd[t + ML * k] : 0.;
+      cv[q] = k >= s0 ? cpr[t + ML * k] : C(0);
+      ev[q] = k >= s0 ? dd[t + ML * k] : C(0);
     }
+  };
+  auto subst = [&](const C (&cv)[ZC], const C (&ev)[ZC], int k1) {
 #pragma unroll
     for (int q = 0; q < ZC; q++) {
       const int k = k1 - q;
       if (k >= s0) {
-        x = ev[q] - cv[q] * x;
+        x = (double)ev[q] - (double)cv[q] * x;
         g[t + ML * k] = (G)x;
       }
+    }
+  };
+  if (N - 2 >= s0) load_b(ca, ea, N - 2);
+  for (int k1 = N - 2; k1 >= s0; k1 -= 2 * ZC) {
+    if (k1 - ZC >= s0) load_b(cb, eb, k1 - ZC);
+    subst(ca, ea, k1);
+    if (k1 - ZC >= s0) {
+      if (k1 - 2 * ZC >= s0) load_b(ca, ea, k1 - 2 * ZC);
+      subst(cb, eb, k1 - ZC);
     }
   }
   if (pin) g[t] = (G)0.;
