@@ -28,22 +28,27 @@ __global__ void k_fill_plane(Dims d, int pitch, T *a, int axis, int dst, int src
   a[qd] = zero ? T(0) : sgn * a[qs];
 }
 
-// flux through the z plane k: sum over interior (i,j) of a/(ap bp), FP64
+// flux through the z plane k: sum over interior (i,j) of a/(ap bp) and of
+// the areas, FP64; FLUXB blocks write partial sums, one warp adds them in a
+// fixed order (deterministic)
+constexpr int FLUXB = 148, FLUXT = 256;
+
 template <class T>
-__global__ void k_plane_flux(Dims d, int pitch, DevMetrics m, const T *a, int k, double *out) {
-  __shared__ double sf[1024], sa[1024];
-  int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
+__global__ void __launch_bounds__(FLUXT)
+    k_plane_flux_part(Dims d, int pitch, DevMetrics m, const T *a, int k, double *part) {
+  __shared__ double sf[FLUXT], sa[FLUXT];
+  const int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1;
   double f = 0., ar = 0.;
-  for (int t = threadIdx.x; t < mi * mj; t += blockDim.x) {
-    int i = d.ix1 + t % mi, j = d.jy1 + t / mi;
-    double areaij = 1.0 / (m.ap[i] * m.bp[j]);
+  for (int t = blockIdx.x * FLUXT + threadIdx.x; t < mi * mj; t += gridDim.x * FLUXT) {
+    const int i = d.ix1 + t % mi, j = d.jy1 + t / mi;
+    const double areaij = 1.0 / (m.ap[i] * m.bp[j]);
     f = f + (double)a[pidx(d, pitch, i, j, k)] * areaij;
     ar = ar + areaij;
   }
   sf[threadIdx.x] = f;
   sa[threadIdx.x] = ar;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+  for (int w = FLUXT / 2; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w) {
       sf[threadIdx.x] += sf[threadIdx.x + w];
       sa[threadIdx.x] += sa[threadIdx.x + w];
@@ -51,8 +56,24 @@ __global__ void k_plane_flux(Dims d, int pitch, DevMetrics m, const T *a, int k,
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    out[0] = sf[0];
-    out[1] = sa[0];
+    part[2 * blockIdx.x] = sf[0];
+    part[2 * blockIdx.x + 1] = sa[0];
+  }
+}
+
+__global__ void k_plane_flux_final(const double *part, double *out) {
+  double f = 0., ar = 0.;
+  for (int b = threadIdx.x; b < FLUXB; b += 32) {
+    f += part[2 * b];
+    ar += part[2 * b + 1];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    f += __shfl_xor_sync(0xffffffffu, f, o);
+    ar += __shfl_xor_sync(0xffffffffu, ar, o);
+  }
+  if (threadIdx.x == 0) {
+    out[0] = f;
+    out[1] = ar;
   }
 }
 
@@ -153,6 +174,18 @@ int bc_fill(eddy_ctx *ctx, int pitch, T *a, int axis, int dst, int src, double s
   return EDDY_OK;
 }
 
+// plane flux (out[0] flux, out[1] area) of the z plane k of `a`; partial
+// sums in ctx->scal + 32
+template <class T>
+int plane_flux(eddy_ctx *ctx, int pitch, const T *a, int k, double *out) {
+  double *part = ctx->scal + 32;
+  bct::k_plane_flux_part<T><<<bct::FLUXB, bct::FLUXT, 0, ctx->stream>>>(ctx->d, pitch, ctx->m, a, k, part);
+  EDDY_LAUNCHED(ctx);
+  bct::k_plane_flux_final<<<1, 32, 0, ctx->stream>>>(part, out);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
 // BOUNDARY (src/boundary.f:7-66): wall types first, then periodic x/y.
 template <class T>
 int bc_boundary(eddy_ctx *ctx, int pitch, T *u, T *v, T *w) {
@@ -221,15 +254,13 @@ int bc_boundinout(eddy_ctx *ctx, int pitch, int opitch, T *ubc, T *vbc, T *wbc, 
       ctx->err = "predictor outlet: source and target pitches differ";
       return EDDY_EINVAL;
     }
-    bct::k_plane_flux<T><<<1, 1024, 0, st>>>(d, pitch, ctx->m, wbc, 1, fin);
-    EDDY_LAUNCHED(ctx);
+    if (int rc = plane_flux<T>(ctx, pitch, wbc, 1, fin)) return rc;
     bct::k_outlet_convective<T, TO><<<(nin + 255) / 256, 256, 0, st>>>(d, pitch, ctx->m, ubc, vbc, wbc, uof, vof,
                                                                         wof, fin, alfxdt);
     EDDY_LAUNCHED(ctx);
     bct::k_yper3<T><<<(d.nx * d.nz + 255) / 256, 256, 0, st>>>(d, pitch, ubc, vbc, wbc);
     EDDY_LAUNCHED(ctx);
-    bct::k_plane_flux<T><<<1, 1024, 0, st>>>(d, pitch, ctx->m, wbc, d.kz2, fout);
-    EDDY_LAUNCHED(ctx);
+    if (int rc = plane_flux<T>(ctx, pitch, wbc, d.kz2, fout)) return rc;
     bct::k_outlet_rescale<T><<<(nin + 255) / 256, 256, 0, st>>>(d, pitch, wbc, fin, fout);
     EDDY_LAUNCHED(ctx);
   } else {

@@ -236,6 +236,10 @@ void free_all(eddy_ctx *ctx) {
   for (ProfEvent &e : ctx->prof_ev) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (ProfEvent &e : ctx->prof_pool) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   if (ctx->blas) cublasDestroy(ctx->blas);
+  if (ctx->ib_stream) cudaStreamSynchronize(ctx->ib_stream);
+  for (cudaEvent_t e : ctx->ib_ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->ib_stream) cudaStreamDestroy(ctx->ib_stream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
 }
 
@@ -285,7 +289,7 @@ int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int n
   return r == CUDA_SUCCESS ? 0 : (int)r;
 }
 
-int make_tensor_map_2d(CUtensorMap *map, const void *base, long long w, long long h, int bx, int by) {
+int make_tensor_map_2d(CUtensorMap *map, const void *base, long long w, long long h, int bx, int by, int swizzle32) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return -1;
   cuuint64_t gdim[2] = {(cuuint64_t)w, (cuuint64_t)h};
@@ -293,8 +297,8 @@ int make_tensor_map_2d(CUtensorMap *map, const void *base, long long w, long lon
   cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
   cuuint32_t est[2] = {1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), gdim, gstr, box, est,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? 0 : (int)r;
 }
 
@@ -345,7 +349,10 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   if (p.closure != 0 && p.closure != 1) return fail(EDDY_EINVAL, "closure must be 0 (dynamic) or 1 (learned)");
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->ib_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ib_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ib_ev[1], cudaEventDisableTiming) != cudaSuccess)
     return fail(EDDY_ECUDA, "cudaStreamCreate failed");
   if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(EDDY_ECUDA, "cublasCreate failed");
   cublasSetStream(ctx->blas, ctx->stream);
@@ -371,8 +378,9 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
     return fail(EDDY_ENOMEM, "device allocation failed");
   cudaMemset(ctx->ilm2, 0, n2xz);
   cudaMemset(ctx->imm2, 0, n2xz);
-  if (cudaMalloc(&ctx->scal, sizeof(double) * 32) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
-  cudaMemset(ctx->scal, 0, sizeof(double) * 32);
+  // scalars [0, 32) and the plane-flux partial sums [32, 32 + 2 * 148)
+  if (cudaMalloc(&ctx->scal, sizeof(double) * 640) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
+  cudaMemset(ctx->scal, 0, sizeof(double) * 640);
   if (cudaMalloc(&ctx->err_flag, sizeof(int)) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
   cudaMemset(ctx->err_flag, 0, sizeof(int));
   rc = poisson_plan_create(ctx);
@@ -616,11 +624,17 @@ int eddy_substep(eddy_ctx *ctx, int is, double dt) {
   double alfxdt = alf[is] * dt, gamxdt = gam[is] * dt, rhoxdt = rho[is] * dt;
   int rc;
   // moving body: RBM, then new tags and stencils (src/Eddy6.f:2163-2380), every
-  // substep over alfxdt, or at the first substep over the whole step
+  // substep over alfxdt, or at the first substep over the whole step.  They
+  // run on the second stream while the predictor runs on the main stream
+  // (the predictor does not read the body's data; the forcing after it waits)
   if (ctx->ib && (ib_every_substep(ctx) || is == 0)) {
-    ProfScope ps(ctx, PROF_IB_REGEN);
-    if ((rc = ib_move(ctx, ib_every_substep(ctx) ? alfxdt : dt))) return rc;
-    if ((rc = ib_regen(ctx))) return rc;
+    if (is == 0 && ctx->ib_prefetched) {
+      ctx->ib_prefetched = 0;  // queued at the end of the previous step (eddy_step)
+    } else {
+      ib_join(ctx);
+      EDDY_CUDA(cudaEventRecord(ctx->ib_ev[0], ctx->stream));
+      ctx->ib_move_dt = ib_every_substep(ctx) ? alfxdt : dt;
+    }
   }
   if (ctx->mixed) return mixed_substep(ctx, alfxdt, gamxdt, rhoxdt);
   double **f = ctx->f;
@@ -628,6 +642,7 @@ int eddy_substep(eddy_ctx *ctx, int is, double dt) {
     ProfScope ps(ctx, PROF_RHS_PRED);
     if ((rc = launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt))) return rc;
   }
+  if ((rc = ib_overlap_regen(ctx))) return rc;
   // momforc_mod2 + velinterior (src/Eddy6.f:2526-2575)
   if (ctx->ib) {
     ProfScope ps(ctx, PROF_IB_FORCE);
@@ -676,6 +691,15 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
       int rc = eddy_substep(ctx, is, dt);
       if (rc) return rc;
     }
+    // within one call the next step's move (same dt) and regeneration run on
+    // the second stream during this step's eddy viscosity; they only need
+    // this step's forcing to be done (the event), and tvinterior below keeps
+    // reading the current tv flag (double-buffered)
+    const bool prefetch = ctx->ib && !ib_every_substep(ctx) && n + 1 < nsteps;
+    if (prefetch) {
+      ib_join(ctx);
+      EDDY_CUDA(cudaEventRecord(ctx->ib_ev[0], ctx->stream));
+    }
     if (ctx->prm.isgs != 0) {
       int rc;
       // the learned closure writes the mixed form's FP32 copies itself
@@ -694,6 +718,13 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
       const bool mirror = ctx->mixed && closure && mixed_views(ctx, &mv) == EDDY_OK;
       if (ctx->ib && (rc = ib_interior(ctx, 3, ctx->f[EDDY_TV], 0.0, mirror ? mv.tv : nullptr, mv.px))) return rc;
       if (ctx->mixed && !closure && (rc = mixed_after_sgs(ctx))) return rc;
+    }
+    if (prefetch) {
+      int rc;
+      if ((rc = ib_swap_tv_flag(ctx))) return rc;
+      ctx->ib_move_dt = dt;
+      if ((rc = ib_overlap_regen(ctx))) return rc;
+      ctx->ib_prefetched = 1;
     }
   }
   return EDDY_OK;

@@ -78,6 +78,14 @@ struct eddy_ctx {
   Dims d{};
   Scalars sc{};
   cudaStream_t stream = nullptr;
+  // immersed-body regeneration overlapped with the predictor: second stream,
+  // [0] recorded on the main stream before the predictor, [1] on ib_stream
+  // after the regeneration; ib_pending: the main stream has not yet waited [1]
+  cudaStream_t ib_stream = nullptr;
+  cudaEvent_t ib_ev[2] = {};
+  int ib_pending = 0;
+  double ib_move_dt = -1.0;  // >= 0: move over this time and regenerate in this substep
+  int ib_prefetched = 0;     // the next step's move and regeneration are already queued
   cublasHandle_t blas = nullptr;
   DevMetrics m{};
   // host copies of the 1-D arrays (1-based, size n+2)
@@ -88,7 +96,7 @@ struct eddy_ctx {
   // SGS arrays
   double *uc = nullptr, *vc = nullptr, *wc = nullptr, *sij = nullptr, *gs = nullptr,
          *mm = nullptr, *lm = nullptr, *dxdydz = nullptr, *ilm2 = nullptr, *imm2 = nullptr;
-  double *scal = nullptr;  // device scalars: [0] pref [1] qin1 [2] qin2 [3] dpm [4] maxdiv
+  double *scal = nullptr;  // device scalars: [0] pref [1] qin1 [2] qin2 [3] dpm [4] maxdiv; [32, 328) flux partials
   PoissonPlan pp{};
   std::string err;
   int64_t launches = 0;
@@ -206,6 +214,14 @@ const double *ib_velocity(eddy_ctx *ctx);
 int ib_set_cadence(eddy_ctx *ctx, int every_substep);
 int ib_every_substep(eddy_ctx *ctx);
 int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror = nullptr, int mpitch = 0);
+// the move and regeneration due in this substep (ctx->ib_move_dt), on
+// ctx->ib_stream after ctx->ib_ev[0], overlapping work queued on the main
+// stream since; ib_join makes the main stream wait for it
+int ib_overlap_regen(eddy_ctx *ctx);
+void ib_join(eddy_ctx *ctx);
+// the tv flag (fq = 3) is double-buffered so the next step's regeneration can
+// run while tvinterior still reads the current one: swap before it
+int ib_swap_tv_flag(eddy_ctx *ctx);
 int ib_download(eddy_ctx *ctx, int which, signed char *out);
 int ib_limits(eddy_ctx *ctx, int *lim6);
 int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,

@@ -67,6 +67,7 @@ struct IbState {
   Box6 lim{};
   signed char *tag[4] = {};   // TAG3D results u, v, w, p
   signed char *flag[5] = {};  // taguo u, v, w, tv; flagp p
+  signed char *flag3b = nullptr;  // second buffer of the tv flag
   signed char *work = nullptr;
   Bins b2, b3;
   // per-point scratch of the geometry search
@@ -1387,6 +1388,7 @@ int ib_release(eddy_ctx *ctx) {
   if (s->sxn) cudaFree(s->sxn);
   for (int q = 0; q < 4; q++) if (s->tag[q]) cudaFree(s->tag[q]);
   for (int q = 0; q < 5; q++) if (s->flag[q]) cudaFree(s->flag[q]);
+  if (s->flag3b) cudaFree(s->flag3b);
   for (StencilSet &S : s->set) {
     void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu};
     for (void *q : ptrs) if (q) cudaFree(q);
@@ -1402,7 +1404,48 @@ int ib_release(eddy_ctx *ctx) {
   return EDDY_OK;
 }
 
+void ib_join(eddy_ctx *ctx) {
+  if (ctx->ib_pending) {
+    cudaStreamWaitEvent(ctx->stream, ctx->ib_ev[1], 0);
+    ctx->ib_pending = 0;
+  }
+}
+
+int ib_swap_tv_flag(eddy_ctx *ctx) {
+  IbState *s = ibs(ctx);
+  if (!s || !s->flag3b) return EDDY_OK;
+  signed char *t = s->flag[3];
+  s->flag[3] = s->flag3b;
+  s->flag3b = t;
+  return EDDY_OK;
+}
+
+int ib_overlap_regen(eddy_ctx *ctx) {
+  if (ctx->ib_move_dt < 0.) return EDDY_OK;
+  const double tmove = ctx->ib_move_dt;
+  ctx->ib_move_dt = -1.;
+  EDDY_CUDA(cudaStreamWaitEvent(ctx->ib_stream, ctx->ib_ev[0], 0));
+  // every launch below (and the profile scope) goes to the second stream
+  struct Swap {
+    eddy_ctx *c;
+    cudaStream_t main;
+    explicit Swap(eddy_ctx *x) : c(x), main(x->stream) { c->stream = c->ib_stream; }
+    ~Swap() { c->stream = main; }
+  };
+  int rc;
+  {
+    Swap sw(ctx);
+    ProfScope ps(ctx, PROF_IB_REGEN);
+    if ((rc = ib_move(ctx, tmove))) return rc;
+    if ((rc = ib_regen(ctx))) return rc;
+  }
+  EDDY_CUDA(cudaEventRecord(ctx->ib_ev[1], ctx->ib_stream));
+  ctx->ib_pending = 1;
+  return EDDY_OK;
+}
+
 int ib_set_body(eddy_ctx *ctx, int nb, const double *vert, const double *normals, const double *vel) {
+  ib_join(ctx);
   ib_release(ctx);
   if (nb <= 0) return EDDY_OK;
   IbState *s = new (std::nothrow) IbState();
@@ -1423,6 +1466,10 @@ int ib_set_body(eddy_ctx *ctx, int nb, const double *vert, const double *normals
   for (int q = 0; q < 5; q++) {
     EDDY_CUDA(cudaMalloc(&s->flag[q], nc));
     EDDY_CUDA(cudaMemset(s->flag[q], 0, nc));
+    if (q == 3) {
+      EDDY_CUDA(cudaMalloc(&s->flag3b, nc));
+      EDDY_CUDA(cudaMemset(s->flag3b, 0, nc));
+    }
   }
   EDDY_CUDA(cudaMalloc(&s->work, nc));
   // coordinate arrays (1-based, size n+1)
@@ -1440,6 +1487,7 @@ int ib_set_body(eddy_ctx *ctx, int nb, const double *vert, const double *normals
 }
 
 int ib_move(eddy_ctx *ctx, double tmove) {
+  ib_join(ctx);
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
   k_move<<<nblk(s->nb), 256, 0, ctx->stream>>>(s->nb, s->v, s->c, s->vel[0] * tmove, s->vel[1] * tmove,
@@ -1450,6 +1498,7 @@ int ib_move(eddy_ctx *ctx, double tmove) {
 
 // the regeneration of src/Eddy6.f:2184-2380 for the current body position
 int ib_regen(eddy_ctx *ctx) {
+  ib_join(ctx);
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
   const Dims &d = ctx->d;
@@ -1545,11 +1594,13 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
 }
 
 int ib_force(eddy_ctx *ctx, int q, int fq, double *a, double b0, double interior, float *mirror, int mpitch) {
+  ib_join(ctx);
   if (!ibs(ctx)) return EDDY_OK;
   return force_t<double>(ctx, q, fq, a, ctx->d.nx, b0, interior, mirror, mpitch);
 }
 
 int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, double interior) {
+  ib_join(ctx);
   if (!ibs(ctx)) return EDDY_OK;
   return force_t<float>(ctx, q, fq, a, pitch, b0, interior, nullptr, 0);
 }
@@ -1557,6 +1608,7 @@ int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, dou
 const double *ib_velocity(eddy_ctx *ctx) { return ibs(ctx) ? ibs(ctx)->vel : nullptr; }
 
 int ib_set_cadence(eddy_ctx *ctx, int every_substep) {
+  ib_join(ctx);
   if (!ibs(ctx)) return EDDY_EINVAL;
   ibs(ctx)->every_substep = every_substep ? 1 : 0;
   return EDDY_OK;
@@ -1566,6 +1618,7 @@ int ib_every_substep(eddy_ctx *ctx) { return ibs(ctx) ? ibs(ctx)->every_substep 
 
 // value where flag fq == 1 (tvinterior), then y periodic planes
 int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror, int mpitch) {
+  ib_join(ctx);
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
   const Dims &d = ctx->d;
@@ -1581,6 +1634,7 @@ int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror, i
 }
 
 int ib_download(eddy_ctx *ctx, int which, signed char *out) {
+  ib_join(ctx);
   IbState *s = ibs(ctx);
   if (!s || which < 0 || which > 8) return EDDY_EINVAL;
   signed char *src = which < 4 ? s->tag[which] : s->flag[which - 4];
@@ -1590,6 +1644,7 @@ int ib_download(eddy_ctx *ctx, int which, signed char *out) {
 }
 
 int ib_limits(eddy_ctx *ctx, int *lim6) {
+  ib_join(ctx);
   IbState *s = ibs(ctx);
   if (!s) return EDDY_EINVAL;
   lim6[0] = s->lim.imin; lim6[1] = s->lim.imax; lim6[2] = s->lim.jmin;
@@ -1599,6 +1654,7 @@ int ib_limits(eddy_ctx *ctx, int *lim6) {
 
 int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
                 int *indx) {
+  ib_join(ctx);
   IbState *s = ibs(ctx);
   if (!s || q < 0 || q > 3) return EDDY_EINVAL;
   StencilSet &S = s->set[q];

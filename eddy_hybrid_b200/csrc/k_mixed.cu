@@ -984,8 +984,8 @@ static int boundinout_pred(eddy_ctx *ctx, double alfxdt) {
   bct::k_inlet_plane<float><<<nblk(n2), 256, 0, st>>>(d, px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEU],
                                                       ctx->f[EDDY_PLANEV], ctx->f[EDDY_PLANEW]);
   EDDY_LAUNCHED(ctx);
-  bct::k_plane_flux<double><<<1, 1024, 0, st>>>(d, d.nx, ctx->m, ctx->f[EDDY_PLANEW], 1, fin);
-  EDDY_LAUNCHED(ctx);
+  int rc;
+  if ((rc = plane_flux<double>(ctx, d.nx, ctx->f[EDDY_PLANEW], 1, fin))) return rc;
   bct::k_outlet_convective<float, float><<<nblk(nin), 256, 0, st>>>(d, px, ctx->m, x->us, x->vs, x->ws, x->uo, x->vo,
                                                                     x->wo, fin, alfxdt);
   EDDY_LAUNCHED(ctx);
@@ -993,8 +993,7 @@ static int boundinout_pred(eddy_ctx *ctx, double alfxdt) {
   EDDY_LAUNCHED(ctx);
   k_plane_from32<<<nblk(n2), 256, 0, st>>>(d, px, x->ws, d.kz2, x->wout);
   EDDY_LAUNCHED(ctx);
-  bct::k_plane_flux<double><<<1, 1024, 0, st>>>(d, d.nx, ctx->m, x->wout, 1, fout);
-  EDDY_LAUNCHED(ctx);
+  if ((rc = plane_flux<double>(ctx, d.nx, x->wout, 1, fout))) return rc;
   k_rescale_plane<<<nblk(nin), 256, 0, st>>>(d, px, x->wout, x->ws, fin, fout);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
@@ -1024,6 +1023,7 @@ int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
     k_zero_faces32<<<nblk(ng), 256, 0, ctx->stream>>>(d, px, x->us, x->vs, x->ws);
     EDDY_LAUNCHED(ctx);
   }
+  if ((rc = ib_overlap_regen(ctx))) return rc;
   // immersed body: momforc_mod2 + velinterior on the FP32 predictor velocities
   if (ctx->ib) {
     ProfScope ps(ctx, PROF_IB_FORCE);

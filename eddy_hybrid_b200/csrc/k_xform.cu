@@ -16,12 +16,13 @@
 //   backward: e = B_e c_even, o = B_o c_odd, f[x] = e + o, f[M-1-x] = e - o,
 // all four matrices H x H.
 //
-// One CTA per 128-line tile, all M outputs in TMEM columns 0..M-1 (M <= 512).
+// One CTA per 128-line tile, all M outputs in TMEM columns 0..M-1 (M <= 432).
 // K is streamed in chunks of 8 through a multi-stage shared-memory pipeline:
-// each A chunk arrives by two 2-D TMA boxes (16 bytes x 128 lines each) so
-// shared memory holds it in the canonical no-swizzle K-major layout
-// [k/4][line][4]; the B chunks (prepared on the host in that layout, hi and
-// lo) arrive by 1-D bulk copies.  Loading, splitting A into hi/lo (and, for
+// each A chunk arrives by one 2-D TMA box (32 bytes x 128 lines) with the
+// 32-byte swizzle, which is the canonical SWIZZLE_32B K-major layout (rows of
+// 32 bytes, the two 16-byte halves of row r exchanged when bit 2 of r is
+// set); the B chunks (prepared on the host in the no-swizzle K-major layout
+// [k/4][n][4], hi and lo) arrive by 1-D bulk copies.  Loading, splitting A into hi/lo (and, for
 // the symmetric forward transform, forming the mirror sums and differences)
 // and the MMAs run in separate warps so the three overlap across stages; the
 // epilogue reads TMEM (lane = line) and stores rows.
@@ -104,6 +105,19 @@ __device__ __forceinline__ float4 tf32_hi(float4 v) {
 
 __device__ __forceinline__ float4 sub4(float4 a, float4 b) {
   return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+
+// SWIZZLE_32B K-major descriptor: rows of 32 bytes, 8-row groups 256 bytes
+// apart (SBO), LBO 16 bytes (unused inside the swizzle atom), version 1
+__device__ __forceinline__ uint64_t make_desc_sw32(const void *smem_base) {
+  const uint64_t addr = tma::smem_u32(smem_base);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;
+  d |= (uint64_t)(16 >> 4) << 16;
+  d |= (uint64_t)(256 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)6 << 61;  // layout type SWIZZLE_32B
+  return d;
 }
 
 // Per-stage layout.  mode 0 (plain): A, A_lo, B_hi, B_lo with B of M rows.
@@ -190,7 +204,7 @@ __global__ void __launch_bounds__(XT, 1)
           // K offset of the A block: plain / first half at 8c; mirror block
           // (forward) at M - 8(c+1); odd-mode block (backward) at H + 8c
           const int k0 = h == 0 ? c * KC : (mode == 1 ? M - (c + 1) * KC : H + c * KC);
-          for (int q = 0; q < KC / 4; q++) load_2d(st_a(s, h) + q * 128 * 16, &amap, k0 + 4 * q, (int)p0, &full[s]);
+          load_2d(st_a(s, h), &amap, k0, (int)p0, &full[s]);
           const size_t boff = (size_t)h * G.nb * G.nb + (size_t)c * (KC / 4) * G.nb * 4;  // floats
           bulk_load(st_bhi(s, h), bhi + boff, G.b_bytes, &full[s]);
           bulk_load(st_blo(s, h), blo + boff, G.b_bytes, &full[s]);
@@ -203,15 +217,15 @@ __global__ void __launch_bounds__(XT, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t lbo_a = 128 * 16, lbo_b = (uint32_t)G.nb * 16;
+      const uint32_t lbo_b = (uint32_t)G.nb * 16;
       for (int c = 0; c < nch; c++) {
         const int s = c % nst;
         if (abort_flag || !umma::mbar_wait(&split[s], (c / nst) & 1)) { fail(); break; }
         umma::fence_after_sync();
         const uint32_t acc = c == 0 ? 0u : 1u;
         for (int h = 0; h < G.na; h++) {
-          const uint64_t ah = umma::make_desc(st_a(s, h), lbo_a, 128);
-          const uint64_t al = umma::make_desc(st_alo(s, h), lbo_a, 128);
+          const uint64_t ah = make_desc_sw32(st_a(s, h));
+          const uint64_t al = make_desc_sw32(st_alo(s, h));
           // columns of this block: [h*H, h*H + nb) in the symmetric form; the
           // plain form splits its M columns into MMAs of at most 256
           for (int n0 = 0; n0 < G.nb; n0 += 256) {
@@ -236,47 +250,54 @@ __global__ void __launch_bounds__(XT, 1)
       const int s = c % nst;
       if (abort_flag) { ok = false; break; }
       if (!umma::mbar_wait(&full[s], (c / nst) & 1)) { fail(); ok = false; break; }
-      // 128 rows x 2 k-groups = 256 float4 per A block; thread t handles
-      // (row t, both k-groups)
+      // 128 rows of 32 bytes = 256 float4 per A block; thread t handles row t
+      // (float4 2t, 2t + 1; which holds which k half depends on the swizzle,
+      // the element-wise split does not care)
       float4 *a1 = reinterpret_cast<float4 *>(st_a(s, 0));
       float4 *l1 = reinterpret_cast<float4 *>(st_alo(s, 0));
       if (mode == 1) {
-        // mirror sums and differences: local k of the mirror block is 7 - k
+        // mirror sums and differences: local k of the mirror block is 7 - k.
+        // Half c of row t sits in 16-byte slot c ^ sw(t) of both blocks, so
+        // slot p of A1 pairs with slot 1 - p of A2 (reversed) whatever sw(t)
         float4 *a2 = reinterpret_cast<float4 *>(st_a(s, 1));
         float4 *l2 = reinterpret_cast<float4 *>(st_alo(s, 1));
-        const float4 x0 = a1[t], x1 = a1[128 + t], y0 = a2[t], y1 = a2[128 + t];
+        const float4 x0 = a1[2 * t], x1 = a1[2 * t + 1], y0 = a2[2 * t], y1 = a2[2 * t + 1];
         const float4 r0 = make_float4(y1.w, y1.z, y1.y, y1.x), r1 = make_float4(y0.w, y0.z, y0.y, y0.x);
         const float4 s0 = make_float4(x0.x + r0.x, x0.y + r0.y, x0.z + r0.z, x0.w + r0.w);
         const float4 s1 = make_float4(x1.x + r1.x, x1.y + r1.y, x1.z + r1.z, x1.w + r1.w);
         const float4 d0 = sub4(x0, r0), d1 = sub4(x1, r1);
         float4 h;
-        h = tf32_hi(s0); a1[t] = h; l1[t] = sub4(s0, h);
-        h = tf32_hi(s1); a1[128 + t] = h; l1[128 + t] = sub4(s1, h);
-        h = tf32_hi(d0); a2[t] = h; l2[t] = sub4(d0, h);
-        h = tf32_hi(d1); a2[128 + t] = h; l2[128 + t] = sub4(d1, h);
+        h = tf32_hi(s0); a1[2 * t] = h; l1[2 * t] = sub4(s0, h);
+        h = tf32_hi(s1); a1[2 * t + 1] = h; l1[2 * t + 1] = sub4(s1, h);
+        h = tf32_hi(d0); a2[2 * t] = h; l2[2 * t] = sub4(d0, h);
+        h = tf32_hi(d1); a2[2 * t + 1] = h; l2[2 * t + 1] = sub4(d1, h);
       } else {
         for (int hb = 0; hb < G.na; hb++) {
           float4 *a = reinterpret_cast<float4 *>(st_a(s, hb));
           float4 *l = reinterpret_cast<float4 *>(st_alo(s, hb));
 #pragma unroll
           for (int e = 0; e < 2; e++) {
-            const float4 v = a[e * 128 + t], h = tf32_hi(v);
-            a[e * 128 + t] = h;
-            l[e * 128 + t] = sub4(v, h);
+            const float4 v = a[2 * t + e], h = tf32_hi(v);
+            a[2 * t + e] = h;
+            l[2 * t + e] = sub4(v, h);
           }
         }
       }
       umma::fence_smem_to_async();
       mbar_arrive(&split[s]);
     }
-    // epilogue: all MMAs complete
+    // epilogue: all MMAs complete, so every stage buffer is free.  Thread t
+    // (row t of the tile) assembles its output row in shared memory (rows
+    // padded to M + 4 floats against bank conflicts) and writes it back with
+    // one bulk copy (the row is contiguous in global memory).
     if (ok && !umma::mbar_wait(&done, 0)) { fail(); ok = false; }
     umma::fence_after_sync();
     if (ok && !abort_flag) {
       const int q4 = warp & 3;
-      const long long row = p0 + q4 * 32 + lane;
+      const int rt = q4 * 32 + lane;
+      const long long row = p0 + rt;
       const uint32_t tl = tm + ((uint32_t)(q4 * 32) << 16);
-      float *orow = out + row * M;
+      float *srow = reinterpret_cast<float *>(base) + (size_t)rt * (M + 4);
       if (mode == 2) {
         // f[x] = e + o, f[M-1-x] = e - o
         for (int c0 = 0; c0 < H; c0 += 32) {
@@ -284,21 +305,19 @@ __global__ void __launch_bounds__(XT, 1)
           tmem_ld32(tl + (uint32_t)c0, e);
           tmem_ld32(tl + (uint32_t)(H + c0), o);
           const int nv = (H - c0 < 32 ? H - c0 : 32) / 4;
-          if (row < P) {
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-              if (q < nv) {
-                float p[4], m[4];
+          for (int q = 0; q < 8; q++) {
+            if (q < nv) {
+              float pv[4], mv[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                  const float ev = __uint_as_float(e[4 * q + u]), ov = __uint_as_float(o[4 * q + u]);
-                  p[u] = ev + ov;
-                  m[u] = ev - ov;
-                }
-                const int x = c0 + 4 * q;
-                *reinterpret_cast<float4 *>(orow + x) = make_float4(p[0], p[1], p[2], p[3]);
-                *reinterpret_cast<float4 *>(orow + (M - 4 - x)) = make_float4(m[3], m[2], m[1], m[0]);
+              for (int u = 0; u < 4; u++) {
+                const float ev = __uint_as_float(e[4 * q + u]), ov = __uint_as_float(o[4 * q + u]);
+                pv[u] = ev + ov;
+                mv[u] = ev - ov;
               }
+              const int x = c0 + 4 * q;
+              *reinterpret_cast<float4 *>(srow + x) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+              *reinterpret_cast<float4 *>(srow + (M - 4 - x)) = make_float4(mv[3], mv[2], mv[1], mv[0]);
             }
           }
         }
@@ -306,16 +325,22 @@ __global__ void __launch_bounds__(XT, 1)
         for (int c0 = 0; c0 < M; c0 += 64) {
           uint32_t r[64];
           umma::tmem_ld64(tl + (uint32_t)c0, r);
-          if (row < P) {
-            float4 *dst = reinterpret_cast<float4 *>(orow + c0);
-            const int nv = (M - c0 < 64 ? M - c0 : 64) / 4;
+          float4 *dst = reinterpret_cast<float4 *>(srow + c0);
+          const int nv = (M - c0 < 64 ? M - c0 : 64) / 4;
 #pragma unroll
-            for (int q = 0; q < 16; q++)
-              if (q < nv)
-                dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
-                                     __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
-          }
+          for (int q = 0; q < 16; q++)
+            if (q < nv)
+              dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                   __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
         }
+      }
+      umma::fence_smem_to_async();
+      if (row < P) {
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(out + row * M),
+                     "r"(tma::smem_u32(srow)), "r"((uint32_t)M * 4u)
+                     : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
       }
     }
   }
@@ -366,9 +391,18 @@ int xform_stages(int mode, int M) {
   return n > MAXST ? MAXST : n;
 }
 
+// dynamic shared memory: the stages, which the epilogue reuses for its
+// 128 output rows of M + 4 floats
+size_t xform_smem(int mode, int M) {
+  const size_t st = (size_t)xform_stages(mode, M) * stage_geom(mode, M).stage;
+  const size_t ep = (size_t)128 * (M + 4) * 4;
+  return (st > ep ? st : ep) + 1024;
+}
+
 }  // namespace
 
-bool xform_supported(int M) { return M >= 16 && M <= 512 && M % 16 == 0; }
+// M <= 432: the epilogue's 128 staged rows of M + 4 floats fit in shared memory
+bool xform_supported(int M) { return M >= 16 && M <= 432 && M % 16 == 0; }
 
 // Transform matrices from the FP64 plan.  Af (col-major, Af(n, x)) maps
 // x values to mode coefficients, Ab (col-major, Ab(x, n)) back.  The split
@@ -431,7 +465,7 @@ int xform_prepare(eddy_ctx *ctx, XformPlan *xp) {
   EDDY_CUDA(cudaMemcpy(xp->lam, lp.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
   size_t smax = 0;
   for (int mode = sym ? 1 : 0; mode < (sym ? 3 : 1); mode++) {
-    const size_t smem = (size_t)xform_stages(mode, M) * stage_geom(mode, M).stage + 1024;
+    const size_t smem = xform_smem(mode, M);
     smax = smem > smax ? smem : smax;
   }
   EDDY_CUDA(cudaFuncSetAttribute(k_xform_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
@@ -453,13 +487,13 @@ int launch_xform(eddy_ctx *ctx, const XformPlan *xp, int dir, const float *in, f
   const long long P = (long long)ctx->pp.L * ctx->pp.N;
   const CUtensorMap *mp = nullptr;
   for (TmaEntry &e : ctx->tmaps)
-    if (e.ptr == in && e.bx == 4 && e.by == -128) mp = &e.map;
+    if (e.ptr == in && e.bx == 8 && e.by == -128) mp = &e.map;
   if (!mp) {
     TmaEntry e;
     e.ptr = in;
-    e.bx = 4;
-    e.by = -128;  // key: 2-D (M, P) view with a 4 x 128 box
-    int r = make_tensor_map_2d(&e.map, in, M, P, 4, 128);
+    e.bx = 8;
+    e.by = -128;  // key: 2-D (M, P) view with an 8 x 128 box, 32-byte swizzle
+    int r = make_tensor_map_2d(&e.map, in, M, P, 8, 128, 1);
     if (r != 0) {
       ctx->err = "cuTensorMapEncodeTiled (transform) failed (" + std::to_string(r) + ")";
       return EDDY_ECUDA;
@@ -469,7 +503,7 @@ int launch_xform(eddy_ctx *ctx, const XformPlan *xp, int dir, const float *in, f
   }
   const int mode = xp->sym ? 1 + dir : 0;
   const int nst = xform_stages(mode, M);
-  const size_t smem = (size_t)nst * stage_geom(mode, M).stage + 1024;
+  const size_t smem = xform_smem(mode, M);
   const unsigned grid = (unsigned)((P + 127) / 128);
   k_xform_tf32<<<grid, XT, smem, ctx->stream>>>(*mp, dir ? xp->bhi : xp->fhi, dir ? xp->blo : xp->flo, out, P, M,
                                                 mode, nst, ctx->err_flag);

@@ -69,8 +69,10 @@ __device__ __forceinline__ void load_3d(void *dst, const CUtensorMap *map, int x
 // Returns 0 on success.
 int make_tensor_map_3d(CUtensorMap *map, const void *base, int nx, int ny, int nz, int bx, int by, int esize,
                        int pitch = 0);
-// 2-D FP32 (w, h) row-major array (row stride w elements) with a (bx, by) box
-int make_tensor_map_2d(CUtensorMap *map, const void *base, long long w, long long h, int bx, int by);
+// 2-D FP32 (w, h) row-major array (row stride w elements) with a (bx, by)
+// box; swizzle32: 32-byte swizzle (bx * 4 must then be 32)
+int make_tensor_map_2d(CUtensorMap *map, const void *base, long long w, long long h, int bx, int by,
+                       int swizzle32 = 0);
 
 // ---------------------------------------------------------------------------
 // Generic k-marching driver over a 4-slot ring of halo planes of NF fields.
