@@ -612,16 +612,23 @@ __global__ void __launch_bounds__(DTX *DTY)
     k_density32(Dims d, DevMetrics32 m, Scalars s, int px, const __grid_constant__ TmaMaps<DNF> maps,
                 float *__restrict__ rha, float *__restrict__ dn, float repr1, float alfxdt, float gamxdt,
                 float rhoxdt, int *err) {
+  // per-column metric values in registers (the tma_march column of this thread)
+  const int ic = min(d.ix1 + (int)(blockIdx.x * DTX + threadIdx.x), d.ix2);
+  const int jc = min(d.jy1 + (int)(blockIdx.y * DTY + threadIdx.y), d.jy2);
+  MetricCol32 mc;
+  mc.ap = reg3(m.ap, ic); mc.au = reg3(m.au, ic);
+  mc.bp = reg3(m.bp, jc); mc.bv = reg3(m.bv, jc);
+  const float bg = m.dens_bg[(ic - 1) + d.nx * (jc - 1)], dfxd_i = m.dfxd[ic];
   tma_march<DNF, DTX, DTY, DKC, float>(d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err,
                                        [&](int i, int j, int k, bool active, const Acc6 &S) {
                                          if (!active) return;
-                                         float rr = rhs_dens<float>(S, m, repr1, i, j, k);
+                                         mc.cp = reg3(m.cp, k); mc.cw = reg3(m.cw, k);
+                                         float rr = rhs_dens<float>(S, mc, repr1, i, j, k);
                                          float dnew = S.at(0, 0, 0, 0) + gamxdt * rr + rhoxdt * S.at(5, 0, 0, 0);
                                          long long q = pidx(d, px, i, j, k);
                                          rha[q] = rr;
-                                         float bg = m.dens_bg[(i - 1) + d.nx * (j - 1)];
                                          if (s.idspngl == 1) dnew = dnew + m.dfxdl[k] * (bg - dnew) * alfxdt;
-                                         if (i >= d.ix2 - s.dspngx1) dnew = dnew + m.dfxd[i] * (bg - dnew) * alfxdt;
+                                         if (i >= d.ix2 - s.dspngx1) dnew = dnew + dfxd_i * (bg - dnew) * alfxdt;
                                          dn[q] = dnew;
                                        });
 }
