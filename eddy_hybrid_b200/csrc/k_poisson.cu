@@ -257,7 +257,7 @@ int solve_from_spec(eddy_ctx *ctx, double *dp) {
     k_line_mean<double><<<1, 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.wz, pp.spec2, ctx->scal + 5);
     EDDY_LAUNCHED(ctx);
     // the eliminated right-hand side overwrites the spectrum in place
-    k_tridiag_lines<double><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
+    k_tridiag_lines<double, double, 8, false><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
         M, L, N, pp.m0, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, pp.spec2, pp.cprime, pp.spec2);
     EDDY_LAUNCHED(ctx);
   }

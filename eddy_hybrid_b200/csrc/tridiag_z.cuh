@@ -39,7 +39,9 @@ __global__ void k_line_mean(int M, int L, int N, int m0, const double *__restric
   if (threadIdx.x == 0) out[0] = s1[0] / s2[0];
 }
 
-template <class G, class C = double, int ZC = 8>
+// DB: issue the next chunk's loads before the current chunk's recurrence (two
+// register buffers; pays off with FP32 storage, the FP64 form keeps one)
+template <class G, class C = double, int ZC = 8, bool DB = true>
 __global__ void __launch_bounds__(128)
     k_tridiag_lines(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
                     const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
@@ -76,13 +78,20 @@ __global__ void __launch_bounds__(128)
       }
     }
   };
-  load_f(fa, s0);
-  for (int k0 = s0; k0 < N; k0 += 2 * ZC) {
-    if (k0 + ZC < N) load_f(fb, k0 + ZC);
-    elim(fa, k0);
-    if (k0 + ZC < N) {
-      if (k0 + 2 * ZC < N) load_f(fa, k0 + 2 * ZC);
-      elim(fb, k0 + ZC);
+  if (DB) {
+    load_f(fa, s0);
+    for (int k0 = s0; k0 < N; k0 += 2 * ZC) {
+      if (k0 + ZC < N) load_f(fb, k0 + ZC);
+      elim(fa, k0);
+      if (k0 + ZC < N) {
+        if (k0 + 2 * ZC < N) load_f(fa, k0 + 2 * ZC);
+        elim(fb, k0 + ZC);
+      }
+    }
+  } else {
+    for (int k0 = s0; k0 < N; k0 += ZC) {
+      load_f(fa, k0);
+      elim(fa, k0);
     }
   }
   // back substitution, same double buffering (chunk k1, k1-1, ..., k1-ZC+1)
@@ -107,13 +116,20 @@ __global__ void __launch_bounds__(128)
       }
     }
   };
-  if (N - 2 >= s0) load_b(ca, ea, N - 2);
-  for (int k1 = N - 2; k1 >= s0; k1 -= 2 * ZC) {
-    if (k1 - ZC >= s0) load_b(cb, eb, k1 - ZC);
-    subst(ca, ea, k1);
-    if (k1 - ZC >= s0) {
-      if (k1 - 2 * ZC >= s0) load_b(ca, ea, k1 - 2 * ZC);
-      subst(cb, eb, k1 - ZC);
+  if (DB) {
+    if (N - 2 >= s0) load_b(ca, ea, N - 2);
+    for (int k1 = N - 2; k1 >= s0; k1 -= 2 * ZC) {
+      if (k1 - ZC >= s0) load_b(cb, eb, k1 - ZC);
+      subst(ca, ea, k1);
+      if (k1 - ZC >= s0) {
+        if (k1 - 2 * ZC >= s0) load_b(ca, ea, k1 - 2 * ZC);
+        subst(cb, eb, k1 - ZC);
+      }
+    }
+  } else {
+    for (int k1 = N - 2; k1 >= s0; k1 -= ZC) {
+      load_b(ca, ea, k1);
+      subst(ca, ea, k1);
     }
   }
   if (pin) g[t] = (G)0.;
