@@ -7,7 +7,8 @@
 //                       the training GEMMs (forward, input gradient, weight
 //                       gradient) all map onto it.
 //  * k_mlp_infer      : fused per-cell inference: features of a 128-cell tile
-//                       -> four MMA layers with bias/activation epilogues from TMEM
+//                       -> three MMA layers with bias/activation epilogues from TMEM
+//                       -> the 64 -> 2 output layer on the CUDA cores
 //                       -> coefficients C_nu, C_kappa -> nu_t = C_nu Delta^2 |S|,
 //                       kappa_t = C_kappa Delta^2 |S|.
 // The closure stands in for the dynamic procedure's test filtering and
@@ -268,11 +269,14 @@ __global__ void k_harvest(Dims d, DevMetrics m, CellGeom cg, double grav, double
 // the threads run the other tile's epilogue.
 constexpr int IT = 128;
 struct InferSmem {
-  unsigned char w1[HID * KIN * 2], w2[HID * HID * 2], w3[HID * HID * 2], w4[NOUT * HID * 2];
+  unsigned char w1[HID * KIN * 2], w2[HID * HID * 2], w3[HID * HID * 2];
   // h[g]: layer input of tile g; the normalised features (layer 1's input,
   // 128 x KIN) occupy its first 4 KB until layer 1's MMA has read them
   unsigned char h[2][128 * HID * 2];
   float b1[HID], b2[HID], b3[HID], b4[NOUT];
+  // output layer rows 0 and 1 in FP32: computed on the CUDA cores from the
+  // layer-3 activations in registers (no fourth MMA round trip)
+  __align__(16) float w4f[2][HID];
   MlpMeta meta;
   uint64_t bar[2];
   uint32_t tmem;
@@ -318,6 +322,26 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tm, int warp, int row, 
     o.w = act2_bf16(x(c0 + 6), x(c0 + 7));
     *reinterpret_cast<uint4 *>(h + umma::kmajor_offset(row, c0, HID)) = o;
   }
+}
+
+// last hidden layer (TMEM + bias -> hard-swish, FP32) and the output layer's
+// two rows: v[n] = b4[n] + sum_c w4[n][c] act[c]
+__device__ __forceinline__ void output_layer(uint32_t tm, int warp, const float *bias, const float (*w4)[HID],
+                                             const float *b4, float *v) {
+  uint32_t r[HID];
+  umma::tmem_ld64(tm + ((uint32_t)(warp * 32) << 16), r);
+  float o0 = b4[0], o1 = b4[1];
+#pragma unroll
+  for (int c = 0; c < HID; c += 4) {
+    const float4 p = *reinterpret_cast<const float4 *>(w4[0] + c), q = *reinterpret_cast<const float4 *>(w4[1] + c);
+    const float a0 = hswish(__uint_as_float(r[c]) + bias[c]), a1 = hswish(__uint_as_float(r[c + 1]) + bias[c + 1]);
+    const float a2 = hswish(__uint_as_float(r[c + 2]) + bias[c + 2]);
+    const float a3 = hswish(__uint_as_float(r[c + 3]) + bias[c + 3]);
+    o0 = fmaf(p.x, a0, fmaf(p.y, a1, fmaf(p.z, a2, fmaf(p.w, a3, o0))));
+    o1 = fmaf(q.x, a0, fmaf(q.y, a1, fmaf(q.z, a2, fmaf(q.w, a3, o1))));
+  }
+  v[0] = o0;
+  v[1] = o1;
 }
 
 // one thread waits on the MMA barrier, the block meets at a barrier (the
@@ -374,19 +398,19 @@ __global__ void __launch_bounds__(IT)
   stage_weights(S.w1, wbf + OFF_W1, HID, KIN);
   stage_weights(S.w2, wbf + OFF_W2, HID, HID);
   stage_weights(S.w3, wbf + OFF_W3, HID, HID);
-  stage_weights(S.w4, wbf + OFF_W4, NOUT, HID);
   for (int e = tid; e < HID; e += IT) {
     S.b1[e] = theta[OFF_B1 + e];
     S.b2[e] = theta[OFF_B2 + e];
     S.b3[e] = theta[OFF_B3 + e];
   }
   if (tid < NOUT) S.b4[tid] = theta[OFF_B4 + tid];
+  for (int e = tid; e < 2 * HID; e += IT) S.w4f[e / HID][e % HID] = theta[OFF_W4 + e];
   for (int e = tid; e < NMETA; e += IT) reinterpret_cast<float *>(&S.meta)[e] = meta[e];
   publish_smem();
   const uint32_t tm = S.tmem;
   const unsigned ninner = (unsigned)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
   const unsigned ntiles = (ninner + 127) / 128, npairs = (ntiles + 1) / 2;
-  const unsigned char *wl[3] = {S.w2, S.w3, S.w4};
+  const unsigned char *wl[2] = {S.w2, S.w3};
   const float *bl[3] = {S.b1, S.b2, S.b3};
   int phase[2] = {0, 0};
   bool ok = true;
@@ -427,26 +451,27 @@ __global__ void __launch_bounds__(IT)
       mma_layer(tm + 64, S.h[1], S.w1, HID, KIN);
       umma::commit(&S.bar[1]);
     }
-    // layers 2..4: epilogue of layer L of one tile while the other tile's
+    // layers 2..3: epilogue of layer L of one tile while the other tile's
     // layer runs on the tensor core
 #pragma unroll
-    for (int L = 0; L < 3; L++) {
+    for (int L = 0; L < 2; L++) {
 #pragma unroll
       for (int g = 0; g < 2; g++) {
         ok = sync_and_wait(&S.bar[g], phase[g]) && ok;
         hidden_epilogue(tm + 64 * g, warp, tid, bl[L], S.h[g]);
         publish_smem();
         if (tid == 0) {
-          mma_layer(tm + 64 * g, S.h[g], wl[L], L == 2 ? NOUT : HID, HID);
+          mma_layer(tm + 64 * g, S.h[g], wl[L], HID, HID);
           umma::commit(&S.bar[g]);
         }
       }
     }
+    // layer 3's activations and the 64 -> 2 output layer in registers
 #pragma unroll
     for (int g = 0; g < 2; g++) {
       ok = sync_and_wait(&S.bar[g], phase[g]) && ok;
-      float v[16];
-      umma::tmem_ld16(tm + 64 * g + ((uint32_t)(warp * 32) << 16), v);
+      float v[2];
+      output_layer(tm + 64 * g, warp, S.b3, S.w4f, S.b4, v);
       const CellIn &C = c[g];
       if (C.valid && ok) {
         long long q = fidx(d, C.i, C.j, C.k);
@@ -457,8 +482,8 @@ __global__ void __launch_bounds__(IT)
           nout++;
         } else {
           // nu_t = C_nu Delta^2 |S|, kappa_t = C_kappa Delta^2 |S|
-          nu = (double)C.del * (double)C.dsr * S.meta.s_nu * softplus(v[0] + S.b4[0]);
-          ka = (double)C.del * (double)C.dsr * S.meta.s_kappa * softplus(v[1] + S.b4[1]);
+          nu = (double)C.del * (double)C.dsr * S.meta.s_nu * softplus(v[0]);
+          ka = (double)C.del * (double)C.dsr * S.meta.s_kappa * softplus(v[1]);
         }
         tv[q] = nu;
         kappa[q] = ka;
