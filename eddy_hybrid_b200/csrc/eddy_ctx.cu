@@ -349,8 +349,13 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   if (p.closure != 0 && p.closure != 1) return fail(EDDY_EINVAL, "closure must be 0 (dynamic) or 1 (learned)");
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
+  // the regeneration's stream has the highest priority: its short kernels
+  // (and the host waits between them) must not queue behind the blocks of a
+  // long kernel on the main stream
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->ib_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->ib_stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ib_ev[0], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ib_ev[1], cudaEventDisableTiming) != cudaSuccess)
     return fail(EDDY_ECUDA, "cudaStreamCreate failed");
@@ -692,10 +697,13 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
       if (rc) return rc;
     }
     // within one call the next step's move (same dt) and regeneration run on
-    // the second stream during this step's eddy viscosity; they only need
-    // this step's forcing to be done (the event), and tvinterior below keeps
-    // reading the current tv flag (double-buffered)
-    const bool prefetch = ctx->ib && !ib_every_substep(ctx) && n + 1 < nsteps;
+    // the second stream during this step's learned closure (whose MMA chain
+    // leaves SMs idle; the dynamic procedure's long kernels would only be
+    // slowed by it); they only need this step's forcing to be done (the
+    // event), and tvinterior below keeps reading the current tv flag
+    // (double-buffered)
+    const bool prefetch = ctx->ib && !ib_every_substep(ctx) && n + 1 < nsteps && ctx->prm.isgs != 0 &&
+                          ctx->prm.closure == 1;
     if (prefetch) {
       ib_join(ctx);
       EDDY_CUDA(cudaEventRecord(ctx->ib_ev[0], ctx->stream));

@@ -218,7 +218,7 @@ __device__ __forceinline__ float &slot32(float *re, float *im, int r, int lane) 
 // to dvec; MODE 1: d = dvec; MODE 2: r = dvec - L phi (FP64 residual of the
 // DIRECT operator: Neumann x and z, periodic y), max|r| -> rmax.
 template <int MODE>
-__global__ void __launch_bounds__(FT32, 3)
+__global__ void __launch_bounds__(FT32, 4)
     k_fwd32(Dims d, DevMetrics m, int px, const float *__restrict__ us, const float *__restrict__ vs,
             const float *__restrict__ ws, const double *__restrict__ win, const double *__restrict__ wout,
             const double *__restrict__ phi, double *__restrict__ dvec, double ralf, double rdy2, int logL,
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(FT32, 3)
   double *D = dvec + fidx(d, ic, d.jy1, k);
   double amax = 0.;
   if (MODE == 0) {
-    constexpr int U0 = 4;
+    constexpr int U0 = 3;
     const long long pb = pidx(d, px, ic, d.jy1, k);
     const float *Us = us + pb, *Vs = vs + pb, *Ws = ws + pb;
     const int pz = px * d.ny;
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(FT32, 3)
         if (j0 + u < je) slot32(re, im, bitrev(j0 + u, logL), lane) = act ? (float)v[u] : 0.f;
     }
   } else {
-    constexpr int U2 = 3;
+    constexpr int U2 = 2;
     const double *P = phi + fidx(d, ic, d.jy1, k);
     const int sz = nx * d.ny;
     const bool has_e = act && i < d.ix2, has_w = act && i > d.ix1;
