@@ -2,14 +2,16 @@
 FP64 solver generates, and write the weights the mixed form loads.
 
 python -m eddy_hybrid_b200.train_closure [--grid 192x128x256] [--frs 0.5,1,2]
-        [--spin 20] [--snaps 4] [--every 5] [--per-snap 1600000] [--epochs 8]
-        [--out eddy_hybrid_b200/closure_weights.npz]
+        [--noise 0.001,0.3] [--spin 5] [--snaps 4] [--every 5] [--per-snap 800000]
+        [--epochs 8] [--out eddy_hybrid_b200/closure_weights.npz]
 
-For each Froude number a plain solver (dynamic Smagorinsky, src/vt.f:16-442)
-runs `spin` steps from the seeded initial state, then every `every` steps a
-sample of interior cells is harvested: the 12 closure features and the
-dynamic model's nu_t / Delta (the target).  The last snapshot of every Froude
-number is held out.  Training runs the library's own tensor-core forward and
+For each Froude number and initial noise amplitude a plain solver (dynamic
+Smagorinsky, src/vt.f:16-442) with the moving sphere runs `spin` steps from the
+seeded initial state, then every `every` steps a sample of interior cells is
+harvested: the 12 closure features and the dynamic model's nu_t / Delta (the
+target).  The small amplitude is the wake workload's own start (activity only
+around the body), the large one gives turbulence-like gradients everywhere.
+The last snapshot of every run is held out.  Training runs the library's own tensor-core forward and
 backward kernels and Adam (eddy_closure_train).  The report records the
 held-out relative nu_t error of the network and of the best constant
 Smagorinsky coefficient (the method without the network).
@@ -38,14 +40,16 @@ def rel(a, b) -> float:
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def harvest(grid=(192, 128, 256), frs=(0.5, 1.0, 2.0), spin=20, snaps=4, every=5, per_snap=1_600_000,
-            re=1e4, noise=0.3, sphere=True, seed=0, log=print):
-    """Run the plain solver at each Froude number and harvest (X, T) samples.
-    Returns the training and held-out sets and the last solver (for training)."""
+def harvest(grid=(192, 128, 256), frs=(0.5, 1.0, 2.0), spin=5, snaps=4, every=5, per_snap=800_000,
+            re=1e4, noises=(0.001, 0.3), sphere=True, seed=0, log=print):
+    """Run the plain solver at each Froude number and noise amplitude and
+    harvest (X, T) samples.  Returns the training and held-out sets and the
+    last solver (for training)."""
     mx, ly, nz_ = grid
     train_x, train_t, test_x, test_t = [], [], [], []
     solver = None
-    for fi, fr in enumerate(frs):
+    runs = [(fr, noise) for noise in noises for fr in frs]
+    for fi, (fr, noise) in enumerate(runs):
         # velocity fluctuations strong enough for the dynamic procedure to
         # produce a non-zero eddy viscosity (its coefficient is clipped at 0)
         w = config.Workload(f"train_fr{fr}", mx=mx, ly=ly, nz_=nz_, re=re, fr=fr, dt=5e-4, sphere=sphere,
@@ -70,7 +74,7 @@ def harvest(grid=(192, 128, 256), frs=(0.5, 1.0, 2.0), spin=20, snaps=4, every=5
             X, T = X[ok], T[ok]
             (test_x if k == snaps - 1 else train_x).append(X)
             (test_t if k == snaps - 1 else train_t).append(T)
-            log(f"  Fr={fr} snapshot {k}: {len(X)} samples, mean nu_t/Delta {T.mean():.3e}")
+            log(f"  Fr={fr} noise={noise} snapshot {k}: {len(X)} samples, mean nu_t/Delta {T.mean():.3e}")
         solver = s
     return (np.concatenate(train_x), np.concatenate(train_t), np.concatenate(test_x), np.concatenate(test_t),
             solver)
@@ -115,12 +119,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--grid", default="192x128x256", help="NX-2 x NY-2 x NZ-2 of the training runs")
     ap.add_argument("--frs", default="0.5,1,2")
-    ap.add_argument("--spin", type=int, default=20)
+    ap.add_argument("--spin", type=int, default=5)
     ap.add_argument("--snaps", type=int, default=4)
     ap.add_argument("--every", type=int, default=5)
-    ap.add_argument("--per-snap", type=int, default=1_600_000)
+    ap.add_argument("--per-snap", type=int, default=800_000)
     ap.add_argument("--epochs", type=int, default=8)
-    ap.add_argument("--noise", type=float, default=0.3, help="initial velocity noise amplitude")
+    ap.add_argument("--noise", default="0.001,0.3", help="initial velocity noise amplitudes (comma list)")
     ap.add_argument("--no-sphere", action="store_true", help="train on flows without the immersed sphere")
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
@@ -129,7 +133,8 @@ def main():
     grid = tuple(int(v) for v in a.grid.split("x"))
     frs = tuple(float(v) for v in a.frs.split(","))
     t0 = time.time()
-    X, T, Xt, Tt, s = harvest(grid, frs, a.spin, a.snaps, a.every, a.per_snap, noise=a.noise,
+    noises = tuple(float(v) for v in a.noise.split(","))
+    X, T, Xt, Tt, s = harvest(grid, frs, a.spin, a.snaps, a.every, a.per_snap, noises=noises,
                               sphere=not a.no_sphere)
     t1 = time.time()
     print(f"harvested {len(X)} training / {len(Xt)} held-out samples in {t1 - t0:.1f} s")
@@ -137,7 +142,7 @@ def main():
     t2 = time.time()
     rep = evaluate(meta, theta, Xt, Tt)
     rep.update({"train_samples": int(len(X)), "grid": list(grid), "frs": list(frs), "epochs": a.epochs,
-                "noise": a.noise, "sphere": not a.no_sphere, "mean_target": float(T.mean()),
+                "noise": list(noises), "sphere": not a.no_sphere, "mean_target": float(T.mean()),
                 "loss_by_epoch": [float(v) for v in hist], "harvest_s": t1 - t0, "train_s": t2 - t1})
     print(json.dumps(rep))
     np.savez(a.out, meta=meta, theta=theta, report=json.dumps(rep))
