@@ -232,7 +232,8 @@ int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, in
 // are the eigenvalues and the null mode in the transform's mode order.
 struct XformPlan {
   int sym = 0;
-  float *fhi = nullptr, *flo = nullptr, *bhi = nullptr, *blo = nullptr;
+  // forward / backward matrices, TF32 hi and lo interleaved in streaming order
+  float *fmat = nullptr, *bmat = nullptr;
   double *lam = nullptr;
   int m0 = 0;
 };

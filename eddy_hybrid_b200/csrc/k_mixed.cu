@@ -734,7 +734,7 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   int rc;
   {
     ProfScope ps(ctx, PROF_GEMM_FWD);
-    if (x->xp.fhi) {
+    if (x->xp.fmat) {
       if ((rc = launch_xform(ctx, &x->xp, 0, s1, s2))) return rc;
     } else {
       bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Af32, M, s1, M, &zero, s2,
@@ -747,8 +747,8 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
     ProfScope ps(ctx, PROF_TRIDIAG);
     long long nl = (long long)M * L;
     // mode order of the transforms: the split form orders even modes first
-    const double *lam = x->xp.fhi ? x->xp.lam : pp.lam;
-    const int m0 = x->xp.fhi ? x->xp.m0 : pp.m0;
+    const double *lam = x->xp.fmat ? x->xp.lam : pp.lam;
+    const int m0 = x->xp.fmat ? x->xp.m0 : pp.m0;
     k_line_mean<float><<<1, 256, 0, ctx->stream>>>(M, L, N, m0, pp.wz, s2, ctx->scal + 5);
     EDDY_LAUNCHED(ctx);
     float *c32 = reinterpret_cast<float *>(pp.cprime);
@@ -758,7 +758,7 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   }
   {
     ProfScope ps(ctx, PROF_GEMM_BWD);
-    if (x->xp.bhi) {
+    if (x->xp.bmat) {
       if ((rc = launch_xform(ctx, &x->xp, 1, s2, s1))) return rc;
     } else {
       bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Ab32, M, s2, M, &zero, s1,

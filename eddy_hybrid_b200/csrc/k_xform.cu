@@ -21,8 +21,9 @@
 // each A chunk arrives by one 2-D TMA box (32 bytes x 128 lines) with the
 // 32-byte swizzle, which is the canonical SWIZZLE_32B K-major layout (rows of
 // 32 bytes, the two 16-byte halves of row r exchanged when bit 2 of r is
-// set); the B chunks (prepared on the host in the no-swizzle K-major layout
-// [k/4][n][4], hi and lo) arrive by 1-D bulk copies.  Loading, splitting A into hi/lo (and, for
+// set); the B chunks of a stage (prepared on the host, in chunk order, as the
+// no-swizzle K-major layout [k/4][n][4] of each block's hi and lo parts)
+// arrive by one 1-D bulk copy.  Loading, splitting A into hi/lo (and, for
 // the symmetric forward transform, forming the mirror sums and differences)
 // and the MMAs run in separate warps so the three overlap across stages; the
 // epilogue reads TMEM (lane = line) and stores rows.
@@ -122,7 +123,8 @@ __device__ __forceinline__ uint64_t make_desc_sw32(const void *smem_base) {
 
 // Per-stage layout.  mode 0 (plain): A, A_lo, B_hi, B_lo with B of M rows.
 // modes 1/2 (symmetric): A1, A1_lo, A2, A2_lo, B1_hi, B1_lo, B2_hi, B2_lo with
-// B1, B2 of H rows each.
+// B1, B2 of H rows each.  The B part of a stage is contiguous, in the order of
+// one chunk of the host-prepared matrix array.
 struct StageGeom {
   int nb;             // rows of one B block (M or H)
   int na;             // A blocks per stage (1 or 2)
@@ -150,8 +152,7 @@ __host__ __device__ inline StageGeom stage_geom(int mode, int M) {
 // error flag, the roles stop issuing work and wait (bounded) for what they
 // already issued before TMEM is released.
 __global__ void __launch_bounds__(XT, 1)
-    k_xform_tf32(const __grid_constant__ CUtensorMap amap, const float *__restrict__ bhi,
-                 const float *__restrict__ blo, float *__restrict__ out, long long P, int M, int mode, int nst,
+    k_xform_tf32(const __grid_constant__ CUtensorMap amap, const float *__restrict__ bmat, float *__restrict__ out, long long P, int M, int mode, int nst,
                  int *err) {
   extern __shared__ __align__(1024) unsigned char xsm[];
   __shared__ __align__(8) uint64_t full[MAXST], split[MAXST], empty[MAXST], done;
@@ -183,11 +184,13 @@ __global__ void __launch_bounds__(XT, 1)
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tm = tmem_base;
-  // block h (0 or 1) of a stage: A_hi, A_lo, B_hi, B_lo
-  auto st_a = [&](int s, int h) { return base + (size_t)s * G.stage + h * (2 * G.a_bytes + 2 * G.b_bytes); };
+  // block h (0 or 1) of a stage: A_hi, A_lo (A blocks first), B_hi, B_lo
+  auto st_a = [&](int s, int h) { return base + (size_t)s * G.stage + h * 2 * G.a_bytes; };
   auto st_alo = [&](int s, int h) { return st_a(s, h) + G.a_bytes; };
-  auto st_bhi = [&](int s, int h) { return st_a(s, h) + 2 * G.a_bytes; };
-  auto st_blo = [&](int s, int h) { return st_a(s, h) + 2 * G.a_bytes + G.b_bytes; };
+  auto st_bhi = [&](int s, int h) {
+    return base + (size_t)s * G.stage + G.na * 2 * G.a_bytes + h * 2 * G.b_bytes;
+  };
+  auto st_blo = [&](int s, int h) { return st_bhi(s, h) + G.b_bytes; };
   auto fail = [&]() {
     abort_flag = 1;
     atomicExch(err, 1);
@@ -195,21 +198,24 @@ __global__ void __launch_bounds__(XT, 1)
   bool ok = true;
   if (warp == 0) {
     if (lane == 0) {
-      int issued = 0;
+      // the per-chunk bookkeeping is kept to increments (stage, phase, B
+      // offset): this thread's issue rate paces the pipeline
+      int issued = 0, s = 0;
+      uint32_t ph = 0;
+      const uint32_t bbytes = G.na * 2 * G.b_bytes;  // B of one chunk, all blocks, hi and lo
+      const uint32_t txb = G.na * G.a_bytes + bbytes;
+      const float *bsrc = bmat;
       for (int c = 0; c < nch && !abort_flag; c++) {
-        const int s = c % nst;
-        if (c >= nst && !umma::mbar_wait(&empty[s], ((c / nst) - 1) & 1)) { fail(); break; }
-        tma::mbar_expect_tx(&full[s], G.na * (G.a_bytes + 2 * G.b_bytes));
-        for (int h = 0; h < G.na; h++) {
-          // K offset of the A block: plain / first half at 8c; mirror block
-          // (forward) at M - 8(c+1); odd-mode block (backward) at H + 8c
-          const int k0 = h == 0 ? c * KC : (mode == 1 ? M - (c + 1) * KC : H + c * KC);
-          load_2d(st_a(s, h), &amap, k0, (int)p0, &full[s]);
-          const size_t boff = (size_t)h * G.nb * G.nb + (size_t)c * (KC / 4) * G.nb * 4;  // floats
-          bulk_load(st_bhi(s, h), bhi + boff, G.b_bytes, &full[s]);
-          bulk_load(st_blo(s, h), blo + boff, G.b_bytes, &full[s]);
-        }
+        if (c >= nst && !umma::mbar_wait(&empty[s], ph ^ 1u)) { fail(); break; }
+        tma::mbar_expect_tx(&full[s], txb);
+        // K offset of the A block: plain / first half at 8c; mirror block
+        // (forward) at M - 8(c+1); odd-mode block (backward) at H + 8c
+        load_2d(st_a(s, 0), &amap, c * KC, (int)p0, &full[s]);
+        if (G.na == 2) load_2d(st_a(s, 1), &amap, mode == 1 ? M - (c + 1) * KC : H + c * KC, (int)p0, &full[s]);
+        bulk_load(st_bhi(s, 0), bsrc, bbytes, &full[s]);
+        bsrc += bbytes / 4;
         issued = c + 1;
+        if (++s == nst) { s = 0; ph ^= 1u; }
       }
       // copies still in flight land before the CTA may exit
       for (int c = issued - nst < 0 ? 0 : issued - nst; c < issued; c++)
@@ -217,69 +223,104 @@ __global__ void __launch_bounds__(XT, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
+      // Descriptors of stage 0, computed once: stage s adds s * stage bytes
+      // / 16 to the 14-bit start-address field (every stage lies inside the
+      // shared window, so the field cannot carry).  Keeping the per-chunk
+      // work to the MMAs lets them issue back to back.  Columns of block h:
+      // [h*H, h*H + nb) in the symmetric form; the plain form splits its M
+      // columns into MMAs of at most 256 (j = 0, 1).
       const uint32_t lbo_b = (uint32_t)G.nb * 16;
+      const uint64_t dstep = (uint64_t)(G.stage >> 4);
+      uint64_t dah[2], dal[2], dbh[2][2], dbl[2][2];
+      uint32_t idj[2], dcol[2][2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        dah[h] = make_desc_sw32(st_a(0, h));
+        dal[h] = make_desc_sw32(st_alo(0, h));
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          dbh[h][j] = umma::make_desc(st_bhi(0, h) + j * 256 * 16, lbo_b, 128);
+          dbl[h][j] = umma::make_desc(st_blo(0, h) + j * 256 * 16, lbo_b, 128);
+          dcol[h][j] = tm + (uint32_t)(h * H + j * 256);
+        }
+      }
+      const int nj = G.nb > 256 ? 2 : 1;
+      idj[0] = idesc_tf32(128, G.nb < 256 ? G.nb : 256);
+      idj[1] = idesc_tf32(128, G.nb > 256 ? G.nb - 256 : 16);
+      int s = 0;
+      uint32_t ph = 0;
       for (int c = 0; c < nch; c++) {
-        const int s = c % nst;
-        if (abort_flag || !umma::mbar_wait(&split[s], (c / nst) & 1)) { fail(); break; }
+        if (abort_flag || !umma::mbar_wait(&split[s], ph)) { fail(); break; }
         umma::fence_after_sync();
+        const uint64_t off = (uint64_t)s * dstep;
         const uint32_t acc = c == 0 ? 0u : 1u;
-        for (int h = 0; h < G.na; h++) {
-          const uint64_t ah = make_desc_sw32(st_a(s, h));
-          const uint64_t al = make_desc_sw32(st_alo(s, h));
-          // columns of this block: [h*H, h*H + nb) in the symmetric form; the
-          // plain form splits its M columns into MMAs of at most 256
-          for (int n0 = 0; n0 < G.nb; n0 += 256) {
-            const int nn = G.nb - n0 < 256 ? G.nb - n0 : 256;
-            const uint32_t id = idesc_tf32(128, nn);
-            const uint64_t bh = umma::make_desc(st_bhi(s, h) + n0 * 16, lbo_b, 128);
-            const uint64_t bl = umma::make_desc(st_blo(s, h) + n0 * 16, lbo_b, 128);
-            const uint32_t d = tm + (uint32_t)(h * H + n0);
-            mma_tf32(d, ah, bh, id, acc);
-            mma_tf32(d, ah, bl, id, 1u);
-            mma_tf32(d, al, bh, id, 1u);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          if (h < G.na) {
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+              if (j < nj) {
+                mma_tf32(dcol[h][j], dah[h] + off, dbh[h][j] + off, idj[j], acc);
+                mma_tf32(dcol[h][j], dah[h] + off, dbl[h][j] + off, idj[j], 1u);
+                mma_tf32(dcol[h][j], dal[h] + off, dbh[h][j] + off, idj[j], 1u);
+              }
+            }
           }
         }
         umma::commit(&empty[s]);
+        if (++s == nst) { s = 0; ph ^= 1u; }
       }
       // the commit after the last issued MMA completes once all of them have
       umma::commit(&done);
     }
   } else {
     const int t = tid - 64;
-    for (int c = 0; c < nch; c++) {
-      const int s = c % nst;
+    const int qsw = (t >> 2) & 1;
+    int s = 0;
+    uint32_t ph = 0;
+    for (int c = 0; c < nch; c++, s = (s + 1 == nst ? 0 : s + 1), ph ^= (s == 0 ? 1u : 0u)) {
       if (abort_flag) { ok = false; break; }
-      if (!umma::mbar_wait(&full[s], (c / nst) & 1)) { fail(); ok = false; break; }
+      if (!umma::mbar_wait(&full[s], ph)) { fail(); ok = false; break; }
       // 128 rows of 32 bytes = 256 float4 per A block; thread t handles row t
       // (float4 2t, 2t + 1; which holds which k half depends on the swizzle,
-      // the element-wise split does not care)
-      float4 *a1 = reinterpret_cast<float4 *>(st_a(s, 0));
-      float4 *l1 = reinterpret_cast<float4 *>(st_alo(s, 0));
+      // the element-wise split does not care).  Each access takes slot
+      // 2t + (e ^ q), q = bit 2 of t: the eight threads of one 128-bit phase
+      // then cover all 32 banks (slot 2t + e alone would pair t with t + 4).
+      float4 *a1 = reinterpret_cast<float4 *>(st_a(s, 0)) + 2 * t;
+      float4 *l1 = reinterpret_cast<float4 *>(st_alo(s, 0)) + 2 * t;
       if (mode == 1) {
         // mirror sums and differences: local k of the mirror block is 7 - k.
         // Half c of row t sits in 16-byte slot c ^ sw(t) of both blocks, so
         // slot p of A1 pairs with slot 1 - p of A2 (reversed) whatever sw(t)
-        float4 *a2 = reinterpret_cast<float4 *>(st_a(s, 1));
-        float4 *l2 = reinterpret_cast<float4 *>(st_alo(s, 1));
-        const float4 x0 = a1[2 * t], x1 = a1[2 * t + 1], y0 = a2[2 * t], y1 = a2[2 * t + 1];
-        const float4 r0 = make_float4(y1.w, y1.z, y1.y, y1.x), r1 = make_float4(y0.w, y0.z, y0.y, y0.x);
-        const float4 s0 = make_float4(x0.x + r0.x, x0.y + r0.y, x0.z + r0.z, x0.w + r0.w);
-        const float4 s1 = make_float4(x1.x + r1.x, x1.y + r1.y, x1.z + r1.z, x1.w + r1.w);
-        const float4 d0 = sub4(x0, r0), d1 = sub4(x1, r1);
-        float4 h;
-        h = tf32_hi(s0); a1[2 * t] = h; l1[2 * t] = sub4(s0, h);
-        h = tf32_hi(s1); a1[2 * t + 1] = h; l1[2 * t + 1] = sub4(s1, h);
-        h = tf32_hi(d0); a2[2 * t] = h; l2[2 * t] = sub4(d0, h);
-        h = tf32_hi(d1); a2[2 * t + 1] = h; l2[2 * t + 1] = sub4(d1, h);
+        float4 *a2 = reinterpret_cast<float4 *>(st_a(s, 1)) + 2 * t;
+        float4 *l2 = reinterpret_cast<float4 *>(st_alo(s, 1)) + 2 * t;
+        // all four reads before any write: slot p of A2 is read for slot 1 - p
+        float4 xs[2], ys[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          xs[e] = a1[e ^ qsw];
+          ys[e] = a2[1 - (e ^ qsw)];
+        }
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int p = e ^ qsw;
+          const float4 x = xs[e], y = ys[e];
+          const float4 r = make_float4(y.w, y.z, y.y, y.x);
+          const float4 sm = make_float4(x.x + r.x, x.y + r.y, x.z + r.z, x.w + r.w), df = sub4(x, r);
+          float4 h;
+          h = tf32_hi(sm); a1[p] = h; l1[p] = sub4(sm, h);
+          h = tf32_hi(df); a2[p] = h; l2[p] = sub4(df, h);
+        }
       } else {
         for (int hb = 0; hb < G.na; hb++) {
-          float4 *a = reinterpret_cast<float4 *>(st_a(s, hb));
-          float4 *l = reinterpret_cast<float4 *>(st_alo(s, hb));
+          float4 *a = reinterpret_cast<float4 *>(st_a(s, hb)) + 2 * t;
+          float4 *l = reinterpret_cast<float4 *>(st_alo(s, hb)) + 2 * t;
 #pragma unroll
           for (int e = 0; e < 2; e++) {
-            const float4 v = a[2 * t + e], h = tf32_hi(v);
-            a[2 * t + e] = h;
-            l[2 * t + e] = sub4(v, h);
+            const int p = e ^ qsw;
+            const float4 v = a[p], h = tf32_hi(v);
+            a[p] = h;
+            l[p] = sub4(v, h);
           }
         }
       }
@@ -365,18 +406,25 @@ void split_tf32(double x, float &h, float &l) {
   l = (float)(x - (double)h);
 }
 
-// append B[n][k] = T(n, k) (nb x nb, T given as a callable) in the [k/4][n][4]
-// layout to hi/lo
+// The na blocks B_h[n][k] = T(h, n, k) (nb x nb each, T given as a callable)
+// as one array in the order the kernel streams them: for each chunk of KC k
+// values, for each block, its hi part then its lo part, each in the
+// no-swizzle K-major layout [KC/4][nb][4] of one stage
 template <class F>
-void append_block(int nb, F T, std::vector<float> &hi, std::vector<float> &lo) {
-  const size_t o0 = hi.size();
-  hi.resize(o0 + (size_t)nb * nb);
-  lo.resize(o0 + (size_t)nb * nb);
-  for (int n = 0; n < nb; n++)
-    for (int k = 0; k < nb; k++) {
-      const size_t o = o0 + ((size_t)(k / 4) * nb + n) * 4 + (k % 4);
-      split_tf32(T(n, k), hi[o], lo[o]);
-    }
+std::vector<float> chunked(int na, int nb, F T) {
+  std::vector<float> v((size_t)na * 2 * nb * nb);
+  size_t o = 0;
+  for (int c = 0; c < nb / KC; c++)
+    for (int h = 0; h < na; h++)
+      for (int part = 0; part < 2; part++)
+        for (int kq = 0; kq < KC / 4; kq++)
+          for (int n = 0; n < nb; n++)
+            for (int e = 0; e < 4; e++) {
+              float hi, lo;
+              split_tf32(T(h, n, c * KC + kq * 4 + e), hi, lo);
+              v[o++] = part ? lo : hi;
+            }
+  return v;
 }
 
 int upload(eddy_ctx *ctx, const std::vector<float> &h, float **d) {
@@ -434,7 +482,7 @@ int xform_prepare(eddy_ctx *ctx, XformPlan *xp) {
     (sg > 0. ? even : odd).push_back(n);
   }
   if (sym && ((int)even.size() != H || (int)odd.size() != H)) sym = false;
-  std::vector<float> fh, fl, bh, bl;
+  std::vector<float> fm, bm;
   std::vector<double> lp(M);
   int m0 = pp.m0;
   if (sym) {
@@ -445,22 +493,18 @@ int xform_prepare(eddy_ctx *ctx, XformPlan *xp) {
       if (perm[m] == pp.m0) m0 = m;
     }
     // forward: B1[m][x] = Af(even[m], x), B2[m][x] = Af(odd[m], x), x < H
-    append_block(H, [&](int m, int x) { return af(even[m], x); }, fh, fl);
-    append_block(H, [&](int m, int x) { return af(odd[m], x); }, fh, fl);
+    fm = chunked(2, H, [&](int h, int m, int x) { return af((h ? odd : even)[m], x); });
     // backward: B1[x][m] = Ab(x, even[m]), B2[x][m] = Ab(x, odd[m]), x < H
-    append_block(H, [&](int x, int m) { return ab(x, even[m]); }, bh, bl);
-    append_block(H, [&](int x, int m) { return ab(x, odd[m]); }, bh, bl);
+    bm = chunked(2, H, [&](int h, int x, int m) { return ab(x, (h ? odd : even)[m]); });
   } else {
     lp = lam;
-    append_block(M, [&](int n, int x) { return af(n, x); }, fh, fl);
-    append_block(M, [&](int x, int n) { return ab(x, n); }, bh, bl);
+    fm = chunked(1, M, [&](int, int n, int x) { return af(n, x); });
+    bm = chunked(1, M, [&](int, int x, int n) { return ab(x, n); });
   }
   xp->sym = sym ? 1 : 0;
   xp->m0 = m0;
   int rc;
-  if ((rc = upload(ctx, fh, &xp->fhi)) || (rc = upload(ctx, fl, &xp->flo)) || (rc = upload(ctx, bh, &xp->bhi)) ||
-      (rc = upload(ctx, bl, &xp->blo)))
-    return rc;
+  if ((rc = upload(ctx, fm, &xp->fmat)) || (rc = upload(ctx, bm, &xp->bmat))) return rc;
   EDDY_CUDA(cudaMalloc(&xp->lam, sizeof(double) * M));
   EDDY_CUDA(cudaMemcpy(xp->lam, lp.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
   size_t smax = 0;
@@ -473,7 +517,7 @@ int xform_prepare(eddy_ctx *ctx, XformPlan *xp) {
 }
 
 void xform_release(XformPlan *xp) {
-  float *p[] = {xp->fhi, xp->flo, xp->bhi, xp->blo};
+  float *p[] = {xp->fmat, xp->bmat};
   for (float *q : p)
     if (q) cudaFree(q);
   if (xp->lam) cudaFree(xp->lam);
@@ -505,7 +549,7 @@ int launch_xform(eddy_ctx *ctx, const XformPlan *xp, int dir, const float *in, f
   const int nst = xform_stages(mode, M);
   const size_t smem = xform_smem(mode, M);
   const unsigned grid = (unsigned)((P + 127) / 128);
-  k_xform_tf32<<<grid, XT, smem, ctx->stream>>>(*mp, dir ? xp->bhi : xp->fhi, dir ? xp->blo : xp->flo, out, P, M,
+  k_xform_tf32<<<grid, XT, smem, ctx->stream>>>(*mp, dir ? xp->bmat : xp->fmat, out, P, M,
                                                 mode, nst, ctx->err_flag);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;

@@ -29,11 +29,15 @@ def _compatible_rhs(o, w, seed=7):
     return d
 
 
-@pytest.mark.parametrize("sweeps,mx", [(1, 24), (2, 24), (3, 24), (1, 32), (2, 48)])
-def test_refined_poisson(oracle, product, sweeps, mx):
+@pytest.mark.parametrize("sweeps,mx,xlim", [(1, 24, None), (2, 24, None), (3, 24, None), (1, 32, None),
+                                           (2, 48, None), (2, 64, None), (2, 128, None), (2, 64, (-3.0, 5.0)),
+                                           (2, 96, (-3.0, 5.0))])
+def test_refined_poisson(oracle, product, sweeps, mx, xlim):
     # mx = 24: FP32 transforms by cuBLAS SGEMM (M not a multiple of 16);
-    # mx = 32, 48: 3xTF32 transforms on the tensor cores
-    w = config.small(mx=mx, ly=16, nz_=20, beta=2.5)
+    # mx >= 32: 3xTF32 transforms on the tensor cores, the even/odd split form
+    # on symmetric grids and the plain form with xlim off centre
+    kw = {} if xlim is None else {"xlim": xlim}
+    w = config.small(mx=mx, ly=16, nz_=20, beta=2.5, **kw)
     o = oracle.OracleSolver(w)
     g = product.Solver(w, precision=MIXED, refine_sweeps=sweeps)
     d = _compatible_rhs(o, w)
@@ -43,9 +47,10 @@ def test_refined_poisson(oracle, product, sweeps, mx):
     res = np.max(np.abs(r)) / np.max(np.abs(inner))
     rr = g.refine_residuals()
     print(f"sweeps={sweeps} final residual {res:.3e} pre-sweep residuals {rr[:sweeps] / np.max(np.abs(inner))}")
-    # the first pre-sweep residual is the FP32 solve's: ~1e-4 relative (an
-    # FP32 solution error of ~1e-7 amplified by the norm of L)
-    assert rr[0] / np.max(np.abs(inner)) < 1e-3
+    # the first pre-sweep residual is the FP32 solve's: 1e-4 to 1e-3 relative
+    # (an FP32 solution error of ~1e-7 amplified by the norm of L, which grows
+    # with the grid's resolution)
+    assert rr[0] / np.max(np.abs(inner)) < 1e-2
     for s in range(1, sweeps):
         assert rr[s] < 1e-2 * rr[s - 1]
     assert res < (1e-9 if sweeps == 1 else 1e-11)
