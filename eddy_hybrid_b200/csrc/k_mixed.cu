@@ -50,8 +50,9 @@ struct MixedState {
   float *twr = nullptr, *twi = nullptr;  // FFT twiddles: forward table then backward table
   double *resid = nullptr;               // max |r| before each sweep (device, 4 entries)
   double *wout = nullptr;                // outlet-face w (NX,NY) in FP64: exact mass balance
-  // 3xTF32 tensor-core transforms (null fhi: FP32 cuBLAS GEMMs with the plan's matrices)
+  // 3xTF32 tensor-core transforms (null fmat: FP32 cuBLAS GEMMs with the plan's matrices)
   XformPlan xp;
+  float *cpz = nullptr;  // z-line c' of every (m, J) line (M*L*N, FP32), computed once per plan
 };
 
 MixedState *ms(eddy_ctx *ctx) { return static_cast<MixedState *>(ctx->mixed); }
@@ -751,9 +752,9 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
     const int m0 = x->xp.fmat ? x->xp.m0 : pp.m0;
     k_line_mean<float><<<1, 256, 0, ctx->stream>>>(M, L, N, m0, pp.wz, s2, ctx->scal + 5);
     EDDY_LAUNCHED(ctx);
-    float *c32 = reinterpret_cast<float *>(pp.cprime);
-    k_tridiag_lines<float, float><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
-        M, L, N, m0, lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, s2, c32, c32 + (size_t)M * L * N);
+    float *e32 = reinterpret_cast<float *>(pp.cprime);
+    k_tridiag_lines<float, float, 8, true, true><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
+        M, L, N, m0, lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, s2, x->cpz, e32);
     EDDY_LAUNCHED(ctx);
   }
   {
@@ -883,11 +884,22 @@ int mixed_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMemset(x->wout, 0, sizeof(double) * (size_t)d.nx * d.ny));
   EDDY_CUDA(cudaMalloc(&x->resid, 4 * sizeof(double)));
   EDDY_CUDA(cudaMemset(x->resid, 0, 4 * sizeof(double)));
-  // the correction solves keep c' and the forward-eliminated right-hand side
-  // in FP32, side by side in the (FP64-sized) c' buffer
   if (L < 8) {
     ctx->err = "the mixed form needs at least 8 cells along y";
     return EDDY_EINVAL;
+  }
+  // the correction solves keep the forward-eliminated right-hand side in FP32
+  // in the (FP64-sized) c' buffer of the plan and read c' from cpz, computed
+  // here once: it does not depend on the right-hand side
+  {
+    const PoissonPlan &pp = ctx->pp;
+    const long long nl = (long long)pp.M * pp.L;
+    EDDY_CUDA(cudaMalloc(&x->cpz, sizeof(float) * (size_t)nl * pp.N));
+    const double *lam = x->xp.fmat ? x->xp.lam : pp.lam;
+    const int m0 = x->xp.fmat ? x->xp.m0 : pp.m0;
+    k_tridiag_cprime<float><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(pp.M, pp.L, pp.N, m0, lam, pp.ak,
+                                                                                  pp.an, pp.bn, pp.cn, x->cpz);
+    EDDY_LAUNCHED(ctx);
   }
   size_t smem = fft32_smem(L);
   if (smem > 48 * 1024) {
@@ -908,7 +920,7 @@ void mixed_release(eddy_ctx *ctx) {
   MixedState *x = ms(ctx);
   if (!x) return;
   float *fl[] = {x->uo, x->vo, x->wo, x->p, x->tv, x->kv, x->us, x->vs,
-                 x->ws, x->ua, x->va, x->wa, x->dens, x->dens_alt, x->rha, x->mbuf, x->twr, x->twi};
+                 x->ws, x->ua, x->va, x->wa, x->dens, x->dens_alt, x->rha, x->mbuf, x->twr, x->twi, x->cpz};
   for (float *p : fl) if (p) cudaFree(p);
   if (x->resid) cudaFree(x->resid);
   if (x->wout) cudaFree(x->wout);

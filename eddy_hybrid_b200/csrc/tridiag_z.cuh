@@ -39,13 +39,40 @@ __global__ void k_line_mean(int M, int L, int N, int m0, const double *__restric
   if (threadIdx.x == 0) out[0] = s1[0] / s2[0];
 }
 
+// c'(k) of every line alone: the eliminated upper diagonal depends only on
+// the line's shift and the z coefficients, not on the right-hand side, so a
+// solve that reads it from here (PC below) does not store it.  Same
+// arithmetic as the elimination in k_tridiag_lines.
+template <class C>
+__global__ void __launch_bounds__(128)
+    k_tridiag_cprime(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
+                     const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
+                     C *__restrict__ cpr) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)M * L) return;
+  const int mi = (int)(t % M), J = (int)(t / M);
+  const long long ML = (long long)M * L;
+  const int s0 = (J == 0 && mi == m0) ? 1 : 0;
+  const double shift = lam[mi] - ak[J];
+  double pc = 0.;
+  for (int k = s0; k < N; k++) {
+    const double a = (k == s0) ? 0. : an[k];
+    const double rden = 1.0 / ((bn[k] + shift) - a * pc);
+    const double c = cn[k] * rden;
+    cpr[t + ML * k] = (C)c;
+    pc = c;
+  }
+}
+
 // DB: issue the next chunk's loads before the current chunk's recurrence (two
-// register buffers; pays off with FP32 storage, the FP64 form keeps one)
-template <class G, class C = double, int ZC = 8, bool DB = true>
+// register buffers; pays off with FP32 storage, the FP64 form keeps one).
+// PC: c' comes precomputed (k_tridiag_cprime) in cpr, which the elimination
+// then only reads; otherwise the elimination writes it there.
+template <class G, class C = double, int ZC = 8, bool DB = true, bool PC = false>
 __global__ void __launch_bounds__(128)
     k_tridiag_lines(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
                     const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
-                    const double *__restrict__ cmean, G *g, C *__restrict__ cpr, C *dd) {
+                    const double *__restrict__ cmean, G *g, C *cpr, C *dd) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)M * L) return;
   const int mi = (int)(t % M), J = (int)(t / M);
@@ -71,7 +98,7 @@ __global__ void __launch_bounds__(128)
         const double rden = 1.0 / ((bn[k] + shift) - a * pc);
         const double c = cn[k] * rden;
         const double e = (((double)f[q] - cm) - a * pd) * rden;
-        cpr[t + ML * k] = (C)c;
+        if (!PC) cpr[t + ML * k] = (C)c;
         dd[t + ML * k] = (C)e;
         pc = c;
         pd = e;
