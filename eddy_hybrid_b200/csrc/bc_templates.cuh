@@ -28,6 +28,34 @@ __global__ void k_fill_plane(Dims d, int pitch, T *a, int axis, int dst, int src
   a[qd] = zero ? T(0) : sgn * a[qs];
 }
 
+// up to FQ_MAX plane fills along one axis in one launch; the fills of a batch
+// are independent (no fill reads or writes a plane another one writes in the
+// same array), so one thread per in-plane position applies all of them
+constexpr int FQ_MAX = 8;
+template <class T>
+struct FillBatch {
+  T *a[FQ_MAX];
+  int dst[FQ_MAX], src[FQ_MAX], zero[FQ_MAX];
+  T sgn[FQ_MAX];
+  int n;
+};
+
+template <class T>
+__global__ void k_fill_planes(Dims d, int pitch, int axis, FillBatch<T> B) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int n1 = axis == 0 ? d.ny : d.nx;
+  int n2 = axis == 2 ? d.ny : d.nz;
+  if (t >= n1 * n2) return;
+  int a1 = 1 + t % n1, a2 = 1 + t / n1;
+  for (int o = 0; o < B.n; o++) {
+    long long qd, qs;
+    if (axis == 0) { qd = pidx(d, pitch, B.dst[o], a1, a2); qs = pidx(d, pitch, B.src[o], a1, a2); }
+    else if (axis == 1) { qd = pidx(d, pitch, a1, B.dst[o], a2); qs = pidx(d, pitch, a1, B.src[o], a2); }
+    else { qd = pidx(d, pitch, a1, a2, B.dst[o]); qs = pidx(d, pitch, a1, a2, B.src[o]); }
+    B.a[o][qd] = B.zero[o] ? T(0) : B.sgn[o] * B.a[o][qs];
+  }
+}
+
 // flux through the z plane k: sum over interior (i,j) of a/(ap bp) and of
 // the areas, FP64; FLUXB blocks write partial sums, one warp adds them in a
 // fixed order (deterministic)
@@ -174,6 +202,47 @@ int bc_fill(eddy_ctx *ctx, int pitch, T *a, int axis, int dst, int src, double s
   return EDDY_OK;
 }
 
+// Plane fills in their given order, batched: consecutive fills along the same
+// axis share one launch until a fill would touch a plane that a queued fill of
+// the same array writes (or write one a queued fill reads), the axis changes
+// or the batch is full.  Every batch is independent inside, so the result is
+// that of the fills one after another.  flush() before anything else that
+// reads or writes the arrays is launched.
+template <class T>
+struct FillQueue {
+  eddy_ctx *ctx;
+  int pitch;
+  int axis = -1;
+  bct::FillBatch<T> b{};
+  FillQueue(eddy_ctx *c, int p) : ctx(c), pitch(p) { b.n = 0; }
+  int flush() {
+    if (b.n == 0) return EDDY_OK;
+    const Dims &d = ctx->d;
+    int n = axis == 0 ? d.ny * d.nz : (axis == 1 ? d.nx * d.nz : d.nx * d.ny);
+    bct::k_fill_planes<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(d, pitch, axis, b);
+    EDDY_LAUNCHED(ctx);
+    b.n = 0;
+    axis = -1;
+    return EDDY_OK;
+  }
+  int add(T *a, int ax, int dst, int src, double sgn, int zero) {
+    bool conflict = (axis >= 0 && ax != axis) || b.n == bct::FQ_MAX;
+    for (int o = 0; o < b.n && !conflict; o++)
+      if (b.a[o] == a && (b.dst[o] == dst || (!zero && b.dst[o] == src) || (!b.zero[o] && b.src[o] == dst)))
+        conflict = true;
+    if (conflict)
+      if (int rc = flush()) return rc;
+    axis = ax;
+    b.a[b.n] = a;
+    b.dst[b.n] = dst;
+    b.src[b.n] = src;
+    b.sgn[b.n] = (T)sgn;
+    b.zero[b.n] = zero;
+    b.n++;
+    return EDDY_OK;
+  }
+};
+
 // plane flux (out[0] flux, out[1] area) of the z plane k of `a`; partial
 // sums in ctx->scal + 32
 template <class T>
@@ -191,8 +260,9 @@ template <class T>
 int bc_boundary(eddy_ctx *ctx, int pitch, T *u, T *v, T *w) {
   const Dims &d = ctx->d;
   int rc;
+  FillQueue<T> q(ctx, pitch);
 #define F(...) \
-  if ((rc = bc_fill<T>(ctx, pitch, __VA_ARGS__)) != EDDY_OK) return rc
+  if ((rc = q.add(__VA_ARGS__)) != EDDY_OK) return rc
   for (int ib = 1; ib <= 6; ib++) {
     int t = d.itype[ib];
     if (t == 50 || t == 60) {
@@ -219,7 +289,7 @@ int bc_boundary(eddy_ctx *ctx, int pitch, T *u, T *v, T *w) {
     F(u, 1, d.ny, d.jy1, 1., 0); F(v, 1, d.ny, d.jy1, 1., 0); F(w, 1, d.ny, d.jy1, 1., 0);
   }
 #undef F
-  return EDDY_OK;
+  return q.flush();
 }
 
 // BOUNDINOUT (src/boundary.f:505-994) for inlet 305 and outlets 710/730;
@@ -280,8 +350,9 @@ template <class T>
 int bc_boundinoutd_dens(eddy_ctx *ctx, int pitch, T *dens) {
   const Dims &d = ctx->d;
   int rc;
+  FillQueue<T> q(ctx, pitch);
 #define F(...) \
-  if ((rc = bc_fill<T>(ctx, pitch, __VA_ARGS__)) != EDDY_OK) return rc
+  if ((rc = q.add(__VA_ARGS__)) != EDDY_OK) return rc
   if (d.itype[5] == 305) {
     bct::k_dens_inlet<T><<<(d.nx * d.ny + 255) / 256, 256, 0, ctx->stream>>>(d, pitch, dens, ctx->f[EDDY_PLANED]);
     EDDY_LAUNCHED(ctx);
@@ -303,7 +374,7 @@ int bc_boundinoutd_dens(eddy_ctx *ctx, int pitch, T *dens) {
   if (d.itype[3] == 500) { F(dens, 1, 1, d.jy2, 1., 0); F(dens, 1, d.ny, d.jy1, 1., 0); }
   if (d.itype[5] == 500) { F(dens, 2, 1, d.kz2, 1., 0); F(dens, 2, d.nz, d.kz1, 1., 0); }
 #undef F
-  return EDDY_OK;
+  return q.flush();
 }
 
 }  // namespace

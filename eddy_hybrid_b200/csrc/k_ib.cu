@@ -1161,13 +1161,18 @@ int scan_launch(eddy_ctx *ctx, int n, const int *cnt, int *start, int *cursor, i
   return EDDY_OK;
 }
 
+// Growth of the buffers sized by the body's current forcing points: half again
+// the need, so a body that moves does not reallocate every step (cudaFree
+// synchronises the whole device and drains the main stream's queue)
+inline size_t grown(size_t need) { return need + need / 2 + 64; }
+
 // a persistent int scratch buffer of at least `need` entries
 int *scratch(eddy_ctx *ctx, IbState *s, int which, size_t need) {
   if (need > s->si_cap[which]) {
     if (s->si[which]) cudaFree(s->si[which]);
     s->si[which] = nullptr;
     s->si_cap[which] = 0;
-    size_t cap = need + need / 2 + 64;
+    size_t cap = grown(need);
     if (cudaMalloc(&s->si[which], sizeof(int) * cap) != cudaSuccess) {
       ctx->err = "immersed-body scratch allocation failed";
       return nullptr;
@@ -1182,7 +1187,7 @@ double *scratch_d(eddy_ctx *ctx, IbState *s, size_t need) {
     if (s->sxn) cudaFree(s->sxn);
     s->sxn = nullptr;
     s->sxn_cap = 0;
-    size_t cap = need + need / 2 + 64;
+    size_t cap = grown(need);
     if (cudaMalloc(&s->sxn, sizeof(double) * cap) != cudaSuccess) {
       ctx->err = "immersed-body scratch allocation failed";
       return nullptr;
@@ -1195,8 +1200,11 @@ double *scratch_d(eddy_ctx *ctx, IbState *s, size_t need) {
 int ensure(eddy_ctx *ctx, int **p, int &cap, int need) {
   if (need <= cap) return EDDY_OK;
   if (*p) cudaFree(*p);
-  EDDY_CUDA(cudaMalloc(p, sizeof(int) * need));
-  cap = need;
+  *p = nullptr;
+  cap = 0;
+  const size_t c = grown((size_t)need);
+  EDDY_CUDA(cudaMalloc(p, sizeof(int) * c));
+  cap = (int)c;
   return EDDY_OK;
 }
 
@@ -1238,8 +1246,11 @@ int build_bins(eddy_ctx *ctx, Bins &b, int dims, const double *lo, const double 
   EDDY_CUDA(cudaStreamSynchronize(st));
   if (total > b.cap) {
     if (b.items) cudaFree(b.items);
-    EDDY_CUDA(cudaMalloc(&b.items, sizeof(int) * (size_t)(total + 1)));
-    b.cap = total;
+    b.items = nullptr;
+    b.cap = 0;
+    const size_t c = grown((size_t)total + 1);
+    EDDY_CUDA(cudaMalloc(&b.items, sizeof(int) * c));
+    b.cap = (int)(c - 1);
   }
   b.nitems = total;
   if (tri2d)
@@ -1345,13 +1356,17 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   if (nv > S.cap) {
     void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu};
     for (void *p : ptrs) if (p) cudaFree(p);
-    EDDY_CUDA(cudaMalloc(&S.ijk, sizeof(int) * 3 * nv));
-    EDDY_CUDA(cudaMalloc(&S.dijk, sizeof(int) * 3 * nv));
-    EDDY_CUDA(cudaMalloc(&S.lev, sizeof(int) * nv));
-    EDDY_CUDA(cudaMalloc(&S.indx, sizeof(int) * 2 * nv));
-    EDDY_CUDA(cudaMalloc(&S.xn, sizeof(double) * 3 * nv));
-    EDDY_CUDA(cudaMalloc(&S.lu, sizeof(double) * 4 * nv));
-    S.cap = nv;
+    S.ijk = S.dijk = S.lev = S.indx = nullptr;
+    S.xn = S.lu = nullptr;
+    S.cap = 0;
+    const size_t c = grown((size_t)nv);
+    EDDY_CUDA(cudaMalloc(&S.ijk, sizeof(int) * 3 * c));
+    EDDY_CUDA(cudaMalloc(&S.dijk, sizeof(int) * 3 * c));
+    EDDY_CUDA(cudaMalloc(&S.lev, sizeof(int) * c));
+    EDDY_CUDA(cudaMalloc(&S.indx, sizeof(int) * 2 * c));
+    EDDY_CUDA(cudaMalloc(&S.xn, sizeof(double) * 3 * c));
+    EDDY_CUDA(cudaMalloc(&S.lu, sizeof(double) * 4 * c));
+    S.cap = (int)c;
   }
   if (nv > 0) {
     const int nbl = (n + CB - 1) / CB;
