@@ -630,8 +630,11 @@ __device__ int knn_warp(const Bins &b, const int *bstart, const int *bitems, con
 // is sorted by a warp bitonic network, and the cube is accepted once the k-th
 // distance is inside it (d_k < (R h)^2) or it spans the whole bin grid.
 // Returns the number found, or -1 when the candidates overflow the buffers
-// (the caller then uses knn_warp).
-constexpr int KCAP = 2048, KSEL = 128, NHB = 64;
+// (the caller then uses knn_warp).  KCAP: the 27-bin cube around a point
+// next to a finely triangulated body holds a few hundred centroids; 1024
+// candidates (4 KB per warp) cover it while halving the shared memory of a
+// block against 2048.
+constexpr int KCAP = 1024, KSEL = 128, NHB = 64;
 struct KnnSmem {
   int id[KCAP];
   double sd[KSEL];
