@@ -6,7 +6,9 @@
 // stored as G (double for the plain form, float for the mixed form's
 // correction solves); the eliminated coefficients c' and right-hand side dd
 // as C (FP64 in the plain form; FP32 in the mixed form, whose solves feed an
-// FP64-residual refinement and need only FP32 accuracy).
+// FP64-residual refinement and need only FP32 accuracy).  The mixed form
+// reads c' from a table computed once per plan (k_tridiag_cprime) instead of
+// writing it in every solve.
 // The singular line (J = 0, m = m0, the constant x mode) is made compatible by
 // removing its z-volume-weighted mean (computed by k_line_mean) and pinned by
 // dropping its first equation; its first entry is set to zero.
