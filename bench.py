@@ -380,7 +380,7 @@ def main():
             g2.upload(n, pinned[n][1])
         g2.step(1)
         for n in io:
-            pinned[n][1][...] = g2.download(n)
+            g2.download(n, out=pinned[n][1])
     e3.record(s2)
     e3.synchronize()
     ems = e2.elapsed_time(e3)

@@ -195,9 +195,18 @@ class Solver:
         a = np.asfortranarray(a, dtype=np.float64)
         self._check(lib().eddy_upload(self.h, FID[name], _ptr(a)), "eddy_upload")
 
-    def download(self, name: str) -> np.ndarray:
+    def download(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """Copy field `name` to the host.  `out`: optional preallocated
+        Fortran-ordered float64 array of the field's shape (for example a view
+        of pinned memory, which the copy then reaches at full link speed);
+        a new array otherwise."""
         shape = self.shape[:2] if name.startswith("plane") else self.shape
-        a = np.zeros(shape, order="F")
+        if out is None:
+            a = np.zeros(shape, order="F")
+        else:
+            if out.dtype != np.float64 or tuple(out.shape) != tuple(shape) or not out.flags.f_contiguous:
+                raise ValueError(f"download({name!r}): out must be a Fortran-ordered float64 array of shape {shape}")
+            a = out
         self._check(lib().eddy_download(self.h, FID[name], _ptr(a)), "eddy_download")
         return a
 

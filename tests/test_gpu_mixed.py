@@ -104,3 +104,9 @@ def test_mixed_upload_download_roundtrip(product):
             np.testing.assert_array_equal(b, a)
         else:
             np.testing.assert_array_equal(b, a.astype(np.float32).astype(np.float64))
+        # the same copy into a caller's buffer
+        out = np.empty((w.nx, w.ny, w.nz), order="F")
+        assert g.download(n, out=out) is out
+        np.testing.assert_array_equal(out, b)
+    with pytest.raises(ValueError):
+        g.download("uo", out=np.empty((w.nx, w.ny, w.nz)))  # C order
