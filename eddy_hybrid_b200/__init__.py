@@ -99,6 +99,7 @@ SIGNATURES = {
                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "eddy_profile_enable": ([C.c_void_p, C.c_uint], C.c_int),
     "eddy_profile_read": ([C.c_void_p, _DP, C.POINTER(C.c_longlong)], C.c_int),
+    "eddy_selftest_wait_bound": ([C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "eddy_max_divergence_noalloc": ([C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "eddy_umma_gemm_bf16": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, _FP, C.c_int], C.c_int),

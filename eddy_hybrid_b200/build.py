@@ -25,6 +25,7 @@ UNITS = {
     "k_density.cu": ["-fmad=false"],
     "k_sgs.cu": ["-fmad=false"],
     "k_noalloc.cu": ["-fmad=false"],
+    "k_selftest.cu": [],
     "k_mlp.cu": [],
     "k_mixed.cu": [],
     "k_xform.cu": [],

@@ -46,10 +46,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait: returns false after `limit` unsuccessful polls
+// bounded wait: returns false after `limit` unsuccessful polls or 2 s of
+// wall time (the global timer, read every 256 polls), whichever comes first,
+// so a wait that cannot complete ends in bounded time whatever the length of
+// one suspended poll
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = (1u << 24)) {
-  for (uint32_t it = 0; it < limit; ++it)
+  if (mbar_try_wait(bar, parity)) return true;
+  uint64_t t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (uint32_t it = 1; it < limit; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0) {
+      uint64_t t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      if (t - t0 > 2000000000ull) return false;
+    }
+  }
   return false;
 }
 

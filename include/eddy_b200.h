@@ -207,6 +207,14 @@ int eddy_max_divergence_noalloc(int nx, int ny, int nz, const double *u, const d
                                 const double *w, const double *ap, const double *bp,
                                 const double *cp, double *out, void *stream);
 
+/* Diagnostic, no counterpart in the reference: one thread of a kernel waits
+ * on a barrier that nothing ever completes, through the bounded wait that all
+ * of this library's kernels use; *gave_up = 1 when the wait returned without
+ * the barrier completing (it should: every wait gives up after 2 s of wall
+ * time), *seconds = how long it waited.  Allocates 16 bytes of device memory
+ * for the result; takes about 2 s. */
+int eddy_selftest_wait_bound(int device, int *gave_up, double *seconds);
+
 /* ---- learned closure (tensor-core MLP), no counterpart in the reference's
  * code: it stands in for the dynamic procedure of src/vt.f:172-431 ---- */
 /* Self-test of the BF16 tensor-core GEMM used by the closure's training:
