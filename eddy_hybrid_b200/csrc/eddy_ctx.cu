@@ -827,7 +827,7 @@ int eddy_sync(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMemcpy(&e, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
   if (e) {
     cudaMemset(ctx->err_flag, 0, sizeof(int));
-    ctx->err = "a device-side bounded wait expired (TMA plane pipeline)";
+    ctx->err = "a device-side bounded wait expired (a kernel's barrier wait gave up)";
     return EDDY_ETIMEOUT;
   }
   return EDDY_OK;
