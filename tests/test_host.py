@@ -64,3 +64,16 @@ def test_create_fails_cleanly_without_valid_config(product):
     w.itype = (60, 60, 60, 60, 305, 730)   # y not periodic: refused
     with pytest.raises(product.EddyError):
         product.Solver(w)
+
+
+def test_download_checks_the_callers_buffer_before_copying(product):
+    # a caller's buffer must be a Fortran-ordered float64 array of the field's
+    # shape; anything else is refused before the library is called (no GPU)
+    s = object.__new__(product.Solver)
+    s.shape = (6, 5, 7)
+    s.h = None
+    for bad in (np.empty((6, 5, 7)),                        # C order
+                np.empty((6, 5, 6), order="F"),             # wrong shape
+                np.empty((6, 5, 7), order="F", dtype=np.float32)):
+        with pytest.raises(ValueError):
+            s.download("uo", out=bad)
