@@ -101,3 +101,62 @@ def test_mass_balance_outflow(oracle):
     qin = (wo[1:-1, 1:-1, 0] * area).sum()
     qout = (wo[1:-1, 1:-1, -2] * area).sum()
     assert abs(qin - qout) < 1e-10 * abs(qin)
+
+
+class _TaylorGreen(config.Workload):
+    """Slip walls in x and z, periodic y, no sponges, no SGS, no density."""
+
+    def params(self):
+        p = super().params()
+        p.update(vspngx1=0, dspngx1=0)
+        return p
+
+
+def _taylor_green(oracle, mx, steps=50, dt=0.01, re=100.0):
+    """Known answer: the decaying Taylor-Green vortex of the reference
+    (src/boundary.f:996-1044, uvel/wvel/pres_taylor_green on 0 < x, y < pi),
+    shifted by pi/2 in x and placed in the x-y plane: u = cos x cos y F,
+    v = sin x sin y F, p = (cos 2y - cos 2x) F^2 / 4, F = exp(-2 nu t), on
+    x in [-pi/2, pi/2] (u = 0 and dv/dx = 0 at the walls: free slip, type
+    60) and y in [-pi, pi] (periodic); uniform in z with w = 0 between slip
+    walls.  Returns the max errors of u and v relative to F, max |w|, the
+    fitted amplitude of u against F, and max |div u|."""
+    import math
+    w = _TaylorGreen("taylor_green", mx=mx, ly=2 * mx, nz_=4, xlim=(-math.pi / 2, math.pi / 2),
+                     ylim=(-math.pi, math.pi), zlim=(-1.0, 1.0), beta=1e-3, re=re, dt=dt, steps=steps,
+                     noise=0.0, isgs=0, idens=0, itype=(60, 60, 500, 500, 60, 60), sphere=False)
+    o = oracle.OracleSolver(w)
+    xu, xc, yv, yc = (o.grid.get(n) for n in ("xu", "xc", "yv", "yc"))
+    sh = (w.nx, w.ny, w.nz)
+    one = np.ones(sh)
+    U = (np.cos(xu)[:, None] * np.cos(yc)[None, :])[:, :, None] * one
+    V = (np.sin(xc)[:, None] * np.sin(yv)[None, :])[:, :, None] * one
+    P = (0.25 * (np.cos(2 * yc)[None, :] - np.cos(2 * xc)[:, None]))[:, :, None] * one
+    z2 = np.zeros(sh[:2], order="F")
+    o.load_initial(dict(uo=np.asfortranarray(U), vo=np.asfortranarray(V), wo=np.zeros(sh, order="F"),
+                        p=np.asfortranarray(P), dens=np.zeros(sh, order="F"),
+                        planeU=z2, planeV=z2, planeW=z2, planeD=z2))
+    o.initialize()
+    o.step(steps)
+    F = math.exp(-2.0 * steps * dt / re)
+    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
+    u, v, ww = o.get("uo"), o.get("vo"), o.get("wo")
+    eu = float(np.max(np.abs(u[inner] - F * U[inner]))) / F
+    ev = float(np.max(np.abs(v[inner] - F * V[inner]))) / F
+    amp = float(np.sum(u[inner] * U[inner]) / np.sum(U[inner] ** 2))
+    return eu, ev, float(np.max(np.abs(ww[inner]))), amp / F, o.max_divergence()
+
+
+def test_taylor_green_decay_known_answer(oracle):
+    # 16 and 32 cells across pi, 50 steps of dt = 0.01 at Re = 100
+    e16 = _taylor_green(oracle, 16)
+    e32 = _taylor_green(oracle, 32)
+    for e in (e16, e32):
+        eu, ev, wmax, amp, div = e
+        assert wmax < 1e-12 and div < 1e-12
+        assert abs(amp - 1.0) < 1e-4          # decay rate exp(-2 nu t)
+    assert e16[0] < 1e-4 and e16[1] < 1e-4    # measured 3.2e-5
+    assert e32[0] < 2.5e-5 and e32[1] < 2.5e-5
+    # second order in space: the error falls by 4 when the spacing halves
+    for a in (0, 1):
+        assert 3.5 < e16[a] / e32[a] < 4.5, (e16[a], e32[a])
