@@ -207,6 +207,8 @@ class Solver:
         else:
             if out.dtype != np.float64 or tuple(out.shape) != tuple(shape) or not out.flags.f_contiguous:
                 raise ValueError(f"download({name!r}): out must be a Fortran-ordered float64 array of shape {shape}")
+            if not out.flags.writeable:
+                raise ValueError(f"download({name!r}): out is read-only")
             a = out
         self._check(lib().eddy_download(self.h, FID[name], _ptr(a)), "eddy_download")
         return a

@@ -223,8 +223,7 @@ void free_all(eddy_ctx *ctx) {
                   m.dfxu, m.dfxw, m.dfxul, m.dfxwl, m.dfxd, m.dfxdl, m.dens_bg};
   for (double *p : mp) if (p) cudaFree(p);
   for (int f = 0; f < EDDY_NFIELDS; f++) if (ctx->f[f]) cudaFree(ctx->f[f]);
-  double *o[] = {ctx->dens_alt, ctx->uc, ctx->vc, ctx->wc, ctx->sij, ctx->gs, ctx->mm, ctx->lm, ctx->dxdydz,
-                 ctx->ilm2, ctx->imm2, ctx->scal};
+  double *o[] = {ctx->dens_alt, ctx->gs, ctx->dxdydz, ctx->ilm2, ctx->imm2, ctx->scal};
   for (double *p : o) if (p) cudaFree(p);
   if (ctx->err_flag) cudaFree(ctx->err_flag);
   poisson_plan_destroy(ctx);
@@ -371,13 +370,11 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
     if (cudaMalloc(&ctx->f[f], b) != cudaSuccess) return fail(EDDY_ENOMEM, "device allocation failed");
     cudaMemset(ctx->f[f], 0, b);
   }
-  double **o[] = {&ctx->dens_alt, &ctx->uc, &ctx->vc, &ctx->wc, &ctx->gs, &ctx->mm, &ctx->lm, &ctx->dxdydz};
+  double **o[] = {&ctx->dens_alt, &ctx->gs, &ctx->dxdydz};
   for (double **pp : o) {
     if (cudaMalloc(pp, n3) != cudaSuccess) return fail(EDDY_ENOMEM, "device allocation failed");
     cudaMemset(*pp, 0, n3);
   }
-  if (cudaMalloc(&ctx->sij, 6 * n3) != cudaSuccess) return fail(EDDY_ENOMEM, "device allocation failed");
-  cudaMemset(ctx->sij, 0, 6 * n3);
   size_t n2xz = sizeof(double) * (size_t)p.nx * p.nz;
   if (cudaMalloc(&ctx->ilm2, n2xz) != cudaSuccess || cudaMalloc(&ctx->imm2, n2xz) != cudaSuccess)
     return fail(EDDY_ENOMEM, "device allocation failed");
@@ -503,7 +500,7 @@ int eddy_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
 int eddy_turvis(eddy_ctx *ctx) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   if (ctx->prm.isgs == 0) return EDDY_OK;
-  int rc = launch_turvis(ctx);
+  int rc = ctx->mixed ? mixed_turvis(ctx) : launch_turvis(ctx);
   if (rc == EDDY_OK && ctx->mixed) rc = mixed_after_sgs(ctx);
   return rc;
 }
@@ -717,7 +714,7 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
         if (closure) {
           rc = launch_closure(ctx, ctx->tv_dyn, ctx->kappa, nullptr);
         } else {
-          rc = launch_turvis(ctx);
+          rc = ctx->mixed ? mixed_turvis(ctx) : launch_turvis(ctx);
         }
         if (rc) return rc;
       }

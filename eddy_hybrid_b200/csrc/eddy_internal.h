@@ -93,9 +93,10 @@ struct eddy_ctx {
   // fields (device, FP64, Fortran layout)
   double *f[EDDY_NFIELDS] = {};
   double *dens_alt = nullptr;  // ping-pong partner of DENS
-  // SGS arrays
-  double *uc = nullptr, *vc = nullptr, *wc = nullptr, *sij = nullptr, *gs = nullptr,
-         *mm = nullptr, *lm = nullptr, *dxdydz = nullptr, *ilm2 = nullptr, *imm2 = nullptr;
+  // dynamic procedure: |S| (NX,NY,NZ), Delta^2 (NX,NY,NZ), y averages of
+  // max(L.M,0) and M.M ((NX,NZ)); the FP32 procedure of the mixed form uses
+  // the same allocations as FP32 storage
+  double *gs = nullptr, *dxdydz = nullptr, *ilm2 = nullptr, *imm2 = nullptr;
   double *scal = nullptr;  // device scalars: [0] pref [1] qin1 [2] qin2 [3] dpm [4] maxdiv; [32, 328) flux partials
   PoissonPlan pp{};
   std::string err;
@@ -188,6 +189,9 @@ int launch_pressure_update(eddy_ctx *ctx);
 int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
 int launch_boundinoutd_dens(eddy_ctx *ctx, double *dens);
 int launch_turvis(eddy_ctx *ctx);
+// FP32 dynamic procedure on FP32 velocities (row pitch px) -> TV (FP64)
+int launch_turvis32(eddy_ctx *ctx, int px, const float *u, const float *v, const float *w, float *gs32,
+                    float *imm32, float *ilm32);
 int launch_filtersize(eddy_ctx *ctx);
 int poisson_plan_create(eddy_ctx *ctx);
 int poisson_plan_destroy(eddy_ctx *ctx);
@@ -266,6 +270,9 @@ int mixed_residuals(eddy_ctx *ctx, double *out, int n);
 // around an eddy-viscosity update: FP64 density for the closure features
 // before, FP32 copies of nu_t / kappa_t after
 int mixed_after_sgs(eddy_ctx *ctx);
+// the eddy viscosity of the mixed form: the dynamic procedure in FP32 on the
+// FP32 velocities (Smagorinsky stays FP64) -> TV
+int mixed_turvis(eddy_ctx *ctx);
 int launch_closure(eddy_ctx *ctx, const double *fallback, double *kappa, unsigned long long *out_of_envelope);
 void mlp_release(eddy_ctx *ctx);
 

@@ -983,6 +983,15 @@ int mixed_after_sgs(eddy_ctx *ctx) {
   return to32(ctx, ctx->prm.closure == 1 ? ctx->kappa : ctx->f[EDDY_TV], x->kv);
 }
 
+int mixed_turvis(eddy_ctx *ctx) {
+  MixedState *x = ms(ctx);
+  if (ctx->prm.isgs != 2) return launch_turvis(ctx);
+  // FP32 scratch lives in the plain procedure's FP64 arrays (|S| holds px*ny*nz
+  // floats in its nx*ny*nz doubles); the two procedures never run at once
+  return launch_turvis32(ctx, x->px, x->uo, x->vo, x->wo, reinterpret_cast<float *>(ctx->gs),
+                         reinterpret_cast<float *>(ctx->imm2), reinterpret_cast<float *>(ctx->ilm2));
+}
+
 int mixed_views(eddy_ctx *ctx, MixedViews *v) {
   MixedState *x = ms(ctx);
   if (!x) return EDDY_EINVAL;

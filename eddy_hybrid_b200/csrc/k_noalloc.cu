@@ -29,9 +29,20 @@ static_assert(EDDY_NOALLOC_MAX_CELLS % kCellsPerBlock == 0, "scratch sizing");
 // these slots.
 static __device__ __align__(256) double g_divmax_partials[kMaxPartials];
 
-constexpr int kMaxDevices = 64;
+// Device address of the scratch array per CUDA context.  A __device__
+// array's address belongs to the context the module was loaded into, so the
+// cache is keyed by the current context (the primary context of a device in
+// the runtime API; a driver-API caller may have made another one current).
+constexpr int kMaxContexts = 64;
 std::mutex g_mu;
-double *g_scratch_addr[kMaxDevices] = {};
+struct ScratchEntry {
+  void *cuctx;
+  double *addr;
+};
+ScratchEntry g_scratch[kMaxContexts] = {};
+int g_nscratch = 0;
+
+typedef int (*CtxGetCurrentFn)(void **);
 
 __global__ void __launch_bounds__(256)
     k_divmax_partial(int nx, int ny, int nz, const double *__restrict__ u, const double *__restrict__ v,
@@ -73,18 +84,36 @@ __global__ void __launch_bounds__(256) k_divmax_final(int nparts, const double *
   if (threadIdx.x == 0) out[0] = sh[0];
 }
 
-// Device address of the scratch array for the current device, looked up once
-// per device (host code cannot use the array's name as a device address).
-int scratch_for_current_device(double **out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EDDY_ECUDA;
+// Look up (once per context) the device address of the scratch array for
+// the context current on this thread; host code cannot use the array's name
+// as a device address.
+int scratch_for_current_context(double **out) {
+  static CtxGetCurrentFn get_ctx = nullptr;
+  static bool resolved = false;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[dev]) {
+  if (!resolved) {
     void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_divmax_partials) != cudaSuccess || !p) return EDDY_ECUDA;
-    g_scratch_addr[dev] = static_cast<double *>(p);
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_ctx = reinterpret_cast<CtxGetCurrentFn>(p);
+    resolved = true;
   }
-  *out = g_scratch_addr[dev];
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return EDDY_ECUDA;
+  // make the device's primary context current if the thread has none yet
+  if (cudaFree(nullptr) != cudaSuccess) return EDDY_ECUDA;
+  void *cuctx = nullptr;
+  if (!get_ctx || get_ctx(&cuctx) != 0 || !cuctx) return EDDY_ECUDA;
+  for (int e = 0; e < g_nscratch; e++)
+    if (g_scratch[e].cuctx == cuctx) {
+      *out = g_scratch[e].addr;
+      return EDDY_OK;
+    }
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_divmax_partials) != cudaSuccess || !p) return EDDY_ECUDA;
+  if (g_nscratch < kMaxContexts) g_scratch[g_nscratch++] = ScratchEntry{cuctx, static_cast<double *>(p)};
+  *out = static_cast<double *>(p);
   return EDDY_OK;
 }
 
@@ -98,8 +127,11 @@ extern "C" int eddy_max_divergence_noalloc(int nx, int ny, int nz, const double 
   long long ncell = (long long)nx * ny * nz;
   if (ncell > (long long)EDDY_NOALLOC_MAX_CELLS) return EDDY_EINVAL;  // beyond the fixed scratch
   double *part = nullptr;
-  int rc = scratch_for_current_device(&part);
+  int rc = scratch_for_current_context(&part);
   if (rc != EDDY_OK) return rc;
+  // a launch error still pending on this thread from earlier work is cleared
+  // here, so the checks below report this entry point's own launches only
+  (void)cudaGetLastError();
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int nparts = (int)((ninner + kCellsPerBlock - 1) / kCellsPerBlock);
   k_divmax_partial<<<nparts, 256, 0, st>>>(nx, ny, nz, u, v, w, ap, bp, cp, ninner, part);

@@ -1,114 +1,117 @@
 // k_sgs.cu -- dynamic eddy viscosity TURVIS (src/vt.f:16-442), Cartesian,
-// y-periodic, y-average branch (vt.f:296-318).
+// y-periodic, y-average branch (vt.f:296-318), z one-sided at both ends.
 //
-//   T0 centred velocities UC,VC,WC over the whole array (vt.f:64-74)
-//   T1 strain S_ij and |S| at interior cells plus the periodic y-ghost rows
-//      (STRAIN vt.f:955-1018, copies vt.f:176-191)
-//   T2 one pass per cell: the 22 test filters (filter3d vt.f:1132-1268, the
-//      x, y, z passes evaluated in the reference's order so the rounding is
-//      the same), M_ij, M_ij M_ij and L_ij M_ij (vt.f:216-290)
-//   T3 clip LM<0 and average MM, LM along y per (i,k) (vt.f:305-316),
-//      BOUNDTURB on the 2-D averages
-//   T4 TV = (ILM/IMM) Delta^2 |S| where IMM > sqrt(eps), >= 0 (vt.f:416-427)
-//      and BOUNDTURB(TV) ghosts.
+// One fused kernel, k_dynamic_march, replaces the reference's sequence of
+// whole-array passes (centring vt.f:64-74, STRAIN vt.f:955-1018, the 22
+// test filters filter3d vt.f:1132-1268, M_ij and L_ij vt.f:216-290, the
+// clipped y averages vt.f:296-318).  A CTA owns a tile of 30 x-columns by
+// KT z-rows and marches along the periodic y axis:
+//   * centred velocities of plane j+1 go into a 3-plane ring in shared memory
+//     (with the x/z halo the strain needs),
+//   * the strain and |S| of plane j are computed per thread (one thread per
+//     (i,k) column of the tile plus a one-cell halo), the x pass of the filter
+//     takes its neighbours by warp shuffles (lanes are x),
+//   * the y pass is accumulated progressively in registers:
+//       Y(j) = (0.25 X(j-1) + 0.5 X(j)) + 0.25 X(j+1),
+//     the reference's operation order, so two partial sums per quantity,
+//   * the completed Y(j-1) goes through shared memory for the z pass
+//     (warps are z rows), then M_ij M_ij and max(L_ij M_ij, 0) are summed
+//     along y in j order and the averages written per (i,k).
+// Every product and sum is the reference's, in the reference's order, so the
+// FP64 instantiation (compiled with -fmad=false) is bit-identical to the
+// separable whole-array passes.  The FP32 instantiation reads the mixed
+// form's FP32 velocities.  Nothing but |S| (for nu_t) and the 2-D averages
+// is written to HBM.
 #include <cmath>
 #include <vector>
 
 #include "eddy_internal.h"
 
-#define A(a, i, j, k) (a)[fidx(d, (i), (j), (k))]
-
 int launch_fill_plane(eddy_ctx *ctx, double *a, int axis, int dst, int src, double sgn, int zero);
 
 namespace {
 
-constexpr int BX = 32, BY = 4, BZ = 2;
+constexpr int TI = 32;      // lanes: x columns ia-1 .. ia+30
+constexpr int TO = 30;      // output columns per tile
+constexpr int KT = 8;       // output z rows per tile
+constexpr int NW = KT + 2;  // warps: z rows ka-1 .. ka+KT
+constexpr int CR = KT + 4;  // centred-velocity ring rows ka-2 .. ka+KT+1
+constexpr int CC = TI + 2;  // centred-velocity ring columns ia-2 .. ia+31
+constexpr int NQ = 22;      // filtered quantities
 
-__global__ void __launch_bounds__(BX *BY *BZ)
-    k_center(Dims d, const double *__restrict__ uo, const double *__restrict__ vo, const double *__restrict__ wo,
-             double *__restrict__ uc, double *__restrict__ vc, double *__restrict__ wc) {
-  int i = 1 + threadIdx.x + blockIdx.x * BX;
-  int j = 1 + threadIdx.y + blockIdx.y * BY;
-  int k = 1 + threadIdx.z + blockIdx.z * BZ;
-  if (i > d.nx || j > d.ny || k > d.nz) return;
-  long long q = fidx(d, i, j, k);
-  // UC
-  if (i >= d.ix1 && i <= d.ix2) uc[q] = 0.5 * (A(uo, i - 1, j, k) + uo[q]);
-  else if (i == 1) uc[q] = 2. * uo[q] - 0.5 * (A(uo, d.ix1 - 1, j, k) + A(uo, d.ix1, j, k));
-  else uc[q] = 2. * A(uo, d.ix2, j, k) - 0.5 * (A(uo, d.ix2 - 1, j, k) + A(uo, d.ix2, j, k));
-  // VC
-  if (j >= d.jy1 && j <= d.jy2) vc[q] = 0.5 * (A(vo, i, j - 1, k) + vo[q]);
-  else if (j == 1) vc[q] = 2. * vo[q] - 0.5 * (A(vo, i, d.jy1 - 1, k) + A(vo, i, d.jy1, k));
-  else vc[q] = 2. * A(vo, i, d.jy2, k) - 0.5 * (A(vo, i, d.jy2 - 1, k) + A(vo, i, d.jy2, k));
-  // WC
-  if (k >= d.kz1 && k <= d.kz2) wc[q] = 0.5 * (A(wo, i, j, k - 1) + wo[q]);
-  else if (k == 1) wc[q] = 2. * wo[q] - 0.5 * (A(wo, i, j, d.kz1 - 1) + A(wo, i, j, d.kz1));
-  else wc[q] = 2. * A(wo, i, j, d.kz2) - 0.5 * (A(wo, i, j, d.kz2 - 1) + A(wo, i, j, d.kz2));
-}
-
-// strain at (i,j,k) interior; sij layout: 6 fields of ncell (xx,yy,zz,xy,xz,yz)
-__global__ void __launch_bounds__(BX *BY *BZ)
-    k_strain(Dims d, DevMetrics m, const double *__restrict__ uc, const double *__restrict__ vc,
-             const double *__restrict__ wc, double *__restrict__ sij, double *__restrict__ gs) {
-  int i = 1 + threadIdx.x + blockIdx.x * BX;
-  int jj = 1 + threadIdx.y + blockIdx.y * BY;
-  int k = 1 + threadIdx.z + blockIdx.z * BZ;
-  if (i < d.ix1 || i > d.ix2 || jj > d.ny || k < d.kz1 || k > d.kz2) return;
-  // periodic y-ghost rows take the value of the mapped interior row
-  int j = jj == 1 ? d.jy2 : (jj == d.ny ? 2 : jj);
-  const int sy = d.nx;
-  const long long sz = (long long)d.nx * d.ny;
-  long long q = fidx(d, i, j, k);
-  const double *au = m.au, *bv = m.bv, *cw = m.cw;
-  double dudxp = au[i] * (uc[q+1] - uc[q]);
-  double dudxm = au[i - 1] * (uc[q] - uc[q-1]);
-  double dudyp = bv[j] * (uc[q+sy] - uc[q]);
-  double dudym = bv[j - 1] * (uc[q] - uc[q-sy]);
-  double dudzp = cw[k] * (uc[q+sz] - uc[q]);
-  double dudzm = cw[k - 1] * (uc[q] - uc[q-sz]);
-  double dvdxp = au[i] * (vc[q+1] - vc[q]);
-  double dvdxm = au[i - 1] * (vc[q] - vc[q-1]);
-  double dvdyp = bv[j] * (vc[q+sy] - vc[q]);
-  double dvdym = bv[j - 1] * (vc[q] - vc[q-sy]);
-  double dvdzp = cw[k] * (vc[q+sz] - vc[q]);
-  double dvdzm = cw[k - 1] * (vc[q] - vc[q-sz]);
-  double dwdxp = au[i] * (wc[q+1] - wc[q]);
-  double dwdxm = au[i - 1] * (wc[q] - wc[q-1]);
-  double dwdyp = bv[j] * (wc[q+sy] - wc[q]);
-  double dwdym = bv[j - 1] * (wc[q] - wc[q-sy]);
-  double dwdzp = cw[k] * (wc[q+sz] - wc[q]);
-  double dwdzm = cw[k - 1] * (wc[q] - wc[q-sz]);
-  double sxx = 0.5 * (dudxp + dudxm);
-  double syy = 0.5 * (dvdyp + dvdym);
-  double szz = 0.5 * (dwdzp + dwdzm);
-  double sxy = 0.25 * (dudyp + dudym + dvdxp + dvdxm);
-  double sxz = 0.25 * (dudzp + dudzm + dwdxp + dwdxm);
-  double syz = 0.25 * (dwdyp + dwdym + dvdzp + dvdzm);
-  long long qo = fidx(d, i, jj, k), n = d.ncell;
-  sij[qo] = sxx; sij[qo + n] = syy; sij[qo + 2 * n] = szz;
-  sij[qo + 3 * n] = sxy; sij[qo + 4 * n] = sxz; sij[qo + 5 * n] = syz;
-  gs[qo] = sqrt(2. * (sxx * sxx + syy * syy + szz * szz) + 4. * (sxy * sxy + syz * syz + sxz * sxz));
-}
-
-// the 22 filtered quantities at one point from the base fields
-struct Base {
-  double uc, vc, wc, g, s[6];
+template <typename T>
+struct MarchSmem {
+  T cen[3][3][CR][CC];  // [plane slot j%3][uc,vc,wc][row][column]
+  T yb[NQ][NW][TI];     // completed y-filtered quantities of one plane
+  T sgb[7][NW][TI];     // |S| and S_ij of plane jy1: the periodic copy in ghost row NY
 };
 
-__device__ __forceinline__ void load_base(const Dims &d, long long q, const double *__restrict__ uc,
-                                          const double *__restrict__ vc, const double *__restrict__ wc,
-                                          const double *__restrict__ gs, const double *__restrict__ sij,
-                                          Base &b) {
-  long long n = d.ncell;
-  b.uc = uc[q]; b.vc = vc[q]; b.wc = wc[q]; b.g = gs[q];
-#pragma unroll
-  for (int c = 0; c < 6; c++) b.s[c] = sij[q + c * n];
+// centred velocities (vt.f:64-74) at (i,j,k), ghost formulas included
+template <typename T>
+__device__ __forceinline__ T cen_u(const Dims &d, int px, const T *__restrict__ u, int i, int j, int k) {
+  long long q = pidx(d, px, i, j, k);
+  if (i >= d.ix1 && i <= d.ix2) return T(0.5) * (u[q - 1] + u[q]);
+  if (i == 1) return T(2.) * u[q] - T(0.5) * (u[pidx(d, px, d.ix1 - 1, j, k)] + u[pidx(d, px, d.ix1, j, k)]);
+  return T(2.) * u[pidx(d, px, d.ix2, j, k)] - T(0.5) * (u[pidx(d, px, d.ix2 - 1, j, k)] + u[pidx(d, px, d.ix2, j, k)]);
+}
+template <typename T>
+__device__ __forceinline__ T cen_v(const Dims &d, int px, const T *__restrict__ v, int i, int j, int k) {
+  if (j >= d.jy1 && j <= d.jy2) return T(0.5) * (v[pidx(d, px, i, j - 1, k)] + v[pidx(d, px, i, j, k)]);
+  if (j == 1)
+    return T(2.) * v[pidx(d, px, i, 1, k)] - T(0.5) * (v[pidx(d, px, i, d.jy1 - 1, k)] + v[pidx(d, px, i, d.jy1, k)]);
+  return T(2.) * v[pidx(d, px, i, d.jy2, k)] - T(0.5) * (v[pidx(d, px, i, d.jy2 - 1, k)] + v[pidx(d, px, i, d.jy2, k)]);
+}
+template <typename T>
+__device__ __forceinline__ T cen_w(const Dims &d, int px, const T *__restrict__ w, int i, int j, int k) {
+  if (k >= d.kz1 && k <= d.kz2) return T(0.5) * (w[pidx(d, px, i, j, k - 1)] + w[pidx(d, px, i, j, k)]);
+  if (k == 1)
+    return T(2.) * w[pidx(d, px, i, j, 1)] - T(0.5) * (w[pidx(d, px, i, j, d.kz1 - 1)] + w[pidx(d, px, i, j, d.kz1)]);
+  return T(2.) * w[pidx(d, px, i, j, d.kz2)] - T(0.5) * (w[pidx(d, px, i, j, d.kz2 - 1)] + w[pidx(d, px, i, j, d.kz2)]);
 }
 
-// order: 0-5 G*S(xx,yy,zz,xy,yz,xz), 6-11 S(xx,yy,zz,xy,yz,xz), 12 G,
-// 13-15 uc,vc,wc, 16-21 uc*uc, vc*vc, wc*wc, uc*vc, vc*wc, uc*wc
-__device__ __forceinline__ double quant(const Base &b, int c) {
-  // S storage order is xx,yy,zz,xy,xz,yz; the reference filters xx,yy,zz,xy,yz,xz
+// STRAIN (vt.f:955-1018) from the seven centred values around a point of each
+// component: c0 centre, then x-, x+, y-, y+, z-, z+.  s: xx,yy,zz,xy,xz,yz.
+template <typename T>
+__device__ __forceinline__ void strain7(const T (&uc)[7], const T (&vc)[7], const T (&wc)[7], T aui, T auim, T bvj,
+                                        T bvjm, T cwk, T cwkm, T (&s)[6], T &g) {
+  T dudxp = aui * (uc[2] - uc[0]);
+  T dudxm = auim * (uc[0] - uc[1]);
+  T dudyp = bvj * (uc[4] - uc[0]);
+  T dudym = bvjm * (uc[0] - uc[3]);
+  T dudzp = cwk * (uc[6] - uc[0]);
+  T dudzm = cwkm * (uc[0] - uc[5]);
+  T dvdxp = aui * (vc[2] - vc[0]);
+  T dvdxm = auim * (vc[0] - vc[1]);
+  T dvdyp = bvj * (vc[4] - vc[0]);
+  T dvdym = bvjm * (vc[0] - vc[3]);
+  T dvdzp = cwk * (vc[6] - vc[0]);
+  T dvdzm = cwkm * (vc[0] - vc[5]);
+  T dwdxp = aui * (wc[2] - wc[0]);
+  T dwdxm = auim * (wc[0] - wc[1]);
+  T dwdyp = bvj * (wc[4] - wc[0]);
+  T dwdym = bvjm * (wc[0] - wc[3]);
+  T dwdzp = cwk * (wc[6] - wc[0]);
+  T dwdzm = cwkm * (wc[0] - wc[5]);
+  s[0] = T(0.5) * (dudxp + dudxm);
+  s[1] = T(0.5) * (dvdyp + dvdym);
+  s[2] = T(0.5) * (dwdzp + dwdzm);
+  s[3] = T(0.25) * (dudyp + dudym + dvdxp + dvdxm);
+  s[4] = T(0.25) * (dudzp + dudzm + dwdxp + dwdxm);
+  s[5] = T(0.25) * (dwdyp + dwdym + dvdzp + dvdzm);
+  g = sqrt(T(2.) * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]) + T(4.) * (s[3] * s[3] + s[5] * s[5] + s[4] * s[4]));
+}
+
+// the base values a point contributes to the 22 filtered quantities
+template <typename T>
+struct Base {
+  T uc, vc, wc, g, s[6];
+};
+
+// quantity c of a base point; order 0-5 G*S(xx,yy,zz,xy,yz,xz), 6-11
+// S(xx,yy,zz,xy,yz,xz), 12 G, 13-15 uc,vc,wc, 16-21 uc*uc, vc*vc, wc*wc,
+// uc*vc, vc*wc, uc*wc (the order of vt.f's filter3d calls)
+template <typename T>
+__device__ __forceinline__ T quant(const Base<T> &b, int c) {
   const int sidx[6] = {0, 1, 2, 3, 5, 4};
   if (c < 6) return b.g * b.s[sidx[c]];
   if (c < 12) return b.s[sidx[c - 6]];
@@ -124,109 +127,224 @@ __device__ __forceinline__ double quant(const Base &b, int c) {
   return b.uc * b.wc;
 }
 
-constexpr int NQ = 22;
-
-__global__ void __launch_bounds__(128)
-    k_dynamic(Dims d, DevMetrics m, const double *__restrict__ uc, const double *__restrict__ vc,
-              const double *__restrict__ wc, const double *__restrict__ gs, const double *__restrict__ sij,
-              const double *__restrict__ dxdydz, double *__restrict__ mm, double *__restrict__ lm,
-              int top_onesided, int bot_onesided) {
-  int i = d.ix1 + threadIdx.x + blockIdx.x * 32;
-  int j = d.jy1 + threadIdx.y + blockIdx.y * 4;
-  int k = d.kz1 + blockIdx.z;
-  if (i > d.ix2 || j > d.jy2) return;
-  // x-pass stencil (vt.f:1156-1169)
-  int xi[3];
-  double wx[3];
-  const double *whx = m.whx, *whz = m.whz;
-  if (i == d.ix1) { xi[0] = d.ix1; xi[1] = d.ix1 + 1; xi[2] = d.ix1 + 2; }
-  else if (i == d.ix2) { xi[0] = d.ix2; xi[1] = d.ix2 - 1; xi[2] = d.ix2 - 2; }
-  else { xi[0] = i - 1; xi[1] = i; xi[2] = i + 1; }
-  wx[0] = whx[i * 3 + 0]; wx[1] = whx[i * 3 + 1]; wx[2] = whx[i * 3 + 2];
-  // z-pass stencil (vt.f:1216-1264)
-  int zk[3];
-  double wz[3] = {whz[k * 3 + 0], whz[k * 3 + 1], whz[k * 3 + 2]};
-  if (k == d.kz1 && bot_onesided) { zk[0] = d.kz1; zk[1] = d.kz1 + 1; zk[2] = d.kz1 + 2; }
-  else if (k == d.kz2 && top_onesided) { zk[0] = d.kz2; zk[1] = d.kz2 - 1; zk[2] = d.kz2 - 2; }
-  else { zk[0] = k - 1; zk[1] = k; zk[2] = k + 1; }
-  const double wy[3] = {0.25, 0.50, 0.25};
-  const long long q0 = fidx(d, i, j, k), nxy = (long long)d.nx * d.ny;
-  double Z[NQ];
-#pragma unroll
-  for (int c = 0; c < NQ; c++) Z[c] = 0.;
-  for (int a = 0; a < 3; a++) {
-    double Y[NQ];
-#pragma unroll
-    for (int c = 0; c < NQ; c++) Y[c] = 0.;
-    for (int b = 0; b < 3; b++) {
-      int jj = j - 1 + b;
-      double X[NQ];
-#pragma unroll
-      for (int c = 0; c < NQ; c++) X[c] = 0.;
-      for (int e = 0; e < 3; e++) {
-        Base bs;
-        load_base(d, q0 + (xi[e] - i) + (long long)(jj - j) * d.nx + (long long)(zk[a] - k) * nxy, uc, vc, wc, gs,
-                  sij, bs);
-#pragma unroll
-        for (int c = 0; c < NQ; c++) {
-          double t = wx[e] * quant(bs, c);
-          X[c] = (e == 0) ? t : X[c] + t;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < NQ; c++) {
-        double t = wy[b] * X[c];
-        Y[c] = (b == 0) ? t : Y[c] + t;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < NQ; c++) {
-      double t = wz[a] * Y[c];
-      Z[c] = (a == 0) ? t : Z[c] + t;
-    }
-  }
-  long long q = fidx(d, i, j, k);
-  const double C = 1.0, R = 6.;
-  double dx = dxdydz[q];
-  double gb = Z[12];
-  double mxx = C * dx * (R * gb * Z[6] - Z[0]);
-  double myy = C * dx * (R * gb * Z[7] - Z[1]);
-  double mzz = C * dx * (R * gb * Z[8] - Z[2]);
-  double mxy = C * dx * (R * gb * Z[9] - Z[3]);
-  double myz = C * dx * (R * gb * Z[10] - Z[4]);
-  double mxz = C * dx * (R * gb * Z[11] - Z[5]);
-  mm[q] = mxx * mxx + myy * myy + mzz * mzz + 2. * (mxy * mxy + myz * myz + mxz * mxz);
-  double uh = Z[13], vh = Z[14], wh = Z[15];
-  double lxx = (Z[16] - uh * uh) * mxx;
-  double lyy = (Z[17] - vh * vh) * myy;
-  double lzz = (Z[18] - wh * wh) * mzz;
-  double lxy = (Z[19] - uh * vh) * mxy;
-  double lyz = (Z[20] - vh * wh) * myz;
-  double lxz = (Z[21] - uh * wh) * mxz;
-  lm[q] = lxx + lyy + lzz + 2. * (lxy + lyz + lxz);
+template <typename T>
+__device__ __forceinline__ T shfl(T v, int src) {
+  return __shfl_sync(0xffffffffu, v, src);
 }
 
-// y averages per (i,k) into 2-D arrays (NX,NZ), summed in j order
-__global__ void k_yavg(Dims d, const double *__restrict__ mm, const double *__restrict__ lm, double *imm2,
-                       double *ilm2) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int mi = d.ix2 - d.ix1 + 1, mk = d.kz2 - d.kz1 + 1;
-  if (t >= mi * mk) return;
-  int i = d.ix1 + t % mi, k = d.kz1 + t / mi;
-  double sm = 0., sl = 0.;
-  for (int j = d.jy1; j <= d.jy2; j++) {
-    long long q = fidx(d, i, j, k);
-    sm += mm[q];
-    double l = lm[q];
-    if (l < 0.) l = 0.;
-    sl += l;
+template <typename T>
+__device__ __forceinline__ Base<T> shfl_base(const Base<T> &b, int src) {
+  Base<T> o;
+  o.uc = shfl(b.uc, src);
+  o.vc = shfl(b.vc, src);
+  o.wc = shfl(b.wc, src);
+  o.g = shfl(b.g, src);
+#pragma unroll
+  for (int c = 0; c < 6; c++) o.s[c] = shfl(b.s[c], src);
+  return o;
+}
+
+// centred velocities of plane j over the ring tile (zero outside the array)
+template <typename T>
+__device__ __forceinline__ void center_plane(const Dims &d, int px, const T *__restrict__ u, const T *__restrict__ v,
+                                             const T *__restrict__ w, int j, int ia, int ka, MarchSmem<T> &sm) {
+  const int slot = j % 3;
+  for (int p = threadIdx.x; p < CR * CC; p += blockDim.x) {
+    int c = p % CC, r = p / CC;
+    int i = ia - 2 + c, k = ka - 2 + r;
+    T a = T(0), b = T(0), e = T(0);
+    if (i >= 1 && i <= d.nx && k >= 1 && k <= d.nz) {
+      a = cen_u(d, px, u, i, j, k);
+      b = cen_v(d, px, v, i, j, k);
+      e = cen_w(d, px, w, i, j, k);
+    }
+    sm.cen[slot][0][r][c] = a;
+    sm.cen[slot][1][r][c] = b;
+    sm.cen[slot][2][r][c] = e;
   }
-  imm2[(i - 1) + d.nx * (k - 1)] = sm / (double)(d.ny - 2);
-  ilm2[(i - 1) + d.nx * (k - 1)] = sl / (double)(d.ny - 2);
+}
+
+// strain of plane j at this thread's (i,k) from the ring (slots of j-1, j, j+1)
+template <typename T>
+__device__ __forceinline__ void strain_at(const Dims &d, const DevMetrics &m, const MarchSmem<T> &sm, int j, int i,
+                                          int k, int lane, int wr, T (&s)[6], T &g) {
+  const int c = lane + 1, r = wr + 1;
+  const int s0 = j % 3, sm1 = (j + 2) % 3, sp1 = (j + 1) % 3;
+  T uc[7], vc[7], wc[7];
+  auto gather = [&](int q, T(&a)[7]) {
+    a[0] = sm.cen[s0][q][r][c];
+    a[1] = sm.cen[s0][q][r][c - 1];
+    a[2] = sm.cen[s0][q][r][c + 1];
+    a[3] = sm.cen[sm1][q][r][c];
+    a[4] = sm.cen[sp1][q][r][c];
+    a[5] = sm.cen[s0][q][r - 1][c];
+    a[6] = sm.cen[s0][q][r + 1][c];
+  };
+  gather(0, uc);
+  gather(1, vc);
+  gather(2, wc);
+  strain7<T>(uc, vc, wc, (T)m.au[i], (T)m.au[i - 1], (T)m.bv[j], (T)m.bv[j - 1], (T)m.cw[k], (T)m.cw[k - 1], s, g);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NW * 32, 1)
+    k_dynamic_march(Dims d, DevMetrics m, int px, const T *__restrict__ u, const T *__restrict__ v,
+                    const T *__restrict__ w, const double *__restrict__ dxdydz, T *__restrict__ gs, int gpitch,
+                    T *__restrict__ imm2, T *__restrict__ ilm2) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  MarchSmem<T> &sm = *reinterpret_cast<MarchSmem<T> *>(smraw);
+  const int lane = threadIdx.x & 31, wr = threadIdx.x >> 5;
+  int ia = d.ix1 + blockIdx.x * TO;
+  if (ia > d.ix2 - TO + 1) ia = d.ix2 - TO + 1;
+  if (ia < d.ix1) ia = d.ix1;
+  int ka = d.kz1 + blockIdx.y * KT;
+  if (ka > d.kz2 - KT + 1) ka = d.kz2 - KT + 1;
+  if (ka < d.kz1) ka = d.kz1;
+  const int i = ia - 1 + lane, k = ka - 1 + wr;
+  const bool inner = i >= d.ix1 && i <= d.ix2 && k >= d.kz1 && k <= d.kz2;  // strain is defined here
+  const bool out = inner && lane >= 1 && lane <= TO && wr >= 1 && wr <= KT;  // this thread owns an output column
+  // x pass (vt.f:1156-1169): interior X = w0 q(i-1) + w1 q(i) + w2 q(i+1);
+  // at ix1 X = w0 q(ix1) + w1 q(ix1+1) + w2 q(ix1+2), at ix2 mirrored
+  const bool xedge = (i == d.ix1) || (i == d.ix2);
+  int srcA, srcB;
+  if (i == d.ix1) { srcA = lane + 1; srcB = lane + 2; }
+  else if (i == d.ix2) { srcA = lane - 1; srcB = lane - 2; }
+  else { srcA = lane - 1; srcB = lane + 1; }
+  srcA = min(max(srcA, 0), 31);
+  srcB = min(max(srcB, 0), 31);
+  T wx0 = T(0), wx1 = T(0), wx2 = T(0);
+  if (i >= 1 && i <= d.nx) { wx0 = (T)m.whx[i * 3]; wx1 = (T)m.whx[i * 3 + 1]; wx2 = (T)m.whx[i * 3 + 2]; }
+  // z pass (vt.f:1216-1264), one-sided at kz1 and kz2 (ITYPE(5), ITYPE(6) > 0)
+  T wz0 = T(0), wz1 = T(0), wz2 = T(0);
+  int zr0 = wr - 1, zr1 = wr, zr2 = wr + 1;
+  if (out) {
+    wz0 = (T)m.whz[k * 3]; wz1 = (T)m.whz[k * 3 + 1]; wz2 = (T)m.whz[k * 3 + 2];
+    if (k == d.kz1) { zr0 = wr; zr1 = wr + 1; zr2 = wr + 2; }
+    else if (k == d.kz2) { zr0 = wr; zr1 = wr - 1; zr2 = wr - 2; }
+  }
+
+  T Ya[NQ], Yb[NQ];  // partial y sums: Ya of plane j-1 (two terms), Yb of plane j (one term)
+  T acc_m = T(0), acc_l = T(0);
+
+  // filtered quantities of this column's plane from its base and its x
+  // neighbours', folded into the y partial sums; returns in Yc the completed
+  // Y of the plane before
+  auto x_and_y = [&](const Base<T> &b, T(&Yc)[NQ]) {
+    Base<T> bA = shfl_base(b, srcA), bB = shfl_base(b, srcB);
+#pragma unroll
+    for (int c = 0; c < NQ; c++) {
+      T q0 = quant(b, c), qA = quant(bA, c), qB = quant(bB, c);
+      T x = xedge ? (wx0 * q0 + wx1 * qA) + wx2 * qB : (wx0 * qA + wx1 * q0) + wx2 * qB;
+      Yc[c] = Ya[c] + T(0.25) * x;
+      Ya[c] = Yb[c] + T(0.50) * x;
+      Yb[c] = T(0.25) * x;
+    }
+  };
+  // z pass of the completed plane j (own row from Yc, the others from shared
+  // memory), M_ij and L_ij (vt.f:216-290), clipped sums in j order
+  auto z_and_ml = [&](const T(&Yc)[NQ], int j) {
+    T Z[NQ];
+#pragma unroll
+    for (int c = 0; c < NQ; c++) {
+      T y0 = zr0 == wr ? Yc[c] : sm.yb[c][zr0][lane];
+      T y1 = zr1 == wr ? Yc[c] : sm.yb[c][zr1][lane];
+      T y2 = sm.yb[c][zr2][lane];
+      Z[c] = (wz0 * y0 + wz1 * y1) + wz2 * y2;
+    }
+    const T C = T(1.0), R = T(6.);
+    T dx = (T)dxdydz[fidx(d, i, j, k)];
+    T gb = Z[12];
+    T mxx = C * dx * (R * gb * Z[6] - Z[0]);
+    T myy = C * dx * (R * gb * Z[7] - Z[1]);
+    T mzz = C * dx * (R * gb * Z[8] - Z[2]);
+    T mxy = C * dx * (R * gb * Z[9] - Z[3]);
+    T myz = C * dx * (R * gb * Z[10] - Z[4]);
+    T mxz = C * dx * (R * gb * Z[11] - Z[5]);
+    T mmv = mxx * mxx + myy * myy + mzz * mzz + T(2.) * (mxy * mxy + myz * myz + mxz * mxz);
+    T uh = Z[13], vh = Z[14], wh = Z[15];
+    T lxx = (Z[16] - uh * uh) * mxx;
+    T lyy = (Z[17] - vh * vh) * myy;
+    T lzz = (Z[18] - wh * wh) * mzz;
+    T lxy = (Z[19] - uh * vh) * mxy;
+    T lyz = (Z[20] - vh * wh) * myz;
+    T lxz = (Z[21] - uh * wh) * mxz;
+    T lmv = lxx + lyy + lzz + T(2.) * (lxy + lyz + lxz);
+    acc_m += mmv;
+    if (lmv < T(0)) lmv = T(0);
+    acc_l += lmv;
+  };
+  auto put_yb = [&](const T(&Yc)[NQ]) {
+#pragma unroll
+    for (int c = 0; c < NQ; c++) sm.yb[c][wr][lane] = Yc[c];
+  };
+
+  // prologue: |S|, S_ij of plane jy2 (the periodic copy in ghost row 1)
+  const int jy1 = d.jy1, jy2 = d.jy2, ny = d.ny;
+  center_plane(d, px, u, v, w, jy2 - 1, ia, ka, sm);
+  center_plane(d, px, u, v, w, jy2, ia, ka, sm);
+  center_plane(d, px, u, v, w, ny, ia, ka, sm);
+  __syncthreads();
+  Base<T> b{};
+  if (inner) strain_at(d, m, sm, jy2, i, k, lane, wr, b.s, b.g);
+  __syncthreads();
+  center_plane(d, px, u, v, w, 1, ia, ka, sm);
+  center_plane(d, px, u, v, w, jy1, ia, ka, sm);
+  __syncthreads();
+  // ghost row 1: centred velocities of row 1, strain of row jy2
+  b.uc = sm.cen[1 % 3][0][wr + 1][lane + 1];
+  b.vc = sm.cen[1 % 3][1][wr + 1][lane + 1];
+  b.wc = sm.cen[1 % 3][2][wr + 1][lane + 1];
+  {
+    T Yc[NQ];
+#pragma unroll
+    for (int c = 0; c < NQ; c++) { Ya[c] = T(0); Yb[c] = T(0); }
+    x_and_y(b, Yc);  // only Yb (first term of Y(jy1)) is kept
+  }
+  for (int j = jy1; j <= jy2; j++) {
+    center_plane(d, px, u, v, w, j + 1, ia, ka, sm);
+    __syncthreads();
+    Base<T> bj{};
+    if (inner) strain_at(d, m, sm, j, i, k, lane, wr, bj.s, bj.g);
+    bj.uc = sm.cen[j % 3][0][wr + 1][lane + 1];
+    bj.vc = sm.cen[j % 3][1][wr + 1][lane + 1];
+    bj.wc = sm.cen[j % 3][2][wr + 1][lane + 1];
+    if (j == jy1) {
+      sm.sgb[0][wr][lane] = bj.g;
+#pragma unroll
+      for (int c = 0; c < 6; c++) sm.sgb[1 + c][wr][lane] = bj.s[c];
+    }
+    if (out) gs[pidx(d, gpitch, i, j, k)] = bj.g;
+    T Yc[NQ];
+    x_and_y(bj, Yc);
+    if (j > jy1) put_yb(Yc);
+    __syncthreads();
+    if (j > jy1 && out) z_and_ml(Yc, j - 1);
+  }
+  // ghost row NY: centred velocities of row NY, strain of row jy1
+  {
+    Base<T> bn{};
+    bn.uc = sm.cen[ny % 3][0][wr + 1][lane + 1];
+    bn.vc = sm.cen[ny % 3][1][wr + 1][lane + 1];
+    bn.wc = sm.cen[ny % 3][2][wr + 1][lane + 1];
+    bn.g = sm.sgb[0][wr][lane];
+#pragma unroll
+    for (int c = 0; c < 6; c++) bn.s[c] = sm.sgb[1 + c][wr][lane];
+    T Yc[NQ];
+    x_and_y(bn, Yc);
+    __syncthreads();  // every z pass of the last loop iteration has read yb
+    put_yb(Yc);
+    __syncthreads();
+    if (out) z_and_ml(Yc, jy2);
+  }
+  if (out) {
+    imm2[(i - 1) + d.nx * (k - 1)] = acc_m / T(d.ny - 2);
+    ilm2[(i - 1) + d.nx * (k - 1)] = acc_l / T(d.ny - 2);
+  }
 }
 
 // BOUNDTURB on a j-independent (NX,NZ) array: x sides then z sides
-__global__ void k_boundturb2(Dims d, double *a, int iflg) {
+template <typename T>
+__global__ void k_boundturb2(Dims d, T *a, int iflg) {
   // single block: the x-side fills, then the z-side fills, in order
   for (int ib = 1; ib <= 6; ib++) {
     int t = d.itype[ib];
@@ -238,7 +356,7 @@ __global__ void k_boundturb2(Dims d, double *a, int iflg) {
       if (t != 0 && t != 500 && t != 300) mode = 2;
     }
     if (!mode || ib == 3 || ib == 4) continue;
-    double sg = mode == 1 ? -1. : 1.;
+    T sg = mode == 1 ? T(-1.) : T(1.);
     if (ib <= 2) {
       int dst = ib == 1 ? 1 : d.nx, src = ib == 1 ? 2 : d.ix2;
       for (int k = 1 + threadIdx.x; k <= d.nz; k += blockDim.x)
@@ -252,84 +370,76 @@ __global__ void k_boundturb2(Dims d, double *a, int iflg) {
   }
 }
 
+// TV = (ILM/IMM) Delta^2 |S| where IMM > sqrt(eps), >= 0 (vt.f:416-427) at
+// interior cells (BOUNDTURB fills the ghosts afterwards)
+template <typename T>
 __global__ void __launch_bounds__(256)
-    k_tv(Dims d, const double *__restrict__ ilm2, const double *__restrict__ imm2,
-         const double *__restrict__ dxdydz, const double *__restrict__ gs, double *__restrict__ tv, double seps) {
+    k_tv(Dims d, const T *__restrict__ ilm2, const T *__restrict__ imm2, const double *__restrict__ dxdydz,
+         const T *__restrict__ gs, int gpitch, double *__restrict__ tv, T seps) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= d.ncell) return;
   int i = 1 + (int)(q % d.nx);
   int k = 1 + (int)(q / ((long long)d.nx * d.ny));
   int j = 1 + (int)((q / d.nx) % d.ny);
   if (i < d.ix1 || i > d.ix2 || j < d.jy1 || j > d.jy2 || k < d.kz1 || k > d.kz2) return;
-  double il = ilm2[(i - 1) + d.nx * (k - 1)], im = imm2[(i - 1) + d.nx * (k - 1)];
-  if (il < 0) il = 0.;
-  double v = 0.;
-  if (im > seps) v = (il / im) * dxdydz[q] * gs[q];
-  if (v < 0.0) v = 0.0;
-  tv[q] = v;
+  T il = ilm2[(i - 1) + d.nx * (k - 1)], im = imm2[(i - 1) + d.nx * (k - 1)];
+  if (il < T(0)) il = T(0);
+  T v = T(0);
+  if (im > seps) v = (il / im) * (T)dxdydz[q] * gs[pidx(d, gpitch, i, j, k)];
+  if (v < T(0)) v = T(0);
+  tv[q] = (double)v;
 }
 
+// Smagorinsky (isgs = 1): TV = css^2 Delta^2 |S| (vt.f:160-168), the strain
+// from the centred velocities of the seven points around each cell
 __global__ void __launch_bounds__(256)
-    k_smag(Dims d, const double *__restrict__ dxdydz, const double *__restrict__ gs, double *__restrict__ tv,
-           double css) {
+    k_smag(Dims d, DevMetrics m, const double *__restrict__ u, const double *__restrict__ v,
+           const double *__restrict__ w, const double *__restrict__ dxdydz, double *__restrict__ tv, double css) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= d.ncell) return;
-  tv[q] = css * css * 1.0 * dxdydz[q] * gs[q];
+  int i = 1 + (int)(q % d.nx);
+  int k = 1 + (int)(q / ((long long)d.nx * d.ny));
+  int j = 1 + (int)((q / d.nx) % d.ny);
+  double g = 0.;
+  if (i >= d.ix1 && i <= d.ix2 && j >= d.jy1 && j <= d.jy2 && k >= d.kz1 && k <= d.kz2) {
+    const int di[7] = {0, -1, 1, 0, 0, 0, 0}, dj[7] = {0, 0, 0, -1, 1, 0, 0}, dk[7] = {0, 0, 0, 0, 0, -1, 1};
+    double uc[7], vc[7], wc[7];
+#pragma unroll
+    for (int p = 0; p < 7; p++) {
+      uc[p] = cen_u(d, d.nx, u, i + di[p], j + dj[p], k + dk[p]);
+      vc[p] = cen_v(d, d.nx, v, i + di[p], j + dj[p], k + dk[p]);
+      wc[p] = cen_w(d, d.nx, w, i + di[p], j + dj[p], k + dk[p]);
+    }
+    double s[6];
+    strain7<double>(uc, vc, wc, m.au[i], m.au[i - 1], m.bv[j], m.bv[j - 1], m.cw[k], m.cw[k - 1], s, g);
+  }
+  tv[q] = css * css * 1.0 * dxdydz[q] * g;
 }
 
-}  // namespace
-
-// FILTERSIZE (vt.f:1096-1127) on the host, same pow as the reference's
-// libm, uploaded once.
-int launch_filtersize(eddy_ctx *ctx) {
+template <typename T>
+int turvis_dynamic(eddy_ctx *ctx, int px, const T *u, const T *v, const T *w, T *gs, T *imm2, T *ilm2) {
   const Dims &d = ctx->d;
-  std::vector<double> dx((size_t)d.ncell);
-  const std::vector<double> &ap = ctx->h[2], &bp = ctx->h[8], &cp = ctx->h[14];
-  const double ppp = 2. / 3.;
-  for (int k = 1; k <= d.nz; k++)
-    for (int j = 1; j <= d.ny; j++)
-      for (int i = 1; i <= d.nx; i++)
-        dx[fidx(d, i, j, k)] = std::pow(std::fabs(1.0) / (ap[i] * bp[j] * cp[k]), ppp);
-  if (d.lp == 0)
-    for (int k = 1; k <= d.nz; k++)
-      for (int i = 1; i <= d.nx; i++) {
-        dx[fidx(d, i, 1, k)] = dx[fidx(d, i, d.ny - 1, k)];
-        dx[fidx(d, i, d.ny, k)] = dx[fidx(d, i, 2, k)];
-      }
-  EDDY_CUDA(cudaMemcpy(ctx->dxdydz, dx.data(), sizeof(double) * dx.size(), cudaMemcpyHostToDevice));
+  cudaStream_t st = ctx->stream;
+  const size_t smem = sizeof(MarchSmem<T>);
+  EDDY_CUDA(cudaFuncSetAttribute(k_dynamic_march<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int mi = d.ix2 - d.ix1 + 1, mk = d.kz2 - d.kz1 + 1;
+  dim3 g((mi + TO - 1) / TO, (mk + KT - 1) / KT);
+  k_dynamic_march<T><<<g, NW * 32, smem, st>>>(d, ctx->m, px, u, v, w, ctx->dxdydz, gs, px, imm2, ilm2);
+  EDDY_LAUNCHED(ctx);
+  k_boundturb2<T><<<1, 256, 0, st>>>(d, ilm2, 0);
+  EDDY_LAUNCHED(ctx);
+  k_boundturb2<T><<<1, 256, 0, st>>>(d, imm2, 1);
+  EDDY_LAUNCHED(ctx);
+  long long nb = (d.ncell + 255) / 256;
+  k_tv<T><<<(unsigned)nb, 256, 0, st>>>(d, ilm2, imm2, ctx->dxdydz, gs, px, ctx->f[EDDY_TV], (T)std::sqrt(ctx->sc.eps));
+  EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
 
-int launch_turvis(eddy_ctx *ctx) {
+// BOUNDTURB(TV,0) (vt.f:700-757)
+int boundturb_tv(eddy_ctx *ctx) {
   const Dims &d = ctx->d;
-  cudaStream_t st = ctx->stream;
-  dim3 blk(BX, BY, BZ), g((d.nx + BX - 1) / BX, (d.ny + BY - 1) / BY, (d.nz + BZ - 1) / BZ);
-  double **f = ctx->f;
-  k_center<<<g, blk, 0, st>>>(d, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], ctx->uc, ctx->vc, ctx->wc);
-  EDDY_LAUNCHED(ctx);
-  k_strain<<<g, blk, 0, st>>>(d, ctx->m, ctx->uc, ctx->vc, ctx->wc, ctx->sij, ctx->gs);
-  EDDY_LAUNCHED(ctx);
-  double *tv = f[EDDY_TV];
-  long long nb = (d.ncell + 255) / 256;
-  if (ctx->prm.isgs == 1) {
-    k_smag<<<(unsigned)nb, 256, 0, st>>>(d, ctx->dxdydz, ctx->gs, tv, ctx->sc.css);
-    EDDY_LAUNCHED(ctx);
-  } else {
-    int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1, mk = d.kz2 - d.kz1 + 1;
-    dim3 g2((mi + 31) / 32, (mj + 3) / 4, mk);
-    k_dynamic<<<g2, dim3(32, 4, 1), 0, st>>>(d, ctx->m, ctx->uc, ctx->vc, ctx->wc, ctx->gs, ctx->sij, ctx->dxdydz,
-                                             ctx->mm, ctx->lm, d.itype[6] > 0, d.itype[5] > 0);
-    EDDY_LAUNCHED(ctx);
-    k_yavg<<<(mi * mk + 255) / 256, 256, 0, st>>>(d, ctx->mm, ctx->lm, ctx->imm2, ctx->ilm2);
-    EDDY_LAUNCHED(ctx);
-    k_boundturb2<<<1, 256, 0, st>>>(d, ctx->ilm2, 0);
-    EDDY_LAUNCHED(ctx);
-    k_boundturb2<<<1, 256, 0, st>>>(d, ctx->imm2, 1);
-    EDDY_LAUNCHED(ctx);
-    k_tv<<<(unsigned)nb, 256, 0, st>>>(d, ctx->ilm2, ctx->imm2, ctx->dxdydz, ctx->gs, tv, std::sqrt(ctx->sc.eps));
-    EDDY_LAUNCHED(ctx);
-  }
-  // BOUNDTURB(TV,0) (vt.f:700-757)
+  double *tv = ctx->f[EDDY_TV];
   int rc;
 #define F(...) \
   if ((rc = launch_fill_plane(ctx, __VA_ARGS__)) != EDDY_OK) return rc
@@ -360,4 +470,53 @@ int launch_turvis(eddy_ctx *ctx) {
   }
 #undef F
   return EDDY_OK;
+}
+
+}  // namespace
+
+// FILTERSIZE (vt.f:1096-1127) on the host, same pow as the reference's
+// libm, uploaded once.
+int launch_filtersize(eddy_ctx *ctx) {
+  const Dims &d = ctx->d;
+  std::vector<double> dx((size_t)d.ncell);
+  const std::vector<double> &ap = ctx->h[2], &bp = ctx->h[8], &cp = ctx->h[14];
+  const double ppp = 2. / 3.;
+  for (int k = 1; k <= d.nz; k++)
+    for (int j = 1; j <= d.ny; j++)
+      for (int i = 1; i <= d.nx; i++)
+        dx[fidx(d, i, j, k)] = std::pow(std::fabs(1.0) / (ap[i] * bp[j] * cp[k]), ppp);
+  if (d.lp == 0)
+    for (int k = 1; k <= d.nz; k++)
+      for (int i = 1; i <= d.nx; i++) {
+        dx[fidx(d, i, 1, k)] = dx[fidx(d, i, d.ny - 1, k)];
+        dx[fidx(d, i, d.ny, k)] = dx[fidx(d, i, 2, k)];
+      }
+  EDDY_CUDA(cudaMemcpy(ctx->dxdydz, dx.data(), sizeof(double) * dx.size(), cudaMemcpyHostToDevice));
+  return EDDY_OK;
+}
+
+// FP64 TURVIS on (UO, VO, WO) -> TV
+int launch_turvis(eddy_ctx *ctx) {
+  const Dims &d = ctx->d;
+  double **f = ctx->f;
+  if (ctx->prm.isgs == 1) {
+    long long nb = (d.ncell + 255) / 256;
+    k_smag<<<(unsigned)nb, 256, 0, ctx->stream>>>(d, ctx->m, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], ctx->dxdydz,
+                                                   f[EDDY_TV], ctx->sc.css);
+    EDDY_LAUNCHED(ctx);
+  } else {
+    int rc = turvis_dynamic<double>(ctx, d.nx, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], ctx->gs, ctx->imm2, ctx->ilm2);
+    if (rc) return rc;
+  }
+  return boundturb_tv(ctx);
+}
+
+// FP32 dynamic procedure on the mixed form's FP32 velocities (row pitch px),
+// the same fused march in single precision; TV (FP64) receives the result.
+// gs32 (px-pitched field) and imm32/ilm32 ((NX,NZ)) are FP32 scratch.
+int launch_turvis32(eddy_ctx *ctx, int px, const float *u, const float *v, const float *w, float *gs32,
+                    float *imm32, float *ilm32) {
+  int rc = turvis_dynamic<float>(ctx, px, u, v, w, gs32, imm32, ilm32);
+  if (rc) return rc;
+  return boundturb_tv(ctx);
 }

@@ -198,9 +198,12 @@ int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts);
  * CP(1:NZ); out: device pointer to one double that receives the result;
  * stream: cudaStream_t (NULL = default stream).  Asynchronous: read out after
  * synchronising the stream.  Returns EDDY_EINVAL when NX*NY*NZ exceeds
- * EDDY_NOALLOC_MAX_CELLS.  The first call on a device looks up the scratch
- * array's device address for that device, so make that first call before any
- * stream capture.  All calls share the one scratch array (each call writes
+ * EDDY_NOALLOC_MAX_CELLS.  The first call in a CUDA context (per device,
+ * the primary context in the runtime API) looks up the scratch array's
+ * device address for that context, so make that first call before any
+ * stream capture.  A launch error left pending on the calling thread by
+ * earlier work is cleared on entry; EDDY_ECUDA reports this call's own
+ * launches.  All calls share the one scratch array (each call writes
  * every slot it reads, so nothing needs clearing): calls that overlap on the
  * GPU race and must be ordered by the caller. */
 int eddy_max_divergence_noalloc(int nx, int ny, int nz, const double *u, const double *v,

@@ -72,8 +72,11 @@ def test_download_checks_the_callers_buffer_before_copying(product):
     s = object.__new__(product.Solver)
     s.shape = (6, 5, 7)
     s.h = None
+    ro = np.empty((6, 5, 7), order="F")
+    ro.flags.writeable = False
     for bad in (np.empty((6, 5, 7)),                        # C order
                 np.empty((6, 5, 6), order="F"),             # wrong shape
-                np.empty((6, 5, 7), order="F", dtype=np.float32)):
+                np.empty((6, 5, 7), order="F", dtype=np.float32),
+                ro):                                        # read-only
         with pytest.raises(ValueError):
             s.download("uo", out=bad)
