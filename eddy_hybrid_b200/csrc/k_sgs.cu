@@ -6,8 +6,10 @@
 // test filters filter3d vt.f:1132-1268, M_ij and L_ij vt.f:216-290, the
 // clipped y averages vt.f:296-318).  A CTA owns a tile of 30 x-columns by
 // KT z-rows and marches along the periodic y axis:
-//   * centred velocities of plane j+1 go into a 3-plane ring in shared memory
-//     (with the x/z halo the strain needs),
+//   * the raw u, v, w tiles of plane j+4 are copied into a 4-plane ring in
+//     shared memory by cp.async while plane j is processed; the centred
+//     velocities of plane j+2 are computed from that ring into a 4-plane ring
+//     of their own (with the x/z halo the strain needs),
 //   * the strain and |S| of plane j are computed per thread (one thread per
 //     (i,k) column of the tile plus a one-cell halo), the x pass of the filter
 //     takes its neighbours by warp shuffles (lanes are x),
@@ -37,14 +39,28 @@ constexpr int KT = 8;       // output z rows per tile
 constexpr int NW = KT + 2;  // warps: z rows ka-1 .. ka+KT
 constexpr int CR = KT + 4;  // centred-velocity ring rows ka-2 .. ka+KT+1
 constexpr int CC = TI + 2;  // centred-velocity ring columns ia-2 .. ia+31
+constexpr int RR = KT + 5;  // raw-velocity ring rows ka-3 .. ka+KT+1
+constexpr int RC = TI + 4;  // raw-velocity ring columns ia-3 .. ia+32
 constexpr int NQ = 22;      // filtered quantities
 
 template <typename T>
 struct MarchSmem {
-  T cen[3][3][CR][CC];  // [plane slot j%3][uc,vc,wc][row][column]
+  T cen[4][3][CR][CC];  // [plane slot j%4][uc,vc,wc][row][column]
+  T raw[4][3][RR][RC];  // [plane slot j%4][u,v,w][row][column]
   T yb[NQ][NW][TI];     // completed y-filtered quantities of one plane
   T sgb[7][NW][TI];     // |S| and S_ij of plane jy1: the periodic copy in ghost row NY
 };
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // centred velocities (vt.f:64-74) at (i,j,k), ghost formulas included
 template <typename T>
@@ -107,48 +123,16 @@ struct Base {
   T uc, vc, wc, g, s[6];
 };
 
-// quantity c of a base point; order 0-5 G*S(xx,yy,zz,xy,yz,xz), 6-11
-// S(xx,yy,zz,xy,yz,xz), 12 G, 13-15 uc,vc,wc, 16-21 uc*uc, vc*vc, wc*wc,
-// uc*vc, vc*wc, uc*wc (the order of vt.f's filter3d calls)
-template <typename T>
-__device__ __forceinline__ T quant(const Base<T> &b, int c) {
-  const int sidx[6] = {0, 1, 2, 3, 5, 4};
-  if (c < 6) return b.g * b.s[sidx[c]];
-  if (c < 12) return b.s[sidx[c - 6]];
-  if (c == 12) return b.g;
-  if (c == 13) return b.uc;
-  if (c == 14) return b.vc;
-  if (c == 15) return b.wc;
-  if (c == 16) return b.uc * b.uc;
-  if (c == 17) return b.vc * b.vc;
-  if (c == 18) return b.wc * b.wc;
-  if (c == 19) return b.uc * b.vc;
-  if (c == 20) return b.vc * b.wc;
-  return b.uc * b.wc;
-}
-
 template <typename T>
 __device__ __forceinline__ T shfl(T v, int src) {
   return __shfl_sync(0xffffffffu, v, src);
-}
-
-template <typename T>
-__device__ __forceinline__ Base<T> shfl_base(const Base<T> &b, int src) {
-  Base<T> o;
-  o.uc = shfl(b.uc, src);
-  o.vc = shfl(b.vc, src);
-  o.wc = shfl(b.wc, src);
-  o.g = shfl(b.g, src);
-#pragma unroll
-  for (int c = 0; c < 6; c++) o.s[c] = shfl(b.s[c], src);
-  return o;
 }
 
 // centred velocities of plane j over the ring tile (zero outside the array)
 template <typename T>
 __device__ __forceinline__ void center_plane(const Dims &d, int px, const T *__restrict__ u, const T *__restrict__ v,
                                              const T *__restrict__ w, int j, int ia, int ka, MarchSmem<T> &sm) {
-  const int slot = j % 3;
+  const int slot = j % 4;
   for (int p = threadIdx.x; p < CR * CC; p += blockDim.x) {
     int c = p % CC, r = p / CC;
     int i = ia - 2 + c, k = ka - 2 + r;
@@ -164,12 +148,63 @@ __device__ __forceinline__ void center_plane(const Dims &d, int px, const T *__r
   }
 }
 
+// raw u, v, w of plane j (2 <= j <= NY-1) over the raw tile into ring slot
+// j%4, 8-byte cp.async copies (FP32 rows start at even elements: ia is even)
+template <typename T>
+__device__ __forceinline__ void issue_raw(const Dims &d, int px, const T *__restrict__ u, const T *__restrict__ v,
+                                          const T *__restrict__ w, int j, int ia, int ka, MarchSmem<T> &sm) {
+  constexpr int EPU = 8 / sizeof(T);  // elements per copy
+  constexpr int UPR = RC / EPU;       // copies per row
+  const int slot = j % 4, i0 = ia - 3, k0 = ka - 3;
+  const int ilim = sizeof(T) == 8 ? d.nx : px;  // last element a copy may touch
+  const bool inside = i0 >= 1 && i0 + RC - 1 <= ilim && k0 >= 1 && k0 + RR - 1 <= d.nz;  // CTA-uniform
+  for (int e = threadIdx.x; e < 3 * RR * UPR; e += blockDim.x) {
+    int uu = e % UPR, rest = e / UPR, rr = rest % RR, q = rest / RR;
+    int i = i0 + uu * EPU, k = k0 + rr;
+    if (!inside && (i < 1 || i + EPU - 1 > ilim || k < 1 || k > d.nz)) continue;
+    const T *src = q == 0 ? u : (q == 1 ? v : w);
+    cp_async8(&sm.raw[slot][q][rr][uu * EPU], src + pidx(d, px, i, j, k));
+  }
+}
+
+// centred velocities (vt.f:64-74) of an interior plane j from the raw ring
+// (slots of j-1 and j); the same formulas and operation order as cen_u/v/w
+template <typename T>
+__device__ __forceinline__ void center_raw(const Dims &d, int j, int ia, int ka, MarchSmem<T> &sm) {
+  const int slot = j % 4, rs = j % 4, rm = (j + 3) % 4, i0 = ia - 3, k0 = ka - 3;
+  auto U = [&](int i, int k) { return sm.raw[rs][0][k - k0][i - i0]; };
+  auto W = [&](int i, int k) { return sm.raw[rs][2][k - k0][i - i0]; };
+  // the ghost formulas apply only in tiles that reach a ghost layer (CTA-uniform)
+  const bool xg = ia - 2 <= 1 || ia + TI - 1 >= d.nx, zg = ka - 2 <= 1 || ka + KT + 1 >= d.nz;
+  for (int p = threadIdx.x; p < CR * CC; p += blockDim.x) {
+    int c = p % CC, r = p / CC;
+    int i = ia - 2 + c, k = ka - 2 + r;
+    // raw-tile coordinates of (i, k), (i-1, k), (i, k-1)
+    int rc = c + 1, rr = r + 1;
+    T a = T(0.5) * (sm.raw[rs][0][rr][rc - 1] + sm.raw[rs][0][rr][rc]);
+    T b = T(0.5) * (sm.raw[rm][1][rr][rc] + sm.raw[rs][1][rr][rc]);
+    T e = T(0.5) * (sm.raw[rs][2][rr - 1][rc] + sm.raw[rs][2][rr][rc]);
+    if (xg) {
+      if (i == 1) a = T(2.) * U(1, k) - T(0.5) * (U(d.ix1 - 1, k) + U(d.ix1, k));
+      else if (i == d.nx) a = T(2.) * U(d.ix2, k) - T(0.5) * (U(d.ix2 - 1, k) + U(d.ix2, k));
+    }
+    if (zg) {
+      if (k == 1) e = T(2.) * W(i, 1) - T(0.5) * (W(i, d.kz1 - 1) + W(i, d.kz1));
+      else if (k == d.nz) e = T(2.) * W(i, d.kz2) - T(0.5) * (W(i, d.kz2 - 1) + W(i, d.kz2));
+    }
+    // positions outside the array are never read by an interior strain
+    sm.cen[slot][0][r][c] = a;
+    sm.cen[slot][1][r][c] = b;
+    sm.cen[slot][2][r][c] = e;
+  }
+}
+
 // strain of plane j at this thread's (i,k) from the ring (slots of j-1, j, j+1)
 template <typename T>
 __device__ __forceinline__ void strain_at(const Dims &d, const DevMetrics &m, const MarchSmem<T> &sm, int j, int i,
                                           int k, int lane, int wr, T (&s)[6], T &g) {
   const int c = lane + 1, r = wr + 1;
-  const int s0 = j % 3, sm1 = (j + 2) % 3, sp1 = (j + 1) % 3;
+  const int s0 = j % 4, sm1 = (j + 3) % 4, sp1 = (j + 1) % 4;
   T uc[7], vc[7], wc[7];
   auto gather = [&](int q, T(&a)[7]) {
     a[0] = sm.cen[s0][q][r][c];
@@ -187,7 +222,7 @@ __device__ __forceinline__ void strain_at(const Dims &d, const DevMetrics &m, co
 }
 
 template <typename T>
-__global__ void __launch_bounds__(NW * 32, 1)
+__global__ void __launch_bounds__(NW * 32, sizeof(T) == 4 ? 2 : 1)
     k_dynamic_march(Dims d, DevMetrics m, int px, const T *__restrict__ u, const T *__restrict__ v,
                     const T *__restrict__ w, const double *__restrict__ dxdydz, T *__restrict__ gs, int gpitch,
                     T *__restrict__ imm2, T *__restrict__ ilm2) {
@@ -223,59 +258,96 @@ __global__ void __launch_bounds__(NW * 32, 1)
     else if (k == d.kz2) { zr0 = wr; zr1 = wr - 1; zr2 = wr - 2; }
   }
 
-  T Ya[NQ], Yb[NQ];  // partial y sums: Ya of plane j-1 (two terms), Yb of plane j (one term)
+  T Ya[NQ] = {}, Yb[NQ] = {};  // partial y sums: Ya of plane j-1 (two terms), Yb of plane j (one term)
   T acc_m = T(0), acc_l = T(0);
 
-  // filtered quantities of this column's plane from its base and its x
-  // neighbours', folded into the y partial sums; returns in Yc the completed
-  // Y of the plane before
-  auto x_and_y = [&](const Base<T> &b, T(&Yc)[NQ]) {
-    Base<T> bA = shfl_base(b, srcA), bB = shfl_base(b, srcB);
+  // x pass of the 22 quantities of this column's plane from its base and its
+  // x neighbours', folded into the y partial sums; the completed Y of the
+  // plane before goes to shared memory (row wr) for the z pass.  Tiles whose
+  // output columns are all interior (the CTA-uniform common case) take the
+  // interior stencil without selects.
+  const bool xfast = ia > d.ix1 && ia + TO - 1 < d.ix2;
+  auto fold = [&](int c, T x) {
+    sm.yb[c][wr][lane] = Ya[c] + T(0.25) * x;
+    Ya[c] = Yb[c] + T(0.50) * x;
+    Yb[c] = T(0.25) * x;
+  };
+  // F, S, B: the values at the first, second and third x-stencil points of
+  // this lane's column; inside (i-1, i, i+1), at ix1 (ix1, ix1+1, ix1+2), at
+  // ix2 (ix2, ix2-1, ix2-2)
+  auto nbr3 = [&](auto &V, auto &F, auto &S, auto &B) {
+    constexpr int N = sizeof(V) / sizeof(T);
+    if (xfast) {
 #pragma unroll
-    for (int c = 0; c < NQ; c++) {
-      T q0 = quant(b, c), qA = quant(bA, c), qB = quant(bB, c);
-      T x = xedge ? (wx0 * q0 + wx1 * qA) + wx2 * qB : (wx0 * qA + wx1 * q0) + wx2 * qB;
-      Yc[c] = Ya[c] + T(0.25) * x;
-      Ya[c] = Yb[c] + T(0.50) * x;
-      Yb[c] = T(0.25) * x;
+      for (int n = 0; n < N; n++) {
+        F[n] = shfl(V[n], max(lane - 1, 0));
+        S[n] = V[n];
+        B[n] = shfl(V[n], min(lane + 1, 31));
+      }
+    } else {
+#pragma unroll
+      for (int n = 0; n < N; n++) {
+        T a = shfl(V[n], srcA);
+        F[n] = xedge ? V[n] : a;
+        S[n] = xedge ? a : V[n];
+        B[n] = shfl(V[n], srcB);
+      }
     }
   };
-  // z pass of the completed plane j (own row from Yc, the others from shared
-  // memory), M_ij and L_ij (vt.f:216-290), clipped sums in j order
-  auto z_and_ml = [&](const T(&Yc)[NQ], int j) {
-    T Z[NQ];
+  auto x_and_y = [&](const Base<T> &b) {
+    // quantities 0-12 from |S| and S_ij (G*S and S in the order xx,yy,zz,xy,yz,xz; G)
+    {
+      T V[7] = {b.g, b.s[0], b.s[1], b.s[2], b.s[3], b.s[5], b.s[4]};
+      T F[7], S[7], B[7];
+      nbr3(V, F, S, B);
 #pragma unroll
-    for (int c = 0; c < NQ; c++) {
-      T y0 = zr0 == wr ? Yc[c] : sm.yb[c][zr0][lane];
-      T y1 = zr1 == wr ? Yc[c] : sm.yb[c][zr1][lane];
-      T y2 = sm.yb[c][zr2][lane];
-      Z[c] = (wz0 * y0 + wz1 * y1) + wz2 * y2;
+      for (int c = 0; c < 6; c++)
+        fold(c, (wx0 * (F[0] * F[1 + c]) + wx1 * (S[0] * S[1 + c])) + wx2 * (B[0] * B[1 + c]));
+#pragma unroll
+      for (int c = 0; c < 6; c++) fold(6 + c, (wx0 * F[1 + c] + wx1 * S[1 + c]) + wx2 * B[1 + c]);
+      fold(12, (wx0 * F[0] + wx1 * S[0]) + wx2 * B[0]);
     }
+    // quantities 13-21 from the centred velocities
+    {
+      T V[3] = {b.uc, b.vc, b.wc};
+      T F[3], S[3], B[3];
+      nbr3(V, F, S, B);
+#pragma unroll
+      for (int c = 0; c < 3; c++) fold(13 + c, (wx0 * F[c] + wx1 * S[c]) + wx2 * B[c]);
+      const int pa[6] = {0, 1, 2, 0, 1, 0}, pb[6] = {0, 1, 2, 1, 2, 2};  // uu vv ww uv vw uw
+#pragma unroll
+      for (int c = 0; c < 6; c++)
+        fold(16 + c, (wx0 * (F[pa[c]] * F[pb[c]]) + wx1 * (S[pa[c]] * S[pb[c]])) + wx2 * (B[pa[c]] * B[pb[c]]));
+    }
+  };
+  // z pass of the completed plane j from shared memory, M_ij and L_ij
+  // (vt.f:216-290), clipped sums in j order
+  auto z_and_ml = [&](int j) {
+    // filtered quantity c at this cell, read when first needed (fewer live registers)
+    auto zq = [&](int c) {
+      return (wz0 * sm.yb[c][zr0][lane] + wz1 * sm.yb[c][zr1][lane]) + wz2 * sm.yb[c][zr2][lane];
+    };
     const T C = T(1.0), R = T(6.);
     T dx = (T)dxdydz[fidx(d, i, j, k)];
-    T gb = Z[12];
-    T mxx = C * dx * (R * gb * Z[6] - Z[0]);
-    T myy = C * dx * (R * gb * Z[7] - Z[1]);
-    T mzz = C * dx * (R * gb * Z[8] - Z[2]);
-    T mxy = C * dx * (R * gb * Z[9] - Z[3]);
-    T myz = C * dx * (R * gb * Z[10] - Z[4]);
-    T mxz = C * dx * (R * gb * Z[11] - Z[5]);
+    T gb = zq(12);
+    T mxx = C * dx * (R * gb * zq(6) - zq(0));
+    T myy = C * dx * (R * gb * zq(7) - zq(1));
+    T mzz = C * dx * (R * gb * zq(8) - zq(2));
+    T mxy = C * dx * (R * gb * zq(9) - zq(3));
+    T myz = C * dx * (R * gb * zq(10) - zq(4));
+    T mxz = C * dx * (R * gb * zq(11) - zq(5));
     T mmv = mxx * mxx + myy * myy + mzz * mzz + T(2.) * (mxy * mxy + myz * myz + mxz * mxz);
-    T uh = Z[13], vh = Z[14], wh = Z[15];
-    T lxx = (Z[16] - uh * uh) * mxx;
-    T lyy = (Z[17] - vh * vh) * myy;
-    T lzz = (Z[18] - wh * wh) * mzz;
-    T lxy = (Z[19] - uh * vh) * mxy;
-    T lyz = (Z[20] - vh * wh) * myz;
-    T lxz = (Z[21] - uh * wh) * mxz;
+    T uh = zq(13), vh = zq(14), wh = zq(15);
+    T lxx = (zq(16) - uh * uh) * mxx;
+    T lyy = (zq(17) - vh * vh) * myy;
+    T lzz = (zq(18) - wh * wh) * mzz;
+    T lxy = (zq(19) - uh * vh) * mxy;
+    T lyz = (zq(20) - vh * wh) * myz;
+    T lxz = (zq(21) - uh * wh) * mxz;
     T lmv = lxx + lyy + lzz + T(2.) * (lxy + lyz + lxz);
     acc_m += mmv;
     if (lmv < T(0)) lmv = T(0);
     acc_l += lmv;
-  };
-  auto put_yb = [&](const T(&Yc)[NQ]) {
-#pragma unroll
-    for (int c = 0; c < NQ; c++) sm.yb[c][wr][lane] = Yc[c];
   };
 
   // prologue: |S|, S_ij of plane jy2 (the periodic copy in ghost row 1)
@@ -287,54 +359,63 @@ __global__ void __launch_bounds__(NW * 32, 1)
   Base<T> b{};
   if (inner) strain_at(d, m, sm, jy2, i, k, lane, wr, b.s, b.g);
   __syncthreads();
+  // raw planes 3, 4, 5 in flight (one copy group each), planes 1..3 centred
+  // directly
+  for (int p = jy1 + 1; p <= jy1 + 3; p++) {
+    if (p <= ny - 1) issue_raw(d, px, u, v, w, p, ia, ka, sm);
+    cp_async_commit();
+  }
   center_plane(d, px, u, v, w, 1, ia, ka, sm);
   center_plane(d, px, u, v, w, jy1, ia, ka, sm);
+  if (jy1 + 1 <= ny) center_plane(d, px, u, v, w, jy1 + 1, ia, ka, sm);
   __syncthreads();
   // ghost row 1: centred velocities of row 1, strain of row jy2
-  b.uc = sm.cen[1 % 3][0][wr + 1][lane + 1];
-  b.vc = sm.cen[1 % 3][1][wr + 1][lane + 1];
-  b.wc = sm.cen[1 % 3][2][wr + 1][lane + 1];
-  {
-    T Yc[NQ];
+  b.uc = sm.cen[1 % 4][0][wr + 1][lane + 1];
+  b.vc = sm.cen[1 % 4][1][wr + 1][lane + 1];
+  b.wc = sm.cen[1 % 4][2][wr + 1][lane + 1];
 #pragma unroll
-    for (int c = 0; c < NQ; c++) { Ya[c] = T(0); Yb[c] = T(0); }
-    x_and_y(b, Yc);  // only Yb (first term of Y(jy1)) is kept
-  }
+  for (int c = 0; c < NQ; c++) { Ya[c] = T(0); Yb[c] = T(0); }
+  x_and_y(b);  // only Yb (first term of Y(jy1)) is used
   for (int j = jy1; j <= jy2; j++) {
-    center_plane(d, px, u, v, w, j + 1, ia, ka, sm);
+    // raw plane j+2 has landed (j+3 may still be in flight); after the
+    // barrier every thread's copies are visible and every read of the slots
+    // reused below (centred plane j-2, raw plane j) is done
+    cp_async_wait<1>();
     __syncthreads();
+    const int pc = j + 2;
+    if (pc <= ny - 1) center_raw(d, pc, ia, ka, sm);
+    else if (pc == ny) center_plane(d, px, u, v, w, ny, ia, ka, sm);
+    if (j + 4 <= ny - 1) issue_raw(d, px, u, v, w, j + 4, ia, ka, sm);
+    cp_async_commit();
     Base<T> bj{};
     if (inner) strain_at(d, m, sm, j, i, k, lane, wr, bj.s, bj.g);
-    bj.uc = sm.cen[j % 3][0][wr + 1][lane + 1];
-    bj.vc = sm.cen[j % 3][1][wr + 1][lane + 1];
-    bj.wc = sm.cen[j % 3][2][wr + 1][lane + 1];
+    bj.uc = sm.cen[j % 4][0][wr + 1][lane + 1];
+    bj.vc = sm.cen[j % 4][1][wr + 1][lane + 1];
+    bj.wc = sm.cen[j % 4][2][wr + 1][lane + 1];
     if (j == jy1) {
       sm.sgb[0][wr][lane] = bj.g;
 #pragma unroll
       for (int c = 0; c < 6; c++) sm.sgb[1 + c][wr][lane] = bj.s[c];
     }
     if (out) gs[pidx(d, gpitch, i, j, k)] = bj.g;
-    T Yc[NQ];
-    x_and_y(bj, Yc);
-    if (j > jy1) put_yb(Yc);
+    x_and_y(bj);  // completes Y(j-1) (unused for j = jy1)
     __syncthreads();
-    if (j > jy1 && out) z_and_ml(Yc, j - 1);
+    if (j > jy1 && out) z_and_ml(j - 1);
   }
+  cp_async_wait<0>();
   // ghost row NY: centred velocities of row NY, strain of row jy1
   {
     Base<T> bn{};
-    bn.uc = sm.cen[ny % 3][0][wr + 1][lane + 1];
-    bn.vc = sm.cen[ny % 3][1][wr + 1][lane + 1];
-    bn.wc = sm.cen[ny % 3][2][wr + 1][lane + 1];
+    bn.uc = sm.cen[ny % 4][0][wr + 1][lane + 1];
+    bn.vc = sm.cen[ny % 4][1][wr + 1][lane + 1];
+    bn.wc = sm.cen[ny % 4][2][wr + 1][lane + 1];
     bn.g = sm.sgb[0][wr][lane];
 #pragma unroll
     for (int c = 0; c < 6; c++) bn.s[c] = sm.sgb[1 + c][wr][lane];
-    T Yc[NQ];
-    x_and_y(bn, Yc);
     __syncthreads();  // every z pass of the last loop iteration has read yb
-    put_yb(Yc);
+    x_and_y(bn);
     __syncthreads();
-    if (out) z_and_ml(Yc, jy2);
+    if (out) z_and_ml(jy2);
   }
   if (out) {
     imm2[(i - 1) + d.nx * (k - 1)] = acc_m / T(d.ny - 2);
