@@ -146,18 +146,25 @@ __device__ bool segtriint(const double *p1, const double *p2, const double *tri,
   return code == 1;
 }
 
-__device__ int locate(const double *xx1, int n, double x) {
-  int jl = 0, ju = n + 1;
-  if (xx1[1] == x) return 1;
-  const bool asc = xx1[n] > xx1[1];
-  while (ju - jl > 1) {
-    int jm = (ju + jl) / 2;
-    if (asc == (x > xx1[jm]))
-      jl = jm;
-    else
-      ju = jm;
+// Position of x in the monotone table xx[1..n] (1-based), the contract of the
+// reference's table search (src/numrec.f:390-422): for an ascending table the
+// number of entries below x (0 below the table, n above it), for a
+// descending one the number of entries >= x; x equal to the first entry
+// gives 1.  A partition-point binary search.
+__device__ int locate(const double *xx, int n, double x) {
+  if (xx[1] == x) return 1;
+  const bool asc = xx[n] > xx[1];
+  int first = 1, count = n;
+  while (count > 0) {
+    const int step = count / 2, m = first + step;
+    if ((x > xx[m]) == asc) {
+      first = m + 1;
+      count -= step + 1;
+    } else {
+      count = step;
+    }
   }
-  return jl;
+  return first - 1;
 }
 
 // ---------------------------------------------------------------------------

@@ -185,6 +185,9 @@ const eo_ib_set *eo_ib_stencils(const eo_ib *ib, int q);
 void eo_ib_body(const eo_ib *ib, double *v, double *c);
 const double *eo_ib_velocity(const eo_ib *ib);
 void eo_ib_set_cadence(eo_ib *ib, int every);
+/* 1: exhaustive candidate and nearest-centroid searches instead of the
+ * binned ones (same results; a cross-check) */
+void eo_ib_set_brute(eo_ib *ib, int brute);
 int eo_ib_every(const eo_ib *ib);
 int eo_locate(const double *xx1, int n, double x);
 int eo_segtriint(const double *p1, const double *p2, const double *a, const double *b, const double *c,

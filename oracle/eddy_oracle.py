@@ -111,6 +111,7 @@ def lib():
         L.eo_ib_geom.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.eo_ib_move.argtypes = [vp, C.c_double]
         L.eo_ib_set_cadence.argtypes = [vp, C.c_int]
+        L.eo_ib_set_brute.argtypes = [vp, C.c_int]
         L.eo_ib_force.argtypes = [vp, C.c_int, dp, C.c_double]
         L.eo_ib_interior.argtypes = [vp, C.c_int, dp, C.c_double]
         L.eo_ib_limits.restype = C.POINTER(C.c_int)
@@ -270,6 +271,9 @@ class OracleIB:
 
     def set_cadence(self, every_substep: int):
         lib().eo_ib_set_cadence(self.h, every_substep)
+
+    def set_brute(self, brute: int):
+        lib().eo_ib_set_brute(self.h, brute)
 
     def move(self, t: float):
         lib().eo_ib_move(self.h, t)

@@ -45,6 +45,9 @@
 #include <string.h>
 
 #include "eddy_oracle.h"
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #define NCR 16
 #define NNTR3D 25
@@ -54,20 +57,26 @@ static long IDX(const eo_grid *g, int i, int j, int k) {
   return (long)(i - 1) + (long)g->nx * ((long)(j - 1) + (long)g->ny * (long)(k - 1));
 }
 
-/* ---- LOCATE (src/numrec.f:390-422): jl with xx(jl) < x <= xx(jl+1), 1-based */
-int eo_locate(const double *xx1, int n, double x) {
-  /* xx1 is 1-based: xx1[1..n] */
-  int jl = 0, ju = n + 1;
-  if (xx1[1] == x) return 1;
-  int asc = xx1[n] > xx1[1];
-  while (ju - jl > 1) {
-    int jm = (ju + jl) / 2;
-    if (asc == (x > xx1[jm]))
-      jl = jm;
-    else
-      ju = jm;
+/* ---- table search with the contract of LOCATE (src/numrec.f:390-422) ----
+ * Position of x in the monotone table xx[1..n] (1-based): for an ascending
+ * table the number of entries below x, i.e. j with xx[j] < x <= xx[j+1]
+ * (0 below the table, n above it); for a descending one the number of
+ * entries >= x; x equal to the first entry gives 1.  A partition-point
+ * binary search over the predicate "entry m lies before x". */
+int eo_locate(const double *xx, int n, double x) {
+  if (xx[1] == x) return 1;
+  const int asc = xx[n] > xx[1];
+  int first = 1, count = n;
+  while (count > 0) {
+    const int step = count / 2, m = first + step;
+    if ((x > xx[m]) == asc) {
+      first = m + 1;
+      count -= step + 1;
+    } else {
+      count = step;
+    }
   }
-  return jl;
+  return first - 1;
 }
 
 /* ---- intersect_triangle (src/rt.f:1263-1330) ---- */
@@ -132,6 +141,13 @@ struct eo_ib {
   eo_ib_set set[4];     /* stencils u, v, w, p */
   int nntr3d, nflu, itagy;
   int every; /* 1: move + regenerate every substep, 0: once per step */
+  int brute; /* 1: exhaustive searches (cross-check of the binned ones) */
+  /* xy bins of the triangles' bounding boxes (TAG3D candidates) and 3-D bins
+   * of the centroids (nearest-centroid lists); rebuilt at every regeneration */
+  double bx0, by0, bx1, by1, bhx, bhy;
+  int bnx, bny, *bstart, *blist;
+  double c0[3], ch[3];
+  int cn[3], *cstart, *clist;
 };
 
 eo_ib *eo_ib_create(const eo_grid *g, int nb, const double *vert, const double *normals, const double *vel) {
@@ -167,6 +183,7 @@ static void set_free(eo_ib_set *s) {
 void eo_ib_free(eo_ib *ib) {
   if (!ib) return;
   free(ib->v); free(ib->c); free(ib->n);
+  free(ib->bstart); free(ib->blist); free(ib->cstart); free(ib->clist);
   for (int q = 0; q < 4; q++) { free(ib->tag[q]); set_free(&ib->set[q]); }
   for (int q = 0; q < 5; q++) free(ib->flag[q]);
   free(ib);
@@ -210,6 +227,82 @@ void eo_ib_limimb(eo_ib *ib) {
   ib->lim[4] = kmin; ib->lim[5] = kmax;
 }
 
+/* ---- exact spatial bins (the reference prunes with ANN kd-trees; the
+ * candidate sets here are supersets filtered by the same exact tests, visited
+ * in ascending triangle order, so results equal the exhaustive search) ---- */
+static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+static void build_bins(eo_ib *ib) {
+  const int nb = ib->nb;
+  free(ib->bstart); free(ib->blist); free(ib->cstart); free(ib->clist);
+  ib->bstart = ib->blist = ib->cstart = ib->clist = NULL;
+  if (nb == 0) return;
+  /* xy bins over the union of the triangles' xy boxes */
+  double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+  for (int t = 0; t < nb; t++)
+    for (int a = 0; a < 3; a++) {
+      const double *p = ib->v + 9 * t + 3 * a;
+      x0 = fmin(x0, p[0]); x1 = fmax(x1, p[0]); y0 = fmin(y0, p[1]); y1 = fmax(y1, p[1]);
+    }
+  int m = (int)ceil(sqrt((double)nb));
+  m = clampi(m, 1, 2048);
+  ib->bx0 = x0; ib->by0 = y0; ib->bx1 = x1; ib->by1 = y1;
+  ib->bhx = (x1 - x0) / m; ib->bhy = (y1 - y0) / m;
+  if (!(ib->bhx > 0)) ib->bhx = 1.0;
+  if (!(ib->bhy > 0)) ib->bhy = 1.0;
+  ib->bnx = m; ib->bny = m;
+  ib->bstart = (int *)calloc((size_t)m * m + 1, sizeof(int));
+  for (int pass = 0; pass < 2; pass++) {
+    int *fill = pass ? (int *)calloc((size_t)m * m, sizeof(int)) : NULL;
+    for (int t = 0; t < nb; t++) {
+      const double *a = ib->v + 9 * t, *b = a + 3, *c = a + 6;
+      double tx0 = fmin(fmin(a[0], b[0]), c[0]), tx1 = fmax(fmax(a[0], b[0]), c[0]);
+      double ty0 = fmin(fmin(a[1], b[1]), c[1]), ty1 = fmax(fmax(a[1], b[1]), c[1]);
+      int i0 = clampi((int)floor((tx0 - x0) / ib->bhx), 0, m - 1), i1 = clampi((int)floor((tx1 - x0) / ib->bhx), 0, m - 1);
+      int j0 = clampi((int)floor((ty0 - y0) / ib->bhy), 0, m - 1), j1 = clampi((int)floor((ty1 - y0) / ib->bhy), 0, m - 1);
+      for (int jb = j0; jb <= j1; jb++)
+        for (int ibn = i0; ibn <= i1; ibn++) {
+          int cell = jb * m + ibn;
+          if (pass == 0) ib->bstart[cell + 1]++;
+          else ib->blist[ib->bstart[cell] + fill[cell]++] = t;
+        }
+    }
+    if (pass == 0) {
+      for (int cidx = 0; cidx < m * m; cidx++) ib->bstart[cidx + 1] += ib->bstart[cidx];
+      ib->blist = (int *)malloc(sizeof(int) * (size_t)(ib->bstart[m * m] > 0 ? ib->bstart[m * m] : 1));
+    } else {
+      free(fill);
+    }
+  }
+  /* 3-D centroid bins, about four centroids per occupied cell of a shell */
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int t = 0; t < nb; t++)
+    for (int d = 0; d < 3; d++) { lo[d] = fmin(lo[d], ib->c[3 * t + d]); hi[d] = fmax(hi[d], ib->c[3 * t + d]); }
+  int n1 = clampi((int)ceil(sqrt((double)nb / 4.0)), 1, 512);
+  int ntot = 1;
+  for (int d = 0; d < 3; d++) {
+    ib->c0[d] = lo[d];
+    ib->cn[d] = n1;
+    ib->ch[d] = (hi[d] - lo[d]) / n1;
+    if (!(ib->ch[d] > 0)) ib->ch[d] = 1.0;
+    ntot *= n1;
+  }
+  ib->cstart = (int *)calloc((size_t)ntot + 1, sizeof(int));
+  ib->clist = (int *)malloc(sizeof(int) * (size_t)nb);
+  int *cell = (int *)malloc(sizeof(int) * (size_t)nb);
+  for (int t = 0; t < nb; t++) {
+    int ci[3];
+    for (int d = 0; d < 3; d++) ci[d] = clampi((int)floor((ib->c[3 * t + d] - ib->c0[d]) / ib->ch[d]), 0, n1 - 1);
+    cell[t] = (ci[2] * n1 + ci[1]) * n1 + ci[0];
+    ib->cstart[cell[t] + 1]++;
+  }
+  for (int cidx = 0; cidx < ntot; cidx++) ib->cstart[cidx + 1] += ib->cstart[cidx];
+  int *fill = (int *)calloc((size_t)ntot, sizeof(int));
+  for (int t = 0; t < nb; t++) ib->clist[ib->cstart[cell[t]] + fill[cell[t]]++] = t;
+  free(fill);
+  free(cell);
+}
+
 /* ---- TAG3D_MOD (src/rt.f:2704-3020) for variable q ---- */
 void eo_ib_tag(eo_ib *ib, int q) {
   const eo_grid *g = ib->g;
@@ -220,12 +313,30 @@ void eo_ib_tag(eo_ib *ib, int q) {
   for (long t = 0; t < nc; t++) ibs[t] = 1;
   const double zmin = g->zw[1], zmax = g->zw[g->nz - 1], zlen = zmax - zmin;
   const double rzmin = fmin(zmin - zlen, -1.0e8), rzmax = fmax(zmax + zlen, 1.0e8);
-  for (int i = ib->lim[0]; i <= ib->lim[1]; i++)
-    for (int j = 2; j <= g->ny - 1; j++) {
+  const int ni = ib->lim[1] - ib->lim[0] + 1, nj = g->ny - 2;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int col = 0; col < ni * nj; col++) {
+      const int i = ib->lim[0] + col / nj, j = 2 + col % nj;
       const double xcc = X[i], ycc = Y[j];
       double zc_[NCR], zo[NCR];
       int nc_ = 0;
-      for (int t = 0; t < ib->nb; t++) {
+      /* candidate triangles: all of them, or the xy bin of the column */
+      int cb = 0, ce = ib->nb;
+      const int *cl = NULL;
+      if (!ib->brute) {
+        cb = ce = 0;
+        /* a triangle whose xy box holds the column was binned over a range
+         * of bins that contains the column's (floor is monotone) */
+        if (ib->nb > 0 && xcc >= ib->bx0 && xcc <= ib->bx1 && ycc >= ib->by0 && ycc <= ib->by1) {
+          int bi = clampi((int)floor((xcc - ib->bx0) / ib->bhx), 0, ib->bnx - 1);
+          int bj = clampi((int)floor((ycc - ib->by0) / ib->bhy), 0, ib->bny - 1);
+          cb = ib->bstart[bj * ib->bnx + bi];
+          ce = ib->bstart[bj * ib->bnx + bi + 1];
+          cl = ib->blist;
+        }
+      }
+      for (int ct = cb; ct < ce; ct++) {
+        const int t = cl ? cl[ct] : ct;
         const double *a = ib->v + 9 * t, *b = a + 3, *c = a + 6;
         if (ycc >= fmin(fmin(a[1], b[1]), c[1]) && ycc <= fmax(fmax(a[1], b[1]), c[1]) &&
             xcc >= fmin(fmin(a[0], b[0]), c[0]) && xcc <= fmax(fmax(a[0], b[0]), c[0])) {
@@ -349,25 +460,64 @@ void eo_ib_flagp(eo_ib *ib) {
   }
 }
 
-/* ---- exact k nearest centroids (ties by triangle index) ---- */
+/* ---- exact k nearest centroids (ties by triangle index): the first k of
+ * all centroids ordered by (squared distance, index) ---- */
+static void topk_insert(double *best, int *bi, int *m, int k, double d2, int t) {
+  if (*m == k && (d2 > best[k - 1] || (d2 == best[k - 1] && t > bi[k - 1]))) return;
+  int p = *m < k ? *m : k - 1;
+  while (p > 0 && (best[p - 1] > d2 || (best[p - 1] == d2 && bi[p - 1] > t))) {
+    best[p] = best[p - 1];
+    bi[p] = bi[p - 1];
+    p--;
+  }
+  best[p] = d2;
+  bi[p] = t;
+  if (*m < k) (*m)++;
+}
+
 static void knn(const eo_ib *ib, const double *q, int k, int *out) {
   double best[NNTR3D];
   int bi[NNTR3D];
   int m = 0;
-  for (int t = 0; t < ib->nb; t++) {
-    const double *c = ib->c + 3 * t;
-    double dx = c[0] - q[0], dy = c[1] - q[1], dz = c[2] - q[2];
-    double d2 = dx * dx + dy * dy + dz * dz;
-    if (m < k || d2 < best[m - 1]) {
-      int p = m < k ? m : k - 1;
-      while (p > 0 && best[p - 1] > d2) {
-        best[p] = best[p - 1];
-        bi[p] = bi[p - 1];
-        p--;
+  if (ib->brute || !ib->cstart) {
+    for (int t = 0; t < ib->nb; t++) {
+      const double *c = ib->c + 3 * t;
+      double dx = c[0] - q[0], dy = c[1] - q[1], dz = c[2] - q[2];
+      topk_insert(best, bi, &m, k, dx * dx + dy * dy + dz * dz, t);
+    }
+  } else {
+    /* rings of cells around the query's cell until no unvisited centroid can
+     * come closer than the k-th found (strictly, with a rounding margin) */
+    const int *n = ib->cn;
+    int ci[3];
+    for (int d = 0; d < 3; d++) ci[d] = clampi((int)floor((q[d] - ib->c0[d]) / ib->ch[d]), 0, n[d] - 1);
+    for (int r = 0;; r++) {
+      int lo[3], hi[3], full = 1;
+      for (int d = 0; d < 3; d++) {
+        lo[d] = ci[d] - r; hi[d] = ci[d] + r;
+        if (lo[d] > 0 || hi[d] < n[d] - 1) full = 0;
       }
-      best[p] = d2;
-      bi[p] = t;
-      if (m < k) m++;
+      for (int z = lo[2] < 0 ? 0 : lo[2]; z <= (hi[2] > n[2] - 1 ? n[2] - 1 : hi[2]); z++)
+        for (int y = lo[1] < 0 ? 0 : lo[1]; y <= (hi[1] > n[1] - 1 ? n[1] - 1 : hi[1]); y++)
+          for (int x = lo[0] < 0 ? 0 : lo[0]; x <= (hi[0] > n[0] - 1 ? n[0] - 1 : hi[0]); x++) {
+            if (x != lo[0] && x != hi[0] && y != lo[1] && y != hi[1] && z != lo[2] && z != hi[2]) continue;
+            int cell = (z * n[1] + y) * n[0] + x;
+            for (int e = ib->cstart[cell]; e < ib->cstart[cell + 1]; e++) {
+              const int t = ib->clist[e];
+              const double *c = ib->c + 3 * t;
+              double dx = c[0] - q[0], dy = c[1] - q[1], dz = c[2] - q[2];
+              topk_insert(best, bi, &m, k, dx * dx + dy * dy + dz * dz, t);
+            }
+          }
+      if (full) break;
+      /* distance from q to the nearest face of the visited box that has
+       * cells beyond it */
+      double dmin = 1e300;
+      for (int d = 0; d < 3; d++) {
+        if (lo[d] > 0) dmin = fmin(dmin, q[d] - (ib->c0[d] + lo[d] * ib->ch[d]));
+        if (hi[d] < n[d] - 1) dmin = fmin(dmin, (ib->c0[d] + (hi[d] + 1) * ib->ch[d]) - q[d]);
+      }
+      if (m == k && dmin > 0 && best[k - 1] * (1.0 + 1e-9) < dmin * dmin) break;
     }
   }
   for (int a = 0; a < m; a++) out[a] = bi[a];
@@ -578,6 +728,9 @@ void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
   for (int ilp = 1; ilp <= ib->nflu && np > 0; ilp++) {
     int nn2 = 0, nres = 0;
     int *res = (int *)malloc(sizeof(int) * np);
+    int *gis = (int *)malloc(sizeof(int) * np);
+    /* the points of one loop are independent (fw changes only between loops) */
+#pragma omp parallel for schedule(dynamic, 8)
     for (int a = 0; a < np; a++) {
       const int p = pend[a];
       const int im = pi[p], jm = pj[p], km = pk[p];
@@ -588,12 +741,18 @@ void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
         const double qv[3] = {X[im], Y[jm], Z[km]};
         int inn[NNTR3D];
         gi = 0;
+        knn(ib, qv, sizes[2], inn);  /* sorted by (distance, index): prefixes are the smaller lists */
         for (int icm = 0; icm < 3; icm++) {
-          knn(ib, qv, sizes[icm], inn);
           gi = eo_ib_grid_intr(ib, q, fw, im, jm, km, inn, sizes[icm], xnv + 3 * p, ddx + 3 * p);
           if (gi != 0 && gi != -2) break;
         }
       }
+      gis[a] = gi;
+    }
+    for (int a = 0; a < np; a++) {
+      const int p = pend[a];
+      const int im = pi[p], jm = pj[p], km = pk[p];
+      const int gi = gis[a];
       if (gi == 1) {
         mrk[p] = 2;
         lev[p] = ilp;
@@ -606,6 +765,7 @@ void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
         flagu[IDX(g, im, jm, km)] = (signed char)(imn == 0 ? 1 : 0);
       }
     }
+    free(gis);
     if (nres > 0) nlev = ilp;
     for (int a = 0; a < nres; a++) fw[IDX(g, pi[res[a]], pj[res[a]], pk[res[a]])] = 0;
     for (int k = 1; k <= g->nz; k++)
@@ -672,6 +832,7 @@ void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
 /* the whole regeneration for the current body position (src/Eddy6.f:2163-2380) */
 void eo_ib_regen(eo_ib *ib) {
   eo_ib_limimb(ib);
+  build_bins(ib);
   for (int q = 0; q < 4; q++) {
     eo_ib_tag(ib, q);
     eo_ib_taguo(ib, q, q);
@@ -735,6 +896,7 @@ void eo_ib_interior(eo_ib *ib, int fq, double *a, double value) {
 const int *eo_ib_limits(const eo_ib *ib) { return ib->lim; }
 const double *eo_ib_velocity(const eo_ib *ib) { return ib->vel; }
 void eo_ib_set_cadence(eo_ib *ib, int every) { ib->every = every ? 1 : 0; }
+void eo_ib_set_brute(eo_ib *ib, int brute) { ib->brute = brute ? 1 : 0; }
 int eo_ib_every(const eo_ib *ib) { return ib->every; }
 const signed char *eo_ib_tags(const eo_ib *ib, int q) { return ib->tag[q]; }
 const signed char *eo_ib_flags(const eo_ib *ib, int fq) { return ib->flag[fq]; }

@@ -81,3 +81,51 @@ def test_velocity_stencil_reproduces_linear_data(sphere_ib):
         b[[0, P[0]]] = b[[P[0], 0]]
         x = np.linalg.solve(U, np.linalg.solve(L, b))
         assert abs(x[0] - c0) < 1e-12
+
+
+@pytest.mark.parametrize("level,shift", [(3, (0.0, 0.0, 0.0)), (5, (0.013, -0.021, 0.37))])
+def test_binned_searches_equal_exhaustive(oracle, level, shift):
+    # the oracle prunes TAG3D candidates and nearest-centroid lists with exact
+    # spatial bins (the reference prunes with ANN kd-trees); tags, flags and
+    # every stencil must equal those of the exhaustive searches
+    w = config.small(mx=40, ly=32, nz_=48)
+    tri, nrm = body.icosphere(level)
+    tri = tri + np.asarray(shift)[None, None, :]
+    out = []
+    for brute in (1, 0):
+        o = oracle.OracleSolver(w)
+        ib = oracle.OracleIB(o, tri, nrm, attach=False)
+        ib.set_brute(brute)
+        ib.regen()
+        out.append((ib, [ib.tags(q) for q in range(4)], [ib.flags(f) for f in range(5)],
+                    [ib.stencils(q) for q in range(4)]))
+    (_, t0, f0, s0), (_, t1, f1, s1) = out
+    for a, b in zip(t0 + f0, t1 + f1):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(s0, s1):
+        assert a["n"] == b["n"] and a["n"] > 0
+        for key in ("i", "j", "k", "di", "dj", "dk", "lev", "xn", "yn", "zn", "lu", "indx"):
+            np.testing.assert_array_equal(a[key], b[key], err_msg=key)
+
+
+def test_locate_contract(oracle):
+    # the table search keeps LOCATE's contract (src/numrec.f:390-422)
+    import ctypes as C
+    lib = oracle.lib()
+    lib.eo_locate.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_double]
+    lib.eo_locate.restype = C.c_int
+    xs = np.array([0.0, -1.0, -0.5, 0.0, 0.0, 0.25, 1.0, 2.0])  # 1-based table xx[1..7], a repeated entry
+    n = 7
+    p = xs.ctypes.data_as(C.POINTER(C.c_double))
+    def ref(x):
+        if xs[1] == x:
+            return 1
+        return int(np.sum(xs[1:n + 1] < x))
+    for x in (-2.0, -1.0, -0.7, -0.5, -0.1, 0.0, 0.1, 0.25, 0.9, 1.0, 2.0, 3.0):
+        assert lib.eo_locate(p, n, x) == ref(x), x
+    d = xs.copy()
+    d[1:n + 1] = xs[1:n + 1][::-1]
+    pd = d.ctypes.data_as(C.POINTER(C.c_double))
+    for x in (-2.0, -0.5, 0.0, 0.3, 2.0, 3.0):
+        want = 1 if d[1] == x else int(np.sum(d[1:n + 1] >= x))
+        assert lib.eo_locate(pd, n, x) == want, x
