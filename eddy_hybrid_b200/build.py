@@ -29,6 +29,7 @@ UNITS = {
     "k_mlp.cu": [],
     "k_mixed.cu": [],
     "k_xform.cu": [],
+    "k_xform64.cu": [],
     "k_ib.cu": ["-fmad=false"],
     "host_eigen.cpp": [],
 }
@@ -61,7 +62,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     if force or _newer(objs, OUT):
-        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", OUT, *objs, "-lcublas"]
+        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", OUT, *objs]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -234,7 +234,6 @@ void free_all(eddy_ctx *ctx) {
   for (double *p : o2) if (p) cudaFree(p);
   for (ProfEvent &e : ctx->prof_ev) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (ProfEvent &e : ctx->prof_pool) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
-  if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->ib_stream) cudaStreamSynchronize(ctx->ib_stream);
   for (cudaEvent_t e : ctx->ib_ev)
     if (e) cudaEventDestroy(e);
@@ -358,9 +357,6 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
       cudaEventCreateWithFlags(&ctx->ib_ev[0], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ib_ev[1], cudaEventDisableTiming) != cudaSuccess)
     return fail(EDDY_ECUDA, "cudaStreamCreate failed");
-  if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(EDDY_ECUDA, "cublasCreate failed");
-  cublasSetStream(ctx->blas, ctx->stream);
-  cublasSetMathMode(ctx->blas, CUBLAS_DEFAULT_MATH);
   build_metrics(ctx, xu_faces, ymin, ymax, zw_faces);
   int rc = upload_metrics(ctx);
   if (rc) return fail(rc, nullptr);

@@ -1,7 +1,6 @@
 // eddy_internal.h -- context layout and kernel launch declarations shared by
 // the CUDA translation units of libeddy_b200.so.
 #pragma once
-#include <cublas_v2.h>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -43,7 +42,13 @@ struct PoissonPlan {
   int M, L, N;          // interior sizes along x, y (FFT), z
   int m0;               // index of the null x-mode
   double *Af, *Ab;      // forward/backward transform matrices (M x M, col-major)
-  float *Af32, *Ab32;   // FP32 copies for the mixed form
+  // FP64 tensor-core transforms (k_xform64.cu): matrices [chunk][row][8] for
+  // the forward (0) and backward (1) directions, split into even and odd
+  // modes when the x operator is mirror-symmetric (dsym); dHp the padded half
+  // size (full size when not split); eigenvalues and null mode in that order
+  double *dA[2];
+  double *dlam;
+  int dsym, dHp, dm0;
   double *lam;          // eigenvalues of the x operator (M)
   double *ak;           // modified wavenumber AK(J/2+1) per packed index (L)
   double *an, *bn, *cn; // z operator (N)
@@ -86,7 +91,6 @@ struct eddy_ctx {
   int ib_pending = 0;
   double ib_move_dt = -1.0;  // >= 0: move over this time and regenerate in this substep
   int ib_prefetched = 0;     // the next step's move and regeneration are already queued
-  cublasHandle_t blas = nullptr;
   DevMetrics m{};
   // host copies of the 1-D arrays (1-based, size n+2)
   std::vector<double> h[28];
@@ -246,6 +250,13 @@ int xform_prepare(eddy_ctx *ctx, XformPlan *xp);
 void xform_release(XformPlan *xp);
 // dir 0: x values -> mode coefficients; 1: back
 int launch_xform(eddy_ctx *ctx, const XformPlan *xp, int dir, const float *in, float *out);
+// FP64 tensor-core transforms over the L*N spectral lines (k_xform64.cu), dir
+// 0 forward, 1 backward, in the mode order of pp.dlam / pp.dm0; FP64 or FP32
+// storage, FP64 arithmetic
+int xform64_prepare(eddy_ctx *ctx, const std::vector<double> &Af, const std::vector<double> &Ab,
+                    const std::vector<double> &lam);
+int launch_xform64(eddy_ctx *ctx, int dir, const double *in, double *out);
+int launch_xform64_f32(eddy_ctx *ctx, int dir, const float *in, float *out);
 
 // mixed-precision form (k_mixed.cu): FP32 stencils and FFTs, FP64 line solves,
 // FP64-residual iterative refinement, FP64 projection onto FP64 master velocities

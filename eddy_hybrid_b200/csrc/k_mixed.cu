@@ -50,7 +50,7 @@ struct MixedState {
   float *twr = nullptr, *twi = nullptr;  // FFT twiddles: forward table then backward table
   double *resid = nullptr;               // max |r| before each sweep (device, 4 entries)
   double *wout = nullptr;                // outlet-face w (NX,NY) in FP64: exact mass balance
-  // 3xTF32 tensor-core transforms (null fmat: FP32 cuBLAS GEMMs with the plan's matrices)
+  // 3xTF32 tensor-core transforms (null fmat: the FP64 tensor-core transforms of k_xform64.cu)
   XformPlan xp;
   float *cpz = nullptr;  // z-line c' of every (m, J) line (M*L*N, FP32), computed once per plan
 };
@@ -728,28 +728,22 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   PoissonPlan &pp = ctx->pp;
   const Dims &d = ctx->d;
   int M = pp.M, L = pp.L, N = pp.N;
-  long long lines = (long long)L * N;
   float *s1 = reinterpret_cast<float *>(pp.spec), *s2 = reinterpret_cast<float *>(pp.spec2);
-  const float one = 1.f, zero = 0.f;
-  cublasStatus_t bs;
   int rc;
   {
     ProfScope ps(ctx, PROF_GEMM_FWD);
     if (x->xp.fmat) {
       if ((rc = launch_xform(ctx, &x->xp, 0, s1, s2))) return rc;
     } else {
-      bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Af32, M, s1, M, &zero, s2,
-                       M);
-      if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (forward transform) failed"; return EDDY_ECUDA; }
-      ctx->launches++;
+      if ((rc = launch_xform64_f32(ctx, 0, s1, s2))) return rc;
     }
   }
   {
     ProfScope ps(ctx, PROF_TRIDIAG);
     long long nl = (long long)M * L;
     // mode order of the transforms: the split form orders even modes first
-    const double *lam = x->xp.fmat ? x->xp.lam : pp.lam;
-    const int m0 = x->xp.fmat ? x->xp.m0 : pp.m0;
+    const double *lam = x->xp.fmat ? x->xp.lam : pp.dlam;
+    const int m0 = x->xp.fmat ? x->xp.m0 : pp.dm0;
     k_line_mean<float><<<1, 256, 0, ctx->stream>>>(M, L, N, m0, pp.wz, s2, ctx->scal + 5);
     EDDY_LAUNCHED(ctx);
     float *e32 = reinterpret_cast<float *>(pp.cprime);
@@ -762,10 +756,7 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
     if (x->xp.bmat) {
       if ((rc = launch_xform(ctx, &x->xp, 1, s2, s1))) return rc;
     } else {
-      bs = cublasSgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Ab32, M, s2, M, &zero, s1,
-                       M);
-      if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasSgemm (backward transform) failed"; return EDDY_ECUDA; }
-      ctx->launches++;
+      if ((rc = launch_xform64_f32(ctx, 1, s2, s1))) return rc;
     }
   }
   ProfScope ps(ctx, PROF_FFT_BWD);
@@ -895,8 +886,8 @@ int mixed_create(eddy_ctx *ctx) {
     const PoissonPlan &pp = ctx->pp;
     const long long nl = (long long)pp.M * pp.L;
     EDDY_CUDA(cudaMalloc(&x->cpz, sizeof(float) * (size_t)nl * pp.N));
-    const double *lam = x->xp.fmat ? x->xp.lam : pp.lam;
-    const int m0 = x->xp.fmat ? x->xp.m0 : pp.m0;
+    const double *lam = x->xp.fmat ? x->xp.lam : pp.dlam;
+    const int m0 = x->xp.fmat ? x->xp.m0 : pp.dm0;
     k_tridiag_cprime<float><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(pp.M, pp.L, pp.N, m0, lam, pp.ak,
                                                                                   pp.an, pp.bn, pp.cn, x->cpz);
     EDDY_LAUNCHED(ctx);

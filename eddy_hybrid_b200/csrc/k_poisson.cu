@@ -3,8 +3,9 @@
 //
 //   1. divergence/alfxdt fused with the forward real FFT along y (packed
 //      FFTPACK order, src/fftpack.f RFFTF) -> spectral array S[k][J][i]
-//   2. eigen-transform of the stretched x operator: one DGEMM over all
-//      (J,k) lines, G = Af * S  (Af = Q^T D^-1/2, D = diag(ap))
+//   2. eigen-transform of the stretched x operator over all (J,k) lines,
+//      G = Af * S  (Af = Q^T D^-1/2, D = diag(ap)), on the FP64 tensor cores
+//      (k_xform64.cu; even/odd split for a mirror-symmetric operator)
 //   3. per (m,J) line a tridiagonal (Thomas) solve along stretched z with
 //      diagonal bn(k) + lambda_m - AK(J); the Neumann null mode (J=0, m=m0)
 //      is pinned by dropping its first z equation
@@ -241,32 +242,25 @@ int solve_from_spec(eddy_ctx *ctx, double *dp) {
   PoissonPlan &pp = ctx->pp;
   const Dims &d = ctx->d;
   int M = pp.M, L = pp.L, N = pp.N;
-  long long lines = (long long)L * N;
-  const double one = 1.0, zero = 0.0;
-  cublasStatus_t bs;
+  int rc;
   {
     ProfScope ps(ctx, PROF_GEMM_FWD);
-    bs = cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Af, M, pp.spec, M, &zero,
-                     pp.spec2, M);
-    if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasDgemm (forward transform) failed"; return EDDY_ECUDA; }
-    ctx->launches++;
+    if ((rc = launch_xform64(ctx, 0, pp.spec, pp.spec2))) return rc;
   }
   long long nl = (long long)M * L;
   {
     ProfScope ps(ctx, PROF_TRIDIAG);
-    k_line_mean<double><<<1, 256, 0, ctx->stream>>>(M, L, N, pp.m0, pp.wz, pp.spec2, ctx->scal + 5);
+    // modes in the transforms' order (even then odd when split)
+    k_line_mean<double><<<1, 256, 0, ctx->stream>>>(M, L, N, pp.dm0, pp.wz, pp.spec2, ctx->scal + 5);
     EDDY_LAUNCHED(ctx);
     // the eliminated right-hand side overwrites the spectrum in place
     k_tridiag_lines<double, double, 8, false><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
-        M, L, N, pp.m0, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, pp.spec2, pp.cprime, pp.spec2);
+        M, L, N, pp.dm0, pp.dlam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, pp.spec2, pp.cprime, pp.spec2);
     EDDY_LAUNCHED(ctx);
   }
   {
     ProfScope ps(ctx, PROF_GEMM_BWD);
-    bs = cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, (int)lines, M, &one, pp.Ab, M, pp.spec2, M, &zero,
-                     pp.spec, M);
-    if (bs != CUBLAS_STATUS_SUCCESS) { ctx->err = "cublasDgemm (backward transform) failed"; return EDDY_ECUDA; }
-    ctx->launches++;
+    if ((rc = launch_xform64(ctx, 1, pp.spec2, pp.spec))) return rc;
   }
   ProfScope psb(ctx, PROF_FFT_BWD);
   k_plane_sum_partial<<<NPART, 256, 0, ctx->stream>>>(M, L, N, pp.spec, pp.red);
@@ -315,7 +309,43 @@ int poisson_plan_create(eddy_ctx *ctx) {
   for (int i = 0; i < M; i++) sq[i] = std::sqrt(ap[i + 2]);
   for (int i = 0; i < M; i++) dd[i] = bm[i];
   for (int i = 0; i < M - 1; i++) ee[i] = sq[i] * sq[i + 1] * au[i + 2];
-  if (tridiag_eigen(M, dd, ee, Q) != 0) { ctx->err = "x-operator eigensolver did not converge"; return EDDY_ESINGULAR; }
+  // A mirror-symmetric operator (the same entries read from either end, bit
+  // for bit) has even and odd eigenvectors [u; flip u] / sqrt 2 and
+  // [u; -flip u] / sqrt 2, u the eigenvectors of the upper half with the
+  // coupling across the middle added to / subtracted from its last diagonal
+  // entry.  Solving the two half-size problems makes the symmetry exact, which
+  // the transforms' even/odd split relies on.
+  bool mirror = M % 2 == 0 && M >= 4;
+  for (int i = 0; i < M && mirror; i++) mirror = dd[i] == dd[M - 1 - i] && sq[i] == sq[M - 1 - i];
+  for (int i = 0; i < M - 1 && mirror; i++) mirror = ee[i] == ee[M - 2 - i];
+  if (mirror) {
+    const int H = M / 2;
+    Q.assign((size_t)M * M, 0.);
+    std::vector<double> lamv(M);
+    for (int par = 0; par < 2; par++) {
+      std::vector<double> dh(dd.begin(), dd.begin() + H), eh(ee.begin(), ee.begin() + (H > 1 ? H - 1 : 1)), Qh;
+      dh[H - 1] = par == 0 ? dh[H - 1] + ee[H - 1] : dh[H - 1] - ee[H - 1];
+      if (tridiag_eigen(H, dh, eh, Qh) != 0) {
+        ctx->err = "x-operator eigensolver did not converge";
+        return EDDY_ESINGULAR;
+      }
+      const double r2 = 1.0 / std::sqrt(2.0);
+      for (int m = 0; m < H; m++) {
+        lamv[par * H + m] = dh[m];
+        for (int i = 0; i < H; i++) {
+          const double v = Qh[(size_t)i * H + m] * r2;
+          Q[(size_t)i * M + par * H + m] = v;
+          Q[(size_t)(M - 1 - i) * M + par * H + m] = par == 0 ? v : -v;
+        }
+      }
+    }
+    dd = lamv;
+  } else if (tridiag_eigen(M, dd, ee, Q) != 0) {
+    ctx->err = "x-operator eigensolver did not converge";
+    return EDDY_ESINGULAR;
+  }
+  // the null mode (constant pressure along x): exact eigenvalue 0 and the
+  // exact normalised vector D^-1/2 1 (even, so it stays in the even set)
   int m0 = 0;
   for (int mm = 1; mm < M; mm++) if (std::fabs(dd[mm]) < std::fabs(dd[m0])) m0 = mm;
   dd[m0] = 0.;
@@ -326,14 +356,11 @@ int poisson_plan_create(eddy_ctx *ctx) {
   for (int i = 0; i < M; i++) Q[(size_t)i * M + m0] = sgn / (sq[i] * nrm);
   pp.m0 = m0;
   std::vector<double> Af((size_t)M * M), Ab((size_t)M * M);
-  std::vector<float> Af32((size_t)M * M), Ab32((size_t)M * M);
   for (int i = 0; i < M; i++)
     for (int mm = 0; mm < M; mm++) {
       double q = Q[(size_t)i * M + mm];
       Af[(size_t)mm + (size_t)M * i] = q / sq[i];  // Af(m,i), column-major
       Ab[(size_t)i + (size_t)M * mm] = sq[i] * q;  // Ab(i,m)
-      Af32[(size_t)mm + (size_t)M * i] = (float)Af[(size_t)mm + (size_t)M * i];
-      Ab32[(size_t)i + (size_t)M * mm] = (float)Ab[(size_t)i + (size_t)M * mm];
     }
   // modified wavenumbers (direct.f:321-331) per packed index J (0-based)
   std::vector<double> akv(L);
@@ -353,8 +380,6 @@ int poisson_plan_create(eddy_ctx *ctx) {
   size_t bytesM2 = sizeof(double) * (size_t)M * M, vol = sizeof(double) * (size_t)M * L * N;
   EDDY_CUDA(cudaMalloc(&pp.Af, bytesM2));
   EDDY_CUDA(cudaMalloc(&pp.Ab, bytesM2));
-  EDDY_CUDA(cudaMalloc(&pp.Af32, bytesM2 / 2));
-  EDDY_CUDA(cudaMalloc(&pp.Ab32, bytesM2 / 2));
   EDDY_CUDA(cudaMalloc(&pp.lam, sizeof(double) * M));
   EDDY_CUDA(cudaMalloc(&pp.ak, sizeof(double) * L));
   EDDY_CUDA(cudaMalloc(&pp.an, sizeof(double) * N));
@@ -369,8 +394,6 @@ int poisson_plan_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMalloc(&pp.red, sizeof(double) * NPART));
   EDDY_CUDA(cudaMemcpy(pp.Af, Af.data(), bytesM2, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.Ab, Ab.data(), bytesM2, cudaMemcpyHostToDevice));
-  EDDY_CUDA(cudaMemcpy(pp.Af32, Af32.data(), bytesM2 / 2, cudaMemcpyHostToDevice));
-  EDDY_CUDA(cudaMemcpy(pp.Ab32, Ab32.data(), bytesM2 / 2, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.lam, dd.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.ak, akv.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.an, an.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
@@ -381,6 +404,8 @@ int poisson_plan_create(eddy_ctx *ctx) {
   EDDY_CUDA(cudaMemcpy(pp.wz, wz.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.twr, twr.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
   EDDY_CUDA(cudaMemcpy(pp.twi, twi.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
+  int rc = xform64_prepare(ctx, Af, Ab, dd);
+  if (rc) return rc;
   size_t smem = sizeof(double) * (2 * L * TI + L);
   if (smem > 48 * 1024) {
     EDDY_CUDA(cudaFuncSetAttribute(k_div_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -391,7 +416,7 @@ int poisson_plan_create(eddy_ctx *ctx) {
 
 int poisson_plan_destroy(eddy_ctx *ctx) {
   PoissonPlan &pp = ctx->pp;
-  void *ptrs[] = {pp.Af, pp.Ab, pp.Af32, pp.Ab32, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, pp.wz,
+  void *ptrs[] = {pp.Af, pp.Ab, pp.dA[0], pp.dA[1], pp.dlam, pp.lam, pp.ak, pp.an, pp.bn, pp.cn, pp.wz,
                   pp.twr, pp.twi, pp.spec, pp.spec2, pp.cprime, pp.red};
   for (void *p : ptrs) if (p) cudaFree(p);
   pp = PoissonPlan{};

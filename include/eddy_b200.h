@@ -26,7 +26,7 @@ extern "C" {
 enum {
   EDDY_OK = 0,
   EDDY_EINVAL = 1,      /* bad argument / unsupported configuration */
-  EDDY_ECUDA = 2,       /* CUDA or cuBLAS error */
+  EDDY_ECUDA = 2,       /* CUDA error */
   EDDY_ENAN = 3,        /* non-finite value detected */
   EDDY_ESINGULAR = 4,   /* singular pivot in a line solve */
   EDDY_ENOCONV = 5,     /* refinement did not converge */
