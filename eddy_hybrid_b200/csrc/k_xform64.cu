@@ -12,10 +12,11 @@
 //   backward X_top = E Y_even + O Y_odd,         X_bot = flip(E Y_even - O Y_odd)
 // which halves the multiply-adds.  Otherwise one M x M product.
 //
-// A CTA takes 32 lines: it stages them (already mirrored into sums and
-// differences for the forward transform) in shared memory once, then streams
-// the matrix through a double-buffered cp.async ring in chunks of 8 along the
-// reduction index.  Warp w owns m-tiles w, w+8, ... of both parities, so the
+// A CTA takes 32 lines and, one parity after the other, stages them (mirrored
+// into sums or differences for the forward transform) in shared memory, then
+// streams that parity's matrix through a double-buffered cp.async ring in
+// chunks of 8 along the reduction index (84 KB of shared memory at M = 384:
+// two CTAs per SM).  Warp w owns m-tiles w, w+8, ... of both parities, so the
 // backward transform forms E+O and E-O in registers.  Input and output may be
 // FP64 (the plain form) or FP32 (the mixed form's correction solves on grids
 // its TF32 tensor-core transform does not take); arithmetic is FP64.
@@ -50,58 +51,23 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-// NP = 2: split form (Hp = padded H, K = H); NP = 1: one product (Hp = padded M, K = M)
+// NP = 2: split form (Hp = padded H, K = H); NP = 1: one product (Hp = padded
+// M, K = M).  The parities run one after the other through the same shared
+// buffers (half the footprint: two CTAs per SM); the backward transform keeps
+// the even part in registers until the odd one is done.
 template <int NP, int MT, int DIR, class TI, class TO>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, NP * MT >= 7 ? 1 : 2)
     k_xform64(int M, int Hp, long long nlines, const double *__restrict__ A, const TI *__restrict__ in,
               TO *__restrict__ out) {
   extern __shared__ __align__(16) double smx[];
-  const int KS = Hp + 4;                       // B row stride (Hp is a multiple of 8)
-  double *Bs = smx;                            // [NP][NL][KS]
-  double *Asm = smx + (size_t)NP * NL * KS;    // [2][NP*Hp][AS]
+  const int KS = Hp + 4;               // B row stride (Hp is a multiple of 8)
+  double *Bs = smx;                    // [NL][KS]
+  double *Asm = smx + (size_t)NL * KS; // [2][Hp][AS]
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t4 = lane & 3;
   const long long l0 = (long long)blockIdx.x * NL;
-  const int H = NP == 2 ? M / 2 : M;          // valid rows / reduction length
+  const int H = NP == 2 ? M / 2 : M;   // valid rows / reduction length
   const int nch = Hp / KC;
-  const int rows = NP * Hp;
-  const size_t chunk = (size_t)rows * KC;      // doubles per matrix chunk in global
-
-  auto issue = [&](int c) {
-    if (c < nch) {
-      double *dst = Asm + (size_t)(c & 1) * rows * AS;
-      const double *src = A + (size_t)c * chunk;
-      for (int e = threadIdx.x; e < rows * (KC / 2); e += NT) {
-        const int r = e / (KC / 2), q = e % (KC / 2);
-        cp_async16(dst + (size_t)r * AS + 2 * q, src + (size_t)r * KC + 2 * q);
-      }
-    }
-    cp_commit();
-  };
-  issue(0);
-  // the 32 lines, mirrored into sums and differences for the forward split
-  for (int e = threadIdx.x; e < NL * Hp; e += NT) {
-    const int l = e / Hp, k = e % Hp;
-    const long long line = l0 + l;
-    double v0 = 0., v1 = 0.;
-    if (line < nlines && k < H) {
-      const TI *src = in + line * (long long)M;
-      if (NP == 2) {
-        if (DIR == 0) {
-          const double a = (double)src[k], b = (double)src[M - 1 - k];
-          v0 = a + b;
-          v1 = a - b;
-        } else {
-          v0 = (double)src[k];
-          v1 = (double)src[H + k];
-        }
-      } else {
-        v0 = (double)src[k];
-      }
-    }
-    Bs[(size_t)l * KS + k] = v0;
-    if (NP == 2) Bs[(size_t)(NL + l) * KS + k] = v1;
-  }
-  issue(1);
+  const size_t chunk = (size_t)Hp * KC; // doubles per matrix chunk in global
 
   double acc[NP][MT][4][2];
 #pragma unroll
@@ -111,72 +77,114 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
       for (int n = 0; n < 4; n++) acc[p][j][n][0] = acc[p][j][n][1] = 0.;
 
-  for (int c = 0; c < nch; c++) {
-    cp_wait<1>();
-    __syncthreads();
-    const double *As = Asm + (size_t)(c & 1) * rows * AS;
 #pragma unroll
-    for (int kk = 0; kk < KC; kk += 4) {
-      double a[NP][MT], b[NP][4];
+  for (int p = 0; p < NP; p++) {
+    const double *Ap = A + (size_t)p * nch * chunk;
+    auto issue = [&](int c) {
+      if (c < nch) {
+        double *dst = Asm + (size_t)(c & 1) * Hp * AS;
+        const double *src = Ap + (size_t)c * chunk;
+        for (int e = threadIdx.x; e < Hp * (KC / 2); e += NT) {
+          const int r = e / (KC / 2), q = e % (KC / 2);
+          cp_async16(dst + (size_t)r * AS + 2 * q, src + (size_t)r * KC + 2 * q);
+        }
+      }
+      cp_commit();
+    };
+    if (p > 0) __syncthreads();  // the previous parity's readers are done with both buffers
+    issue(0);
+    // the 32 lines of this parity (forward split: sums for the even part,
+    // differences for the odd one); each thread issues a batch of loads
+    // before its first shared store
+    constexpr int UB = 8;
+    for (int e0 = threadIdx.x; e0 < NL * Hp; e0 += NT * UB) {
+      double v0[UB], v1[UB];
 #pragma unroll
-      for (int p = 0; p < NP; p++) {
+      for (int u = 0; u < UB; u++) {
+        const int e = e0 + u * NT;
+        const int l = e / Hp, k = e % Hp;
+        const long long line = l0 + l;
+        v0[u] = 0.;
+        v1[u] = 0.;
+        if (e < NL * Hp && line < nlines && k < H) {
+          const TI *src = in + line * (long long)M;
+          if (NP == 2 && DIR == 0) {
+            v0[u] = (double)src[k];
+            v1[u] = (double)src[M - 1 - k];
+          } else {
+            v0[u] = (double)src[p * H + k];
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UB; u++) {
+        const int e = e0 + u * NT;
+        if (e >= NL * Hp) break;
+        const int l = e / Hp, k = e % Hp;
+        Bs[(size_t)l * KS + k] = (NP == 2 && DIR == 0) ? (p == 0 ? v0[u] + v1[u] : v0[u] - v1[u]) : v0[u];
+      }
+    }
+    issue(1);
+    for (int c = 0; c < nch; c++) {
+      cp_wait<1>();
+      __syncthreads();
+      const double *As = Asm + (size_t)(c & 1) * Hp * AS;
+#pragma unroll
+      for (int kk = 0; kk < KC; kk += 4) {
+        double a[MT], b[4];
 #pragma unroll
         for (int j = 0; j < MT; j++) {
           const int mt = w + 8 * j;
-          a[p][j] = mt * 8 < Hp ? As[(size_t)(p * Hp + mt * 8 + g) * AS + kk + t4] : 0.;
+          a[j] = mt * 8 < Hp ? As[(size_t)(mt * 8 + g) * AS + kk + t4] : 0.;
         }
 #pragma unroll
-        for (int n = 0; n < 4; n++) b[p][n] = Bs[(size_t)(p * NL + n * 8 + g) * KS + c * KC + kk + t4];
-      }
-#pragma unroll
-      for (int p = 0; p < NP; p++)
+        for (int n = 0; n < 4; n++) b[n] = Bs[(size_t)(n * 8 + g) * KS + c * KC + kk + t4];
 #pragma unroll
         for (int j = 0; j < MT; j++)
           if ((w + 8 * j) * 8 < Hp) {
 #pragma unroll
-            for (int n = 0; n < 4; n++) dmma(acc[p][j][n][0], acc[p][j][n][1], a[p][j], b[p][n]);
+            for (int n = 0; n < 4; n++) dmma(acc[p][j][n][0], acc[p][j][n][1], a[j], b[n]);
           }
-    }
-    __syncthreads();  // every warp is done with this buffer
-    issue(c + 2);
-  }
-  cp_wait<0>();
-
-  // lane: row g of each m-tile, lines 2*t4 and 2*t4+1 of each line tile
-#pragma unroll
-  for (int j = 0; j < MT; j++) {
-    const int m = (w + 8 * j) * 8 + g;
-    if (m >= H) continue;
-#pragma unroll
-    for (int n = 0; n < 4; n++)
-#pragma unroll
-      for (int e = 0; e < 2; e++) {
-        const long long line = l0 + n * 8 + 2 * t4 + e;
-        if (line >= nlines) continue;
-        TO *dst = out + line * (long long)M;
-        if (NP == 1) {
-          dst[m] = (TO)acc[0][j][n][e];
-        } else if (DIR == 0) {
-          dst[m] = (TO)acc[0][j][n][e];
-          dst[H + m] = (TO)acc[1][j][n][e];
-        } else {
-          const double E = acc[0][j][n][e], O = acc[1 % NP][j][n][e];
-          dst[m] = (TO)(E + O);
-          dst[M - 1 - m] = (TO)(E - O);
-        }
       }
+      __syncthreads();  // every warp is done with this buffer
+      issue(c + 2);
+    }
+    cp_wait<0>();
+    // lane: row g of each m-tile, lines 2*t4 and 2*t4+1 of each line tile.
+    // Modes (forward, or the unsplit product) are stored per parity; the
+    // split backward transform combines both parities after the last one.
+    if (DIR == 0 || NP == 1 || p == NP - 1) {
+#pragma unroll
+      for (int j = 0; j < MT; j++) {
+        const int m = (w + 8 * j) * 8 + g;
+        if (m >= H) continue;
+#pragma unroll
+        for (int n = 0; n < 4; n++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const long long line = l0 + n * 8 + 2 * t4 + e;
+            if (line >= nlines) continue;
+            TO *dst = out + line * (long long)M;
+            if (DIR == 0 || NP == 1) {
+              dst[p * H + m] = (TO)acc[p][j][n][e];
+            } else {
+              const double E = acc[0][j][n][e], O = acc[NP - 1][j][n][e];
+              dst[m] = (TO)(E + O);
+              dst[M - 1 - m] = (TO)(E - O);
+            }
+          }
+      }
+    }
   }
 }
 
-size_t xform64_smem(int np, int hp) {
-  return sizeof(double) * ((size_t)np * NL * (hp + 4) + (size_t)2 * np * hp * AS);
-}
+size_t xform64_smem(int hp) { return sizeof(double) * ((size_t)NL * (hp + 4) + (size_t)2 * hp * AS); }
 
 template <int NP, int MT, int DIR, class TI, class TO>
 int launch_t(eddy_ctx *ctx, const double *A, const TI *in, TO *out) {
   const PoissonPlan &pp = ctx->pp;
   const long long nlines = (long long)pp.L * pp.N;
-  const size_t smem = xform64_smem(NP, pp.dHp);
+  const size_t smem = xform64_smem(pp.dHp);
   EDDY_CUDA(cudaFuncSetAttribute(k_xform64<NP, MT, DIR, TI, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
   const unsigned grid = (unsigned)((nlines + NL - 1) / NL);
@@ -214,7 +222,7 @@ int dispatch(eddy_ctx *ctx, const TI *in, TO *out) {
 
 }  // namespace
 
-// Split (or plain) transform matrices in chunk-major order [chunk][row][KC],
+// Split (or plain) transform matrices in [parity][chunk][row][KC] order,
 // rows zero-padded to Hp, the reduction index zero-padded to Hp; the
 // eigenvalues and the null mode in the transforms' mode order.
 int xform64_prepare(eddy_ctx *ctx, const std::vector<double> &Af, const std::vector<double> &Ab,
@@ -251,12 +259,12 @@ int xform64_prepare(eddy_ctx *ctx, const std::vector<double> &Af, const std::vec
   if (sym) {
     for (int m = 0; m < H; m++) { perm[m] = even[m]; perm[H + m] = odd[m]; }
   }
-  const int rows = np * hp, nch = hp / KC;
-  std::vector<double> F((size_t)nch * rows * KC, 0.), B((size_t)nch * rows * KC, 0.);
+  const int nch = hp / KC;
+  std::vector<double> F((size_t)np * nch * hp * KC, 0.), B(F.size(), 0.);
   for (int p = 0; p < np; p++)
     for (int r = 0; r < K; r++)
       for (int k = 0; k < K; k++) {
-        const size_t o = ((size_t)(k / KC) * rows + (size_t)(p * hp + r)) * KC + k % KC;
+        const size_t o = (((size_t)p * nch + (size_t)(k / KC)) * hp + (size_t)r) * KC + k % KC;
         if (sym) {
           F[o] = af(perm[p * H + r], k);  // row: mode r of parity p, column: x
           B[o] = ab(r, perm[p * H + k]);  // row: x, column: mode k of parity p
