@@ -44,7 +44,7 @@ class Params(C.Structure):
                 ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
                 ("dspngx3in", C.c_int), ("dspngx3out", C.c_int),
                 ("precision", C.c_int), ("refine_sweeps", C.c_int),
-                ("closure", C.c_int)]
+                ("closure", C.c_int), ("imply", C.c_int)]
 
 
 def make_params(d: dict, precision: int = PLAIN_FP64, refine_sweeps: int = 2,
@@ -74,6 +74,15 @@ SIGNATURES = {
     "eddy_get_metric": ([C.c_void_p, C.c_int, _DP, C.c_int], C.c_int),
     "eddy_grid_metric": ([C.POINTER(Params), _DP, C.c_double, C.c_double, _DP, C.c_int, _DP, C.c_int], C.c_int),
     "eddy_rhs_predictord": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
+    "eddy_inversey": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_cfl": ([C.c_void_p, _DP], C.c_int),
+    "eddy_field_extrema": ([C.c_void_p, C.c_int, _DP, _DP], C.c_int),
+    "eddy_ioscalar_write": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.c_int, C.c_double, C.c_double,
+                             C.c_double], C.c_int),
+    "eddy_ioscalar_read": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.POINTER(C.c_int), _DP, _DP, _DP],
+                           C.c_int),
+    "eddy_save_field": ([C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_double], C.c_int),
+    "eddy_load_field": ([C.c_void_p, C.c_int, C.c_char_p, C.POINTER(C.c_int), _DP, _DP, _DP], C.c_int),
     "eddy_boundary": ([C.c_void_p, C.c_int], C.c_int),
     "eddy_boundinout": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
     "eddy_direct": ([C.c_void_p, C.c_double], C.c_int),
@@ -132,6 +141,26 @@ def lib():
             fn.restype = res
         _lib = L
     return _lib
+
+
+def write_ioscalar(path: str, a: np.ndarray, nstep: int, time: float, dtm1: float, grav: float):
+    """Host array (NX,NY,NZ) to a restart file in the IOSCALAR layout."""
+    a = np.asfortranarray(a, dtype=np.float64)
+    nx, ny, nz = a.shape
+    rc = lib().eddy_ioscalar_write(path.encode(), nx, ny, nz, _ptr(a), nstep, time, dtm1, grav)
+    if rc:
+        raise EddyError(f"eddy_ioscalar_write failed ({rc})")
+
+
+def read_ioscalar(path: str, shape) -> tuple:
+    """Restart file to a host array of `shape`; returns (array, nstep, time, dtm1, grav)."""
+    a = np.zeros(shape, order="F")
+    ns, t, dt, gr = C.c_int(0), C.c_double(0.), C.c_double(0.), C.c_double(0.)
+    rc = lib().eddy_ioscalar_read(path.encode(), shape[0], shape[1], shape[2], _ptr(a), C.byref(ns), C.byref(t),
+                                  C.byref(dt), C.byref(gr))
+    if rc:
+        raise EddyError(f"eddy_ioscalar_read failed ({rc}): missing, truncated or another grid")
+    return a, ns.value, t.value, dt.value, gr.value
 
 
 def _ptr(a: np.ndarray):
@@ -212,6 +241,47 @@ class Solver:
             a = out
         self._check(lib().eddy_download(self.h, FID[name], _ptr(a)), "eddy_download")
         return a
+
+    # restart files: the reference's set and names, <dir>/<field>_<step:08d>.res
+    # (src/Eddy6.f:3391-3408), in the IOSCALAR layout
+    RESTART_FIELDS = ("uo", "vo", "wo", "p", "tv", "dens")
+    RESTART_NAMES = {"uo": "u", "vo": "v", "wo": "w", "p": "p", "tv": "tv", "dens": "dens"}
+
+    def save_restart(self, directory: str, step: int, time: float, dt: float | None = None):
+        dt = self.w.dt if dt is None else dt
+        for n in self.RESTART_FIELDS:
+            path = os.path.join(directory, f"{self.RESTART_NAMES[n]}_{step:08d}.res").encode()
+            self._check(lib().eddy_save_field(self.h, FID[n], path, step, time, dt), "eddy_save_field")
+
+    def load_restart(self, directory: str, step: int) -> dict:
+        ns, t, dt, gr = C.c_int(0), C.c_double(0.), C.c_double(0.), C.c_double(0.)
+        for n in self.RESTART_FIELDS:
+            path = os.path.join(directory, f"{self.RESTART_NAMES[n]}_{step:08d}.res").encode()
+            self._check(lib().eddy_load_field(self.h, FID[n], path, C.byref(ns), C.byref(t), C.byref(dt),
+                                              C.byref(gr)), "eddy_load_field")
+        return {"nstep": ns.value, "time": t.value, "dtm1": dt.value, "grav": gr.value}
+
+    def cfl(self) -> float:
+        v = C.c_double(0.)
+        self._check(lib().eddy_cfl(self.h, C.byref(v)), "eddy_cfl")
+        return v.value
+
+    def step_cfl(self, cflc: float, nsteps: int = 1) -> list:
+        """Constant-CFL stepping (icfl = 1): before every step DTM1 = CFLC / CFLM
+        (src/Eddy6.f:2114-2128); returns the time steps taken."""
+        dts = []
+        for _ in range(nsteps):
+            dt = cflc / self.cfl()
+            if dt <= 1e-6:
+                raise EddyError(f"constant-CFL time step {dt:.3e} <= 1e-6 (the reference stops here)")
+            self.step(1, dt)
+            dts.append(dt)
+        return dts
+
+    def extrema(self, name: str) -> tuple:
+        lo, hi = C.c_double(0.), C.c_double(0.)
+        self._check(lib().eddy_field_extrema(self.h, FID[name], C.byref(lo), C.byref(hi)), "eddy_field_extrema")
+        return lo.value, hi.value
 
     def load_initial(self, fields: dict):
         for k, v in fields.items():

@@ -31,7 +31,10 @@ UNITS = {
     "k_xform.cu": [],
     "k_xform64.cu": [],
     "k_ib.cu": ["-fmad=false"],
+    "k_implicit.cu": ["-fmad=false"],
+    "k_diag.cu": ["-fmad=false"],
     "host_eigen.cpp": [],
+    "host_restart.cpp": [],
 }
 
 

@@ -79,6 +79,7 @@ class Workload:
     itype: tuple = ITYPE_WAKE
     sphere: bool = True
     body_speed: float = 0.0
+    imply: int = 0     # Crank-Nicolson viscous terms along y (the reference input's IMPLY)
 
     @property
     def nx(self) -> int:
@@ -112,6 +113,7 @@ class Workload:
             vspngx1=max(2, self.mx // 24), dspngx1=max(2, self.mx // 24),
             vspngx3in=0, vspngx3out=0, dspngx3in=0,
             dspngx3out=max(4, self.nz_ // 14),
+            imply=self.imply,
         )
 
 

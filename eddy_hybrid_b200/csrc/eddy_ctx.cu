@@ -200,7 +200,7 @@ void build_metrics(eddy_ctx *ctx, const double *xf, double ymin, double ymax, co
   Scalars &s = ctx->sc;
   s.ru1 = p.ru1; s.prn = p.prn; s.grav = p.grav; s.dpdx = p.dpdx; s.dpdy = p.dpdy; s.dpdz = p.dpdz;
   s.eps = p.eps; s.css = p.css; s.vspngx1 = p.vspngx1; s.dspngx1 = p.dspngx1;
-  s.ivspngl = ivs; s.idspngl = ids; s.idens = p.idens; s.isgs = p.isgs;
+  s.ivspngl = ivs; s.idspngl = ids; s.idens = p.idens; s.isgs = p.isgs; s.imply = p.imply;
 }
 
 int upload_metrics(eddy_ctx *ctx) {
@@ -223,7 +223,7 @@ void free_all(eddy_ctx *ctx) {
                   m.dfxu, m.dfxw, m.dfxul, m.dfxwl, m.dfxd, m.dfxdl, m.dens_bg};
   for (double *p : mp) if (p) cudaFree(p);
   for (int f = 0; f < EDDY_NFIELDS; f++) if (ctx->f[f]) cudaFree(ctx->f[f]);
-  double *o[] = {ctx->dens_alt, ctx->gs, ctx->dxdydz, ctx->ilm2, ctx->imm2, ctx->scal};
+  double *o[] = {ctx->dens_alt, ctx->gs, ctx->dxdydz, ctx->ilm2, ctx->imm2, ctx->scal, ctx->diag};
   for (double *p : o) if (p) cudaFree(p);
   if (ctx->err_flag) cudaFree(ctx->err_flag);
   poisson_plan_destroy(ctx);
@@ -345,6 +345,10 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   if (p.precision != EDDY_PLAIN_FP64 && p.precision != EDDY_MIXED)
     return fail(EDDY_EINVAL, "precision must be EDDY_PLAIN_FP64 or EDDY_MIXED");
   if (p.closure != 0 && p.closure != 1) return fail(EDDY_EINVAL, "closure must be 0 (dynamic) or 1 (learned)");
+  if (p.imply != 0 && p.imply != 1) return fail(EDDY_EINVAL, "imply must be 0 or 1");
+  if (p.imply == 1 && (p.precision != EDDY_PLAIN_FP64 || p.closure != 0))
+    return fail(EDDY_EINVAL, "the implicit y terms (imply = 1) are built for the plain FP64 form with the dynamic model");
+  if (p.imply == 1 && p.ny - 2 < 3) return fail(EDDY_EINVAL, "imply = 1 needs at least 3 cells along y");
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
   // the regeneration's stream has the highest priority: its short kernels
@@ -379,6 +383,7 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   // scalars [0, 32) and the plane-flux partial sums [32, 32 + 2 * 148)
   if (cudaMalloc(&ctx->scal, sizeof(double) * 640) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
   cudaMemset(ctx->scal, 0, sizeof(double) * 640);
+  if (cudaMalloc(&ctx->diag, sizeof(double) * 600) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
   if (cudaMalloc(&ctx->err_flag, sizeof(int)) != cudaSuccess) return fail(EDDY_ENOMEM, "allocation failed");
   cudaMemset(ctx->err_flag, 0, sizeof(int));
   rc = poisson_plan_create(ctx);
@@ -431,6 +436,28 @@ int eddy_download(eddy_ctx *ctx, int field, double *host) {
   return EDDY_OK;
 }
 
+int eddy_save_field(eddy_ctx *ctx, int field, const char *path, int nstep, double time, double dtm1) {
+  if (check_ctx(ctx) || field < 0 || field >= EDDY_PLANEU || !path) return EDDY_EINVAL;
+  std::vector<double> h((size_t)ctx->d.ncell);
+  int rc = eddy_download(ctx, field, h.data());
+  if (rc) return rc;
+  rc = eddy_ioscalar_write(path, ctx->d.nx, ctx->d.ny, ctx->d.nz, h.data(), nstep, time, dtm1, ctx->sc.grav);
+  if (rc) ctx->err = std::string("cannot write the restart file ") + path;
+  return rc;
+}
+
+int eddy_load_field(eddy_ctx *ctx, int field, const char *path, int *nstep, double *time, double *dtm1,
+                    double *grav) {
+  if (check_ctx(ctx) || field < 0 || field >= EDDY_PLANEU || !path) return EDDY_EINVAL;
+  std::vector<double> h((size_t)ctx->d.ncell);
+  int rc = eddy_ioscalar_read(path, ctx->d.nx, ctx->d.ny, ctx->d.nz, h.data(), nstep, time, dtm1, grav);
+  if (rc) {
+    ctx->err = std::string("cannot read the restart file ") + path + " (missing, truncated or another grid)";
+    return rc;
+  }
+  return eddy_upload(ctx, field, h.data());
+}
+
 int eddy_get_metric(eddy_ctx *ctx, int which, double *out, int n) {
   if (check_ctx(ctx) || which < 0 || which >= 28 || !out) return -1;
   const std::vector<double> &h = ctx->h[which];
@@ -455,6 +482,15 @@ int eddy_grid_metric(const eddy_params *prm, const double *xu_faces, double ymin
 int eddy_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   return launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt);
+}
+
+int eddy_inversey(eddy_ctx *ctx, double alfxdt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  if (ctx->prm.imply != 1) {
+    ctx->err = "eddy_inversey needs imply = 1";
+    return EDDY_EINVAL;
+  }
+  return launch_inversey(ctx, alfxdt);
 }
 
 int eddy_boundary(eddy_ctx *ctx, int set) {
@@ -504,6 +540,11 @@ int eddy_turvis(eddy_ctx *ctx) {
 int eddy_ib_set_body(eddy_ctx *ctx, int nb, const double *vertices, const double *normals,
                      const double *velocity) {
   if (check_ctx(ctx) || nb < 0 || (nb > 0 && (!vertices || !normals))) return EDDY_EINVAL;
+  if (nb > 0 && ctx->prm.imply == 1) {
+    ctx->err = "an immersed body with the implicit y terms (the reference's forcing of UB, src/Eddy6.f:2490-2520) "
+               "is not supported";
+    return EDDY_EINVAL;
+  }
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
   return ib_set_body(ctx, nb, vertices, normals, velocity);
 }
@@ -639,6 +680,11 @@ int eddy_substep(eddy_ctx *ctx, int is, double dt) {
   {
     ProfScope ps(ctx, PROF_RHS_PRED);
     if ((rc = launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt))) return rc;
+  }
+  // Crank-Nicolson y lines (src/Eddy6.f:2596-2599; no immersed body)
+  if (ctx->sc.imply == 1) {
+    ProfScope ps(ctx, PROF_TRIDIAG);
+    if ((rc = launch_inversey(ctx, alfxdt))) return rc;
   }
   if ((rc = ib_overlap_regen(ctx))) return rc;
   // momforc_mod2 + velinterior (src/Eddy6.f:2526-2575)

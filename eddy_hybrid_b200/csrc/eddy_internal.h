@@ -35,6 +35,7 @@ struct Dims {
 struct Scalars {
   double ru1, prn, grav, dpdx, dpdy, dpdz, eps, css;
   int vspngx1, dspngx1, ivspngl, idspngl, idens, isgs;
+  int imply;  // IMPLY: Crank-Nicolson viscous terms along y
 };
 
 // Poisson plan (src/direct.f SAVE state): eigen-transform of the x operator.
@@ -101,11 +102,13 @@ struct eddy_ctx {
   // max(L.M,0) and M.M ((NX,NZ)); the FP32 procedure of the mixed form uses
   // the same allocations as FP32 storage
   double *gs = nullptr, *dxdydz = nullptr, *ilm2 = nullptr, *imm2 = nullptr;
+  double *diag = nullptr;  // diagnostics scratch (k_diag.cu): 2*296 partials + 2 results
   double *scal = nullptr;  // device scalars: [0] pref [1] qin1 [2] qin2 [3] dpm [4] maxdiv; [32, 328) flux partials
   PoissonPlan pp{};
   std::string err;
   int64_t launches = 0;
   double dely = 0., delysq = 0.;
+  double alfxdt_last = 0.;  // alfxdt of the last CORRECT (the IMPLY pressure correction)
   double *xc_dev = nullptr;     // x cell centres (1-based, NX+2)
   double *kappa = nullptr;      // eddy diffusivity of the learned closure (NX,NY,NZ)
   double *tv_dyn = nullptr;     // last dynamic-model nu_t: closure fallback (NX,NY,NZ)
@@ -193,6 +196,10 @@ int launch_pressure_update(eddy_ctx *ctx);
 int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
 int launch_boundinoutd_dens(eddy_ctx *ctx, double *dens);
 int launch_turvis(eddy_ctx *ctx);
+// Crank-Nicolson y lines (k_implicit.cu): INVERSEY on US, VS, WS and
+// INVERSEYD on RS (IMPLY = 1)
+int launch_inversey(eddy_ctx *ctx, double alfxdt);
+int launch_inverseyd(eddy_ctx *ctx, double alfxdt);
 // FP32 dynamic procedure on FP32 velocities (row pitch px) -> TV (FP64)
 int launch_turvis32(eddy_ctx *ctx, int px, const float *u, const float *v, const float *w, float *gs32,
                     float *imm32, float *ilm32);

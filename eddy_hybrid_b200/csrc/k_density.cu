@@ -1,7 +1,12 @@
 // k_density.cu -- density equation: RHS_DENSITY (src/rhs_density.f:4-175)
 // fused with DENSITY (src/density.f:6-99) and its sponges, plus the
 // BOUNDINOUTD / BOUNDARY_DENS ghost fills (src/boundary.f:2001-2281).
-// Explicit form: the Crank-Nicolson part RS is zero in the interior.
+// Explicit form: the Crank-Nicolson part RS is zero in the interior and the
+// update, its sponges and the ghost copy run in one pass.  With IMPLY = 1 the
+// y diffusion is the C.N. part: the predicted density goes to RS, INVERSEYD
+// solves its y lines, DENS = RS over the whole array (density.f:96-100, so
+// the ghost cells take RS's, which only BOUNDARY_DENS writes: at slip walls
+// (type 60) the x ghosts become zero, as in the reference), then the sponges.
 #include "eddy_internal.h"
 #include "tma_ring.cuh"
 #include "bc_templates.cuh"
@@ -33,6 +38,39 @@ __global__ void __launch_bounds__(DTX *DTY)
         if (i >= d.ix2 - s.dspngx1) dnew = dnew + m.dfxd[i] * (bg - dnew) * alfxdt * 1.0;
         dn[q] = dnew;
       });
+}
+
+// IMPLY = 1: RHS_DENSITY with the y diffusion as the C.N. part rt, the
+// DENSITY update with +coef*rt, no sponges yet; the predicted density to rs
+__global__ void __launch_bounds__(DTX *DTY)
+    k_density_cn(Dims d, DevMetrics m, const __grid_constant__ TmaMaps<DNF> maps, double *__restrict__ rha,
+                 double *__restrict__ rs, double repr1, double alfxdt, double gamxdt, double rhoxdt, int *err) {
+  tma_march<DNF, DTX, DTY, DKC>(
+      d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err,
+      [&](int i, int j, int k, bool active, const RingAcc<DTX, DTY, DNF> &S) {
+        if (!active) return;
+        double rt = 0.;
+        double rr = rhs_dens<double, DevMetrics, RingAcc<DTX, DTY, DNF>, true>(S, m, repr1, i, j, k, &rt);
+        double coef = 0.5 * alfxdt;
+        double dnew = S.at(0, 0, 0, 0) + gamxdt * rr + rhoxdt * S.at(5, 0, 0, 0) + coef * rt;
+        long long q = fidx(d, i, j, k);
+        rha[q] = rr;
+        rs[q] = dnew;
+      });
+}
+
+// the density sponges (density.f:103-127) on the interior
+__global__ void __launch_bounds__(256) k_dens_sponge(Dims d, DevMetrics m, Scalars s, double *dens, double alfxdt) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1, mk = d.kz2 - d.kz1 + 1;
+  if (t >= (long long)mi * mj * mk) return;
+  const int i = d.ix1 + (int)(t % mi), j = d.jy1 + (int)((t / mi) % mj), k = d.kz1 + (int)(t / ((long long)mi * mj));
+  const long long q = fidx(d, i, j, k);
+  const double bg = m.dens_bg[(i - 1) + d.nx * (j - 1)];
+  double v = dens[q];
+  if (s.idspngl == 1) v = v + m.dfxdl[k] * (bg - v) * alfxdt * 1.0;
+  if (i >= d.ix2 - s.dspngx1) v = v + m.dfxd[i] * (bg - v) * alfxdt * 1.0;
+  dens[q] = v;
 }
 
 __global__ void k_dens_ghost_copy(Dims d, const double *__restrict__ dens, double *__restrict__ dn) {
@@ -79,8 +117,22 @@ int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
     maps.m[q] = *mp;
   }
   size_t smem = ring_smem_bytes<DNF, DTX, DTY>();
-  EDDY_CUDA(cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 g((d.ix2 - d.ix1 + DTX) / DTX, (d.jy2 - d.jy1 + DTY) / DTY, (d.kz2 - d.kz1 + DKC) / DKC);
+  if (ctx->sc.imply == 1) {
+    EDDY_CUDA(cudaFuncSetAttribute(k_density_cn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_density_cn<<<g, dim3(DTX, DTY), smem, ctx->stream>>>(d, ctx->m, maps, ctx->f[EDDY_RHA], ctx->f[EDDY_RS],
+                                                          repr1, alfxdt, gamxdt, rhoxdt, ctx->err_flag);
+    EDDY_LAUNCHED(ctx);
+    if ((rc = launch_inverseyd(ctx, alfxdt))) return rc;
+    EDDY_CUDA(cudaMemcpyAsync(ctx->f[EDDY_DENS], ctx->f[EDDY_RS], sizeof(double) * (size_t)d.ncell,
+                              cudaMemcpyDeviceToDevice, ctx->stream));
+    const long long ni = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);
+    k_dens_sponge<<<(unsigned)((ni + 255) / 256), 256, 0, ctx->stream>>>(d, ctx->m, ctx->sc, ctx->f[EDDY_DENS],
+                                                                          alfxdt);
+    EDDY_LAUNCHED(ctx);
+    return launch_boundinoutd_dens(ctx, ctx->f[EDDY_DENS]);
+  }
+  EDDY_CUDA(cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_density<<<g, dim3(DTX, DTY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, ctx->f[EDDY_RHA], ctx->dens_alt,
                                                      repr1, alfxdt, gamxdt, rhoxdt, ctx->err_flag);
   EDDY_LAUNCHED(ctx);

@@ -1,0 +1,161 @@
+// k_implicit.cu -- Crank-Nicolson viscous terms along the periodic y axis
+// (IMPLY = 1, IMPLYDCMP = 0): INVERSEY (src/timeindeg.f:120-340) on the
+// predicted velocities US, VS, WS and INVERSEYD (src/density.f:383-460) on
+// the predicted density RS.
+//
+// Every (i,k) line of a component is one periodic tridiagonal system over the
+// jy1..jy2 cells, (1 + D) x = r with D the C.N. half of the y diffusion.  One
+// thread solves one line (threads along i: every row access is coalesced):
+// the corner entries by Sherman-Morrison on top of a Thomas elimination, the
+// published method of the reference's solver (src/numrec.f:754-800), in its
+// operation order, so that with -fmad=false the result is the reference
+// restatement's bit for bit.  The forward sweep writes the eliminated
+// solution in place, the multipliers and the Sherman-Morrison vector to two
+// scratch fields; two more sweeps finish the back substitution and the
+// correction.  Only the viscous part is implicit (IMPLCY = 0: the convective
+// coefficients of the reference are exact zeros).  Cartesian: rp = ru = 1.
+#include "eddy_internal.h"
+
+namespace {
+
+// row j of line (i,k): sub-, main and super-diagonal
+struct RowV {  // v: viscosity 2 tv(j) and 2 tv(j+1) on the faces (timeindeg.f:151-167)
+  const double *tv, *bv, *bp;
+  double coef, ru1;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double tvjp = 2. * tv[fidx(d, i, j + 1, k)] + ru1, tvjm = 2. * tv[fidx(d, i, j, k)] + ru1;
+    const double coefy = 1.0 * coef * bv[j] / (1.0 * 1.0);
+    a = -coefy * bp[j] * tvjm;
+    c = -coefy * bp[j + 1] * tvjp;
+    b = 1.0 + (-a - c);
+  }
+};
+struct RowW {  // w: edge viscosity averaged over four cells (timeindeg.f:220-240)
+  const double *tv, *bw, *bv;
+  double coef, ru1;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double tvjp = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k + 1)] +
+                                tv[fidx(d, i, j + 1, k)]) + ru1;
+    const double tvjm = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i, j - 1, k + 1)] +
+                                tv[fidx(d, i, j - 1, k)]) + ru1;
+    const double coefy = 1.0 * coef * bw[j] / (1.0 * 1.0);
+    a = -coefy * bv[j - 1] * tvjm;
+    c = -coefy * bv[j] * tvjp;
+    b = 1.0 + (-a - c);
+  }
+};
+struct RowU {  // u (timeindeg.f:290-312)
+  const double *tv, *bu, *bv;
+  double coef, ru1;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double tvjp = 0.25 * (tv[fidx(d, i + 1, j, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j + 1, k)] +
+                                tv[fidx(d, i, j + 1, k)]) + ru1;
+    const double tvjm = 0.25 * (tv[fidx(d, i + 1, j, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j - 1, k)] +
+                                tv[fidx(d, i, j - 1, k)]) + ru1;
+    const double coefy = 1.0 * coef * bu[j] / (1.0 * 1.0);
+    a = -coefy * bv[j - 1] * tvjm;
+    c = -coefy * bv[j] * tvjp;
+    b = 1.0 + (-a - c);
+  }
+};
+struct RowD {  // density (density.f:425-440): both faces take 0.5 (tv(j) + tv(j+1)) + ru1/prn
+  const double *tv, *bp;
+  double coef, kmol;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double tvjp = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k)]) + kmol;
+    const double tvjm = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k)]) + kmol;
+    const double coefy = 1.0 * coef * bp[j] / (1.0 * 1.0);
+    a = -coefy * bp[j - 1] * tvjm;
+    c = -coefy * bp[j] * tvjp;
+    b = 1.0 + (-a - c);
+  }
+};
+
+// lines i in [i0, i0+ni), k in [k0, k0+nk); rows jy1..jy2 (n = jy2 - 1 >= 3);
+// x: right-hand side in, solution out (in place); gam, z: scratch fields
+template <class Row>
+__global__ void __launch_bounds__(128) k_cyclic_lines(Dims d, Row row, int i0, int ni, int k0, int nk, double *x,
+                                                      double *gam, double *z) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)ni * nk) return;
+  const int i = i0 + (int)(t % ni), k = k0 + (int)(t / ni);
+  const int n = d.jy2 - 1;
+  // forward elimination of A' x = r and A' z = (gamma, 0, .., 0, alpha), A'
+  // the matrix with b1' = b1 - gamma, bn' = bn - alpha beta / gamma
+  double beta = 0., gamma = 1., bet = 1., cprev = 0., xp = 0., zp = 0.;
+  for (int r = 0; r < n; r++) {
+    const int j = d.jy1 + r;
+    const long long q = fidx(d, i, j, k);
+    double a, b, c;
+    row(d, i, j, k, a, b, c);
+    const double rr = x[q];
+    if (r == 0) {
+      beta = a;
+      gamma = -b;
+      bet = b - gamma;
+      xp = rr / bet;
+      zp = gamma / bet;
+    } else {
+      const double bb = r == n - 1 ? b - c * beta / gamma : b;
+      const double g = cprev / bet;
+      bet = bb - a * g;
+      const double u = r == n - 1 ? c : 0.;
+      xp = (rr - a * xp) / bet;
+      zp = (u - a * zp) / bet;
+      gam[q] = g;
+    }
+    x[q] = xp;
+    z[q] = zp;
+    cprev = c;
+  }
+  // back substitution (the last row stands)
+  const double xn = xp, zn = zp;
+  for (int r = n - 2; r >= 0; r--) {
+    const long long q = fidx(d, i, d.jy1 + r, k), qn = q + d.nx;
+    const double g = gam[qn];
+    xp = x[q] - g * xp;
+    zp = z[q] - g * zp;
+    x[q] = xp;
+    z[q] = zp;
+  }
+  // Sherman-Morrison correction for the two corner entries
+  const double fact = (xp + beta * xn / gamma) / (1. + zp + beta * zn / gamma);
+  for (int r = 0; r < n; r++) {
+    const long long q = fidx(d, i, d.jy1 + r, k);
+    x[q] = x[q] - fact * z[q];
+  }
+}
+
+template <class Row>
+int lines(eddy_ctx *ctx, const Row &row, int i0, int i1, int k0, int k1, double *x) {
+  const int ni = i1 - i0 + 1, nk = k1 - k0 + 1;
+  if (ni <= 0 || nk <= 0) return EDDY_OK;
+  const long long nl = (long long)ni * nk;
+  k_cyclic_lines<Row><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(ctx->d, row, i0, ni, k0, nk, x,
+                                                                              ctx->f[EDDY_UB], ctx->f[EDDY_VB]);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+}  // namespace
+
+// INVERSEY: v lines (i in [2, NX-1], k in [kz1, kz2]), then w (i in [2, NX-1],
+// k in [kbw, kew]), then u (i in [2, NX-2], k in [kz1, kz2]); REFRESHBC is a
+// no-op on one rank with non-periodic z
+int launch_inversey(eddy_ctx *ctx, double alfxdt) {
+  const Dims &d = ctx->d;
+  const DevMetrics &m = ctx->m;
+  double **f = ctx->f;
+  const double coef = 0.5 * alfxdt, ru1 = ctx->sc.ru1;
+  int rc;
+  if ((rc = lines(ctx, RowV{f[EDDY_TV], m.bv, m.bp, coef, ru1}, 2, d.nx - 1, d.kz1, d.kz2, f[EDDY_VS]))) return rc;
+  if ((rc = lines(ctx, RowW{f[EDDY_TV], m.bw, m.bv, coef, ru1}, 2, d.nx - 1, d.kbw, d.kew, f[EDDY_WS]))) return rc;
+  return lines(ctx, RowU{f[EDDY_TV], m.bu, m.bv, coef, ru1}, 2, d.nx - 2, d.kz1, d.kz2, f[EDDY_US]);
+}
+
+// INVERSEYD on RS: i in [2, NX-1], k in [kbw, kew] (the reference's w range)
+int launch_inverseyd(eddy_ctx *ctx, double alfxdt) {
+  const Dims &d = ctx->d;
+  return lines(ctx, RowD{ctx->f[EDDY_TV], ctx->m.bp, 0.5 * alfxdt, ctx->sc.ru1 / ctx->sc.prn}, 2, d.nx - 1, d.kbw, d.kew,
+               ctx->f[EDDY_RS]);
+}

@@ -31,6 +31,7 @@ struct MomAcc {
   __device__ __forceinline__ double t(int di, int dj, int dk) const { return r.at(3, di, dj, dk); }
 };
 
+template <bool IMPLY>
 __global__ void __launch_bounds__(TX *TY)
     k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const __grid_constant__ TmaMaps<NFLD> maps,
                      double *__restrict__ us, double *__restrict__ vs, double *__restrict__ ws,
@@ -47,9 +48,10 @@ __global__ void __launch_bounds__(TX *TY)
         // ---- u ----
         double uval = 0.0;
         if (kin && jin && i >= d.ibu && i <= d.ieu) {
-          double ur = rhs_u<double>(S, m, s.ru1, i, j, k);
+          double ucn = 0.0;  // the C.N. part (IMPLY), else 0
+          double ur = rhs_u<double, DevMetrics, MomAcc, IMPLY>(S, m, s.ru1, i, j, k, &ucn);
           double ustar = R.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * R.at(6, 0, 0, 0) -
-                         alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdx;
+                         alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) + coef * ucn - alfxdt * s.dpdx;
           if (s.idens == 1)
             ustar = ustar - coefd * 0.50 * s.grav *
                                 ((R.at(5, 1, 0, 0) - m.dens_bg[i + d.nx * (j - 1)]) +
@@ -63,9 +65,10 @@ __global__ void __launch_bounds__(TX *TY)
         // ---- v ----
         double vval = 0.0;
         if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
-          double vr = rhs_v<double>(S, m, s.ru1, i, j, k);
+          double vcn = 0.0;
+          double vr = rhs_v<double, DevMetrics, MomAcc, IMPLY>(S, m, s.ru1, i, j, k, &vcn);
           double vstar = R.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * R.at(7, 0, 0, 0) -
-                         alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdy;
+                         alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) + coef * vcn - alfxdt * s.dpdy;
           va[q] = vr;
           if (i >= d.ix2 - s.vspngx1) vstar = vstar + m.dfxw[i] * (0. - vstar) * alfxdt * 1.0;
           if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin)
@@ -76,9 +79,10 @@ __global__ void __launch_bounds__(TX *TY)
         // ---- w ----
         double wval = 0.0;
         if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
-          double wr = rhs_w<double>(S, m, s.ru1, i, j, k);
+          double wcn = 0.0;
+          double wr = rhs_w<double, DevMetrics, MomAcc, IMPLY>(S, m, s.ru1, i, j, k, &wcn);
           double wstar = R.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * R.at(8, 0, 0, 0) -
-                         alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) + coef * 0.0 - alfxdt * s.dpdz;
+                         alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) + coef * wcn - alfxdt * s.dpdz;
           wa[q] = wr;
           if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1. - wstar) * alfxdt * 1.0;
           if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1. - wstar) * alfxdt * 1.0;
@@ -133,19 +137,32 @@ __global__ void __launch_bounds__(BX *BY *BZ)
 }
 
 // pref = sum_j (p+dp)(ix1,j,2) / (NY-2), summed in order (src/Eddy6.f:2802)
-__global__ void k_pref(Dims d, const double *p, const double *dp, double *out) {
+// P + DP, then with IMPLY the correction of src/Eddy6.f:2775-2785 (rp = 1,
+// RVIMPLY = 1) on i in [2, ix2], j in [2, jy2], k in [2, kz2]; cimp =
+// 0.5 alfxdt ru1 / dely^2, 0 without IMPLY
+__device__ __forceinline__ double p_plus_dp(const Dims &d, const double *p, const double *dp, long long q, int i,
+                                            int j, int k, double cimp) {
+  double v = p[q] + dp[q];
+  if (cimp != 0.0 && i >= 2 && i <= d.ix2 && j >= 2 && j <= d.jy2 && k >= 2 && k <= d.kz2)
+    v = v - cimp * ((dp[q - d.nx] - 2. * dp[q]) + dp[q + d.nx]) * 1.0;
+  return v;
+}
+
+__global__ void k_pref(Dims d, const double *p, const double *dp, double *out, double cimp) {
   double s = 0.;
   for (int j = d.jy1; j <= d.jy2; j++) {
     long long q = fidx(d, d.ix1, j, 2);
-    s += p[q] + dp[q];
+    s += p_plus_dp(d, p, dp, q, d.ix1, j, 2, cimp);
   }
   out[0] = s / (double)(d.ny - 2);
 }
 
-__global__ void __launch_bounds__(256) k_pupdate(Dims d, double *p, const double *dp, const double *pref) {
+__global__ void __launch_bounds__(256)
+    k_pupdate(Dims d, double *p, const double *dp, const double *pref, double cimp) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= d.ncell) return;
-  p[q] = (p[q] + dp[q]) - pref[0];
+  const int i = 1 + (int)(q % d.nx), j = 1 + (int)((q / d.nx) % d.ny), k = 1 + (int)(q / ((long long)d.nx * d.ny));
+  p[q] = p_plus_dp(d, p, dp, q, i, j, k, cimp) - pref[0];
 }
 
 // final pressure ghosts: value of the mapped interior cell (the composition
@@ -211,11 +228,12 @@ int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rh
     maps.m[q] = *mp;
   }
   size_t smem = ring_smem_bytes<NFLD, TX, TY>();
-  EDDY_CUDA(cudaFuncSetAttribute(k_rhs_predictord, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 g((d.ix2 - d.ix1 + TX) / TX, (d.jy2 - d.jy1 + TY) / TY, (d.kz2 - d.kz1 + KCHUNK) / KCHUNK);
-  k_rhs_predictord<<<g, dim3(TX, TY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, f[EDDY_US], f[EDDY_VS],
-                                                          f[EDDY_WS], f[EDDY_UA], f[EDDY_VA], f[EDDY_WA], alfxdt,
-                                                          gamxdt, rhoxdt, ctx->err_flag);
+  auto kern = ctx->sc.imply == 1 ? k_rhs_predictord<true> : k_rhs_predictord<false>;
+  EDDY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<g, dim3(TX, TY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, f[EDDY_US], f[EDDY_VS], f[EDDY_WS],
+                                              f[EDDY_UA], f[EDDY_VA], f[EDDY_WA], alfxdt, gamxdt, rhoxdt,
+                                              ctx->err_flag);
   EDDY_LAUNCHED(ctx);
   long long nghost = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
   k_zero_faces3<<<(unsigned)((nghost + 255) / 256), 256, 0, ctx->stream>>>(d, f[EDDY_US], f[EDDY_VS],
@@ -237,6 +255,7 @@ int launch_boundinout(eddy_ctx *ctx, double *ubc, double *vbc, double *wbc, cons
 
 int launch_correct(eddy_ctx *ctx, double alfxdt) {
   const Dims &d = ctx->d;
+  ctx->alfxdt_last = alfxdt;
   double **f = ctx->f;
   k_correct<<<grid3(d), dim3(BX, BY, BZ), 0, ctx->stream>>>(d, ctx->m, f[EDDY_US], f[EDDY_VS], f[EDDY_WS],
                                                             f[EDDY_DP], f[EDDY_UO], f[EDDY_VO], f[EDDY_WO],
@@ -248,9 +267,11 @@ int launch_correct(eddy_ctx *ctx, double alfxdt) {
 int launch_pressure_update(eddy_ctx *ctx) {
   const Dims &d = ctx->d;
   double *p = ctx->f[EDDY_P], *dp = ctx->f[EDDY_DP];
-  k_pref<<<1, 1, 0, ctx->stream>>>(d, p, dp, ctx->scal);
+  const double cimp = ctx->sc.imply == 1 ? 0.5 * ctx->alfxdt_last * ctx->sc.ru1 / ((ctx->dely * 1.0) * (ctx->dely * 1.0))
+                                         : 0.0;
+  k_pref<<<1, 1, 0, ctx->stream>>>(d, p, dp, ctx->scal, cimp);
   EDDY_LAUNCHED(ctx);
-  k_pupdate<<<(unsigned)((d.ncell + 255) / 256), 256, 0, ctx->stream>>>(d, p, dp, ctx->scal);
+  k_pupdate<<<(unsigned)((d.ncell + 255) / 256), 256, 0, ctx->stream>>>(d, p, dp, ctx->scal, cimp);
   EDDY_LAUNCHED(ctx);
   // immersed body: correctpres_mod2 + presinterior (src/Eddy6.f:2881-2897)
   if (ctx->ib) {

@@ -1,12 +1,13 @@
 // stencil_density.cuh -- density right-hand side of src/rhs_density.f:55-165
-// (Cartesian, explicit diffusion), templated on the arithmetic type T and on
+// (Cartesian; CN = true: IMPLY = 1, the y diffusion returned as the
+// Crank-Nicolson part in *cn), templated on the arithmetic type T and on
 // a neighbour accessor: S.at(f, di, dj, dk) with f = 0 density, 1 eddy
 // diffusivity, 2 u, 3 v, 4 w.  With T = double the operation order is the
 // reference's (the plain form is compiled with -fmad=false).
 #pragma once
 
-template <class T, class M, class Acc>
-__device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, int j, int k) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, int j, int k, T *cn = nullptr) {
   auto dens = [&](int a, int b, int c) { return S.at(0, a, b, c); };
   auto kv = [&](int a, int b, int c) { return S.at(1, a, b, c); };
   T qxp = S.at(2, 0, 0, 0), qxm = S.at(2, -1, 0, 0);
@@ -42,5 +43,10 @@ __device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, 
   T t11 = m.ap[i] * (txxp - txxm);
   T t22 = m.bp[j] * (tyyp - tyym);
   T t33 = m.cp[k] * (tzzp - tzzm);
+  if (CN) {
+    // IMPLY = 1 (src/rhs_density.f:149-156): the y diffusion is the C.N. part
+    *cn = t22;
+    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33;
+  }
   return h11 + h22 + h33 + t11 + t22 + t33;
 }

@@ -1,5 +1,6 @@
 // stencil_rhs.cuh -- explicit momentum right-hand side of src/rhs.f:4-438
-// (Cartesian, explicit branch), templated on the arithmetic type T and on a
+// (Cartesian; CN = true: IMPLY = 1, the y viscous term returned as the
+// Crank-Nicolson part in *cn), templated on the arithmetic type T and on a
 // neighbour accessor: S.u/v/w/t(di,dj,dk) return uo/vo/wo/tv at the offset
 // from the current cell.  With T = double the operation order is exactly the
 // reference's (the plain form is compiled with -fmad=false); with T = float
@@ -8,8 +9,8 @@
 
 // ---------------------------------------------------------------------------
 // u-momentum explicit RHS at a u point (src/rhs.f:77-172)
-template <class T, class M, class Acc>
-__device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j, int k) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
   T qxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * T(0.5);
   T qxm = (S.u(0, 0, 0) + S.u(-1, 0, 0)) * T(0.5);
   T uxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * T(0.5);
@@ -54,12 +55,17 @@ __device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j
   T t33 = m.cu[k] * (tzzp - tzzm);
   T s22 = m.bu[j] * (txyp - txym);
   T s33 = m.cu[k] * (txzp - txzm);
+  if (CN) {
+    // IMPLY = 1 (src/rhs.f:175-191): the y viscous term is the C.N. part
+    *cn = t22;
+    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33 + s22 + s33;
+  }
   return h11 + h22 + h33 + t11 + t22 + t33 + s22 + s33;
 }
 
 // v-momentum (src/rhs.f:219-321)
-template <class T, class M, class Acc>
-__device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j, int k) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
   T vxp = (S.v(1, 0, 0) + S.v(0, 0, 0)) * T(0.5);
   T vxm = (S.v(0, 0, 0) + S.v(-1, 0, 0)) * T(0.5);
   T vyp = (S.v(0, 1, 0) + S.v(0, 0, 0)) * T(0.5);
@@ -102,12 +108,16 @@ __device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j
   T t33 = m.cv[k] * (tzzp - tzzm);
   T s11 = m.av[i] * (txyp - txym);
   T s33 = m.cv[k] * (tyzp - tyzm);
+  if (CN) {
+    *cn = t22;
+    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33 + s11 + s33;
+  }
   return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s33;
 }
 
 // w-momentum (src/rhs.f:347-422)
-template <class T, class M, class Acc>
-__device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j, int k) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
   T wxp = (S.w(1, 0, 0) + S.w(0, 0, 0)) * T(0.5);
   T wxm = (S.w(0, 0, 0) + S.w(-1, 0, 0)) * T(0.5);
   T wyp = (S.w(0, 1, 0) + S.w(0, 0, 0)) * T(0.5);
@@ -150,6 +160,10 @@ __device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j
   T t33 = m.cw[k] * (tzzp - tzzm);
   T s11 = m.aw[i] * (txzp - txzm);
   T s22 = m.bw[j] * (tyzp - tyzm);
+  if (CN) {
+    *cn = t22;
+    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33 + s11 + s22;
+  }
   return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s22;
 }
 

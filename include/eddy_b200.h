@@ -59,6 +59,12 @@ typedef struct {
   int precision;             /* EDDY_PLAIN_FP64 or EDDY_MIXED */
   int refine_sweeps;         /* mixed form: FP64-residual refinement sweeps (1-3) */
   int closure;               /* 0 = dynamic TURVIS, 1 = learned MLP closure */
+  int imply;                 /* IMPLY (src/inpall.f:42): 1 = the viscous terms along y
+                                Crank-Nicolson implicit (INVERSEY src/timeindeg.f:120,
+                                INVERSEYD src/density.f:383), over the whole x range
+                                (IMPLYDCMP = 0); plain form without an immersed body.
+                                The implicit convective and x terms (IMPLCY, IMPLX,
+                                IMPLCX) are not supported. */
 } eddy_params;
 
 typedef struct eddy_ctx eddy_ctx;
@@ -76,6 +82,24 @@ int eddy_destroy(eddy_ctx *ctx);
 /* Copy a field between the host (Fortran-ordered FP64) and the device. */
 int eddy_upload(eddy_ctx *ctx, int field, const double *host);
 int eddy_download(eddy_ctx *ctx, int field, double *host);
+/* Restart files in the layout of the reference's IOSCALAR (src/io.f:114-200,
+ * serial case; written at src/Eddy6.f:3391-3408, read at :780-803):
+ * Fortran unformatted sequential records with 4-byte length markers --
+ * (NX, NY, NZ, 1) int32, one record of NX*NY float64 per z plane, nstep
+ * int32, TIME float64, (DTM1, grav) float64.  Host-only functions on a
+ * Fortran-ordered (NX,NY,NZ) array; reading refuses a file of another grid
+ * or a truncated one with EDDY_EINVAL. */
+int eddy_ioscalar_write(const char *path, int nx, int ny, int nz, const double *a, int nstep, double time,
+                        double dtm1, double grav);
+int eddy_ioscalar_read(const char *path, int nx, int ny, int nz, double *a, int *nstep, double *time,
+                       double *dtm1, double *grav);
+/* The same from and to a device field (one of the (NX,NY,NZ) fields; grav
+ * written is the context's).  A restart is UO, VO, WO, P, TV and DENS
+ * (the reference's set); stepping continues from them without
+ * eddy_initialize.  Null out-pointers are skipped. */
+int eddy_save_field(eddy_ctx *ctx, int field, const char *path, int nstep, double time, double dtm1);
+int eddy_load_field(eddy_ctx *ctx, int field, const char *path, int *nstep, double *time, double *dtm1,
+                    double *grav);
 /* Read one of the 1-D metric arrays the context built (same numbering as the
  * oracle: 0 xu 1 xc 2 ap 3 au 4 av 5 aw 6 yv 7 yc 8 bp 9 bu 10 bv 11 bw
  * 12 zw 13 zc 14 cp 15 cu 16 cv 17 cw 18 whx 19 why 20 whz 21 dfxu 22 dfxw
@@ -90,6 +114,10 @@ int eddy_grid_metric(const eddy_params *prm, const double *xu_faces, double ymin
 /* RHS (src/rhs.f:4) fused with PREDICTORD (src/timeindeg.f:1041): uo,vo,wo,
  * tv,p,dens,ua.. -> us,vs,ws (u*), ua,va,wa (new explicit RHS). */
 int eddy_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
+/* INVERSEY (src/timeindeg.f:120-340): the Crank-Nicolson y lines of US, VS,
+ * WS after the predictor, viscous part (imply = 1 only).  The density's
+ * INVERSEYD (src/density.f:383) runs inside eddy_density when imply = 1. */
+int eddy_inversey(eddy_ctx *ctx, double alfxdt);
 /* BOUNDARY (src/boundary.f:7) on the provisional (set=0: US,VS,WS) or the
  * corrected (set=1: UO,VO,WO) velocity. */
 int eddy_boundary(eddy_ctx *ctx, int set);
@@ -170,6 +198,14 @@ int eddy_refine_residuals(eddy_ctx *ctx, double *out, int n);
 
 /* Diagnostics: max |div u| of (UO,VO,WO) over the interior (src/info.f:32). */
 int eddy_max_divergence(eddy_ctx *ctx, double *out);
+/* CALCFL (src/timestep.f:2-78), Cartesian: the interior maximum of the
+ * per-cell max of the convective constraints |u|/dx and the viscous ones
+ * 2 (ru1 + tv)/dx^2 per axis (the y viscous one dropped with imply = 1); the
+ * reference's constant-CFL run takes DTM1 = CFLC / CFLM (src/Eddy6.f:2118). */
+int eddy_cfl(eddy_ctx *ctx, double *cflm);
+/* SCRINFO's extrema (src/info.f:5-164): min and max of a field over the
+ * interior. */
+int eddy_field_extrema(eddy_ctx *ctx, int field, double *vmin, double *vmax);
 
 /* Kernel-category timing with CUDA events on the context stream (the
  * device-side counterpart of the reference's CLOCK array, src/info.f:350 and

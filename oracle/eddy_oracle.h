@@ -40,6 +40,7 @@ typedef struct {
   double eps;              /* dynamic-model cutoff (IMM > sqrt(eps)) */
   double css;              /* Smagorinsky constant */
   int vspngx1, dspngx1, vspngx3in, vspngx3out, dspngx3in, dspngx3out;
+  int imply;               /* 1: Crank-Nicolson viscous terms along y (INVERSEY/INVERSEYD) */
 } eo_params;
 
 /* 1-D metric arrays (src/common.h:51-54), 1-based: arrays have n+1 entries. */
@@ -85,6 +86,7 @@ typedef struct {
       *uc, *vc, *wc, *dxdydz, *cles;
   double *planeU, *planeV, *planeW, *planeD; /* (NX,NY) inflow planes */
   double time;
+  double alfxdt_last; /* alfxdt of the last CORRECT (the pressure update's implicit correction) */
   double pref_last;
   double qin_last, qout_last;
   struct eo_ib *ib;  /* immersed body (NULL: none) */
@@ -117,6 +119,16 @@ void eo_correct(eo_state *s, double alfxdt);
 void eo_pressure_update(eo_state *s);
 void eo_rhs_density(eo_state *s);
 void eo_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt);
+/* INVERSEY (src/timeindeg.f:120-340) on US,VS,WS and INVERSEYD
+ * (src/density.f:383-460) on RS: the Crank-Nicolson y lines, IMPLY = 1 */
+void eo_inversey(eo_state *s, double alfxdt);
+/* CALCFL (src/timestep.f:2-78): CFLM over the interior */
+double eo_calcfl(eo_state *s);
+void eo_inverseyd(eo_state *s, double alfxdt);
+/* periodic tridiagonal system (cyclic, src/numrec.f:754-779): n unknowns,
+ * a sub-, b main, c super-diagonal, alpha = A(n,1), beta = A(1,n); work >= 4n */
+void eo_cyclic(const double *a, const double *b, const double *c, double alpha, double beta, const double *r,
+               double *x, int n, double *work);
 void eo_boundary_dens(eo_state *s, double *d);
 void eo_boundinoutd(eo_state *s, double *d);
 void eo_turvis(eo_state *s);

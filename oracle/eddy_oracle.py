@@ -32,7 +32,7 @@ class Params(C.Structure):
                 ("dpdy", C.c_double), ("dpdz", C.c_double), ("eps", C.c_double),
                 ("css", C.c_double), ("vspngx1", C.c_int), ("dspngx1", C.c_int),
                 ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
-                ("dspngx3in", C.c_int), ("dspngx3out", C.c_int)]
+                ("dspngx3in", C.c_int), ("dspngx3out", C.c_int), ("imply", C.c_int)]
 
 
 class IBSet(C.Structure):
@@ -93,6 +93,9 @@ def lib():
         L.eo_pressure_update.argtypes = [C.c_void_p]
         L.eo_rhs_density.argtypes = [C.c_void_p]
         L.eo_call_rhs_predictord.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.eo_inversey.argtypes = [C.c_void_p, C.c_double]
+        L.eo_calcfl.argtypes = [C.c_void_p]
+        L.eo_calcfl.restype = C.c_double
         L.eo_call_density.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
         L.eo_call_boundary.argtypes = [C.c_void_p, C.c_int]
         L.eo_call_boundinout.argtypes = [C.c_void_p, C.c_int, C.c_double]
@@ -218,6 +221,12 @@ class OracleSolver:
     # one method per product C-ABI entry point
     def rhs_predictord(self, alf, gam, rho):
         lib().eo_call_rhs_predictord(self.h, alf, gam, rho)
+
+    def inversey(self, alf):
+        lib().eo_inversey(self.h, alf)
+
+    def calcfl(self) -> float:
+        return lib().eo_calcfl(self.h)
 
     def boundary(self, set_):
         lib().eo_call_boundary(self.h, set_)

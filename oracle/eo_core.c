@@ -3,8 +3,11 @@
  * fractional step.  TEST INFRASTRUCTURE ONLY.  Compiled with
  * -ffp-contract=off so every expression keeps the reference's operation order.
  *
- * Cartesian branch only (icyl=0, ru=rp=1), explicit viscous/convective terms
- * (implx=imply=implcx=implcy=0: the Crank-Nicolson parts ut,vt,wt are zero).
+ * Cartesian branch only (icyl=0, ru=rp=1).  The viscous terms along y may be
+ * Crank-Nicolson implicit (IMPLY = 1, over the whole x range): RHS then keeps
+ * them out of the explicit part and returns them as the C.N. parts ut,vt,wt
+ * (src/rhs.f:175-191), INVERSEY/INVERSEYD solve the periodic y lines; the
+ * other implicit options (implx, implcx, implcy) are 0.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -121,6 +124,8 @@ void eo_rhs(eo_state *s, const double *uo, const double *vo, const double *wo,
   const double *bp = g->bp, *bu = g->bu, *bv = g->bv, *bw = g->bw;
   const double *cp = g->cp, *cu = g->cu, *cv = g->cv, *cw = g->cw;
   long n = s->ncell;
+  /* rflag* of src/rhs.f:49-52 with ruimply = rvimply = 1 (IMPLYDCMP = 0) */
+  const double rflagx = 0., rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
   memcpy(qr, uo, sizeof(double) * (size_t)n);
   memset(ut, 0, sizeof(double) * (size_t)n); memset(ur, 0, sizeof(double) * (size_t)n);
   memset(vt, 0, sizeof(double) * (size_t)n); memset(vr, 0, sizeof(double) * (size_t)n);
@@ -174,7 +179,9 @@ void eo_rhs(eo_state *s, const double *uo, const double *vo, const double *wo,
         double t33 = cu[k] * (tzzp - tzzm);
         double s22 = bu[j] * (txyp - txym);
         double s33 = cu[k] * (txzp - txzm);
-        A(ur, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33 + s22 + s33;
+        A(ur, i, j, k) = (1. - rflagcx * 1.) * h11 + (1. - rflagcy * 1.) * h22 + h33 + (1. - rflagx * 1.) * t11 +
+                         (1. - rflagy * 1.) * t22 + t33 + s22 + s33;
+        A(ut, i, j, k) = rflagx * 1. * t11 + rflagy * 1. * t22 + rflagcx * 1. * h11 + rflagcy * 1. * h22;
       }
   /* v component (rhs.f:219-335) */
 #pragma omp parallel for schedule(static)
@@ -223,7 +230,9 @@ void eo_rhs(eo_state *s, const double *uo, const double *vo, const double *wo,
         double t33 = cv[k] * (tzzp - tzzm);
         double s11 = av[i] * (txyp - txym);
         double s33 = cv[k] * (tyzp - tyzm);
-        A(vr, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33 + s11 + s33;
+        A(vr, i, j, k) = (1. - rflagcx * 1.) * h11 + (1. - rflagcy * 1.) * h22 + h33 + (1. - rflagx * 1.) * t11 +
+                         (1. - rflagy * 1.) * t22 + t33 + s11 + s33;
+        A(vt, i, j, k) = rflagx * 1. * t11 + rflagy * 1. * t22 + rflagcx * 1. * h11 + rflagcy * 1. * h22;
       }
   /* w component (rhs.f:347-428) */
 #pragma omp parallel for schedule(static)
@@ -272,7 +281,9 @@ void eo_rhs(eo_state *s, const double *uo, const double *vo, const double *wo,
         double t33 = cw[k] * (tzzp - tzzm);
         double s11 = aw[i] * (txzp - txzm);
         double s22 = bw[j] * (tyzp - tyzm);
-        A(wr, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33 + s11 + s22;
+        A(wr, i, j, k) = (1. - rflagcx * 1.) * h11 + (1. - rflagcy * 1.) * h22 + h33 + (1. - rflagx * 1.) * t11 +
+                         (1. - rflagy * 1.) * t22 + t33 + s11 + s22;
+        A(wt, i, j, k) = rflagx * 1. * t11 + rflagy * 1. * t22 + rflagcx * 1. * h11 + rflagcy * 1. * h22;
       }
 }
 
@@ -549,6 +560,7 @@ void eo_divergence(eo_state *s, const double *us, const double *vs, const double
 
 /* CORRECT: src/timeindeg.f:981-1028: (us,vs,ws,dp) -> (uo,vo,wo) */
 void eo_correct(eo_state *s, double alfxdt) {
+  s->alfxdt_last = alfxdt;
   const eo_grid *g = s->g;
   double *uo = s->uo, *vo = s->vo, *wo = s->wo, *us = s->us, *vs = s->vs, *ws = s->ws, *dp = s->dp;
 #pragma omp parallel for schedule(static)
@@ -575,6 +587,17 @@ void eo_pressure_update(eo_state *s) {
   const int *it = s->prm.itype;
   double *p = s->p, *dp = s->dp;
   for (long q = 0; q < s->ncell; q++) p[q] = p[q] + dp[q];
+  /* implicit y terms: the extra pressure correction (src/Eddy6.f:2775-2785;
+   * rp = 1, RVIMPLY = 1); every right-hand value is the pre-update P */
+  if (s->prm.imply == 1) {
+    const double c = 0.5 * s->alfxdt_last * s->prm.ru1 / ((g->dely * 1.0) * (g->dely * 1.0));
+#pragma omp parallel for schedule(static)
+    for (int k = 2; k <= g->kz2; k++)
+      for (int j = 2; j <= g->jy2; j++)
+        for (int i = 2; i <= g->ix2; i++)
+          A(p, i, j, k) = A(p, i, j, k) -
+                          c * ((A(dp, i, j - 1, k) - 2. * A(dp, i, j, k)) + A(dp, i, j + 1, k)) * 1.0;
+  }
   double pref = 0.;
   for (int j = g->jy1; j <= g->jy2; j++) pref += A(p, g->ix1, j, 2);
   pref = pref / (double)(NY - 2);
@@ -605,12 +628,14 @@ void eo_pressure_update(eo_state *s) {
   else { fill_y_plane(g, p, 1, g->jy1, 1., 0); fill_y_plane(g, p, NY, g->jy2, 1., 0); }
 }
 
-/* RHS_DENSITY: src/rhs_density.f:4-175 (rr -> rhb, rt -> rs; explicit) */
+/* RHS_DENSITY: src/rhs_density.f:4-175 (rr -> rhb, rt -> rs: the explicit
+ * part and the C.N. part, the y diffusion when IMPLY = 1) */
 void eo_rhs_density(eo_state *s) {
   const eo_grid *g = s->g;
   double *uo = s->uo, *vo = s->vo, *wo = s->wo, *dens = s->dens, *kv = s->tv;
   double *rr = s->rhb, *rt = s->rs;
   double repr1 = s->prm.ru1 / s->prm.prn;
+  const double rflagx = 0., rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
   memset(rr, 0, sizeof(double) * (size_t)s->ncell);
 #pragma omp parallel for schedule(static)
   for (int k = g->kz1; k <= g->kz2; k++)
@@ -649,8 +674,9 @@ void eo_rhs_density(eo_state *s) {
         double t11 = g->ap[i] * (txxp - txxm);
         double t22 = g->bp[j] * (tyyp - tyym);
         double t33 = g->cp[k] * (tzzp - tzzm);
-        A(rr, i, j, k) = h11 + h22 + h33 + t11 + t22 + t33;
-        A(rt, i, j, k) = 0.;
+        A(rr, i, j, k) = (1. - rflagcx * 1.) * h11 + (1. - rflagcy * 1.) * h22 + h33 + (1. - rflagx * 1.) * t11 +
+                         (1. - rflagy * 1.) * t22 + t33;
+        A(rt, i, j, k) = rflagx * 1. * t11 + rflagy * 1. * t22 + rflagcx * 1. * h11 + rflagcy * 1. * h22;
       }
 }
 
@@ -715,6 +741,12 @@ void eo_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
       }
   for (long q = 0; q < s->ncell; q++) rhb[q] = rs[q] + 0.5 * alfxdt * rhb[q];
   eo_boundary_dens(s, rhb);
+  /* implicit y diffusion, then the whole array is copied (density.f:96-100):
+   * ghost cells take RS's, which nothing above writes but BOUNDARY_DENS */
+  if (s->prm.imply == 1) {
+    eo_inverseyd(s, alfxdt);
+    memcpy(dens, rs, sizeof(double) * (size_t)s->ncell);
+  }
   if (g->idspngl == 1) {
 #pragma omp parallel for schedule(static)
     for (int k = g->kz1; k <= g->kz2; k++)
@@ -727,4 +759,151 @@ void eo_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
     for (int j = g->jy1; j <= g->jy2; j++)
       for (int i = g->ix2 - s->prm.dspngx1; i <= g->ix2; i++)
         A(dens, i, j, k) = A(dens, i, j, k) + g->dfxd[i] * (DBG(i, j) - A(dens, i, j, k)) * alfxdt * 1.0;
+}
+
+
+/* ---- Crank-Nicolson y lines ----
+ * cyclic: the Sherman-Morrison treatment of the two corner entries on top of
+ * the Thomas elimination (the published method of src/numrec.f:754-800),
+ * with its operation order: gamma = -b1, b1' = b1 - gamma,
+ * bn' = bn - alpha*beta/gamma; solve A' x = r and A' z = (gamma,0..0,alpha);
+ * x -= z (x1 + beta xn / gamma) / (1 + z1 + beta zn / gamma). */
+static void thomas(const double *a, const double *b, const double *c, const double *r, double *u, int n,
+                   double *gam) {
+  double bet = b[0];
+  u[0] = r[0] / bet;
+  for (int j = 1; j < n; j++) {
+    gam[j] = c[j - 1] / bet;
+    bet = b[j] - a[j] * gam[j];
+    u[j] = (r[j] - a[j] * u[j - 1]) / bet;
+  }
+  for (int j = n - 2; j >= 0; j--) u[j] = u[j] - gam[j + 1] * u[j + 1];
+}
+
+void eo_cyclic(const double *a, const double *b, const double *c, double alpha, double beta, const double *r,
+               double *x, int n, double *work) {
+  double *bb = work, *u = work + n, *z = work + 2 * n, *gam = work + 3 * n;
+  const double gamma = -b[0];
+  bb[0] = b[0] - gamma;
+  bb[n - 1] = b[n - 1] - alpha * beta / gamma;
+  for (int i = 1; i < n - 1; i++) bb[i] = b[i];
+  thomas(a, bb, c, r, x, n, gam);
+  u[0] = gamma;
+  u[n - 1] = alpha;
+  for (int i = 1; i < n - 1; i++) u[i] = 0.;
+  thomas(a, bb, c, u, z, n, gam);
+  const double fact = (x[0] + beta * x[n - 1] / gamma) / (1. + z[0] + beta * z[n - 1] / gamma);
+  for (int i = 0; i < n; i++) x[i] = x[i] - fact * z[i];
+}
+
+/* INVERSEY (src/timeindeg.f:120-340), viscous part (implcy = 0: the
+ * convective coefficients and right-hand-side terms are exact zeros),
+ * Cartesian (rp = ru = 1), IMPLYDCMP = 0: v lines for i in [2, NX-1],
+ * w lines for i in [2, NX-1] and k in [kbw, kew], u lines for i in [2, NX-2];
+ * j periodic over [jy1, jy2].  REFRESHBC is a no-op on one rank with
+ * non-periodic z. */
+void eo_inversey(eo_state *s, double alfxdt) {
+  const eo_grid *g = s->g;
+  const double coef = 0.5 * alfxdt, ru1 = s->prm.ru1, rflagy = 1.0;
+  const int n = g->jy2 - 1;
+  double *us = s->us, *vs = s->vs, *ws = s->ws;
+  const double *tv = s->tv;
+  const double *bp = g->bp, *bu = g->bu, *bv = g->bv, *bw = g->bw;
+#pragma omp parallel
+  {
+    double *ay = malloc(sizeof(double) * n), *by = malloc(sizeof(double) * n), *cy = malloc(sizeof(double) * n),
+           *ry = malloc(sizeof(double) * n), *x = malloc(sizeof(double) * n), *wk = malloc(sizeof(double) * 4 * n);
+    /* v */
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kz1; k <= g->kz2; k++)
+      for (int i = 2; i <= NX - 1; i++) {
+        for (int j = g->jbv; j <= g->jev; j++) {
+          const int jj = j - 2;
+          const double tvjp = 2. * A(tv, i, j + 1, k) + ru1, tvjm = 2. * A(tv, i, j, k) + ru1;
+          ry[jj] = A(vs, i, j, k);
+          const double coefy = rflagy * coef * bv[j] / (1.0 * 1.0);
+          const double ayv = -coefy * bp[j] * tvjm, cyv = -coefy * bp[j + 1] * tvjp, byv = -ayv - cyv;
+          ay[jj] = ayv;
+          cy[jj] = cyv;
+          by[jj] = 1.0 + byv;
+        }
+        eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
+        for (int j = g->jbv; j <= g->jev; j++) A(vs, i, j, k) = x[j - 2];
+      }
+    /* w */
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kbw; k <= g->kew; k++)
+      for (int i = 2; i <= NX - 1; i++) {
+        for (int j = g->jy1; j <= g->jy2; j++) {
+          const int jj = j - 2;
+          const double tvjp =
+              0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i, j + 1, k + 1) + A(tv, i, j + 1, k)) + ru1;
+          const double tvjm =
+              0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i, j - 1, k + 1) + A(tv, i, j - 1, k)) + ru1;
+          ry[jj] = A(ws, i, j, k);
+          const double coefy = rflagy * coef * bw[j] / (1.0 * 1.0);
+          const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+          ay[jj] = ayv;
+          cy[jj] = cyv;
+          by[jj] = 1.0 + byv;
+        }
+        eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
+        for (int j = g->jy1; j <= g->jy2; j++) A(ws, i, j, k) = x[j - 2];
+      }
+    /* u */
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kz1; k <= g->kz2; k++)
+      for (int i = 2; i <= NX - 2; i++) {
+        for (int j = g->jy1; j <= g->jy2; j++) {
+          const int jj = j - 2;
+          const double tvjp =
+              0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j + 1, k) + A(tv, i, j + 1, k)) + ru1;
+          const double tvjm =
+              0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j - 1, k) + A(tv, i, j - 1, k)) + ru1;
+          ry[jj] = A(us, i, j, k);
+          const double coefy = rflagy * coef * bu[j] / (1.0 * 1.0);
+          const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+          ay[jj] = ayv;
+          cy[jj] = cyv;
+          by[jj] = 1.0 + byv;
+        }
+        eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
+        for (int j = g->jy1; j <= g->jy2; j++) A(us, i, j, k) = x[j - 2];
+      }
+    free(ay); free(by); free(cy); free(ry); free(x); free(wk);
+  }
+}
+
+/* INVERSEYD (src/density.f:383-460) on RS: k in [kbw, kew], i in [2, NX-1],
+ * and, as there, the same face diffusivity 0.5(tv(j) + tv(j+1)) + ru1/prn on
+ * both sides of a cell */
+void eo_inverseyd(eo_state *s, double alfxdt) {
+  const eo_grid *g = s->g;
+  const double coef = 0.5 * alfxdt, rflagy = 1.0, kmol = s->prm.ru1 / s->prm.prn;
+  const int n = g->jy2 - 1;
+  double *rs = s->rs;
+  const double *tv = s->tv, *bp = g->bp;
+#pragma omp parallel
+  {
+    double *ay = malloc(sizeof(double) * n), *by = malloc(sizeof(double) * n), *cy = malloc(sizeof(double) * n),
+           *ry = malloc(sizeof(double) * n), *x = malloc(sizeof(double) * n), *wk = malloc(sizeof(double) * 4 * n);
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kbw; k <= g->kew; k++)
+      for (int i = 2; i <= NX - 1; i++) {
+        for (int j = g->jy1; j <= g->jy2; j++) {
+          const int jj = j - 2;
+          const double tvjp = 0.5 * (A(tv, i, j, k) + A(tv, i, j + 1, k)) + kmol;
+          const double tvjm = 0.5 * (A(tv, i, j, k) + A(tv, i, j + 1, k)) + kmol;
+          ry[jj] = A(rs, i, j, k);
+          const double coefy = rflagy * coef * bp[j] / (1.0 * 1.0);
+          const double ayv = -coefy * bp[j - 1] * tvjm, cyv = -coefy * bp[j] * tvjp, byv = -ayv - cyv;
+          ay[jj] = ayv;
+          cy[jj] = cyv;
+          by[jj] = 1.0 + byv;
+        }
+        eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
+        for (int j = g->jy1; j <= g->jy2; j++) A(rs, i, j, k) = x[j - 2];
+      }
+    free(ay); free(by); free(cy); free(ry); free(x); free(wk);
+  }
 }

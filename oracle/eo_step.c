@@ -46,6 +46,8 @@ void eo_substep(eo_state *s, int is, double dtm1) {
     eo_ib_interior(s->ib, 1, s->vs, vel[1]);
     eo_ib_interior(s->ib, 2, s->ws, vel[2]);
   }
+  /* Crank-Nicolson y lines (:2596-2599; the IBM = 0 sequence) */
+  if (s->prm.imply == 1) eo_inversey(s, alfxdt);
   /* :2689-2704 */
   eo_boundary(s, s->us, s->vs, s->ws);
   eo_boundinout(s, s->us, s->vs, s->ws, s->uo, s->vo, s->wo, alfxdt, 1);
@@ -189,4 +191,30 @@ double eo_max_divergence(eo_state *s) {
       }
 #undef OA
   return mx;
+}
+
+/* CALCFL (src/timestep.f:2-78), Cartesian: CONST = 2, rp = 1, the implicit
+ * flags RFLAGY = IMPLY, the others 0; returns CFLM over the interior */
+double eo_calcfl(eo_state *s) {
+  const eo_grid *g = s->g;
+  const double cst = 2., rflagx = 0., rflagcx = 0., rflagcy = 0., rflagy = (double)s->prm.imply;
+  const int nx = g->nx, ny = g->ny;
+  double cflm = 0.;
+  for (int k = g->kz1; k <= g->kz2; k++)
+    for (int j = g->jy1; j <= g->jy2; j++)
+      for (int i = g->ix1; i <= g->ix2; i++) {
+        const size_t q = (size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1));
+        const double cflx = (1. - rflagcx * 1.) * 0.5 * fabs(s->uo[q - 1] + s->uo[q]) * g->ap[i];
+        const double cfly = (1. - rflagcy * 1.) * 0.5 * fabs(s->vo[q - nx] + s->vo[q]) * g->bp[j] / 1.0;
+        const double cflz = 0.5 * fabs(s->wo[q - (size_t)nx * ny] + s->wo[q]) * g->cp[k];
+        const double totvx = s->prm.ru1 + s->tv[q];
+        const double cflvx = (1. - rflagx * 1.) * (g->ap[i] * g->ap[i]);
+        const double by = g->bp[j] / 1.0;
+        const double cflvy = (1. - rflagy * 1.) * (by * by);
+        const double cflvz = g->cp[k] * g->cp[k];
+        double c = fmax(fmax(fmax(cflx, cfly), fmax(cflz, cst * totvx * cflvx)),
+                        fmax(cst * totvx * cflvy, cst * totvx * cflvz));
+        cflm = fmax(cflm, c);
+      }
+  return cflm;
 }

@@ -80,3 +80,42 @@ def test_download_checks_the_callers_buffer_before_copying(product):
                 ro):                                        # read-only
         with pytest.raises(ValueError):
             s.download("uo", out=bad)
+
+
+def test_restart_file_layout_is_ioscalars(product, tmp_path):
+    # the reference's IOSCALAR (src/io.f:150-175, serial): Fortran unformatted
+    # records framed by 4-byte lengths -- (NX, NY, NZ, 1), one NX*NY plane per
+    # k, nstep, TIME, (DTM1, grav)
+    nx, ny, nz = 5, 4, 3
+    a = np.asfortranarray(np.arange(nx * ny * nz, dtype=np.float64).reshape((nx, ny, nz), order="F") * 0.25 - 3.0)
+    path = str(tmp_path / "u_00000042.res")
+    product.write_ioscalar(path, a, 42, 1.5, 5e-4, 1.0)
+    raw = open(path, "rb").read()
+    pos = 0
+
+    def rec(nbytes):
+        nonlocal pos
+        n0 = int(np.frombuffer(raw, np.int32, 1, pos)[0])
+        assert n0 == nbytes
+        body = raw[pos + 4: pos + 4 + nbytes]
+        n1 = int(np.frombuffer(raw, np.int32, 1, pos + 4 + nbytes)[0])
+        assert n1 == nbytes
+        pos += nbytes + 8
+        return body
+
+    assert list(np.frombuffer(rec(16), np.int32)) == [nx, ny, nz, 1]
+    for k in range(nz):
+        np.testing.assert_array_equal(np.frombuffer(rec(8 * nx * ny), np.float64), a[:, :, k].ravel(order="F"))
+    assert int(np.frombuffer(rec(4), np.int32)[0]) == 42
+    assert float(np.frombuffer(rec(8), np.float64)[0]) == 1.5
+    assert list(np.frombuffer(rec(16), np.float64)) == [5e-4, 1.0]
+    assert pos == len(raw)
+    b, ns, t, dt, gr = product.read_ioscalar(path, (nx, ny, nz))
+    np.testing.assert_array_equal(a, b)
+    assert (ns, t, dt, gr) == (42, 1.5, 5e-4, 1.0)
+    # another grid, or a truncated file, is refused
+    with pytest.raises(product.EddyError):
+        product.read_ioscalar(path, (nx, ny, nz + 1))
+    open(path, "wb").write(raw[:-10])
+    with pytest.raises(product.EddyError):
+        product.read_ioscalar(path, (nx, ny, nz))
