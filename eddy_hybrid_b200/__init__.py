@@ -106,6 +106,7 @@ SIGNATURES = {
     "eddy_ib_limits": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "eddy_ib_stencils": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "eddy_ib_stencil_kinds": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "eddy_profile_enable": ([C.c_void_p, C.c_uint], C.c_int),
     "eddy_profile_read": ([C.c_void_p, _DP, C.POINTER(C.c_longlong)], C.c_int),
     "eddy_selftest_wait_bound": ([C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
@@ -343,9 +344,13 @@ class Solver:
         vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
         self._check(lib().eddy_ib_stencils(self.h, q, C.byref(n), C.byref(nl), vp(ijk), vp(dijk), vp(lev), vp(xn),
                                            vp(lu), vp(indx)), "eddy_ib_stencils")
+        mrk = np.zeros(max(m, 1), np.int32)
+        dr = np.zeros(max(m, 1), np.int32)
+        xe = np.zeros(3 * max(m, 1))
+        self._check(lib().eddy_ib_stencil_kinds(self.h, q, vp(mrk), vp(dr), vp(xe)), "eddy_ib_stencil_kinds")
         return {"n": m, "nlev": nl.value, "ijk": ijk[:3 * m].reshape(m, 3), "dijk": dijk[:3 * m].reshape(m, 3),
                 "lev": lev[:m], "xn": xn[:3 * m].reshape(m, 3), "lu": lu[:4 * m].reshape(m, 4),
-                "indx": indx[:2 * m].reshape(m, 2)}
+                "indx": indx[:2 * m].reshape(m, 2), "mrk": mrk[:m], "dir": dr[:m], "xe": xe[:3 * m].reshape(m, 3)}
 
     def refine_residuals(self) -> np.ndarray:
         """max |d - L phi| before each refinement sweep of the last mixed solve."""

@@ -595,6 +595,11 @@ int eddy_ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dij
   return ib_stencils(ctx, q, n, nlev, ijk, dijk, lev, xn, lu, indx);
 }
 
+int eddy_ib_stencil_kinds(eddy_ctx *ctx, int q, int *mrk, int *dir, double *xe) {
+  if (check_ctx(ctx) || !ctx->ib) return EDDY_EINVAL;
+  return ib_stencil_kinds(ctx, q, mrk, dir, xe);
+}
+
 int eddy_refine_residuals(eddy_ctx *ctx, double *out, int n) {
   if (check_ctx(ctx) || !out || n < 1) return EDDY_EINVAL;
   if (!ctx->mixed) {

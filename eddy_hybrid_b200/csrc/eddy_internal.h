@@ -241,6 +241,7 @@ int ib_download(eddy_ctx *ctx, int which, signed char *out);
 int ib_limits(eddy_ctx *ctx, int *lim6);
 int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
                 int *indx);
+int ib_stencil_kinds(eddy_ctx *ctx, int q, int *mrk, int *dir, double *xe);
 
 // tensor-core (3xTF32) eigen-transforms of the mixed solve (k_xform.cu).
 // sym: mirror-symmetric split form, modes ordered even then odd; lam and m0

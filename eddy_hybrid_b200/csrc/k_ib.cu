@@ -53,8 +53,8 @@ struct Bins {
 // stencils of one variable (device arrays) and host level offsets
 struct StencilSet {
   int n = 0, nlev = 0, cap = 0;
-  int *ijk = nullptr, *dijk = nullptr, *lev = nullptr, *indx = nullptr;
-  double *xn = nullptr, *lu = nullptr;
+  int *ijk = nullptr, *dijk = nullptr, *lev = nullptr, *indx = nullptr, *mrk = nullptr, *dir = nullptr;
+  double *xn = nullptr, *lu = nullptr, *xe = nullptr;
   std::vector<int> lev_start;
 };
 
@@ -80,7 +80,7 @@ struct IbState {
   bool ready = false;
   int every_substep = 0;  // 1: move + regenerate every substep (IBM > 1), 0: once per step
   // persistent scratch (grown on demand, never freed during a run)
-  enum { S_BINCNT = 0, S_BCNT, S_BOFF, S_CUR, S_STATUS, S_LEV, S_DD, S_ORDER, S_CNT, S_BSUM, S_NI };
+  enum { S_BINCNT = 0, S_BCNT, S_BOFF, S_CUR, S_INN, S_ORDER, S_CNT, S_BSUM, S_NI };
   int *si[S_NI] = {};
   size_t si_cap[S_NI] = {};
   double *sxn = nullptr;
@@ -165,6 +165,317 @@ __device__ int locate(const double *xx, int n, double x) {
     }
   }
   return first - 1;
+}
+
+// ---------------------------------------------------------------------------
+// face and ray primitives of the normal-direction and closest-point stencil
+// searches, Cartesian (the same operations as the oracle's); sums start from
+// zero as the reference's DOTPROD / DOTPRODUCT / vecmag do (src/triinter.f:119,
+// src/rt.f:2101,2164)
+__device__ __forceinline__ double dotz3(const double *a, const double *b) {
+  double s = 0.;
+  s = s + a[0] * b[0];
+  s = s + a[1] * b[1];
+  s = s + a[2] * b[2];
+  return s;
+}
+
+__device__ __forceinline__ double magz3(const double *a) {
+  double s = 0.;
+  s = s + a[0] * a[0];
+  s = s + a[1] * a[1];
+  s = s + a[2] * a[2];
+  return sqrt(s);
+}
+
+// ray_seg_int (src/rt.f:2054-2096): ray p + a q (a >= 0) against the segment
+// r + b s (0 <= b <= 1)
+__device__ int ray_seg(const double *p, const double *q, const double *r, const double *s) {
+  double f0 = s[1], f1 = -s[0];
+  const double d0 = (0. + f0 * q[0]) + f1 * q[1];
+  if (d0 == 0.) return 0;
+  const double g0 = r[0] - p[0], g1 = r[1] - p[1];
+  const double a = ((0. + f0 * g0) + f1 * g1) / d0;
+  if (!(a >= 0.)) return 0;
+  f0 = q[1];
+  f1 = -q[0];
+  const double b = ((0. + f0 * g0) + f1 * g1) / d0;
+  return b >= 0.0 && b <= 1.0;
+}
+
+// point_poly_clasf (src/rt.f:1590-1625): the ray towards (1000, 0) against
+// the edges v1-v2, v2-v3, v3-v4 (the closing edge is not tested, as in the
+// reference); an odd count is inside
+__device__ int point_in_face(double x, double y, const double (*V)[3], int u, int v) {
+  const double p[2] = {x, y}, q[2] = {1000., 0.};
+  int cross = 0;
+  for (int e = 0; e < 3; e++) {
+    const double r[2] = {V[e][u], V[e][v]};
+    const double s[2] = {V[e + 1][u] - V[e][u], V[e + 1][v] - V[e][v]};
+    cross += ray_seg(p, q, r, s);
+  }
+  return cross % 2;
+}
+
+// plane_tri + cross (src/rt.f:2130-2155, 1250-1259)
+__device__ void face_plane(const double (*V)[3], double *pn, double &dd) {
+  double s1[3], s2[3];
+  for (int a = 0; a < 3; a++) {
+    s1[a] = V[1][a] - V[0][a];
+    s2[a] = V[2][a] - V[0][a];
+  }
+  pn[0] = s1[1] * s2[2] - s2[1] * s1[2];
+  pn[1] = s1[2] * s2[0] - s2[2] * s1[0];
+  pn[2] = s1[0] * s2[1] - s2[0] * s1[1];
+  dd = -((pn[0] * V[0][0] + pn[1] * V[0][1]) + pn[2] * V[0][2]);
+}
+
+// ray_poly_int (src/rt.f:1507-1580) and ray_xzface_int (src/rt.f:1740-1845):
+// the plane hit at t >= 0, then the polygon test in the coordinate plane of
+// the largest signed normal entry (xz = false) or the x and z ranges (xz)
+__device__ int ray_quad(const double *q, const double *r, const double (*V)[3], bool xz, double *xi) {
+  double pn[3], dd;
+  face_plane(V, pn, dd);
+  const double vd = dotz3(pn, r);
+  if (vd == 0.) return 0;
+  const double v1 = -(dotz3(pn, q) + dd);
+  const double t = v1 / vd;
+  if (xz ? (t < 0.) : !(t >= 0.)) return 0;
+  xi[0] = q[0] + t * r[0];
+  xi[1] = q[1] + t * r[1];
+  xi[2] = q[2] + t * r[2];
+  if (xz) {
+    double rmin = V[0][0], rmax = V[1][0], zmin = V[0][2], zmax = V[3][2];
+    if (rmin > rmax) { const double a = rmin; rmin = rmax; rmax = a; }
+    if (zmin > zmax) { const double a = zmin; zmin = zmax; zmax = a; }
+    if (xi[0] < rmin || xi[0] > rmax) return 0;
+    if (xi[2] < zmin || xi[2] > zmax) return 0;
+    return 1;
+  }
+  int dir = 0;
+  if (pn[1] > pn[dir]) dir = 1;
+  if (pn[2] > pn[dir]) dir = 2;
+  if (dir == 0) return point_in_face(xi[1], xi[2], V, 1, 2);
+  if (dir == 1) return point_in_face(xi[0], xi[2], V, 0, 2);
+  return point_in_face(xi[0], xi[1], V, 0, 1);
+}
+
+// ray_face_int (src/rt.f:1395-1500), Cartesian: the ray q + t r against the
+// face of cell (i, j, k) normal to axis dir (1..3); faces that would reach
+// past the arrays count as missed
+__device__ int ray_face(const Dims &d, const Axes &ax, const double *q, const double *r, int i, int j, int k, int dir,
+                        double *xi) {
+  if (i < 1 || i > d.nx || j < 1 || j > d.ny || k < 1 || k > d.nz) return 0;
+  const int i1 = dir == 1 ? i : i + 1, j1 = dir == 2 ? j : j + 1, k1 = dir == 3 ? k : k + 1;
+  if (i1 > d.nx || j1 > d.ny || k1 > d.nz) return 0;
+  const double *X = ax.x, *Y = ax.y, *Z = ax.z;
+  double V[4][3];
+  if (dir == 1) {
+    V[0][0] = X[i]; V[0][1] = Y[j]; V[0][2] = Z[k];
+    V[1][0] = X[i]; V[1][1] = Y[j1]; V[1][2] = Z[k];
+    V[2][0] = X[i]; V[2][1] = Y[j1]; V[2][2] = Z[k1];
+    V[3][0] = X[i]; V[3][1] = Y[j]; V[3][2] = Z[k1];
+  } else if (dir == 2) {
+    V[0][0] = X[i]; V[0][1] = Y[j]; V[0][2] = Z[k];
+    V[1][0] = X[i1]; V[1][1] = Y[j]; V[1][2] = Z[k];
+    V[2][0] = X[i1]; V[2][1] = Y[j]; V[2][2] = Z[k1];
+    V[3][0] = X[i]; V[3][1] = Y[j]; V[3][2] = Z[k1];
+  } else {
+    V[0][0] = X[i]; V[0][1] = Y[j]; V[0][2] = Z[k];
+    V[1][0] = X[i1]; V[1][1] = Y[j]; V[1][2] = Z[k];
+    V[2][0] = X[i1]; V[2][1] = Y[j1]; V[2][2] = Z[k];
+    V[3][0] = X[i]; V[3][1] = Y[j1]; V[3][2] = Z[k];
+  }
+  return ray_quad(q, r, V, dir == 2, xi);
+}
+
+// fluidface (src/matint.f:4124-4170): 1 all nodes fluid, 0 a forcing node,
+// -1 a body node; faces reaching past the arrays give 0
+__device__ int fluid_face(const Dims &d, const signed char *flag, int i, int j, int k, int dir) {
+  if (i < 1 || i > d.nx || j < 1 || j > d.ny) return 0;
+  const int i1 = dir == 1 ? i : i + 1, j1 = dir == 2 ? j : j + 1, k1 = dir == 3 ? k : k + 1;
+  if (k < 1 || i1 > d.nx || j1 > d.ny || k1 > d.nz) return 0;
+  int t[4];
+  t[0] = flag[lidx(d.nx, d.ny, i, j, k)];
+  if (dir == 1) {
+    t[1] = flag[lidx(d.nx, d.ny, i, j1, k)]; t[2] = flag[lidx(d.nx, d.ny, i, j, k1)];
+    t[3] = flag[lidx(d.nx, d.ny, i, j1, k1)];
+  } else if (dir == 2) {
+    t[1] = flag[lidx(d.nx, d.ny, i1, j, k)]; t[2] = flag[lidx(d.nx, d.ny, i, j, k1)];
+    t[3] = flag[lidx(d.nx, d.ny, i1, j, k1)];
+  } else {
+    t[1] = flag[lidx(d.nx, d.ny, i1, j, k)]; t[2] = flag[lidx(d.nx, d.ny, i, j1, k)];
+    t[3] = flag[lidx(d.nx, d.ny, i1, j1, k)];
+  }
+  int any = 0, pos = 0;
+  for (int a = 0; a < 4; a++) {
+    any |= t[a] != 0;
+    pos |= t[a] > 0;
+  }
+  return pos ? -1 : (any ? 0 : 1);
+}
+
+// the first face the ray from grid point (im, jm, km) along r meets, tried
+// normal to x, then y, then z (the cell side of each from the signs of r,
+// vec_ijkext_gridpoint src/devel.f:5296-5410); the fluidface code of that
+// face, or 2 when the ray meets none of the three
+__device__ int ray_first_face(const Dims &d, const Axes &ax, const signed char *flag, const double *q,
+                              const double *r, int im, int jm, int km, double *xe, int &dir) {
+  const int pi = !(r[0] < 0), pj = !(r[1] < 0), pk = !(r[2] < 0);
+  for (int dd = 1; dd <= 3; dd++) {
+    const int ei = dd == 1 ? (pi ? 1 : -1) : (pi ? 0 : -1);
+    const int ej = dd == 2 ? (pj ? 1 : -1) : (pj ? 0 : -1);
+    const int ek = dd == 3 ? (pk ? 1 : -1) : (pk ? 0 : -1);
+    if (ray_face(d, ax, q, r, im + ei, jm + ej, km + ek, dd, xe)) {
+      dir = dd;
+      return fluid_face(d, flag, im + ei, jm + ej, km + ek, dd);
+    }
+  }
+  return 2;
+}
+
+// closest (src/numrec.f:425-474): the entry of the table nearest to x
+__device__ int closest_entry(const double *xx, int n, double x) {
+  int j = locate(xx, n, x);
+  if (j > 0 && j < n) {
+    if (fabs(x - xx[j]) > fabs(x - xx[j + 1])) j = j + 1;
+  } else if (j < 1) {
+    j = 1;
+  } else if (j > n) {
+    j = n;
+  }
+  return j;
+}
+
+// the cell face normal to axis dir holding point xp (recheckface,
+// interp_cellface): the nearest node along dir, LOCATE along the others
+__device__ void face_of_point(const Dims &d, const Axes &ax, const double *xp, int dir, int &i, int &j, int &k) {
+  i = dir == 1 ? closest_entry(ax.x, d.nx, xp[0]) : locate(ax.x, d.nx, xp[0]);
+  j = dir == 2 ? closest_entry(ax.y, d.ny, xp[1]) : locate(ax.y, d.ny, xp[1]);
+  k = dir == 3 ? closest_entry(ax.z, d.nz, xp[2]) : locate(ax.z, d.nz, xp[2]);
+}
+
+// recheckface (src/devel.f:8107-8175): 1 fluid face, -1 a forcing node, -2 a
+// body node
+__device__ int recheck_face(const Dims &d, const Axes &ax, const signed char *flag, const double *xp, int dir) {
+  int i, j, k;
+  face_of_point(d, ax, xp, dir, i, j, k);
+  const int f = fluid_face(d, flag, i, j, k, dir);
+  return f == 0 ? -1 : (f == -1 ? -2 : f);
+}
+
+// tri_closest_pt (src/rt.f:2525-2700): the point of triangle tv nearest to p
+// by the published region decomposition of the (s, t) parameter plane
+// (D. Eberly, Geometric Tools)
+__device__ void tri_nearest(const double *tv, const double *p, double *out) {
+  double e0[3], e1[3], df[3];
+  for (int a = 0; a < 3; a++) {
+    e0[a] = tv[3 + a] - tv[a];
+    e1[a] = tv[6 + a] - tv[a];
+    df[a] = tv[a] - p[a];
+  }
+  const double a00 = dotz3(e0, e0), a01 = dotz3(e0, e1), a11 = dotz3(e1, e1);
+  const double b0 = dotz3(e0, df), b1 = dotz3(e1, df);
+  const double det = fabs(a00 * a11 - a01 * a01);
+  double s = a01 * b1 - a11 * b0, t = a01 * b0 - a00 * b1;
+  if (s + t <= det) {
+    if (s < 0) {
+      if (t < 0) {
+        if (b0 < 0.0) {
+          t = 0.0;
+          s = (-b0 >= a00) ? 1.0 : -b0 / a00;
+        } else {
+          s = 0.0;
+          t = b1 > 0.0 ? 0.0 : (-b1 >= a11 ? 1.0 : -b1 / a11);
+        }
+      } else {
+        s = 0.0;
+        t = b1 >= 0.0 ? 0.0 : (-b1 > a11 ? 1.0 : -b1 / a11);
+      }
+    } else if (t < 0.0) {
+      t = 0.0;
+      s = b0 >= 0.0 ? 0.0 : (-b0 >= a00 ? 1.0 : -b0 / a00);
+    } else {
+      const double inv = 1.0 / det;
+      s = s * inv;
+      t = t * inv;
+    }
+  } else {
+    if (s < 0.0) {
+      const double tmp0 = a01 + b0, tmp1 = a11 + b1;
+      if (tmp1 > tmp0) {
+        const double numer = tmp1 - tmp0, denom = a00 - 2.0 * a01 + a11;
+        if (numer >= denom) {
+          s = 1.0; t = 0.0;
+        } else {
+          s = numer / denom; t = 1.0 - s;
+        }
+      } else {
+        s = 0.0;
+        t = tmp1 <= 0.0 ? 1.0 : (b1 >= 0.0 ? 0.0 : -b1 / a11);
+      }
+    } else if (t < 0.0) {
+      const double tmp0 = a01 + b1, tmp1 = a00 + b0;
+      if (tmp1 > tmp0) {
+        const double numer = tmp1 - tmp0, denom = a00 - 2.0 * a01 + a11;
+        if (numer >= denom) {
+          t = 1.0; s = 0.0;
+        } else {
+          t = numer / denom; s = 1.0 - t;
+        }
+      } else {
+        t = 0.0;
+        s = tmp1 < 0.0 ? 1.0 : (b0 >= 0.0 ? 0.0 : -b0 / a00);
+      }
+    } else {
+      const double numer = a11 + b1 - a01 - b0;
+      if (numer <= 0.0) {
+        s = 0.0; t = 1.0;
+      } else {
+        const double denom = a00 - 2.0 * a01 + a11;
+        if (numer >= denom) {
+          s = 1.0; t = 0.0;
+        } else {
+          s = numer / denom; t = 1.0 - s;
+        }
+      }
+    }
+  }
+  for (int a = 0; a < 3; a++) out[a] = (tv[a] + s * e0[a]) + t * e1[a];
+}
+
+// interp_cellface (src/interp.f:3-82), Cartesian: bilinear value of a on the
+// cell face normal to axis dir through xp, y indices periodic (index_bnd)
+template <class T>
+__device__ double interp_face(const Dims &d, const Axes &ax, int pitch, const T *a, const double *xp, int dir) {
+  int i, j, k;
+  face_of_point(d, ax, xp, dir, i, j, k);
+  i = min(max(i, 1), dir == 1 ? d.nx : d.nx - 1);
+  j = min(max(j, 1), dir == 2 ? d.ny : d.ny - 1);
+  k = min(max(k, 1), dir == 3 ? d.nz : d.nz - 1);
+  int j0 = j, j1 = j + 1;
+  if (j0 <= 1) j0 = d.ny - 2 + j0; else if (j0 >= d.ny) j0 = j0 - d.ny + 2;
+  if (j1 <= 1) j1 = d.ny - 2 + j1; else if (j1 >= d.ny) j1 = j1 - d.ny + 2;
+  const double *X = ax.x, *Y = ax.y, *Z = ax.z;
+  if (dir == 1) {
+    const double b1 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]), c1 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
+    return (((1 - b1) * (1 - c1) * (double)a[pidx(d, pitch, i, j0, k)] +
+             b1 * (1 - c1) * (double)a[pidx(d, pitch, i, j1, k)]) +
+            (1 - b1) * c1 * (double)a[pidx(d, pitch, i, j0, k + 1)]) +
+           b1 * c1 * (double)a[pidx(d, pitch, i, j1, k + 1)];
+  }
+  if (dir == 2) {
+    const double a1 = (xp[0] - X[i]) / (X[i + 1] - X[i]), c1 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
+    return (((1 - a1) * (1 - c1) * (double)a[pidx(d, pitch, i, j0, k)] +
+             a1 * (1 - c1) * (double)a[pidx(d, pitch, i + 1, j0, k)]) +
+            (1 - a1) * c1 * (double)a[pidx(d, pitch, i, j0, k + 1)]) +
+           a1 * c1 * (double)a[pidx(d, pitch, i + 1, j0, k + 1)];
+  }
+  const double a1 = (xp[0] - X[i]) / (X[i + 1] - X[i]), b1 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]);
+  return (((1 - a1) * (1 - b1) * (double)a[pidx(d, pitch, i, j0, k)] +
+           a1 * (1 - b1) * (double)a[pidx(d, pitch, i + 1, j0, k)]) +
+          (1 - a1) * b1 * (double)a[pidx(d, pitch, i, j1, k)]) +
+         a1 * b1 * (double)a[pidx(d, pitch, i + 1, j1, k)];
 }
 
 // ---------------------------------------------------------------------------
@@ -820,44 +1131,74 @@ __device__ double unitdot(const double *x, const double *xn, const double *nrm) 
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
 
-// grid_intr (src/matint.f:800-1160), isrt = 0, igrdint = 1, one warp: lane
-// d < 26 takes grid direction d.  The physical directions (flag <= 0) are
-// the ones the reference visits, in the order of their criterion (fluid
-// first, then boundary, each by index); every direction's result (first
-// candidate triangle, in list order, crossed by the 10x extended grid segment
-// with the extension point on the outward side) is independent of the
-// others, so the lanes search concurrently and the recorded intersections are
-// then numbered in visiting order for the selection (dot product with the
-// normal + flag * number, first maximum).  Returns (to every lane) 1, -1
-// (extension point is a forcing point), 0 (no intersection), -2 (only
-// inward ones); lane 0 writes xn, dd.
+// one forcing point's search state across the dependency loops of geom_mod:
+// mrk (0 new; 1, 2, 3 valid: normal direction, grid line, closest point;
+// -1, -2, -3 waiting on that stencil), the triangle fp (-1 none), the face
+// axis dir, the candidate list stage icm (lists of 3, 5, 25), the loop lev
+// that made it valid, the body point xn and the extension ext (face point
+// for mrk 1, 3; grid offsets for 2)
+struct GeomPt {
+  int mrk, fp, dir, icm, lev, pad;
+  double xn[3], ext[3];
+};
+static_assert(sizeof(GeomPt) == 72, "GeomPt layout");
+
+__device__ __forceinline__ int list_len(int icm) { return icm == 0 ? 3 : (icm == 1 ? 5 : NNTR3D); }
+
+// grid_intr (src/matint.f:800-1160), igrdint = 1, one warp: lane d < 26
+// takes grid direction d.  The directions are visited in the order of the
+// criterion isrt (0: fluid neighbours, then forcing ones; 1: fluid
+// neighbours by the cosine of the direction with the normal of triangle fp;
+// 2: the same over fluid and forcing neighbours), the first nphy of them
+// (nphy = the number of non-body neighbours), each taking the first
+// candidate triangle, in list order, that its 10x extended grid segment
+// crosses with the extension point on the outward side.  The directions are
+// independent, so the lanes search at once; the recorded crossings are
+// numbered in visiting order for the selection (cosine + flag * number,
+// first maximum).  One scan serves the list lengths from stage icm0 on: the
+// first length with a result other than 0 / -2 decides (the reference's
+// widening loop).  Returns (to every lane) 1, -1 (a forcing extension
+// point), 0 (no crossing), -2 (inward crossings only) and the stage reached;
+// on 1 / -1 the selecting lane writes xn, ext, fp of S.
 __device__ int grid_intr_warp(const Dims &d, const Axes &ax, const double *v, const double *nrm,
-                              const signed char *flag, int im, int jm, int km, const int *inn, int nn, double *xn,
-                              int *dd) {
+                              const signed char *flag, int im, int jm, int km, const int *inn, int icm0, int isrt,
+                              GeomPt &S, int &icm_out) {
   const int lane = threadIdx.x & 31;
   const bool dirl = lane < 26;
   const int id = dirl ? c_gind[lane][0] : 0, jd = dirl ? c_gind[lane][1] : 0, kd = dirl ? c_gind[lane][2] : 0;
   const int fext = dirl ? flag[lidx(d.nx, d.ny, im + id, jm + jd, km + kd)] : 1;
-  const double crit = !dirl ? -100.0 : (fext == 0 ? 1.0 : (fext < 0 ? 0.5 : -2.0));
+  const double p0[3] = {ax.x[im], ax.y[jm], ax.z[km]};
+  const double pe[3] = {ax.x[im + id], ax.y[jm + jd], ax.z[km + kd]};
+  double crit = -100.0;
+  if (dirl) {
+    crit = -2.0;
+    if (isrt == 0) {
+      crit = fext == 0 ? 1.0 : (fext < 0 ? 0.5 : -2.0);
+    } else if ((isrt == 1 && fext == 0) || (isrt == 2 && fext <= 0)) {
+      double r[3] = {pe[0] - p0[0], pe[1] - p0[1], pe[2] - p0[2]};
+      const double m = magz3(r);
+      r[0] = r[0] / m; r[1] = r[1] / m; r[2] = r[2] / m;
+      crit = dotz3(r, nrm + 3 * S.fp);
+    }
+  }
   // visiting slot: rank by (criterion descending, index ascending)
   int rank = 0;
   for (int e = 0; e < 26; e++) {
     const double ce = __shfl_sync(0xffffffffu, crit, e);
     if (ce > crit || (ce == crit && e < lane)) rank++;
   }
-  const double p0[3] = {ax.x[im], ax.y[jm], ax.z[km]};
-  const double pe[3] = {ax.x[im + id], ax.y[jm + jd], ax.z[km + kd]};
-  // one scan of the candidate list serves the three list lengths: a
-  // direction's result for length k is its first valid crossing if that lies
-  // within the first k candidates; hits are counted up to it (or up to k)
+  const int nphy = __popc(__ballot_sync(0xffffffffu, dirl && fext <= 0));
+  const bool visit = dirl && rank < nphy && fext <= 0;
+  // a direction's result for list length k is its first valid crossing if
+  // that lies within the first k candidates; hits are counted up to it
   int pos = 1 << 20, h3 = 0, h5 = 0, hall = 0, tri = -1;
   double xm[3] = {0., 0., 0.};
-  if (dirl && fext <= 0) {
+  if (visit) {
     double r[3] = {pe[0] - p0[0], pe[1] - p0[1], pe[2] - p0[2]};
     r[0] = r[0] * 10.0; r[1] = r[1] * 10.0; r[2] = r[2] * 10.0;
     const double s1[3] = {p0[0] - r[0], p0[1] - r[1], p0[2] - r[2]};
     const double s2[3] = {p0[0] + r[0], p0[1] + r[1], p0[2] + r[2]};
-    for (int in = 0; in < nn; in++) {
+    for (int in = 0; in < NNTR3D; in++) {
       const int n = inn[in];
       if (n < 0) continue;
       double x3[3];
@@ -875,8 +1216,10 @@ __device__ int grid_intr_warp(const Dims &d, const Axes &ax, const double *v, co
     }
   }
   int gi = 0;
-  for (int lv = 0; lv < 3; lv++) {
-    const int kk = lv == 0 ? 3 : (lv == 1 ? 5 : nn);
+  icm_out = icm0;
+  for (int lv = icm0; lv < 3; lv++) {
+    icm_out = lv;
+    const int kk = list_len(lv);
     const bool rec = pos < kk;
     const int hits = rec ? hall : (lv == 0 ? h3 : (lv == 1 ? h5 : hall));
     const unsigned smask = __reduce_or_sync(0xffffffffu, rec ? (1u << rank) : 0u);
@@ -906,14 +1249,126 @@ __device__ int grid_intr_warp(const Dims &d, const Axes &ax, const double *v, co
         blane = olane;
       }
     }
+    __syncwarp();
     if (lane == blane) {
-      xn[0] = xm[0]; xn[1] = xm[1]; xn[2] = xm[2];
-      dd[0] = id; dd[1] = jd; dd[2] = kd;
+      S.xn[0] = xm[0]; S.xn[1] = xm[1]; S.xn[2] = xm[2];
+      S.ext[0] = id; S.ext[1] = jd; S.ext[2] = kd;
+      S.fp = tri;
     }
+    __syncwarp();
     const int cand = __shfl_sync(0xffffffffu, fext < 0 ? 1 : 0, blane);
     return cand ? -1 : 1;
   }
   return gi;
+}
+
+// norm_intr (src/matint.f:1404-1690) for the list lengths from stage 0 on,
+// one warp: lane l takes candidate l (the normal segment of 10 normals each
+// way through the point, then the normal ray's first face).  Per length the
+// first candidate crossing with a fluid (1) or forcing-node (-1) face
+// decides; else -2 if a crossing met a face with a body node, else 0.  The
+// geom loop widens while the result is 0.  Returns the result and the stage;
+// writes S.fp (the last crossing triangle up to the decision) and, on 1 /
+// -1, xn, ext, dir.
+__device__ int norm_intr_warp(const Dims &d, const Axes &ax, const double *v, const double *nrm,
+                              const signed char *flag, int im, int jm, int km, const int *inn, GeomPt &S,
+                              int &icm_out) {
+  const int lane = threadIdx.x & 31;
+  const double p0[3] = {ax.x[im], ax.y[jm], ax.z[km]};
+  const int n = lane < NNTR3D ? inn[lane] : -1;
+  bool crossed = false;
+  int f = 2, dir = 0;
+  double xm[3] = {0., 0., 0.}, xe[3] = {0., 0., 0.};
+  if (n >= 0) {
+    const double *un = nrm + 3 * n;
+    const double s1[3] = {p0[0] - 10.0 * -un[0], p0[1] - 10.0 * -un[1], p0[2] - 10.0 * -un[2]};
+    const double s2[3] = {p0[0] + 10.0 * -un[0], p0[1] + 10.0 * -un[1], p0[2] + 10.0 * -un[2]};
+    crossed = segtriint(s1, s2, v + 9 * n, xm);
+    if (crossed) {
+      const double r[3] = {fabs(10.0) * un[0], fabs(10.0) * un[1], fabs(10.0) * un[2]};
+      f = ray_first_face(d, ax, flag, p0, r, im, jm, km, xe, dir);
+    }
+  }
+  const unsigned mcross = __ballot_sync(0xffffffffu, crossed);
+  const unsigned mvalid = __ballot_sync(0xffffffffu, crossed && (f == 1 || f == 0));
+  const unsigned mbody = __ballot_sync(0xffffffffu, crossed && f == -1);
+  int res = 0;
+  for (int lv = 0; lv < 3; lv++) {
+    icm_out = lv;
+    const unsigned lim = (1u << list_len(lv)) - 1u;
+    const unsigned mv = mvalid & lim;
+    if (mv) {
+      const int fv = __ffs(mv) - 1;
+      const int fsel = __shfl_sync(0xffffffffu, f, fv);
+      __syncwarp();
+      if (lane == fv) {
+        S.xn[0] = xm[0]; S.xn[1] = xm[1]; S.xn[2] = xm[2];
+        S.ext[0] = xe[0]; S.ext[1] = xe[1]; S.ext[2] = xe[2];
+        S.dir = dir;
+        S.fp = n;
+      }
+      __syncwarp();
+      return fsel == 1 ? 1 : -1;
+    }
+    res = (mbody & lim) ? -2 : 0;
+    const unsigned mc = mcross & lim;
+    if (mc) {
+      const int last = 31 - __clz(mc);
+      const int nl = __shfl_sync(0xffffffffu, n, last);
+      __syncwarp();
+      if (lane == 0) S.fp = nl;
+      __syncwarp();
+    }
+    if (res != 0) return res;
+  }
+  return res;
+}
+
+// closest_intr (src/matint.f:1693-1985) over the candidates of stage icm,
+// one warp: lane l takes candidate l (its nearest point to the forcing point
+// and the ray from there through the point, turned to the triangle's outward
+// side, to its first face).  The first candidate with a fluid face decides,
+// else the first with a forcing-node face; fp ends as the last candidate.
+// Returns 1, -1, -2 (no such face), 0 (no candidate).
+__device__ int closest_intr_warp(const Dims &d, const Axes &ax, const double *v, const double *nrm,
+                                 const signed char *flag, int im, int jm, int km, const int *inn, int nn,
+                                 GeomPt &S) {
+  const int lane = threadIdx.x & 31;
+  const double p0[3] = {ax.x[im], ax.y[jm], ax.z[km]};
+  const int n = lane < nn ? inn[lane] : -1;
+  int f = 2, dir = 0;
+  double pn[3] = {0., 0., 0.}, xe[3] = {0., 0., 0.};
+  if (n >= 0) {
+    const double *un = nrm + 3 * n;
+    tri_nearest(v + 9 * n, p0, pn);
+    const double dv[3] = {p0[0] - pn[0], p0[1] - pn[1], p0[2] - pn[2]};
+    const double mag = magz3(dv);
+    double r[3] = {fabs(100.0) * dv[0] / mag, fabs(100.0) * dv[1] / mag, fabs(100.0) * dv[2] / mag};
+    if (dotz3(dv, un) < 0) {
+      r[0] = -r[0]; r[1] = -r[1]; r[2] = -r[2];
+    }
+    f = ray_first_face(d, ax, flag, p0, r, im, jm, km, xe, dir);
+  }
+  const unsigned mcand = __ballot_sync(0xffffffffu, n >= 0);
+  const unsigned mrec = __ballot_sync(0xffffffffu, n >= 0 && (f == 1 || f == 0));
+  const unsigned mfl = __ballot_sync(0xffffffffu, n >= 0 && f == 1);
+  if (mcand) {
+    const int last = 31 - __clz(mcand);
+    const int nl = __shfl_sync(0xffffffffu, n, last);
+    __syncwarp();
+    if (lane == 0) S.fp = nl;
+    __syncwarp();
+  }
+  if (!mrec) return mcand ? -2 : 0;
+  const int sel = __ffs(mfl ? mfl : mrec) - 1;
+  __syncwarp();
+  if (lane == sel) {
+    S.xn[0] = pn[0]; S.xn[1] = pn[1]; S.xn[2] = pn[2];
+    S.ext[0] = xe[0]; S.ext[1] = xe[1]; S.ext[2] = xe[2];
+    S.dir = dir;
+  }
+  __syncwarp();
+  return mfl ? 1 : -1;
 }
 
 // ludcmp for n = 2 (implicit partial pivoting), column-major a11 a21 a12 a22
@@ -981,95 +1436,162 @@ __device__ __forceinline__ void lusolve2(const double *a, const int *indx, doubl
   }
 }
 
-// first dependency loop, one warp per forcing point: grid_intr with the
-// candidate lists of the 3, 5, 25 nearest centroids; status: 1 resolved, -2
-// waits for its extension point, 0 dropped
 constexpr int GW = 4;  // warps (points) per block
+
+// geom_mod's treatment of the points of loop ilp (src/devel.f:9470-9755),
+// one warp per point: loop 1 treats every point (its nearest-centroid list
+// is computed and kept), later loops the waiting ones (mrk < 0).  A new
+// point tries the normal-direction stencil, else the grid-line stencil, else
+// the closest-point stencil; waiting points are rechecked against the
+// working flags fw.  mimdif (change in the number of points treated from the
+// previous loop) and ndif (loops without change) are geom_mod's.  Valid
+// points record the loop; points without a stencil are dropped (flag =
+// inonvld).  cnt[0] counts the valid points, cnt[1] the waiting ones.
 __global__ void __launch_bounds__(GW * 32)
-    k_geom_first(Dims d, Axes ax, int n, const int *ijk, const double *v, const double *c, const double *nrm, Bins b,
-                 const int *bstart, const int *bitems, const signed char *fw, int *status, double *xn, int *dd) {
+    k_geom_pass(Dims d, Axes ax, int n, const int *ijk, const double *v, const double *c, const double *nrm, Bins b,
+                const int *bstart, const int *bitems, const signed char *fw, signed char *flag, signed char inonvld,
+                GeomPt *pts, int *inn_all, int ilp, int mimdif, int ndif, int *cnt) {
   __shared__ int inn_s[GW][NNTR3D];
   __shared__ KnnSmem ks[GW];
+  __shared__ GeomPt sp[GW];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.x * GW + w;
   if (p >= n) return;  // whole warp
+  if (ilp > 1 && pts[p].mrk >= 0) return;
   const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
-  const double qv[3] = {ax.x[im], ax.y[jm], ax.z[km]};
-  // the exact nearest-centroid list is sorted, so the 3- and 5-lists are its
-  // prefixes; grid_intr_warp evaluates the three lengths in one scan
-  if (knn_warp2(b, bstart, bitems, c, qv, NNTR3D, inn_s[w], ks[w]) < 0)
-    knn_warp(b, bstart, bitems, c, qv, NNTR3D, inn_s[w]);
-  const int gi = grid_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn_s[w], NNTR3D, xn + 3 * p, dd + 3 * p);
-  __syncwarp();
-  if (lane == 0) status[p] = gi == 1 ? 1 : (gi == -1 ? -2 : 0);
-}
-
-// later loops: a waiting point resolves once its extension point is no longer
-// a forcing point in the working flags
-__global__ void k_geom_recheck(Dims d, int n, const int *ijk, const int *dd, const signed char *fw, int *status,
-                               int *lev, int ilp, int last) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n || status[p] != -2) return;
-  const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
-  if (fw[lidx(d.nx, d.ny, im + dd[3 * p], jm + dd[3 * p + 1], km + dd[3 * p + 2])] == 0) {
-    status[p] = 1;
-    lev[p] = ilp;
-  } else if (last) {
-    status[p] = 0;
+  int *inn = inn_s[w];
+  if (ilp == 1) {
+    const double qv[3] = {ax.x[im], ax.y[jm], ax.z[km]};
+    // the exact nearest-centroid list is sorted, so the lists of 3 and 5 are
+    // its prefixes
+    if (knn_warp2(b, bstart, bitems, c, qv, NNTR3D, inn, ks[w]) < 0) knn_warp(b, bstart, bitems, c, qv, NNTR3D, inn);
+    __syncwarp();
+    if (lane < NNTR3D) inn_all[(long long)NNTR3D * p + lane] = inn[lane];
+  } else if (lane < NNTR3D) {
+    inn[lane] = inn_all[(long long)NNTR3D * p + lane];
   }
-}
-
-// points resolved in loop ilp: working flag 0, level recorded, counter
-__global__ void k_geom_mark(Dims d, int n, const int *ijk, int *status, int *lev, int ilp, signed char *fw,
-                            int *cnt) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  if (status[p] == 1) {
-    if (ilp == 1) lev[p] = 1;
-    if (lev[p] == ilp) {
-      fw[lidx(d.nx, d.ny, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2])] = 0;
-      atomicAdd(&cnt[0], 1);
+  GeomPt &S = sp[w];
+  if (lane == 0) {
+    S = pts[p];
+    if (ilp == 1) {
+      S.mrk = 0;
+      S.fp = -1;
+      S.dir = 0;
+      S.icm = 0;
+      S.lev = 0;
     }
-  } else if (status[p] == -2) {
-    atomicAdd(&cnt[1], 1);
+  }
+  __syncwarp();
+  const int mrk0 = S.mrk;
+  int res;  // new mrk
+  {
+    int intrs = 0;
+    if (mrk0 == -1) {
+      intrs = recheck_face(d, ax, fw, S.ext, S.dir);
+    } else if (mrk0 == 0) {
+      int icm = 0;
+      intrs = norm_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, S, icm);
+      __syncwarp();
+      if (lane == 0) {
+        S.icm = icm;
+        if (intrs == 0) S.fp = -1;
+      }
+      __syncwarp();
+    }
+    if (im <= 2) intrs = 0;
+    if (intrs == 1) {
+      res = 1;
+    } else if (intrs == -1 && ilp < NFLU && mimdif != 0) {
+      res = -1;
+    } else {
+      int gintrs = 0;
+      if (mrk0 == -2 && ndif < 3) {
+        gintrs = fw[lidx(d.nx, d.ny, im + (int)S.ext[0], jm + (int)S.ext[1], km + (int)S.ext[2])] == 0 ? 1 : -1;
+      } else {
+        const int srt = S.fp >= 0 ? (ndif < 2 ? 1 : 2) : 0;
+        int icm = S.icm;
+        gintrs = grid_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, S.icm, srt, S, icm);
+        __syncwarp();
+        if (lane == 0) S.icm = icm;
+        __syncwarp();
+      }
+      if (gintrs == 1) {
+        res = 2;
+      } else if (gintrs == -1 && ilp < NFLU) {
+        res = -2;
+      } else {
+        int cintrs;
+        if (mrk0 == -3)
+          cintrs = recheck_face(d, ax, fw, S.ext, S.dir);
+        else
+          cintrs = closest_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, list_len(S.icm), S);
+        if (cintrs == 1)
+          res = 3;
+        else if (cintrs == -1 && ilp < NFLU && ndif < 2)
+          res = -3;
+        else
+          res = 0;
+      }
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    S.mrk = res;
+    if (res > 0) {
+      S.lev = ilp;
+      atomicAdd(&cnt[0], 1);
+    } else if (res < 0) {
+      atomicAdd(&cnt[1], 1);
+    } else {
+      flag[lidx(d.nx, d.ny, im, jm, km)] = inonvld;
+    }
+    pts[p] = S;
   }
 }
 
-// dropped points: the variable's flag becomes fluid (velocity) or interior (pressure)
-__global__ void k_geom_drop(Dims d, int n, const int *ijk, int *status, signed char *flag, signed char value,
-                            int drop_waiting) {
+// the points made valid in loop ilp become fluid in the working flags
+// (physical_mrk2flag1_mod, src/devel.f:10022-10060)
+__global__ void k_geom_mark(Dims d, int n, const int *ijk, const GeomPt *pts, int ilp, signed char *fw) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  if (status[p] == 0 || (drop_waiting && status[p] == -2)) {
-    status[p] = 0;
-    flag[lidx(d.nx, d.ny, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2])] = value;
-  }
+  if (pts[p].mrk > 0 && pts[p].lev == ilp) fw[lidx(d.nx, d.ny, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2])] = 0;
 }
 
-// output order: by level, then forcpts order (position = level offset + rank)
-__global__ void k_geom_rank_count(int n, const int *status, const int *lev, int nlev, int *levcnt) {
+// number of valid points per level
+__global__ void k_geom_rank_count(int n, const GeomPt *pts, int *levcnt) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n || status[p] != 1) return;
-  atomicAdd(&levcnt[lev[p] - 1], 1);
+  if (p >= n || pts[p].mrk <= 0) return;
+  atomicAdd(&levcnt[pts[p].lev - 1], 1);
 }
 
-// mtrx (src/devel.f:1159-1290) for the resolved points, written at their
-// final position; pos computed by a stable per-level prefix over the list
-__global__ void k_geom_emit(Dims d, Axes ax, int n, const int *ijk, const int *status, const int *lev,
-                            const int *order, const double *xnp, const int *ddp, int imn, int *oijk, int *odd,
-                            int *olev, double *oxn, double *olu, int *oindx) {
+// mtrx (src/devel.f:1159-1290), Cartesian, for the valid points, written at
+// their final position (level, then forcpts order): the extension point is
+// the grid point for mrk 2, the face point otherwise
+__global__ void k_geom_emit(Dims d, Axes ax, int n, const int *ijk, const GeomPt *pts, const int *order, int imn,
+                            int *oijk, int *odd, int *olev, double *oxn, double *olu, int *oindx, int *omrk,
+                            int *odir, double *oxe) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n || status[p] != 1) return;
+  if (p >= n || pts[p].mrk <= 0) return;
+  const GeomPt s = pts[p];
   const int o = order[p];
   const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
-  const int di = ddp[3 * p], dj = ddp[3 * p + 1], dk = ddp[3 * p + 2];
+  const bool grid = s.mrk == 2;
+  const int di = grid ? (int)s.ext[0] : 0, dj = grid ? (int)s.ext[1] : 0, dk = grid ? (int)s.ext[2] : 0;
   oijk[3 * o] = im; oijk[3 * o + 1] = jm; oijk[3 * o + 2] = km;
   odd[3 * o] = di; odd[3 * o + 1] = dj; odd[3 * o + 2] = dk;
-  olev[o] = lev[p];
-  const double xnx = xnp[3 * p], xny = xnp[3 * p + 1], xnz = xnp[3 * p + 2];
+  olev[o] = s.lev;
+  omrk[o] = s.mrk;
+  odir[o] = grid ? 0 : s.dir;
+  oxe[3 * o] = grid ? 0. : s.ext[0]; oxe[3 * o + 1] = grid ? 0. : s.ext[1]; oxe[3 * o + 2] = grid ? 0. : s.ext[2];
+  const double xnx = s.xn[0], xny = s.xn[1], xnz = s.xn[2];
   oxn[3 * o] = xnx; oxn[3 * o + 1] = xny; oxn[3 * o + 2] = xnz;
   const double xu = ax.x[im], yu = ax.y[jm], zu = ax.z[km];
-  const double x1 = ax.x[im + di], y1 = ax.y[jm + dj], z1 = ax.z[km + dk];
+  double x1, y1, z1;
+  if (grid) {
+    x1 = ax.x[im + di]; y1 = ax.y[jm + dj]; z1 = ax.z[km + dk];
+  } else {
+    x1 = s.ext[0]; y1 = s.ext[1]; z1 = s.ext[2];
+  }
   const double is1 = imn == 1 ? -1. : 1.;
   const double so = sqrt(((xu - xnx) * (xu - xnx) + (yu - xny) * (yu - xny)) + (zu - xnz) * (zu - xnz)) * is1;
   const double s1 = sqrt(((xu - x1) * (xu - x1) + (yu - y1) * (yu - y1)) + (zu - z1) * (zu - z1)) * 1.0;
@@ -1084,20 +1606,19 @@ __global__ void k_geom_emit(Dims d, Axes ax, int n, const int *ijk, const int *s
   for (int q = 0; q < 4; q++) olu[4 * o + q] = A[q];
 }
 
-// stable per-level ranks: order[p] = levstart[l] + (number of resolved
-// points of level l before p), computed per level by block counts + scan
-__global__ void k_level_count(int n, const int *status, const int *lev, int l, int *bcnt) {
+// stable per-level ranks: order[p] = levstart[l] + (number of valid points
+// of level l before p), computed per level by block counts + scan
+__global__ void k_level_count(int n, const GeomPt *pts, int l, int *bcnt) {
   const int p = blockIdx.x * CB + threadIdx.x;
-  const bool on = p < n && status[p] == 1 && lev[p] == l;
+  const bool on = p < n && pts[p].mrk > 0 && pts[p].lev == l;
   const int c = __syncthreads_count(on ? 1 : 0);
   if (threadIdx.x == 0) bcnt[blockIdx.x] = c;
 }
 
-__global__ void k_level_rank(int n, const int *status, const int *lev, int l, int base, const int *boff,
-                             int *order) {
+__global__ void k_level_rank(int n, const GeomPt *pts, int l, int base, const int *boff, int *order) {
   __shared__ int wsum[CB / 32];
   const int p = blockIdx.x * CB + threadIdx.x;
-  const bool on = p < n && status[p] == 1 && lev[p] == l;
+  const bool on = p < n && pts[p].mrk > 0 && pts[p].lev == l;
   const unsigned bal = __ballot_sync(0xffffffffu, on);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) wsum[w] = __popc(bal);
@@ -1109,19 +1630,28 @@ __global__ void k_level_rank(int n, const int *status, const int *lev, int l, in
 
 // ---------------------------------------------------------------------------
 // forcing (momforc_mod2 explicit / correctpres_mod2, correctdens_mod2 with a
-// zero normal gradient) for the points of one level; T storage with row pitch
+// zero normal gradient) for the points of one level: the extension value is
+// the grid point's (mrk 2) or the bilinear value on the fluid face
+// (interp_cellface, mrk 1 and 3); T storage with row pitch
 template <class T>
-__global__ void k_force(Dims d, int pitch, int o0, int o1, const int *ijk, const int *dd, const double *lu,
-                        const int *indx, T *a, double b0, float *mirror, int mpitch) {
+__global__ void k_force(Dims d, Axes ax, int pitch, int o0, int o1, const int *ijk, const int *dd, const int *mrk,
+                        const int *dir, const double *xe, const double *lu, const int *indx, T *a, double b0,
+                        float *mirror, int mpitch) {
   const int o = o0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= o1) return;
   const int im = ijk[3 * o], jm = ijk[3 * o + 1], km = ijk[3 * o + 2];
-  int i1 = im + dd[3 * o], j1 = jm + dd[3 * o + 1], k1 = km + dd[3 * o + 2];
-  if (j1 <= 1)
-    j1 = d.ny - 2 + j1;
-  else if (j1 >= d.ny)
-    j1 = j1 - d.ny + 2;
-  double b[2] = {b0, (double)a[pidx(d, pitch, i1, j1, k1)]};
+  double ae;
+  if (mrk[o] == 2) {
+    int i1 = im + dd[3 * o], j1 = jm + dd[3 * o + 1], k1 = km + dd[3 * o + 2];
+    if (j1 <= 1)
+      j1 = d.ny - 2 + j1;
+    else if (j1 >= d.ny)
+      j1 = j1 - d.ny + 2;
+    ae = (double)a[pidx(d, pitch, i1, j1, k1)];
+  } else {
+    ae = interp_face<T>(d, ax, pitch, a, xe + 3 * o, dir[o]);
+  }
+  double b[2] = {b0, ae};
   lusolve2(lu + 4 * o, indx + 2 * o, b);
   a[pidx(d, pitch, im, jm, km)] = (T)b[0];
   if (mirror) mirror[pidx(d, mpitch, im, jm, km)] = (float)b[0];
@@ -1315,45 +1845,42 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   S.nlev = 0;
   S.lev_start.assign(1, 0);
   if (n == 0) return EDDY_OK;
-  // per-point scratch
-  int *status = scratch(ctx, s, IbState::S_STATUS, n), *lev = scratch(ctx, s, IbState::S_LEV, n),
-      *dd = scratch(ctx, s, IbState::S_DD, 3 * (size_t)n), *order = scratch(ctx, s, IbState::S_ORDER, n),
+  // per-point search state, nearest-centroid lists, output positions
+  int *inn = scratch(ctx, s, IbState::S_INN, (size_t)NNTR3D * n), *order = scratch(ctx, s, IbState::S_ORDER, n),
       *cnt = scratch(ctx, s, IbState::S_CNT, NFLU + 2);
-  double *xn = scratch_d(ctx, s, 3 * (size_t)n);
-  if (!status || !lev || !dd || !order || !cnt || !xn) return EDDY_ENOMEM;
-  EDDY_CUDA(cudaMemsetAsync(lev, 0, sizeof(int) * n, st));
+  GeomPt *pts = reinterpret_cast<GeomPt *>(scratch_d(ctx, s, (sizeof(GeomPt) / sizeof(double)) * (size_t)n));
+  if (!inn || !order || !cnt || !pts) return EDDY_ENOMEM;
   signed char *fw = s->work;
   const size_t nc = (size_t)d.ncell;
   EDDY_CUDA(cudaMemcpyAsync(fw, flag, nc, cudaMemcpyDeviceToDevice, st));
   Axes ax = axes_of(ctx, q);
-  k_geom_first<<<(unsigned)((n + GW - 1) / GW), GW * 32, 0, st>>>(d, ax, n, s->pts, s->v, s->c, s->n, s->b3,
-                                                                   s->b3.start, s->b3.items, fw, status, xn, dd);
-  EDDY_LAUNCHED(ctx);
-  k_geom_drop<<<nblk(n), 256, 0, st>>>(d, n, s->pts, status, flag, (signed char)(imn == 0 ? 1 : 0), 0);
-  EDDY_LAUNCHED(ctx);
-  int nlev = 0;
+  const signed char inonvld = (signed char)(imn == 0 ? 1 : 0);
+  // the dependency loops of geom_mod (src/devel.f:9420-9770): np points are
+  // treated in a loop (all of them in the first); the points it makes valid
+  // become fluid in the working flags, whose y ghost planes are refreshed
+  int np = n, prev = 0, ndif = 0, nlev = 0;
   for (int ilp = 1; ilp <= NFLU; ilp++) {
-    if (ilp > 1) {
-      k_geom_recheck<<<nblk(n), 256, 0, st>>>(d, n, s->pts, dd, fw, status, lev, ilp, ilp == NFLU);
-      EDDY_LAUNCHED(ctx);
-    }
+    const int mimdif = np - prev;
+    prev = np;
+    if (mimdif == 0) ndif++;
+    if (np == 0) break;
     EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, st));
-    k_geom_mark<<<nblk(n), 256, 0, st>>>(d, n, s->pts, status, lev, ilp, fw, cnt);
+    k_geom_pass<<<(unsigned)((n + GW - 1) / GW), GW * 32, 0, st>>>(d, ax, n, s->pts, s->v, s->c, s->n, s->b3,
+                                                                    s->b3.start, s->b3.items, fw, flag, inonvld, pts,
+                                                                    inn, ilp, mimdif, ndif, cnt);
+    EDDY_LAUNCHED(ctx);
+    k_geom_mark<<<nblk(n), 256, 0, st>>>(d, n, s->pts, pts, ilp, fw);
     EDDY_LAUNCHED(ctx);
     k_yper_i8<<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, fw, 1, d.nx, 1, d.nz);
     EDDY_LAUNCHED(ctx);
     EDDY_CUDA(cudaMemcpyAsync(s->hcnt, cnt, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
     EDDY_CUDA(cudaStreamSynchronize(st));
-    const int nres = s->hcnt[0], nwait = s->hcnt[1];
-    if (nres > 0) nlev = ilp;
-    // done, or no progress: points still waiting are dropped below
-    if (nwait == 0 || nres == 0) break;
+    if (s->hcnt[0] > 0) nlev = ilp;
+    np = s->hcnt[1];
   }
-  k_geom_drop<<<nblk(n), 256, 0, st>>>(d, n, s->pts, status, flag, (signed char)(imn == 0 ? 1 : 0), 1);
-  EDDY_LAUNCHED(ctx);
   // level sizes -> offsets
   EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (NFLU + 2), st));
-  k_geom_rank_count<<<nblk(n), 256, 0, st>>>(n, status, lev, nlev, cnt + 1);
+  k_geom_rank_count<<<nblk(n), 256, 0, st>>>(n, pts, cnt + 1);
   EDDY_LAUNCHED(ctx);
   std::vector<int> lc(NFLU + 2, 0);
   EDDY_CUDA(cudaMemcpyAsync(lc.data(), cnt + 1, sizeof(int) * (NFLU + 1), cudaMemcpyDeviceToHost, st));
@@ -1364,18 +1891,21 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   S.n = nv;
   S.nlev = nlev;
   if (nv > S.cap) {
-    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu};
+    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu, S.mrk, S.dir, S.xe};
     for (void *p : ptrs) if (p) cudaFree(p);
-    S.ijk = S.dijk = S.lev = S.indx = nullptr;
-    S.xn = S.lu = nullptr;
+    S.ijk = S.dijk = S.lev = S.indx = S.mrk = S.dir = nullptr;
+    S.xn = S.lu = S.xe = nullptr;
     S.cap = 0;
     const size_t c = grown((size_t)nv);
     EDDY_CUDA(cudaMalloc(&S.ijk, sizeof(int) * 3 * c));
     EDDY_CUDA(cudaMalloc(&S.dijk, sizeof(int) * 3 * c));
     EDDY_CUDA(cudaMalloc(&S.lev, sizeof(int) * c));
     EDDY_CUDA(cudaMalloc(&S.indx, sizeof(int) * 2 * c));
+    EDDY_CUDA(cudaMalloc(&S.mrk, sizeof(int) * c));
+    EDDY_CUDA(cudaMalloc(&S.dir, sizeof(int) * c));
     EDDY_CUDA(cudaMalloc(&S.xn, sizeof(double) * 3 * c));
     EDDY_CUDA(cudaMalloc(&S.lu, sizeof(double) * 4 * c));
+    EDDY_CUDA(cudaMalloc(&S.xe, sizeof(double) * 3 * c));
     S.cap = (int)c;
   }
   if (nv > 0) {
@@ -1384,17 +1914,17 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
         *cur = scratch(ctx, s, IbState::S_CUR, nbl);
     if (!bcnt || !boff || !cur) return EDDY_ENOMEM;
     for (int l = 1; l <= nlev; l++) {
-      k_level_count<<<nbl, CB, 0, st>>>(n, status, lev, l, bcnt);
+      k_level_count<<<nbl, CB, 0, st>>>(n, pts, l, bcnt);
       EDDY_LAUNCHED(ctx);
       int *bsum = scratch(ctx, s, IbState::S_BSUM, (nbl + SB - 1) / SB + 1);
       if (!bsum) return EDDY_ENOMEM;
       int rc0 = scan_launch(ctx, nbl, bcnt, boff, cur, bsum);
       if (rc0) return rc0;
-      k_level_rank<<<nbl, CB, 0, st>>>(n, status, lev, l, S.lev_start[l - 1], boff, order);
+      k_level_rank<<<nbl, CB, 0, st>>>(n, pts, l, S.lev_start[l - 1], boff, order);
       EDDY_LAUNCHED(ctx);
     }
-    k_geom_emit<<<nblk(n), 256, 0, st>>>(d, ax, n, s->pts, status, lev, order, xn, dd, imn, S.ijk, S.dijk, S.lev,
-                                         S.xn, S.lu, S.indx);
+    k_geom_emit<<<nblk(n), 256, 0, st>>>(d, ax, n, s->pts, pts, order, imn, S.ijk, S.dijk, S.lev, S.xn, S.lu,
+                                         S.indx, S.mrk, S.dir, S.xe);
     EDDY_LAUNCHED(ctx);
   }
   return EDDY_OK;
@@ -1415,7 +1945,7 @@ int ib_release(eddy_ctx *ctx) {
   for (int q = 0; q < 5; q++) if (s->flag[q]) cudaFree(s->flag[q]);
   if (s->flag3b) cudaFree(s->flag3b);
   for (StencilSet &S : s->set) {
-    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu};
+    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu, S.mrk, S.dir, S.xe};
     for (void *q : ptrs) if (q) cudaFree(q);
   }
   if (s->hcnt) cudaFreeHost(s->hcnt);
@@ -1600,8 +2130,8 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
   for (int l = 0; l < S.nlev; l++) {
     const int o0 = S.lev_start[l], o1 = S.lev_start[l + 1];
     if (o1 > o0) {
-      k_force<T><<<nblk(o1 - o0, 128), 128, 0, st>>>(d, pitch, o0, o1, S.ijk, S.dijk, S.lu, S.indx, a, b0, mirror,
-                                                     mpitch);
+      k_force<T><<<nblk(o1 - o0, 128), 128, 0, st>>>(d, axes_of(ctx, q), pitch, o0, o1, S.ijk, S.dijk, S.mrk, S.dir,
+                                                     S.xe, S.lu, S.indx, a, b0, mirror, mpitch);
       EDDY_LAUNCHED(ctx);
     }
     k_yper_field<T><<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, pitch, a, mirror, mpitch);
@@ -1693,6 +2223,21 @@ int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, in
     if (xn) EDDY_CUDA(cudaMemcpyAsync(xn, S.xn, sizeof(double) * 3 * S.n, cudaMemcpyDeviceToHost, st));
     if (lu) EDDY_CUDA(cudaMemcpyAsync(lu, S.lu, sizeof(double) * 4 * S.n, cudaMemcpyDeviceToHost, st));
     if (indx) EDDY_CUDA(cudaMemcpyAsync(indx, S.indx, sizeof(int) * 2 * S.n, cudaMemcpyDeviceToHost, st));
+  }
+  EDDY_CUDA(cudaStreamSynchronize(st));
+  return EDDY_OK;
+}
+
+int ib_stencil_kinds(eddy_ctx *ctx, int q, int *mrk, int *dir, double *xe) {
+  ib_join(ctx);
+  IbState *s = ibs(ctx);
+  if (!s || q < 0 || q > 3) return EDDY_EINVAL;
+  StencilSet &S = s->set[q];
+  cudaStream_t st = ctx->stream;
+  if (S.n > 0) {
+    if (mrk) EDDY_CUDA(cudaMemcpyAsync(mrk, S.mrk, sizeof(int) * S.n, cudaMemcpyDeviceToHost, st));
+    if (dir) EDDY_CUDA(cudaMemcpyAsync(dir, S.dir, sizeof(int) * S.n, cudaMemcpyDeviceToHost, st));
+    if (xe) EDDY_CUDA(cudaMemcpyAsync(xe, S.xe, sizeof(double) * 3 * S.n, cudaMemcpyDeviceToHost, st));
   }
   EDDY_CUDA(cudaStreamSynchronize(st));
   return EDDY_OK;

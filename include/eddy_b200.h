@@ -185,11 +185,20 @@ int eddy_ib_flags(eddy_ctx *ctx, int which, signed char *out);
 int eddy_ib_limits(eddy_ctx *ctx, int *lim6);
 /* Stencils of set q (0 u, 1 v, 2 w, 3 p), ordered by dependency loop: n, the
  * number of loops, forcing points ijk[3n] (1-based), extension offsets
- * dijk[3n], loop lev[n], body intersection xn[3n], LU factors lu[4n]
- * (column-major a11 a21 a12 a22) and pivots indx[2n].  Null arrays are
- * skipped (call once with nulls for n). */
+ * dijk[3n] (grid-line stencils; 0 for the others), loop lev[n], body
+ * intersection xn[3n], LU factors lu[4n] (column-major a11 a21 a12 a22) and
+ * pivots indx[2n] (geom_mod + mtrx, src/devel.f:9265-9800, 1159-1290).  Null
+ * arrays are skipped (call once with nulls for n). */
 int eddy_ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn,
                      double *lu, int *indx);
+/* The kind of each stencil of set q, in the order of eddy_ib_stencils:
+ * mrk[n] (1 along the body normal, norm_intr src/matint.f:1404; 2 along a
+ * grid line, grid_intr :800; 3 through the closest body point, closest_intr
+ * :1693), and for kinds 1 and 3 the axis dir[n] (1..3) normal to the fluid
+ * cell face the stencil's ray crosses and the crossing point xe[3n], where
+ * the forcing interpolates (interp_cellface, src/interp.f:3); dir and xe
+ * are 0 for kind 2.  Null arrays are skipped. */
+int eddy_ib_stencil_kinds(eddy_ctx *ctx, int q, int *mrk, int *dir, double *xe);
 
 /* Mixed form only (no counterpart in the reference): max |d - L phi| of the
  * last refined Poisson solve before each sweep s, out[s] for s < min(n, 4);

@@ -171,12 +171,15 @@ typedef struct eo_ib eo_ib;
 typedef struct {
   int n, nlev;
   int *i, *j, *k;       /* forcing points (1-based) */
-  int *di, *dj, *dk;    /* extension point offsets (grid-line stencil) */
+  int *di, *dj, *dk;    /* mrk 2: extension point offsets (grid-line stencil), else 0 */
   int *lev;             /* dependency loop (1-based) */
   int *indx;            /* [n][2] LU pivots (0-based rows) */
   double *xn, *yn, *zn; /* body intersection */
   double *lu;           /* [n][4] LU factors, column-major a11 a21 a12 a22 */
   int *lev_start;       /* [nlev+1] offsets of each level */
+  int *mrk;             /* stencil kind: 1 normal direction, 2 grid line, 3 closest point */
+  int *dir;             /* mrk 1, 3: axis (1..3) normal to the fluid face crossed */
+  double *xe, *ye, *ze; /* mrk 1, 3: extension point on that face (interp_cellface) */
 } eo_ib_set;
 /* vert [nb][3][3] (x,y,z of vertices a,b,c), normals [nb][3], vel[3] */
 eo_ib *eo_ib_create(const eo_grid *g, int nb, const double *vert, const double *normals, const double *vel);
@@ -207,7 +210,7 @@ int eo_segtriint(const double *p1, const double *p2, const double *a, const doub
 void eo_lu2(double *a, int *indx);
 void eo_lusolve2(const double *a, const int *indx, double *b);
 int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int jm, int km, const int *inn,
-                    int nn, double *xn, int *dd);
+                    int nn, int isrt, double *xn, double *ext, int *fp);
 /* attach a body to the solver: the substep then moves it, regenerates the
  * stencils and applies the forcing (src/Eddy6.f:2163-2380, 2526-2575,
  * 2881-2897, 2972-2983) */

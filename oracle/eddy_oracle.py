@@ -38,7 +38,8 @@ class Params(C.Structure):
 class IBSet(C.Structure):
     _fields_ = [("n", C.c_int), ("nlev", C.c_int)] + \
         [(f, C.POINTER(C.c_int)) for f in ("i", "j", "k", "di", "dj", "dk", "lev", "indx")] + \
-        [(f, C.POINTER(C.c_double)) for f in ("xn", "yn", "zn", "lu")] + [("lev_start", C.POINTER(C.c_int))]
+        [(f, C.POINTER(C.c_double)) for f in ("xn", "yn", "zn", "lu")] + [("lev_start", C.POINTER(C.c_int))] + \
+        [(f, C.POINTER(C.c_int)) for f in ("mrk", "dir")] + [(f, C.POINTER(C.c_double)) for f in ("xe", "ye", "ze")]
 
 
 def make_params(d: dict) -> Params:
@@ -306,9 +307,9 @@ class OracleIB:
         S = lib().eo_ib_stencils(self.h, q).contents
         n = S.n
         out = {"n": n, "nlev": S.nlev}
-        for f in ("i", "j", "k", "di", "dj", "dk", "lev"):
+        for f in ("i", "j", "k", "di", "dj", "dk", "lev", "mrk", "dir"):
             out[f] = np.ctypeslib.as_array(getattr(S, f), shape=(n,)).copy() if n else np.zeros(0, np.int32)
-        for f in ("xn", "yn", "zn"):
+        for f in ("xn", "yn", "zn", "xe", "ye", "ze"):
             out[f] = np.ctypeslib.as_array(getattr(S, f), shape=(n,)).copy() if n else np.zeros(0)
         out["lu"] = np.ctypeslib.as_array(S.lu, shape=(4 * n,)).copy().reshape(n, 4) if n else np.zeros((0, 4))
         out["indx"] = np.ctypeslib.as_array(S.indx, shape=(2 * n,)).copy().reshape(n, 2) if n else \

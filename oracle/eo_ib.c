@@ -12,8 +12,17 @@
  *   taguo             src/devel.f:8-110      interior / forcing / fluid flags
  *   flagp             src/matint.f:135-260   pressure flags
  *   forcpts           src/matint.f:3388-3430 forcing-point list (k, j, i order)
+ *   norm_intr         src/matint.f:1404-1690 normal-direction stencil
  *   grid_intr         src/matint.f:800-1160  grid-line stencil (26 directions)
+ *   closest_intr      src/matint.f:1693-1985 closest-point stencil
+ *   tri_closest_pt    src/rt.f:2525-2700     (published region method)
+ *   ray_face_int,     src/rt.f:1395-1845, 2054-2155 ray / cell-face tests
+ *   ray_poly_int, ray_xzface_int, point_poly_clasf, ray_seg_int, plane_tri
+ *   vec_ijkext_gridpoint src/devel.f:5296-5410
+ *   fluidface, closest src/matint.f:4124-4170, src/numrec.f:425-474
+ *   recheckface       src/devel.f:8107-8175
  *   geom_mod          src/devel.f:9265-9800  dependency loops
+ *   interp_cellface   src/interp.f:3-82      face interpolation (forcing)
  *   mtrx              src/devel.f:1159-1290  2x2 systems
  *   ludcmp / lubksb   src/numrec.f:22-118    LU with implicit partial pivoting
  *                                            (the published Crout algorithm,
@@ -29,15 +38,16 @@
  *    against a column; here every triangle whose xy bounding box contains the
  *    column is tested, which is the set the reference's bounding-box test
  *    accepts when the search radius covers the triangle.
- *  * geom_mod's normal-direction and closest-point stencils (norm_intr,
- *    closest_intr, ANN committee3 + recheckface) are not restated: every
- *    forcing point takes the grid-line stencil of grid_intr (mrk = 2), with
- *    the 3-D nearest-centroid candidate lists of sizes 3, 5, nntr3d computed
- *    exactly (ties by triangle index).  A point whose extension point is a
- *    forcing point waits for a later dependency loop; a loop that resolves no
- *    point ends the search and the remaining points are dropped, as are
- *    points with no valid grid-line stencil (the velocity flag becomes fluid,
- *    the pressure flag interior, as geom_mod's "not valid" branch does).
+ *  * geom_mod (ivelrcn = 0) is restated with its three stencils and their
+ *    order: the normal direction (mrk 1), the grid line (mrk 2), the closest
+ *    point (mrk 3), each over the 3-D nearest-centroid candidate lists of
+ *    sizes 3, 5, nntr3d (ANN committee3), computed exactly here (ties by
+ *    triangle index; ANN's tie order is not specified).  Points whose
+ *    stencil touches a forcing point wait for a later dependency loop under
+ *    the reference's mimdif / ndif rules; points left without a stencil are
+ *    dropped (the velocity flag becomes fluid, the pressure flag interior).
+ *  * Faces and cells that would reach past the arrays count as missed (the
+ *    reference bounds-checks i and j only; no case here reaches them).
  *  * The body translates at a constant velocity: ubd/vbd/wbd are constants.
  */
 #include <math.h>
@@ -177,6 +187,7 @@ eo_ib *eo_ib_create(const eo_grid *g, int nb, const double *vert, const double *
 static void set_free(eo_ib_set *s) {
   free(s->i); free(s->j); free(s->k); free(s->di); free(s->dj); free(s->dk);
   free(s->lev); free(s->indx); free(s->xn); free(s->yn); free(s->zn); free(s->lu); free(s->lev_start);
+  free(s->mrk); free(s->dir); free(s->xe); free(s->ye); free(s->ze);
   memset(s, 0, sizeof(*s));
 }
 
@@ -540,23 +551,493 @@ static double unitdot(const double *x, const double *xn, const double *nrm) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
 
-/* grid_intr (src/matint.f:800-1160), isrt = 0, igrdint = 1: returns 1 (fluid
- * extension point), -1 (extension point is a forcing point), 0 (no
- * intersection), -2 (intersections only behind) */
-int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int jm, int km, const int *inn,
-                    int nn, double *xn, int *dd) {
+/* ---- face and ray primitives of the stencil searches (Cartesian) ----
+ * Sums start from zero as the reference's DOTPROD / DOTPRODUCT / vecmag do
+ * (src/triinter.f:119, src/rt.f:2101,2164). */
+static double dotz3(const double *a, const double *b) {
+  double s = 0.;
+  s = s + a[0] * b[0];
+  s = s + a[1] * b[1];
+  s = s + a[2] * b[2];
+  return s;
+}
+
+static double magz3(const double *a) {
+  double s = 0.;
+  s = s + a[0] * a[0];
+  s = s + a[1] * a[1];
+  s = s + a[2] * a[2];
+  return sqrt(s);
+}
+
+/* ray_seg_int (src/rt.f:2054-2096): ray p + a q (a >= 0) against the segment
+ * r + b s (0 <= b <= 1) */
+static int ray_seg(const double *p, const double *q, const double *r, const double *s) {
+  double f[2] = {s[1], -s[0]};
+  const double d0 = (0. + f[0] * q[0]) + f[1] * q[1];
+  if (d0 == 0.) return 0;
+  const double g[2] = {r[0] - p[0], r[1] - p[1]};
+  const double a = ((0. + f[0] * g[0]) + f[1] * g[1]) / d0;
+  if (!(a >= 0.)) return 0;
+  f[0] = q[1];
+  f[1] = -q[0];
+  const double b = ((0. + f[0] * g[0]) + f[1] * g[1]) / d0;
+  return b >= 0.0 && b <= 1.0;
+}
+
+/* point_poly_clasf (src/rt.f:1590-1625): crossings of the ray towards
+ * (1000, 0) with the edges v1-v2, v2-v3, v3-v4 of the 4-vertex polygon (the
+ * closing edge v4-v1 is not tested, as in the reference); odd is inside */
+static int point_in_face(double x, double y, const double V[4][3], int u, int v) {
+  const double p[2] = {x, y}, q[2] = {1000., 0.};
+  int cross = 0;
+  for (int e = 0; e < 3; e++) {
+    const double r[2] = {V[e][u], V[e][v]};
+    const double s[2] = {V[e + 1][u] - V[e][u], V[e + 1][v] - V[e][v]};
+    cross += ray_seg(p, q, r, s);
+  }
+  return cross % 2;
+}
+
+/* plane_tri + cross (src/rt.f:2130-2155, 1250-1259): A x + B y + C z + D = 0
+ * through the first three vertices */
+static void face_plane(const double V[4][3], double *pn, double *dd) {
+  double s1[3], s2[3];
+  for (int a = 0; a < 3; a++) {
+    s1[a] = V[1][a] - V[0][a];
+    s2[a] = V[2][a] - V[0][a];
+  }
+  pn[0] = s1[1] * s2[2] - s2[1] * s1[2];
+  pn[1] = s1[2] * s2[0] - s2[2] * s1[0];
+  pn[2] = s1[0] * s2[1] - s2[0] * s1[1];
+  *dd = -((pn[0] * V[0][0] + pn[1] * V[0][1]) + pn[2] * V[0][2]);
+}
+
+/* ray_poly_int (src/rt.f:1507-1580): plane hit at t >= 0, then the polygon
+ * test in the coordinate plane picked by the largest (signed) normal entry */
+static int ray_poly(const double *q, const double *r, const double V[4][3], double *xi) {
+  double pn[3], dd;
+  face_plane(V, pn, &dd);
+  const double vd = dotz3(pn, r);
+  if (vd == 0.) return 0;
+  const double v1 = -(dotz3(pn, q) + dd);
+  const double t = v1 / vd;
+  if (!(t >= 0.)) return 0;
+  xi[0] = q[0] + t * r[0];
+  xi[1] = q[1] + t * r[1];
+  xi[2] = q[2] + t * r[2];
+  int dir = 0;
+  if (pn[1] > pn[dir]) dir = 1;
+  if (pn[2] > pn[dir]) dir = 2;
+  if (dir == 0) return point_in_face(xi[1], xi[2], V, 1, 2);
+  if (dir == 1) return point_in_face(xi[0], xi[2], V, 0, 2);
+  return point_in_face(xi[0], xi[1], V, 0, 1);
+}
+
+/* ray_xzface_int (src/rt.f:1740-1845), Cartesian: plane hit at t >= 0 inside
+ * the x and z ranges of the face */
+static int ray_xzface(const double *q, const double *r, const double V[4][3], double *xi) {
+  double pn[3], dd;
+  face_plane(V, pn, &dd);
+  const double vd = dotz3(pn, r);
+  if (vd == 0.) return 0;
+  const double v1 = -(dotz3(pn, q) + dd);
+  const double t = v1 / vd;
+  if (t < 0.) return 0;
+  xi[0] = q[0] + t * r[0];
+  xi[1] = q[1] + t * r[1];
+  xi[2] = q[2] + t * r[2];
+  double rmin = V[0][0], rmax = V[1][0], zmin = V[0][2], zmax = V[3][2];
+  if (rmin > rmax) { const double a = rmin; rmin = rmax; rmax = a; }
+  if (zmin > zmax) { const double a = zmin; zmin = zmax; zmax = a; }
+  if (xi[0] < rmin || xi[0] > rmax) return 0;
+  if (xi[2] < zmin || xi[2] > zmax) return 0;
+  return 1;
+}
+
+/* ray_face_int (src/rt.f:1395-1500), Cartesian: the ray q + t r against the
+ * face of cell (i, j, k) normal to axis dir (1..3).  Faces that would reach
+ * past the arrays count as missed (the reference checks i and j only). */
+static int ray_face(const eo_grid *g, const double *X, const double *Y, const double *Z, const double *q,
+                    const double *r, int i, int j, int k, int dir, double *xi) {
+  if (i < 1 || i > g->nx || j < 1 || j > g->ny) return 0;
+  if (k < 1 || k > g->nz) return 0;
+  const int i1 = dir == 1 ? i : i + 1, j1 = dir == 2 ? j : j + 1, k1 = dir == 3 ? k : k + 1;
+  if (i1 > g->nx || j1 > g->ny || k1 > g->nz) return 0;
+  double V[4][3];
+  if (dir == 1) {
+    const double v[4][3] = {{X[i], Y[j], Z[k]}, {X[i], Y[j1], Z[k]}, {X[i], Y[j1], Z[k1]}, {X[i], Y[j], Z[k1]}};
+    memcpy(V, v, sizeof(V));
+    return ray_poly(q, r, V, xi);
+  }
+  if (dir == 2) {
+    const double v[4][3] = {{X[i], Y[j], Z[k]}, {X[i1], Y[j], Z[k]}, {X[i1], Y[j], Z[k1]}, {X[i], Y[j], Z[k1]}};
+    memcpy(V, v, sizeof(V));
+    return ray_xzface(q, r, V, xi);
+  }
+  const double v[4][3] = {{X[i], Y[j], Z[k]}, {X[i1], Y[j], Z[k]}, {X[i1], Y[j1], Z[k]}, {X[i], Y[j1], Z[k]}};
+  memcpy(V, v, sizeof(V));
+  return ray_poly(q, r, V, xi);
+}
+
+/* vec_ijkext_gridpoint (src/devel.f:5296-5410), Cartesian: the cell whose
+ * face normal to axis dir the ray from a grid point along r crosses first */
+static void ray_cell(const double *r, int dir, int *e) {
+  const int pi = !(r[0] < 0), pj = !(r[1] < 0), pk = !(r[2] < 0);
+  if (dir == 1) {
+    e[0] = pi ? 1 : -1; e[1] = pj ? 0 : -1; e[2] = pk ? 0 : -1;
+  } else if (dir == 2) {
+    e[0] = pi ? 0 : -1; e[1] = pj ? 1 : -1; e[2] = pk ? 0 : -1;
+  } else {
+    e[0] = pi ? 0 : -1; e[1] = pj ? 0 : -1; e[2] = pk ? 1 : -1;
+  }
+}
+
+/* fluidface (src/matint.f:4124-4170): 1 all four nodes fluid, 0 a forcing
+ * node, -1 a body node; faces reaching past the arrays give 0 */
+static int fluid_face(const eo_grid *g, const signed char *flag, int i, int j, int k, int dir) {
+  if (i < 1 || i > g->nx || j < 1 || j > g->ny) return 0;
+  const int i1 = dir == 1 ? i : i + 1, j1 = dir == 2 ? j : j + 1, k1 = dir == 3 ? k : k + 1;
+  if (k < 1 || i1 > g->nx || j1 > g->ny || k1 > g->nz) return 0;
+  int t[4];
+  if (dir == 1) {
+    t[0] = flag[IDX(g, i, j, k)]; t[1] = flag[IDX(g, i, j1, k)];
+    t[2] = flag[IDX(g, i, j, k1)]; t[3] = flag[IDX(g, i, j1, k1)];
+  } else if (dir == 2) {
+    t[0] = flag[IDX(g, i, j, k)]; t[1] = flag[IDX(g, i1, j, k)];
+    t[2] = flag[IDX(g, i, j, k1)]; t[3] = flag[IDX(g, i1, j, k1)];
+  } else {
+    t[0] = flag[IDX(g, i, j, k)]; t[1] = flag[IDX(g, i1, j, k)];
+    t[2] = flag[IDX(g, i, j1, k)]; t[3] = flag[IDX(g, i1, j1, k)];
+  }
+  int any = 0, pos = 0;
+  for (int a = 0; a < 4; a++) {
+    any |= t[a] != 0;
+    pos |= t[a] > 0;
+  }
+  return pos ? -1 : (any ? 0 : 1);
+}
+
+/* closest (src/numrec.f:425-474): the entry of the monotone table nearest
+ * to x, from the LOCATE position and its upper neighbour */
+static int closest_entry(const double *xx, int n, double x) {
+  int j = eo_locate(xx, n, x);
+  if (j > 0 && j < n) {
+    if (fabs(x - xx[j]) > fabs(x - xx[j + 1])) j = j + 1;
+  } else if (j < 1) {
+    j = 1;
+  } else if (j > n) {
+    j = n;
+  }
+  return j;
+}
+
+/* the cell face normal to axis dir holding point xp: the nearest node along
+ * dir, the LOCATE cells along the other two (recheckface / interp_cellface) */
+static void face_of_point(const eo_grid *g, const double *X, const double *Y, const double *Z, const double *xp,
+                          int dir, int *i, int *j, int *k) {
+  *i = dir == 1 ? closest_entry(X, g->nx, xp[0]) : eo_locate(X, g->nx, xp[0]);
+  *j = dir == 2 ? closest_entry(Y, g->ny, xp[1]) : eo_locate(Y, g->ny, xp[1]);
+  *k = dir == 3 ? closest_entry(Z, g->nz, xp[2]) : eo_locate(Z, g->nz, xp[2]);
+}
+
+/* recheckface (src/devel.f:8107-8175), Cartesian: 1 fluid face, -1 a forcing
+ * node, -2 a body node */
+static int recheck_face(const eo_grid *g, const double *X, const double *Y, const double *Z, const signed char *flag,
+                        const double *xp, int dir) {
+  int i, j, k;
+  face_of_point(g, X, Y, Z, xp, dir, &i, &j, &k);
+  const int f = fluid_face(g, flag, i, j, k, dir);
+  return f == 0 ? -1 : (f == -1 ? -2 : f);
+}
+
+/* tri_closest_pt (src/rt.f:2525-2700): the point of triangle (v0, v1, v2)
+ * nearest to p, by the published region decomposition of the (s, t)
+ * parameter plane (D. Eberly, "Distance Between Point and Triangle in 3D",
+ * Geometric Tools); only s and t are needed, not the distance */
+static void tri_nearest(const double *tv, const double *p, double *out) {
+  double e0[3], e1[3], df[3];
+  for (int a = 0; a < 3; a++) {
+    e0[a] = tv[3 + a] - tv[a];
+    e1[a] = tv[6 + a] - tv[a];
+    df[a] = tv[a] - p[a];
+  }
+  const double a00 = dotz3(e0, e0), a01 = dotz3(e0, e1), a11 = dotz3(e1, e1);
+  const double b0 = dotz3(e0, df), b1 = dotz3(e1, df);
+  const double det = fabs(a00 * a11 - a01 * a01);
+  double s = a01 * b1 - a11 * b0, t = a01 * b0 - a00 * b1;
+  if (s + t <= det) {
+    if (s < 0) {
+      if (t < 0) { /* region 4 */
+        if (b0 < 0.0) {
+          t = 0.0;
+          s = (-b0 >= a00) ? 1.0 : -b0 / a00;
+        } else {
+          s = 0.0;
+          if (b1 > 0.0)
+            t = 0.0;
+          else if (-b1 >= a11)
+            t = 1.0;
+          else
+            t = -b1 / a11;
+        }
+      } else { /* region 3 */
+        s = 0.0;
+        if (b1 >= 0.0)
+          t = 0.0;
+        else if (-b1 > a11)
+          t = 1.0;
+        else
+          t = -b1 / a11;
+      }
+    } else if (t < 0.0) { /* region 5 */
+      t = 0.0;
+      if (b0 >= 0.0)
+        s = 0.0;
+      else if (-b0 >= a00)
+        s = 1.0;
+      else
+        s = -b0 / a00;
+    } else { /* region 0 */
+      const double inv = 1.0 / det;
+      s = s * inv;
+      t = t * inv;
+    }
+  } else {
+    if (s < 0.0) { /* region 2 */
+      const double tmp0 = a01 + b0, tmp1 = a11 + b1;
+      if (tmp1 > tmp0) {
+        const double numer = tmp1 - tmp0, denom = a00 - 2.0 * a01 + a11;
+        if (numer >= denom) {
+          s = 1.0; t = 0.0;
+        } else {
+          s = numer / denom; t = 1.0 - s;
+        }
+      } else {
+        s = 0.0;
+        if (tmp1 <= 0.0)
+          t = 1.0;
+        else if (b1 >= 0.0)
+          t = 0.0;
+        else
+          t = -b1 / a11;
+      }
+    } else if (t < 0.0) { /* region 6 */
+      const double tmp0 = a01 + b1, tmp1 = a00 + b0;
+      if (tmp1 > tmp0) {
+        const double numer = tmp1 - tmp0, denom = a00 - 2.0 * a01 + a11;
+        if (numer >= denom) {
+          t = 1.0; s = 0.0;
+        } else {
+          t = numer / denom; s = 1.0 - t;
+        }
+      } else {
+        t = 0.0;
+        if (tmp1 < 0.0)
+          s = 1.0;
+        else if (b0 >= 0.0)
+          s = 0.0;
+        else
+          s = -b0 / a00;
+      }
+    } else { /* region 1 */
+      const double numer = a11 + b1 - a01 - b0;
+      if (numer <= 0.0) {
+        s = 0.0; t = 1.0;
+      } else {
+        const double denom = a00 - 2.0 * a01 + a11;
+        if (numer >= denom) {
+          s = 1.0; t = 0.0;
+        } else {
+          s = numer / denom; t = 1.0 - s;
+        }
+      }
+    }
+  }
+  for (int a = 0; a < 3; a++) out[a] = (tv[a] + s * e0[a]) + t * e1[a];
+}
+
+/* one stencil search's result: body point xn, extension point xe on a fluid
+ * face normal to axis dir, triangle fp (0-based, -1 none) */
+typedef struct {
+  double xn[3], xe[3];
+  int dir, fp;
+} eo_hit;
+
+/* the first fluid face the ray q + t r crosses: tried along x, then y, then
+ * z (the z cell side from the sign of sz), as norm_intr and closest_intr do.
+ * Returns the fluidface code of the face found (1, 0, -1), or 2 when the ray
+ * meets none of the three; xe and dir of the face found. */
+static int ray_first_face(const eo_grid *g, const double *X, const double *Y, const double *Z,
+                          const signed char *flag, const double *q, const double *r, int im, int jm, int km,
+                          double *xe, int *dir) {
+  int e[3];
+  for (int d = 1; d <= 3; d++) {
+    ray_cell(r, d, e);
+    if (ray_face(g, X, Y, Z, q, r, im + e[0], jm + e[1], km + e[2], d, xe)) {
+      *dir = d;
+      return fluid_face(g, flag, im + e[0], jm + e[1], km + e[2], d);
+    }
+  }
+  return 2;
+}
+
+/* norm_intr (src/matint.f:1404-1690): the normal of each candidate triangle
+ * through the point (segment of 10 normals each way); the first triangle the
+ * segment crosses whose normal ray from the point meets a face that is fluid
+ * (1) or holds a forcing node (-1) decides.  Returns 1, -1, -2 (only faces
+ * with body nodes), 0 (no triangle crossed, or no face met). */
+static int norm_intr(const eo_ib *ib, int q, const signed char *flag, int im, int jm, int km, const int *inn, int nn,
+                     eo_hit *h) {
   const eo_grid *g = ib->g;
   const double *X, *Y, *Z;
   var_axes(g, q, &X, &Y, &Z);
+  const double p0[3] = {X[im], Y[jm], Z[km]};
+  int res = 0;
+  for (int in = 0; in < nn; in++) {
+    const int n = inn[in];
+    if (n < 0) continue;
+    const double *un = ib->n + 3 * n;
+    const double s1[3] = {p0[0] - 10.0 * -un[0], p0[1] - 10.0 * -un[1], p0[2] - 10.0 * -un[2]};
+    const double s2[3] = {p0[0] + 10.0 * -un[0], p0[1] + 10.0 * -un[1], p0[2] + 10.0 * -un[2]};
+    double xm[3];
+    if (!eo_segtriint(s1, s2, ib->v + 9 * n, ib->v + 9 * n + 3, ib->v + 9 * n + 6, xm)) continue;
+    const double r[3] = {fabs(10.0) * un[0], fabs(10.0) * un[1], fabs(10.0) * un[2]};
+    h->fp = n;
+    double xe[3];
+    int dir = 0;
+    const int f = ray_first_face(g, X, Y, Z, flag, p0, r, im, jm, km, xe, &dir);
+    if (f == 1 || f == 0) {
+      memcpy(h->xn, xm, sizeof(xm));
+      memcpy(h->xe, xe, sizeof(xe));
+      h->dir = dir;
+      return f == 1 ? 1 : -1;
+    }
+    if (f == -1) res = -2;
+  }
+  return res;
+}
+
+/* closest_intr (src/matint.f:1693-1985): for every candidate triangle its
+ * nearest point to the point, and the ray from that point through the
+ * forcing point (turned to the triangle's outward side) to the first face it
+ * meets; the first fluid face among the candidates decides, else the first
+ * face holding a forcing node.  fp ends as the last candidate, as in the
+ * reference.  Returns 1, -1, -2 (faces with body nodes only, or none met), 0
+ * (no candidate). */
+static int closest_intr(const eo_ib *ib, int q, const signed char *flag, int im, int jm, int km, const int *inn,
+                        int nn, eo_hit *h) {
+  const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
+  const double p0[3] = {X[im], Y[jm], Z[km]};
+  int ibint = 0, nrec = 0, sel = -1, first = -1;
+  for (int in = 0; in < nn; in++) {
+    const int n = inn[in];
+    if (n < 0) continue;
+    const double *un = ib->n + 3 * n;
+    double pn[3];
+    tri_nearest(ib->v + 9 * n, p0, pn);
+    ibint++;
+    const double d[3] = {p0[0] - pn[0], p0[1] - pn[1], p0[2] - pn[2]};
+    const double mag = magz3(d);
+    double r[3] = {fabs(100.0) * d[0] / mag, fabs(100.0) * d[1] / mag, fabs(100.0) * d[2] / mag};
+    if (dotz3(d, un) < 0) {
+      r[0] = -r[0]; r[1] = -r[1]; r[2] = -r[2];
+    }
+    h->fp = n;
+    double xe[3];
+    int dir = 0;
+    const int f = ray_first_face(g, X, Y, Z, flag, p0, r, im, jm, km, xe, &dir);
+    if (f == 1 || f == 0) {
+      nrec++;
+      if (first < 0) {
+        first = 0;
+        memcpy(h->xn, pn, sizeof(pn));
+        memcpy(h->xe, xe, sizeof(xe));
+        h->dir = dir;
+        sel = f == 1;
+      }
+      if (f == 1 && sel == 0) {
+        /* the first fluid face wins over an earlier forcing-node face */
+        memcpy(h->xn, pn, sizeof(pn));
+        memcpy(h->xe, xe, sizeof(xe));
+        h->dir = dir;
+        sel = 1;
+      }
+    }
+  }
+  if (nrec == 0) return ibint == 0 ? 0 : -2;
+  return sel ? 1 : -1;
+}
+
+/* interp_cellface (src/interp.f:3-82), Cartesian: bilinear interpolation of
+ * a on the cell face normal to axis dir through xp; y indices periodic
+ * (index_bnd, src/matint.f:4377-4405) */
+static double interp_face(const eo_grid *g, const double *X, const double *Y, const double *Z, const double *a,
+                          const double *xp, int dir) {
+  int i, j, k;
+  face_of_point(g, X, Y, Z, xp, dir, &i, &j, &k);
+  /* cells inside the tables (a face point always lies inside them) */
+  i = clampi(i, 1, dir == 1 ? g->nx : g->nx - 1);
+  j = clampi(j, 1, dir == 2 ? g->ny : g->ny - 1);
+  k = clampi(k, 1, dir == 3 ? g->nz : g->nz - 1);
+  int jj[2] = {j, j + 1};
+  for (int b = 0; b < 2; b++) {
+    if (jj[b] <= 1)
+      jj[b] = g->ny - 2 + jj[b];
+    else if (jj[b] >= g->ny)
+      jj[b] = jj[b] - g->ny + 2;
+  }
+  if (dir == 1) {
+    const double b1 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]), c1 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
+    return (((1 - b1) * (1 - c1) * a[IDX(g, i, jj[0], k)] + b1 * (1 - c1) * a[IDX(g, i, jj[1], k)]) +
+            (1 - b1) * c1 * a[IDX(g, i, jj[0], k + 1)]) +
+           b1 * c1 * a[IDX(g, i, jj[1], k + 1)];
+  }
+  if (dir == 2) {
+    const double a1 = (xp[0] - X[i]) / (X[i + 1] - X[i]), c1 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
+    return (((1 - a1) * (1 - c1) * a[IDX(g, i, jj[0], k)] + a1 * (1 - c1) * a[IDX(g, i + 1, jj[0], k)]) +
+            (1 - a1) * c1 * a[IDX(g, i, jj[0], k + 1)]) +
+           a1 * c1 * a[IDX(g, i + 1, jj[0], k + 1)];
+  }
+  const double a1 = (xp[0] - X[i]) / (X[i + 1] - X[i]), b1 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]);
+  return (((1 - a1) * (1 - b1) * a[IDX(g, i, jj[0], k)] + a1 * (1 - b1) * a[IDX(g, i + 1, jj[0], k)]) +
+          (1 - a1) * b1 * a[IDX(g, i, jj[1], k)]) +
+         a1 * b1 * a[IDX(g, i + 1, jj[1], k)];
+}
+
+/* grid_intr (src/matint.f:800-1160), igrdint = 1: the 26 grid directions in
+ * the order of the criterion isrt (0: fluid, then forcing neighbours; 1: the
+ * fluid neighbours by the cosine of the direction with the normal of
+ * triangle fp; 2: the same for fluid and forcing neighbours), the first
+ * candidate triangle the 10x extended grid segment crosses with the
+ * extension point on its outward side.  Returns 1 (fluid extension point),
+ * -1 (a forcing point), 0 (no crossing), -2 (inward crossings only); on 1
+ * and -1 the body point xn, the offsets dd (as reals in ext) and the
+ * triangle fp. */
+int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int jm, int km, const int *inn,
+                    int nn, int isrt, double *xn, double *ext, int *fp) {
+  const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
+  const double p0[3] = {X[im], Y[jm], Z[km]};
   double crit[26];
   int ord[26];
   for (int i = 0; i < 26; i++) {
-    int f = flag[IDX(g, im + GIND[i][0], jm + GIND[i][1], km + GIND[i][2])];
+    const int f = flag[IDX(g, im + GIND[i][0], jm + GIND[i][1], km + GIND[i][2])];
     crit[i] = -2.0;
-    if (f == 0)
-      crit[i] = 1.0;
-    else if (f < 0)
-      crit[i] = 0.5;
+    if (isrt == 0) {
+      if (f == 0)
+        crit[i] = 1.0;
+      else if (f < 0)
+        crit[i] = 0.5;
+    } else if ((isrt == 1 && f == 0) || (isrt == 2 && f <= 0)) {
+      double r[3] = {X[im + GIND[i][0]] - p0[0], Y[jm + GIND[i][1]] - p0[1], Z[km + GIND[i][2]] - p0[2]};
+      const double m = magz3(r);
+      r[0] = r[0] / m; r[1] = r[1] / m; r[2] = r[2] / m;
+      crit[i] = dotz3(r, ib->n + 3 * *fp);
+    }
   }
   int nphy = 0;
   for (int i = 0; i < 26; i++) {
@@ -570,7 +1051,6 @@ int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int
   int intrs = 0, ibint = 0;
   double xint[26][3];
   int tri[26], dir[26], icand[26];
-  const double p0[3] = {X[im], Y[jm], Z[km]};
   for (int i = 0; i < nphy; i++) {
     const int ii = ord[i];
     const int id = GIND[ii][0], jd = GIND[ii][1], kd = GIND[ii][2];
@@ -588,16 +1068,13 @@ int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int
       double xm[3];
       if (eo_segtriint(s1, s2, a, a + 3, a + 6, xm)) {
         ibint++;
-        double dp = unitdot(pe, p0, ib->n + 3 * n);
-        if (dp > 0.0) {
-          if (fext == 0 || fext < 0) {
-            xint[intrs][0] = xm[0]; xint[intrs][1] = xm[1]; xint[intrs][2] = xm[2];
-            tri[intrs] = n;
-            dir[intrs] = ii;
-            icand[intrs] = fext < 0;
-            intrs++;
-            break;
-          }
+        if (unitdot(pe, p0, ib->n + 3 * n) > 0.0) {
+          xint[intrs][0] = xm[0]; xint[intrs][1] = xm[1]; xint[intrs][2] = xm[2];
+          tri[intrs] = n;
+          dir[intrs] = ii;
+          icand[intrs] = fext < 0;
+          intrs++;
+          break;
         }
       }
     }
@@ -616,8 +1093,87 @@ int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int
     }
   }
   xn[0] = xint[bsel][0]; xn[1] = xint[bsel][1]; xn[2] = xint[bsel][2];
-  dd[0] = GIND[dir[bsel]][0]; dd[1] = GIND[dir[bsel]][1]; dd[2] = GIND[dir[bsel]][2];
+  ext[0] = GIND[dir[bsel]][0]; ext[1] = GIND[dir[bsel]][1]; ext[2] = GIND[dir[bsel]][2];
+  *fp = tri[bsel];
   return icand[bsel] ? -1 : 1;
+}
+
+/* one forcing point's search state across the dependency loops (geom_mod):
+ * mrk (0 new; 1, 2, 3 valid; -1, -2, -3 waiting on the normal, grid-line or
+ * closest-point stencil), the triangle fp, the face axis dir, the candidate
+ * list stage icm (lists of 3, 5, nntr3d nearest centroids), the body point
+ * and the extension (face coordinates for mrk 1, 3; grid offsets for 2) */
+typedef struct {
+  int mrk, fp, dir, icm;
+  double xn[3], ext[3];
+} eo_pt;
+
+/* geom_mod's treatment of one point in loop ilp (src/devel.f:9470-9755):
+ * the normal-direction stencil for a new point, else the grid-line stencil,
+ * else the closest-point stencil; waiting points are rechecked against the
+ * working flags.  Returns the new mrk (0: not valid, the point is dropped). */
+static int geom_point(const eo_ib *ib, int q, const signed char *fw, int im, int jm, int km, const int *inn,
+                      int ilp, int mimdif, int ndif, eo_pt *st) {
+  const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
+  const int nfu = ib->nflu;
+  const int sizes[3] = {3, 5, ib->nntr3d};
+  int intrs = 0;
+  if (st->mrk == -1) {
+    intrs = recheck_face(g, X, Y, Z, fw, st->ext, st->dir);
+  } else if (st->mrk == 0) {
+    for (int icm = 0; icm < 3; icm++) {
+      st->icm = icm;
+      eo_hit h;
+      h.fp = st->fp;
+      intrs = norm_intr(ib, q, fw, im, jm, km, inn, sizes[icm], &h);
+      st->fp = h.fp;
+      if (intrs == 1 || intrs == -1) {
+        memcpy(st->xn, h.xn, sizeof(h.xn));
+        memcpy(st->ext, h.xe, sizeof(h.xe));
+        st->dir = h.dir;
+      }
+      if (intrs != 0) break;
+    }
+    if (intrs == 0) st->fp = -1;
+  }
+  if (im <= 2) intrs = 0;
+  if (intrs == 1) return 1;
+  if (intrs == -1 && ilp < nfu && mimdif != 0) return -1;
+  int gintrs = 0;
+  if (st->mrk == -2 && ndif < 3) {
+    gintrs = fw[IDX(g, im + (int)st->ext[0], jm + (int)st->ext[1], km + (int)st->ext[2])] == 0 ? 1 : -1;
+  } else {
+    int srt = 0;
+    if (st->fp >= 0) srt = ndif < 2 ? 1 : 2;
+    int icm = st->icm;
+    while (icm < 3) {
+      gintrs = eo_ib_grid_intr(ib, q, fw, im, jm, km, inn, sizes[icm], srt, st->xn, st->ext, &st->fp);
+      if (gintrs != 0 && gintrs != -2) break;
+      icm++;
+      if (icm < 3) st->icm = icm;
+    }
+  }
+  if (gintrs == 1) return 2;
+  if (gintrs == -1 && ilp < nfu) return -2;
+  int cintrs;
+  if (st->mrk == -3) {
+    cintrs = recheck_face(g, X, Y, Z, fw, st->ext, st->dir);
+  } else {
+    eo_hit h;
+    h.fp = st->fp;
+    cintrs = closest_intr(ib, q, fw, im, jm, km, inn, sizes[st->icm], &h);
+    st->fp = h.fp;
+    if (cintrs == 1 || cintrs == -1) {
+      memcpy(st->xn, h.xn, sizeof(h.xn));
+      memcpy(st->ext, h.xe, sizeof(h.xe));
+      st->dir = h.dir;
+    }
+  }
+  if (cintrs == 1) return 3;
+  if (cintrs == -1 && ilp < nfu && ndif < 2) return -3;
+  return 0;
 }
 
 /* ---- ludcmp/lubksb for n = 2 (implicit partial pivoting, Crout) ---- */
@@ -687,7 +1243,15 @@ void eo_lusolve2(const double *a, const int *indx, double *b) {
   }
 }
 
-/* ---- forcpts + geom_mod (grid-line stencils) + mtrx, variable q (flag fq) ---- */
+/* ---- forcpts + geom_mod + mtrx, variable q (flag fq) ----
+ * The dependency loops of geom_mod (src/devel.f:9420-9770) on one rank:
+ * mimdif is the change in the number of points treated from one loop to the
+ * next and ndif counts the loops without change; a loop treats its points
+ * against the working flags of the previous loops, then the points it made
+ * valid become fluid in those flags (physical_mrk2flag1_mod) and the y ghost
+ * planes are refreshed.  Points are treated in forcpts order; the output is
+ * ordered by the loop that made a point valid, then forcpts order
+ * (rord_forcpts1). */
 void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
   const eo_grid *g = ib->g;
   const double *X, *Y, *Z;
@@ -714,58 +1278,50 @@ void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
           pi[n] = i; pj[n] = j; pk[n] = k;
           n++;
         }
-  long nc = (long)g->nx * g->ny * g->nz;
+  const long nc = (long)g->nx * g->ny * g->nz;
+  const int n1 = n > 0 ? n : 1;
   signed char *fw = (signed char *)malloc(nc);
   memcpy(fw, flagu, nc);
-  int *mrk = (int *)calloc(n > 0 ? n : 1, sizeof(int)), *lev = (int *)calloc(n > 0 ? n : 1, sizeof(int));
-  int *ddx = (int *)calloc(3 * (n > 0 ? n : 1), sizeof(int));
-  double *xnv = (double *)calloc(3 * (n > 0 ? n : 1), sizeof(double));
-  int *pend = (int *)malloc(sizeof(int) * (n > 0 ? n : 1)), *nxt = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
-  int np = n;
-  for (int a = 0; a < n; a++) pend[a] = a;
-  const int sizes[3] = {3, 5, ib->nntr3d};
-  int nlev = 0;
-  for (int ilp = 1; ilp <= ib->nflu && np > 0; ilp++) {
-    int nn2 = 0, nres = 0;
-    int *res = (int *)malloc(sizeof(int) * np);
-    int *gis = (int *)malloc(sizeof(int) * np);
-    /* the points of one loop are independent (fw changes only between loops) */
+  eo_pt *st = (eo_pt *)calloc(n1, sizeof(eo_pt));
+  int *lev = (int *)calloc(n1, sizeof(int)), *inn = (int *)malloc(sizeof(int) * NNTR3D * n1);
+  int *pend = (int *)malloc(sizeof(int) * n1), *nxt = (int *)malloc(sizeof(int) * n1);
+  int *res = (int *)malloc(sizeof(int) * n1), *out = (int *)malloc(sizeof(int) * n1);
+  /* the nearest-centroid lists: sorted by (distance, index), so the lists
+   * of 3 and 5 are prefixes of the nntr3d list */
 #pragma omp parallel for schedule(dynamic, 8)
+  for (int p = 0; p < n; p++) {
+    const double qv[3] = {X[pi[p]], Y[pj[p]], Z[pk[p]]};
+    knn(ib, qv, ib->nntr3d, inn + NNTR3D * p);
+    st[p].fp = -1;
+  }
+  const signed char inonvld = (signed char)(imn == 0 ? 1 : 0);
+  int np = n, prev = 0, ndif = 0, nlev = 0;
+  for (int a = 0; a < n; a++) pend[a] = a;
+  for (int ilp = 1; ilp <= ib->nflu; ilp++) {
+    const int mimdif = np - prev;
+    prev = np;
+    if (mimdif == 0) ndif++;
+    if (np == 0) break;
+    /* the points of one loop are independent: the working flags change
+     * only between loops */
+#pragma omp parallel for schedule(dynamic, 4)
     for (int a = 0; a < np; a++) {
       const int p = pend[a];
-      const int im = pi[p], jm = pj[p], km = pk[p];
-      int gi;
-      if (mrk[p] == -2) {
-        gi = fw[IDX(g, im + ddx[3 * p], jm + ddx[3 * p + 1], km + ddx[3 * p + 2])] == 0 ? 1 : -1;
-      } else {
-        const double qv[3] = {X[im], Y[jm], Z[km]};
-        int inn[NNTR3D];
-        gi = 0;
-        knn(ib, qv, sizes[2], inn);  /* sorted by (distance, index): prefixes are the smaller lists */
-        for (int icm = 0; icm < 3; icm++) {
-          gi = eo_ib_grid_intr(ib, q, fw, im, jm, km, inn, sizes[icm], xnv + 3 * p, ddx + 3 * p);
-          if (gi != 0 && gi != -2) break;
-        }
-      }
-      gis[a] = gi;
+      out[a] = geom_point(ib, q, fw, pi[p], pj[p], pk[p], inn + NNTR3D * p, ilp, mimdif, ndif, st + p);
     }
+    int nres = 0, nn2 = 0;
     for (int a = 0; a < np; a++) {
       const int p = pend[a];
-      const int im = pi[p], jm = pj[p], km = pk[p];
-      const int gi = gis[a];
-      if (gi == 1) {
-        mrk[p] = 2;
+      st[p].mrk = out[a];
+      if (out[a] > 0) {
         lev[p] = ilp;
         res[nres++] = p;
-      } else if (gi == -1 && ilp < ib->nflu) {
-        mrk[p] = -2;
+      } else if (out[a] < 0) {
         nxt[nn2++] = p;
       } else {
-        mrk[p] = 0;
-        flagu[IDX(g, im, jm, km)] = (signed char)(imn == 0 ? 1 : 0);
+        flagu[IDX(g, pi[p], pj[p], pk[p])] = inonvld;
       }
     }
-    free(gis);
     if (nres > 0) nlev = ilp;
     for (int a = 0; a < nres; a++) fw[IDX(g, pi[res[a]], pj[res[a]], pk[res[a]])] = 0;
     for (int k = 1; k <= g->nz; k++)
@@ -773,43 +1329,47 @@ void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
         fw[IDX(g, i, 1, k)] = fw[IDX(g, i, g->ny - 1, k)];
         fw[IDX(g, i, g->ny, k)] = fw[IDX(g, i, 2, k)];
       }
-    free(res);
-    if (nres == 0) {
-      /* no progress: the remaining points are dropped */
-      for (int a = 0; a < nn2; a++) {
-        int p = nxt[a];
-        mrk[p] = 0;
-        flagu[IDX(g, pi[p], pj[p], pk[p])] = (signed char)(imn == 0 ? 1 : 0);
-      }
-      nn2 = 0;
-    }
     int *t = pend; pend = nxt; nxt = t;
     np = nn2;
   }
   /* outputs ordered by level, then forcpts order */
   int nv = 0;
-  for (int a = 0; a < n; a++) nv += mrk[a] == 2;
+  for (int a = 0; a < n; a++) nv += st[a].mrk > 0;
   S->n = nv;
   S->nlev = nlev;
-  int m1 = nv > 0 ? nv : 1;
+  const int m1 = nv > 0 ? nv : 1;
   S->i = (int *)malloc(sizeof(int) * m1); S->j = (int *)malloc(sizeof(int) * m1); S->k = (int *)malloc(sizeof(int) * m1);
   S->di = (int *)malloc(sizeof(int) * m1); S->dj = (int *)malloc(sizeof(int) * m1); S->dk = (int *)malloc(sizeof(int) * m1);
   S->lev = (int *)malloc(sizeof(int) * m1); S->indx = (int *)malloc(sizeof(int) * 2 * m1);
   S->xn = (double *)malloc(sizeof(double) * m1); S->yn = (double *)malloc(sizeof(double) * m1);
   S->zn = (double *)malloc(sizeof(double) * m1); S->lu = (double *)malloc(sizeof(double) * 4 * m1);
+  S->mrk = (int *)malloc(sizeof(int) * m1); S->dir = (int *)malloc(sizeof(int) * m1);
+  S->xe = (double *)malloc(sizeof(double) * m1); S->ye = (double *)malloc(sizeof(double) * m1);
+  S->ze = (double *)malloc(sizeof(double) * m1);
   S->lev_start = (int *)malloc(sizeof(int) * (nlev + 2));
   int o = 0;
   for (int l = 1; l <= nlev; l++) {
     S->lev_start[l - 1] = o;
     for (int a = 0; a < n; a++) {
-      if (mrk[a] != 2 || lev[a] != l) continue;
+      if (st[a].mrk <= 0 || lev[a] != l) continue;
+      const eo_pt *s = st + a;
+      const int grid = s->mrk == 2;
       S->i[o] = pi[a]; S->j[o] = pj[a]; S->k[o] = pk[a];
-      S->di[o] = ddx[3 * a]; S->dj[o] = ddx[3 * a + 1]; S->dk[o] = ddx[3 * a + 2];
+      S->di[o] = grid ? (int)s->ext[0] : 0; S->dj[o] = grid ? (int)s->ext[1] : 0; S->dk[o] = grid ? (int)s->ext[2] : 0;
+      S->xe[o] = grid ? 0. : s->ext[0]; S->ye[o] = grid ? 0. : s->ext[1]; S->ze[o] = grid ? 0. : s->ext[2];
+      S->mrk[o] = s->mrk;
+      S->dir[o] = grid ? 0 : s->dir;
       S->lev[o] = l;
-      S->xn[o] = xnv[3 * a]; S->yn[o] = xnv[3 * a + 1]; S->zn[o] = xnv[3 * a + 2];
-      /* mtrx (src/devel.f:1159-1290), Cartesian, mrk = 2 */
+      S->xn[o] = s->xn[0]; S->yn[o] = s->xn[1]; S->zn[o] = s->xn[2];
+      /* mtrx (src/devel.f:1159-1290), Cartesian: the extension point is the
+       * grid point for mrk = 2, the face point otherwise */
       const double xu = X[pi[a]], yu = Y[pj[a]], zu = Z[pk[a]];
-      const double x1 = X[pi[a] + S->di[o]], y1 = Y[pj[a] + S->dj[o]], z1 = Z[pk[a] + S->dk[o]];
+      double x1, y1, z1;
+      if (grid) {
+        x1 = X[pi[a] + S->di[o]]; y1 = Y[pj[a] + S->dj[o]]; z1 = Z[pk[a] + S->dk[o]];
+      } else {
+        x1 = s->ext[0]; y1 = s->ext[1]; z1 = s->ext[2];
+      }
       const double is1 = imn == 1 ? -1. : 1.;
       double so = sqrt(((xu - S->xn[o]) * (xu - S->xn[o]) + (yu - S->yn[o]) * (yu - S->yn[o])) +
                        (zu - S->zn[o]) * (zu - S->zn[o])) * is1;
@@ -826,7 +1386,7 @@ void eo_ib_geom(eo_ib *ib, int q, int fq, int imn) {
     }
   }
   S->lev_start[nlev] = o;
-  free(pi); free(pj); free(pk); free(fw); free(mrk); free(lev); free(ddx); free(xnv); free(pend); free(nxt);
+  free(pi); free(pj); free(pk); free(fw); free(st); free(lev); free(inn); free(pend); free(nxt); free(res); free(out);
 }
 
 /* the whole regeneration for the current body position (src/Eddy6.f:2163-2380) */
@@ -861,18 +1421,31 @@ static void yper(const eo_grid *g, double *a) {
 }
 
 /* momforc_mod2 explicit (src/momforc.f:1400-1470) / correctpres_mod2 with a
- * zero normal gradient: levels in order, y periodic planes after each */
+ * zero normal gradient (src/momforc.f:1690-1705): the extension value is the
+ * grid point's (mrk 2) or interpolated on the fluid face (mrk 1, 3); levels
+ * in order, y periodic planes after each */
 void eo_ib_force(eo_ib *ib, int q, double *a, double b0) {
   const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
   eo_ib_set *S = &ib->set[q];
   for (int l = 0; l < S->nlev; l++) {
     for (int o = S->lev_start[l]; o < S->lev_start[l + 1]; o++) {
-      int i1 = S->i[o] + S->di[o], j1 = S->j[o] + S->dj[o], k1 = S->k[o] + S->dk[o];
-      if (j1 <= 1)
-        j1 = g->ny - 2 + j1;
-      else if (j1 >= g->ny)
-        j1 = j1 - g->ny + 2;
-      double b[2] = {b0, a[IDX(g, i1, j1, k1)]};
+      double ae;
+      if (S->mrk[o] == 2) {
+        int i1 = S->i[o] + S->di[o], j1 = S->j[o] + S->dj[o], k1 = S->k[o] + S->dk[o];
+        if (j1 <= 1)
+          j1 = g->ny - 2 + j1;
+        else if (j1 >= g->ny)
+          j1 = j1 - g->ny + 2;
+        ae = a[IDX(g, i1, j1, k1)];
+      } else {
+        /* normal-direction and closest-point stencils: the value on the
+         * fluid face (interp_cellface) */
+        const double xe[3] = {S->xe[o], S->ye[o], S->ze[o]};
+        ae = interp_face(g, X, Y, Z, a, xe, S->dir[o]);
+      }
+      double b[2] = {b0, ae};
       eo_lusolve2(S->lu + 4 * o, S->indx + 2 * o, b);
       a[IDX(g, S->i[o], S->j[o], S->k[o])] = b[0];
     }

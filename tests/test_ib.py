@@ -4,7 +4,8 @@ The reference's only IB record (run/stats_imb.dat) needs a grid and STL that
 are not in the repository, so the restated tagging is pinned by invariants of
 a sphere at the origin: mirror symmetry of the tags across x = 0 (the x grid
 and the icosphere are exactly symmetric), the interior volume against the
-sphere volume, and the forcing-point stencils reproducing linear data.
+sphere volume, the share of normal-direction stencils the record shows, and
+the forcing-point stencils reproducing linear data.
 """
 import numpy as np
 import pytest
@@ -42,45 +43,123 @@ def test_interior_volume_matches_sphere(sphere_ib):
     assert abs(v - np.pi / 6) / (np.pi / 6) < 0.1, v
 
 
+def _axes(o, q):
+    names = (("xu", "yc", "zc"), ("xc", "yv", "zc"), ("xc", "yc", "zw"), ("xc", "yc", "zc"))[q]
+    return [np.concatenate([[0.0], o.grid.get(n)]) for n in names]   # 1-based
+
+
+def _points(o, S, q, a):
+    """forcing point, body point and extension point of stencil a"""
+    X, Y, Z = _axes(o, q)
+    i, j, k = S["i"][a], S["j"][a], S["k"][a]
+    p = np.array([X[i], Y[j], Z[k]])
+    xn = np.array([S["xn"][a], S["yn"][a], S["zn"][a]])
+    if S["mrk"][a] == 2:
+        e = np.array([X[i + S["di"][a]], Y[j + S["dj"][a]], Z[k + S["dk"][a]]])
+    else:
+        e = np.array([S["xe"][a], S["ye"][a], S["ze"][a]])
+    return p, xn, e
+
+
 def test_flags_and_stencils_consistent(sphere_ib):
     w, o, ib = sphere_ib
     for q, fq in ((0, 0), (1, 1), (2, 2), (3, 4)):
         F = ib.flags(fq)
         S = ib.stencils(q)
         assert S["n"] > 0 and S["nlev"] >= 1
-        # every stencil point is a forcing point, every extension point is not interior
+        assert set(np.unique(S["mrk"])) <= {1, 2, 3}
+        X, Y, Z = _axes(o, q)
         for a in range(S["n"]):
             i, j, k = S["i"][a] - 1, S["j"][a] - 1, S["k"][a] - 1
             assert F[i, j, k] == -1
-            e = (i + S["di"][a], j + S["dj"][a], k + S["dk"][a])
-            assert F[e] <= 0
+            if S["mrk"][a] == 2:
+                # grid-line stencil: the extension point is not interior
+                e = (i + S["di"][a], j + S["dj"][a], k + S["dk"][a])
+                assert F[e] <= 0
+            else:
+                # face stencils: the extension point lies on a cell face
+                # normal to axis dir, inside the grid
+                d = S["dir"][a]
+                assert d in (1, 2, 3)
+                xe = (S["xe"][a], S["ye"][a], S["ze"][a])
+                ax = (X, Y, Z)[d - 1]
+                assert np.min(np.abs(ax[1:] - xe[d - 1])) < 1e-12
         # levels are non-decreasing along the list
         assert np.all(np.diff(S["lev"]) >= 0)
+
+
+def test_normal_direction_stencils_dominate(sphere_ib):
+    # as in the reference's record of its own run (run/stats_imb.dat: 65% of
+    # the pressure points along the normal, 13% along grid lines), most
+    # points take the normal-direction stencil
+    w, o, ib = sphere_ib
+    for q in range(4):
+        m = ib.stencils(q)["mrk"]
+        assert (m == 1).mean() > 0.5, (q, np.bincount(m))
+
+
+def test_face_stencils_collinear(sphere_ib):
+    # body point, forcing point and extension point lie on one line; for the
+    # velocity points (outside the body) the body point and the extension
+    # point are on opposite sides, the pressure points (inside) have both on
+    # the outward side
+    w, o, ib = sphere_ib
+    for q in range(4):
+        S = ib.stencils(q)
+        for a in range(S["n"]):
+            p, xn, e = _points(o, S, q, a)
+            u, v = xn - p, e - p
+            assert np.linalg.norm(np.cross(u, v)) <= 1e-9 * np.linalg.norm(u) * np.linalg.norm(v) + 1e-15
+            if q < 3:
+                assert np.dot(u, v) <= 1e-15
+            else:
+                assert np.linalg.norm(v) >= np.linalg.norm(u) * (1 - 1e-12) or np.dot(u, v) <= 1e-15
 
 
 def test_velocity_stencil_reproduces_linear_data(sphere_ib):
     """u(s) = c0 + c1 s along the stencil line: forcing with the body value and
     the extension value of a linear field returns its value at the point."""
     w, o, ib = sphere_ib
-    S = ib.stencils(0)
-    # 1-based coordinate lookups
-    xu, yc, zc = (np.concatenate([[0.0], o.grid.get(n)]) for n in ("xu", "yc", "zc"))
-    for a in range(0, S["n"], max(1, S["n"] // 25)):
-        i, j, k = S["i"][a], S["j"][a], S["k"][a]
-        p = np.array([xu[i], yc[j], zc[k]])
-        e = np.array([xu[i + S["di"][a]], yc[j + S["dj"][a]], zc[k + S["dk"][a]]])
-        xn = np.array([S["xn"][a], S["yn"][a], S["zn"][a]])
-        so, s1 = -np.linalg.norm(p - xn), np.linalg.norm(p - e)
-        c0, c1 = 0.7, -1.3
-        A = S["lu"][a]
-        # rebuild L U with the pivot and solve, as lubksb does
-        L = np.array([[1.0, 0.0], [A[1], 1.0]])
-        U = np.array([[A[0], A[2]], [0.0, A[3]]])
-        b = np.array([c0 + c1 * so, c0 + c1 * s1])
-        P = S["indx"][a]
-        b[[0, P[0]]] = b[[P[0], 0]]
-        x = np.linalg.solve(U, np.linalg.solve(L, b))
-        assert abs(x[0] - c0) < 1e-12
+    for q in range(3):
+        S = ib.stencils(q)
+        for a in range(S["n"]):
+            p, xn, e = _points(o, S, q, a)
+            so, s1 = -np.linalg.norm(p - xn), np.linalg.norm(p - e)
+            c0, c1 = 0.7, -1.3
+            A = S["lu"][a]
+            # rebuild L U with the pivot and solve, as lubksb does
+            L = np.array([[1.0, 0.0], [A[1], 1.0]])
+            U = np.array([[A[0], A[2]], [0.0, A[3]]])
+            b = np.array([c0 + c1 * so, c0 + c1 * s1])
+            P = S["indx"][a]
+            b[[0, P[0]]] = b[[P[0], 0]]
+            x = np.linalg.solve(U, np.linalg.solve(L, b))
+            assert abs(x[0] - c0) < 1e-12
+
+
+def test_forcing_interpolates_linear_fields(oracle):
+    # the pressure forcing with a zero normal gradient sets a point to the
+    # extension value: the grid point's for mrk 2, the bilinear value on the
+    # fluid face (interp_cellface) for mrk 1 and 3, which for a linear field
+    # is the field's value at the extension point.  Points of the first
+    # level read only unforced fluid values.
+    w = config.small(mx=64, ly=48, nz_=96)
+    o = oracle.OracleSolver(w)
+    tri, nrm = body.icosphere(5)
+    ib = oracle.OracleIB(o, tri, nrm, attach=False)
+    ib.regen()
+    S = ib.stencils(3)
+    X, Y, Z = _axes(o, 3)
+    f = lambda x, y, z: 1.0 + 0.3 * x - 0.2 * y + 0.45 * z   # noqa: E731
+    a = f(X[1:, None, None], Y[None, 1:, None], Z[None, None, 1:])
+    forced = ib.force(3, a, 0.0)
+    seen = set()
+    for n in range(S["lev_start"][1]):
+        p, xn, e = _points(o, S, 3, n)
+        got = forced[S["i"][n] - 1, S["j"][n] - 1, S["k"][n] - 1]
+        assert abs(got - f(*e)) < 1e-12, (n, S["mrk"][n], got, f(*e))
+        seen.add(int(S["mrk"][n]))
+    assert {1, 2} <= seen, seen
 
 
 @pytest.mark.parametrize("level,shift", [(3, (0.0, 0.0, 0.0)), (5, (0.013, -0.021, 0.37))])
@@ -104,7 +183,8 @@ def test_binned_searches_equal_exhaustive(oracle, level, shift):
         np.testing.assert_array_equal(a, b)
     for a, b in zip(s0, s1):
         assert a["n"] == b["n"] and a["n"] > 0
-        for key in ("i", "j", "k", "di", "dj", "dk", "lev", "xn", "yn", "zn", "lu", "indx"):
+        for key in ("i", "j", "k", "di", "dj", "dk", "lev", "xn", "yn", "zn", "lu", "indx", "mrk", "dir", "xe",
+                    "ye", "ze"):
             np.testing.assert_array_equal(a[key], b[key], err_msg=key)
 
 
