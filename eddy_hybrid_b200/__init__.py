@@ -82,6 +82,15 @@ SIGNATURES = {
     "eddy_ioscalar_read": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.POINTER(C.c_int), _DP, _DP, _DP],
                            C.c_int),
     "eddy_save_field": ([C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_double], C.c_int),
+    "eddy_read_hybrid_plane": ([C.c_char_p, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP, C.POINTER(C.c_int), _DP],
+                               C.c_int),
+    "eddy_inflow_sequence": ([C.c_void_p, C.c_int, _DP, C.c_int, C.c_int], C.c_int),
+    "eddy_inflow_cycle": ([C.c_void_p, C.c_int], C.c_int),
+    "eddy_set_time": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_get_time": ([C.c_void_p, _DP], C.c_int),
+    "eddy_probes_set": ([C.c_void_p, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "eddy_probes_read": ([C.c_void_p, _DP, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "eddy_plane": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _DP], C.c_int),
     "eddy_load_field": ([C.c_void_p, C.c_int, C.c_char_p, C.POINTER(C.c_int), _DP, _DP, _DP], C.c_int),
     "eddy_boundary": ([C.c_void_p, C.c_int], C.c_int),
     "eddy_boundinout": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
@@ -162,6 +171,50 @@ def read_ioscalar(path: str, shape) -> tuple:
     if rc:
         raise EddyError(f"eddy_ioscalar_read failed ({rc}): missing, truncated or another grid")
     return a, ns.value, t.value, dt.value, gr.value
+
+
+def write_hybrid_plane(path: str, u, v, w, d, p=None, icycle: int = 0, time: float = 0.0, dtm1: float = 0.0,
+                       grav: float = 0.0, rho: float = 0.0, re: float = 0.0, pr: float = 0.0, index: int = 0,
+                       xc=None, xu=None, yc=None, yv=None, zcg: float = 0.0, zwg: float = 0.0):
+    """An inflow-plane file in the layout the reference's read_hybrid reads
+    (src/hybrid.f:162-200): Fortran unformatted sequential records with
+    4-byte length markers; the planes are (NX, NY) arrays."""
+    import struct
+    u = np.asfortranarray(u, dtype=np.float64)
+    nx, ny = u.shape
+    zero = np.zeros((nx, ny))
+    planes = [u, v, w, zero if p is None else p, d]
+    xc = np.zeros(nx) if xc is None else xc
+    xu = np.zeros(nx) if xu is None else xu
+    yc = np.zeros(ny) if yc is None else yc
+    yv = np.zeros(ny) if yv is None else yv
+
+    def rec(f, payload: bytes):
+        f.write(struct.pack("<I", len(payload)) + payload + struct.pack("<I", len(payload)))
+
+    with open(path, "wb") as f:
+        rec(f, struct.pack("<i", icycle))
+        rec(f, struct.pack("<6d", time, dtm1, grav, rho, re, pr))
+        rec(f, struct.pack("<3i", 3, 0, index))
+        rec(f, struct.pack("<2d", zcg, zwg))
+        rec(f, struct.pack("<3i", nx, 0, ny))
+        rec(f, np.concatenate([np.asarray(xc, np.float64), np.asarray(xu, np.float64)]).tobytes())
+        rec(f, np.concatenate([np.asarray(yc, np.float64), np.asarray(yv, np.float64)]).tobytes())
+        for a in planes:
+            rec(f, np.asfortranarray(a, dtype=np.float64).tobytes(order="F"))
+
+
+def read_hybrid_plane(path: str, nx: int, ny: int) -> dict:
+    """An inflow-plane file (read_hybrid's layout) through the library's
+    reader: planes u, v, w, p, d of shape (NX, NY), icycle and time."""
+    out = {k: np.zeros((nx, ny), order="F") for k in ("u", "v", "w", "p", "d")}
+    ic, t = C.c_int(0), C.c_double(0.)
+    rc = lib().eddy_read_hybrid_plane(path.encode(), nx, ny, *(_ptr(out[k]) for k in ("u", "v", "w", "p", "d")),
+                                      C.byref(ic), C.byref(t))
+    if rc:
+        raise EddyError(f"eddy_read_hybrid_plane failed ({rc}): missing, truncated or another grid")
+    out["icycle"], out["time"] = ic.value, t.value
+    return out
 
 
 def _ptr(a: np.ndarray):
@@ -261,6 +314,55 @@ class Solver:
             self._check(lib().eddy_load_field(self.h, FID[n], path, C.byref(ns), C.byref(t), C.byref(dt),
                                               C.byref(gr)), "eddy_load_field")
         return {"nstep": ns.value, "time": t.value, "dtm1": dt.value, "grav": gr.value}
+
+    def set_inflow_sequence(self, planes, iref: int, nstep: int = 0):
+        """The hybrid inlet's plane sequence, (n, 4, NX, NY) u, v, w, rho in
+        feed order, kept on the device and cycled by the steps; cells with
+        x index >= iref take the last plane; the step counter starts at nstep."""
+        a = np.ascontiguousarray(np.asarray(planes, dtype=np.float64).transpose(0, 1, 3, 2))
+        n = a.shape[0]
+        self._check(lib().eddy_inflow_sequence(self.h, n, a.ctypes.data_as(_DP), iref, nstep),
+                    "eddy_inflow_sequence")
+
+    @property
+    def time(self) -> float:
+        t = C.c_double(0.)
+        self._check(lib().eddy_get_time(self.h, C.byref(t)), "eddy_get_time")
+        return t.value
+
+    @time.setter
+    def time(self, t: float):
+        self._check(lib().eddy_set_time(self.h, t), "eddy_set_time")
+
+    def set_probes(self, ijk, capacity: int = 1024):
+        """Time probes at 1-based cells ijk (n, 3), recorded on the device
+        after every step."""
+        a = np.ascontiguousarray(np.asarray(ijk, dtype=np.int32).reshape(-1, 3))
+        self._check(lib().eddy_probes_set(self.h, a.shape[0], a.ctypes.data_as(C.c_void_p), capacity),
+                    "eddy_probes_set")
+        self._nprobe = a.shape[0]
+
+    def read_probes(self, max_samples: int = 1 << 20) -> np.ndarray:
+        """The recorded samples, (nsamples, nprobe, 5): time, u, v, w, p."""
+        n = getattr(self, "_nprobe", 0)
+        out = np.zeros(max(1, max_samples * n * 5))
+        cnt = C.c_int(0)
+        self._check(lib().eddy_probes_read(self.h, out.ctypes.data_as(_DP), max_samples, C.byref(cnt)),
+                    "eddy_probes_read")
+        m = min(cnt.value, max_samples)
+        return out[: m * n * 5].reshape(m, n, 5)
+
+    def plane(self, name: str, axis: int, index: int, center: int = 0) -> np.ndarray:
+        """One plane of a field computed on the device (center: the
+        yface_velocity mode 0..4); axis 1, 2, 3 hold i, j, k at index."""
+        nx, ny, nz = self.w.nx, self.w.ny, self.w.nz
+        shape = {1: (ny, nz), 2: (nx, nz), 3: (nx, ny)}[axis]
+        out = np.zeros(shape, order="F")
+        self._check(lib().eddy_plane(self.h, FID[name], center, axis, index, _ptr(out)), "eddy_plane")
+        return out
+
+    def set_cycle(self, icycle: int):
+        self._check(lib().eddy_inflow_cycle(self.h, icycle), "eddy_inflow_cycle")
 
     def cfl(self) -> float:
         v = C.c_double(0.)

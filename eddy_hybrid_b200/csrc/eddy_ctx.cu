@@ -223,7 +223,9 @@ void free_all(eddy_ctx *ctx) {
                   m.dfxu, m.dfxw, m.dfxul, m.dfxwl, m.dfxd, m.dfxdl, m.dens_bg};
   for (double *p : mp) if (p) cudaFree(p);
   for (int f = 0; f < EDDY_NFIELDS; f++) if (ctx->f[f]) cudaFree(ctx->f[f]);
-  double *o[] = {ctx->dens_alt, ctx->gs, ctx->dxdydz, ctx->ilm2, ctx->imm2, ctx->scal, ctx->diag};
+  double *o[] = {ctx->dens_alt, ctx->gs, ctx->dxdydz, ctx->ilm2, ctx->imm2, ctx->scal, ctx->diag, ctx->feed,
+                 ctx->probe_buf, ctx->plane_buf};
+  if (ctx->probe_ijk) cudaFree(ctx->probe_ijk);
   for (double *p : o) if (p) cudaFree(p);
   if (ctx->err_flag) cudaFree(ctx->err_flag);
   poisson_plan_destroy(ctx);
@@ -661,7 +663,76 @@ int eddy_initialize(eddy_ctx *ctx, double dt) {
   return EDDY_OK;
 }
 
+// sequence_hybrid (src/hybrid.f:213-260): the inflow planes of sequence
+// position pos, the cells i >= iref from the last (reference) plane; one
+// thread per (i, j)
+__global__ void k_feed_load(int nx, int ny, const double *feed, int pos, int last, int iref, double *pu, double *pv,
+                            double *pw, double *pd) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n2 = (long long)nx * ny;
+  if (t >= n2) return;
+  const int i = 1 + t % nx;
+  const double *src = feed + (long long)(i >= iref ? last : pos) * 4 * n2;
+  pu[t] = src[t];
+  pv[t] = src[n2 + t];
+  pw[t] = src[2 * n2 + t];
+  pd[t] = src[3 * n2 + t];
+}
+
+// the plane of cycle c into the inlet planes: position c - n floor(c / n) of
+// the feed (icycle_feed, src/hybrid.f:224-232)
+static int feed_load(eddy_ctx *ctx, int c) {
+  if (!ctx->feed || ctx->feed_n <= 0) return EDDY_OK;
+  const int n = ctx->feed_n;
+  const int pos = c - (int)std::floor((double)c / (double)n) * n;
+  const long long n2 = (long long)ctx->d.nx * ctx->d.ny;
+  double **f = ctx->f;
+  k_feed_load<<<(unsigned)((n2 + 255) / 256), 256, 0, ctx->stream>>>(ctx->d.nx, ctx->d.ny, ctx->feed, pos, n - 1,
+                                                                     ctx->feed_iref, f[EDDY_PLANEU], f[EDDY_PLANEV],
+                                                                     f[EDDY_PLANEW], f[EDDY_PLANED]);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
+int eddy_inflow_sequence(eddy_ctx *ctx, int n, const double *planes, int iref, int nstep) {
+  if (check_ctx(ctx) || n < 0 || (n > 0 && !planes)) return EDDY_EINVAL;
+  if (ctx->feed) {
+    EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->feed);
+    ctx->feed = nullptr;
+  }
+  ctx->feed_n = 0;
+  if (n == 0) return EDDY_OK;
+  const size_t b = sizeof(double) * 4 * (size_t)ctx->d.nx * ctx->d.ny * (size_t)n;
+  EDDY_CUDA(cudaMalloc(&ctx->feed, b));
+  EDDY_CUDA(cudaMemcpyAsync(ctx->feed, planes, b, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->feed_n = n;
+  ctx->feed_iref = iref;
+  ctx->icycle = nstep;
+  // the start-up read of cycle nstep - 1 (src/Eddy6.f:806-814)
+  int rc = feed_load(ctx, nstep - 1);
+  if (rc) return rc;
+  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return EDDY_OK;
+}
+
+int eddy_inflow_cycle(eddy_ctx *ctx, int icycle) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  ctx->icycle = icycle;
+  return EDDY_OK;
+}
+
+static int substep_core(eddy_ctx *ctx, int is, double dt);
+
+// one substep, then the inflow plane of the current cycle (sequence_hybrid
+// after each substep, src/Eddy6.f:2985-2991)
 int eddy_substep(eddy_ctx *ctx, int is, double dt) {
+  int rc = substep_core(ctx, is, dt);
+  if (rc) return rc;
+  return feed_load(ctx, ctx->icycle);
+}
+
+static int substep_core(eddy_ctx *ctx, int is, double dt) {
   if (check_ctx(ctx) || is < 0 || is > 2) return EDDY_EINVAL;
   double gam[3], rho[3], alf[3];
   scheme(ctx->prm.ischm, gam, rho, alf);
@@ -736,6 +807,7 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
   if (check_ctx(ctx) || nsteps < 0) return EDDY_EINVAL;
   int nsub = ctx->prm.ischm == 1 ? 1 : 3;
   for (int n = 0; n < nsteps; n++) {
+    ctx->icycle++;  // do icycle=1+nstep,... (src/Eddy6.f:2095)
     for (int is = 0; is < nsub; is++) {
       int rc = eddy_substep(ctx, is, dt);
       if (rc) return rc;
@@ -778,7 +850,26 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
       if ((rc = ib_overlap_regen(ctx))) return rc;
       ctx->ib_prefetched = 1;
     }
+    // TIME after the step (the RK3 / AB2 alphas sum to one), then the time
+    // probes (rec_timeprobes_all, src/Eddy6.f:3640)
+    ctx->time += dt;
+    if (ctx->nprobe > 0) {
+      int rc = probes_record(ctx);
+      if (rc) return rc;
+    }
   }
+  return EDDY_OK;
+}
+
+int eddy_set_time(eddy_ctx *ctx, double time) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  ctx->time = time;
+  return EDDY_OK;
+}
+
+int eddy_get_time(eddy_ctx *ctx, double *time) {
+  if (check_ctx(ctx) || !time) return EDDY_EINVAL;
+  *time = ctx->time;
   return EDDY_OK;
 }
 

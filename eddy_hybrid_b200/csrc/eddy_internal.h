@@ -109,6 +109,18 @@ struct eddy_ctx {
   int64_t launches = 0;
   double dely = 0., delysq = 0.;
   double alfxdt_last = 0.;  // alfxdt of the last CORRECT (the IMPLY pressure correction)
+  // hybrid inflow sequence (device-resident): feed_n planes [n][4][NX*NY] of
+  // u, v, w, rho in feed order; x indices >= feed_iref take the last plane;
+  // icycle is the driver's step counter (src/Eddy6.f:2095)
+  double *feed = nullptr;
+  int feed_n = 0, feed_iref = 0, icycle = 0;
+  double time = 0.;  // TIME: advanced by DTM1 per step in eddy_step
+  // time probes (rec_timeprobes_all): probe cells (1-based ijk), and a
+  // device buffer of samples [cap][n][5] (time, u, v, w, p), count recorded
+  int *probe_ijk = nullptr;
+  double *probe_buf = nullptr;
+  int nprobe = 0, probe_cap = 0, probe_count = 0;
+  double *plane_buf = nullptr;  // staging of eddy_plane (the largest plane of the grid)
   double *xc_dev = nullptr;     // x cell centres (1-based, NX+2)
   double *kappa = nullptr;      // eddy diffusivity of the learned closure (NX,NY,NZ)
   double *tv_dyn = nullptr;     // last dynamic-model nu_t: closure fallback (NX,NY,NZ)
@@ -242,6 +254,7 @@ int ib_limits(eddy_ctx *ctx, int *lim6);
 int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
                 int *indx);
 int ib_stencil_kinds(eddy_ctx *ctx, int q, int *mrk, int *dir, double *xe);
+int probes_record(eddy_ctx *ctx);
 
 // tensor-core (3xTF32) eigen-transforms of the mixed solve (k_xform.cu).
 // sym: mirror-symmetric split form, modes ordered even then odd; lam and m0

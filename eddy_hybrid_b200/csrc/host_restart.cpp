@@ -9,6 +9,17 @@
 //   DTM1, grav               two float64
 // Host-only: the device entry points (eddy_save_field / eddy_load_field) copy
 // through a host buffer around these.
+//
+// Also the inflow-plane files of the hybrid inlet (read_hybrid,
+// src/hybrid.f:162-200), the same record framing:
+//   icycle                                   int32
+//   TIME, DTM1, grav, rho, Re, Pr            six float64
+//   dir, (unused), index                     three int32
+//   zcg, zwg                                 two float64
+//   NX, (unused), NY                         three int32
+//   xc(1:NX), xu(1:NX)                       2 NX float64
+//   yc(1:NY), yv(1:NY)                       2 NY float64
+//   planeU, planeV, planeW, planeP, planeD   NX*NY float64 each
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -70,5 +81,33 @@ extern "C" int eddy_ioscalar_read(const char *path, int nx, int ny, int nz, doub
   if (time) *time = t;
   if (dtm1) *dtm1 = t2[0];
   if (grav) *grav = t2[1];
+  return EDDY_OK;
+}
+
+extern "C" int eddy_read_hybrid_plane(const char *path, int nx, int ny, double *u, double *v, double *w, double *p,
+                                      double *d, int *icycle, double *time) {
+  if (!path || nx < 1 || ny < 1) return EDDY_EINVAL;
+  const uint64_t n2 = (uint64_t)nx * ny;
+  if (n2 * sizeof(double) > 0x7fffffffu) return EDDY_EINVAL;
+  FILE *f = fopen(path, "rb");
+  if (!f) return EDDY_EINVAL;
+  int32_t ic = 0, i3[3] = {0, 0, 0}, dims[3] = {0, 0, 0};
+  double t6[6], z2[2];
+  std::vector<double> axes(2 * (size_t)(nx > ny ? nx : ny)), plane(n2);
+  bool ok = get_record(f, &ic, 4) && get_record(f, t6, sizeof t6) && get_record(f, i3, sizeof i3) &&
+            get_record(f, z2, sizeof z2) && get_record(f, dims, sizeof dims);
+  // a plane of another grid is refused (the reference reads it unchecked)
+  ok = ok && dims[0] == nx && dims[2] == ny;
+  ok = ok && get_record(f, axes.data(), (uint32_t)(2 * nx * sizeof(double))) &&
+       get_record(f, axes.data(), (uint32_t)(2 * ny * sizeof(double)));
+  double *out[5] = {u, v, w, p, d};
+  for (int q = 0; ok && q < 5; q++) {
+    ok = get_record(f, plane.data(), (uint32_t)(n2 * sizeof(double)));
+    if (ok && out[q]) memcpy(out[q], plane.data(), n2 * sizeof(double));
+  }
+  fclose(f);
+  if (!ok) return EDDY_EINVAL;
+  if (icycle) *icycle = ic;
+  if (time) *time = t6[0];
   return EDDY_OK;
 }

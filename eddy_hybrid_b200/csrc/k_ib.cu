@@ -77,6 +77,7 @@ struct IbState {
   int pcap = 0;
   StencilSet set[4];
   int *hcnt = nullptr;  // pinned host counters
+  int coop_blocks_per_sm = 0, nsm = 0;  // residency of the cooperative loop kernel
   bool ready = false;
   int every_substep = 0;  // 1: move + regenerate every substep (IBM > 1), 0: once per step
   // persistent scratch (grown on demand, never freed during a run)
@@ -1438,115 +1439,106 @@ __device__ __forceinline__ void lusolve2(const double *a, const int *indx, doubl
 
 constexpr int GW = 4;  // warps (points) per block
 
-// geom_mod's treatment of the points of loop ilp (src/devel.f:9470-9755),
-// one warp per point: loop 1 treats every point (its nearest-centroid list
-// is computed and kept), later loops the waiting ones (mrk < 0).  A new
-// point tries the normal-direction stencil, else the grid-line stencil, else
-// the closest-point stencil; waiting points are rechecked against the
-// working flags fw.  mimdif (change in the number of points treated from the
-// previous loop) and ndif (loops without change) are geom_mod's.  Valid
-// points record the loop; points without a stencil are dropped (flag =
-// inonvld).  cnt[0] counts the valid points, cnt[1] the waiting ones.
+// geom_mod's treatment of one point in loop ilp (src/devel.f:9470-9755), one
+// warp: a new point tries the normal-direction stencil, else the grid-line
+// stencil, else the closest-point stencil; waiting points are rechecked
+// against the working flags fw.  mimdif (change in the number of points
+// treated from the previous loop) and ndif (loops without change) are
+// geom_mod's.  S (shared) holds the point's state; returns the new mrk (0:
+// no stencil).
+__device__ int geom_decide(const Dims &d, const Axes &ax, const double *v, const double *nrm, const signed char *fw,
+                           int im, int jm, int km, const int *inn, int ilp, int mimdif, int ndif, GeomPt &S) {
+  const int lane = threadIdx.x & 31;
+  const int mrk0 = S.mrk;
+  int intrs = 0;
+  if (mrk0 == -1) {
+    intrs = recheck_face(d, ax, fw, S.ext, S.dir);
+  } else if (mrk0 == 0) {
+    int icm = 0;
+    intrs = norm_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, S, icm);
+    __syncwarp();
+    if (lane == 0) {
+      S.icm = icm;
+      if (intrs == 0) S.fp = -1;
+    }
+    __syncwarp();
+  }
+  if (im <= 2) intrs = 0;
+  if (intrs == 1) return 1;
+  if (intrs == -1 && ilp < NFLU && mimdif != 0) return -1;
+  int gintrs = 0;
+  if (mrk0 == -2 && ndif < 3) {
+    gintrs = fw[lidx(d.nx, d.ny, im + (int)S.ext[0], jm + (int)S.ext[1], km + (int)S.ext[2])] == 0 ? 1 : -1;
+  } else {
+    const int srt = S.fp >= 0 ? (ndif < 2 ? 1 : 2) : 0;
+    int icm = S.icm;
+    gintrs = grid_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, S.icm, srt, S, icm);
+    __syncwarp();
+    if (lane == 0) S.icm = icm;
+    __syncwarp();
+  }
+  if (gintrs == 1) return 2;
+  if (gintrs == -1 && ilp < NFLU) return -2;
+  int cintrs;
+  if (mrk0 == -3)
+    cintrs = recheck_face(d, ax, fw, S.ext, S.dir);
+  else
+    cintrs = closest_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, list_len(S.icm), S);
+  if (cintrs == 1) return 3;
+  if (cintrs == -1 && ilp < NFLU && ndif < 2) return -3;
+  return 0;
+}
+
+// the outcome of a point (lane 0): valid points record the loop, waiting
+// ones are counted, points without a stencil are dropped (flag = inonvld);
+// cnt[0] counts the valid points, cnt[1] the waiting ones
+__device__ __forceinline__ void geom_finish(const Dims &d, int im, int jm, int km, int res, int ilp, GeomPt &S,
+                                            GeomPt *pt, signed char *flag, signed char inonvld, int *cnt) {
+  S.mrk = res;
+  if (res > 0) {
+    S.lev = ilp;
+    atomicAdd(&cnt[0], 1);
+  } else if (res < 0) {
+    atomicAdd(&cnt[1], 1);
+  } else {
+    flag[lidx(d.nx, d.ny, im, jm, km)] = inonvld;
+  }
+  *pt = S;
+}
+
+// the first dependency loop over every point, one warp each: the exact
+// nearest-centroid list (kept for the later loops), then geom_decide
 __global__ void __launch_bounds__(GW * 32)
     k_geom_pass(Dims d, Axes ax, int n, const int *ijk, const double *v, const double *c, const double *nrm, Bins b,
                 const int *bstart, const int *bitems, const signed char *fw, signed char *flag, signed char inonvld,
-                GeomPt *pts, int *inn_all, int ilp, int mimdif, int ndif, int *cnt) {
+                GeomPt *pts, int *inn_all, int *cnt) {
   __shared__ int inn_s[GW][NNTR3D];
   __shared__ KnnSmem ks[GW];
   __shared__ GeomPt sp[GW];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.x * GW + w;
   if (p >= n) return;  // whole warp
-  if (ilp > 1 && pts[p].mrk >= 0) return;
   const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
   int *inn = inn_s[w];
-  if (ilp == 1) {
-    const double qv[3] = {ax.x[im], ax.y[jm], ax.z[km]};
-    // the exact nearest-centroid list is sorted, so the lists of 3 and 5 are
-    // its prefixes
-    if (knn_warp2(b, bstart, bitems, c, qv, NNTR3D, inn, ks[w]) < 0) knn_warp(b, bstart, bitems, c, qv, NNTR3D, inn);
-    __syncwarp();
-    if (lane < NNTR3D) inn_all[(long long)NNTR3D * p + lane] = inn[lane];
-  } else if (lane < NNTR3D) {
-    inn[lane] = inn_all[(long long)NNTR3D * p + lane];
-  }
+  const double qv[3] = {ax.x[im], ax.y[jm], ax.z[km]};
+  // the exact nearest-centroid list is sorted, so the lists of 3 and 5 are
+  // its prefixes
+  if (knn_warp2(b, bstart, bitems, c, qv, NNTR3D, inn, ks[w]) < 0) knn_warp(b, bstart, bitems, c, qv, NNTR3D, inn);
+  __syncwarp();
+  if (lane < NNTR3D) inn_all[(long long)NNTR3D * p + lane] = inn[lane];
   GeomPt &S = sp[w];
   if (lane == 0) {
-    S = pts[p];
-    if (ilp == 1) {
-      S.mrk = 0;
-      S.fp = -1;
-      S.dir = 0;
-      S.icm = 0;
-      S.lev = 0;
-    }
+    S.mrk = 0;
+    S.fp = -1;
+    S.dir = 0;
+    S.icm = 0;
+    S.lev = 0;
+    S.pad = 0;
   }
   __syncwarp();
-  const int mrk0 = S.mrk;
-  int res;  // new mrk
-  {
-    int intrs = 0;
-    if (mrk0 == -1) {
-      intrs = recheck_face(d, ax, fw, S.ext, S.dir);
-    } else if (mrk0 == 0) {
-      int icm = 0;
-      intrs = norm_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, S, icm);
-      __syncwarp();
-      if (lane == 0) {
-        S.icm = icm;
-        if (intrs == 0) S.fp = -1;
-      }
-      __syncwarp();
-    }
-    if (im <= 2) intrs = 0;
-    if (intrs == 1) {
-      res = 1;
-    } else if (intrs == -1 && ilp < NFLU && mimdif != 0) {
-      res = -1;
-    } else {
-      int gintrs = 0;
-      if (mrk0 == -2 && ndif < 3) {
-        gintrs = fw[lidx(d.nx, d.ny, im + (int)S.ext[0], jm + (int)S.ext[1], km + (int)S.ext[2])] == 0 ? 1 : -1;
-      } else {
-        const int srt = S.fp >= 0 ? (ndif < 2 ? 1 : 2) : 0;
-        int icm = S.icm;
-        gintrs = grid_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, S.icm, srt, S, icm);
-        __syncwarp();
-        if (lane == 0) S.icm = icm;
-        __syncwarp();
-      }
-      if (gintrs == 1) {
-        res = 2;
-      } else if (gintrs == -1 && ilp < NFLU) {
-        res = -2;
-      } else {
-        int cintrs;
-        if (mrk0 == -3)
-          cintrs = recheck_face(d, ax, fw, S.ext, S.dir);
-        else
-          cintrs = closest_intr_warp(d, ax, v, nrm, fw, im, jm, km, inn, list_len(S.icm), S);
-        if (cintrs == 1)
-          res = 3;
-        else if (cintrs == -1 && ilp < NFLU && ndif < 2)
-          res = -3;
-        else
-          res = 0;
-      }
-    }
-  }
+  const int res = geom_decide(d, ax, v, nrm, fw, im, jm, km, inn, 1, n, 0, S);
   __syncwarp();
-  if (lane == 0) {
-    S.mrk = res;
-    if (res > 0) {
-      S.lev = ilp;
-      atomicAdd(&cnt[0], 1);
-    } else if (res < 0) {
-      atomicAdd(&cnt[1], 1);
-    } else {
-      flag[lidx(d.nx, d.ny, im, jm, km)] = inonvld;
-    }
-    pts[p] = S;
-  }
+  if (lane == 0) geom_finish(d, im, jm, km, res, 1, S, pts + p, flag, inonvld, cnt);
 }
 
 // the points made valid in loop ilp become fluid in the working flags
@@ -1555,6 +1547,94 @@ __global__ void k_geom_mark(Dims d, int n, const int *ijk, const GeomPt *pts, in
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   if (pts[p].mrk > 0 && pts[p].lev == ilp) fw[lidx(d.nx, d.ny, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2])] = 0;
+}
+
+// grid-wide barrier of a cooperative launch (every block resident): a
+// monotone arrival counter, zeroed before the launch; barrier g completes
+// when g * gridDim.x blocks have arrived.  The wait gives up after 2 s, or
+// once another block has given up, sets the error word and reports failure
+// so that the kernel returns instead of hanging.
+__device__ bool grid_barrier(unsigned *count, unsigned g, int *err) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+    const unsigned target = g * gridDim.x;
+    int ok = 1;
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (unsigned it = 0;; ++it) {
+      if (*(volatile unsigned *)count >= target) break;
+      if (*(volatile int *)err) {
+        ok = 0;
+        break;
+      }
+      if ((it & 63u) == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > 2000000000ull) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// dependency loops 2..NFLU in one cooperative launch (no host round trip per
+// loop): each loop treats the waiting points (warps stride over the list),
+// then, after a grid barrier, the points it made valid become fluid in the
+// working flags together with their y periodic images (the ghost planes were
+// refreshed whole after loop 1, so this equals refreshing them whole), and
+// after another barrier every block reads the loop's counts from cnt (loop l
+// at cnt[2 l], cnt[2 l + 1]) to set the next loop's mimdif and ndif.
+__global__ void __launch_bounds__(GW * 32)
+    k_geom_loops(Dims d, Axes ax, int n, const int *ijk, const double *v, const double *nrm, signed char *fw,
+                 signed char *flag, signed char inonvld, GeomPt *pts, const int *inn_all, int *cnt, unsigned *bar,
+                 int *err) {
+  __shared__ int inn_s[GW][NNTR3D];
+  __shared__ GeomPt sp[GW];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * GW, gw = blockIdx.x * GW + w;
+  const int nthr = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+  int prev = n, ndif = 0;  // loop 1 treated every point, with mimdif = n
+  unsigned g = 0;
+  for (int ilp = 2; ilp <= NFLU; ilp++) {
+    const int np = __ldcg(&cnt[2 * (ilp - 1) + 1]);
+    const int mimdif = np - prev;
+    prev = np;
+    if (mimdif == 0) ndif++;
+    if (np == 0) break;
+    for (int p = gw; p < n; p += nwarps) {
+      if (__ldcg(&pts[p].mrk) >= 0) continue;  // the whole warp
+      const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
+      if (lane < NNTR3D) inn_s[w][lane] = inn_all[(long long)NNTR3D * p + lane];
+      GeomPt &S = sp[w];
+      if (lane == 0) S = pts[p];
+      __syncwarp();
+      const int res = geom_decide(d, ax, v, nrm, fw, im, jm, km, inn_s[w], ilp, mimdif, ndif, S);
+      __syncwarp();
+      if (lane == 0) geom_finish(d, im, jm, km, res, ilp, S, pts + p, flag, inonvld, cnt + 2 * ilp);
+      __syncwarp();
+    }
+    if (!grid_barrier(bar, ++g, err)) return;
+    for (int p = gt; p < n; p += nthr) {
+      if (__ldcg(&pts[p].mrk) > 0 && __ldcg(&pts[p].lev) == ilp) {
+        const int i = ijk[3 * p], j = ijk[3 * p + 1], k = ijk[3 * p + 2];
+        fw[lidx(d.nx, d.ny, i, j, k)] = 0;
+        if (j == d.ny - 1) fw[lidx(d.nx, d.ny, i, 1, k)] = 0;
+        if (j == 2) fw[lidx(d.nx, d.ny, i, d.ny, k)] = 0;
+      }
+    }
+    if (!grid_barrier(bar, ++g, err)) return;
+  }
 }
 
 // number of valid points per level
@@ -1630,31 +1710,59 @@ __global__ void k_level_rank(int n, const GeomPt *pts, int l, int base, const in
 
 // ---------------------------------------------------------------------------
 // forcing (momforc_mod2 explicit / correctpres_mod2, correctdens_mod2 with a
-// zero normal gradient) for the points of one level: the extension value is
-// the grid point's (mrk 2) or the bilinear value on the fluid face
-// (interp_cellface, mrk 1 and 3); T storage with row pitch
+// zero normal gradient) of stencil o: the extension value is the grid
+// point's (mrk 2) or the bilinear value on the fluid face (interp_cellface,
+// mrk 1 and 3); T storage with row pitch
+struct ForceArgs {
+  const int *ijk, *dd, *mrk, *dir, *indx;
+  const double *xe, *lu;
+};
+
 template <class T>
-__global__ void k_force(Dims d, Axes ax, int pitch, int o0, int o1, const int *ijk, const int *dd, const int *mrk,
-                        const int *dir, const double *xe, const double *lu, const int *indx, T *a, double b0,
-                        float *mirror, int mpitch) {
-  const int o = o0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= o1) return;
-  const int im = ijk[3 * o], jm = ijk[3 * o + 1], km = ijk[3 * o + 2];
+__device__ __forceinline__ void force_point(const Dims &d, const Axes &ax, int pitch, int o, const ForceArgs &fa,
+                                            T *a, double b0, float *mirror, int mpitch) {
+  const int im = fa.ijk[3 * o], jm = fa.ijk[3 * o + 1], km = fa.ijk[3 * o + 2];
   double ae;
-  if (mrk[o] == 2) {
-    int i1 = im + dd[3 * o], j1 = jm + dd[3 * o + 1], k1 = km + dd[3 * o + 2];
+  if (fa.mrk[o] == 2) {
+    int i1 = im + fa.dd[3 * o], j1 = jm + fa.dd[3 * o + 1], k1 = km + fa.dd[3 * o + 2];
     if (j1 <= 1)
       j1 = d.ny - 2 + j1;
     else if (j1 >= d.ny)
       j1 = j1 - d.ny + 2;
     ae = (double)a[pidx(d, pitch, i1, j1, k1)];
   } else {
-    ae = interp_face<T>(d, ax, pitch, a, xe + 3 * o, dir[o]);
+    ae = interp_face<T>(d, ax, pitch, a, fa.xe + 3 * o, fa.dir[o]);
   }
   double b[2] = {b0, ae};
-  lusolve2(lu + 4 * o, indx + 2 * o, b);
+  lusolve2(fa.lu + 4 * o, fa.indx + 2 * o, b);
   a[pidx(d, pitch, im, jm, km)] = (T)b[0];
   if (mirror) mirror[pidx(d, mpitch, im, jm, km)] = (float)b[0];
+}
+
+// the points of one level, one thread each
+template <class T>
+__global__ void k_force(Dims d, Axes ax, int pitch, int o0, int o1, ForceArgs fa, T *a, double b0, float *mirror,
+                        int mpitch) {
+  const int o = o0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= o1) return;
+  force_point<T>(d, ax, pitch, o, fa, a, b0, mirror, mpitch);
+}
+
+// offsets of the dependency levels (level l: [v[l], v[l+1]))
+struct LevOffsets {
+  int v[NFLU + 2];
+};
+
+// levels l0..l1-1 in order by one CTA: a level reads what the earlier ones
+// wrote, which the block barrier makes visible
+template <class T>
+__global__ void __launch_bounds__(1024) k_force_levels(Dims d, Axes ax, int pitch, LevOffsets ls, int l0, int l1,
+                                                       ForceArgs fa, T *a, double b0, float *mirror, int mpitch) {
+  for (int l = l0; l < l1; l++) {
+    for (int o = ls.v[l] + threadIdx.x; o < ls.v[l + 1]; o += blockDim.x)
+      force_point<T>(d, ax, pitch, o, fa, a, b0, mirror, mpitch);
+    __syncthreads();
+  }
 }
 
 // y periodic planes of a field (whole (i, k) range)
@@ -1847,7 +1955,7 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   if (n == 0) return EDDY_OK;
   // per-point search state, nearest-centroid lists, output positions
   int *inn = scratch(ctx, s, IbState::S_INN, (size_t)NNTR3D * n), *order = scratch(ctx, s, IbState::S_ORDER, n),
-      *cnt = scratch(ctx, s, IbState::S_CNT, NFLU + 2);
+      *cnt = scratch(ctx, s, IbState::S_CNT, 3 * (NFLU + 2) + 2);
   GeomPt *pts = reinterpret_cast<GeomPt *>(scratch_d(ctx, s, (sizeof(GeomPt) / sizeof(double)) * (size_t)n));
   if (!inn || !order || !cnt || !pts) return EDDY_ENOMEM;
   signed char *fw = s->work;
@@ -1855,36 +1963,57 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   EDDY_CUDA(cudaMemcpyAsync(fw, flag, nc, cudaMemcpyDeviceToDevice, st));
   Axes ax = axes_of(ctx, q);
   const signed char inonvld = (signed char)(imn == 0 ? 1 : 0);
-  // the dependency loops of geom_mod (src/devel.f:9420-9770): np points are
-  // treated in a loop (all of them in the first); the points it makes valid
-  // become fluid in the working flags, whose y ghost planes are refreshed
-  int np = n, prev = 0, ndif = 0, nlev = 0;
-  for (int ilp = 1; ilp <= NFLU; ilp++) {
-    const int mimdif = np - prev;
-    prev = np;
-    if (mimdif == 0) ndif++;
-    if (np == 0) break;
-    EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * 2, st));
-    k_geom_pass<<<(unsigned)((n + GW - 1) / GW), GW * 32, 0, st>>>(d, ax, n, s->pts, s->v, s->c, s->n, s->b3,
-                                                                    s->b3.start, s->b3.items, fw, flag, inonvld, pts,
-                                                                    inn, ilp, mimdif, ndif, cnt);
+  // the dependency loops of geom_mod (src/devel.f:9420-9770): loop 1 over
+  // every point (with the nearest-centroid searches), its valid points made
+  // fluid in the working flags and their y ghost planes refreshed whole; then
+  // loops 2..NFLU in one cooperative launch that keeps the loop control on
+  // the device.  cnt: loop l's valid / waiting counts at [2 l], [2 l + 1];
+  // level counts from LC; the barrier counter last.
+  constexpr int LC = 2 * (NFLU + 2);
+  EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (LC + NFLU + 3), st));
+  k_geom_pass<<<(unsigned)((n + GW - 1) / GW), GW * 32, 0, st>>>(d, ax, n, s->pts, s->v, s->c, s->n, s->b3,
+                                                                  s->b3.start, s->b3.items, fw, flag, inonvld, pts, inn,
+                                                                  cnt + 2);
+  EDDY_LAUNCHED(ctx);
+  k_geom_mark<<<nblk(n), 256, 0, st>>>(d, n, s->pts, pts, 1, fw);
+  EDDY_LAUNCHED(ctx);
+  k_yper_i8<<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, fw, 1, d.nx, 1, d.nz);
+  EDDY_LAUNCHED(ctx);
+  {
+    if (s->coop_blocks_per_sm <= 0) {
+      int nsm = 0, per = 0;
+      EDDY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+      EDDY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_geom_loops, GW * 32, 0));
+      s->coop_blocks_per_sm = std::max(1, per);
+      s->nsm = nsm;
+    }
+    const int grid = (int)std::max(1LL, std::min((long long)s->coop_blocks_per_sm * s->nsm, (long long)(n + GW - 1) / GW));
+    const Dims dd = d;
+    const Axes axx = ax;
+    int nn = n;
+    const int *ijk = s->pts;
+    const double *vv = s->v, *nrm = s->n;
+    signed char *fwp = fw, *flp = flag, inv = inonvld;
+    GeomPt *ptp = pts;
+    const int *innp = inn;
+    int *cntp = cnt;
+    unsigned *bar = reinterpret_cast<unsigned *>(cnt + LC + NFLU + 2);
+    int *err = ctx->err_flag;
+    void *args[] = {(void *)&dd, (void *)&axx, (void *)&nn, (void *)&ijk, (void *)&vv, (void *)&nrm, (void *)&fwp,
+                    (void *)&flp, (void *)&inv, (void *)&ptp, (void *)&innp, (void *)&cntp, (void *)&bar,
+                    (void *)&err};
+    EDDY_CUDA(cudaLaunchCooperativeKernel((const void *)k_geom_loops, dim3(grid), dim3(GW * 32), args, 0, st));
     EDDY_LAUNCHED(ctx);
-    k_geom_mark<<<nblk(n), 256, 0, st>>>(d, n, s->pts, pts, ilp, fw);
-    EDDY_LAUNCHED(ctx);
-    k_yper_i8<<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, fw, 1, d.nx, 1, d.nz);
-    EDDY_LAUNCHED(ctx);
-    EDDY_CUDA(cudaMemcpyAsync(s->hcnt, cnt, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
-    EDDY_CUDA(cudaStreamSynchronize(st));
-    if (s->hcnt[0] > 0) nlev = ilp;
-    np = s->hcnt[1];
   }
-  // level sizes -> offsets
-  EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (NFLU + 2), st));
-  k_geom_rank_count<<<nblk(n), 256, 0, st>>>(n, pts, cnt + 1);
+  // level sizes -> offsets (the one read-back of the loops)
+  k_geom_rank_count<<<nblk(n), 256, 0, st>>>(n, pts, cnt + LC + 1);
   EDDY_LAUNCHED(ctx);
   std::vector<int> lc(NFLU + 2, 0);
-  EDDY_CUDA(cudaMemcpyAsync(lc.data(), cnt + 1, sizeof(int) * (NFLU + 1), cudaMemcpyDeviceToHost, st));
+  EDDY_CUDA(cudaMemcpyAsync(lc.data(), cnt + LC + 1, sizeof(int) * (NFLU + 1), cudaMemcpyDeviceToHost, st));
   EDDY_CUDA(cudaStreamSynchronize(st));
+  int nlev = 0;
+  for (int l = 0; l < NFLU; l++)
+    if (lc[l] > 0) nlev = l + 1;
   S.lev_start.assign(nlev + 1, 0);
   for (int l = 0; l < nlev; l++) S.lev_start[l + 1] = S.lev_start[l] + lc[l];
   const int nv = S.lev_start[nlev];
@@ -2127,13 +2256,36 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
   const Dims &d = ctx->d;
   cudaStream_t st = ctx->stream;
   StencilSet &S = s->set[q];
-  for (int l = 0; l < S.nlev; l++) {
-    const int o0 = S.lev_start[l], o1 = S.lev_start[l + 1];
-    if (o1 > o0) {
-      k_force<T><<<nblk(o1 - o0, 128), 128, 0, st>>>(d, axes_of(ctx, q), pitch, o0, o1, S.ijk, S.dijk, S.mrk, S.dir,
-                                                     S.xe, S.lu, S.indx, a, b0, mirror, mpitch);
+  // The reference refreshes the y ghost planes after every level.  Forcing
+  // points lie in j = 2..NY-1 and every read wraps j into that range
+  // (index_bnd), so no level reads a ghost plane and one refresh after the
+  // last level leaves the same state.  Large levels get a grid each; runs of
+  // small ones go to one CTA that steps through them.
+  const Axes ax = axes_of(ctx, q);
+  const ForceArgs fa{S.ijk, S.dijk, S.mrk, S.dir, S.indx, S.xe, S.lu};
+  constexpr int BIG = 4096;
+  LevOffsets ls{};
+  for (int l = 0; l <= S.nlev && l < NFLU + 2; l++) ls.v[l] = S.lev_start[l];
+  int run0 = -1;
+  for (int l = 0; l <= S.nlev; l++) {
+    const bool end = l == S.nlev;
+    const int cnt = end ? 0 : S.lev_start[l + 1] - S.lev_start[l];
+    if (!end && cnt <= BIG) {
+      if (run0 < 0) run0 = l;
+      continue;
+    }
+    if (run0 >= 0) {
+      k_force_levels<T><<<1, 1024, 0, st>>>(d, ax, pitch, ls, run0, l, fa, a, b0, mirror, mpitch);
+      EDDY_LAUNCHED(ctx);
+      run0 = -1;
+    }
+    if (!end) {
+      k_force<T><<<nblk(cnt, 128), 128, 0, st>>>(d, ax, pitch, S.lev_start[l], S.lev_start[l + 1], fa, a, b0,
+                                                  mirror, mpitch);
       EDDY_LAUNCHED(ctx);
     }
+  }
+  if (S.nlev > 0) {
     k_yper_field<T><<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, pitch, a, mirror, mpitch);
     EDDY_LAUNCHED(ctx);
   }

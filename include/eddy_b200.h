@@ -100,6 +100,28 @@ int eddy_ioscalar_read(const char *path, int nx, int ny, int nz, double *a, int 
 int eddy_save_field(eddy_ctx *ctx, int field, const char *path, int nstep, double time, double dtm1);
 int eddy_load_field(eddy_ctx *ctx, int field, const char *path, int *nstep, double *time, double *dtm1,
                     double *grav);
+/* The hybrid inlet's inflow planes (src/hybrid.f:162-260).  A plane file in
+ * the layout read_hybrid reads (Fortran unformatted records: icycle; TIME,
+ * DTM1, grav, rho, Re, Pr; dir, -, index; zcg, zwg; NX, -, NY; xc, xu; yc,
+ * yv; planeU, planeV, planeW, planeP, planeD), host-only; a file of another
+ * grid or a truncated one is refused with EDDY_EINVAL; null outputs are
+ * skipped. */
+int eddy_read_hybrid_plane(const char *path, int nx, int ny, double *u, double *v, double *w, double *p, double *d,
+                           int *icycle, double *time);
+/* The sequence of n inflow planes, planes[n][4][NX*NY] (u, v, w, rho in feed
+ * order, Fortran-ordered planes: the contents of the files start_feed,
+ * start_feed + stride_feed, ..., end_feed), kept on the device.  Sets the
+ * step counter to nstep and loads the plane of cycle nstep - 1, as the
+ * start-up call src/Eddy6.f:806-814 does; every eddy_substep then loads the
+ * plane of the current cycle (sequence_hybrid after each substep,
+ * src/Eddy6.f:2985-2991: position c - n floor(c/n) of the feed), the cells
+ * i >= iref from the last plane (the reference's steady far field; it has
+ * iref = 116; NX + 1 turns that off).  eddy_step advances the
+ * counter at the start of each step (src/Eddy6.f:2095); a driver stepping
+ * with eddy_substep sets it with eddy_inflow_cycle before each step.  n = 0
+ * removes the sequence (the inlet planes then stay as uploaded). */
+int eddy_inflow_sequence(eddy_ctx *ctx, int n, const double *planes, int iref, int nstep);
+int eddy_inflow_cycle(eddy_ctx *ctx, int icycle);
 /* Read one of the 1-D metric arrays the context built (same numbering as the
  * oracle: 0 xu 1 xc 2 ap 3 au 4 av 5 aw 6 yv 7 yc 8 bp 9 bu 10 bv 11 bw
  * 12 zw 13 zc 14 cp 15 cu 16 cv 17 cw 18 whx 19 why 20 whz 21 dfxu 22 dfxw
@@ -215,6 +237,29 @@ int eddy_cfl(eddy_ctx *ctx, double *cflm);
 /* SCRINFO's extrema (src/info.f:5-164): min and max of a field over the
  * interior. */
 int eddy_field_extrema(eddy_ctx *ctx, int field, double *vmin, double *vmax);
+
+/* Simulation time TIME: eddy_step advances it by dt per step (the RK3 and
+ * AB2 coefficients sum to one); set it when starting from a restart. */
+int eddy_set_time(eddy_ctx *ctx, double time);
+int eddy_get_time(eddy_ctx *ctx, double *time);
+/* Time probes on the device (rec_timeprobes_all, src/stats.f:132-185,
+ * called every step at src/Eddy6.f:3640): n probe cells ijk[3n] (1-based,
+ * the contents of probes.input, src/stats.f:48-66) and room for `capacity`
+ * samples.  After every step of eddy_step the cell values of UO, VO, WO and
+ * P at each probe are recorded with TIME, on the device; samples past the
+ * capacity are dropped.  eddy_probes_read copies up to max_samples samples,
+ * out[s][probe][5] = (time, u, v, w, p), consumes them, and returns in
+ * *nsamples the number recorded before the read.  n = 0 removes the probes. */
+int eddy_probes_set(eddy_ctx *ctx, int n, const int *ijk, int capacity);
+int eddy_probes_read(eddy_ctx *ctx, double *out, int max_samples, int *nsamples);
+/* One plane of a 3-D field, computed on the device and copied to out
+ * (WRITE_PLANES / yface_velocity, src/Planes.f:1-543, without the file):
+ * center 0 or 2 the cell values, 1 the average of u over (i-1, i) x (j,
+ * j+1), 3 of w over (k-1, k) x (j, j+1) (both 0 outside i, k = 2..N-1 and j
+ * = 1..NY-1), 4 the average over (j, j+1) (0 at j = NY); axis 1 the (j, k)
+ * plane at i = index (out[NY*NZ]), 2 the (i, k) plane at j = index
+ * (out[NX*NZ]), 3 the (i, j) plane at k = index (out[NX*NY]); Fortran order. */
+int eddy_plane(eddy_ctx *ctx, int field, int center, int axis, int index, double *out);
 
 /* Kernel-category timing with CUDA events on the context stream (the
  * device-side counterpart of the reference's CLOCK array, src/info.f:350 and

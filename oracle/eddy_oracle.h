@@ -85,6 +85,11 @@ typedef struct {
   double *g_s, *sxx, *syy, *szz, *sxy, *syz, *sxz, *ilm, *imm, *lm, *mm,
       *uc, *vc, *wc, *dxdydz, *cles;
   double *planeU, *planeV, *planeW, *planeD; /* (NX,NY) inflow planes */
+  /* hybrid inflow sequence (src/hybrid.f:213-260): feed_n planes of u, v, w,
+   * rho in feed order ([n][4][NX*NY]); x indices >= feed_iref take the last
+   * plane (the reference plane); icycle is the driver's step counter */
+  double *feed;
+  int feed_n, feed_iref, icycle;
   double time;
   double alfxdt_last; /* alfxdt of the last CORRECT (the pressure update's implicit correction) */
   double pref_last;
@@ -215,6 +220,16 @@ int eo_ib_grid_intr(const eo_ib *ib, int q, const signed char *flag, int im, int
  * stencils and applies the forcing (src/Eddy6.f:2163-2380, 2526-2575,
  * 2881-2897, 2972-2983) */
 void eo_state_set_ib(eo_state *s, eo_ib *ib);
+/* hybrid inflow sequence: n planes of (u, v, w, rho) in feed order, each
+ * NX*NY (Fortran order), copied in; the cells i >= iref take the last plane
+ * (sequence_hybrid, src/hybrid.f:250-258; the reference has iref = 116); the
+ * step counter is set to nstep and the plane of cycle nstep - 1 loaded, as
+ * the start-up call src/Eddy6.f:806-814 does.  eo_step then loads the plane
+ * of the current cycle after every substep (src/Eddy6.f:2985-2991). */
+void eo_feed_set(eo_state *s, int n, const double *planes, int iref, int nstep);
+/* the sequence position of cycle c (sequence_hybrid's icycle_feed, as a
+ * 0-based position in feed order) */
+int eo_feed_position(int c, int n);
 
 /* ---- deterministic noise: SplitMix64 counter generator ---- */
 uint64_t eo_splitmix64(uint64_t x);

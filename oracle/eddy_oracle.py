@@ -128,6 +128,9 @@ def lib():
         L.eo_ib_stencils.argtypes = [vp, C.c_int]
         L.eo_ib_body.argtypes = [vp, dp, dp]
         L.eo_state_set_ib.argtypes = [vp, vp]
+        L.eo_feed_set.argtypes = [vp, C.c_int, dp, C.c_int, C.c_int]
+        L.eo_feed_position.argtypes = [C.c_int, C.c_int]
+        L.eo_feed_position.restype = C.c_int
         L.eo_locate.restype = C.c_int
         L.eo_locate.argtypes = [dp, C.c_int, C.c_double]
         _lib = L
@@ -252,6 +255,11 @@ class OracleSolver:
 
     def max_divergence(self):
         return lib().eo_max_divergence(self.h)
+
+    def set_inflow_sequence(self, planes: np.ndarray, iref: int, nstep: int = 0):
+        """planes: (n, 4, NX, NY) inflow planes u, v, w, rho in feed order"""
+        a = np.ascontiguousarray(np.asarray(planes, dtype=np.float64).transpose(0, 1, 3, 2))
+        lib().eo_feed_set(self.h, a.shape[0], a.ctypes.data_as(C.POINTER(C.c_double)), iref, nstep)
 
     def __del__(self):
         if getattr(self, "h", None):

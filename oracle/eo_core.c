@@ -75,6 +75,7 @@ void eo_state_free(eo_state *s) {
                   s->vc, s->wc, s->dxdydz, s->cles, s->planeU, s->planeV,
                   s->planeW, s->planeD};
   for (size_t i = 0; i < sizeof(f3) / sizeof(f3[0]); i++) free(f3[i]);
+  free(s->feed);
   free(s);
 }
 

@@ -84,6 +84,44 @@ void eo_substep(eo_state *s, int is, double dtm1) {
 
 void eo_state_set_ib(eo_state *s, eo_ib *ib) { s->ib = ib; }
 
+/* sequence_hybrid (src/hybrid.f:224-232): icycle_feed = start + stride*c -
+ * stride*floor(c/num)*num, i.e. position c - num*floor(c/num) of the feed */
+int eo_feed_position(int c, int n) {
+  const int nfc = (int)floor((double)c / (double)n);
+  return c - nfc * n;
+}
+
+/* the plane of cycle c into planeU..planeD; i >= iref from the last plane
+ * (src/hybrid.f:250-258) */
+static void feed_load(eo_state *s, int c) {
+  if (!s->feed || s->feed_n <= 0) return;
+  const int nx = s->prm.nx, ny = s->prm.ny;
+  const long n2 = (long)nx * ny;
+  const double *src = s->feed + (long)eo_feed_position(c, s->feed_n) * 4 * n2;
+  const double *ref = s->feed + (long)(s->feed_n - 1) * 4 * n2;
+  double *dst[4] = {s->planeU, s->planeV, s->planeW, s->planeD};
+  for (int f = 0; f < 4; f++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        const long q = (long)(i - 1) + (long)nx * (j - 1);
+        dst[f][q] = i >= s->feed_iref ? ref[f * n2 + q] : src[f * n2 + q];
+      }
+}
+
+void eo_feed_set(eo_state *s, int n, const double *planes, int iref, int nstep) {
+  free(s->feed);
+  s->feed = NULL;
+  s->feed_n = 0;
+  if (n <= 0) return;
+  const long n2 = (long)s->prm.nx * s->prm.ny;
+  s->feed = (double *)malloc(sizeof(double) * 4 * n2 * n);
+  memcpy(s->feed, planes, sizeof(double) * 4 * n2 * n);
+  s->feed_n = n;
+  s->feed_iref = iref;
+  s->icycle = nstep;
+  feed_load(s, nstep - 1);
+}
+
 void eo_step(eo_state *s, double dtm1, int nsteps, int poisson_method) {
   double gam[3], rho[3], alf[3];
   scheme(s->prm.ischm, gam, rho, alf);
@@ -91,8 +129,10 @@ void eo_step(eo_state *s, double dtm1, int nsteps, int poisson_method) {
   int nsub = (s->prm.ischm == 1) ? 1 : 3;
   for (int n = 0; n < nsteps; n++) {
     double tlevel = s->time;
+    s->icycle++; /* do icycle=1+nstep,... (:2095) */
     for (int is = 0; is < nsub; is++) {
       eo_substep(s, is, dtm1);
+      feed_load(s, s->icycle); /* sequence_hybrid after each substep (:2985-2991) */
       double sa = 0.;
       for (int q = 0; q <= is; q++) sa += alf[q];
       tlevel = s->time + sa * dtm1;
