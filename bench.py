@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--small", action="store_true", help="tiny grid (smoke)")
     ap.add_argument("--medium", action="store_true",
                     help="128x192x128 grid (~3M cells, ~1 GB on the device) for ncu captures")
+    ap.add_argument("--profile", default=None, choices=["plain", "mixed"],
+                    help="run one form (warm-up + steps, the dynamic model) and exit without timing: the "
+                         "command to put under a profiler")
     ap.add_argument("--grid", default=None,
                     help="NZ-2xNX-2xNY-2 of the wake workload, e.g. 64x384x256 (6.3M cells, fields larger "
                          "than L2, a few GB on the device) for ncu captures")
@@ -381,6 +384,16 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         return {"ms": ms, "prof": prof, "launches": launches, "clocks": clk, "stream": st}
+
+    if args.profile:
+        g = make(eb.PLAIN_FP64 if args.profile == "plain" else eb.MIXED, 0)
+        g.load_initial(config.initial_fields(w, g.metric("dens_bg")[: w.nx]))
+        g.initialize()
+        g.step(args.warmup)
+        g.step(args.steps)
+        g.sync()
+        log(f"profile run: {args.profile} form, {args.warmup} + {args.steps} steps of {w.name}")
+        return
 
     # ---- plain FP64 form (the accuracy reference: bit-exact / 1e-11 against the CPU oracle) ----
     g0 = make(eb.PLAIN_FP64, 0)

@@ -55,6 +55,8 @@ struct StencilSet {
   int n = 0, nlev = 0, cap = 0;
   int *ijk = nullptr, *dijk = nullptr, *lev = nullptr, *indx = nullptr, *mrk = nullptr, *dir = nullptr;
   double *xn = nullptr, *lu = nullptr, *xe = nullptr;
+  int *fijk = nullptr;   // face stencils: interpolation cell (i, j, j+1 periodic, k)
+  double *fw = nullptr;  // and its two weights
   std::vector<int> lev_start;
 };
 
@@ -81,7 +83,7 @@ struct IbState {
   bool ready = false;
   int every_substep = 0;  // 1: move + regenerate every substep (IBM > 1), 0: once per step
   // persistent scratch (grown on demand, never freed during a run)
-  enum { S_BINCNT = 0, S_BCNT, S_BOFF, S_CUR, S_INN, S_ORDER, S_CNT, S_BSUM, S_NI };
+  enum { S_BINCNT = 0, S_BCNT, S_BOFF, S_CUR, S_INN, S_ORDER, S_CNT, S_BSUM, S_LCNT, S_LOFF, S_NI };
   int *si[S_NI] = {};
   size_t si_cap[S_NI] = {};
   double *sxn = nullptr;
@@ -445,10 +447,12 @@ __device__ void tri_nearest(const double *tv, const double *p, double *out) {
   for (int a = 0; a < 3; a++) out[a] = (tv[a] + s * e0[a]) + t * e1[a];
 }
 
-// interp_cellface (src/interp.f:3-82), Cartesian: bilinear value of a on the
-// cell face normal to axis dir through xp, y indices periodic (index_bnd)
-template <class T>
-__device__ double interp_face(const Dims &d, const Axes &ax, int pitch, const T *a, const double *xp, int dir) {
+// interp_cellface (src/interp.f:3-82), Cartesian, the geometric part: the
+// cell face normal to axis dir holding xp (closest node along dir, LOCATE
+// cells along the others, kept inside the tables), its y indices j and j+1
+// made periodic (index_bnd), and the two interpolation weights (y and z for
+// dir 1, x and z for dir 2, x and y for dir 3).  The forcing applies them.
+__device__ void face_weights(const Dims &d, const Axes &ax, const double *xp, int dir, int *fijk, double *fw) {
   int i, j, k;
   face_of_point(d, ax, xp, dir, i, j, k);
   i = min(max(i, 1), dir == 1 ? d.nx : d.nx - 1);
@@ -458,25 +462,19 @@ __device__ double interp_face(const Dims &d, const Axes &ax, int pitch, const T 
   if (j0 <= 1) j0 = d.ny - 2 + j0; else if (j0 >= d.ny) j0 = j0 - d.ny + 2;
   if (j1 <= 1) j1 = d.ny - 2 + j1; else if (j1 >= d.ny) j1 = j1 - d.ny + 2;
   const double *X = ax.x, *Y = ax.y, *Z = ax.z;
+  double w1, w2;
   if (dir == 1) {
-    const double b1 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]), c1 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
-    return (((1 - b1) * (1 - c1) * (double)a[pidx(d, pitch, i, j0, k)] +
-             b1 * (1 - c1) * (double)a[pidx(d, pitch, i, j1, k)]) +
-            (1 - b1) * c1 * (double)a[pidx(d, pitch, i, j0, k + 1)]) +
-           b1 * c1 * (double)a[pidx(d, pitch, i, j1, k + 1)];
+    w1 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]);
+    w2 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
+  } else if (dir == 2) {
+    w1 = (xp[0] - X[i]) / (X[i + 1] - X[i]);
+    w2 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
+  } else {
+    w1 = (xp[0] - X[i]) / (X[i + 1] - X[i]);
+    w2 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]);
   }
-  if (dir == 2) {
-    const double a1 = (xp[0] - X[i]) / (X[i + 1] - X[i]), c1 = (xp[2] - Z[k]) / (Z[k + 1] - Z[k]);
-    return (((1 - a1) * (1 - c1) * (double)a[pidx(d, pitch, i, j0, k)] +
-             a1 * (1 - c1) * (double)a[pidx(d, pitch, i + 1, j0, k)]) +
-            (1 - a1) * c1 * (double)a[pidx(d, pitch, i, j0, k + 1)]) +
-           a1 * c1 * (double)a[pidx(d, pitch, i + 1, j0, k + 1)];
-  }
-  const double a1 = (xp[0] - X[i]) / (X[i + 1] - X[i]), b1 = (xp[1] - Y[j]) / (Y[j + 1] - Y[j]);
-  return (((1 - a1) * (1 - b1) * (double)a[pidx(d, pitch, i, j0, k)] +
-           a1 * (1 - b1) * (double)a[pidx(d, pitch, i + 1, j0, k)]) +
-          (1 - a1) * b1 * (double)a[pidx(d, pitch, i, j1, k)]) +
-         a1 * b1 * (double)a[pidx(d, pitch, i + 1, j1, k)];
+  fijk[0] = i; fijk[1] = j0; fijk[2] = j1; fijk[3] = k;
+  fw[0] = w1; fw[1] = w2;
 }
 
 // ---------------------------------------------------------------------------
@@ -1549,6 +1547,30 @@ __global__ void k_geom_mark(Dims d, int n, const int *ijk, const GeomPt *pts, in
   if (pts[p].mrk > 0 && pts[p].lev == ilp) fw[lidx(d.nx, d.ny, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2])] = 0;
 }
 
+constexpr int GEOM_NONE = 200, GEOM_NEED = 100;
+
+// the part of geom_decide that a waiting point settles on its own, one lane
+// per point: the recheck of a waiting normal-direction stencil and the flag
+// check of a waiting grid-line stencil; GEOM_NEED when the point goes on to
+// a grid-line or closest-point search (a warp's work).  geom_decide repeats
+// these steps with the same result.
+__device__ int geom_cheap(const Dims &d, const Axes &ax, const signed char *fw, int im, int jm, int km,
+                          const GeomPt &S, int ilp, int mimdif, int ndif) {
+  if (S.mrk == -1) {
+    int intrs = recheck_face(d, ax, fw, S.ext, S.dir);
+    if (im <= 2) intrs = 0;
+    if (intrs == 1) return 1;
+    if (intrs == -1 && ilp < NFLU && mimdif != 0) return -1;
+    return GEOM_NEED;
+  }
+  if (S.mrk == -2 && ndif < 3) {
+    const int g = fw[lidx(d.nx, d.ny, im + (int)S.ext[0], jm + (int)S.ext[1], km + (int)S.ext[2])] == 0 ? 1 : -1;
+    if (g == 1) return 2;
+    if (g == -1 && ilp < NFLU) return -2;
+  }
+  return GEOM_NEED;
+}
+
 // grid-wide barrier of a cooperative launch (every block resident): a
 // monotone arrival counter, zeroed before the launch; barrier g completes
 // when g * gridDim.x blocks have arrived.  The wait gives up after 2 s, or
@@ -1589,7 +1611,8 @@ __device__ bool grid_barrier(unsigned *count, unsigned g, int *err) {
 }
 
 // dependency loops 2..NFLU in one cooperative launch (no host round trip per
-// loop): each loop treats the waiting points (warps stride over the list),
+// loop): each loop treats the waiting points (a lane each for the rechecks,
+// the warp for the searches),
 // then, after a grid barrier, the points it made valid become fluid in the
 // working flags together with their y periodic images (the ghost planes were
 // refreshed whole after loop 1, so this equals refreshing them whole), and
@@ -1612,17 +1635,34 @@ __global__ void __launch_bounds__(GW * 32)
     prev = np;
     if (mimdif == 0) ndif++;
     if (np == 0) break;
-    for (int p = gw; p < n; p += nwarps) {
-      if (__ldcg(&pts[p].mrk) >= 0) continue;  // the whole warp
-      const int im = ijk[3 * p], jm = ijk[3 * p + 1], km = ijk[3 * p + 2];
-      if (lane < NNTR3D) inn_s[w][lane] = inn_all[(long long)NNTR3D * p + lane];
-      GeomPt &S = sp[w];
-      if (lane == 0) S = pts[p];
-      __syncwarp();
-      const int res = geom_decide(d, ax, v, nrm, fw, im, jm, km, inn_s[w], ilp, mimdif, ndif, S);
-      __syncwarp();
-      if (lane == 0) geom_finish(d, im, jm, km, res, ilp, S, pts + p, flag, inonvld, cnt + 2 * ilp);
-      __syncwarp();
+    // lane l of a warp takes point base + l; the points the cheap checks do
+    // not settle are then searched by the whole warp, one after the other
+    // (a warp keeps the same points in every loop)
+    for (int base = gw * 32; base < n; base += nwarps * 32) {
+      const int p = base + lane;
+      int res = GEOM_NONE;
+      GeomPt S;
+      if (p < n) {
+        S = pts[p];
+        if (S.mrk < 0) res = geom_cheap(d, ax, fw, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2], S, ilp, mimdif, ndif);
+      }
+      if (res != GEOM_NONE && res != GEOM_NEED)
+        geom_finish(d, ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2], res, ilp, S, pts + p, flag, inonvld,
+                    cnt + 2 * ilp);
+      unsigned need = __ballot_sync(0xffffffffu, res == GEOM_NEED);
+      while (need) {
+        const int q = base + __ffs(need) - 1;
+        need &= need - 1;
+        const int im = ijk[3 * q], jm = ijk[3 * q + 1], km = ijk[3 * q + 2];
+        if (lane < NNTR3D) inn_s[w][lane] = inn_all[(long long)NNTR3D * q + lane];
+        GeomPt &Sw = sp[w];
+        if (lane == 0) Sw = pts[q];
+        __syncwarp();
+        const int r = geom_decide(d, ax, v, nrm, fw, im, jm, km, inn_s[w], ilp, mimdif, ndif, Sw);
+        __syncwarp();
+        if (lane == 0) geom_finish(d, im, jm, km, r, ilp, Sw, pts + q, flag, inonvld, cnt + 2 * ilp);
+        __syncwarp();
+      }
     }
     if (!grid_barrier(bar, ++g, err)) return;
     for (int p = gt; p < n; p += nthr) {
@@ -1637,19 +1677,13 @@ __global__ void __launch_bounds__(GW * 32)
   }
 }
 
-// number of valid points per level
-__global__ void k_geom_rank_count(int n, const GeomPt *pts, int *levcnt) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n || pts[p].mrk <= 0) return;
-  atomicAdd(&levcnt[pts[p].lev - 1], 1);
-}
 
 // mtrx (src/devel.f:1159-1290), Cartesian, for the valid points, written at
 // their final position (level, then forcpts order): the extension point is
 // the grid point for mrk 2, the face point otherwise
 __global__ void k_geom_emit(Dims d, Axes ax, int n, const int *ijk, const GeomPt *pts, const int *order, int imn,
                             int *oijk, int *odd, int *olev, double *oxn, double *olu, int *oindx, int *omrk,
-                            int *odir, double *oxe) {
+                            int *odir, double *oxe, int *ofijk, double *ofw) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n || pts[p].mrk <= 0) return;
   const GeomPt s = pts[p];
@@ -1663,6 +1697,12 @@ __global__ void k_geom_emit(Dims d, Axes ax, int n, const int *ijk, const GeomPt
   omrk[o] = s.mrk;
   odir[o] = grid ? 0 : s.dir;
   oxe[3 * o] = grid ? 0. : s.ext[0]; oxe[3 * o + 1] = grid ? 0. : s.ext[1]; oxe[3 * o + 2] = grid ? 0. : s.ext[2];
+  if (grid) {
+    ofijk[4 * o] = ofijk[4 * o + 1] = ofijk[4 * o + 2] = ofijk[4 * o + 3] = 0;
+    ofw[2 * o] = ofw[2 * o + 1] = 0.;
+  } else {
+    face_weights(d, ax, s.ext, s.dir, ofijk + 4 * o, ofw + 2 * o);
+  }
   const double xnx = s.xn[0], xny = s.xn[1], xnz = s.xn[2];
   oxn[3 * o] = xnx; oxn[3 * o + 1] = xny; oxn[3 * o + 2] = xnz;
   const double xu = ax.x[im], yu = ax.y[jm], zu = ax.z[km];
@@ -1686,26 +1726,59 @@ __global__ void k_geom_emit(Dims d, Axes ax, int n, const int *ijk, const GeomPt
   for (int q = 0; q < 4; q++) olu[4 * o + q] = A[q];
 }
 
-// stable per-level ranks: order[p] = levstart[l] + (number of valid points
-// of level l before p), computed per level by block counts + scan
-__global__ void k_level_count(int n, const GeomPt *pts, int l, int *bcnt) {
+// The output order (rord_forcpts1): by level, then forcpts order.  Three
+// launches for all levels: per-block level counts, one scan over blocks and
+// levels, then each valid point's position = level start + the counts of its
+// level in earlier blocks + its rank among the same level in the block.
+__global__ void k_level_hist(int n, const GeomPt *pts, int *bcnt) {
+  __shared__ int h[NFLU];
+  for (int l = threadIdx.x; l < NFLU; l += blockDim.x) h[l] = 0;
+  __syncthreads();
   const int p = blockIdx.x * CB + threadIdx.x;
-  const bool on = p < n && pts[p].mrk > 0 && pts[p].lev == l;
-  const int c = __syncthreads_count(on ? 1 : 0);
-  if (threadIdx.x == 0) bcnt[blockIdx.x] = c;
+  if (p < n && pts[p].mrk > 0) atomicAdd(&h[pts[p].lev - 1], 1);
+  __syncthreads();
+  for (int l = threadIdx.x; l < NFLU; l += blockDim.x) bcnt[(long long)blockIdx.x * NFLU + l] = h[l];
 }
 
-__global__ void k_level_rank(int n, const GeomPt *pts, int l, int base, const int *boff, int *order) {
-  __shared__ int wsum[CB / 32];
-  const int p = blockIdx.x * CB + threadIdx.x;
-  const bool on = p < n && pts[p].mrk > 0 && pts[p].lev == l;
-  const unsigned bal = __ballot_sync(0xffffffffu, on);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) wsum[w] = __popc(bal);
+// one block: thread l scans level l over the blocks (boff exclusive, total);
+// then the level starts (start[l], start[NFLU] = number of valid points)
+__global__ void k_level_scan(int nb, const int *bcnt, int *boff, int *total, int *start) {
+  const int l = threadIdx.x;
+  if (l < NFLU) {
+    int sum = 0;
+    for (int b = 0; b < nb; b++) {
+      boff[(long long)b * NFLU + l] = sum;
+      sum += bcnt[(long long)b * NFLU + l];
+    }
+    total[l] = sum;
+  }
   __syncthreads();
-  int r = boff[blockIdx.x];
-  for (int q = 0; q < w; q++) r += wsum[q];
-  if (on) order[p] = base + r + __popc(bal & ((1u << lane) - 1u));
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int m = 0; m < NFLU; m++) {
+      start[m] = o;
+      o += total[m];
+    }
+    start[NFLU] = o;
+  }
+}
+
+__global__ void k_level_order(int n, const GeomPt *pts, const int *boff, const int *start, int *order) {
+  __shared__ int wc[CB / 32][NFLU];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int l = lane; l < NFLU; l += 32) wc[w][l] = 0;
+  const int p = blockIdx.x * CB + threadIdx.x;
+  const bool on = p < n && pts[p].mrk > 0;
+  const int l = on ? pts[p].lev - 1 : -1;
+  const unsigned same = __match_any_sync(0xffffffffu, l);
+  const int r = __popc(same & ((1u << lane) - 1u));
+  __syncwarp();
+  if (on && r == 0) wc[w][l] = __popc(same);
+  __syncthreads();
+  if (!on) return;
+  int o = start[l] + boff[(long long)blockIdx.x * NFLU + l] + r;
+  for (int q = 0; q < w; q++) o += wc[q][l];
+  order[p] = o;
 }
 
 // ---------------------------------------------------------------------------
@@ -1714,8 +1787,8 @@ __global__ void k_level_rank(int n, const GeomPt *pts, int l, int base, const in
 // point's (mrk 2) or the bilinear value on the fluid face (interp_cellface,
 // mrk 1 and 3); T storage with row pitch
 struct ForceArgs {
-  const int *ijk, *dd, *mrk, *dir, *indx;
-  const double *xe, *lu;
+  const int *ijk, *dd, *mrk, *dir, *indx, *fijk;
+  const double *lu, *fw;
 };
 
 template <class T>
@@ -1731,7 +1804,24 @@ __device__ __forceinline__ void force_point(const Dims &d, const Axes &ax, int p
       j1 = j1 - d.ny + 2;
     ae = (double)a[pidx(d, pitch, i1, j1, k1)];
   } else {
-    ae = interp_face<T>(d, ax, pitch, a, fa.xe + 3 * o, fa.dir[o]);
+    // interp_cellface's bilinear value on the face, from the cell and
+    // weights found at regeneration
+    const int *c = fa.fijk + 4 * o;
+    const int i = c[0], j0 = c[1], j1 = c[2], k = c[3], dr = fa.dir[o];
+    const double w1 = fa.fw[2 * o], w2 = fa.fw[2 * o + 1];
+    long long q00, q10, q01, q11;
+    if (dr == 1) {
+      q00 = pidx(d, pitch, i, j0, k); q10 = pidx(d, pitch, i, j1, k);
+      q01 = pidx(d, pitch, i, j0, k + 1); q11 = pidx(d, pitch, i, j1, k + 1);
+    } else if (dr == 2) {
+      q00 = pidx(d, pitch, i, j0, k); q10 = pidx(d, pitch, i + 1, j0, k);
+      q01 = pidx(d, pitch, i, j0, k + 1); q11 = pidx(d, pitch, i + 1, j0, k + 1);
+    } else {
+      q00 = pidx(d, pitch, i, j0, k); q10 = pidx(d, pitch, i + 1, j0, k);
+      q01 = pidx(d, pitch, i, j1, k); q11 = pidx(d, pitch, i + 1, j1, k);
+    }
+    ae = (((1 - w1) * (1 - w2) * (double)a[q00] + w1 * (1 - w2) * (double)a[q10]) + (1 - w1) * w2 * (double)a[q01]) +
+         w1 * w2 * (double)a[q11];
   }
   double b[2] = {b0, ae};
   lusolve2(fa.lu + 4 * o, fa.indx + 2 * o, b);
@@ -1955,7 +2045,7 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   if (n == 0) return EDDY_OK;
   // per-point search state, nearest-centroid lists, output positions
   int *inn = scratch(ctx, s, IbState::S_INN, (size_t)NNTR3D * n), *order = scratch(ctx, s, IbState::S_ORDER, n),
-      *cnt = scratch(ctx, s, IbState::S_CNT, 3 * (NFLU + 2) + 2);
+      *cnt = scratch(ctx, s, IbState::S_CNT, 2 * (NFLU + 2) + 2 * NFLU + 4);
   GeomPt *pts = reinterpret_cast<GeomPt *>(scratch_d(ctx, s, (sizeof(GeomPt) / sizeof(double)) * (size_t)n));
   if (!inn || !order || !cnt || !pts) return EDDY_ENOMEM;
   signed char *fw = s->work;
@@ -1968,9 +2058,9 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   // fluid in the working flags and their y ghost planes refreshed whole; then
   // loops 2..NFLU in one cooperative launch that keeps the loop control on
   // the device.  cnt: loop l's valid / waiting counts at [2 l], [2 l + 1];
-  // level counts from LC; the barrier counter last.
+  // the barrier counter at LC; then the level totals and starts.
   constexpr int LC = 2 * (NFLU + 2);
-  EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (LC + NFLU + 3), st));
+  EDDY_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (LC + 1), st));
   k_geom_pass<<<(unsigned)((n + GW - 1) / GW), GW * 32, 0, st>>>(d, ax, n, s->pts, s->v, s->c, s->n, s->b3,
                                                                   s->b3.start, s->b3.items, fw, flag, inonvld, pts, inn,
                                                                   cnt + 2);
@@ -1987,7 +2077,8 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
       s->coop_blocks_per_sm = std::max(1, per);
       s->nsm = nsm;
     }
-    const int grid = (int)std::max(1LL, std::min((long long)s->coop_blocks_per_sm * s->nsm, (long long)(n + GW - 1) / GW));
+    const int grid =
+        (int)std::max(1LL, std::min((long long)s->coop_blocks_per_sm * s->nsm, (long long)(n + 32 * GW - 1) / (32 * GW)));
     const Dims dd = d;
     const Axes axx = ax;
     int nn = n;
@@ -1997,7 +2088,7 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
     GeomPt *ptp = pts;
     const int *innp = inn;
     int *cntp = cnt;
-    unsigned *bar = reinterpret_cast<unsigned *>(cnt + LC + NFLU + 2);
+    unsigned *bar = reinterpret_cast<unsigned *>(cnt + LC);
     int *err = ctx->err_flag;
     void *args[] = {(void *)&dd, (void *)&axx, (void *)&nn, (void *)&ijk, (void *)&vv, (void *)&nrm, (void *)&fwp,
                     (void *)&flp, (void *)&inv, (void *)&ptp, (void *)&innp, (void *)&cntp, (void *)&bar,
@@ -2005,11 +2096,20 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
     EDDY_CUDA(cudaLaunchCooperativeKernel((const void *)k_geom_loops, dim3(grid), dim3(GW * 32), args, 0, st));
     EDDY_LAUNCHED(ctx);
   }
-  // level sizes -> offsets (the one read-back of the loops)
-  k_geom_rank_count<<<nblk(n), 256, 0, st>>>(n, pts, cnt + LC + 1);
+  // level sizes and output positions (the one read-back of the loops)
+  const int nbl = (n + CB - 1) / CB;
+  int *lcnt = scratch(ctx, s, IbState::S_LCNT, (size_t)nbl * NFLU),
+      *loff = scratch(ctx, s, IbState::S_LOFF, (size_t)nbl * NFLU);
+  if (!lcnt || !loff) return EDDY_ENOMEM;
+  int *tot = cnt + LC + 1, *lstart = cnt + LC + 1 + NFLU;  // NFLU totals, NFLU + 1 starts
+  k_level_hist<<<nbl, CB, 0, st>>>(n, pts, lcnt);
+  EDDY_LAUNCHED(ctx);
+  k_level_scan<<<1, 32, 0, st>>>(nbl, lcnt, loff, tot, lstart);
+  EDDY_LAUNCHED(ctx);
+  k_level_order<<<nbl, CB, 0, st>>>(n, pts, loff, lstart, order);
   EDDY_LAUNCHED(ctx);
   std::vector<int> lc(NFLU + 2, 0);
-  EDDY_CUDA(cudaMemcpyAsync(lc.data(), cnt + LC + 1, sizeof(int) * (NFLU + 1), cudaMemcpyDeviceToHost, st));
+  EDDY_CUDA(cudaMemcpyAsync(lc.data(), tot, sizeof(int) * NFLU, cudaMemcpyDeviceToHost, st));
   EDDY_CUDA(cudaStreamSynchronize(st));
   int nlev = 0;
   for (int l = 0; l < NFLU; l++)
@@ -2020,10 +2120,10 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   S.n = nv;
   S.nlev = nlev;
   if (nv > S.cap) {
-    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu, S.mrk, S.dir, S.xe};
+    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu, S.mrk, S.dir, S.xe, S.fijk, S.fw};
     for (void *p : ptrs) if (p) cudaFree(p);
-    S.ijk = S.dijk = S.lev = S.indx = S.mrk = S.dir = nullptr;
-    S.xn = S.lu = S.xe = nullptr;
+    S.ijk = S.dijk = S.lev = S.indx = S.mrk = S.dir = S.fijk = nullptr;
+    S.xn = S.lu = S.xe = S.fw = nullptr;
     S.cap = 0;
     const size_t c = grown((size_t)nv);
     EDDY_CUDA(cudaMalloc(&S.ijk, sizeof(int) * 3 * c));
@@ -2035,25 +2135,13 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
     EDDY_CUDA(cudaMalloc(&S.xn, sizeof(double) * 3 * c));
     EDDY_CUDA(cudaMalloc(&S.lu, sizeof(double) * 4 * c));
     EDDY_CUDA(cudaMalloc(&S.xe, sizeof(double) * 3 * c));
+    EDDY_CUDA(cudaMalloc(&S.fijk, sizeof(int) * 4 * c));
+    EDDY_CUDA(cudaMalloc(&S.fw, sizeof(double) * 2 * c));
     S.cap = (int)c;
   }
   if (nv > 0) {
-    const int nbl = (n + CB - 1) / CB;
-    int *bcnt = scratch(ctx, s, IbState::S_BCNT, nbl), *boff = scratch(ctx, s, IbState::S_BOFF, nbl + 1),
-        *cur = scratch(ctx, s, IbState::S_CUR, nbl);
-    if (!bcnt || !boff || !cur) return EDDY_ENOMEM;
-    for (int l = 1; l <= nlev; l++) {
-      k_level_count<<<nbl, CB, 0, st>>>(n, pts, l, bcnt);
-      EDDY_LAUNCHED(ctx);
-      int *bsum = scratch(ctx, s, IbState::S_BSUM, (nbl + SB - 1) / SB + 1);
-      if (!bsum) return EDDY_ENOMEM;
-      int rc0 = scan_launch(ctx, nbl, bcnt, boff, cur, bsum);
-      if (rc0) return rc0;
-      k_level_rank<<<nbl, CB, 0, st>>>(n, pts, l, S.lev_start[l - 1], boff, order);
-      EDDY_LAUNCHED(ctx);
-    }
     k_geom_emit<<<nblk(n), 256, 0, st>>>(d, ax, n, s->pts, pts, order, imn, S.ijk, S.dijk, S.lev, S.xn, S.lu,
-                                         S.indx, S.mrk, S.dir, S.xe);
+                                         S.indx, S.mrk, S.dir, S.xe, S.fijk, S.fw);
     EDDY_LAUNCHED(ctx);
   }
   return EDDY_OK;
@@ -2074,7 +2162,7 @@ int ib_release(eddy_ctx *ctx) {
   for (int q = 0; q < 5; q++) if (s->flag[q]) cudaFree(s->flag[q]);
   if (s->flag3b) cudaFree(s->flag3b);
   for (StencilSet &S : s->set) {
-    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu, S.mrk, S.dir, S.xe};
+    void *ptrs[] = {S.ijk, S.dijk, S.lev, S.indx, S.xn, S.lu, S.mrk, S.dir, S.xe, S.fijk, S.fw};
     for (void *q : ptrs) if (q) cudaFree(q);
   }
   if (s->hcnt) cudaFreeHost(s->hcnt);
@@ -2262,7 +2350,7 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
   // last level leaves the same state.  Large levels get a grid each; runs of
   // small ones go to one CTA that steps through them.
   const Axes ax = axes_of(ctx, q);
-  const ForceArgs fa{S.ijk, S.dijk, S.mrk, S.dir, S.indx, S.xe, S.lu};
+  const ForceArgs fa{S.ijk, S.dijk, S.mrk, S.dir, S.indx, S.fijk, S.lu, S.fw};
   constexpr int BIG = 4096;
   LevOffsets ls{};
   for (int l = 0; l <= S.nlev && l < NFLU + 2; l++) ls.v[l] = S.lev_start[l];

@@ -142,6 +142,26 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def yface_velocity(u: np.ndarray, mode: int) -> np.ndarray:
+    """yface_velocity (src/Planes.f:481-543) of an (NX,NY,NZ) field, 0-based
+    arrays: mode 1 the average over (i-1, i) x (j, j+1) for i = 2..NX-1, j =
+    1..NY-1, k = 2..NZ-1 (1-based), 3 over (k-1, k) x (j, j+1), 4 over (j,
+    j+1) for j = 1..NY-1; 0 and 2 the field itself; zero elsewhere."""
+    u = np.asarray(u, dtype=np.float64)
+    out = np.zeros_like(u)
+    if mode in (0, 2):
+        return u.copy()
+    if mode == 1:
+        out[1:-1, :-1, 1:-1] = 0.250 * (((u[1:-1, :-1, 1:-1] + u[:-2, :-1, 1:-1]) + u[1:-1, 1:, 1:-1])
+                                        + u[:-2, 1:, 1:-1])
+    elif mode == 3:
+        out[1:-1, :-1, 1:-1] = 0.250 * (((u[1:-1, :-1, 1:-1] + u[1:-1, :-1, :-2]) + u[1:-1, 1:, 1:-1])
+                                        + u[1:-1, 1:, :-2])
+    elif mode == 4:
+        out[:, :-1, :] = 0.50 * (u[:, :-1, :] + u[:, 1:, :])
+    return out
+
+
 def rfftf(x: np.ndarray) -> np.ndarray:
     r = np.ascontiguousarray(x, dtype=np.float64).copy()
     lib().eo_rfftf(len(r), _ptr(r))
