@@ -227,7 +227,7 @@ ALG_BYTES_MIXED = {
     "div_fft_fwd": 3 * 4 + 8 + 4,  # R u*,v*,w* FP32  W d FP64, spectrum FP32
     "refine_residual": 8 + 8 + 4,  # R phi, d FP64  W spectrum FP32
     "transform_fwd": 2 * 4,
-    "z_line_solve": 2 * 4,
+    "z_line_solve": 5 * 4,     # R rhs, W eliminated; R eliminated, c' table, W solution (FP32)
     "transform_bwd": 2 * 4,
     "fft_bwd": 2 * 4,
     "correct": 3 * 4 + 8 + 3 * 8 + 3 * 4,  # R u*,v*,w* FP32, dp  W u,v,w FP64 + FP32 copies

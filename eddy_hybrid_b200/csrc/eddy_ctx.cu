@@ -813,13 +813,10 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
       if (rc) return rc;
     }
     // within one call the next step's move (same dt) and regeneration run on
-    // the second stream during this step's learned closure (whose MMA chain
-    // leaves SMs idle; the dynamic procedure's long kernels would only be
-    // slowed by it); they only need this step's forcing to be done (the
-    // event), and tvinterior below keeps reading the current tv flag
-    // (double-buffered)
-    const bool prefetch = ctx->ib && !ib_every_substep(ctx) && n + 1 < nsteps && ctx->prm.isgs != 0 &&
-                          ctx->prm.closure == 1;
+    // the second stream during this step's eddy viscosity update; they only
+    // need this step's forcing to be done (the event), and tvinterior below
+    // keeps reading the current tv flag (double-buffered)
+    const bool prefetch = ctx->ib && !ib_every_substep(ctx) && n + 1 < nsteps && ctx->prm.isgs != 0;
     if (prefetch) {
       ib_join(ctx);
       EDDY_CUDA(cudaEventRecord(ctx->ib_ev[0], ctx->stream));

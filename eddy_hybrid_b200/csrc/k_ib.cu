@@ -1740,24 +1740,35 @@ __global__ void k_level_hist(int n, const GeomPt *pts, int *bcnt) {
   for (int l = threadIdx.x; l < NFLU; l += blockDim.x) bcnt[(long long)blockIdx.x * NFLU + l] = h[l];
 }
 
-// one block: thread l scans level l over the blocks (boff exclusive, total);
-// then the level starts (start[l], start[NFLU] = number of valid points)
-__global__ void k_level_scan(int nb, const int *bcnt, int *boff, int *total, int *start) {
-  const int l = threadIdx.x;
-  if (l < NFLU) {
-    int sum = 0;
-    for (int b = 0; b < nb; b++) {
-      boff[(long long)b * NFLU + l] = sum;
-      sum += bcnt[(long long)b * NFLU + l];
+// one block, warp l scans level l over the blocks 32 at a time (boff
+// exclusive, total); then the level starts (start[l], start[NFLU] = number
+// of valid points)
+__global__ void __launch_bounds__(32 * NFLU) k_level_scan(int nb, const int *bcnt, int *boff, int *total,
+                                                          int *start) {
+  __shared__ int tot_s[NFLU];
+  const int l = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int run = 0;
+  for (int b0 = 0; b0 < nb; b0 += 32) {
+    const int b = b0 + lane;
+    const int v = b < nb ? bcnt[(long long)b * NFLU + l] : 0;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    total[l] = sum;
+    if (b < nb) boff[(long long)b * NFLU + l] = run + x - v;
+    run += __shfl_sync(0xffffffffu, x, 31);
+  }
+  if (lane == 0) {
+    total[l] = run;
+    tot_s[l] = run;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     int o = 0;
     for (int m = 0; m < NFLU; m++) {
       start[m] = o;
-      o += total[m];
+      o += tot_s[m];
     }
     start[NFLU] = o;
   }
@@ -2104,7 +2115,7 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   int *tot = cnt + LC + 1, *lstart = cnt + LC + 1 + NFLU;  // NFLU totals, NFLU + 1 starts
   k_level_hist<<<nbl, CB, 0, st>>>(n, pts, lcnt);
   EDDY_LAUNCHED(ctx);
-  k_level_scan<<<1, 32, 0, st>>>(nbl, lcnt, loff, tot, lstart);
+  k_level_scan<<<1, 32 * NFLU, 0, st>>>(nbl, lcnt, loff, tot, lstart);
   EDDY_LAUNCHED(ctx);
   k_level_order<<<nbl, CB, 0, st>>>(n, pts, loff, lstart, order);
   EDDY_LAUNCHED(ctx);

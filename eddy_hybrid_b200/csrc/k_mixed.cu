@@ -68,6 +68,20 @@ __global__ void k_to32(Dims d, int px, const double *__restrict__ a, float *__re
   b[pidx(d, px, i, j, k)] = (float)a[t];
 }
 
+// one FP64 array to two FP32 copies (read once)
+__global__ void k_to32x2(Dims d, int px, const double *__restrict__ a, float *__restrict__ b,
+                         float *__restrict__ c) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.ncell) return;
+  int i = 1 + (int)(t % d.nx);
+  long long r = t / d.nx;
+  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
+  const float v = (float)a[t];
+  const long long q = pidx(d, px, i, j, k);
+  b[q] = v;
+  c[q] = v;
+}
+
 __global__ void k_to64(Dims d, int px, const float *__restrict__ b, double *__restrict__ a) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= d.ncell) return;
@@ -969,9 +983,15 @@ int mixed_to64(eddy_ctx *ctx, int field) {
 int mixed_after_sgs(eddy_ctx *ctx) {
   MixedState *x = ms(ctx);
   ProfScope ps(ctx, PROF_CONVERT);
-  int rc = to32(ctx, ctx->f[EDDY_TV], x->tv);
-  if (rc) return rc;
-  return to32(ctx, ctx->prm.closure == 1 ? ctx->kappa : ctx->f[EDDY_TV], x->kv);
+  if (ctx->prm.closure == 1) {
+    int rc = to32(ctx, ctx->f[EDDY_TV], x->tv);
+    if (rc) return rc;
+    return to32(ctx, ctx->kappa, x->kv);
+  }
+  // the dynamic model's diffusivity is its viscosity: both copies in one pass
+  k_to32x2<<<nblk(ctx->d.ncell), 256, 0, ctx->stream>>>(ctx->d, x->px, ctx->f[EDDY_TV], x->tv, x->kv);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
 }
 
 int mixed_turvis(eddy_ctx *ctx) {
