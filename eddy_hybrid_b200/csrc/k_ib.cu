@@ -749,10 +749,11 @@ __global__ void k_yper_i8(Dims d, signed char *a, int i0, int i1, int k0, int k1
 
 // taguo (src/devel.f:8-110) over the body box: 1 interior, -1 forcing
 __global__ void k_taguo(Dims d, Box6 L, int itagy, const signed char *f, signed char *fo) {
-  const int ni = L.imax - L.imin + 1, nj = L.jmax - L.jmin + 1, nk = L.kmax - L.kmin + 1;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)ni * nj * nk) return;
-  const int i = L.imin + (int)(t % ni), j = L.jmin + (int)((t / ni) % nj), k = L.kmin + (int)(t / ((long long)ni * nj));
+  // blockIdx.y is the plane k of the box; 32-bit arithmetic inside it
+  const int ni = L.imax - L.imin + 1, nj = L.jmax - L.jmin + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ni * nj) return;
+  const int j = L.jmin + t / ni, i = L.imin + (t - (j - L.jmin) * ni), k = L.kmin + blockIdx.y;
   const long long q = lidx(d.nx, d.ny, i, j, k);
   const int c = f[q];
   signed char o = (c == -1) ? 1 : 0;
@@ -1885,10 +1886,11 @@ __global__ void k_yper_field(Dims d, int pitch, T *a, float *mirror, int mpitch)
 template <class T>
 __global__ void k_interior(Dims d, int pitch, Box6 L, const signed char *flag, T *a, double value, float *mirror,
                            int mpitch) {
-  const int ni = L.imax - L.imin + 1, nj = L.jmax - L.jmin + 1, nk = L.kmax - L.kmin + 1;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)ni * nj * nk) return;
-  const int i = L.imin + (int)(t % ni), j = L.jmin + (int)((t / ni) % nj), k = L.kmin + (int)(t / ((long long)ni * nj));
+  // blockIdx.y is the plane k of the box; 32-bit arithmetic inside it
+  const int ni = L.imax - L.imin + 1, nj = L.jmax - L.jmin + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ni * nj) return;
+  const int j = L.jmin + t / ni, i = L.imin + (t - (j - L.jmin) * ni), k = L.kmin + blockIdx.y;
   if (flag[lidx(d.nx, d.ny, i, j, k)] == 1) {
     a[pidx(d, pitch, i, j, k)] = (T)value;
     if (mirror) mirror[pidx(d, mpitch, i, j, k)] = (float)value;
@@ -1896,6 +1898,10 @@ __global__ void k_interior(Dims d, int pitch, Box6 L, const signed char *flag, T
 }
 
 inline unsigned nblk(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+// the body box as (planes of 256-thread blocks) x (its k planes)
+inline dim3 box_grid(const Box6 &L) {
+  return dim3((unsigned)(((L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) + 255) / 256), (unsigned)(L.kmax - L.kmin + 1));
+}
 
 // exclusive scan with start[n] = total (bsum: scratch of >= ceil(n/SB) ints)
 int scan_launch(eddy_ctx *ctx, int n, const int *cnt, int *start, int *cursor, int *bsum) {
@@ -2391,7 +2397,7 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
   const Box6 L = s->lim;
   const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
   if (nbx > 0) {
-    k_interior<T><<<nblk(nbx), 256, 0, st>>>(d, pitch, L, s->flag[fq], a, interior, mirror, mpitch);
+    k_interior<T><<<box_grid(L), 256, 0, st>>>(d, pitch, L, s->flag[fq], a, interior, mirror, mpitch);
     EDDY_LAUNCHED(ctx);
   }
   k_yper_field<T><<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, pitch, a, mirror, mpitch);
@@ -2431,7 +2437,7 @@ int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror, i
   const Box6 L = s->lim;
   const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
   if (nbx > 0) {
-    k_interior<double><<<nblk(nbx), 256, 0, ctx->stream>>>(d, d.nx, L, s->flag[fq], a, value, mirror, mpitch);
+    k_interior<double><<<box_grid(L), 256, 0, ctx->stream>>>(d, d.nx, L, s->flag[fq], a, value, mirror, mpitch);
     EDDY_LAUNCHED(ctx);
   }
   k_yper_field<double><<<nblk((long long)d.nx * d.nz), 256, 0, ctx->stream>>>(d, d.nx, a, mirror, mpitch);

@@ -58,37 +58,45 @@ struct MixedState {
 MixedState *ms(eddy_ctx *ctx) { return static_cast<MixedState *>(ctx->mixed); }
 
 // ---------------------------------------------------------------------------
-// precision copies over the whole (NX,NY,NZ) array
+// precision copies over the whole (NX,NY,NZ) array: blockIdx.y is the plane k,
+// x runs over the NX*NY cells of the plane (32-bit index arithmetic)
+struct PlaneCell {
+  int i, j, k;
+  long long t;  // the FP64 (unpadded) index
+};
+
+__device__ __forceinline__ bool plane_cell(const Dims &d, PlaneCell &c) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n2 = d.nx * d.ny;
+  if (q >= n2) return false;
+  c.k = 1 + blockIdx.y;
+  c.j = 1 + q / d.nx;
+  c.i = 1 + (q - (c.j - 1) * d.nx);
+  c.t = (long long)blockIdx.y * n2 + q;
+  return true;
+}
+
 __global__ void k_to32(Dims d, int px, const double *__restrict__ a, float *__restrict__ b) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.ncell) return;
-  int i = 1 + (int)(t % d.nx);
-  long long r = t / d.nx;
-  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
-  b[pidx(d, px, i, j, k)] = (float)a[t];
+  PlaneCell c;
+  if (!plane_cell(d, c)) return;
+  b[pidx(d, px, c.i, c.j, c.k)] = (float)a[c.t];
 }
 
 // one FP64 array to two FP32 copies (read once)
 __global__ void k_to32x2(Dims d, int px, const double *__restrict__ a, float *__restrict__ b,
-                         float *__restrict__ c) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.ncell) return;
-  int i = 1 + (int)(t % d.nx);
-  long long r = t / d.nx;
-  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
-  const float v = (float)a[t];
-  const long long q = pidx(d, px, i, j, k);
+                         float *__restrict__ cc) {
+  PlaneCell c;
+  if (!plane_cell(d, c)) return;
+  const float v = (float)a[c.t];
+  const long long q = pidx(d, px, c.i, c.j, c.k);
   b[q] = v;
-  c[q] = v;
+  cc[q] = v;
 }
 
 __global__ void k_to64(Dims d, int px, const float *__restrict__ b, double *__restrict__ a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.ncell) return;
-  int i = 1 + (int)(t % d.nx);
-  long long r = t / d.nx;
-  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
-  a[t] = (double)b[pidx(d, px, i, j, k)];
+  PlaneCell c;
+  if (!plane_cell(d, c)) return;
+  a[c.t] = (double)b[pidx(d, px, c.i, c.j, c.k)];
 }
 
 // ---------------------------------------------------------------------------
@@ -574,14 +582,11 @@ __global__ void k_pref_m(Dims d, const double *p, const double *dp, double *out)
 __global__ void __launch_bounds__(256)
     k_pupdate_m(Dims d, int px, double *__restrict__ p, const double *__restrict__ dp,
                 const double *__restrict__ pref, float *__restrict__ p32) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.ncell) return;
-  double v = (p[t] + dp[t]) - pref[0];
-  p[t] = v;
-  int i = 1 + (int)(t % d.nx);
-  long long r = t / d.nx;
-  int j = 1 + (int)(r % d.ny), k = 1 + (int)(r / d.ny);
-  p32[pidx(d, px, i, j, k)] = (float)v;
+  PlaneCell c;
+  if (!plane_cell(d, c)) return;
+  const double v = (p[c.t] + dp[c.t]) - pref[0];
+  p[c.t] = v;
+  p32[pidx(d, px, c.i, c.j, c.k)] = (float)v;
 }
 
 __device__ __forceinline__ int map_axis(int a, int n, int lo, int hi, int periodic, int active) {
@@ -716,15 +721,16 @@ const CUtensorMap *tmap32(eddy_ctx *ctx, const float *ptr, int bx, int by) {
 constexpr int NPART = 296;
 
 inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
+inline dim3 plane_grid(const Dims &d) { return dim3((unsigned)((d.nx * d.ny + 255) / 256), (unsigned)d.nz); }
 
 int to32(eddy_ctx *ctx, const double *a, float *b) {
-  k_to32<<<nblk(ctx->d.ncell), 256, 0, ctx->stream>>>(ctx->d, ms(ctx)->px, a, b);
+  k_to32<<<plane_grid(ctx->d), 256, 0, ctx->stream>>>(ctx->d, ms(ctx)->px, a, b);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
 
 int to64(eddy_ctx *ctx, const float *b, double *a) {
-  k_to64<<<nblk(ctx->d.ncell), 256, 0, ctx->stream>>>(ctx->d, ms(ctx)->px, b, a);
+  k_to64<<<plane_grid(ctx->d), 256, 0, ctx->stream>>>(ctx->d, ms(ctx)->px, b, a);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
@@ -989,7 +995,7 @@ int mixed_after_sgs(eddy_ctx *ctx) {
     return to32(ctx, ctx->kappa, x->kv);
   }
   // the dynamic model's diffusivity is its viscosity: both copies in one pass
-  k_to32x2<<<nblk(ctx->d.ncell), 256, 0, ctx->stream>>>(ctx->d, x->px, ctx->f[EDDY_TV], x->tv, x->kv);
+  k_to32x2<<<plane_grid(ctx->d), 256, 0, ctx->stream>>>(ctx->d, x->px, ctx->f[EDDY_TV], x->tv, x->kv);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
@@ -1104,7 +1110,7 @@ int mixed_substep(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
     ProfScope ps(ctx, PROF_PUPDATE);
     k_pref_m<<<1, 32, 0, ctx->stream>>>(d, f[EDDY_P], f[EDDY_DP], ctx->scal);
     EDDY_LAUNCHED(ctx);
-    k_pupdate_m<<<nblk(d.ncell), 256, 0, ctx->stream>>>(d, px, f[EDDY_P], f[EDDY_DP], ctx->scal, x->p);
+    k_pupdate_m<<<plane_grid(d), 256, 0, ctx->stream>>>(d, px, f[EDDY_P], f[EDDY_DP], ctx->scal, x->p);
     EDDY_LAUNCHED(ctx);
     if (ctx->ib && (rc = ib_force(ctx, 3, 4, f[EDDY_P], 0.0, 0.0, x->p, px))) return rc;
     long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;

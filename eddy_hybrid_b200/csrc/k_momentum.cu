@@ -159,9 +159,12 @@ __global__ void k_pref(Dims d, const double *p, const double *dp, double *out, d
 
 __global__ void __launch_bounds__(256)
     k_pupdate(Dims d, double *p, const double *dp, const double *pref, double cimp) {
-  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= d.ncell) return;
-  const int i = 1 + (int)(q % d.nx), j = 1 + (int)((q / d.nx) % d.ny), k = 1 + (int)(q / ((long long)d.nx * d.ny));
+  // blockIdx.y is the plane k; 32-bit index arithmetic inside the plane
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n2 = d.nx * d.ny;
+  if (t >= n2) return;
+  const int k = 1 + blockIdx.y, j = 1 + t / d.nx, i = 1 + (t - (j - 1) * d.nx);
+  const long long q = (long long)blockIdx.y * n2 + t;
   p[q] = p_plus_dp(d, p, dp, q, i, j, k, cimp) - pref[0];
 }
 
@@ -271,7 +274,8 @@ int launch_pressure_update(eddy_ctx *ctx) {
                                          : 0.0;
   k_pref<<<1, 1, 0, ctx->stream>>>(d, p, dp, ctx->scal, cimp);
   EDDY_LAUNCHED(ctx);
-  k_pupdate<<<(unsigned)((d.ncell + 255) / 256), 256, 0, ctx->stream>>>(d, p, dp, ctx->scal, cimp);
+  k_pupdate<<<dim3((unsigned)((d.nx * d.ny + 255) / 256), (unsigned)d.nz), 256, 0, ctx->stream>>>(d, p, dp, ctx->scal,
+                                                                                                   cimp);
   EDDY_LAUNCHED(ctx);
   // immersed body: correctpres_mod2 + presinterior (src/Eddy6.f:2881-2897)
   if (ctx->ib) {
