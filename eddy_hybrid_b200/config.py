@@ -75,6 +75,7 @@ class Workload:
     seed: int = 42
     noise: float = 1e-3
     isgs: int = 2
+    ischm: int = 3          # 3 RK3, 1 AB2 (src/inpall.f:218-235)
     idens: int = 1
     itype: tuple = ITYPE_WAKE
     sphere: bool = True
@@ -105,7 +106,7 @@ class Workload:
     def params(self) -> dict:
         """Solver parameters (names as the reference's COMMON blocks)."""
         return dict(
-            nx=self.nx, ny=self.ny, nz=self.nz, itype=self.itype, ischm=3,
+            nx=self.nx, ny=self.ny, nz=self.nz, itype=self.itype, ischm=self.ischm,
             isgs=self.isgs, idens=self.idens, ru1=1.0 / self.re, prn=self.pr,
             # Fr = N D / U with D = U = 1 and N^2 = -grav*denP1, denP1 = -1
             denP1=-1.0, grav=self.fr ** 2, dpdx=0.0, dpdy=0.0, dpdz=0.0,

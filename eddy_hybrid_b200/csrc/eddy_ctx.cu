@@ -318,6 +318,8 @@ const CUtensorMap *ctx_tensor_map(eddy_ctx *ctx, const double *ptr, int bx, int 
   return &ctx->tmaps.back().map;
 }
 
+thread_local cudaStream_t tl_stream = nullptr;
+
 extern "C" {
 
 int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, double ymin, double ymax,
@@ -411,6 +413,7 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
 
 int eddy_destroy(eddy_ctx *ctx) {
   if (!ctx) return EDDY_OK;
+  if (ctx->ib_thread.joinable()) ctx->ib_thread.join();
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_all(ctx);
   delete ctx;
@@ -746,7 +749,7 @@ static int substep_core(eddy_ctx *ctx, int is, double dt) {
     if (is == 0 && ctx->ib_prefetched) {
       ctx->ib_prefetched = 0;  // queued at the end of the previous step (eddy_step)
     } else {
-      ib_join(ctx);
+      if ((rc = ib_join(ctx))) return rc;
       EDDY_CUDA(cudaEventRecord(ctx->ib_ev[0], ctx->stream));
       ctx->ib_move_dt = ib_every_substep(ctx) ? alfxdt : dt;
     }
@@ -818,7 +821,8 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
     // keeps reading the current tv flag (double-buffered)
     const bool prefetch = ctx->ib && !ib_every_substep(ctx) && n + 1 < nsteps && ctx->prm.isgs != 0;
     if (prefetch) {
-      ib_join(ctx);
+      int rc = ib_join(ctx);
+      if (rc) return rc;
       EDDY_CUDA(cudaEventRecord(ctx->ib_ev[0], ctx->stream));
     }
     if (ctx->prm.isgs != 0) {
@@ -843,8 +847,7 @@ int eddy_step(eddy_ctx *ctx, double dt, int nsteps) {
     if (prefetch) {
       int rc;
       if ((rc = ib_swap_tv_flag(ctx))) return rc;
-      ctx->ib_move_dt = dt;
-      if ((rc = ib_overlap_regen(ctx))) return rc;
+      if ((rc = ib_prefetch_async(ctx, dt))) return rc;
       ctx->ib_prefetched = 1;
     }
     // TIME after the step (the RK3 / AB2 alphas sum to one), then the time
@@ -936,7 +939,10 @@ int eddy_profile_enable(eddy_ctx *ctx, unsigned mask) {
 
 int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
+  if (int rcj = ib_join(ctx)) return rcj;
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ctx->ib) EDDY_CUDA(cudaStreamSynchronize(ctx->ib_stream));
+  std::lock_guard<std::mutex> lk(ctx->prof_mu);
   for (ProfEvent &e : ctx->prof_ev) {
     float t = 0.f;
     EDDY_CUDA(cudaEventElapsedTime(&t, e.a, e.b));
@@ -954,6 +960,7 @@ int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts) {
 
 int eddy_sync(eddy_ctx *ctx) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
+  if (int rcj = ib_join(ctx)) return rcj;
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
   int e = 0;
   EDDY_CUDA(cudaMemcpy(&e, ctx->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
@@ -971,7 +978,7 @@ int eddy_last_error(eddy_ctx *ctx, char *buf, int len) {
   return EDDY_OK;
 }
 
-int64_t eddy_launch_count(eddy_ctx *ctx) { return ctx ? ctx->launches : -1; }
+int64_t eddy_launch_count(eddy_ctx *ctx) { return ctx ? ctx->launches.load() : -1; }
 
 void *eddy_stream(eddy_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 

@@ -4,6 +4,10 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
+#include <thread>
+
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -106,7 +110,11 @@ struct eddy_ctx {
   double *scal = nullptr;  // device scalars: [0] pref [1] qin1 [2] qin2 [3] dpm [4] maxdiv; [32, 328) flux partials
   PoissonPlan pp{};
   std::string err;
-  int64_t launches = 0;
+  std::atomic<int64_t> launches{0};
+  // the prefetched immersed-body regeneration runs its host side on a helper
+  // thread (its launches go to ib_stream); joined before the body is used
+  std::thread ib_thread;
+  int ib_thread_rc = 0;
   double dely = 0., delysq = 0.;
   double alfxdt_last = 0.;  // alfxdt of the last CORRECT (the IMPLY pressure correction)
   // hybrid inflow sequence (device-resident): feed_n planes [n][4][NX*NY] of
@@ -133,34 +141,52 @@ struct eddy_ctx {
   unsigned prof_mask = 0;
   std::vector<ProfEvent> prof_ev;   // recorded in this window
   std::vector<ProfEvent> prof_pool; // reusable events
+  std::mutex prof_mu;               // the helper thread records events too
   double prof_ms[PROF_NCAT] = {};
   int *err_flag = nullptr;            // device word set by kernels whose bounded waits expire
   std::vector<TmaEntry> tmaps;        // cached tensor maps per (field pointer, box)
   long long prof_n[PROF_NCAT] = {};
 };
 
+// The stream the calling host thread issues work to: the context's main
+// stream, or the one a scope set (the immersed-body regeneration's).
+extern thread_local cudaStream_t tl_stream;
+inline cudaStream_t cur_stream(const eddy_ctx *ctx) { return tl_stream ? tl_stream : ctx->stream; }
+struct StreamScope {
+  cudaStream_t prev;
+  explicit StreamScope(cudaStream_t s) : prev(tl_stream) { tl_stream = s; }
+  ~StreamScope() { tl_stream = prev; }
+};
+
 // RAII scope: records a start event now and a stop event at scope exit when
-// the category is enabled.
+// the category is enabled (on the calling thread's stream).
 struct ProfScope {
   eddy_ctx *c;
   int cat;
   bool on;
+  cudaStream_t st;
   ProfEvent ev{};
-  ProfScope(eddy_ctx *ctx, int category) : c(ctx), cat(category), on((ctx->prof_mask >> category) & 1u) {
+  ProfScope(eddy_ctx *ctx, int category)
+      : c(ctx), cat(category), on((ctx->prof_mask >> category) & 1u), st(cur_stream(ctx)) {
     if (!on) return;
-    if (!c->prof_pool.empty()) {
-      ev = c->prof_pool.back();
-      c->prof_pool.pop_back();
-    } else {
+    {
+      std::lock_guard<std::mutex> lk(c->prof_mu);
+      if (!c->prof_pool.empty()) {
+        ev = c->prof_pool.back();
+        c->prof_pool.pop_back();
+      }
+    }
+    if (!ev.a) {
       cudaEventCreate(&ev.a);
       cudaEventCreate(&ev.b);
     }
     ev.cat = cat;
-    cudaEventRecord(ev.a, c->stream);
+    cudaEventRecord(ev.a, st);
   }
   ~ProfScope() {
     if (!on) return;
-    cudaEventRecord(ev.b, c->stream);
+    cudaEventRecord(ev.b, st);
+    std::lock_guard<std::mutex> lk(c->prof_mu);
     c->prof_ev.push_back(ev);
   }
 };
@@ -245,7 +271,8 @@ int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror = 
 // ctx->ib_stream after ctx->ib_ev[0], overlapping work queued on the main
 // stream since; ib_join makes the main stream wait for it
 int ib_overlap_regen(eddy_ctx *ctx);
-void ib_join(eddy_ctx *ctx);
+int ib_join(eddy_ctx *ctx);
+int ib_prefetch_async(eddy_ctx *ctx, double tmove);
 // the tv flag (fq = 3) is double-buffered so the next step's regeneration can
 // run while tvinterior still reads the current one: swap before it
 int ib_swap_tv_flag(eddy_ctx *ctx);

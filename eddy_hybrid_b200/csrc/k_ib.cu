@@ -1905,7 +1905,7 @@ inline dim3 box_grid(const Box6 &L) {
 
 // exclusive scan with start[n] = total (bsum: scratch of >= ceil(n/SB) ints)
 int scan_launch(eddy_ctx *ctx, int n, const int *cnt, int *start, int *cursor, int *bsum) {
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = cur_stream(ctx);
   const int nb = (n + SB - 1) / SB;
   k_scan_sums<<<nb, SB, 0, st>>>(n, cnt, bsum);
   EDDY_LAUNCHED(ctx);
@@ -1980,7 +1980,7 @@ int build_bins(eddy_ctx *ctx, Bins &b, int dims, const double *lo, const double 
     EDDY_CUDA(cudaMalloc(&b.start, sizeof(int) * (nbins + 1)));
     EDDY_CUDA(cudaMalloc(&b.cursor, sizeof(int) * nbins));
   }
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = cur_stream(ctx);
   EDDY_CUDA(cudaMemsetAsync(b.cursor, 0, sizeof(int) * nbins, st));
   if (tri2d)
     k_bin2_count<<<nblk(ntri), 256, 0, st>>>(ntri, data, b, b.cursor);
@@ -2030,7 +2030,7 @@ Axes axes_of(eddy_ctx *ctx, int q) {
 int geom(eddy_ctx *ctx, int q, int fq, int imn) {
   IbState *s = ibs(ctx);
   const Dims &d = ctx->d;
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = cur_stream(ctx);
   Box6 L = s->lim;
   signed char *flag = s->flag[fq];
   // forcpts
@@ -2168,6 +2168,7 @@ int geom(eddy_ctx *ctx, int q, int fq, int imn) {
 
 // ===========================================================================
 int ib_release(eddy_ctx *ctx) {
+  if (ctx->ib_thread.joinable()) ctx->ib_thread.join();
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
   void *p[] = {s->v, s->c, s->n, s->red, s->dlim, s->work, s->pts, s->b2.start, s->b2.items, s->b2.cursor,
@@ -2193,11 +2194,19 @@ int ib_release(eddy_ctx *ctx) {
   return EDDY_OK;
 }
 
-void ib_join(eddy_ctx *ctx) {
+int ib_join(eddy_ctx *ctx) {
+  int rc = EDDY_OK;
+  if (ctx->ib_thread.joinable() && ctx->ib_thread.get_id() != std::this_thread::get_id()) {
+    ctx->ib_thread.join();
+    rc = ctx->ib_thread_rc;
+    ctx->ib_thread_rc = 0;
+    if (rc) ctx->ib_pending = 0;
+  }
   if (ctx->ib_pending) {
     cudaStreamWaitEvent(ctx->stream, ctx->ib_ev[1], 0);
     ctx->ib_pending = 0;
   }
+  return rc;
 }
 
 int ib_swap_tv_flag(eddy_ctx *ctx) {
@@ -2209,32 +2218,51 @@ int ib_swap_tv_flag(eddy_ctx *ctx) {
   return EDDY_OK;
 }
 
+static int ib_move_impl(eddy_ctx *ctx, double tmove);
+static int ib_regen_impl(eddy_ctx *ctx);
+
+// move the body over tmove and regenerate on the second stream (after the
+// main stream's event ib_ev[0]); records ib_ev[1] when done
+static int regen_on_ib_stream(eddy_ctx *ctx, double tmove) {
+  EDDY_CUDA(cudaStreamWaitEvent(ctx->ib_stream, ctx->ib_ev[0], 0));
+  int rc;
+  {
+    StreamScope sc(ctx->ib_stream);
+    ProfScope ps(ctx, PROF_IB_REGEN);
+    if ((rc = ib_move_impl(ctx, tmove))) return rc;
+    if ((rc = ib_regen_impl(ctx))) return rc;
+  }
+  EDDY_CUDA(cudaEventRecord(ctx->ib_ev[1], ctx->ib_stream));
+  return EDDY_OK;
+}
+
 int ib_overlap_regen(eddy_ctx *ctx) {
   if (ctx->ib_move_dt < 0.) return EDDY_OK;
   const double tmove = ctx->ib_move_dt;
   ctx->ib_move_dt = -1.;
-  EDDY_CUDA(cudaStreamWaitEvent(ctx->ib_stream, ctx->ib_ev[0], 0));
-  // every launch below (and the profile scope) goes to the second stream
-  struct Swap {
-    eddy_ctx *c;
-    cudaStream_t main;
-    explicit Swap(eddy_ctx *x) : c(x), main(x->stream) { c->stream = c->ib_stream; }
-    ~Swap() { c->stream = main; }
-  };
-  int rc;
-  {
-    Swap sw(ctx);
-    ProfScope ps(ctx, PROF_IB_REGEN);
-    if ((rc = ib_move(ctx, tmove))) return rc;
-    if ((rc = ib_regen(ctx))) return rc;
-  }
-  EDDY_CUDA(cudaEventRecord(ctx->ib_ev[1], ctx->ib_stream));
+  int rc = regen_on_ib_stream(ctx, tmove);
+  if (rc) return rc;
   ctx->ib_pending = 1;
   return EDDY_OK;
 }
 
+// the same with its host side (the few count read-backs that size the
+// outputs) on a helper thread, so that the calling thread goes on queuing
+// main-stream work; ib_join joins it before the body's data are used
+int ib_prefetch_async(eddy_ctx *ctx, double tmove) {
+  int rc = ib_join(ctx);
+  if (rc) return rc;
+  ctx->ib_thread_rc = 0;
+  ctx->ib_pending = 1;
+  ctx->ib_thread = std::thread([ctx, tmove]() {
+    cudaSetDevice(ctx->device);
+    ctx->ib_thread_rc = regen_on_ib_stream(ctx, tmove);
+  });
+  return EDDY_OK;
+}
+
 int ib_set_body(eddy_ctx *ctx, int nb, const double *vert, const double *normals, const double *vel) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   ib_release(ctx);
   if (nb <= 0) return EDDY_OK;
   IbState *s = new (std::nothrow) IbState();
@@ -2268,18 +2296,23 @@ int ib_set_body(eddy_ctx *ctx, int nb, const double *vert, const double *normals
     EDDY_CUDA(cudaMalloc(&ctx->ibax[a], sizeof(double) * h.size()));
     EDDY_CUDA(cudaMemcpy(ctx->ibax[a], h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
   }
-  k_centroids<<<nblk(nb), 256, 0, ctx->stream>>>(nb, s->v, s->c);
+  k_centroids<<<nblk(nb), 256, 0, cur_stream(ctx)>>>(nb, s->v, s->c);
   EDDY_LAUNCHED(ctx);
-  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  EDDY_CUDA(cudaStreamSynchronize(cur_stream(ctx)));
   s->ready = true;
   return EDDY_OK;
 }
 
 int ib_move(eddy_ctx *ctx, double tmove) {
-  ib_join(ctx);
+  int rc = ib_join(ctx);
+  if (rc) return rc;
+  return ib_move_impl(ctx, tmove);
+}
+
+static int ib_move_impl(eddy_ctx *ctx, double tmove) {
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
-  k_move<<<nblk(s->nb), 256, 0, ctx->stream>>>(s->nb, s->v, s->c, s->vel[0] * tmove, s->vel[1] * tmove,
+  k_move<<<nblk(s->nb), 256, 0, cur_stream(ctx)>>>(s->nb, s->v, s->c, s->vel[0] * tmove, s->vel[1] * tmove,
                                                s->vel[2] * tmove);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
@@ -2287,11 +2320,16 @@ int ib_move(eddy_ctx *ctx, double tmove) {
 
 // the regeneration of src/Eddy6.f:2184-2380 for the current body position
 int ib_regen(eddy_ctx *ctx) {
-  ib_join(ctx);
+  int rc0 = ib_join(ctx);
+  if (rc0) return rc0;
+  return ib_regen_impl(ctx);
+}
+
+static int ib_regen_impl(eddy_ctx *ctx) {
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
   const Dims &d = ctx->d;
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = cur_stream(ctx);
   int rc;
   long long *keys = reinterpret_cast<long long *>(s->red + 10);
   k_bounds_init<<<1, 32, 0, st>>>(keys);
@@ -2332,7 +2370,7 @@ int ib_regen(eddy_ctx *ctx) {
     EDDY_CUDA(cudaMemsetAsync(s->flag[q], 0, nc, st));
     const long long nbx = (long long)ni * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
     if (nbx > 0) {
-      k_taguo<<<nblk(nbx), 256, 0, st>>>(d, L, 0, s->tag[q], s->flag[q]);
+      k_taguo<<<box_grid(L), 256, 0, st>>>(d, L, 0, s->tag[q], s->flag[q]);
       EDDY_LAUNCHED(ctx);
     }
     k_yper_i8<<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, s->flag[q], 1, d.nx, 1, d.nz);
@@ -2359,7 +2397,7 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
                    int mpitch) {
   IbState *s = ibs(ctx);
   const Dims &d = ctx->d;
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = cur_stream(ctx);
   StencilSet &S = s->set[q];
   // The reference refreshes the y ghost planes after every level.  Forcing
   // points lie in j = 2..NY-1 and every read wraps j into that range
@@ -2406,13 +2444,13 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
 }
 
 int ib_force(eddy_ctx *ctx, int q, int fq, double *a, double b0, double interior, float *mirror, int mpitch) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   if (!ibs(ctx)) return EDDY_OK;
   return force_t<double>(ctx, q, fq, a, ctx->d.nx, b0, interior, mirror, mpitch);
 }
 
 int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, double interior) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   if (!ibs(ctx)) return EDDY_OK;
   return force_t<float>(ctx, q, fq, a, pitch, b0, interior, nullptr, 0);
 }
@@ -2420,7 +2458,7 @@ int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, dou
 const double *ib_velocity(eddy_ctx *ctx) { return ibs(ctx) ? ibs(ctx)->vel : nullptr; }
 
 int ib_set_cadence(eddy_ctx *ctx, int every_substep) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   if (!ibs(ctx)) return EDDY_EINVAL;
   ibs(ctx)->every_substep = every_substep ? 1 : 0;
   return EDDY_OK;
@@ -2430,33 +2468,33 @@ int ib_every_substep(eddy_ctx *ctx) { return ibs(ctx) ? ibs(ctx)->every_substep 
 
 // value where flag fq == 1 (tvinterior), then y periodic planes
 int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror, int mpitch) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   IbState *s = ibs(ctx);
   if (!s) return EDDY_OK;
   const Dims &d = ctx->d;
   const Box6 L = s->lim;
   const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
   if (nbx > 0) {
-    k_interior<double><<<box_grid(L), 256, 0, ctx->stream>>>(d, d.nx, L, s->flag[fq], a, value, mirror, mpitch);
+    k_interior<double><<<box_grid(L), 256, 0, cur_stream(ctx)>>>(d, d.nx, L, s->flag[fq], a, value, mirror, mpitch);
     EDDY_LAUNCHED(ctx);
   }
-  k_yper_field<double><<<nblk((long long)d.nx * d.nz), 256, 0, ctx->stream>>>(d, d.nx, a, mirror, mpitch);
+  k_yper_field<double><<<nblk((long long)d.nx * d.nz), 256, 0, cur_stream(ctx)>>>(d, d.nx, a, mirror, mpitch);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
 
 int ib_download(eddy_ctx *ctx, int which, signed char *out) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   IbState *s = ibs(ctx);
   if (!s || which < 0 || which > 8) return EDDY_EINVAL;
   signed char *src = which < 4 ? s->tag[which] : s->flag[which - 4];
-  EDDY_CUDA(cudaMemcpyAsync(out, src, (size_t)ctx->d.ncell, cudaMemcpyDeviceToHost, ctx->stream));
-  EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
+  EDDY_CUDA(cudaMemcpyAsync(out, src, (size_t)ctx->d.ncell, cudaMemcpyDeviceToHost, cur_stream(ctx)));
+  EDDY_CUDA(cudaStreamSynchronize(cur_stream(ctx)));
   return EDDY_OK;
 }
 
 int ib_limits(eddy_ctx *ctx, int *lim6) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   IbState *s = ibs(ctx);
   if (!s) return EDDY_EINVAL;
   lim6[0] = s->lim.imin; lim6[1] = s->lim.imax; lim6[2] = s->lim.jmin;
@@ -2466,13 +2504,13 @@ int ib_limits(eddy_ctx *ctx, int *lim6) {
 
 int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
                 int *indx) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   IbState *s = ibs(ctx);
   if (!s || q < 0 || q > 3) return EDDY_EINVAL;
   StencilSet &S = s->set[q];
   if (n) *n = S.n;
   if (nlev) *nlev = S.nlev;
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = cur_stream(ctx);
   if (S.n > 0) {
     if (ijk) EDDY_CUDA(cudaMemcpyAsync(ijk, S.ijk, sizeof(int) * 3 * S.n, cudaMemcpyDeviceToHost, st));
     if (dijk) EDDY_CUDA(cudaMemcpyAsync(dijk, S.dijk, sizeof(int) * 3 * S.n, cudaMemcpyDeviceToHost, st));
@@ -2486,11 +2524,11 @@ int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, in
 }
 
 int ib_stencil_kinds(eddy_ctx *ctx, int q, int *mrk, int *dir, double *xe) {
-  ib_join(ctx);
+  if (int rcj = ib_join(ctx)) return rcj;
   IbState *s = ibs(ctx);
   if (!s || q < 0 || q > 3) return EDDY_EINVAL;
   StencilSet &S = s->set[q];
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = cur_stream(ctx);
   if (S.n > 0) {
     if (mrk) EDDY_CUDA(cudaMemcpyAsync(mrk, S.mrk, sizeof(int) * S.n, cudaMemcpyDeviceToHost, st));
     if (dir) EDDY_CUDA(cudaMemcpyAsync(dir, S.dir, sizeof(int) * S.n, cudaMemcpyDeviceToHost, st));

@@ -149,6 +149,32 @@ def test_full_step_parity(oracle, product, shape):
     assert o.max_divergence() < 1e-12
 
 
+@pytest.mark.parametrize("ischm,isgs", [(1, 2), (3, 1), (3, 0)])
+def test_step_parity_schemes_and_sgs_models(oracle, product, ischm, isgs):
+    # AB2 (one substep, src/inpall.f:218-235), the static Smagorinsky model and
+    # no SGS model, 10 steps against the oracle
+    w = config.small(mx=16, ly=8, nz_=24, noise=0.2, re=2000.0, ischm=ischm, isgs=isgs)
+    o = oracle.OracleSolver(w)
+    f = config.initial_fields(w, o.grid.get("dens_bg")[: w.nx])
+    o.load_initial(f)
+    o.initialize()
+    g = product.Solver(w)
+    g.load_initial(f)
+    g.initialize()
+    scale = run_with_scale(o, 10)
+    g.step(10)
+    names = ("uo", "vo", "wo", "dens") + (("tv",) if isgs else ())
+    for n in names:
+        e = rel_err(g.download(n), o.get(n))
+        assert e < 1e-11, (n, e)
+    if isgs:
+        assert float(np.max(o.get("tv")[1:-1, 1:-1, 1:-1])) > 0
+    pg = g.download("p")
+    assert p_err(pg, o.get("p"), scale) < P_BAR
+    assert p_profile_err(pg, o.get("p"), scale) < P_PROFILE_BAR
+    assert g.max_divergence() < 1e-12
+
+
 @pytest.fixture(scope="module")
 def wimply():
     # the reference's own input runs the y viscous terms Crank-Nicolson (IMPLY = 1)
