@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--profile", default=None, choices=["plain", "mixed"],
                     help="run one form (warm-up + steps, the dynamic model) and exit without timing: the "
                          "command to put under a profiler")
+    ap.add_argument("--deploy", action="store_true",
+                    help="the learned closure deployed on 768x512x384 (Re 2e4, Fr 1, the moving sphere) for "
+                         "--deploy-steps steps against a plain FP64 run: nu_t error against the dynamic model and "
+                         "the wake-centreline velocity; prints one JSON line")
+    ap.add_argument("--deploy-steps", type=int, default=200)
     ap.add_argument("--grid", default=None,
                     help="NZ-2xNX-2xNY-2 of the wake workload, e.g. 64x384x256 (6.3M cells, fields larger "
                          "than L2, a few GB on the device) for ncu captures")
@@ -337,10 +342,74 @@ def closure_weights(g_plain, w, log):
     return meta, theta, rep
 
 
+def run_deploy(args):
+    """The learned closure deployed on the 768x512x384 wake (streamwise x
+    vertical x periodic; Re 2e4, Fr 1, the sphere moving at U = 1, dt 5e-4)
+    with the dynamic-model fallback outside the training envelope, against a
+    plain FP64 run with the dynamic model from the same start: after the
+    steps, the closure's nu_t against the dynamic model's on the closure
+    run's state, and the streamwise velocity along the wake centreline (the
+    line through the body centre, x = y = 0) of the two runs."""
+    import numpy as np
+    import eddy_hybrid_b200 as eb
+    from eddy_hybrid_b200 import body as bd
+    from eddy_hybrid_b200 import closure as cl
+    from eddy_hybrid_b200 import config
+    log = lambda *a: print(*a, file=sys.stderr, flush=True)  # noqa: E731
+    w = config.Workload("wake_768x512x384", mx=512, ly=384, nz_=768, re=2e4, fr=1.0, dt=5e-4, body_speed=1.0)
+    xu = np.diff(w.faces()[0])
+    tri, nrm = bd.icosphere(bd.level_for_spacing(max(float(xu.min()), 0.004)))
+    vel = bd.body_velocity(w)
+    out = {"workload": w.name, "cells": w.ncell, "steps": args.deploy_steps, "re": w.re, "fr": w.fr,
+           "triangles": int(len(tri))}
+    runs = {}
+    for form in ("plain", "closure"):
+        g = eb.Solver(w, precision=eb.PLAIN_FP64 if form == "plain" else eb.MIXED, refine_sweeps=args.sweeps,
+                      closure=1 if form == "closure" else 0)
+        g.set_body(tri, nrm, vel)
+        if form == "closure":
+            meta, theta, rep = closure_weights(None, w, log)
+            cl.Closure(g).set(meta, theta)
+            out["closure_weights"] = rep.get("source")
+        g.load_initial(config.initial_fields(w, g.metric("dens_bg")[: w.nx]))
+        g.initialize()
+        t0 = time.time()
+        g.step(args.deploy_steps)
+        g.sync()
+        out[f"{form}_s_per_step"] = (time.time() - t0) / args.deploy_steps
+        xc, yc = g.metric("xc")[: w.nx], g.metric("yc")[: w.ny]
+        ic, jc = int(np.argmin(np.abs(xc))), int(np.argmin(np.abs(yc)))
+        wo = g.download("wo")
+        runs[form] = {"line": np.array(wo[ic, jc, 1:-1]), "ymean": np.array(wo[ic, 1:-1, 1:-1].mean(axis=0))}
+        if form == "closure":
+            c = cl.Closure(g)
+            nout = c.apply()
+            nu_c = g.download("tv")[1:-1, 1:-1, 1:-1]
+            c.refresh_fallback()
+            nu_d = g.download("tv")[1:-1, 1:-1, 1:-1]
+            out["nu_t_rel_err_vs_dynamic"] = float(np.linalg.norm(nu_c - nu_d) / max(np.linalg.norm(nu_d), 1e-300))
+            out["cells_outside_envelope"] = int(nout)
+            out["max_div_u"] = g.max_divergence()
+        log(f"deploy {form}: {out[f'{form}_s_per_step'] * 1e3:.1f} ms/step (wall)")
+        g.close()
+        del g
+    for key in ("line", "ymean"):
+        a, b = runs["closure"][key], runs["plain"][key]
+        out[f"centreline_w_{key}"] = {"max_abs_diff": float(np.max(np.abs(a - b))),
+                                      "rms_diff": float(np.sqrt(np.mean((a - b) ** 2))),
+                                      "plain_min": float(b.min()), "closure_min": float(a.min())}
+    out["note"] = ("streamwise velocity w along the centreline (x = y = 0, and averaged over the periodic y at "
+                   "x = 0) after the steps, free stream 1; wall-clock seconds per step include the host's "
+                   "step loop")
+    print(json.dumps({"deploy": out}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.deploy:
+        return run_deploy(args)
     rank, world, local, dist = dist_init(args.gpus)
     import numpy as np
     import torch

@@ -5,11 +5,45 @@
 // butterfly performs exactly the operations of the two radix-2 stages it
 // replaces, with the same table twiddles, so results equal the radix-2
 // sequence of FFTPACK order used by the oracle bit for bit.
-// tw*: shared-memory table exp(s 2 pi i r / L), r < L/2.
+// tw*: shared-memory table exp(s 2 pi i r / L), r < L/2 (read with stride ts:
+// a sub-transform of length L/ts uses every ts-th entry).
+//
+// Lines of length L = r 2^m, r = 1 or 3 (the periodic extents FFTPACK's
+// radix-2/3 factors cover, e.g. 384 = 3 x 128): with r = 3 the input is
+// decimated by 3 (element j to block j mod 3, at the bit-reversed position of
+// j / 3), each block is transformed by the radix-2^2 passes, and one pass of
+// radix-3 butterflies combines them.  A length is passed as the code
+// m | r << 8.
 #pragma once
 
+__host__ __device__ inline int fft_len(int code) { return (code >> 8) << (code & 255); }
+
+// the code of a line length L = r 2^m (r = 1 or 3, m >= 1), or -1
+inline int fft_code(int L) {
+  int r = 1;
+  if (L % 3 == 0) {
+    r = 3;
+    L /= 3;
+  }
+  int m = 0;
+  while ((1 << m) < L) m++;
+  if (m < 1 || (1 << m) != L) return -1;
+  return m | (r << 8);
+}
+
+__device__ __forceinline__ int fft_bitrev(int x, int logn) {
+  return (int)(__brev((unsigned)x) >> (32 - logn));
+}
+
+// the shared-memory slot of input element j of a line
+__device__ __forceinline__ int fft_slot(int j, int code) {
+  const int m = code & 255;
+  if ((code >> 8) == 1) return fft_bitrev(j, m);
+  return (j % 3) * (1 << m) + fft_bitrev(j / 3, m);
+}
+
 template <class T, int TI>
-__device__ __forceinline__ void fft_lines_r22(T *re, T *im, int logL, const T *twr, const T *twi) {
+__device__ __forceinline__ void fft_lines_r22(T *re, T *im, int logL, const T *twr, const T *twi, int ts = 1) {
   const int L = 1 << logL;
   int s = 0;
   if (logL & 1) {  // one radix-2 stage of half-length 1 (twiddle index 0)
@@ -35,9 +69,9 @@ __device__ __forceinline__ void fft_lines_r22(T *re, T *im, int logL, const T *t
       const int ii = bf % TI, pq = bf / TI;
       const int q = pq & (h - 1), grp = pq >> s;
       const int i0 = grp * 4 * h + q;
-      const T w1r = twr[q * st1], w1i = twi[q * st1];
-      const T w2r = twr[q * st2], w2i = twi[q * st2];
-      const T w3r = twr[(q + h) * st2], w3i = twi[(q + h) * st2];
+      const T w1r = twr[q * st1 * ts], w1i = twi[q * st1 * ts];
+      const T w2r = twr[q * st2 * ts], w2i = twi[q * st2 * ts];
+      const T w3r = twr[(q + h) * st2 * ts], w3i = twi[(q + h) * st2 * ts];
       T x0r = re[i0 * TI + ii], x0i = im[i0 * TI + ii];
       T x1r = re[(i0 + h) * TI + ii], x1i = im[(i0 + h) * TI + ii];
       T x2r = re[(i0 + 2 * h) * TI + ii], x2i = im[(i0 + 2 * h) * TI + ii];
@@ -64,6 +98,49 @@ __device__ __forceinline__ void fft_lines_r22(T *re, T *im, int logL, const T *t
     }
     __syncthreads();
   }
+}
+
+// a line of length fft_len(code), input in fft_slot order, output in
+// natural order (in place)
+template <class T, int TI>
+__device__ __forceinline__ void fft_lines_any(T *re, T *im, int code, const T *twr, const T *twi) {
+  const int m = code & 255;
+  if ((code >> 8) == 1) {
+    fft_lines_r22<T, TI>(re, im, m, twr, twi, 1);
+    return;
+  }
+  const int L3 = 1 << m, half = 3 * L3 / 2;
+  for (int b = 0; b < 3; b++) fft_lines_r22<T, TI>(re + b * L3 * TI, im + b * L3 * TI, m, twr, twi, 3);
+  // W^e from the table of e < L/2 (W^(L/2) = -1 beyond)
+  auto tw = [&](int e, T &wr, T &wi) {
+    if (e < half) {
+      wr = twr[e];
+      wi = twi[e];
+    } else {
+      wr = -twr[e - half];
+      wi = -twi[e - half];
+    }
+  };
+  T ur, ui, vr, vi;  // the cube roots W^(L/3), W^(2L/3)
+  tw(L3, ur, ui);
+  tw(2 * L3, vr, vi);
+  for (int bf = threadIdx.x; bf < TI * L3; bf += blockDim.x) {
+    const int ii = bf % TI, k = bf / TI;
+    T w1r, w1i, w2r, w2i;
+    tw(k, w1r, w1i);
+    tw(2 * k, w2r, w2i);
+    const int pa = k * TI + ii, pb = (L3 + k) * TI + ii, pc = (2 * L3 + k) * TI + ii;
+    const T ar = re[pa], ai = im[pa], br = re[pb], bi = im[pb], cr = re[pc], ci = im[pc];
+    const T t1r = w1r * br - w1i * bi, t1i = w1r * bi + w1i * br;
+    const T t2r = w2r * cr - w2i * ci, t2i = w2r * ci + w2i * cr;
+    re[pa] = ar + t1r + t2r;
+    im[pa] = ai + t1i + t2i;
+    re[pb] = ar + (ur * t1r - ui * t1i) + (vr * t2r - vi * t2i);
+    im[pb] = ai + (ur * t1i + ui * t1r) + (vr * t2i + vi * t2r);
+    re[pc] = ar + (vr * t1r - vi * t1i) + (ur * t2r - ui * t2i);
+    im[pc] = ai + (vr * t1i + vi * t1r) + (ur * t2i + ui * t2r);
+  }
+  __syncthreads();
 }
 
 // copy a twiddle table of L/2 entries from global to shared memory

@@ -225,7 +225,6 @@ constexpr int TI32 = 32, FT32 = 256, HL32 = TI32 / 2;
 
 inline size_t fft32_smem(int L) { return sizeof(float) * (2 * (size_t)L * HL32 + HL32 + L); }
 
-__device__ __forceinline__ int bitrev(int x, int logn) { return (int)(__brev((unsigned)x) >> (32 - logn)); }
 
 #include "fft_lines.cuh"
 
@@ -244,14 +243,14 @@ template <int MODE>
 __global__ void __launch_bounds__(FT32, 4)
     k_fwd32(Dims d, DevMetrics m, int px, const float *__restrict__ us, const float *__restrict__ vs,
             const float *__restrict__ ws, const double *__restrict__ win, const double *__restrict__ wout,
-            const double *__restrict__ phi, double *__restrict__ dvec, double ralf, double rdy2, int logL,
+            const double *__restrict__ phi, double *__restrict__ dvec, double ralf, double rdy2, int code,
             const float *__restrict__ twr, const float *__restrict__ twi, float *__restrict__ spec,
             unsigned long long *rmax) {
   constexpr int U = 8;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ float smf[];
   __shared__ double red[FT32 / 32];
-  const int L = 1 << logL, M = d.nx - 2;
+  const int L = fft_len(code), M = d.nx - 2;
   float *re = smf, *im = smf + L * HL32 + HL32;
   float *tsr = im + L * HL32, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
@@ -301,7 +300,7 @@ __global__ void __launch_bounds__(FT32, 4)
           x = act ? x * ralf : 0.;
           vprev = vc;
           if (act) D[jj * nx] = x;
-          slot32(re, im, bitrev(jj, logL), lane) = (float)x;
+          slot32(re, im, fft_slot(jj, code), lane) = (float)x;
         }
       }
     }
@@ -312,7 +311,7 @@ __global__ void __launch_bounds__(FT32, 4)
       for (int u = 0; u < U; u++) v[u] = (j0 + u < je) ? D[(j0 + u) * nx] : 0.;
 #pragma unroll
       for (int u = 0; u < U; u++)
-        if (j0 + u < je) slot32(re, im, bitrev(j0 + u, logL), lane) = act ? (float)v[u] : 0.f;
+        if (j0 + u < je) slot32(re, im, fft_slot(j0 + u, code), lane) = act ? (float)v[u] : 0.f;
     }
   } else {
     constexpr int U2 = 2;
@@ -324,7 +323,7 @@ __global__ void __launch_bounds__(FT32, 4)
     const double ct = m.cp[k] * m.cw[k], cb = m.cp[k] * m.cw[k - 1];
     double cprev = 0., ccur = 0.;
     if (jb < je) {
-      cprev = P[((jb - 1 + L) & (L - 1)) * nx];
+      cprev = P[((jb - 1 + L) % L) * nx];
       ccur = P[jb * nx];
     }
     for (int j0 = jb; j0 < je; j0 += U2) {
@@ -335,7 +334,7 @@ __global__ void __launch_bounds__(FT32, 4)
         const int jj = j0 + u;
         if (jj < je) {
           const int o = jj * nx;
-          cn[u] = P[((jj + 1) & (L - 1)) * nx];
+          cn[u] = P[(jj + 1 == L ? 0 : jj + 1) * nx];
           tt[u] = kt ? P[o + sz] : 0.;
           bb[u] = kb ? P[o - sz] : 0.;
           dd[u] = D[o];
@@ -357,7 +356,7 @@ __global__ void __launch_bounds__(FT32, 4)
                              cb * (pbm - c);
           const double x = act ? dd[u] - lap : 0.;
           amax = fmax(amax, fabs(x));
-          slot32(re, im, bitrev(jj, logL), lane) = (float)x;
+          slot32(re, im, fft_slot(jj, code), lane) = (float)x;
           cprev = c;
           ccur = cn[u];
         }
@@ -372,14 +371,14 @@ __global__ void __launch_bounds__(FT32, 4)
     for (int w = 0; w < FT32 / 32; w++) b = fmax(b, red[w]);
     atomicMax(rmax, (unsigned long long)__double_as_longlong(b));
   }
-  fft_lines_r22<float, HL32>(re, im, logL, tsr, tsi);
+  fft_lines_any<float, HL32>(re, im, code, tsr, tsi);
   // separate the two real transforms: A_q = (Z_q + conj Z_{L-q}) / 2,
   // B_q = (Z_q - conj Z_{L-q}) / 2i; packed order [a0, a1, b1, ..., a_{L/2}]
   const int pl = lane & (HL32 - 1);
   const bool second = lane >= HL32;
   float *S = spec + (long long)(ic - d.ix1) + (long long)M * L * (k - d.kz1);
   for (int q = warp; q <= L / 2; q += FT32 / 32) {
-    const int qm = (L - q) & (L - 1);
+    const int qm = q == 0 ? 0 : L - q;
     const float zr = re[q * HL32 + pl], zi = im[q * HL32 + pl];
     const float wr = re[qm * HL32 + pl], wi = im[qm * HL32 + pl];
     const float vr = second ? 0.5f * (zi + wi) : 0.5f * (zr + wr);
@@ -403,12 +402,12 @@ __global__ void __launch_bounds__(FT32, 4)
 // half) and Z_{L-q} (high half).
 template <int ACC>
 __global__ void __launch_bounds__(FT32, 4)
-    k_bwd32(Dims d, const float *__restrict__ spec, const double *__restrict__ dpm, int logL,
+    k_bwd32(Dims d, const float *__restrict__ spec, const double *__restrict__ dpm, int code,
             const float *__restrict__ twr, const float *__restrict__ twi, double *__restrict__ phi) {
   constexpr int U = 4;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ float smf[];
-  const int L = 1 << logL, M = d.nx - 2;
+  const int L = fft_len(code), M = d.nx - 2;
   float *re = smf, *im = smf + L * HL32 + HL32;
   float *tsr = im + L * HL32, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
@@ -446,11 +445,11 @@ __global__ void __launch_bounds__(FT32, 4)
         const float ar = a[u] * rl, ai = b[u] * rl;
         const float orr = __shfl_xor_sync(FULL, ar, HL32), oi = __shfl_xor_sync(FULL, ai, HL32);
         if (low) {  // own A_q, other B_q: Z_q = (Ar - Bi) + i (Ai + Br)
-          const int r = bitrev(q, logL);
+          const int r = fft_slot(q, code);
           re[r * HL32 + pl] = ar - oi;
           im[r * HL32 + pl] = ai + orr;
         } else if (q != 0 && q != L / 2) {  // own B_q, other A_q: Z_{L-q} = (Ar + Bi) + i (Br - Ai)
-          const int r = bitrev(L - q, logL);
+          const int r = fft_slot(L - q, code);
           re[r * HL32 + pl] = orr + ai;
           im[r * HL32 + pl] = ar - oi;
         }
@@ -458,7 +457,7 @@ __global__ void __launch_bounds__(FT32, 4)
     }
   }
   __syncthreads();
-  fft_lines_r22<float, HL32>(re, im, logL, tsr, tsi);
+  fft_lines_any<float, HL32>(re, im, code, tsr, tsi);
   // real part -> line pl, imaginary part -> line pl + 16
   const int JW = (L + 7) / 8, jb = min(L, warp * JW), je = min(L, jb + JW);
   const int nx = d.nx;
@@ -735,11 +734,6 @@ int to64(eddy_ctx *ctx, const float *b, double *a) {
   return EDDY_OK;
 }
 
-int log2i(int L) {
-  int l = 0;
-  while ((1 << l) < L) l++;
-  return l;
-}
 
 // FP32 spectral solve of the transformed right-hand side in pp.spec (as
 // float) -> phi (set or accumulate)
@@ -767,7 +761,7 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
     k_line_mean<float><<<1, 256, 0, ctx->stream>>>(M, L, N, m0, pp.wz, s2, ctx->scal + 5);
     EDDY_LAUNCHED(ctx);
     float *e32 = reinterpret_cast<float *>(pp.cprime);
-    k_tridiag_lines<float, float, 8, true, true><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
+    k_tridiag_lines<float, float, 8, true, true, 16><<<(unsigned)((nl + 127) / 128), 128, 0, ctx->stream>>>(
         M, L, N, m0, lam, pp.ak, pp.an, pp.bn, pp.cn, ctx->scal + 5, s2, x->cpz, e32);
     EDDY_LAUNCHED(ctx);
   }
@@ -787,9 +781,9 @@ int solve32(eddy_ctx *ctx, double *phi, int accumulate) {
   size_t smem = fft32_smem(L);
   dim3 g((M + TI32 - 1) / TI32, N);
   if (accumulate)
-    k_bwd32<1><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi);
+    k_bwd32<1><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, fft_code(L), x->twr + L / 2, x->twi + L / 2, phi);
   else
-    k_bwd32<0><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, log2i(L), x->twr + L / 2, x->twi + L / 2, phi);
+    k_bwd32<0><<<g, FT32, smem, ctx->stream>>>(d, s1, ctx->scal + 3, fft_code(L), x->twr + L / 2, x->twi + L / 2, phi);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;
 }
@@ -805,7 +799,7 @@ int fwd32(eddy_ctx *ctx, int mode, double alfxdt, const double *phi, double *dve
   ProfScope ps(ctx, mode == 2 ? PROF_REFINE : PROF_DIV_FFT);
   auto *rm = reinterpret_cast<unsigned long long *>(x->resid + sweep);
   float *sp = reinterpret_cast<float *>(pp.spec);
-  const int lg = log2i(pp.L);
+  const int lg = fft_code(pp.L);
   const double rdy2 = 1.0 / ctx->delysq;
   if (mode == 0)
     k_fwd32<0><<<g, FT32, smem, ctx->stream>>>(d, ctx->m, x->px, x->us, x->vs, x->ws, ctx->f[EDDY_PLANEW], x->wout,

@@ -25,10 +25,6 @@ namespace {
 constexpr int TI = 16;     // lines (consecutive i) per FFT block
 constexpr int FT = 256;    // threads per FFT block
 
-__device__ __forceinline__ int bitrev(int x, int logn) {
-  return (int)(__brev((unsigned)x) >> (32 - logn));
-}
-
 #include "fft_lines.cuh"
 
 // Step 1.  mode 0: f = divergence(us,vs,ws)/alfxdt (src/timeindeg.f:941-949,
@@ -36,10 +32,10 @@ __device__ __forceinline__ int bitrev(int x, int logn) {
 __global__ void __launch_bounds__(FT, 3)
     k_div_fft_fwd(Dims d, DevMetrics m, const double *__restrict__ us, const double *__restrict__ vs,
                   const double *__restrict__ ws, const double *__restrict__ rhs, int mode, double alfxdt,
-                  int logL, const double *__restrict__ twr, const double *__restrict__ twi,
+                  int code, const double *__restrict__ twr, const double *__restrict__ twi,
                   double *__restrict__ spec) {
   extern __shared__ double sm[];
-  const int L = 1 << logL, M = d.nx - 2;
+  const int L = fft_len(code), M = d.nx - 2;
   double *re = sm, *im = sm + L * TI;
   double *tsr = sm + 2 * L * TI, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
@@ -71,14 +67,14 @@ __global__ void __launch_bounds__(FT, 3)
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * FT;
       if (t < NT) {
-        const int ii = t % TI, r = bitrev(t / TI, logL);
+        const int ii = t % TI, r = fft_slot(t / TI, code);
         re[r * TI + ii] = v[u];
         im[r * TI + ii] = 0.;
       }
     }
   }
   __syncthreads();
-  fft_lines_r22<double, TI>(re, im, logL, tsr, tsi);
+  fft_lines_any<double, TI>(re, im, code, tsr, tsi);
   // packed order [a0, a1, b1, ..., a_{L/2}]
   long long lineK = (long long)(k - d.kz1) * L;
   for (int t = threadIdx.x; t < L * TI; t += blockDim.x) {
@@ -98,10 +94,10 @@ __global__ void __launch_bounds__(FT, 3)
 
 // Step 5: (S - dpm[J==0]) / L, Hermitian extension, inverse DIT, real part.
 __global__ void __launch_bounds__(FT, 3)
-    k_fft_bwd(Dims d, const double *__restrict__ spec, const double *__restrict__ dpm, int logL,
+    k_fft_bwd(Dims d, const double *__restrict__ spec, const double *__restrict__ dpm, int code,
               const double *__restrict__ twr, const double *__restrict__ twi, double *__restrict__ dp) {
   extern __shared__ double sm[];
-  const int L = 1 << logL, M = d.nx - 2;
+  const int L = fft_len(code), M = d.nx - 2;
   double *re = sm, *im = sm + L * TI;
   double *tsr = sm + 2 * L * TI, *tsi = tsr + L / 2;
   load_twiddles(tsr, tsi, twr, twi, L / 2);
@@ -137,14 +133,14 @@ __global__ void __launch_bounds__(FT, 3)
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * FT;
       if (t < NT) {
-        const int ii = t % TI, r = bitrev(t / TI, logL);
+        const int ii = t % TI, r = fft_slot(t / TI, code);
         re[r * TI + ii] = xr[u];
         im[r * TI + ii] = xi[u];
       }
     }
   }
   __syncthreads();
-  fft_lines_r22<double, TI>(re, im, logL, tsr, tsi);
+  fft_lines_any<double, TI>(re, im, code, tsr, tsi);
   for (int t = threadIdx.x; t < L * TI; t += blockDim.x) {
     int ii = t % TI, jj = t / TI;
     int i = i0 + ii;
@@ -267,11 +263,10 @@ int solve_from_spec(eddy_ctx *ctx, double *dp) {
   EDDY_LAUNCHED(ctx);
   k_plane_sum_final<<<1, 32, 0, ctx->stream>>>(NPART, (long long)M * N, pp.red, ctx->scal + 3);
   EDDY_LAUNCHED(ctx);
-  int logL = 0;
-  while ((1 << logL) < L) logL++;
+  const int code = fft_code(L);
   size_t smem = sizeof(double) * (2 * L * TI + L);
   dim3 g((M + TI - 1) / TI, N);
-  k_fft_bwd<<<g, FT, smem, ctx->stream>>>(d, pp.spec, ctx->scal + 3, logL, pp.twr + L / 2, pp.twi + L / 2, dp);
+  k_fft_bwd<<<g, FT, smem, ctx->stream>>>(d, pp.spec, ctx->scal + 3, code, pp.twr + L / 2, pp.twi + L / 2, dp);
   EDDY_LAUNCHED(ctx);
   long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
   k_dp_ghost<<<(unsigned)((ng + 255) / 256), 256, 0, ctx->stream>>>(d, dp);
@@ -290,8 +285,8 @@ int poisson_plan_create(eddy_ctx *ctx) {
     ctx->err = "DIRECT on the device needs Neumann x and z and periodic y";
     return EDDY_EINVAL;
   }
-  if (L < 2 || (L & (L - 1)) != 0) {
-    ctx->err = "the periodic (FFT) extent NY-2 must be a power of two";
+  if (fft_code(L) < 0) {
+    ctx->err = "the periodic (FFT) extent NY-2 must be 2^m or 3 x 2^m (m >= 1)";
     return EDDY_EINVAL;
   }
   if (M < 3 || N < 3) { ctx->err = "grid too small"; return EDDY_EINVAL; }
@@ -427,12 +422,11 @@ static int fwd(eddy_ctx *ctx, const double *us, const double *vs, const double *
                double alfxdt) {
   PoissonPlan &pp = ctx->pp;
   const Dims &d = ctx->d;
-  int logL = 0;
-  while ((1 << logL) < pp.L) logL++;
+  const int code = fft_code(pp.L);
   size_t smem = sizeof(double) * (2 * pp.L * TI + pp.L);
   dim3 g((pp.M + TI - 1) / TI, pp.N);
   ProfScope ps(ctx, PROF_DIV_FFT);
-  k_div_fft_fwd<<<g, FT, smem, ctx->stream>>>(d, ctx->m, us, vs, ws, rhs, mode, alfxdt, logL, pp.twr, pp.twi,
+  k_div_fft_fwd<<<g, FT, smem, ctx->stream>>>(d, ctx->m, us, vs, ws, rhs, mode, alfxdt, code, pp.twr, pp.twi,
                                               pp.spec);
   EDDY_LAUNCHED(ctx);
   return EDDY_OK;

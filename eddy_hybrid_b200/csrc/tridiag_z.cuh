@@ -70,7 +70,9 @@ __global__ void __launch_bounds__(128)
 // register buffers; pays off with FP32 storage, the FP64 form keeps one).
 // PC: c' comes precomputed (k_tridiag_cprime) in cpr, which the elimination
 // then only reads; otherwise the elimination writes it there.
-template <class G, class C = double, int ZC = 8, bool DB = true, bool PC = false>
+// ZF: chunk of the forward sweep (one load per plane there against two in the
+// back substitution, so a longer chunk keeps as many bytes in flight).
+template <class G, class C = double, int ZC = 8, bool DB = true, bool PC = false, int ZF = ZC>
 __global__ void __launch_bounds__(128)
     k_tridiag_lines(int M, int L, int N, int m0, const double *__restrict__ lam, const double *__restrict__ ak,
                     const double *__restrict__ an, const double *__restrict__ bn, const double *__restrict__ cn,
@@ -86,14 +88,14 @@ __global__ void __launch_bounds__(128)
   double pc = 0., pd = 0.;
   // forward elimination; the loads of the next chunk are issued before the
   // recurrence over the current one (two register buffers)
-  G fa[ZC], fb[ZC];
-  auto load_f = [&](G (&f)[ZC], int k0) {
+  G fa[ZF], fb[ZF];
+  auto load_f = [&](G (&f)[ZF], int k0) {
 #pragma unroll
-    for (int q = 0; q < ZC; q++) f[q] = (k0 + q < N) ? g[t + ML * (k0 + q)] : G(0);
+    for (int q = 0; q < ZF; q++) f[q] = (k0 + q < N) ? g[t + ML * (k0 + q)] : G(0);
   };
-  auto elim = [&](const G (&f)[ZC], int k0) {
+  auto elim = [&](const G (&f)[ZF], int k0) {
 #pragma unroll
-    for (int q = 0; q < ZC; q++) {
+    for (int q = 0; q < ZF; q++) {
       const int k = k0 + q;
       if (k < N) {
         const double a = (k == s0) ? 0. : an[k];
@@ -109,16 +111,16 @@ __global__ void __launch_bounds__(128)
   };
   if (DB) {
     load_f(fa, s0);
-    for (int k0 = s0; k0 < N; k0 += 2 * ZC) {
-      if (k0 + ZC < N) load_f(fb, k0 + ZC);
+    for (int k0 = s0; k0 < N; k0 += 2 * ZF) {
+      if (k0 + ZF < N) load_f(fb, k0 + ZF);
       elim(fa, k0);
-      if (k0 + ZC < N) {
-        if (k0 + 2 * ZC < N) load_f(fa, k0 + 2 * ZC);
-        elim(fb, k0 + ZC);
+      if (k0 + ZF < N) {
+        if (k0 + 2 * ZF < N) load_f(fa, k0 + 2 * ZF);
+        elim(fb, k0 + ZF);
       }
     }
   } else {
-    for (int k0 = s0; k0 < N; k0 += ZC) {
+    for (int k0 = s0; k0 < N; k0 += ZF) {
       load_f(fa, k0);
       elim(fa, k0);
     }

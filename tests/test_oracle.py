@@ -160,3 +160,19 @@ def test_taylor_green_decay_known_answer(oracle):
     # second order in space: the error falls by 4 when the spacing halves
     for a in (0, 1):
         assert 3.5 < e16[a] / e32[a] < 4.5, (e16[a], e32[a])
+
+
+@pytest.mark.parametrize("n", [6, 12, 24, 48, 96, 384])
+def test_fft_non_power_of_two_matches_numpy(oracle, n):
+    # lengths 3 x 2^m (the transform of the 384-wide periodic extent): the
+    # oracle's transform against numpy's FFT, in FFTPACK's packed order
+    x = np.random.RandomState(n).randn(n)
+    r = oracle.rfftf(x)
+    f = np.fft.rfft(x)
+    want = np.empty(n)
+    want[0] = f[0].real
+    want[1:-1:2] = f[1:n // 2].real
+    want[2:-1:2] = f[1:n // 2].imag
+    want[-1] = f[n // 2].real
+    np.testing.assert_allclose(r, want, rtol=0, atol=1e-12 * np.max(np.abs(want)))
+    np.testing.assert_allclose(oracle.rfftb(r), n * x, rtol=0, atol=1e-11 * n * np.max(np.abs(x)))
