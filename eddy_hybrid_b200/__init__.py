@@ -44,7 +44,7 @@ class Params(C.Structure):
                 ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
                 ("dspngx3in", C.c_int), ("dspngx3out", C.c_int),
                 ("precision", C.c_int), ("refine_sweeps", C.c_int),
-                ("closure", C.c_int), ("imply", C.c_int)]
+                ("closure", C.c_int), ("imply", C.c_int), ("implx", C.c_int)]
 
 
 def make_params(d: dict, precision: int = PLAIN_FP64, refine_sweeps: int = 2,
@@ -75,6 +75,7 @@ SIGNATURES = {
     "eddy_grid_metric": ([C.POINTER(Params), _DP, C.c_double, C.c_double, _DP, C.c_int, _DP, C.c_int], C.c_int),
     "eddy_rhs_predictord": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
     "eddy_inversey": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_inversex": ([C.c_void_p, C.c_double], C.c_int),
     "eddy_cfl": ([C.c_void_p, _DP], C.c_int),
     "eddy_field_extrema": ([C.c_void_p, C.c_int, _DP, _DP], C.c_int),
     "eddy_ioscalar_write": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.c_int, C.c_double, C.c_double,

@@ -201,6 +201,7 @@ void build_metrics(eddy_ctx *ctx, const double *xf, double ymin, double ymax, co
   s.ru1 = p.ru1; s.prn = p.prn; s.grav = p.grav; s.dpdx = p.dpdx; s.dpdy = p.dpdy; s.dpdz = p.dpdz;
   s.eps = p.eps; s.css = p.css; s.vspngx1 = p.vspngx1; s.dspngx1 = p.dspngx1;
   s.ivspngl = ivs; s.idspngl = ids; s.idens = p.idens; s.isgs = p.isgs; s.imply = p.imply;
+  s.implx = p.implx;
 }
 
 int upload_metrics(eddy_ctx *ctx) {
@@ -353,6 +354,11 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
   if (p.imply == 1 && (p.precision != EDDY_PLAIN_FP64 || p.closure != 0))
     return fail(EDDY_EINVAL, "the implicit y terms (imply = 1) are built for the plain FP64 form with the dynamic model");
   if (p.imply == 1 && p.ny - 2 < 3) return fail(EDDY_EINVAL, "imply = 1 needs at least 3 cells along y");
+  if (p.implx != 0 && p.implx != 1) return fail(EDDY_EINVAL, "implx must be 0 or 1");
+  if (p.implx == 1 && (p.precision != EDDY_PLAIN_FP64 || p.closure != 0))
+    return fail(EDDY_EINVAL, "the implicit x terms (implx = 1) are built for the plain FP64 form with the dynamic model");
+  if (p.implx == 1 && (p.itype[1] != 60 || p.itype[2] != 60))
+    return fail(EDDY_EINVAL, "implx = 1 is built for slip walls (type 60) on both x boundaries");
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
   // the regeneration's stream has the highest priority: its short kernels
@@ -498,6 +504,15 @@ int eddy_inversey(eddy_ctx *ctx, double alfxdt) {
   return launch_inversey(ctx, alfxdt);
 }
 
+int eddy_inversex(eddy_ctx *ctx, double alfxdt) {
+  if (check_ctx(ctx)) return EDDY_EINVAL;
+  if (ctx->prm.implx != 1) {
+    ctx->err = "eddy_inversex needs implx = 1";
+    return EDDY_EINVAL;
+  }
+  return launch_inversex(ctx, alfxdt);
+}
+
 int eddy_boundary(eddy_ctx *ctx, int set) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
   double **f = ctx->f;
@@ -545,8 +560,8 @@ int eddy_turvis(eddy_ctx *ctx) {
 int eddy_ib_set_body(eddy_ctx *ctx, int nb, const double *vertices, const double *normals,
                      const double *velocity) {
   if (check_ctx(ctx) || nb < 0 || (nb > 0 && (!vertices || !normals))) return EDDY_EINVAL;
-  if (nb > 0 && ctx->prm.imply == 1) {
-    ctx->err = "an immersed body with the implicit y terms (the reference's forcing of UB, src/Eddy6.f:2490-2520) "
+  if (nb > 0 && (ctx->prm.imply == 1 || ctx->prm.implx == 1)) {
+    ctx->err = "an immersed body with the implicit terms (the reference's forcing of UB, src/Eddy6.f:2490-2520) "
                "is not supported";
     return EDDY_EINVAL;
   }
@@ -760,10 +775,14 @@ static int substep_core(eddy_ctx *ctx, int is, double dt) {
     ProfScope ps(ctx, PROF_RHS_PRED);
     if ((rc = launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt))) return rc;
   }
-  // Crank-Nicolson y lines (src/Eddy6.f:2596-2599; no immersed body)
+  // Crank-Nicolson y, then x lines (src/Eddy6.f:2596-2607; no immersed body)
   if (ctx->sc.imply == 1) {
     ProfScope ps(ctx, PROF_TRIDIAG);
     if ((rc = launch_inversey(ctx, alfxdt))) return rc;
+  }
+  if (ctx->sc.implx == 1) {
+    ProfScope ps(ctx, PROF_TRIDIAG);
+    if ((rc = launch_inversex(ctx, alfxdt))) return rc;
   }
   if ((rc = ib_overlap_regen(ctx))) return rc;
   // momforc_mod2 + velinterior (src/Eddy6.f:2526-2575)

@@ -40,6 +40,7 @@ struct Scalars {
   double ru1, prn, grav, dpdx, dpdy, dpdz, eps, css;
   int vspngx1, dspngx1, ivspngl, idspngl, idens, isgs;
   int imply;  // IMPLY: Crank-Nicolson viscous terms along y
+  int implx;  // IMPLX: Crank-Nicolson viscous terms along x
 };
 
 // Poisson plan (src/direct.f SAVE state): eigen-transform of the x operator.
@@ -238,6 +239,8 @@ int launch_turvis(eddy_ctx *ctx);
 // INVERSEYD on RS (IMPLY = 1)
 int launch_inversey(eddy_ctx *ctx, double alfxdt);
 int launch_inverseyd(eddy_ctx *ctx, double alfxdt);
+int launch_inversex(eddy_ctx *ctx, double alfxdt);
+int launch_inversexd(eddy_ctx *ctx, double alfxdt);
 // FP32 dynamic procedure on FP32 velocities (row pitch px) -> TV (FP64)
 int launch_turvis32(eddy_ctx *ctx, int px, const float *u, const float *v, const float *w, float *gs32,
                     float *imm32, float *ilm32);

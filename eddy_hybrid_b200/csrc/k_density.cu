@@ -2,11 +2,12 @@
 // fused with DENSITY (src/density.f:6-99) and its sponges, plus the
 // BOUNDINOUTD / BOUNDARY_DENS ghost fills (src/boundary.f:2001-2281).
 // Explicit form: the Crank-Nicolson part RS is zero in the interior and the
-// update, its sponges and the ghost copy run in one pass.  With IMPLY = 1 the
-// y diffusion is the C.N. part: the predicted density goes to RS, INVERSEYD
-// solves its y lines, DENS = RS over the whole array (density.f:96-100, so
-// the ghost cells take RS's, which only BOUNDARY_DENS writes: at slip walls
-// (type 60) the x ghosts become zero, as in the reference), then the sponges.
+// update, its sponges and the ghost copy run in one pass.  With IMPLY = 1
+// (IMPLX = 1) the y (x) diffusion is the C.N. part: the predicted density
+// goes to RS, INVERSEYD (INVERSEXD) solves its lines, DENS = RS over the whole
+// array (density.f:89-104, so the ghost cells take RS's, which only
+// BOUNDARY_DENS writes: at slip walls (type 60) the x ghosts become zero, as
+// in the reference), then the sponges.
 #include "eddy_internal.h"
 #include "tma_ring.cuh"
 #include "bc_templates.cuh"
@@ -40,8 +41,10 @@ __global__ void __launch_bounds__(DTX *DTY)
       });
 }
 
-// IMPLY = 1: RHS_DENSITY with the y diffusion as the C.N. part rt, the
-// DENSITY update with +coef*rt, no sponges yet; the predicted density to rs
+// IMPLY = 1 or IMPLX = 1 (CN bit 0, bit 1): RHS_DENSITY with the diffusion
+// along those axes as the C.N. part rt, the DENSITY update with +coef*rt, no
+// sponges yet; the predicted density to rs
+template <int CN>
 __global__ void __launch_bounds__(DTX *DTY)
     k_density_cn(Dims d, DevMetrics m, const __grid_constant__ TmaMaps<DNF> maps, double *__restrict__ rha,
                  double *__restrict__ rs, double repr1, double alfxdt, double gamxdt, double rhoxdt, int *err) {
@@ -50,7 +53,7 @@ __global__ void __launch_bounds__(DTX *DTY)
       [&](int i, int j, int k, bool active, const RingAcc<DTX, DTY, DNF> &S) {
         if (!active) return;
         double rt = 0.;
-        double rr = rhs_dens<double, DevMetrics, RingAcc<DTX, DTY, DNF>, true>(S, m, repr1, i, j, k, &rt);
+        double rr = rhs_dens<double, DevMetrics, RingAcc<DTX, DTY, DNF>, CN>(S, m, repr1, i, j, k, &rt);
         double coef = 0.5 * alfxdt;
         double dnew = S.at(0, 0, 0, 0) + gamxdt * rr + rhoxdt * S.at(5, 0, 0, 0) + coef * rt;
         long long q = fidx(d, i, j, k);
@@ -118,12 +121,19 @@ int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   }
   size_t smem = ring_smem_bytes<DNF, DTX, DTY>();
   dim3 g((d.ix2 - d.ix1 + DTX) / DTX, (d.jy2 - d.jy1 + DTY) / DTY, (d.kz2 - d.kz1 + DKC) / DKC);
-  if (ctx->sc.imply == 1) {
-    EDDY_CUDA(cudaFuncSetAttribute(k_density_cn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_density_cn<<<g, dim3(DTX, DTY), smem, ctx->stream>>>(d, ctx->m, maps, ctx->f[EDDY_RHA], ctx->f[EDDY_RS],
-                                                          repr1, alfxdt, gamxdt, rhoxdt, ctx->err_flag);
+  const int cn = (ctx->sc.imply == 1 ? 1 : 0) | (ctx->sc.implx == 1 ? 2 : 0);
+  if (cn) {
+    auto kern = cn == 3 ? k_density_cn<3> : cn == 2 ? k_density_cn<2> : k_density_cn<1>;
+    EDDY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<g, dim3(DTX, DTY), smem, ctx->stream>>>(d, ctx->m, maps, ctx->f[EDDY_RHA], ctx->f[EDDY_RS], repr1, alfxdt,
+                                                  gamxdt, rhoxdt, ctx->err_flag);
     EDDY_LAUNCHED(ctx);
-    if ((rc = launch_inverseyd(ctx, alfxdt))) return rc;
+    // INVERSEYD then INVERSEXD on RS, each followed by DENS = RS in the
+    // reference (density.f:89-104); nothing reads DENS between, so one copy
+    if (cn & 1)
+      if ((rc = launch_inverseyd(ctx, alfxdt))) return rc;
+    if (cn & 2)
+      if ((rc = launch_inversexd(ctx, alfxdt))) return rc;
     EDDY_CUDA(cudaMemcpyAsync(ctx->f[EDDY_DENS], ctx->f[EDDY_RS], sizeof(double) * (size_t)d.ncell,
                               cudaMemcpyDeviceToDevice, ctx->stream));
     const long long ni = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);

@@ -1,7 +1,8 @@
 // k_implicit.cu -- Crank-Nicolson viscous terms along the periodic y axis
 // (IMPLY = 1, IMPLYDCMP = 0): INVERSEY (src/timeindeg.f:120-340) on the
 // predicted velocities US, VS, WS and INVERSEYD (src/density.f:383-460) on
-// the predicted density RS.
+// the predicted density RS; and along x (IMPLX = 1, IMPLXDCMP = 0): INVERSEX
+// (src/timeindeg.f:344-690) and INVERSEXD (src/density.f:129-290).
 //
 // Every (i,k) line of a component is one periodic tridiagonal system over the
 // jy1..jy2 cells, (1 + D) x = r with D the C.N. half of the y diffusion.  One
@@ -137,7 +138,149 @@ int lines(eddy_ctx *ctx, const Row &row, int i0, int i1, int k0, int k1, double 
   return EDDY_OK;
 }
 
+// ---- x lines (IMPLX = 1) ----
+// Every (j,k) line is one tridiagonal system over i1..i2 solved by tridag
+// (src/numrec.f:783-802) in its operation order, one thread per line (the
+// threads walk their lines in step; consecutive i of a line share a sector,
+// so the strided rows stay cached).  The boundary tables of
+// src/timeindeg.f:370-434 for one implicit region over the whole x range and
+// slip walls (type 60) on both x boundaries: rdir = 0; u takes its wall
+// value UB = 0 (BOUND060 zeroes the wall-normal velocity, rperb = 1); v, w
+// and the density are Neumann (IBC = -1, src/setup.f:21-40: bdirb = 1,
+// rdirb = 0, rperb = 0), so the first and last rows take b + a and b + c and
+// every right-hand-side correction is a times an exact zero.
+struct RowXU {  // u (timeindeg.f:441-486): viscosity 2 tv(i) and 2 tv(i+1)
+  const double *tv, *au, *ap;
+  double coef, ru1;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double tvip = 2. * tv[fidx(d, i + 1, j, k)] + ru1, tvim = 2. * tv[fidx(d, i, j, k)] + ru1;
+    const double coefx = 1.0 * coef * au[i];
+    a = -coefx * ap[i] * tvim;
+    c = -coefx * ap[i + 1] * tvip;
+    b = 1.0 + (-a - c);
+  }
+};
+struct RowXV {  // v (timeindeg.f:528-560)
+  const double *tv, *av, *au;
+  double coef, ru1;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double tvip = 0.25 * (tv[fidx(d, i, j + 1, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j + 1, k)] +
+                                tv[fidx(d, i + 1, j, k)]) + ru1;
+    const double tvim = 0.25 * (tv[fidx(d, i, j + 1, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i - 1, j + 1, k)] +
+                                tv[fidx(d, i - 1, j, k)]) + ru1;
+    const double coefx = 1.0 * coef * av[i] / 1.0;
+    a = -coefx * au[i - 1] * tvim;
+    c = -coefx * au[i] * tvip;
+    b = 1.0 + (-a - c);
+  }
+};
+struct RowXW {  // w (timeindeg.f:594-626)
+  const double *tv, *aw, *au;
+  double coef, ru1;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double tvip = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j, k + 1)] +
+                                tv[fidx(d, i + 1, j, k)]) + ru1;
+    const double tvim = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i - 1, j, k + 1)] +
+                                tv[fidx(d, i - 1, j, k)]) + ru1;
+    const double coefx = 1.0 * coef * aw[i] / 1.0;
+    a = -coefx * au[i - 1] * tvim;
+    c = -coefx * au[i] * tvip;
+    b = 1.0 + (-a - c);
+  }
+};
+struct RowXD {  // density (density.f:212-240): the molecular diffusivity ru1/prn on both faces
+  const double *aw, *au;
+  double coef, kmol;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+    const double coefx = 1.0 * coef * aw[i] / 1.0;
+    a = -coefx * au[i - 1] * kmol;
+    c = -coefx * au[i] * kmol;
+    b = 1.0 + (-a - c);
+  }
+};
+
+// lines j in [j0, j0+nj), k in [k0, k0+nk); rows i1..i2; NEU: Neumann walls
+// (b + a on the first row, b + c on the last); x: right-hand side in,
+// solution out (in place); gam: scratch field for the multipliers
+template <class Row, bool NEU>
+__global__ void __launch_bounds__(64) k_x_lines(Dims d, Row row, int i1, int i2, int j0, int nj, int k0, int nk,
+                                                double *x, double *gam) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nj * nk) return;
+  const int j = j0 + (int)(t % nj), k = k0 + (int)(t / nj);
+  const long long q1 = fidx(d, i1, j, k);
+  double bet = 1., up = 0., cprev = 0.;
+  for (int i = i1; i <= i2; i++) {
+    const long long q = q1 + (i - i1);
+    double a, b, c;
+    row(d, i, j, k, a, b, c);
+    double r = x[q];
+    if (i == i1) {
+      if (NEU) b = b + 1.0 * a;
+      r = r - a * 0.0;
+    }
+    if (i == i2) {
+      if (NEU) b = b + 1.0 * c;
+      r = r - c * 0.0;
+    }
+    if (i == i1) {
+      bet = b;
+      up = r / bet;
+    } else {
+      const double g = cprev / bet;
+      gam[q] = g;
+      bet = b - a * g;
+      up = (r - a * up) / bet;
+    }
+    x[q] = up;
+    cprev = c;
+  }
+  for (int i = i2 - 1; i >= i1; i--) {
+    const long long q = q1 + (i - i1);
+    up = x[q] - gam[q + 1] * up;
+    x[q] = up;
+  }
+}
+
+template <class Row, bool NEU>
+int xlines(eddy_ctx *ctx, const Row &row, int i1, int i2, int j0, int j1, int k0, int k1, double *x, double *gam) {
+  const int nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+  if (nj <= 0 || nk <= 0 || i2 < i1) return EDDY_OK;
+  const long long nl = (long long)nj * nk;
+  k_x_lines<Row, NEU><<<(unsigned)((nl + 63) / 64), 64, 0, ctx->stream>>>(ctx->d, row, i1, i2, j0, nj, k0, nk, x,
+                                                                          gam);
+  EDDY_LAUNCHED(ctx);
+  return EDDY_OK;
+}
+
 }  // namespace
+
+// INVERSEX: u lines (i in [2, NX-2], j in [jy1, jy2], k in [kz1, kz2]), then v
+// (i in [2, NX-1], j in [jbv, jev]) and w (i in [2, NX-1], k in [kbw, kew]);
+// the v and w systems read US only through the convective terms, which are
+// exact zeros (IMPLCX = 0); REFRESHBC is a no-op on one rank
+int launch_inversex(eddy_ctx *ctx, double alfxdt) {
+  const Dims &d = ctx->d;
+  const DevMetrics &m = ctx->m;
+  double **f = ctx->f;
+  const double coef = 0.5 * alfxdt, ru1 = ctx->sc.ru1;
+  int rc;
+  if ((rc = xlines<RowXU, false>(ctx, RowXU{f[EDDY_TV], m.au, m.ap, coef, ru1}, 2, d.nx - 2, d.jy1, d.jy2, d.kz1,
+                                 d.kz2, f[EDDY_US], f[EDDY_UB])))
+    return rc;
+  if ((rc = xlines<RowXV, true>(ctx, RowXV{f[EDDY_TV], m.av, m.au, coef, ru1}, 2, d.nx - 1, d.jbv, d.jev, d.kz1,
+                                d.kz2, f[EDDY_VS], f[EDDY_VB])))
+    return rc;
+  return xlines<RowXW, true>(ctx, RowXW{f[EDDY_TV], m.aw, m.au, coef, ru1}, 2, d.nx - 1, d.jy1, d.jy2, d.kbw, d.kew,
+                             f[EDDY_WS], f[EDDY_WB]);
+}
+
+// INVERSEXD on RS: i in [2, NX-1], j in [jy1, jy2], k in [kbw, kew]
+int launch_inversexd(eddy_ctx *ctx, double alfxdt) {
+  const Dims &d = ctx->d;
+  return xlines<RowXD, true>(ctx, RowXD{ctx->m.aw, ctx->m.au, 0.5 * alfxdt, ctx->sc.ru1 / ctx->sc.prn}, 2, d.nx - 1,
+                             d.jy1, d.jy2, d.kbw, d.kew, ctx->f[EDDY_RS], ctx->f[EDDY_UB]);
+}
 
 // INVERSEY: v lines (i in [2, NX-1], k in [kz1, kz2]), then w (i in [2, NX-1],
 // k in [kbw, kew]), then u (i in [2, NX-2], k in [kz1, kz2]); REFRESHBC is a

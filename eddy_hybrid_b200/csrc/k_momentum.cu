@@ -31,7 +31,8 @@ struct MomAcc {
   __device__ __forceinline__ double t(int di, int dj, int dk) const { return r.at(3, di, dj, dk); }
 };
 
-template <bool IMPLY>
+// CN: bit 0 IMPLY, bit 1 IMPLX (the C.N. parts of those axes' viscous terms)
+template <int CN>
 __global__ void __launch_bounds__(TX *TY)
     k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const __grid_constant__ TmaMaps<NFLD> maps,
                      double *__restrict__ us, double *__restrict__ vs, double *__restrict__ ws,
@@ -48,8 +49,8 @@ __global__ void __launch_bounds__(TX *TY)
         // ---- u ----
         double uval = 0.0;
         if (kin && jin && i >= d.ibu && i <= d.ieu) {
-          double ucn = 0.0;  // the C.N. part (IMPLY), else 0
-          double ur = rhs_u<double, DevMetrics, MomAcc, IMPLY>(S, m, s.ru1, i, j, k, &ucn);
+          double ucn = 0.0;  // the C.N. part (IMPLY / IMPLX), else 0
+          double ur = rhs_u<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &ucn);
           double ustar = R.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * R.at(6, 0, 0, 0) -
                          alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) + coef * ucn - alfxdt * s.dpdx;
           if (s.idens == 1)
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(TX *TY)
         double vval = 0.0;
         if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
           double vcn = 0.0;
-          double vr = rhs_v<double, DevMetrics, MomAcc, IMPLY>(S, m, s.ru1, i, j, k, &vcn);
+          double vr = rhs_v<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &vcn);
           double vstar = R.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * R.at(7, 0, 0, 0) -
                          alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) + coef * vcn - alfxdt * s.dpdy;
           va[q] = vr;
@@ -80,7 +81,7 @@ __global__ void __launch_bounds__(TX *TY)
         double wval = 0.0;
         if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
           double wcn = 0.0;
-          double wr = rhs_w<double, DevMetrics, MomAcc, IMPLY>(S, m, s.ru1, i, j, k, &wcn);
+          double wr = rhs_w<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &wcn);
           double wstar = R.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * R.at(8, 0, 0, 0) -
                          alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) + coef * wcn - alfxdt * s.dpdz;
           wa[q] = wr;
@@ -138,34 +139,39 @@ __global__ void __launch_bounds__(BX *BY *BZ)
 
 // pref = sum_j (p+dp)(ix1,j,2) / (NY-2), summed in order (src/Eddy6.f:2802)
 // P + DP, then with IMPLY the correction of src/Eddy6.f:2775-2785 (rp = 1,
-// RVIMPLY = 1) on i in [2, ix2], j in [2, jy2], k in [2, kz2]; cimp =
-// 0.5 alfxdt ru1 / dely^2, 0 without IMPLY
-__device__ __forceinline__ double p_plus_dp(const Dims &d, const double *p, const double *dp, long long q, int i,
-                                            int j, int k, double cimp) {
+// RVIMPLY = 1) and with IMPLX that of :2787-2795 (rp = ru = 1, RVIMPLX = 1),
+// both on i in [2, ix2], j in [2, jy2], k in [2, kz2]; cimp = 0.5 alfxdt ru1 /
+// dely^2, 0 without IMPLY; cimpx = 0.5 alfxdt ru1, 0 without IMPLX
+__device__ __forceinline__ double p_plus_dp(const Dims &d, const DevMetrics &m, const double *p, const double *dp,
+                                            long long q, int i, int j, int k, double cimp, double cimpx) {
   double v = p[q] + dp[q];
-  if (cimp != 0.0 && i >= 2 && i <= d.ix2 && j >= 2 && j <= d.jy2 && k >= 2 && k <= d.kz2)
-    v = v - cimp * ((dp[q - d.nx] - 2. * dp[q]) + dp[q + d.nx]) * 1.0;
+  const bool in = i >= 2 && i <= d.ix2 && j >= 2 && j <= d.jy2 && k >= 2 && k <= d.kz2;
+  if (cimp != 0.0 && in) v = v - cimp * ((dp[q - d.nx] - 2. * dp[q]) + dp[q + d.nx]) * 1.0;
+  if (cimpx != 0.0 && in)
+    v = v - cimpx * m.ap[i] / 1.0 *
+                ((dp[q + 1] - dp[q]) * m.au[i] * 1.0 - (dp[q] - dp[q - 1]) * m.au[i - 1] * 1.0) * 1.0;
   return v;
 }
 
-__global__ void k_pref(Dims d, const double *p, const double *dp, double *out, double cimp) {
+__global__ void k_pref(Dims d, DevMetrics m, const double *p, const double *dp, double *out, double cimp,
+                       double cimpx) {
   double s = 0.;
   for (int j = d.jy1; j <= d.jy2; j++) {
     long long q = fidx(d, d.ix1, j, 2);
-    s += p_plus_dp(d, p, dp, q, d.ix1, j, 2, cimp);
+    s += p_plus_dp(d, m, p, dp, q, d.ix1, j, 2, cimp, cimpx);
   }
   out[0] = s / (double)(d.ny - 2);
 }
 
 __global__ void __launch_bounds__(256)
-    k_pupdate(Dims d, double *p, const double *dp, const double *pref, double cimp) {
+    k_pupdate(Dims d, DevMetrics m, double *p, const double *dp, const double *pref, double cimp, double cimpx) {
   // blockIdx.y is the plane k; 32-bit index arithmetic inside the plane
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = d.nx * d.ny;
   if (t >= n2) return;
   const int k = 1 + blockIdx.y, j = 1 + t / d.nx, i = 1 + (t - (j - 1) * d.nx);
   const long long q = (long long)blockIdx.y * n2 + t;
-  p[q] = p_plus_dp(d, p, dp, q, i, j, k, cimp) - pref[0];
+  p[q] = p_plus_dp(d, m, p, dp, q, i, j, k, cimp, cimpx) - pref[0];
 }
 
 // final pressure ghosts: value of the mapped interior cell (the composition
@@ -232,7 +238,9 @@ int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rh
   }
   size_t smem = ring_smem_bytes<NFLD, TX, TY>();
   dim3 g((d.ix2 - d.ix1 + TX) / TX, (d.jy2 - d.jy1 + TY) / TY, (d.kz2 - d.kz1 + KCHUNK) / KCHUNK);
-  auto kern = ctx->sc.imply == 1 ? k_rhs_predictord<true> : k_rhs_predictord<false>;
+  const int cn = (ctx->sc.imply == 1 ? 1 : 0) | (ctx->sc.implx == 1 ? 2 : 0);
+  auto kern = cn == 3 ? k_rhs_predictord<3> : cn == 2 ? k_rhs_predictord<2> : cn == 1 ? k_rhs_predictord<1>
+                                                                                     : k_rhs_predictord<0>;
   EDDY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<g, dim3(TX, TY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, f[EDDY_US], f[EDDY_VS], f[EDDY_WS],
                                               f[EDDY_UA], f[EDDY_VA], f[EDDY_WA], alfxdt, gamxdt, rhoxdt,
@@ -272,10 +280,11 @@ int launch_pressure_update(eddy_ctx *ctx) {
   double *p = ctx->f[EDDY_P], *dp = ctx->f[EDDY_DP];
   const double cimp = ctx->sc.imply == 1 ? 0.5 * ctx->alfxdt_last * ctx->sc.ru1 / ((ctx->dely * 1.0) * (ctx->dely * 1.0))
                                          : 0.0;
-  k_pref<<<1, 1, 0, ctx->stream>>>(d, p, dp, ctx->scal, cimp);
+  const double cimpx = ctx->sc.implx == 1 ? 0.5 * ctx->alfxdt_last * ctx->sc.ru1 : 0.0;
+  k_pref<<<1, 1, 0, ctx->stream>>>(d, ctx->m, p, dp, ctx->scal, cimp, cimpx);
   EDDY_LAUNCHED(ctx);
-  k_pupdate<<<dim3((unsigned)((d.nx * d.ny + 255) / 256), (unsigned)d.nz), 256, 0, ctx->stream>>>(d, p, dp, ctx->scal,
-                                                                                                   cimp);
+  k_pupdate<<<dim3((unsigned)((d.nx * d.ny + 255) / 256), (unsigned)d.nz), 256, 0, ctx->stream>>>(
+      d, ctx->m, p, dp, ctx->scal, cimp, cimpx);
   EDDY_LAUNCHED(ctx);
   // immersed body: correctpres_mod2 + presinterior (src/Eddy6.f:2881-2897)
   if (ctx->ib) {

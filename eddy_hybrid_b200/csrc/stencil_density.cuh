@@ -1,12 +1,13 @@
 // stencil_density.cuh -- density right-hand side of src/rhs_density.f:55-165
-// (Cartesian; CN = true: IMPLY = 1, the y diffusion returned as the
-// Crank-Nicolson part in *cn), templated on the arithmetic type T and on
+// (Cartesian; CN bit 0: IMPLY = 1, bit 1: IMPLX = 1, the diffusion along those
+// axes returned as the Crank-Nicolson part in *cn), templated on the arithmetic type T and on
 // a neighbour accessor: S.at(f, di, dj, dk) with f = 0 density, 1 eddy
 // diffusivity, 2 u, 3 v, 4 w.  With T = double the operation order is the
 // reference's (the plain form is compiled with -fmad=false).
 #pragma once
+#include "stencil_cn.cuh"
 
-template <class T, class M, class Acc, bool CN = false>
+template <class T, class M, class Acc, int CN = 0>
 __device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, int j, int k, T *cn = nullptr) {
   auto dens = [&](int a, int b, int c) { return S.at(0, a, b, c); };
   auto kv = [&](int a, int b, int c) { return S.at(1, a, b, c); };
@@ -44,9 +45,10 @@ __device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, 
   T t22 = m.bp[j] * (tyyp - tyym);
   T t33 = m.cp[k] * (tzzp - tzzm);
   if (CN) {
-    // IMPLY = 1 (src/rhs_density.f:149-156): the y diffusion is the C.N. part
-    *cn = t22;
-    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33;
+    // src/rhs_density.f:147-156: the diffusion along the implicit axes is the
+    // C.N. part
+    *cn = cn_part<T, CN>(t11, t22);
+    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33;
   }
   return h11 + h22 + h33 + t11 + t22 + t33;
 }

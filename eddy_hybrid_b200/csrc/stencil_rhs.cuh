@@ -1,15 +1,16 @@
 // stencil_rhs.cuh -- explicit momentum right-hand side of src/rhs.f:4-438
-// (Cartesian; CN = true: IMPLY = 1, the y viscous term returned as the
-// Crank-Nicolson part in *cn), templated on the arithmetic type T and on a
-// neighbour accessor: S.u/v/w/t(di,dj,dk) return uo/vo/wo/tv at the offset
-// from the current cell.  With T = double the operation order is exactly the
-// reference's (the plain form is compiled with -fmad=false); with T = float
-// the mixed form accumulates in FP32.
+// (Cartesian; CN bit 0: IMPLY = 1, bit 1: IMPLX = 1, the viscous terms along
+// those axes returned as the Crank-Nicolson part in *cn), templated on the
+// arithmetic type T and on a neighbour accessor: S.u/v/w/t(di,dj,dk) return
+// uo/vo/wo/tv at the offset from the current cell.  With T = double the
+// operation order is exactly the reference's (the plain form is compiled with
+// -fmad=false); with T = float the mixed form accumulates in FP32.
 #pragma once
+#include "stencil_cn.cuh"
 
 // ---------------------------------------------------------------------------
 // u-momentum explicit RHS at a u point (src/rhs.f:77-172)
-template <class T, class M, class Acc, bool CN = false>
+template <class T, class M, class Acc, int CN = 0>
 __device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
   T qxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * T(0.5);
   T qxm = (S.u(0, 0, 0) + S.u(-1, 0, 0)) * T(0.5);
@@ -56,15 +57,17 @@ __device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j
   T s22 = m.bu[j] * (txyp - txym);
   T s33 = m.cu[k] * (txzp - txzm);
   if (CN) {
-    // IMPLY = 1 (src/rhs.f:175-191): the y viscous term is the C.N. part
-    *cn = t22;
-    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33 + s22 + s33;
+    // src/rhs.f:175-191: the viscous terms along the implicit axes are the
+    // C.N. part (rflagx = IMPLX, rflagy = IMPLY, ruimplx = ruimply = 1)
+    *cn = cn_part<T, CN>(t11, t22);
+    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33 +
+           s22 + s33;
   }
   return h11 + h22 + h33 + t11 + t22 + t33 + s22 + s33;
 }
 
 // v-momentum (src/rhs.f:219-321)
-template <class T, class M, class Acc, bool CN = false>
+template <class T, class M, class Acc, int CN = 0>
 __device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
   T vxp = (S.v(1, 0, 0) + S.v(0, 0, 0)) * T(0.5);
   T vxm = (S.v(0, 0, 0) + S.v(-1, 0, 0)) * T(0.5);
@@ -109,14 +112,15 @@ __device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j
   T s11 = m.av[i] * (txyp - txym);
   T s33 = m.cv[k] * (tyzp - tyzm);
   if (CN) {
-    *cn = t22;
-    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33 + s11 + s33;
+    *cn = cn_part<T, CN>(t11, t22);
+    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33 +
+           s11 + s33;
   }
   return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s33;
 }
 
 // w-momentum (src/rhs.f:347-422)
-template <class T, class M, class Acc, bool CN = false>
+template <class T, class M, class Acc, int CN = 0>
 __device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
   T wxp = (S.w(1, 0, 0) + S.w(0, 0, 0)) * T(0.5);
   T wxm = (S.w(0, 0, 0) + S.w(-1, 0, 0)) * T(0.5);
@@ -161,8 +165,9 @@ __device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j
   T s11 = m.aw[i] * (txzp - txzm);
   T s22 = m.bw[j] * (tyzp - tyzm);
   if (CN) {
-    *cn = t22;
-    return h11 + h22 + h33 + t11 + (T(1.) - T(1.)) * t22 + t33 + s11 + s22;
+    *cn = cn_part<T, CN>(t11, t22);
+    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33 +
+           s11 + s22;
   }
   return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s22;
 }

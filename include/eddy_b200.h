@@ -63,8 +63,13 @@ typedef struct {
                                 Crank-Nicolson implicit (INVERSEY src/timeindeg.f:120,
                                 INVERSEYD src/density.f:383), over the whole x range
                                 (IMPLYDCMP = 0); plain form without an immersed body.
-                                The implicit convective and x terms (IMPLCY, IMPLX,
-                                IMPLCX) are not supported. */
+                                The implicit convective terms (IMPLCY, IMPLCX) are
+                                not supported. */
+  int implx;                 /* IMPLX: 1 = the viscous terms along x Crank-Nicolson
+                                implicit (INVERSEX src/timeindeg.f:344, INVERSEXD
+                                src/density.f:129) over the whole x range
+                                (IMPLXDCMP = 0), with slip walls (type 60) on both
+                                x boundaries; plain form without an immersed body. */
 } eddy_params;
 
 typedef struct eddy_ctx eddy_ctx;
@@ -140,6 +145,11 @@ int eddy_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhox
  * WS after the predictor, viscous part (imply = 1 only).  The density's
  * INVERSEYD (src/density.f:383) runs inside eddy_density when imply = 1. */
 int eddy_inversey(eddy_ctx *ctx, double alfxdt);
+/* INVERSEX (src/timeindeg.f:344-690): the Crank-Nicolson x lines of US, then
+ * VS and WS, viscous part (implx = 1 only; after eddy_inversey when both are
+ * on, as src/Eddy6.f:2597-2607 orders them).  INVERSEXD (src/density.f:129)
+ * runs inside eddy_density when implx = 1. */
+int eddy_inversex(eddy_ctx *ctx, double alfxdt);
 /* BOUNDARY (src/boundary.f:7) on the provisional (set=0: US,VS,WS) or the
  * corrected (set=1: UO,VO,WO) velocity. */
 int eddy_boundary(eddy_ctx *ctx, int set);

@@ -41,6 +41,7 @@ typedef struct {
   double css;              /* Smagorinsky constant */
   int vspngx1, dspngx1, vspngx3in, vspngx3out, dspngx3in, dspngx3out;
   int imply;               /* 1: Crank-Nicolson viscous terms along y (INVERSEY/INVERSEYD) */
+  int implx;               /* 1: Crank-Nicolson viscous terms along x (INVERSEX/INVERSEXD) */
 } eo_params;
 
 /* 1-D metric arrays (src/common.h:51-54), 1-based: arrays have n+1 entries. */
@@ -130,6 +131,9 @@ void eo_inversey(eo_state *s, double alfxdt);
 /* CALCFL (src/timestep.f:2-78): CFLM over the interior */
 double eo_calcfl(eo_state *s);
 void eo_inverseyd(eo_state *s, double alfxdt);
+void eo_inversex_walls(eo_state *s, double alfxdt);
+void eo_inversex(eo_state *s, double alfxdt);
+void eo_inversexd(eo_state *s, double alfxdt);
 /* periodic tridiagonal system (cyclic, src/numrec.f:754-779): n unknowns,
  * a sub-, b main, c super-diagonal, alpha = A(n,1), beta = A(1,n); work >= 4n */
 void eo_cyclic(const double *a, const double *b, const double *c, double alpha, double beta, const double *r,

@@ -32,7 +32,8 @@ class Params(C.Structure):
                 ("dpdy", C.c_double), ("dpdz", C.c_double), ("eps", C.c_double),
                 ("css", C.c_double), ("vspngx1", C.c_int), ("dspngx1", C.c_int),
                 ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
-                ("dspngx3in", C.c_int), ("dspngx3out", C.c_int), ("imply", C.c_int)]
+                ("dspngx3in", C.c_int), ("dspngx3out", C.c_int), ("imply", C.c_int),
+                ("implx", C.c_int)]
 
 
 class IBSet(C.Structure):
@@ -95,6 +96,8 @@ def lib():
         L.eo_rhs_density.argtypes = [C.c_void_p]
         L.eo_call_rhs_predictord.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
         L.eo_inversey.argtypes = [C.c_void_p, C.c_double]
+        L.eo_inversex.argtypes = [C.c_void_p, C.c_double]
+        L.eo_inversex_walls.argtypes = [C.c_void_p, C.c_double]
         L.eo_calcfl.argtypes = [C.c_void_p]
         L.eo_calcfl.restype = C.c_double
         L.eo_call_density.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
@@ -248,6 +251,13 @@ class OracleSolver:
 
     def inversey(self, alf):
         lib().eo_inversey(self.h, alf)
+
+    def inversex_walls(self, alf):
+        """UB, VB, WB wall planes before the line solves (src/Eddy6.f:2582-2591)."""
+        lib().eo_inversex_walls(self.h, alf)
+
+    def inversex(self, alf):
+        lib().eo_inversex(self.h, alf)
 
     def calcfl(self) -> float:
         return lib().eo_calcfl(self.h)

@@ -112,7 +112,8 @@ int eo_get(eo_state *s, int id, double *dst) {
 }
 
 /* ------------------------------------------------------------------------
- * RHS: src/rhs.f:4-438 (icyl=0, all rflag* = 0 so the C.N. parts vanish).
+ * RHS: src/rhs.f:4-438 (icyl=0; rflagx = IMPLX, rflagy = IMPLY, the
+ * convective flags 0: ut,vt,wt take the C.N. viscous parts).
  * ut,vt,wt and ur,vr,wr are zeroed over the whole array first (rhs.f:65-70);
  * qr = uo (rhs.f:58).
  * ---------------------------------------------------------------------- */
@@ -125,8 +126,9 @@ void eo_rhs(eo_state *s, const double *uo, const double *vo, const double *wo,
   const double *bp = g->bp, *bu = g->bu, *bv = g->bv, *bw = g->bw;
   const double *cp = g->cp, *cu = g->cu, *cv = g->cv, *cw = g->cw;
   long n = s->ncell;
-  /* rflag* of src/rhs.f:49-52 with ruimply = rvimply = 1 (IMPLYDCMP = 0) */
-  const double rflagx = 0., rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
+  /* rflag* of src/rhs.f:49-52 with ruimplx = rvimplx = ruimply = rvimply = 1
+   * (IMPLXDCMP = IMPLYDCMP = 0) */
+  const double rflagx = (double)s->prm.implx, rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
   memcpy(qr, uo, sizeof(double) * (size_t)n);
   memset(ut, 0, sizeof(double) * (size_t)n); memset(ur, 0, sizeof(double) * (size_t)n);
   memset(vt, 0, sizeof(double) * (size_t)n); memset(vr, 0, sizeof(double) * (size_t)n);
@@ -599,6 +601,18 @@ void eo_pressure_update(eo_state *s) {
           A(p, i, j, k) = A(p, i, j, k) -
                           c * ((A(dp, i, j - 1, k) - 2. * A(dp, i, j, k)) + A(dp, i, j + 1, k)) * 1.0;
   }
+  /* implicit x terms (src/Eddy6.f:2787-2795; rp = ru = 1, RVIMPLX = 1) */
+  if (s->prm.implx == 1) {
+    const double c = 0.5 * s->alfxdt_last * s->prm.ru1;
+#pragma omp parallel for schedule(static)
+    for (int k = 2; k <= g->kz2; k++)
+      for (int j = 2; j <= g->jy2; j++)
+        for (int i = 2; i <= g->ix2; i++)
+          A(p, i, j, k) = A(p, i, j, k) - c * g->ap[i] / 1.0 *
+                                              ((A(dp, i + 1, j, k) - A(dp, i, j, k)) * g->au[i] * 1.0 -
+                                               (A(dp, i, j, k) - A(dp, i - 1, j, k)) * g->au[i - 1] * 1.0) *
+                                              1.0;
+  }
   double pref = 0.;
   for (int j = g->jy1; j <= g->jy2; j++) pref += A(p, g->ix1, j, 2);
   pref = pref / (double)(NY - 2);
@@ -636,7 +650,7 @@ void eo_rhs_density(eo_state *s) {
   double *uo = s->uo, *vo = s->vo, *wo = s->wo, *dens = s->dens, *kv = s->tv;
   double *rr = s->rhb, *rt = s->rs;
   double repr1 = s->prm.ru1 / s->prm.prn;
-  const double rflagx = 0., rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
+  const double rflagx = (double)s->prm.implx, rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
   memset(rr, 0, sizeof(double) * (size_t)s->ncell);
 #pragma omp parallel for schedule(static)
   for (int k = g->kz1; k <= g->kz2; k++)
@@ -725,7 +739,8 @@ void eo_boundinoutd(eo_state *s, double *d) {
   if (it[6] == 710) fill_z_plane(g, d, g->kz2, g->kz2 - 1, 1., 0);
 }
 
-/* DENSITY: src/density.f:6-127 (explicit: no INVERSEYD/INVERSEXD) */
+/* DENSITY: src/density.f:6-127 (INVERSEYD with IMPLY = 1, INVERSEXD with
+ * IMPLX = 1) */
 void eo_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
   const eo_grid *g = s->g;
   double *dens = s->dens, *rha = s->rha, *rhb = s->rhb, *rs = s->rs;
@@ -746,6 +761,11 @@ void eo_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
    * ghost cells take RS's, which nothing above writes but BOUNDARY_DENS */
   if (s->prm.imply == 1) {
     eo_inverseyd(s, alfxdt);
+    memcpy(dens, rs, sizeof(double) * (size_t)s->ncell);
+  }
+  /* implicit x diffusion (density.f:101-104) */
+  if (s->prm.implx == 1) {
+    eo_inversexd(s, alfxdt);
     memcpy(dens, rs, sizeof(double) * (size_t)s->ncell);
   }
   if (g->idspngl == 1) {
@@ -906,5 +926,209 @@ void eo_inverseyd(eo_state *s, double alfxdt) {
         for (int j = g->jy1; j <= g->jy2; j++) A(rs, i, j, k) = x[j - 2];
       }
     free(ay); free(by); free(cy); free(ry); free(x); free(wk);
+  }
+}
+
+/* ---- Crank-Nicolson x lines ----
+ * Boundary tables of INVERSEX / INVERSEXD (src/timeindeg.f:370-434,
+ * src/density.f:150-204) for the one implicit region of IMPLXDCMP = 0
+ * (i1 = 2 = IBU, i2 = NX-1 = IX2, src/inpall.f:703-709) and non-periodic x:
+ * rdir = 0 on both sides; u takes its wall value from UB (rperb = 1); v and w
+ * (and the density, on w's row) are Dirichlet (rdirb 2, bdirb -1) where
+ * IBC = 1 and Neumann (rdirb 0, bdirb 1) otherwise, IBC as src/setup.f:18-49
+ * sets it from ITYPE.  Index [q][side], q = 0 u, 1 v, 2 w. */
+typedef struct {
+  double rdir[3][2], rperb[3][2], rdirb[3][2], bdirb[3][2], bneub[3][2];
+} xbc_tables;
+
+static int ibc_of(int itype, int side, int q) {
+  if (side == 0) {
+    if (itype == 50 || itype == 300) return 1;
+    if (itype == 60) return q == 0 ? 1 : -1;
+    if (itype == 81) return q == 1 ? -1 : 1;
+    return 1;
+  }
+  if (itype == 50) return 1;
+  if (itype == 60 || itype == 80) return q == 0 ? 1 : -1;
+  if (itype == 81) return q == 1 ? -1 : 1;
+  return 1;
+}
+
+static void x_tables(const eo_state *s, xbc_tables *t) {
+  for (int q = 0; q < 3; q++)
+    for (int sd = 0; sd < 2; sd++) {
+      t->rdir[q][sd] = 0.;
+      t->rperb[q][sd] = q == 0 ? 1. : 0.;
+      t->bneub[q][sd] = 0.;
+      if (q == 0) {
+        t->rdirb[q][sd] = 0.;
+        t->bdirb[q][sd] = 0.;
+      } else if (ibc_of(s->prm.itype[1 + sd], sd, q) == 1) {
+        t->rdirb[q][sd] = 2.;
+        t->bdirb[q][sd] = -1.;
+      } else {
+        t->rdirb[q][sd] = 0.;
+        t->bdirb[q][sd] = 1.;
+      }
+    }
+}
+
+/* the boundary planes of UB, VB, WB before the x lines, IBM = 0
+ * (src/Eddy6.f:2582-2591): UB(IX1) = US(IX1) + alfxdt/2 UB(IX1), the same at
+ * IX2 and for v, w, then BOUNDARY twice; UB.. hold the C.N. parts of RHS */
+void eo_inversex_walls(eo_state *s, double alfxdt) {
+  const eo_grid *g = s->g;
+  double *b[3] = {s->ub, s->vb, s->wb};
+  const double *st[3] = {s->us, s->vs, s->ws};
+  const int is[2] = {g->ix1, g->ix2};
+  for (int q = 0; q < 3; q++)
+    for (int e = 0; e < 2; e++)
+      for (int k = 1; k <= NZ; k++)
+        for (int j = 1; j <= NY; j++) A(b[q], is[e], j, k) = A(st[q], is[e], j, k) + 0.5 * alfxdt * A(b[q], is[e], j, k);
+  eo_boundary(s, s->ub, s->vb, s->wb);
+  eo_boundary(s, s->ub, s->vb, s->wb);
+}
+
+/* INVERSEX (src/timeindeg.f:344-690), viscous part (implcx = 0: the
+ * convective coefficients and right-hand-side terms are exact zeros),
+ * Cartesian (rp = ru = 1), IMPLXDCMP = 0: u lines for i in [2, NX-2], then
+ * v lines (j in [jbv, jev]) and w lines (k in [kbw, kew]) for i in [2, NX-1];
+ * tridag (src/numrec.f:783-802) on each.  REFRESHBC is a no-op on one rank
+ * with non-periodic z. */
+void eo_inversex(eo_state *s, double alfxdt) {
+  const eo_grid *g = s->g;
+  const double coef = 0.5 * alfxdt, ru1 = s->prm.ru1, rflagx = 1.0;
+  double *us = s->us, *vs = s->vs, *ws = s->ws;
+  const double *ub = s->ub, *vb = s->vb, *wb = s->wb, *tv = s->tv;
+  const double *ap = g->ap, *au = g->au, *av = g->av, *aw = g->aw;
+  xbc_tables t;
+  x_tables(s, &t);
+  const int nmax = NX;
+#pragma omp parallel
+  {
+    double *ax = malloc(sizeof(double) * nmax), *bx = malloc(sizeof(double) * nmax),
+           *cx = malloc(sizeof(double) * nmax), *rx = malloc(sizeof(double) * nmax),
+           *x = malloc(sizeof(double) * nmax), *gam = malloc(sizeof(double) * nmax);
+    /* u */
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kz1; k <= g->kz2; k++)
+      for (int j = g->jy1; j <= g->jy2; j++) {
+        const int i1 = 2, i2 = NX - 2, n = i2 - i1 + 1;
+        for (int i = i1; i <= i2; i++) {
+          const int ii = i - i1;
+          const double tvip = 2. * A(tv, i + 1, j, k) + ru1, tvim = 2. * A(tv, i, j, k) + ru1;
+          rx[ii] = A(us, i, j, k);
+          const double coefx = rflagx * coef * au[i];
+          const double axv = -coefx * ap[i] * tvim, cxv = -coefx * ap[i + 1] * tvip, bxv = -axv - cxv;
+          ax[ii] = axv;
+          cx[ii] = cxv;
+          bx[ii] = 1.0 + bxv;
+        }
+        rx[0] = rx[0] - ax[0] * (A(us, i1 - 1, j, k) * t.rdir[0][0] + A(ub, i1 - 1, j, k) * t.rperb[0][0]);
+        rx[n - 1] =
+            rx[n - 1] - cx[n - 1] * (A(us, i2 + 1, j, k) * t.rdir[0][1] + A(ub, i2 + 1, j, k) * t.rperb[0][1]);
+        thomas(ax, bx, cx, rx, x, n, gam);
+        for (int i = i1; i <= i2; i++) A(us, i, j, k) = x[i - i1];
+      }
+    /* v */
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kz1; k <= g->kz2; k++)
+      for (int j = g->jbv; j <= g->jev; j++) {
+        const int i1 = 2, i2 = NX - 1, n = i2 - i1 + 1;
+        for (int i = i1; i <= i2; i++) {
+          const int ii = i - i1;
+          const double tvip =
+              0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i + 1, j + 1, k) + A(tv, i + 1, j, k)) + ru1;
+          const double tvim =
+              0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i - 1, j + 1, k) + A(tv, i - 1, j, k)) + ru1;
+          rx[ii] = A(vs, i, j, k);
+          const double coefx = rflagx * coef * av[i] / 1.0;
+          const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
+          ax[ii] = axv;
+          cx[ii] = cxv;
+          bx[ii] = 1.0 + bxv;
+        }
+        bx[0] = bx[0] + (t.bdirb[1][0] + t.bneub[1][0]) * ax[0];
+        bx[n - 1] = bx[n - 1] + (t.bdirb[1][1] + t.bneub[1][1]) * cx[n - 1];
+        rx[0] = rx[0] - ax[0] * (A(vs, i1 - 1, j, k) * t.rdir[1][0] + A(vb, i1 - 1, j, k) * t.rperb[1][0] +
+                                 0.5 * (A(vb, i1, j, k) + A(vb, i1 - 1, j, k)) * t.rdirb[1][0]);
+        rx[n - 1] = rx[n - 1] - cx[n - 1] * (A(vs, i2 + 1, j, k) * t.rdir[1][1] + A(vb, i2 + 1, j, k) * t.rperb[1][1] +
+                                             0.5 * (A(vb, i2, j, k) + A(vb, i2 + 1, j, k)) * t.rdirb[1][1]);
+        thomas(ax, bx, cx, rx, x, n, gam);
+        for (int i = i1; i <= i2; i++) A(vs, i, j, k) = x[i - i1];
+      }
+    /* w */
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kbw; k <= g->kew; k++)
+      for (int j = g->jy1; j <= g->jy2; j++) {
+        const int i1 = 2, i2 = NX - 1, n = i2 - i1 + 1;
+        for (int i = i1; i <= i2; i++) {
+          const int ii = i - i1;
+          const double tvip =
+              0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i + 1, j, k + 1) + A(tv, i + 1, j, k)) + ru1;
+          const double tvim =
+              0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i - 1, j, k + 1) + A(tv, i - 1, j, k)) + ru1;
+          rx[ii] = A(ws, i, j, k);
+          const double coefx = rflagx * coef * aw[i] / 1.0;
+          const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
+          ax[ii] = axv;
+          cx[ii] = cxv;
+          bx[ii] = 1.0 + bxv;
+        }
+        bx[0] = bx[0] + (t.bdirb[2][0] + t.bneub[2][0]) * ax[0];
+        bx[n - 1] = bx[n - 1] + (t.bdirb[2][1] + t.bneub[2][1]) * cx[n - 1];
+        rx[0] = rx[0] - ax[0] * (A(ws, i1 - 1, j, k) * t.rdir[2][0] + A(wb, i1 - 1, j, k) * t.rperb[2][0] +
+                                 0.5 * (A(wb, i1, j, k) + A(wb, i1 - 1, j, k)) * t.rdirb[2][0]);
+        rx[n - 1] = rx[n - 1] - cx[n - 1] * (A(ws, i2 + 1, j, k) * t.rdir[2][1] + A(wb, i2 + 1, j, k) * t.rperb[2][1] +
+                                             0.5 * (A(wb, i2, j, k) + A(wb, i2 + 1, j, k)) * t.rdirb[2][1]);
+        thomas(ax, bx, cx, rx, x, n, gam);
+        for (int i = i1; i <= i2; i++) A(ws, i, j, k) = x[i - i1];
+      }
+    free(ax); free(bx); free(cx); free(rx); free(x); free(gam);
+  }
+}
+
+/* INVERSEXD (src/density.f:129-290) on RS with RHB (the explicit predicted
+ * density after BOUNDARY_DENS) for the wall values: k in [kbw, kew],
+ * i in [2, NX-1], w's boundary row, and, as there, the molecular diffusivity
+ * ru1/prn alone on both faces (the eddy diffusivity's x part, dropped from
+ * the explicit right-hand side with IMPLX = 1, is not restored here) */
+void eo_inversexd(eo_state *s, double alfxdt) {
+  const eo_grid *g = s->g;
+  const double coef = 0.5 * alfxdt, rflagx = 1.0, kmol = s->prm.ru1 / s->prm.prn;
+  double *rs = s->rs;
+  const double *rhb = s->rhb, *au = g->au, *aw = g->aw;
+  xbc_tables t;
+  x_tables(s, &t);
+  const int nmax = NX;
+#pragma omp parallel
+  {
+    double *ax = malloc(sizeof(double) * nmax), *bx = malloc(sizeof(double) * nmax),
+           *cx = malloc(sizeof(double) * nmax), *rx = malloc(sizeof(double) * nmax),
+           *x = malloc(sizeof(double) * nmax), *gam = malloc(sizeof(double) * nmax);
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kbw; k <= g->kew; k++)
+      for (int j = g->jy1; j <= g->jy2; j++) {
+        const int i1 = 2, i2 = NX - 1, n = i2 - i1 + 1;
+        for (int i = i1; i <= i2; i++) {
+          const int ii = i - i1;
+          const double tvip = kmol, tvim = kmol;
+          rx[ii] = A(rs, i, j, k);
+          const double coefx = rflagx * coef * aw[i] / 1.0;
+          const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
+          ax[ii] = axv;
+          cx[ii] = cxv;
+          bx[ii] = 1.0 + bxv;
+        }
+        bx[0] = bx[0] + (t.bdirb[2][0] + t.bneub[2][0]) * ax[0];
+        bx[n - 1] = bx[n - 1] + (t.bdirb[2][1] + t.bneub[2][1]) * cx[n - 1];
+        rx[0] = rx[0] - ax[0] * (A(rs, i1 - 1, j, k) * t.rdir[2][0] + A(rhb, i1 - 1, j, k) * t.rperb[2][0] +
+                                 0.5 * (A(rhb, i1, j, k) + A(rhb, i1 - 1, j, k)) * t.rdirb[2][0]);
+        rx[n - 1] = rx[n - 1] - cx[n - 1] * (A(rs, i2 + 1, j, k) * t.rdir[2][1] + A(rhb, i2 + 1, j, k) * t.rperb[2][1] +
+                                             0.5 * (A(rhb, i2, j, k) + A(rhb, i2 + 1, j, k)) * t.rdirb[2][1]);
+        thomas(ax, bx, cx, rx, x, n, gam);
+        for (int i = i1; i <= i2; i++) A(rs, i, j, k) = x[i - i1];
+      }
+    free(ax); free(bx); free(cx); free(rx); free(x); free(gam);
   }
 }

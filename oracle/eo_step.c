@@ -46,8 +46,10 @@ void eo_substep(eo_state *s, int is, double dtm1) {
     eo_ib_interior(s->ib, 1, s->vs, vel[1]);
     eo_ib_interior(s->ib, 2, s->ws, vel[2]);
   }
-  /* Crank-Nicolson y lines (:2596-2599; the IBM = 0 sequence) */
+  /* Crank-Nicolson y, then x lines (:2582-2607; the IBM = 0 sequence) */
+  if (s->prm.implx == 1) eo_inversex_walls(s, alfxdt);
   if (s->prm.imply == 1) eo_inversey(s, alfxdt);
+  if (s->prm.implx == 1) eo_inversex(s, alfxdt);
   /* :2689-2704 */
   eo_boundary(s, s->us, s->vs, s->ws);
   eo_boundinout(s, s->us, s->vs, s->ws, s->uo, s->vo, s->wo, alfxdt, 1);
@@ -234,10 +236,11 @@ double eo_max_divergence(eo_state *s) {
 }
 
 /* CALCFL (src/timestep.f:2-78), Cartesian: CONST = 2, rp = 1, the implicit
- * flags RFLAGY = IMPLY, the others 0; returns CFLM over the interior */
+ * flags RFLAGX = IMPLX, RFLAGY = IMPLY, the convective ones 0; returns CFLM
+ * over the interior */
 double eo_calcfl(eo_state *s) {
   const eo_grid *g = s->g;
-  const double cst = 2., rflagx = 0., rflagcx = 0., rflagcy = 0., rflagy = (double)s->prm.imply;
+  const double cst = 2., rflagx = (double)s->prm.implx, rflagcx = 0., rflagcy = 0., rflagy = (double)s->prm.imply;
   const int nx = g->nx, ny = g->ny;
   double cflm = 0.;
   for (int k = g->kz1; k <= g->kz2; k++)

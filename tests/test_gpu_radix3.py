@@ -23,7 +23,7 @@ def _rhs(o, w, seed=7):
     return d
 
 
-@pytest.mark.parametrize("ly", [12, 24, 48, 96])
+@pytest.mark.parametrize("ly", [12, 24, 48, 96, 384])
 def test_poisson_radix3_plain_and_mixed(oracle, product, ly):
     w = config.small(mx=32, ly=ly, nz_=20, beta=2.5)
     o = oracle.OracleSolver(w)

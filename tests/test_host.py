@@ -64,6 +64,16 @@ def test_create_fails_cleanly_without_valid_config(product):
     w.itype = (60, 60, 60, 60, 305, 730)   # y not periodic: refused
     with pytest.raises(product.EddyError):
         product.Solver(w)
+    # the implicit x terms are built for slip walls on both x sides and the
+    # plain FP64 form only: anything else is refused before any device work
+    for kw in ({"implx": 1, "itype": (60, 82, 500, 500, 305, 730)}, {"implx": 2}):
+        w = config.small(mx=12, ly=8, nz_=16)
+        for k, v in kw.items():
+            setattr(w, k, v)
+        with pytest.raises(product.EddyError):
+            product.Solver(w)
+    with pytest.raises(product.EddyError):
+        product.Solver(config.small(mx=12, ly=8, nz_=16, implx=1), precision=product.MIXED)
 
 
 def test_download_checks_the_callers_buffer_before_copying(product):

@@ -51,3 +51,73 @@ def test_implicit_y_step_is_projected_and_close_to_explicit(oracle):
         # same equations, Crank-Nicolson instead of explicit y diffusion: an
         # O(dt^2) difference, not zero and not large
         assert 0 < d < 5e-3, (n, d)
+
+
+def _xpair(oracle, implx, imply, steps):
+    w = config.small(mx=16, ly=16, nz_=24, noise=0.2, re=500.0, imply=imply, implx=implx)
+    o = oracle.OracleSolver(w)
+    o.load_initial(config.initial_fields(w, o.grid.get("dens_bg")[: w.nx]))
+    o.initialize()
+    o.step(steps)
+    return o
+
+
+def test_inversex_lines_solve_their_systems(oracle):
+    # every x line after INVERSEX satisfies the Crank-Nicolson system of
+    # src/timeindeg.f:441-686 as a numpy restatement assembles it: u with
+    # zero wall values at i = 1 and NX-1, v and w with Neumann walls
+    w = config.small(mx=16, ly=8, nz_=12, noise=0.3, re=50.0, implx=1)
+    o = oracle.OracleSolver(w)
+    o.load_initial(config.initial_fields(w, o.grid.get("dens_bg")[: w.nx]))
+    o.initialize()
+    rng = np.random.default_rng(5)
+    tv = np.abs(rng.standard_normal((w.nx, w.ny, w.nz))) * 1e-2
+    o.set("tv", np.asfortranarray(tv))
+    alf = 2 / 15 * 1e-2
+    o.rhs_predictord(alf, 5 / 12 * 1e-2, -17 / 60 * 1e-2)
+    before = {n: o.get(n).copy() for n in ("us", "vs", "ws")}
+    o.inversex_walls(alf)
+    o.inversex(alf)
+    after = {n: o.get(n) for n in ("us", "vs", "ws")}
+    g = {n: o.grid.get(n) for n in ("ap", "au", "av", "aw")}
+    coef, ru1, nx = 0.5 * alf, 1.0 / w.re, w.nx
+    worst = 0.0
+    for comp in ("us", "vs", "ws"):
+        r, x = before[comp], after[comp]
+        i = np.arange(2, nx if comp != "us" else nx - 1)  # Fortran indices 2..NX-1 (u: NX-2)
+        ks = range(2, w.nz - 1) if comp != "ws" else range(2, w.nz - 2)
+        for k in ks:
+            for j in range(2, w.ny):
+                T = lambda ii, dj=0, dk=0: tv[ii - 1, j - 1 + dj, k - 1 + dk]  # noqa: E731
+                if comp == "us":
+                    cx = coef * g["au"][i - 1]
+                    a = -cx * g["ap"][i - 1] * (2 * T(i) + ru1)
+                    c = -cx * g["ap"][i] * (2 * T(i + 1) + ru1)
+                    xl = np.concatenate([[0.0], x[i[:-1] - 1, j - 1, k - 1]])
+                    xr = np.concatenate([x[i[1:] - 1, j - 1, k - 1], [0.0]])
+                else:
+                    dj, dk = (1, 0) if comp == "vs" else (0, 1)
+                    tp = 0.25 * (T(i, dj, dk) + T(i) + T(i + 1, dj, dk) + T(i + 1)) + ru1
+                    tm = 0.25 * (T(i, dj, dk) + T(i) + T(i - 1, dj, dk) + T(i - 1)) + ru1
+                    cx = coef * g["av" if comp == "vs" else "aw"][i - 1]
+                    a = -cx * g["au"][i - 2] * tm
+                    c = -cx * g["au"][i - 1] * tp
+                    xs = x[i - 1, j - 1, k - 1]
+                    xl = np.concatenate([[xs[0]], xs[:-1]])  # Neumann: ghost = first cell
+                    xr = np.concatenate([xs[1:], [xs[-1]]])
+                b = 1.0 - a - c
+                res = a * xl + b * x[i - 1, j - 1, k - 1] + c * xr - r[i - 1, j - 1, k - 1]
+                worst = max(worst, float(np.max(np.abs(res)) / np.max(np.abs(r[i - 1, j - 1, k - 1]))))
+        assert not np.array_equal(before[comp], after[comp]), comp
+    assert worst < 1e-13, worst
+
+
+@pytest.mark.parametrize("imply", [0, 1])
+def test_implicit_x_step_is_projected_and_close_to_explicit(oracle, imply):
+    oi, oe = _xpair(oracle, 1, imply, 4), _xpair(oracle, 0, imply, 4)
+    assert oi.max_divergence() < 1e-12
+    for n in ("uo", "vo", "wo", "dens", "p"):
+        a, b = oi.get(n)[1:-1, 1:-1, 1:-1], oe.get(n)[1:-1, 1:-1, 1:-1]
+        assert np.all(np.isfinite(a)), n
+        d = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+        assert 0 < d < 5e-3, (n, d)
