@@ -16,7 +16,7 @@
 //   backward: e = B_e c_even, o = B_o c_odd, f[x] = e + o, f[M-1-x] = e - o,
 // all four matrices H x H.
 //
-// One CTA per 128-line tile, all M outputs in TMEM columns 0..M-1 (M <= 432).
+// One CTA per 128-line tile, all M outputs in TMEM columns 0..M-1 (M <= 512).
 // K is streamed in chunks of 8 through a multi-stage shared-memory pipeline:
 // each A chunk arrives by one 2-D TMA box (32 bytes x 128 lines) with the
 // 32-byte swizzle, which is the canonical SWIZZLE_32B K-major layout (rows of
@@ -132,6 +132,10 @@ struct StageGeom {
   uint32_t b_bytes;   // nb x KC floats (one of hi / lo)
   uint32_t stage;     // bytes per stage
 };
+
+// output passes of the epilogue: rows of more than 432 floats are staged
+// in two halves (128 rows of W + 4 floats must fit the shared memory)
+__host__ __device__ inline int xform_passes(int M) { return M > 432 ? 2 : 1; }
 
 __host__ __device__ inline StageGeom stage_geom(int mode, int M) {
   StageGeom g;
@@ -329,8 +333,10 @@ __global__ void __launch_bounds__(XT, 1)
     }
     // epilogue: all MMAs complete, so every stage buffer is free.  Thread t
     // (row t of the tile) assembles its output row in shared memory (rows
-    // padded to M + 4 floats against bank conflicts) and writes it back with
-    // one bulk copy (the row is contiguous in global memory).
+    // padded to W + 4 floats against bank conflicts) and writes it back with
+    // one bulk copy (the row is contiguous in global memory).  Rows wider
+    // than 432 floats go out in two halves of W = M/2 columns, the second
+    // staged once the first copy has read the buffer.
     if (ok && !umma::mbar_wait(&done, 0)) { fail(); ok = false; }
     umma::fence_after_sync();
     if (ok && !abort_flag) {
@@ -338,51 +344,60 @@ __global__ void __launch_bounds__(XT, 1)
       const int rt = q4 * 32 + lane;
       const long long row = p0 + rt;
       const uint32_t tl = tm + ((uint32_t)(q4 * 32) << 16);
-      float *srow = reinterpret_cast<float *>(base) + (size_t)rt * (M + 4);
-      if (mode == 2) {
-        // f[x] = e + o, f[M-1-x] = e - o
-        for (int c0 = 0; c0 < H; c0 += 32) {
-          uint32_t e[32], o[32];
-          tmem_ld32(tl + (uint32_t)c0, e);
-          tmem_ld32(tl + (uint32_t)(H + c0), o);
-          const int nv = (H - c0 < 32 ? H - c0 : 32) / 4;
+      const int npass = xform_passes(M), W = M / npass;
+      float *srow = reinterpret_cast<float *>(base) + (size_t)rt * (W + 4);
+      for (int pass = 0; pass < npass; pass++) {
+        if (pass) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        if (mode == 2) {
+          // f[x] = e + o, f[M-1-x] = e - o; with two passes the first writes
+          // columns 0..H-1 (the sums), the second H..M-1 (the differences)
+          for (int c0 = 0; c0 < H; c0 += 32) {
+            uint32_t e[32], o[32];
+            tmem_ld32(tl + (uint32_t)c0, e);
+            tmem_ld32(tl + (uint32_t)(H + c0), o);
+            const int nv = (H - c0 < 32 ? H - c0 : 32) / 4;
 #pragma unroll
-          for (int q = 0; q < 8; q++) {
-            if (q < nv) {
-              float pv[4], mv[4];
+            for (int q = 0; q < 8; q++) {
+              if (q < nv) {
+                float pv[4], mv[4];
 #pragma unroll
-              for (int u = 0; u < 4; u++) {
-                const float ev = __uint_as_float(e[4 * q + u]), ov = __uint_as_float(o[4 * q + u]);
-                pv[u] = ev + ov;
-                mv[u] = ev - ov;
+                for (int u = 0; u < 4; u++) {
+                  const float ev = __uint_as_float(e[4 * q + u]), ov = __uint_as_float(o[4 * q + u]);
+                  pv[u] = ev + ov;
+                  mv[u] = ev - ov;
+                }
+                const int x = c0 + 4 * q;
+                if (pass == 0)
+                  *reinterpret_cast<float4 *>(srow + x) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+                if (npass == 1 || pass == 1)
+                  *reinterpret_cast<float4 *>(srow + (M - 4 - x - pass * W)) =
+                      make_float4(mv[3], mv[2], mv[1], mv[0]);
               }
-              const int x = c0 + 4 * q;
-              *reinterpret_cast<float4 *>(srow + x) = make_float4(pv[0], pv[1], pv[2], pv[3]);
-              *reinterpret_cast<float4 *>(srow + (M - 4 - x)) = make_float4(mv[3], mv[2], mv[1], mv[0]);
             }
           }
-        }
-      } else {
-        for (int c0 = 0; c0 < M; c0 += 64) {
-          uint32_t r[64];
-          umma::tmem_ld64(tl + (uint32_t)c0, r);
-          float4 *dst = reinterpret_cast<float4 *>(srow + c0);
-          const int nv = (M - c0 < 64 ? M - c0 : 64) / 4;
+        } else {
+          const int cb = pass * W, ce = cb + W;
+          for (int c0 = cb; c0 < ce; c0 += 64) {
+            uint32_t r[64];
+            umma::tmem_ld64(tl + (uint32_t)c0, r);
+            float4 *dst = reinterpret_cast<float4 *>(srow + (c0 - cb));
+            const int nv = (ce - c0 < 64 ? ce - c0 : 64) / 4;
 #pragma unroll
-          for (int q = 0; q < 16; q++)
-            if (q < nv)
-              dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
-                                   __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+            for (int q = 0; q < 16; q++)
+              if (q < nv)
+                dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                     __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+          }
+        }
+        umma::fence_smem_to_async();
+        if (row < P) {
+          asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(out + row * M + pass * W),
+                       "r"(tma::smem_u32(srow)), "r"((uint32_t)W * 4u)
+                       : "memory");
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
       }
-      umma::fence_smem_to_async();
-      if (row < P) {
-        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(out + row * M),
-                     "r"(tma::smem_u32(srow)), "r"((uint32_t)M * 4u)
-                     : "memory");
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-      }
+      if (row < P) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
     }
   }
   // on the error path the MMAs already issued may still run: wait (bounded)
@@ -440,17 +455,18 @@ int xform_stages(int mode, int M) {
 }
 
 // dynamic shared memory: the stages, which the epilogue reuses for its
-// 128 output rows of M + 4 floats
+// 128 output rows of W + 4 floats (W = M / passes)
 size_t xform_smem(int mode, int M) {
   const size_t st = (size_t)xform_stages(mode, M) * stage_geom(mode, M).stage;
-  const size_t ep = (size_t)128 * (M + 4) * 4;
+  const size_t ep = (size_t)128 * (M / xform_passes(M) + 4) * 4;
   return (st > ep ? st : ep) + 1024;
 }
 
 }  // namespace
 
-// M <= 432: the epilogue's 128 staged rows of M + 4 floats fit in shared memory
-bool xform_supported(int M) { return M >= 16 && M <= 432 && M % 16 == 0; }
+// M <= 512: all M accumulator columns fit the 512 TMEM columns of an SM (one
+// CTA per SM), the epilogue stages rows in at most two passes
+bool xform_supported(int M) { return M >= 16 && M <= 512 && M % 16 == 0; }
 
 // Transform matrices from the FP64 plan.  Af (col-major, Af(n, x)) maps
 // x values to mode coefficients, Ab (col-major, Ab(x, n)) back.  The split

@@ -31,11 +31,18 @@ def _compatible_rhs(o, w, seed=7):
 
 @pytest.mark.parametrize("sweeps,mx,xlim", [(1, 24, None), (2, 24, None), (3, 24, None), (1, 32, None),
                                            (2, 48, None), (2, 64, None), (2, 128, None), (2, 64, (-3.0, 5.0)),
-                                           (2, 96, (-3.0, 5.0))])
+                                           (2, 96, (-3.0, 5.0)), (2, 448, None), (2, 512, None),
+                                           (2, 448, (-3.0, 5.0))])
 def test_refined_poisson(oracle, product, sweeps, mx, xlim):
-    # mx = 24: FP32 transforms by cuBLAS SGEMM (M not a multiple of 16);
-    # mx >= 32: 3xTF32 transforms on the tensor cores, the even/odd split form
-    # on symmetric grids and the plain form with xlim off centre
+    # mx = 24: FP32 data through the FP64 tensor-core transform of the plain
+    # form (M not a multiple of 16); mx >= 32: 3xTF32 transforms on the
+    # tcgen05 tensor cores, the even/odd split form on symmetric grids and the
+    # plain form with xlim off centre; mx = 448, 512: rows written back in two
+    # halves.  (The plain FP64 plan takes an off-centre grid up to 448.)
+    # At 448 and 512 cells with stretching 2.5 the operator's conditioning
+    # sets the floor: the bars there are the FP64 direct solve's own residual
+    # and its distance to the refined solution.
+    wide = mx >= 448
     kw = {} if xlim is None else {"xlim": xlim}
     w = config.small(mx=mx, ly=16, nz_=20, beta=2.5, **kw)
     o = oracle.OracleSolver(w)
@@ -50,18 +57,25 @@ def test_refined_poisson(oracle, product, sweeps, mx, xlim):
     # the first pre-sweep residual is the FP32 solve's: 1e-4 to 1e-3 relative
     # (an FP32 solution error of ~1e-7 amplified by the norm of L, which grows
     # with the grid's resolution)
-    assert rr[0] / np.max(np.abs(inner)) < 1e-2
+    assert rr[0] / np.max(np.abs(inner)) < (5e-2 if wide else 1e-2)
     for s in range(1, sweeps):
         assert rr[s] < 1e-2 * rr[s - 1]
-    assert res < (1e-9 if sweeps == 1 else 1e-11)
     # against the FP64 solution, up to the additive constant of the Neumann
     # null space (the FP32 mean removal leaves ~1e-8; the pressure update's
     # reference value removes any constant)
     o.set("dp", d)
     o.direct(1)
-    xo = o.get("dp")[1:-1, 1:-1, 1:-1]
+    xo_full = o.get("dp")
+    xo = xo_full[1:-1, 1:-1, 1:-1]
     xg = x[1:-1, 1:-1, 1:-1]
     xg = xg - np.mean(xg - xo)
+    if wide:
+        ro = np.max(np.abs(o.apply_laplacian(xo_full)[1:-1, 1:-1, 1:-1] - inner)) / np.max(np.abs(inner))
+        print(f"FP64 direct residual {ro:.3e}")
+        assert res < max(1e-11, 2 * ro)
+        assert rel_err(xg, xo) < 1e-9
+        return
+    assert res < (1e-9 if sweeps == 1 else 1e-11)
     assert rel_err(xg, xo) < (1e-8 if sweeps == 1 else 1e-11)
 
 
