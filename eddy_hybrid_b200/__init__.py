@@ -76,6 +76,8 @@ SIGNATURES = {
     "eddy_rhs_predictord": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
     "eddy_inversey": ([C.c_void_p, C.c_double], C.c_int),
     "eddy_inversex": ([C.c_void_p, C.c_double], C.c_int),
+    "eddy_body_force_cv": ([C.c_void_p, _DP, C.c_double, C.c_int, _DP], C.c_int),
+    "eddy_body_force_cv_reset": ([C.c_void_p], C.c_int),
     "eddy_cfl": ([C.c_void_p, _DP], C.c_int),
     "eddy_field_extrema": ([C.c_void_p, C.c_int, _DP, _DP], C.c_int),
     "eddy_ioscalar_write": ([C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.c_int, C.c_double, C.c_double,
@@ -361,6 +363,21 @@ class Solver:
         out = np.zeros(shape, order="F")
         self._check(lib().eddy_plane(self.h, FID[name], center, axis, index, _ptr(out)), "eddy_plane")
         return out
+
+    def body_force_cv(self, cvlim, dt: float, icycle: int) -> np.ndarray:
+        """calcfrc (src/calcforce.f:3): the 56 control-volume force terms of
+        eddy_body_force_cv; the volume's momentum of this call is kept for the
+        next call's unsteady term."""
+        cv = np.ascontiguousarray(cvlim, dtype=np.float64)
+        if cv.shape != (4,):
+            raise ValueError("cvlim holds (x1, x2, z1, z2)")
+        out = np.zeros(56)
+        self._check(lib().eddy_body_force_cv(self.h, _ptr(cv), float(dt), int(icycle), _ptr(out)),
+                    "eddy_body_force_cv")
+        return out
+
+    def body_force_cv_reset(self):
+        self._check(lib().eddy_body_force_cv_reset(self.h), "eddy_body_force_cv_reset")
 
     def set_cycle(self, icycle: int):
         self._check(lib().eddy_inflow_cycle(self.h, icycle), "eddy_inflow_cycle")

@@ -33,6 +33,7 @@ UNITS = {
     "k_ib.cu": ["-fmad=false"],
     "k_implicit.cu": ["-fmad=false"],
     "k_diag.cu": ["-fmad=false"],
+    "k_force.cu": ["-fmad=false"],
     "host_eigen.cpp": [],
     "host_restart.cpp": [],
 }

@@ -225,7 +225,7 @@ void free_all(eddy_ctx *ctx) {
   for (double *p : mp) if (p) cudaFree(p);
   for (int f = 0; f < EDDY_NFIELDS; f++) if (ctx->f[f]) cudaFree(ctx->f[f]);
   double *o[] = {ctx->dens_alt, ctx->gs, ctx->dxdydz, ctx->ilm2, ctx->imm2, ctx->scal, ctx->diag, ctx->feed,
-                 ctx->probe_buf, ctx->plane_buf};
+                 ctx->probe_buf, ctx->plane_buf, ctx->cv_buf};
   if (ctx->probe_ijk) cudaFree(ctx->probe_ijk);
   for (double *p : o) if (p) cudaFree(p);
   if (ctx->err_flag) cudaFree(ctx->err_flag);

@@ -130,6 +130,10 @@ struct eddy_ctx {
   double *probe_buf = nullptr;
   int nprobe = 0, probe_cap = 0, probe_count = 0;
   double *plane_buf = nullptr;  // staging of eddy_plane (the largest plane of the grid)
+  // control-volume body force (k_force.cu): partial sums, and the volume's
+  // momentum of the previous call (FB of calcfrc)
+  double *cv_buf = nullptr;
+  double cv_fb[3] = {0., 0., 0.};
   double *xc_dev = nullptr;     // x cell centres (1-based, NX+2)
   double *kappa = nullptr;      // eddy diffusivity of the learned closure (NX,NY,NZ)
   double *tv_dyn = nullptr;     // last dynamic-model nu_t: closure fallback (NX,NY,NZ)
@@ -284,6 +288,8 @@ int ib_limits(eddy_ctx *ctx, int *lim6);
 int ib_stencils(eddy_ctx *ctx, int q, int *n, int *nlev, int *ijk, int *dijk, int *lev, double *xn, double *lu,
                 int *indx);
 int ib_stencil_kinds(eddy_ctx *ctx, int q, int *mrk, int *dir, double *xe);
+// the device flag array fq of the body (nullptr without one)
+const signed char *ib_flag_dev(eddy_ctx *ctx, int fq);
 int probes_record(eddy_ctx *ctx);
 
 // tensor-core (3xTF32) eigen-transforms of the mixed solve (k_xform.cu).

@@ -2493,6 +2493,11 @@ int ib_download(eddy_ctx *ctx, int which, signed char *out) {
   return EDDY_OK;
 }
 
+const signed char *ib_flag_dev(eddy_ctx *ctx, int fq) {
+  IbState *s = ibs(ctx);
+  return (s && fq >= 0 && fq < 5) ? s->flag[fq] : nullptr;
+}
+
 int ib_limits(eddy_ctx *ctx, int *lim6) {
   if (int rcj = ib_join(ctx)) return rcj;
   IbState *s = ibs(ctx);

@@ -12,8 +12,9 @@
  *
  * Axes follow the reference: x = x_ref (stretched), y = y_ref (uniform,
  * periodic, FFT axis), z = z_ref (stretched).  Boundary types supported on
- * the hot path: 60 (slip wall) and 50 (no-slip) on x, 500 on y, 305 (hybrid
- * inlet plane) and 710/720/730 (outlets) on z.
+ * the hot path: 60 (slip wall) and 82 (the stratified-wave condition of
+ * BOUND082) on x, 500 on y, 305 (hybrid inlet plane) and 730 (convective
+ * outlet) on z.
  */
 #ifndef EDDY_B200_H
 #define EDDY_B200_H
@@ -270,6 +271,21 @@ int eddy_probes_read(eddy_ctx *ctx, double *out, int max_samples, int *nsamples)
  * plane at i = index (out[NY*NZ]), 2 the (i, k) plane at j = index
  * (out[NX*NZ]), 3 the (i, j) plane at k = index (out[NX*NY]); Fortran order. */
 int eddy_plane(eddy_ctx *ctx, int field, int center, int axis, int index, double *out);
+/* calcfrc (src/calcforce.f:3-779, Cartesian branch): the force on the body
+ * by the control-volume approach on UO, VO, WO, P and the body's flags (no
+ * body: all fluid).  cvlim = CVLIM (x1, x2, z1, z2): the volume spans the x
+ * faces closest to x1, x2 (closest, src/numrec.f:433) and the z faces that
+ * locate (src/numrec.f:390) finds for z1, z2, adjusted as the reference does
+ * where it reaches past the domain; faces on the outermost planes are refused
+ * (EDDY_EINVAL).  The volume's momentum is kept in the context between calls:
+ * the unsteady term is (now - previous) / dt, zero when icycle == 0 (FB of
+ * the reference; eddy_body_force_cv_reset clears it).  out[56]: FX(1..6),
+ * FY(1..6) (zero in Cartesian coordinates), FZ(1..6) (inlet, outlet, top,
+ * bottom, j = 1, j = JY2 faces), the unsteady terms (3), the force on the
+ * body -(SUM(F) + unsteady) per component (3), Finlet(1..8), Foutlet(1..8),
+ * Ftop(1..8), Fbot(1..8) as the reference writes them to its force files. */
+int eddy_body_force_cv(eddy_ctx *ctx, const double *cvlim, double dt, int icycle, double *out);
+int eddy_body_force_cv_reset(eddy_ctx *ctx);
 
 /* Kernel-category timing with CUDA events on the context stream (the
  * device-side counterpart of the reference's CLOCK array, src/info.f:350 and

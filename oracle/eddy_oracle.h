@@ -134,6 +134,10 @@ void eo_inverseyd(eo_state *s, double alfxdt);
 void eo_inversex_walls(eo_state *s, double alfxdt);
 void eo_inversex(eo_state *s, double alfxdt);
 void eo_inversexd(eo_state *s, double alfxdt);
+/* calcfrc (src/calcforce.f:3-779), Cartesian, and its index helpers */
+int eo_closest(const double *xx, int n, double x);
+void eo_cv_range(const eo_grid *g, const double cvlim[4], int cv[6]);
+void eo_calcfrc(eo_state *s, const double cvlim[4], double dt, int icycle, double fb[3], double out[56]);
 /* periodic tridiagonal system (cyclic, src/numrec.f:754-779): n unknowns,
  * a sub-, b main, c super-diagonal, alpha = A(n,1), beta = A(1,n); work >= 4n */
 void eo_cyclic(const double *a, const double *b, const double *c, double alpha, double beta, const double *r,

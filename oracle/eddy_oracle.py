@@ -100,6 +100,9 @@ def lib():
         L.eo_inversex_walls.argtypes = [C.c_void_p, C.c_double]
         L.eo_calcfl.argtypes = [C.c_void_p]
         L.eo_calcfl.restype = C.c_double
+        _P = C.POINTER(C.c_double)
+        L.eo_calcfrc.argtypes = [C.c_void_p, _P, C.c_double, C.c_int, _P, _P]
+        L.eo_cv_range.argtypes = [C.c_void_p, _P, C.POINTER(C.c_int)]
         L.eo_call_density.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
         L.eo_call_boundary.argtypes = [C.c_void_p, C.c_int]
         L.eo_call_boundinout.argtypes = [C.c_void_p, C.c_int, C.c_double]
@@ -261,6 +264,23 @@ class OracleSolver:
 
     def calcfl(self) -> float:
         return lib().eo_calcfl(self.h)
+
+    def calcfrc(self, cvlim, dt: float, icycle: int, fb: np.ndarray) -> np.ndarray:
+        """calcfrc (src/calcforce.f:3): the 56 force terms; fb (3,) the
+        control volume's momentum of the previous call, updated in place."""
+        P = C.POINTER(C.c_double)
+        cv = np.ascontiguousarray(cvlim, dtype=np.float64)
+        assert fb.dtype == np.float64 and fb.flags.c_contiguous and fb.shape == (3,)
+        out = np.zeros(56)
+        lib().eo_calcfrc(self.h, cv.ctypes.data_as(P), dt, icycle, fb.ctypes.data_as(P), out.ctypes.data_as(P))
+        return out
+
+    def cv_range(self, cvlim) -> tuple:
+        """ICB, ICE, KCB, KCE, KBFLAG, KEFLAG of the control volume."""
+        cv = np.ascontiguousarray(cvlim, dtype=np.float64)
+        r = (C.c_int * 6)()
+        lib().eo_cv_range(self.grid.h, cv.ctypes.data_as(C.POINTER(C.c_double)), r)
+        return tuple(r)
 
     def boundary(self, set_):
         lib().eo_call_boundary(self.h, set_)
