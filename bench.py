@@ -234,12 +234,29 @@ ALG_BYTES_MIXED = {
     "transform_fwd": 2 * 4,
     "z_line_solve": 5 * 4,     # R rhs, W eliminated; R eliminated, c' table, W solution (FP32)
     "transform_bwd": 2 * 4,
-    "fft_bwd": 2 * 4,
+    "fft_bwd": 4 + 8,          # R spectrum FP32  W solution FP64 (the corrections also R it: below)
     "correct": 3 * 4 + 8 + 3 * 8 + 3 * 4,  # R u*,v*,w* FP32, dp  W u,v,w FP64 + FP32 copies
     "pressure_update": 8 + 8 + 8 + 4,      # R p,dp  W p FP64, p FP32
     "density": 6 * 4 + 2 * 4,              # R rho,kappa,u,v,w,rha  W rho,rha (FP32)
     "precision_copy": 4 + 8,               # one FP32<->FP64 copy
 }
+
+
+def step_alg_bytes(alg, sweeps, mixed):
+    """Algorithmic bytes per cell of one step, the sum of the per-launch
+    figures above: three substeps of RHS + predictor, divergence + FFT, the
+    Poisson solve (mixed: 1 + sweeps solves, sweeps residuals, the backward
+    passes writing (then adding to) the FP64 solution), CORRECT, the pressure
+    update and the density, then the eddy viscosity (R u, v, w, W nu_t; the
+    mixed form's FP32 copy of nu_t included)."""
+    sub = alg["rhs_predictor"] + alg["div_fft_fwd"] + alg["correct"] + alg["pressure_update"] + alg["density"]
+    solve = alg["transform_fwd"] + alg["z_line_solve"] + alg["transform_bwd"]
+    if mixed:
+        sub += (1 + sweeps) * solve + sweeps * alg["refine_residual"] + 12 + 20 * sweeps
+        return 3 * sub + 3 * 4 + 8 + alg["precision_copy"]
+    return 3 * (sub + solve + alg["fft_bwd"]) + alg["eddy_viscosity"]
+
+
 # the learned closure: R u,v,w,rho FP32  W nu_t,kappa_t FP64 + FP32 copies
 CLOSURE_BYTES = 4 * 4 + 2 * 8 + 2 * 4
 MLP_FLOP_PER_CELL = 2 * (12 * 64 + 64 * 64 + 64 * 64 + 64 * 2)   # algorithmic (unpadded) 12-64-64-64-2
@@ -514,6 +531,9 @@ def main():
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     mixed_alg = dict(ALG_BYTES_MIXED)
+    # of the 1 + sweeps backward passes per solve, the corrections add their
+    # result to the FP64 solution (R and W): the mean bytes per launch
+    mixed_alg["fft_bwd"] = (12 + 20 * sweeps) / (1 + sweeps)
     forms = {
         "plain": {"solver": g0, "r": r0, "dtype": "f64", "closure": False,
                   "desc": "plain FP64 (dynamic model)",
@@ -590,8 +610,7 @@ def main():
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
                 "algorithmic_bytes_per_cell": alg[dom], "form": head}
-    step_bytes = {"plain": 944, "mixed_dynamic": 3 * (188 + 48 * sweeps) + 24,
-                  "chosen": 3 * (188 + 48 * sweeps) + 24}[head]
+    step_bytes = step_alg_bytes(ALG_BYTES if head == "plain" else mixed_alg, sweeps, head != "plain")
     roofline["whole_step"] = {"algorithmic_bytes_per_cell_step": step_bytes,
                               "achieved_gbs": step_bytes * ncell / (msH / args.steps / 1e3) / 1e9,
                               "frac": step_bytes * ncell / (msH / args.steps / 1e3) / 1e9 / hbm}

@@ -404,7 +404,7 @@ template <int ACC>
 __global__ void __launch_bounds__(FT32, 4)
     k_bwd32(Dims d, const float *__restrict__ spec, const double *__restrict__ dpm, int code,
             const float *__restrict__ twr, const float *__restrict__ twi, double *__restrict__ phi) {
-  constexpr int U = 4;
+  constexpr int U = 8;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ float smf[];
   const int L = fft_len(code), M = d.nx - 2;
