@@ -24,6 +24,7 @@ UNITS = {
     "k_poisson.cu": ["-fmad=false"],
     "k_density.cu": ["-fmad=false"],
     "k_sgs.cu": ["-fmad=false"],
+    "k_sgs32.cu": [],
     "k_noalloc.cu": ["-fmad=false"],
     "k_selftest.cu": [],
     "k_mlp.cu": [],
