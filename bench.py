@@ -214,7 +214,9 @@ def run_reference(args):
                     f"equations on a {w.nz_}x{w.mx}x{w.ly} grid (1/8 of the cells) with the moving sphere "
                     f"({ntri} triangles, regenerated every step); {dt:.2f} s on {cores} threads"}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt / max(args.steps, 1) * 1e3, "ms_per_step_of": f"the {w.nz_}x{w.mx}x{w.ly} sample",
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"wake_512x384x256 sampled on {w.nz_}x{w.mx}x{w.ly}",
                        "form": "plain FP64 (CPU oracle port of the reference loops)",
