@@ -162,7 +162,9 @@ __global__ void __launch_bounds__(XT, 1)
   __shared__ __align__(8) uint64_t full[MAXST], split[MAXST], empty[MAXST], done;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
-  unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(xsm) + 1023) & ~uintptr_t(1023));
+  // 1024-byte aligned stage area, as an offset into the shared array (the
+  // shared address space stays visible to the compiler)
+  unsigned char *base = xsm + ((1024u - (unsigned)(reinterpret_cast<uintptr_t>(xsm) & 1023u)) & 1023u);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const StageGeom G = stage_geom(mode, M);
   const int H = M / 2;

@@ -129,7 +129,10 @@ __device__ __forceinline__ void tma_march(int ix1, int ix2, int jy1, int jy2, in
   constexpr int NSLOT = 4, SLOT = NF * G::PLANE;
   extern __shared__ unsigned char smraw_[];
   __shared__ __align__(8) uint64_t bar[NSLOT];
-  T *sm = reinterpret_cast<T *>((reinterpret_cast<uintptr_t>(smraw_) + 127) & ~uintptr_t(127));
+  // 128-byte aligned ring start, as an offset into the shared array (pointer
+  // arithmetic on it keeps the shared address space visible to the compiler)
+  const unsigned align_off = (128u - (unsigned)(reinterpret_cast<uintptr_t>(smraw_) & 127u)) & 127u;
+  T *sm = reinterpret_cast<T *>(smraw_ + align_off);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = ix1 + blockIdx.x * TX, j0 = jy1 + blockIdx.y * TY;
   const int k0 = kz1 + blockIdx.z * KC;
