@@ -53,3 +53,20 @@ def test_body_force_cv_refuses_outer_planes(product):
     g = product.Solver(w)
     with pytest.raises(product.EddyError):
         g.body_force_cv((-99.0, 1.0, -1.0, 1.0), 1e-3, 0)
+
+
+@pytest.mark.parametrize("cv", [(-1.5, 1.5, -99.0, 2.0), (-1.5, 1.5, -1.5, 99.0), (-1.5, 1.5, -99.0, 99.0)])
+def test_body_force_cv_volumes_past_the_domain(oracle, product, cv):
+    # the reference's adjusted ranges when the volume reaches past an end of
+    # the domain: the missing face is skipped, the volume clipped
+    w = config.small(mx=24, ly=8, nz_=32, noise=0.2, re=2000.0)
+    o = oracle.OracleSolver(w)
+    f = config.initial_fields(w, o.grid.get("dens_bg")[: w.nx])
+    o.load_initial(f)
+    o.initialize()
+    o.step(2)
+    g = product.Solver(w)
+    for n in ("uo", "vo", "wo", "p"):
+        g.upload(n, o.get(n))
+    fb = np.zeros(3)
+    _close(g.body_force_cv(cv, w.dt, 0), o.calcfrc(cv, w.dt, 0, fb))
