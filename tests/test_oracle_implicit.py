@@ -121,3 +121,64 @@ def test_implicit_x_step_is_projected_and_close_to_explicit(oracle, imply):
         assert np.all(np.isfinite(a)), n
         d = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
         assert 0 < d < 5e-3, (n, d)
+
+
+def _mode_state(oracle, beta=2.0, **kw):
+    w = config.small(mx=32, ly=16, nz_=12, isgs=0, idens=0, re=20.0, beta=beta, **kw)
+    o = oracle.OracleSolver(w)
+    z = np.zeros((w.nx, w.ny, w.nz), order="F")
+    for n in ("uo", "vo", "wo", "p", "tv", "dens", "ua", "va", "wa"):
+        o.set(n, z)
+    return o, w
+
+
+def test_crank_nicolson_y_damps_a_y_mode_by_its_factor(oracle):
+    # w = sin(k y) is an eigenvector of the periodic y operator, with u = v = 0
+    # and p = 0 nothing else acts on it: the predictor's explicit half and
+    # INVERSEY's implicit half give w* = w (1 + c lam) / (1 - c lam), c = alfxdt
+    # ru1 / 2, lam = -(2 / dy^2)(1 - cos(k dy))
+    o, w = _mode_state(oracle, imply=1)
+    yc = o.grid.get("yc")
+    ly = w.ylim[1] - w.ylim[0]
+    dy = ly / w.ly
+    for m in (1, 3):
+        kk = 2 * np.pi * m / ly
+        wo = np.asfortranarray(np.broadcast_to(np.sin(kk * (yc - w.ylim[0]))[None, :, None], (w.nx, w.ny, w.nz)))
+        o.set("wo", wo)
+        alf = 2 / 15 * 1e-2
+        o.rhs_predictord(alf, 8 / 15 * 1e-2, 0.0)
+        o.inversey(alf)
+        lam = -(2 / dy ** 2) * (1 - np.cos(kk * dy))
+        c = 0.5 * alf / w.re
+        want = wo * (1 + c * lam) / (1 - c * lam)
+        ws = o.get("ws")
+        i_end = w.nx - 2 - max(2, w.mx // 24) - 1   # clear of the x sponge
+        sl = (slice(1, i_end), slice(1, w.ny - 1), slice(1, w.nz - 2))
+        assert np.max(np.abs(ws[sl] - want[sl])) < 1e-12
+        assert np.max(np.abs(o.get("us"))) == 0 and np.max(np.abs(o.get("vs")[sl])) == 0
+
+
+def test_crank_nicolson_x_lines_damp_x_modes_by_their_factor(oracle):
+    # on a (nearly) uniform x grid sin(pi m x / Lx) on the u faces (zero at the
+    # walls) and cos(pi m x / Lx) at the cell centres (Neumann) are
+    # eigenvectors of the x lines of INVERSEX: v* = v / (1 - c lam)
+    o, w = _mode_state(oracle, beta=1e-4, implx=1)
+    xu, xc = o.grid.get("xu"), o.grid.get("xc")
+    lx = w.xlim[1] - w.xlim[0]
+    dx = lx / w.mx
+    alf = 2 / 15 * 1e-2
+    c = 0.5 * alf / w.re
+    for m in (1, 2):
+        lam = -(2 / dx ** 2) * (1 - np.cos(np.pi * m / w.mx))
+        us = np.sin(np.pi * m * (xu - w.xlim[0]) / lx)[:, None, None] * np.ones((1, w.ny, w.nz))
+        vs = np.cos(np.pi * m * (xc - w.xlim[0]) / lx)[:, None, None] * np.ones((1, w.ny, w.nz))
+        us[-1] = 0.0
+        for n, a in (("us", us), ("vs", vs), ("ws", vs)):
+            o.set(n, np.asfortranarray(a))
+        o.inversex_walls(alf)
+        o.inversex(alf)
+        f = 1.0 / (1 - c * lam)
+        ku = slice(1, w.nz - 1)
+        assert np.max(np.abs(o.get("us")[1:w.nx - 2, 1:-1, ku] - f * us[1:w.nx - 2, 1:-1, ku])) < 1e-6
+        assert np.max(np.abs(o.get("vs")[1:-1, 1:-1, ku] - f * vs[1:-1, 1:-1, ku])) < 1e-6
+        assert np.max(np.abs(o.get("ws")[1:-1, 1:-1, 1:w.nz - 2] - f * vs[1:-1, 1:-1, 1:w.nz - 2])) < 1e-6
