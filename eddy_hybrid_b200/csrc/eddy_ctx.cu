@@ -560,11 +560,6 @@ int eddy_turvis(eddy_ctx *ctx) {
 int eddy_ib_set_body(eddy_ctx *ctx, int nb, const double *vertices, const double *normals,
                      const double *velocity) {
   if (check_ctx(ctx) || nb < 0 || (nb > 0 && (!vertices || !normals))) return EDDY_EINVAL;
-  if (nb > 0 && (ctx->prm.imply == 1 || ctx->prm.implx == 1)) {
-    ctx->err = "an immersed body with the implicit terms (the reference's forcing of UB, src/Eddy6.f:2490-2520) "
-               "is not supported";
-    return EDDY_EINVAL;
-  }
   EDDY_CUDA(cudaStreamSynchronize(ctx->stream));
   return ib_set_body(ctx, nb, vertices, normals, velocity);
 }
@@ -775,7 +770,26 @@ static int substep_core(eddy_ctx *ctx, int is, double dt) {
     ProfScope ps(ctx, PROF_RHS_PRED);
     if ((rc = launch_rhs_predictord(ctx, alfxdt, gamxdt, rhoxdt))) return rc;
   }
-  // Crank-Nicolson y, then x lines (src/Eddy6.f:2596-2607; no immersed body)
+  const bool implicit = ctx->sc.imply == 1 || ctx->sc.implx == 1;
+  // with a body and the C.N. steps the forcing comes first, from the explicit
+  // estimate UB the predictor wrote (src/Eddy6.f:2495-2575, impl = 1)
+  if (ctx->ib && implicit) {
+    if ((rc = ib_overlap_regen(ctx))) return rc;
+    {
+      ProfScope ps(ctx, PROF_BC);
+      if ((rc = launch_boundary(ctx, f[EDDY_UB], f[EDDY_VB], f[EDDY_WB]))) return rc;
+      if ((rc = launch_boundinout(ctx, f[EDDY_UB], f[EDDY_VB], f[EDDY_WB], f[EDDY_UO], f[EDDY_VO], f[EDDY_WO],
+                                  alfxdt, 1)))
+        return rc;
+      if ((rc = launch_boundary(ctx, f[EDDY_UB], f[EDDY_VB], f[EDDY_WB]))) return rc;
+    }
+    ProfScope ps(ctx, PROF_IB_FORCE);
+    const double *vb = ib_velocity(ctx);
+    if ((rc = ib_force_impl(ctx, 0, 0, f[EDDY_US], f[EDDY_UB], vb[0]))) return rc;
+    if ((rc = ib_force_impl(ctx, 1, 1, f[EDDY_VS], f[EDDY_VB], vb[1]))) return rc;
+    if ((rc = ib_force_impl(ctx, 2, 2, f[EDDY_WS], f[EDDY_WB], vb[2]))) return rc;
+  }
+  // Crank-Nicolson y, then x lines (src/Eddy6.f:2596-2607)
   if (ctx->sc.imply == 1) {
     ProfScope ps(ctx, PROF_TRIDIAG);
     if ((rc = launch_inversey(ctx, alfxdt))) return rc;
@@ -784,9 +798,9 @@ static int substep_core(eddy_ctx *ctx, int is, double dt) {
     ProfScope ps(ctx, PROF_TRIDIAG);
     if ((rc = launch_inversex(ctx, alfxdt))) return rc;
   }
-  if ((rc = ib_overlap_regen(ctx))) return rc;
+  if (!implicit && (rc = ib_overlap_regen(ctx))) return rc;
   // momforc_mod2 + velinterior (src/Eddy6.f:2526-2575)
-  if (ctx->ib) {
+  if (ctx->ib && !implicit) {
     ProfScope ps(ctx, PROF_IB_FORCE);
     const double *vb = ib_velocity(ctx);
     if ((rc = ib_force(ctx, 0, 0, f[EDDY_US], vb[0], vb[0], nullptr, 0))) return rc;

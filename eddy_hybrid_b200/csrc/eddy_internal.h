@@ -270,6 +270,10 @@ int ib_regen(eddy_ctx *ctx);
 // row pitch mpitch) receives every written value when non-null
 int ib_force(eddy_ctx *ctx, int q, int fq, double *a, double b0, double interior, float *mirror, int mpitch);
 int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, double interior);
+// the implicit forcing of the C.N. steps (impl = 1): stencil values from ub
+// (the explicit estimate), a + b(1) - ub at the forcing points (ub takes it
+// too), a - ub + b0 inside the body
+int ib_force_impl(eddy_ctx *ctx, int q, int fq, double *a, double *ub, double b0);
 const double *ib_velocity(eddy_ctx *ctx);
 int ib_set_cadence(eddy_ctx *ctx, int every_substep);
 int ib_every_substep(eddy_ctx *ctx);

@@ -140,7 +140,10 @@ int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
     k_dens_sponge<<<(unsigned)((ni + 255) / 256), 256, 0, ctx->stream>>>(d, ctx->m, ctx->sc, ctx->f[EDDY_DENS],
                                                                           alfxdt);
     EDDY_LAUNCHED(ctx);
-    return launch_boundinoutd_dens(ctx, ctx->f[EDDY_DENS]);
+    if ((rc = launch_boundinoutd_dens(ctx, ctx->f[EDDY_DENS]))) return rc;
+    // immersed body: correctdens_mod2 + densinterior (src/Eddy6.f:2972-2983)
+    if (ctx->ib) return ib_force(ctx, 3, 4, ctx->f[EDDY_DENS], 0.0, 0.0, nullptr, 0);
+    return EDDY_OK;
   }
   EDDY_CUDA(cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_density<<<g, dim3(DTX, DTY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, ctx->f[EDDY_RHA], ctx->dens_alt,

@@ -1803,10 +1803,15 @@ struct ForceArgs {
   const double *lu, *fw;
 };
 
+// src: null for the explicit forcing (momforc_mod2 impl = 0: the stencil
+// values from a, the point takes b(1)); else the implicit one (impl = 1,
+// src/momforc.f:1280-1340): the stencil values from src (UB), the point takes
+// a + b(1) - src, which src then takes too
 template <class T>
 __device__ __forceinline__ void force_point(const Dims &d, const Axes &ax, int pitch, int o, const ForceArgs &fa,
-                                            T *a, double b0, float *mirror, int mpitch) {
+                                            T *a, T *src, double b0, float *mirror, int mpitch) {
   const int im = fa.ijk[3 * o], jm = fa.ijk[3 * o + 1], km = fa.ijk[3 * o + 2];
+  const T *r = src ? src : a;
   double ae;
   if (fa.mrk[o] == 2) {
     int i1 = im + fa.dd[3 * o], j1 = jm + fa.dd[3 * o + 1], k1 = km + fa.dd[3 * o + 2];
@@ -1814,7 +1819,7 @@ __device__ __forceinline__ void force_point(const Dims &d, const Axes &ax, int p
       j1 = d.ny - 2 + j1;
     else if (j1 >= d.ny)
       j1 = j1 - d.ny + 2;
-    ae = (double)a[pidx(d, pitch, i1, j1, k1)];
+    ae = (double)r[pidx(d, pitch, i1, j1, k1)];
   } else {
     // interp_cellface's bilinear value on the face, from the cell and
     // weights found at regeneration
@@ -1832,22 +1837,28 @@ __device__ __forceinline__ void force_point(const Dims &d, const Axes &ax, int p
       q00 = pidx(d, pitch, i, j0, k); q10 = pidx(d, pitch, i + 1, j0, k);
       q01 = pidx(d, pitch, i, j1, k); q11 = pidx(d, pitch, i + 1, j1, k);
     }
-    ae = (((1 - w1) * (1 - w2) * (double)a[q00] + w1 * (1 - w2) * (double)a[q10]) + (1 - w1) * w2 * (double)a[q01]) +
-         w1 * w2 * (double)a[q11];
+    ae = (((1 - w1) * (1 - w2) * (double)r[q00] + w1 * (1 - w2) * (double)r[q10]) + (1 - w1) * w2 * (double)r[q01]) +
+         w1 * w2 * (double)r[q11];
   }
   double b[2] = {b0, ae};
   lusolve2(fa.lu + 4 * o, fa.indx + 2 * o, b);
-  a[pidx(d, pitch, im, jm, km)] = (T)b[0];
-  if (mirror) mirror[pidx(d, mpitch, im, jm, km)] = (float)b[0];
+  const long long c = pidx(d, pitch, im, jm, km);
+  double v = b[0];
+  if (src) {
+    v = (double)a[c] + b[0] - (double)src[c];
+    src[c] = (T)v;
+  }
+  a[c] = (T)v;
+  if (mirror) mirror[pidx(d, mpitch, im, jm, km)] = (float)v;
 }
 
 // the points of one level, one thread each
 template <class T>
-__global__ void k_force(Dims d, Axes ax, int pitch, int o0, int o1, ForceArgs fa, T *a, double b0, float *mirror,
-                        int mpitch) {
+__global__ void k_force(Dims d, Axes ax, int pitch, int o0, int o1, ForceArgs fa, T *a, T *src, double b0,
+                        float *mirror, int mpitch) {
   const int o = o0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= o1) return;
-  force_point<T>(d, ax, pitch, o, fa, a, b0, mirror, mpitch);
+  force_point<T>(d, ax, pitch, o, fa, a, src, b0, mirror, mpitch);
 }
 
 // offsets of the dependency levels (level l: [v[l], v[l+1]))
@@ -1859,10 +1870,11 @@ struct LevOffsets {
 // wrote, which the block barrier makes visible
 template <class T>
 __global__ void __launch_bounds__(1024) k_force_levels(Dims d, Axes ax, int pitch, LevOffsets ls, int l0, int l1,
-                                                       ForceArgs fa, T *a, double b0, float *mirror, int mpitch) {
+                                                       ForceArgs fa, T *a, T *src, double b0, float *mirror,
+                                                       int mpitch) {
   for (int l = l0; l < l1; l++) {
     for (int o = ls.v[l] + threadIdx.x; o < ls.v[l + 1]; o += blockDim.x)
-      force_point<T>(d, ax, pitch, o, fa, a, b0, mirror, mpitch);
+      force_point<T>(d, ax, pitch, o, fa, a, src, b0, mirror, mpitch);
     __syncthreads();
   }
 }
@@ -1882,18 +1894,21 @@ __global__ void k_yper_field(Dims d, int pitch, T *a, float *mirror, int mpitch)
   }
 }
 
-// interior value at flag == 1 over the body box
+// interior value at flag == 1 over the body box; with src (velinterior impl
+// = 1, src/momforc.f:235-248) a - src + value instead
 template <class T>
-__global__ void k_interior(Dims d, int pitch, Box6 L, const signed char *flag, T *a, double value, float *mirror,
-                           int mpitch) {
+__global__ void k_interior(Dims d, int pitch, Box6 L, const signed char *flag, T *a, const T *src, double value,
+                           float *mirror, int mpitch) {
   // blockIdx.y is the plane k of the box; 32-bit arithmetic inside it
   const int ni = L.imax - L.imin + 1, nj = L.jmax - L.jmin + 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ni * nj) return;
   const int j = L.jmin + t / ni, i = L.imin + (t - (j - L.jmin) * ni), k = L.kmin + blockIdx.y;
   if (flag[lidx(d.nx, d.ny, i, j, k)] == 1) {
-    a[pidx(d, pitch, i, j, k)] = (T)value;
-    if (mirror) mirror[pidx(d, mpitch, i, j, k)] = (float)value;
+    const long long c = pidx(d, pitch, i, j, k);
+    const double v = src ? (double)a[c] - (double)src[c] + value : value;
+    a[c] = (T)v;
+    if (mirror) mirror[pidx(d, mpitch, i, j, k)] = (float)v;
   }
 }
 
@@ -2394,7 +2409,7 @@ static int ib_regen_impl(eddy_ctx *ctx) {
 // forcing of an array by stencil set q, then its interior value at flag fq
 template <class T>
 static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, double interior, float *mirror,
-                   int mpitch) {
+                   int mpitch, T *src = nullptr) {
   IbState *s = ibs(ctx);
   const Dims &d = ctx->d;
   cudaStream_t st = cur_stream(ctx);
@@ -2418,12 +2433,12 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
       continue;
     }
     if (run0 >= 0) {
-      k_force_levels<T><<<1, 1024, 0, st>>>(d, ax, pitch, ls, run0, l, fa, a, b0, mirror, mpitch);
+      k_force_levels<T><<<1, 1024, 0, st>>>(d, ax, pitch, ls, run0, l, fa, a, src, b0, mirror, mpitch);
       EDDY_LAUNCHED(ctx);
       run0 = -1;
     }
     if (!end) {
-      k_force<T><<<nblk(cnt, 128), 128, 0, st>>>(d, ax, pitch, S.lev_start[l], S.lev_start[l + 1], fa, a, b0,
+      k_force<T><<<nblk(cnt, 128), 128, 0, st>>>(d, ax, pitch, S.lev_start[l], S.lev_start[l + 1], fa, a, src, b0,
                                                   mirror, mpitch);
       EDDY_LAUNCHED(ctx);
     }
@@ -2435,7 +2450,7 @@ static int force_t(eddy_ctx *ctx, int q, int fq, T *a, int pitch, double b0, dou
   const Box6 L = s->lim;
   const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
   if (nbx > 0) {
-    k_interior<T><<<box_grid(L), 256, 0, st>>>(d, pitch, L, s->flag[fq], a, interior, mirror, mpitch);
+    k_interior<T><<<box_grid(L), 256, 0, st>>>(d, pitch, L, s->flag[fq], a, src, interior, mirror, mpitch);
     EDDY_LAUNCHED(ctx);
   }
   k_yper_field<T><<<nblk((long long)d.nx * d.nz), 256, 0, st>>>(d, pitch, a, mirror, mpitch);
@@ -2447,6 +2462,14 @@ int ib_force(eddy_ctx *ctx, int q, int fq, double *a, double b0, double interior
   if (int rcj = ib_join(ctx)) return rcj;
   if (!ibs(ctx)) return EDDY_OK;
   return force_t<double>(ctx, q, fq, a, ctx->d.nx, b0, interior, mirror, mpitch);
+}
+
+// the implicit forcing (momforc_mod2 and velinterior with impl = 1): stencil
+// values from ub, a := a + b(1) - ub at the forcing points, a - ub + b0 inside
+int ib_force_impl(eddy_ctx *ctx, int q, int fq, double *a, double *ub, double b0) {
+  if (int rcj = ib_join(ctx)) return rcj;
+  if (!ibs(ctx)) return EDDY_OK;
+  return force_t<double>(ctx, q, fq, a, ctx->d.nx, b0, b0, nullptr, 0, ub);
 }
 
 int ib_force32(eddy_ctx *ctx, int q, int fq, float *a, int pitch, double b0, double interior) {
@@ -2475,7 +2498,8 @@ int ib_interior(eddy_ctx *ctx, int fq, double *a, double value, float *mirror, i
   const Box6 L = s->lim;
   const long long nbx = (long long)(L.imax - L.imin + 1) * (L.jmax - L.jmin + 1) * std::max(0, L.kmax - L.kmin + 1);
   if (nbx > 0) {
-    k_interior<double><<<box_grid(L), 256, 0, cur_stream(ctx)>>>(d, d.nx, L, s->flag[fq], a, value, mirror, mpitch);
+    k_interior<double><<<box_grid(L), 256, 0, cur_stream(ctx)>>>(d, d.nx, L, s->flag[fq], a, nullptr, value, mirror,
+                                                                 mpitch);
     EDDY_LAUNCHED(ctx);
   }
   k_yper_field<double><<<nblk((long long)d.nx * d.nz), 256, 0, cur_stream(ctx)>>>(d, d.nx, a, mirror, mpitch);

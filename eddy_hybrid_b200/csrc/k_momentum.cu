@@ -32,12 +32,16 @@ struct MomAcc {
 };
 
 // CN: bit 0 IMPLY, bit 1 IMPLX (the C.N. parts of those axes' viscous terms)
+// ub, vb, wb (C.N. steps with an immersed body, else null): the explicit
+// estimate u* + alfxdt/2 (C.N. part) the implicit forcing reads
+// (UB = US + 0.5*ALFXDT*UB, src/Eddy6.f:2499-2501)
 template <int CN>
 __global__ void __launch_bounds__(TX *TY)
     k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const __grid_constant__ TmaMaps<NFLD> maps,
                      double *__restrict__ us, double *__restrict__ vs, double *__restrict__ ws,
                      double *__restrict__ ua, double *__restrict__ va, double *__restrict__ wa, double alfxdt,
-                     double gamxdt, double rhoxdt, int *err) {
+                     double gamxdt, double rhoxdt, int *err, double *__restrict__ ub, double *__restrict__ vb,
+                     double *__restrict__ wb) {
   const double coef = 0.5 * alfxdt, coefd = alfxdt;
   tma_march<NFLD, TX, TY, KCHUNK>(
       d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err, [&](int i, int j, int k, bool active, const Acc9 &R) {
@@ -47,7 +51,7 @@ __global__ void __launch_bounds__(TX *TY)
         const bool jin = j >= d.jy1 && j <= d.jy2;
         const bool kin = (k >= d.kz1 && k <= d.kz2);
         // ---- u ----
-        double uval = 0.0;
+        double uval = 0.0, ubv = 0.0;
         if (kin && jin && i >= d.ibu && i <= d.ieu) {
           double ucn = 0.0;  // the C.N. part (IMPLY / IMPLX), else 0
           double ur = rhs_u<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &ucn);
@@ -61,10 +65,12 @@ __global__ void __launch_bounds__(TX *TY)
           if (i >= d.ieu - s.vspngx1) ustar = ustar + m.dfxu[i] * (0. - ustar) * alfxdt * 1.0;
           if (s.ivspngl == 1) ustar = ustar + m.dfxul[k] * (0. - ustar) * alfxdt * 1.0;
           uval = ustar;
+          ubv = ustar + coef * ucn;
         }
         us[q] = uval;
+        if (ub) ub[q] = ubv;
         // ---- v ----
-        double vval = 0.0;
+        double vval = 0.0, vbv = 0.0;
         if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
           double vcn = 0.0;
           double vr = rhs_v<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &vcn);
@@ -75,10 +81,12 @@ __global__ void __launch_bounds__(TX *TY)
           if (s.ivspngl == 1 && i >= d.ibu && i <= d.ieu && jin)
             vstar = vstar + m.dfxwl[k] * (0. - vstar) * alfxdt * 1.0;
           vval = vstar;
+          vbv = vstar + coef * vcn;
         }
         vs[q] = vval;
+        if (vb) vb[q] = vbv;
         // ---- w ----
-        double wval = 0.0;
+        double wval = 0.0, wbv = 0.0;
         if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
           double wcn = 0.0;
           double wr = rhs_w<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &wcn);
@@ -88,8 +96,10 @@ __global__ void __launch_bounds__(TX *TY)
           if (i >= d.ix2 - s.vspngx1) wstar = wstar + m.dfxw[i] * (1. - wstar) * alfxdt * 1.0;
           if (s.ivspngl == 1) wstar = wstar + m.dfxwl[k] * (1. - wstar) * alfxdt * 1.0;
           wval = wstar;
+          wbv = wstar + coef * wcn;
         }
         ws[q] = wval;
+        if (wb) wb[q] = wbv;
       });
 }
 
@@ -242,14 +252,20 @@ int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rh
   auto kern = cn == 3 ? k_rhs_predictord<3> : cn == 2 ? k_rhs_predictord<2> : cn == 1 ? k_rhs_predictord<1>
                                                                                      : k_rhs_predictord<0>;
   EDDY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const bool est = cn && ctx->ib;  // the implicit forcing's explicit estimate
+  double *ub = est ? f[EDDY_UB] : nullptr, *vb = est ? f[EDDY_VB] : nullptr, *wb = est ? f[EDDY_WB] : nullptr;
   kern<<<g, dim3(TX, TY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, f[EDDY_US], f[EDDY_VS], f[EDDY_WS],
                                               f[EDDY_UA], f[EDDY_VA], f[EDDY_WA], alfxdt, gamxdt, rhoxdt,
-                                              ctx->err_flag);
+                                              ctx->err_flag, ub, vb, wb);
   EDDY_LAUNCHED(ctx);
   long long nghost = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
   k_zero_faces3<<<(unsigned)((nghost + 255) / 256), 256, 0, ctx->stream>>>(d, f[EDDY_US], f[EDDY_VS],
                                                                             f[EDDY_WS]);
   EDDY_LAUNCHED(ctx);
+  if (est) {
+    k_zero_faces3<<<(unsigned)((nghost + 255) / 256), 256, 0, ctx->stream>>>(d, ub, vb, wb);
+    EDDY_LAUNCHED(ctx);
+  }
   return EDDY_OK;
 }
 

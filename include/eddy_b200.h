@@ -63,14 +63,16 @@ typedef struct {
   int imply;                 /* IMPLY (src/inpall.f:42): 1 = the viscous terms along y
                                 Crank-Nicolson implicit (INVERSEY src/timeindeg.f:120,
                                 INVERSEYD src/density.f:383), over the whole x range
-                                (IMPLYDCMP = 0); plain form without an immersed body.
+                                (IMPLYDCMP = 0); plain form.  With an immersed body
+                                the velocity forcing runs before the line solves,
+                                from the explicit estimate (src/Eddy6.f:2495-2575).
                                 The implicit convective terms (IMPLCY, IMPLCX) are
                                 not supported. */
   int implx;                 /* IMPLX: 1 = the viscous terms along x Crank-Nicolson
                                 implicit (INVERSEX src/timeindeg.f:344, INVERSEXD
                                 src/density.f:129) over the whole x range
                                 (IMPLXDCMP = 0), with slip walls (type 60) on both
-                                x boundaries; plain form without an immersed body. */
+                                x boundaries; plain form. */
 } eddy_params;
 
 typedef struct eddy_ctx eddy_ctx;

@@ -206,6 +206,8 @@ void eo_ib_regen(eo_ib *ib);
 void eo_ib_move(eo_ib *ib, double tmove);
 void eo_ib_force(eo_ib *ib, int q, double *a, double b0);
 void eo_ib_interior(eo_ib *ib, int fq, double *a, double value);
+void eo_ib_force_impl(eo_ib *ib, int q, double *us, double *ub, double b0);
+void eo_ib_interior_impl(eo_ib *ib, int fq, double *us, const double *ub, double value);
 const int *eo_ib_limits(const eo_ib *ib);
 const signed char *eo_ib_tags(const eo_ib *ib, int q);
 const signed char *eo_ib_flags(const eo_ib *ib, int fq);

@@ -1453,6 +1453,52 @@ void eo_ib_force(eo_ib *ib, int q, double *a, double b0) {
   }
 }
 
+/* momforc_mod2 with impl = 1 (src/momforc.f:1280-1372): the stencil values
+ * come from UB (the explicit estimate us + alfxdt/2 C.N. part); each forcing
+ * point takes us + b(1) - ub, which ub then takes too (later levels read it);
+ * the y ghost planes of us are refreshed after every level */
+void eo_ib_force_impl(eo_ib *ib, int q, double *us, double *ub, double b0) {
+  const eo_grid *g = ib->g;
+  const double *X, *Y, *Z;
+  var_axes(g, q, &X, &Y, &Z);
+  eo_ib_set *S = &ib->set[q];
+  for (int l = 0; l < S->nlev; l++) {
+    for (int o = S->lev_start[l]; o < S->lev_start[l + 1]; o++) {
+      double ae;
+      if (S->mrk[o] == 2) {
+        int i1 = S->i[o] + S->di[o], j1 = S->j[o] + S->dj[o], k1 = S->k[o] + S->dk[o];
+        if (j1 <= 1)
+          j1 = g->ny - 2 + j1;
+        else if (j1 >= g->ny)
+          j1 = j1 - g->ny + 2;
+        ae = ub[IDX(g, i1, j1, k1)];
+      } else {
+        const double xe[3] = {S->xe[o], S->ye[o], S->ze[o]};
+        ae = interp_face(g, X, Y, Z, ub, xe, S->dir[o]);
+      }
+      double b[2] = {b0, ae};
+      eo_lusolve2(S->lu + 4 * o, S->indx + 2 * o, b);
+      const size_t c = IDX(g, S->i[o], S->j[o], S->k[o]);
+      us[c] = us[c] + b[0] - ub[c];
+      ub[c] = us[c];
+    }
+    yper(g, us);
+  }
+}
+
+/* velinterior with impl = 1 (src/momforc.f:235-248): us - ub + the body
+ * velocity at flag == 1 */
+void eo_ib_interior_impl(eo_ib *ib, int fq, double *us, const double *ub, double value) {
+  const eo_grid *g = ib->g;
+  const int *L = ib->lim;
+  const signed char *f = ib->flag[fq];
+  for (int k = L[4]; k <= L[5]; k++)
+    for (int j = L[2]; j <= L[3]; j++)
+      for (int i = L[0]; i <= L[1]; i++)
+        if (f[IDX(g, i, j, k)] == 1) us[IDX(g, i, j, k)] = us[IDX(g, i, j, k)] - ub[IDX(g, i, j, k)] + value;
+  yper(g, us);
+}
+
 /* velinterior / presinterior / densinterior / tvinterior: value at flag == 1 */
 void eo_ib_interior(eo_ib *ib, int fq, double *a, double value) {
   const eo_grid *g = ib->g;

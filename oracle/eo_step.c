@@ -36,8 +36,27 @@ void eo_substep(eo_state *s, int is, double dtm1) {
   eo_rhs(s, s->uo, s->vo, s->wo, s->tv, s->us, s->vs, s->ws, s->ub, s->vb, s->wb, s->dp);
   /* :2484 */
   eo_predictord(s, alfxdt, gamxdt, rhoxdt);
+  const int implicit = s->prm.imply == 1 || s->prm.implx == 1;
   /* momentum forcing and body velocity inside (:2526-2575) */
-  if (s->ib) {
+  if (s->ib && implicit) {
+    /* :2495-2520: UB = US + alfxdt/2 UB (UB holds the C.N. parts), its
+     * boundary conditions, then the forcing of US from it (impl = 1) */
+    for (long q = 0; q < s->ncell; q++) {
+      s->ub[q] = s->us[q] + 0.5 * alfxdt * s->ub[q];
+      s->vb[q] = s->vs[q] + 0.5 * alfxdt * s->vb[q];
+      s->wb[q] = s->ws[q] + 0.5 * alfxdt * s->wb[q];
+    }
+    eo_boundary(s, s->ub, s->vb, s->wb);
+    eo_boundinout(s, s->ub, s->vb, s->wb, s->uo, s->vo, s->wo, alfxdt, 1);
+    eo_boundary(s, s->ub, s->vb, s->wb);
+    const double *vel = eo_ib_velocity(s->ib);
+    eo_ib_force_impl(s->ib, 0, s->us, s->ub, vel[0]);
+    eo_ib_force_impl(s->ib, 1, s->vs, s->vb, vel[1]);
+    eo_ib_force_impl(s->ib, 2, s->ws, s->wb, vel[2]);
+    eo_ib_interior_impl(s->ib, 0, s->us, s->ub, vel[0]);
+    eo_ib_interior_impl(s->ib, 1, s->vs, s->vb, vel[1]);
+    eo_ib_interior_impl(s->ib, 2, s->ws, s->wb, vel[2]);
+  } else if (s->ib) {
     const double *vel = eo_ib_velocity(s->ib);
     eo_ib_force(s->ib, 0, s->us, vel[0]);
     eo_ib_force(s->ib, 1, s->vs, vel[1]);
@@ -46,8 +65,9 @@ void eo_substep(eo_state *s, int is, double dtm1) {
     eo_ib_interior(s->ib, 1, s->vs, vel[1]);
     eo_ib_interior(s->ib, 2, s->ws, vel[2]);
   }
-  /* Crank-Nicolson y, then x lines (:2582-2607; the IBM = 0 sequence) */
-  if (s->prm.implx == 1) eo_inversex_walls(s, alfxdt);
+  /* Crank-Nicolson y, then x lines (:2582-2607; the IBM = 0 planes of UB
+   * only without a body) */
+  if (s->prm.implx == 1 && !s->ib) eo_inversex_walls(s, alfxdt);
   if (s->prm.imply == 1) eo_inversey(s, alfxdt);
   if (s->prm.implx == 1) eo_inversex(s, alfxdt);
   /* :2689-2704 */

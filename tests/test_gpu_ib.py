@@ -112,3 +112,26 @@ def test_mixed_form_with_sphere(oracle, product):
         a, b = g.download(n)[1:-1, 1:-1, 1:-1], o.get(n)[1:-1, 1:-1, 1:-1]
         assert float(np.sqrt(np.mean((a - b) ** 2))) < 1e-4, n
     assert g.max_divergence() < 1e-10
+
+
+@pytest.mark.parametrize("imply,implx", [(1, 0), (0, 1), (1, 1)])
+def test_steps_with_moving_sphere_crank_nicolson(oracle, product, imply, implx):
+    # the C.N. steps with a body: the forcing from the explicit estimate UB
+    # before the line solves (momforc_mod2 / velinterior with impl = 1)
+    w = config.small(mx=32, ly=16, nz_=40, noise=0.2, re=2000.0, imply=imply, implx=implx)
+    vel = (0.0, 0.0, -1.0)
+    o, ib, g = _pair(oracle, product, w, 3, vel, attach=True)
+    f = _initial(o, w)
+    o.load_initial(f)
+    o.initialize()
+    g.load_initial(f)
+    g.initialize()
+    scale = run_with_scale(o, 3)
+    g.step(3)
+    for n in ("uo", "vo", "wo", "dens", "tv"):
+        e = rel_err(g.download(n), o.get(n))
+        assert e < 1e-11, (n, e)
+    pg = g.download("p")
+    assert p_err(pg, o.get("p"), scale) < P_BAR
+    assert p_profile_err(pg, o.get("p"), scale) < P_PROFILE_BAR
+    assert g.max_divergence() < 1e-12
