@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--profile", default=None, choices=["plain", "mixed"],
                     help="run one form (warm-up + steps, the dynamic model) and exit without timing: the "
                          "command to put under a profiler")
+    ap.add_argument("--poisson", action="store_true",
+                    help="time the 256^3 Poisson solve alone (plain FP64 and refined FP32)")
     ap.add_argument("--deploy", action="store_true",
                     help="the learned closure deployed on 768x512x384 (Re 2e4, Fr 1, the moving sphere) for "
                          "--deploy-steps steps against a plain FP64 run: nu_t error against the dynamic model and "
@@ -432,12 +434,70 @@ def run_deploy(args):
     print(json.dumps({"deploy": out}), flush=True)
 
 
+def run_poisson(args):
+    """The Poisson solve in isolation on the 256^3 grid stretched 2.5 along x
+    and z around the periodic y (seed-7 N(0,1) right-hand side, its
+    volume-weighted mean removed): the plain FP64 solve and the mixed form's
+    FP32 transforms with two FP64-residual sweeps, timed on the device (CUDA
+    events around repeated solves of a device-resident right-hand side).  Their
+    accuracy against the oracle is the parity tests' (config 1)."""
+    import ctypes
+    import numpy as np
+    import torch
+    import eddy_hybrid_b200 as eb
+    from eddy_hybrid_b200 import config
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    w = config.poisson_256x256x256()
+    rng = np.random.RandomState(7)
+    d = np.zeros((w.nx, w.ny, w.nz), order="F")
+    d[1:-1, 1:-1, 1:-1] = rng.randn(w.mx, w.ly, w.nz_)
+    out = {"workload": w.name, "cells": w.ncell, "repeats": args.steps, "warmup": args.warmup}
+    for name, prec in (("plain_fp64", eb.PLAIN_FP64), ("refined_fp32_2_sweeps", eb.MIXED)):
+        g = eb.Solver(w, precision=prec, refine_sweeps=2)
+        ap, cp = g.metric("ap")[: w.nx], g.metric("cp")[: w.nz]
+        vol = (1 / ap[1:-1])[:, None, None] * np.ones((1, w.ly, 1)) * (1 / cp[1:-1])[None, None, :]
+        dd = d.copy(order="F")
+        inner = dd[1:-1, 1:-1, 1:-1]
+        inner -= (inner * vol).sum() / vol.sum()
+        rhs = torch.from_numpy(dd.ravel(order="F").copy()).to(dev)
+        sol = torch.empty_like(rhs)
+        pr = ctypes.cast(rhs.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        ps = ctypes.cast(sol.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        stream = torch.cuda.ExternalStream(g.stream, device=dev)
+
+        def solve():
+            g._check(eb.lib().eddy_poisson_solve(g.h, pr, ps, 1), "eddy_poisson_solve")
+
+        torch.cuda.synchronize()
+        for _ in range(args.warmup):
+            solve()
+        g.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            solve()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        r = {"ms_per_solve": ms, "Mcells_per_s": w.ncell / (ms / 1e3) / 1e6}
+        if prec == eb.MIXED:
+            r["pre_sweep_residuals_relative"] = [float(v) / float(np.max(np.abs(inner)))
+                                                 for v in g.refine_residuals()[:2]]
+        out[name] = r
+        g.close()
+        del g
+    print(json.dumps({"poisson": out}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.deploy:
         return run_deploy(args)
+    if args.poisson:
+        return run_poisson(args)
     rank, world, local, dist = dist_init(args.gpus)
     import numpy as np
     import torch
