@@ -44,7 +44,8 @@ class Params(C.Structure):
                 ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
                 ("dspngx3in", C.c_int), ("dspngx3out", C.c_int),
                 ("precision", C.c_int), ("refine_sweeps", C.c_int),
-                ("closure", C.c_int), ("imply", C.c_int), ("implx", C.c_int)]
+                ("closure", C.c_int), ("imply", C.c_int), ("implx", C.c_int),
+                ("implcx", C.c_int), ("implcy", C.c_int)]
 
 
 def make_params(d: dict, precision: int = PLAIN_FP64, refine_sweeps: int = 2,

@@ -82,6 +82,8 @@ class Workload:
     body_speed: float = 0.0
     imply: int = 0     # Crank-Nicolson viscous terms along y (the reference input's IMPLY)
     implx: int = 0     # Crank-Nicolson viscous terms along x (IMPLX)
+    implcx: int = 0    # Crank-Nicolson convective terms along x (IMPLCX)
+    implcy: int = 0    # Crank-Nicolson convective terms along y (IMPLCY)
 
     @property
     def nx(self) -> int:
@@ -115,7 +117,7 @@ class Workload:
             vspngx1=max(2, self.mx // 24), dspngx1=max(2, self.mx // 24),
             vspngx3in=0, vspngx3out=0, dspngx3in=0,
             dspngx3out=max(4, self.nz_ // 14),
-            imply=self.imply, implx=self.implx,
+            imply=self.imply, implx=self.implx, implcx=self.implcx, implcy=self.implcy,
         )
 
 

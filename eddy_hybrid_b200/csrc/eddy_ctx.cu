@@ -201,7 +201,7 @@ void build_metrics(eddy_ctx *ctx, const double *xf, double ymin, double ymax, co
   s.ru1 = p.ru1; s.prn = p.prn; s.grav = p.grav; s.dpdx = p.dpdx; s.dpdy = p.dpdy; s.dpdz = p.dpdz;
   s.eps = p.eps; s.css = p.css; s.vspngx1 = p.vspngx1; s.dspngx1 = p.dspngx1;
   s.ivspngl = ivs; s.idspngl = ids; s.idens = p.idens; s.isgs = p.isgs; s.imply = p.imply;
-  s.implx = p.implx;
+  s.implx = p.implx; s.implcx = p.implcx; s.implcy = p.implcy;
 }
 
 int upload_metrics(eddy_ctx *ctx) {
@@ -359,6 +359,14 @@ int eddy_create(eddy_ctx **out, const eddy_params *prm, const double *xu_faces, 
     return fail(EDDY_EINVAL, "the implicit x terms (implx = 1) are built for the plain FP64 form with the dynamic model");
   if (p.implx == 1 && (p.itype[1] != 60 || p.itype[2] != 60))
     return fail(EDDY_EINVAL, "implx = 1 is built for slip walls (type 60) on both x boundaries");
+  if (p.implcx != 0 && p.implcx != 1) return fail(EDDY_EINVAL, "implcx must be 0 or 1");
+  if (p.implcy != 0 && p.implcy != 1) return fail(EDDY_EINVAL, "implcy must be 0 or 1");
+  if ((p.implcx == 1 || p.implcy == 1) && (p.precision != EDDY_PLAIN_FP64 || p.closure != 0))
+    return fail(EDDY_EINVAL,
+                "the implicit convective terms (implcx, implcy = 1) are built for the plain FP64 form with the dynamic model");
+  if (p.implcx == 1 && (p.itype[1] != 60 || p.itype[2] != 60))
+    return fail(EDDY_EINVAL, "implcx = 1 is built for slip walls (type 60) on both x boundaries");
+  if (p.implcy == 1 && p.ny - 2 < 3) return fail(EDDY_EINVAL, "implcy = 1 needs at least 3 cells along y");
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return fail(EDDY_ECUDA, "cudaSetDevice failed");
   // the regeneration's stream has the highest priority: its short kernels
@@ -497,8 +505,8 @@ int eddy_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhox
 
 int eddy_inversey(eddy_ctx *ctx, double alfxdt) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
-  if (ctx->prm.imply != 1) {
-    ctx->err = "eddy_inversey needs imply = 1";
+  if (ctx->prm.imply != 1 && ctx->prm.implcy != 1) {
+    ctx->err = "eddy_inversey needs imply = 1 or implcy = 1";
     return EDDY_EINVAL;
   }
   return launch_inversey(ctx, alfxdt);
@@ -506,8 +514,8 @@ int eddy_inversey(eddy_ctx *ctx, double alfxdt) {
 
 int eddy_inversex(eddy_ctx *ctx, double alfxdt) {
   if (check_ctx(ctx)) return EDDY_EINVAL;
-  if (ctx->prm.implx != 1) {
-    ctx->err = "eddy_inversex needs implx = 1";
+  if (ctx->prm.implx != 1 && ctx->prm.implcx != 1) {
+    ctx->err = "eddy_inversex needs implx = 1 or implcx = 1";
     return EDDY_EINVAL;
   }
   return launch_inversex(ctx, alfxdt);
@@ -789,23 +797,24 @@ static int substep_core(eddy_ctx *ctx, int is, double dt) {
     if ((rc = ib_force_impl(ctx, 1, 1, f[EDDY_VS], f[EDDY_VB], vb[1]))) return rc;
     if ((rc = ib_force_impl(ctx, 2, 2, f[EDDY_WS], f[EDDY_WB], vb[2]))) return rc;
   }
-  // Crank-Nicolson y, then x lines (src/Eddy6.f:2596-2607)
-  if (ctx->sc.imply == 1) {
-    ProfScope ps(ctx, PROF_TRIDIAG);
-    if ((rc = launch_inversey(ctx, alfxdt))) return rc;
-  }
-  if (ctx->sc.implx == 1) {
-    ProfScope ps(ctx, PROF_TRIDIAG);
-    if ((rc = launch_inversex(ctx, alfxdt))) return rc;
-  }
   if (!implicit && (rc = ib_overlap_regen(ctx))) return rc;
-  // momforc_mod2 + velinterior (src/Eddy6.f:2526-2575)
+  // momforc_mod2 + velinterior (src/Eddy6.f:2526-2575), before any line
+  // solve of the convective terms alone (impl = 0)
   if (ctx->ib && !implicit) {
     ProfScope ps(ctx, PROF_IB_FORCE);
     const double *vb = ib_velocity(ctx);
     if ((rc = ib_force(ctx, 0, 0, f[EDDY_US], vb[0], vb[0], nullptr, 0))) return rc;
     if ((rc = ib_force(ctx, 1, 1, f[EDDY_VS], vb[1], vb[1], nullptr, 0))) return rc;
     if ((rc = ib_force(ctx, 2, 2, f[EDDY_WS], vb[2], vb[2], nullptr, 0))) return rc;
+  }
+  // Crank-Nicolson y, then x lines (src/Eddy6.f:2596-2607)
+  if (ctx->sc.imply == 1 || ctx->sc.implcy == 1) {
+    ProfScope ps(ctx, PROF_TRIDIAG);
+    if ((rc = launch_inversey(ctx, alfxdt))) return rc;
+  }
+  if (ctx->sc.implx == 1 || ctx->sc.implcx == 1) {
+    ProfScope ps(ctx, PROF_TRIDIAG);
+    if ((rc = launch_inversex(ctx, alfxdt))) return rc;
   }
   {
     ProfScope ps(ctx, PROF_BC);

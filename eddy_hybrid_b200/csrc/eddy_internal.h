@@ -41,6 +41,7 @@ struct Scalars {
   int vspngx1, dspngx1, ivspngl, idspngl, idens, isgs;
   int imply;  // IMPLY: Crank-Nicolson viscous terms along y
   int implx;  // IMPLX: Crank-Nicolson viscous terms along x
+  int implcx, implcy;  // IMPLCX, IMPLCY: Crank-Nicolson convective terms along x, y
 };
 
 // Poisson plan (src/direct.f SAVE state): eigen-transform of the x operator.
@@ -243,6 +244,7 @@ int launch_turvis(eddy_ctx *ctx);
 // INVERSEYD on RS (IMPLY = 1)
 int launch_inversey(eddy_ctx *ctx, double alfxdt);
 int launch_inverseyd(eddy_ctx *ctx, double alfxdt);
+int launch_inverseyd_new(eddy_ctx *ctx, double alfxdt);
 int launch_inversex(eddy_ctx *ctx, double alfxdt);
 int launch_inversexd(eddy_ctx *ctx, double alfxdt);
 // FP32 dynamic procedure on FP32 velocities (row pitch px) -> TV (FP64)

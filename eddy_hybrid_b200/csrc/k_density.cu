@@ -41,19 +41,19 @@ __global__ void __launch_bounds__(DTX *DTY)
       });
 }
 
-// IMPLY = 1 or IMPLX = 1 (CN bit 0, bit 1): RHS_DENSITY with the diffusion
-// along those axes as the C.N. part rt, the DENSITY update with +coef*rt, no
-// sponges yet; the predicted density to rs
-template <int CN>
+// any of IMPLX, IMPLY, IMPLCX, IMPLCY = 1: RHS_DENSITY with the terms the flags
+// in f name as the C.N. part rt, the DENSITY update with +coef*rt, no sponges
+// yet; the predicted density to rs
 __global__ void __launch_bounds__(DTX *DTY)
     k_density_cn(Dims d, DevMetrics m, const __grid_constant__ TmaMaps<DNF> maps, double *__restrict__ rha,
-                 double *__restrict__ rs, double repr1, double alfxdt, double gamxdt, double rhoxdt, int *err) {
+                 double *__restrict__ rs, double repr1, double alfxdt, double gamxdt, double rhoxdt, int *err,
+                 CnFlags<double> f) {
   tma_march<DNF, DTX, DTY, DKC>(
       d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err,
       [&](int i, int j, int k, bool active, const RingAcc<DTX, DTY, DNF> &S) {
         if (!active) return;
         double rt = 0.;
-        double rr = rhs_dens<double, DevMetrics, RingAcc<DTX, DTY, DNF>, CN>(S, m, repr1, i, j, k, &rt);
+        double rr = rhs_dens<double, DevMetrics, RingAcc<DTX, DTY, DNF>, true>(S, m, repr1, i, j, k, &rt, &f);
         double coef = 0.5 * alfxdt;
         double dnew = S.at(0, 0, 0, 0) + gamxdt * rr + rhoxdt * S.at(5, 0, 0, 0) + coef * rt;
         long long q = fidx(d, i, j, k);
@@ -121,19 +121,29 @@ int launch_density(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt) {
   }
   size_t smem = ring_smem_bytes<DNF, DTX, DTY>();
   dim3 g((d.ix2 - d.ix1 + DTX) / DTX, (d.jy2 - d.jy1 + DTY) / DTY, (d.kz2 - d.kz1 + DKC) / DKC);
-  const int cn = (ctx->sc.imply == 1 ? 1 : 0) | (ctx->sc.implx == 1 ? 2 : 0);
-  if (cn) {
-    auto kern = cn == 3 ? k_density_cn<3> : cn == 2 ? k_density_cn<2> : k_density_cn<1>;
-    EDDY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<g, dim3(DTX, DTY), smem, ctx->stream>>>(d, ctx->m, maps, ctx->f[EDDY_RHA], ctx->f[EDDY_RS], repr1, alfxdt,
-                                                  gamxdt, rhoxdt, ctx->err_flag);
+  const Scalars &sc = ctx->sc;
+  const CnFlags<double> fl{(double)sc.implx, (double)sc.imply, (double)sc.implcx, (double)sc.implcy};
+  if (sc.imply == 1 || sc.implx == 1 || sc.implcx == 1 || sc.implcy == 1) {
+    EDDY_CUDA(cudaFuncSetAttribute(k_density_cn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_density_cn<<<g, dim3(DTX, DTY), smem, ctx->stream>>>(d, ctx->m, maps, ctx->f[EDDY_RHA], ctx->f[EDDY_RS], repr1,
+                                                          alfxdt, gamxdt, rhoxdt, ctx->err_flag, fl);
     EDDY_LAUNCHED(ctx);
-    // INVERSEYD then INVERSEXD on RS, each followed by DENS = RS in the
-    // reference (density.f:89-104); nothing reads DENS between, so one copy
-    if (cn & 1)
-      if ((rc = launch_inverseyd(ctx, alfxdt))) return rc;
-    if (cn & 2)
+    // INVERSEYD_NEW (IMPLY and IMPLCY) or INVERSEYD (IMPLY), then INVERSEXD
+    // (IMPLX or IMPLCX) on RS, each followed by DENS = RS in the reference
+    // (density.f:89-104); nothing reads DENS between, so one copy.  With IMPLCY
+    // alone the density has no line solve and no whole-array copy: the new
+    // interior lands in DENS, which keeps its own ghost cells, as there.
+    const bool ysolve = sc.imply == 1, xsolve = sc.implx == 1 || sc.implcx == 1;
+    if (ysolve)
+      if ((rc = sc.implcy == 1 ? launch_inverseyd_new(ctx, alfxdt) : launch_inverseyd(ctx, alfxdt))) return rc;
+    if (xsolve)
       if ((rc = launch_inversexd(ctx, alfxdt))) return rc;
+    if (!ysolve && !xsolve) {
+      const long long ng = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
+      k_dens_ghost_copy<<<(unsigned)((ng + 255) / 256), 256, 0, ctx->stream>>>(d, ctx->f[EDDY_DENS],
+                                                                               ctx->f[EDDY_RS]);
+      EDDY_LAUNCHED(ctx);
+    }
     EDDY_CUDA(cudaMemcpyAsync(ctx->f[EDDY_DENS], ctx->f[EDDY_RS], sizeof(double) * (size_t)d.ncell,
                               cudaMemcpyDeviceToDevice, ctx->stream));
     const long long ni = (long long)(d.ix2 - d.ix1 + 1) * (d.jy2 - d.jy1 + 1) * (d.kz2 - d.kz1 + 1);

@@ -17,9 +17,9 @@ constexpr int NB = 296;  // blocks of the first stage (2 per SM)
 __global__ void __launch_bounds__(256)
     k_cfl_partial(Dims d, DevMetrics m, const double *__restrict__ uo, const double *__restrict__ vo,
                   const double *__restrict__ wo, const double *__restrict__ tv, double ru1, double rflagx,
-                  double rflagy, double *part) {
+                  double rflagy, double rflagcx, double rflagcy, double *part) {
   __shared__ double sh[256];
-  const double cst = 2., rflagcx = 0., rflagcy = 0.;
+  const double cst = 2.;
   const long long mi = d.ix2 - d.ix1 + 1, mj = d.jy2 - d.jy1 + 1, mk = d.kz2 - d.kz1 + 1, n = mi * mj * mk;
   double mx = 0.;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -215,7 +215,8 @@ extern "C" int eddy_cfl(eddy_ctx *ctx, double *cflm) {
   double **f = ctx->f;
   double *part = ctx->diag, *out = ctx->diag + 2 * NB;
   k_cfl_partial<<<NB, 256, 0, ctx->stream>>>(d, ctx->m, f[EDDY_UO], f[EDDY_VO], f[EDDY_WO], f[EDDY_TV], ctx->sc.ru1,
-                                              (double)ctx->sc.implx, (double)ctx->sc.imply, part);
+                                              (double)ctx->sc.implx, (double)ctx->sc.imply,
+                                              (double)ctx->sc.implcx, (double)ctx->sc.implcy, part);
   EDDY_LAUNCHED(ctx);
   k_final<<<1, 32, 0, ctx->stream>>>(NB, part, out, 0);
   EDDY_LAUNCHED(ctx);

@@ -1,7 +1,8 @@
-// k_implicit.cu -- Crank-Nicolson viscous terms along the periodic y axis
-// (IMPLY = 1, IMPLYDCMP = 0): INVERSEY (src/timeindeg.f:120-340) on the
-// predicted velocities US, VS, WS and INVERSEYD (src/density.f:383-460) on
-// the predicted density RS; and along x (IMPLX = 1, IMPLXDCMP = 0): INVERSEX
+// k_implicit.cu -- Crank-Nicolson viscous (IMPLY) and convective (IMPLCY)
+// terms along the periodic y axis (IMPLYDCMP = 0): INVERSEY
+// (src/timeindeg.f:120-340) on the predicted velocities US, VS, WS and
+// INVERSEYD / INVERSEYD_NEW (src/density.f:290-460) on the predicted density
+// RS; and along x (IMPLX, IMPLCX; IMPLXDCMP = 0): INVERSEX
 // (src/timeindeg.f:344-690) and INVERSEXD (src/density.f:129-290).
 //
 // Every (i,k) line of a component is one periodic tridiagonal system over the
@@ -13,62 +14,101 @@
 // restatement's bit for bit.  The forward sweep writes the eliminated
 // solution in place, the multipliers and the Sherman-Morrison vector to two
 // scratch fields; two more sweeps finish the back substitution and the
-// correction.  Only the viscous part is implicit (IMPLCY = 0: the convective
-// coefficients of the reference are exact zeros).  Cartesian: rp = ru = 1.
+// correction.  The flags scale their coefficients at run time: a flag of 0
+// multiplies its terms by an exact zero, as the reference's rflag factors do.
+// Cartesian: rp = ru = 1.
 #include "eddy_internal.h"
 
 namespace {
 
-// row j of line (i,k): sub-, main and super-diagonal
-struct RowV {  // v: viscosity 2 tv(j) and 2 tv(j+1) on the faces (timeindeg.f:151-167)
-  const double *tv, *bv, *bp;
-  double coef, ru1;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+// row j of line (i,k): sub-, main and super-diagonal and an addend of the
+// right-hand side.  fy = rflagy (IMPLY) scales the viscous coefficients, fc =
+// rflagcy (IMPLCY) the convective ones (timeindeg.f:150-312)
+struct RowV {  // v: viscosity 2 tv(j) and 2 tv(j+1) on the faces; convection about VO
+  const double *tv, *bv, *bp, *vo;
+  double coef, ru1, fy, fc;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 2. * tv[fidx(d, i, j + 1, k)] + ru1, tvjm = 2. * tv[fidx(d, i, j, k)] + ru1;
-    const double coefy = 1.0 * coef * bv[j] / (1.0 * 1.0);
-    a = -coefy * bp[j] * tvjm;
-    c = -coefy * bp[j + 1] * tvjp;
-    b = 1.0 + (-a - c);
+    const double coefy = fy * coef * bv[j] / (1.0 * 1.0);
+    const double ayv = -coefy * bp[j] * tvjm, cyv = -coefy * bp[j + 1] * tvjp, byv = -ayv - cyv;
+    const double vm = vo[fidx(d, i, j - 1, k)], v0 = vo[fidx(d, i, j, k)], vp = vo[fidx(d, i, j + 1, k)];
+    const double coefc = fc * coef * bv[j] / 1.0;
+    const double ayc = -0.25 * coefc * (vm + v0) * 2.0, cyc = 0.25 * coefc * (vp + v0) * 2.0, byc = ayc + cyc;
+    a = ayv + ayc;
+    c = cyv + cyc;
+    b = 1.0 + byv + byc;
+    const double vyp = (vp + v0) * 0.5, vym = (v0 + vm) * 0.5;
+    r = coefc * (vyp * vyp - vym * vym);
   }
 };
-struct RowW {  // w: edge viscosity averaged over four cells (timeindeg.f:220-240)
-  const double *tv, *bw, *bv;
-  double coef, ru1;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+struct RowW {  // w: edge viscosity averaged over four cells; convection about the provisional VS
+  const double *tv, *bw, *bv, *vs;
+  double coef, ru1, fy, fc;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k + 1)] +
                                 tv[fidx(d, i, j + 1, k)]) + ru1;
     const double tvjm = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i, j - 1, k + 1)] +
                                 tv[fidx(d, i, j - 1, k)]) + ru1;
-    const double coefy = 1.0 * coef * bw[j] / (1.0 * 1.0);
-    a = -coefy * bv[j - 1] * tvjm;
-    c = -coefy * bv[j] * tvjp;
-    b = 1.0 + (-a - c);
+    const double coefy = fy * coef * bw[j] / (1.0 * 1.0);
+    const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+    const double vzp = (vs[fidx(d, i, j, k + 1)] + vs[fidx(d, i, j, k)]) * 0.5;
+    const double vzm = (vs[fidx(d, i, j - 1, k + 1)] + vs[fidx(d, i, j - 1, k)]) * 0.5;
+    const double coefc = fc * 0.5 * coef * bw[j] / 1.0;
+    const double ayc = -coefc * vzm, cyc = coefc * vzp, byc = ayc + cyc;
+    a = ayv + ayc;
+    c = cyv + cyc;
+    b = 1.0 + byv + byc;
+    r = 0.;
   }
 };
-struct RowU {  // u (timeindeg.f:290-312)
-  const double *tv, *bu, *bv;
-  double coef, ru1;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+struct RowU {  // u (timeindeg.f:290-312); convection about the provisional VS
+  const double *tv, *bu, *bv, *vs;
+  double coef, ru1, fy, fc;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 0.25 * (tv[fidx(d, i + 1, j, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j + 1, k)] +
                                 tv[fidx(d, i, j + 1, k)]) + ru1;
     const double tvjm = 0.25 * (tv[fidx(d, i + 1, j, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j - 1, k)] +
                                 tv[fidx(d, i, j - 1, k)]) + ru1;
-    const double coefy = 1.0 * coef * bu[j] / (1.0 * 1.0);
-    a = -coefy * bv[j - 1] * tvjm;
-    c = -coefy * bv[j] * tvjp;
-    b = 1.0 + (-a - c);
+    const double coefy = fy * coef * bu[j] / (1.0 * 1.0);
+    const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+    const double vxp = (vs[fidx(d, i + 1, j, k)] + vs[fidx(d, i, j, k)]) * 0.5;
+    const double vxm = (vs[fidx(d, i + 1, j - 1, k)] + vs[fidx(d, i, j - 1, k)]) * 0.5;
+    const double coefc = fc * 0.5 * coef * bu[j] / 1.0;
+    const double ayc = -coefc * vxm, cyc = coefc * vxp, byc = ayc + cyc;
+    a = ayv + ayc;
+    c = cyv + cyc;
+    b = 1.0 + byv + byc;
+    r = 0.;
   }
 };
 struct RowD {  // density (density.f:425-440): both faces take 0.5 (tv(j) + tv(j+1)) + ru1/prn
   const double *tv, *bp;
   double coef, kmol;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k)]) + kmol;
     const double tvjm = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k)]) + kmol;
     const double coefy = 1.0 * coef * bp[j] / (1.0 * 1.0);
     a = -coefy * bp[j - 1] * tvjm;
     c = -coefy * bp[j] * tvjp;
     b = 1.0 + (-a - c);
+    r = 0.;
+  }
+};
+struct RowDN {  // density, INVERSEYD_NEW (density.f:322-352): faces 0.5 (tv(j) + tv(j+/-1)) + ru1/prn, convection by VO
+  const double *tv, *bp, *bv, *vo;
+  double coef, kmol, fy, fc;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
+    const double tvjp = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k)]) + kmol;
+    const double tvjm = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j - 1, k)]) + kmol;
+    const double coefy = fy * coef * bp[j] / (1.0 * 1.0);
+    const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+    const double vzp = vo[fidx(d, i, j, k)], vzm = vo[fidx(d, i, j - 1, k)];
+    const double coefc = fc * 0.5 * coef * bp[j] / 1.0;
+    const double ayc = -coefc * vzm, cyc = coefc * vzp, byc = ayc + cyc;
+    a = ayv + ayc;
+    c = cyv + cyc;
+    b = 1.0 + byv + byc;
+    r = 0.;
   }
 };
 
@@ -87,9 +127,9 @@ __global__ void __launch_bounds__(128) k_cyclic_lines(Dims d, Row row, int i0, i
   for (int r = 0; r < n; r++) {
     const int j = d.jy1 + r;
     const long long q = fidx(d, i, j, k);
-    double a, b, c;
-    row(d, i, j, k, a, b, c);
-    const double rr = x[q];
+    double a, b, c, dr;
+    row(d, i, j, k, a, b, c, dr);
+    const double rr = x[q] + dr;
     if (r == 0) {
       beta = a;
       gamma = -b;
@@ -138,7 +178,7 @@ int lines(eddy_ctx *ctx, const Row &row, int i0, int i1, int k0, int k1, double 
   return EDDY_OK;
 }
 
-// ---- x lines (IMPLX = 1) ----
+// ---- x lines (IMPLX or IMPLCX = 1) ----
 // Every (j,k) line is one tridiagonal system over i1..i2 solved by tridag
 // (src/numrec.f:783-802) in its operation order, one thread per line (the
 // threads walk their lines in step; consecutive i of a line share a sector,
@@ -149,53 +189,73 @@ int lines(eddy_ctx *ctx, const Row &row, int i0, int i1, int k0, int k1, double 
 // and the density are Neumann (IBC = -1, src/setup.f:21-40: bdirb = 1,
 // rdirb = 0, rperb = 0), so the first and last rows take b + a and b + c and
 // every right-hand-side correction is a times an exact zero.
-struct RowXU {  // u (timeindeg.f:441-486): viscosity 2 tv(i) and 2 tv(i+1)
-  const double *tv, *au, *ap;
-  double coef, ru1;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+struct RowXU {  // u (timeindeg.f:441-486): viscosity 2 tv(i) and 2 tv(i+1); convection about UO
+  const double *tv, *au, *ap, *uo;
+  double coef, ru1, fx, fc;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvip = 2. * tv[fidx(d, i + 1, j, k)] + ru1, tvim = 2. * tv[fidx(d, i, j, k)] + ru1;
-    const double coefx = 1.0 * coef * au[i];
-    a = -coefx * ap[i] * tvim;
-    c = -coefx * ap[i + 1] * tvip;
-    b = 1.0 + (-a - c);
+    const double coefx = fx * coef * au[i];
+    const double axv = -coefx * ap[i] * tvim, cxv = -coefx * ap[i + 1] * tvip, bxv = -axv - cxv;
+    const double um = uo[fidx(d, i - 1, j, k)], u0 = uo[fidx(d, i, j, k)], up = uo[fidx(d, i + 1, j, k)];
+    const double coefc = fc * coef * au[i] / 1.0;
+    const double qxm = (u0 + um) * 0.5, qxp = (u0 + up) * 0.5;
+    const double axc = -coefc * qxm, cxc = coefc * qxp, bxc = axc + cxc;
+    a = axv + axc;
+    c = cxv + cxc;
+    b = 1.0 + bxv + bxc;
+    const double uxp = (up + u0) * 0.5, uxm = (um + u0) * 0.5;
+    r = coefc * (qxp * uxp - qxm * uxm);
   }
 };
-struct RowXV {  // v (timeindeg.f:528-560)
-  const double *tv, *av, *au;
-  double coef, ru1;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+struct RowXV {  // v (timeindeg.f:528-560); convection about the provisional US
+  const double *tv, *av, *au, *us;
+  double coef, ru1, fx, fc;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvip = 0.25 * (tv[fidx(d, i, j + 1, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j + 1, k)] +
                                 tv[fidx(d, i + 1, j, k)]) + ru1;
     const double tvim = 0.25 * (tv[fidx(d, i, j + 1, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i - 1, j + 1, k)] +
                                 tv[fidx(d, i - 1, j, k)]) + ru1;
-    const double coefx = 1.0 * coef * av[i] / 1.0;
-    a = -coefx * au[i - 1] * tvim;
-    c = -coefx * au[i] * tvip;
-    b = 1.0 + (-a - c);
+    const double coefx = fx * coef * av[i] / 1.0;
+    const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
+    const double coefc = fc * 0.5 * coef * av[i] / 1.0;
+    const double qyp = 1.0 * (us[fidx(d, i, j + 1, k)] + us[fidx(d, i, j, k)]) * 0.5;
+    const double qym = 1.0 * (us[fidx(d, i - 1, j + 1, k)] + us[fidx(d, i - 1, j, k)]) * 0.5;
+    const double axc = -coefc * qym, cxc = coefc * qyp, bxc = axc + cxc;
+    a = axv + axc;
+    c = cxv + cxc;
+    b = 1.0 + bxv + bxc;
+    r = 0.;
   }
 };
-struct RowXW {  // w (timeindeg.f:594-626)
-  const double *tv, *aw, *au;
-  double coef, ru1;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
+struct RowXW {  // w (timeindeg.f:594-626); convection about the provisional US
+  const double *tv, *aw, *au, *us;
+  double coef, ru1, fx, fc;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvip = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j, k + 1)] +
                                 tv[fidx(d, i + 1, j, k)]) + ru1;
     const double tvim = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i - 1, j, k + 1)] +
                                 tv[fidx(d, i - 1, j, k)]) + ru1;
-    const double coefx = 1.0 * coef * aw[i] / 1.0;
-    a = -coefx * au[i - 1] * tvim;
-    c = -coefx * au[i] * tvip;
-    b = 1.0 + (-a - c);
+    const double coefx = fx * coef * aw[i] / 1.0;
+    const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
+    const double coefc = fc * 0.5 * coef * aw[i] / 1.0;
+    const double qzp = 1.0 * (us[fidx(d, i, j, k + 1)] + us[fidx(d, i, j, k)]) * 0.5;
+    const double qzm = 1.0 * (us[fidx(d, i - 1, j, k + 1)] + us[fidx(d, i - 1, j, k)]) * 0.5;
+    const double axc = -coefc * qzm, cxc = coefc * qzp, bxc = axc + cxc;
+    a = axv + axc;
+    c = cxv + cxc;
+    b = 1.0 + bxv + bxc;
+    r = 0.;
   }
 };
 struct RowXD {  // density (density.f:212-240): the molecular diffusivity ru1/prn on both faces
   const double *aw, *au;
-  double coef, kmol;
-  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c) const {
-    const double coefx = 1.0 * coef * aw[i] / 1.0;
+  double coef, kmol, fx;
+  __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
+    const double coefx = fx * coef * aw[i] / 1.0;
     a = -coefx * au[i - 1] * kmol;
     c = -coefx * au[i] * kmol;
     b = 1.0 + (-a - c);
+    r = 0.;
   }
 };
 
@@ -212,9 +272,9 @@ __global__ void __launch_bounds__(64) k_x_lines(Dims d, Row row, int i1, int i2,
   double bet = 1., up = 0., cprev = 0.;
   for (int i = i1; i <= i2; i++) {
     const long long q = q1 + (i - i1);
-    double a, b, c;
-    row(d, i, j, k, a, b, c);
-    double r = x[q];
+    double a, b, c, dr;
+    row(d, i, j, k, a, b, c, dr);
+    double r = x[q] + dr;
     if (i == i1) {
       if (NEU) b = b + 1.0 * a;
       r = r - a * 0.0;
@@ -257,29 +317,32 @@ int xlines(eddy_ctx *ctx, const Row &row, int i1, int i2, int j0, int j1, int k0
 
 // INVERSEX: u lines (i in [2, NX-2], j in [jy1, jy2], k in [kz1, kz2]), then v
 // (i in [2, NX-1], j in [jbv, jev]) and w (i in [2, NX-1], k in [kbw, kew]);
-// the v and w systems read US only through the convective terms, which are
-// exact zeros (IMPLCX = 0); REFRESHBC is a no-op on one rank
+// rflagx = IMPLX and rflagcx = IMPLCX: the u systems linearise the convection
+// about UO, the v and w systems about the u lines' result in US (the launches
+// run in that order on one stream); REFRESHBC is a no-op on one rank
 int launch_inversex(eddy_ctx *ctx, double alfxdt) {
   const Dims &d = ctx->d;
   const DevMetrics &m = ctx->m;
   double **f = ctx->f;
   const double coef = 0.5 * alfxdt, ru1 = ctx->sc.ru1;
   int rc;
-  if ((rc = xlines<RowXU, false>(ctx, RowXU{f[EDDY_TV], m.au, m.ap, coef, ru1}, 2, d.nx - 2, d.jy1, d.jy2, d.kz1,
-                                 d.kz2, f[EDDY_US], f[EDDY_UB])))
+  const double fx = (double)ctx->sc.implx, fc = (double)ctx->sc.implcx;
+  if ((rc = xlines<RowXU, false>(ctx, RowXU{f[EDDY_TV], m.au, m.ap, f[EDDY_UO], coef, ru1, fx, fc}, 2, d.nx - 2,
+                                 d.jy1, d.jy2, d.kz1, d.kz2, f[EDDY_US], f[EDDY_UB])))
     return rc;
-  if ((rc = xlines<RowXV, true>(ctx, RowXV{f[EDDY_TV], m.av, m.au, coef, ru1}, 2, d.nx - 1, d.jbv, d.jev, d.kz1,
-                                d.kz2, f[EDDY_VS], f[EDDY_VB])))
+  if ((rc = xlines<RowXV, true>(ctx, RowXV{f[EDDY_TV], m.av, m.au, f[EDDY_US], coef, ru1, fx, fc}, 2, d.nx - 1,
+                                d.jbv, d.jev, d.kz1, d.kz2, f[EDDY_VS], f[EDDY_VB])))
     return rc;
-  return xlines<RowXW, true>(ctx, RowXW{f[EDDY_TV], m.aw, m.au, coef, ru1}, 2, d.nx - 1, d.jy1, d.jy2, d.kbw, d.kew,
-                             f[EDDY_WS], f[EDDY_WB]);
+  return xlines<RowXW, true>(ctx, RowXW{f[EDDY_TV], m.aw, m.au, f[EDDY_US], coef, ru1, fx, fc}, 2, d.nx - 1, d.jy1,
+                             d.jy2, d.kbw, d.kew, f[EDDY_WS], f[EDDY_WB]);
 }
 
 // INVERSEXD on RS: i in [2, NX-1], j in [jy1, jy2], k in [kbw, kew]
 int launch_inversexd(eddy_ctx *ctx, double alfxdt) {
   const Dims &d = ctx->d;
-  return xlines<RowXD, true>(ctx, RowXD{ctx->m.aw, ctx->m.au, 0.5 * alfxdt, ctx->sc.ru1 / ctx->sc.prn}, 2, d.nx - 1,
-                             d.jy1, d.jy2, d.kbw, d.kew, ctx->f[EDDY_RS], ctx->f[EDDY_UB]);
+  return xlines<RowXD, true>(ctx, RowXD{ctx->m.aw, ctx->m.au, 0.5 * alfxdt, ctx->sc.ru1 / ctx->sc.prn,
+                                        (double)ctx->sc.implx},
+                             2, d.nx - 1, d.jy1, d.jy2, d.kbw, d.kew, ctx->f[EDDY_RS], ctx->f[EDDY_UB]);
 }
 
 // INVERSEY: v lines (i in [2, NX-1], k in [kz1, kz2]), then w (i in [2, NX-1],
@@ -291,9 +354,24 @@ int launch_inversey(eddy_ctx *ctx, double alfxdt) {
   double **f = ctx->f;
   const double coef = 0.5 * alfxdt, ru1 = ctx->sc.ru1;
   int rc;
-  if ((rc = lines(ctx, RowV{f[EDDY_TV], m.bv, m.bp, coef, ru1}, 2, d.nx - 1, d.kz1, d.kz2, f[EDDY_VS]))) return rc;
-  if ((rc = lines(ctx, RowW{f[EDDY_TV], m.bw, m.bv, coef, ru1}, 2, d.nx - 1, d.kbw, d.kew, f[EDDY_WS]))) return rc;
-  return lines(ctx, RowU{f[EDDY_TV], m.bu, m.bv, coef, ru1}, 2, d.nx - 2, d.kz1, d.kz2, f[EDDY_US]);
+  const double fy = (double)ctx->sc.imply, fc = (double)ctx->sc.implcy;
+  if ((rc = lines(ctx, RowV{f[EDDY_TV], m.bv, m.bp, f[EDDY_VO], coef, ru1, fy, fc}, 2, d.nx - 1, d.kz1, d.kz2,
+                  f[EDDY_VS])))
+    return rc;
+  if ((rc = lines(ctx, RowW{f[EDDY_TV], m.bw, m.bv, f[EDDY_VS], coef, ru1, fy, fc}, 2, d.nx - 1, d.kbw, d.kew,
+                  f[EDDY_WS])))
+    return rc;
+  return lines(ctx, RowU{f[EDDY_TV], m.bu, m.bv, f[EDDY_VS], coef, ru1, fy, fc}, 2, d.nx - 2, d.kz1, d.kz2,
+               f[EDDY_US]);
+}
+
+// INVERSEYD_NEW on RS (IMPLY = IMPLCY = 1): i in [2, NX-1], k in [kbw, kew]
+int launch_inverseyd_new(eddy_ctx *ctx, double alfxdt) {
+  const Dims &d = ctx->d;
+  const DevMetrics &m = ctx->m;
+  return lines(ctx, RowDN{ctx->f[EDDY_TV], m.bp, m.bv, ctx->f[EDDY_VO], 0.5 * alfxdt, ctx->sc.ru1 / ctx->sc.prn,
+                          (double)ctx->sc.imply, (double)ctx->sc.implcy},
+               2, d.nx - 1, d.kbw, d.kew, ctx->f[EDDY_RS]);
 }
 
 // INVERSEYD on RS: i in [2, NX-1], k in [kbw, kew] (the reference's w range)

@@ -31,17 +31,17 @@ struct MomAcc {
   __device__ __forceinline__ double t(int di, int dj, int dk) const { return r.at(3, di, dj, dk); }
 };
 
-// CN: bit 0 IMPLY, bit 1 IMPLX (the C.N. parts of those axes' viscous terms)
-// ub, vb, wb (C.N. steps with an immersed body, else null): the explicit
-// estimate u* + alfxdt/2 (C.N. part) the implicit forcing reads
-// (UB = US + 0.5*ALFXDT*UB, src/Eddy6.f:2499-2501)
-template <int CN>
+// CN: any implicit flag on, f the terms that form the C.N. part; ub, vb, wb
+// (viscous C.N. steps with an immersed body, else null): the explicit estimate u* +
+// alfxdt/2 (C.N. part) the implicit forcing reads (UB = US + 0.5*ALFXDT*UB,
+// src/Eddy6.f:2499-2501)
+template <bool CN>
 __global__ void __launch_bounds__(TX *TY)
     k_rhs_predictord(Dims d, DevMetrics m, Scalars s, const __grid_constant__ TmaMaps<NFLD> maps,
                      double *__restrict__ us, double *__restrict__ vs, double *__restrict__ ws,
                      double *__restrict__ ua, double *__restrict__ va, double *__restrict__ wa, double alfxdt,
                      double gamxdt, double rhoxdt, int *err, double *__restrict__ ub, double *__restrict__ vb,
-                     double *__restrict__ wb) {
+                     double *__restrict__ wb, CnFlags<double> f) {
   const double coef = 0.5 * alfxdt, coefd = alfxdt;
   tma_march<NFLD, TX, TY, KCHUNK>(
       d.ix1, d.ix2, d.jy1, d.jy2, d.kz1, d.kz2, maps, err, [&](int i, int j, int k, bool active, const Acc9 &R) {
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(TX *TY)
         double uval = 0.0, ubv = 0.0;
         if (kin && jin && i >= d.ibu && i <= d.ieu) {
           double ucn = 0.0;  // the C.N. part (IMPLY / IMPLX), else 0
-          double ur = rhs_u<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &ucn);
+          double ur = rhs_u<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &ucn, &f);
           double ustar = R.at(0, 0, 0, 0) + gamxdt * ur + rhoxdt * R.at(6, 0, 0, 0) -
                          alfxdt * m.au[i] * (R.at(4, 1, 0, 0) - R.at(4, 0, 0, 0)) + coef * ucn - alfxdt * s.dpdx;
           if (s.idens == 1)
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(TX *TY)
         double vval = 0.0, vbv = 0.0;
         if (kin && j >= d.jbv && j <= d.jev && i >= d.ix1 && i <= d.ix2) {
           double vcn = 0.0;
-          double vr = rhs_v<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &vcn);
+          double vr = rhs_v<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &vcn, &f);
           double vstar = R.at(1, 0, 0, 0) + gamxdt * vr + rhoxdt * R.at(7, 0, 0, 0) -
                          alfxdt * m.bv[j] * (R.at(4, 0, 1, 0) - R.at(4, 0, 0, 0)) + coef * vcn - alfxdt * s.dpdy;
           va[q] = vr;
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(TX *TY)
         double wval = 0.0, wbv = 0.0;
         if (k >= d.kbw && k <= d.kew && jin && i >= d.ix1 && i <= d.ix2) {
           double wcn = 0.0;
-          double wr = rhs_w<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &wcn);
+          double wr = rhs_w<double, DevMetrics, MomAcc, CN>(S, m, s.ru1, i, j, k, &wcn, &f);
           double wstar = R.at(2, 0, 0, 0) + gamxdt * wr + rhoxdt * R.at(8, 0, 0, 0) -
                          alfxdt * m.cw[k] * (R.at(4, 0, 0, 1) - R.at(4, 0, 0, 0)) + coef * wcn - alfxdt * s.dpdz;
           wa[q] = wr;
@@ -248,15 +248,17 @@ int launch_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rh
   }
   size_t smem = ring_smem_bytes<NFLD, TX, TY>();
   dim3 g((d.ix2 - d.ix1 + TX) / TX, (d.jy2 - d.jy1 + TY) / TY, (d.kz2 - d.kz1 + KCHUNK) / KCHUNK);
-  const int cn = (ctx->sc.imply == 1 ? 1 : 0) | (ctx->sc.implx == 1 ? 2 : 0);
-  auto kern = cn == 3 ? k_rhs_predictord<3> : cn == 2 ? k_rhs_predictord<2> : cn == 1 ? k_rhs_predictord<1>
-                                                                                     : k_rhs_predictord<0>;
+  const CnFlags<double> fl{(double)ctx->sc.implx, (double)ctx->sc.imply, (double)ctx->sc.implcx,
+                           (double)ctx->sc.implcy};
+  const bool cn = ctx->sc.imply == 1 || ctx->sc.implx == 1 || ctx->sc.implcx == 1 || ctx->sc.implcy == 1;
+  auto kern = cn ? k_rhs_predictord<true> : k_rhs_predictord<false>;
   EDDY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const bool est = cn && ctx->ib;  // the implicit forcing's explicit estimate
+  // the implicit forcing's explicit estimate (impl = 1: viscous C.N. steps with a body)
+  const bool est = (ctx->sc.imply == 1 || ctx->sc.implx == 1) && ctx->ib;
   double *ub = est ? f[EDDY_UB] : nullptr, *vb = est ? f[EDDY_VB] : nullptr, *wb = est ? f[EDDY_WB] : nullptr;
   kern<<<g, dim3(TX, TY), smem, ctx->stream>>>(d, ctx->m, ctx->sc, maps, f[EDDY_US], f[EDDY_VS], f[EDDY_WS],
                                               f[EDDY_UA], f[EDDY_VA], f[EDDY_WA], alfxdt, gamxdt, rhoxdt,
-                                              ctx->err_flag, ub, vb, wb);
+                                              ctx->err_flag, ub, vb, wb, fl);
   EDDY_LAUNCHED(ctx);
   long long nghost = 2LL * d.nx * d.ny + 2LL * d.nx * d.nz + 2LL * d.ny * d.nz;
   k_zero_faces3<<<(unsigned)((nghost + 255) / 256), 256, 0, ctx->stream>>>(d, f[EDDY_US], f[EDDY_VS],

@@ -1,14 +1,15 @@
 // stencil_density.cuh -- density right-hand side of src/rhs_density.f:55-165
-// (Cartesian; CN bit 0: IMPLY = 1, bit 1: IMPLX = 1, the diffusion along those
-// axes returned as the Crank-Nicolson part in *cn), templated on the arithmetic type T and on
+// (Cartesian; with CN the terms the flags f select are returned as the
+// Crank-Nicolson part in *cn, stencil_cn.cuh), templated on the arithmetic type T and on
 // a neighbour accessor: S.at(f, di, dj, dk) with f = 0 density, 1 eddy
 // diffusivity, 2 u, 3 v, 4 w.  With T = double the operation order is the
 // reference's (the plain form is compiled with -fmad=false).
 #pragma once
 #include "stencil_cn.cuh"
 
-template <class T, class M, class Acc, int CN = 0>
-__device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, int j, int k, T *cn = nullptr) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, int j, int k, T *cn = nullptr,
+                                       const CnFlags<T> *f = nullptr) {
   auto dens = [&](int a, int b, int c) { return S.at(0, a, b, c); };
   auto kv = [&](int a, int b, int c) { return S.at(1, a, b, c); };
   T qxp = S.at(2, 0, 0, 0), qxm = S.at(2, -1, 0, 0);
@@ -45,10 +46,10 @@ __device__ __forceinline__ T rhs_dens(const Acc &S, const M &m, T repr1, int i, 
   T t22 = m.bp[j] * (tyyp - tyym);
   T t33 = m.cp[k] * (tzzp - tzzm);
   if (CN) {
-    // src/rhs_density.f:147-156: the diffusion along the implicit axes is the
-    // C.N. part
-    *cn = cn_part<T, CN>(t11, t22);
-    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33;
+    // src/rhs_density.f:147-156
+    *cn = cn_part(*f, t11, t22, h11, h22);
+    return (T(1.) - f->fcx) * h11 + (T(1.) - f->fcy) * h22 + h33 + (T(1.) - f->fx) * t11 + (T(1.) - f->fy) * t22 +
+           t33;
   }
   return h11 + h22 + h33 + t11 + t22 + t33;
 }

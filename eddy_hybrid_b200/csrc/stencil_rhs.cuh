@@ -1,6 +1,6 @@
 // stencil_rhs.cuh -- explicit momentum right-hand side of src/rhs.f:4-438
-// (Cartesian; CN bit 0: IMPLY = 1, bit 1: IMPLX = 1, the viscous terms along
-// those axes returned as the Crank-Nicolson part in *cn), templated on the
+// (Cartesian; with CN the terms the flags f select are returned as the
+// Crank-Nicolson part in *cn, stencil_cn.cuh), templated on the
 // arithmetic type T and on a neighbour accessor: S.u/v/w/t(di,dj,dk) return
 // uo/vo/wo/tv at the offset from the current cell.  With T = double the
 // operation order is exactly the reference's (the plain form is compiled with
@@ -10,8 +10,9 @@
 
 // ---------------------------------------------------------------------------
 // u-momentum explicit RHS at a u point (src/rhs.f:77-172)
-template <class T, class M, class Acc, int CN = 0>
-__device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr,
+                                    const CnFlags<T> *f = nullptr) {
   T qxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * T(0.5);
   T qxm = (S.u(0, 0, 0) + S.u(-1, 0, 0)) * T(0.5);
   T uxp = (S.u(1, 0, 0) + S.u(0, 0, 0)) * T(0.5);
@@ -57,18 +58,18 @@ __device__ __forceinline__ T rhs_u(const Acc &S, const M &m, T ru1, int i, int j
   T s22 = m.bu[j] * (txyp - txym);
   T s33 = m.cu[k] * (txzp - txzm);
   if (CN) {
-    // src/rhs.f:175-191: the viscous terms along the implicit axes are the
-    // C.N. part (rflagx = IMPLX, rflagy = IMPLY, ruimplx = ruimply = 1)
-    *cn = cn_part<T, CN>(t11, t22);
-    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33 +
-           s22 + s33;
+    // src/rhs.f:175-191 (ruimplx = ruimply = 1)
+    *cn = cn_part(*f, t11, t22, h11, h22);
+    return (T(1.) - f->fcx) * h11 + (T(1.) - f->fcy) * h22 + h33 + (T(1.) - f->fx) * t11 + (T(1.) - f->fy) * t22 +
+           t33 + s22 + s33;
   }
   return h11 + h22 + h33 + t11 + t22 + t33 + s22 + s33;
 }
 
 // v-momentum (src/rhs.f:219-321)
-template <class T, class M, class Acc, int CN = 0>
-__device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr,
+                                    const CnFlags<T> *f = nullptr) {
   T vxp = (S.v(1, 0, 0) + S.v(0, 0, 0)) * T(0.5);
   T vxm = (S.v(0, 0, 0) + S.v(-1, 0, 0)) * T(0.5);
   T vyp = (S.v(0, 1, 0) + S.v(0, 0, 0)) * T(0.5);
@@ -112,16 +113,17 @@ __device__ __forceinline__ T rhs_v(const Acc &S, const M &m, T ru1, int i, int j
   T s11 = m.av[i] * (txyp - txym);
   T s33 = m.cv[k] * (tyzp - tyzm);
   if (CN) {
-    *cn = cn_part<T, CN>(t11, t22);
-    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33 +
-           s11 + s33;
+    *cn = cn_part(*f, t11, t22, h11, h22);
+    return (T(1.) - f->fcx) * h11 + (T(1.) - f->fcy) * h22 + h33 + (T(1.) - f->fx) * t11 + (T(1.) - f->fy) * t22 +
+           t33 + s11 + s33;
   }
   return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s33;
 }
 
 // w-momentum (src/rhs.f:347-422)
-template <class T, class M, class Acc, int CN = 0>
-__device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr) {
+template <class T, class M, class Acc, bool CN = false>
+__device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j, int k, T *cn = nullptr,
+                                    const CnFlags<T> *f = nullptr) {
   T wxp = (S.w(1, 0, 0) + S.w(0, 0, 0)) * T(0.5);
   T wxm = (S.w(0, 0, 0) + S.w(-1, 0, 0)) * T(0.5);
   T wyp = (S.w(0, 1, 0) + S.w(0, 0, 0)) * T(0.5);
@@ -165,9 +167,9 @@ __device__ __forceinline__ T rhs_w(const Acc &S, const M &m, T ru1, int i, int j
   T s11 = m.aw[i] * (txzp - txzm);
   T s22 = m.bw[j] * (tyzp - tyzm);
   if (CN) {
-    *cn = cn_part<T, CN>(t11, t22);
-    return h11 + h22 + h33 + (T(1.) - cn_flag<T, CN & 2>()) * t11 + (T(1.) - cn_flag<T, CN & 1>()) * t22 + t33 +
-           s11 + s22;
+    *cn = cn_part(*f, t11, t22, h11, h22);
+    return (T(1.) - f->fcx) * h11 + (T(1.) - f->fcy) * h22 + h33 + (T(1.) - f->fx) * t11 + (T(1.) - f->fy) * t22 +
+           t33 + s11 + s22;
   }
   return h11 + h22 + h33 + t11 + t22 + t33 + s11 + s22;
 }

@@ -65,14 +65,20 @@ typedef struct {
                                 INVERSEYD src/density.f:383), over the whole x range
                                 (IMPLYDCMP = 0); plain form.  With an immersed body
                                 the velocity forcing runs before the line solves,
-                                from the explicit estimate (src/Eddy6.f:2495-2575).
-                                The implicit convective terms (IMPLCY, IMPLCX) are
-                                not supported. */
+                                from the explicit estimate (src/Eddy6.f:2495-2575). */
   int implx;                 /* IMPLX: 1 = the viscous terms along x Crank-Nicolson
                                 implicit (INVERSEX src/timeindeg.f:344, INVERSEXD
                                 src/density.f:129) over the whole x range
                                 (IMPLXDCMP = 0), with slip walls (type 60) on both
                                 x boundaries; plain form. */
+  int implcx, implcy;        /* IMPLCX, IMPLCY: 1 = the convective terms along x / y
+                                Crank-Nicolson implicit inside the same line solves
+                                (linearised about UO / VO and the provisional US /
+                                VS as src/timeindeg.f:120-690 does; INVERSEYD_NEW,
+                                src/density.f:290, for the density when IMPLY and
+                                IMPLCY are both 1); plain form.  With a body and
+                                neither IMPLX nor IMPLY the forcing runs before
+                                the line solves, on US. */
 } eddy_params;
 
 typedef struct eddy_ctx eddy_ctx;
@@ -145,13 +151,16 @@ int eddy_grid_metric(const eddy_params *prm, const double *xu_faces, double ymin
  * tv,p,dens,ua.. -> us,vs,ws (u*), ua,va,wa (new explicit RHS). */
 int eddy_rhs_predictord(eddy_ctx *ctx, double alfxdt, double gamxdt, double rhoxdt);
 /* INVERSEY (src/timeindeg.f:120-340): the Crank-Nicolson y lines of US, VS,
- * WS after the predictor, viscous part (imply = 1 only).  The density's
- * INVERSEYD (src/density.f:383) runs inside eddy_density when imply = 1. */
+ * WS after the predictor, the viscous (imply) and convective (implcy) parts;
+ * one of the two must be on.  The density's INVERSEYD (src/density.f:383) or
+ * INVERSEYD_NEW (src/density.f:290, imply and implcy) runs inside
+ * eddy_density. */
 int eddy_inversey(eddy_ctx *ctx, double alfxdt);
 /* INVERSEX (src/timeindeg.f:344-690): the Crank-Nicolson x lines of US, then
- * VS and WS, viscous part (implx = 1 only; after eddy_inversey when both are
- * on, as src/Eddy6.f:2597-2607 orders them).  INVERSEXD (src/density.f:129)
- * runs inside eddy_density when implx = 1. */
+ * VS and WS, the viscous (implx) and convective (implcx) parts; one of the two
+ * must be on (after eddy_inversey when both axes are, as src/Eddy6.f:2597-2607
+ * orders them).  INVERSEXD (src/density.f:129) runs inside eddy_density when
+ * implx or implcx is 1. */
 int eddy_inversex(eddy_ctx *ctx, double alfxdt);
 /* BOUNDARY (src/boundary.f:7) on the provisional (set=0: US,VS,WS) or the
  * corrected (set=1: UO,VO,WO) velocity. */
@@ -244,7 +253,7 @@ int eddy_refine_residuals(eddy_ctx *ctx, double *out, int n);
 int eddy_max_divergence(eddy_ctx *ctx, double *out);
 /* CALCFL (src/timestep.f:2-78), Cartesian: the interior maximum of the
  * per-cell max of the convective constraints |u|/dx and the viscous ones
- * 2 (ru1 + tv)/dx^2 per axis (the y viscous one dropped with imply = 1); the
+ * 2 (ru1 + tv)/dx^2 per axis (each dropped with its implicit flag); the
  * reference's constant-CFL run takes DTM1 = CFLC / CFLM (src/Eddy6.f:2118). */
 int eddy_cfl(eddy_ctx *ctx, double *cflm);
 /* SCRINFO's extrema (src/info.f:5-164): min and max of a field over the

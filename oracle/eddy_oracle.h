@@ -42,6 +42,7 @@ typedef struct {
   int vspngx1, dspngx1, vspngx3in, vspngx3out, dspngx3in, dspngx3out;
   int imply;               /* 1: Crank-Nicolson viscous terms along y (INVERSEY/INVERSEYD) */
   int implx;               /* 1: Crank-Nicolson viscous terms along x (INVERSEX/INVERSEXD) */
+  int implcx, implcy;      /* 1: Crank-Nicolson convective terms along x / y */
 } eo_params;
 
 /* 1-D metric arrays (src/common.h:51-54), 1-based: arrays have n+1 entries. */
@@ -131,6 +132,7 @@ void eo_inversey(eo_state *s, double alfxdt);
 /* CALCFL (src/timestep.f:2-78): CFLM over the interior */
 double eo_calcfl(eo_state *s);
 void eo_inverseyd(eo_state *s, double alfxdt);
+void eo_inverseyd_new(eo_state *s, double alfxdt);
 void eo_inversex_walls(eo_state *s, double alfxdt);
 void eo_inversex(eo_state *s, double alfxdt);
 void eo_inversexd(eo_state *s, double alfxdt);

@@ -33,7 +33,7 @@ class Params(C.Structure):
                 ("css", C.c_double), ("vspngx1", C.c_int), ("dspngx1", C.c_int),
                 ("vspngx3in", C.c_int), ("vspngx3out", C.c_int),
                 ("dspngx3in", C.c_int), ("dspngx3out", C.c_int), ("imply", C.c_int),
-                ("implx", C.c_int)]
+                ("implx", C.c_int), ("implcx", C.c_int), ("implcy", C.c_int)]
 
 
 class IBSet(C.Structure):

@@ -112,8 +112,8 @@ int eo_get(eo_state *s, int id, double *dst) {
 }
 
 /* ------------------------------------------------------------------------
- * RHS: src/rhs.f:4-438 (icyl=0; rflagx = IMPLX, rflagy = IMPLY, the
- * convective flags 0: ut,vt,wt take the C.N. viscous parts).
+ * RHS: src/rhs.f:4-438 (icyl=0; rflagx = IMPLX, rflagy = IMPLY, rflagcx =
+ * IMPLCX, rflagcy = IMPLCY: ut,vt,wt take the C.N. parts).
  * ut,vt,wt and ur,vr,wr are zeroed over the whole array first (rhs.f:65-70);
  * qr = uo (rhs.f:58).
  * ---------------------------------------------------------------------- */
@@ -128,7 +128,8 @@ void eo_rhs(eo_state *s, const double *uo, const double *vo, const double *wo,
   long n = s->ncell;
   /* rflag* of src/rhs.f:49-52 with ruimplx = rvimplx = ruimply = rvimply = 1
    * (IMPLXDCMP = IMPLYDCMP = 0) */
-  const double rflagx = (double)s->prm.implx, rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
+  const double rflagx = (double)s->prm.implx, rflagcx = (double)s->prm.implcx, rflagy = (double)s->prm.imply,
+               rflagcy = (double)s->prm.implcy;
   memcpy(qr, uo, sizeof(double) * (size_t)n);
   memset(ut, 0, sizeof(double) * (size_t)n); memset(ur, 0, sizeof(double) * (size_t)n);
   memset(vt, 0, sizeof(double) * (size_t)n); memset(vr, 0, sizeof(double) * (size_t)n);
@@ -650,7 +651,8 @@ void eo_rhs_density(eo_state *s) {
   double *uo = s->uo, *vo = s->vo, *wo = s->wo, *dens = s->dens, *kv = s->tv;
   double *rr = s->rhb, *rt = s->rs;
   double repr1 = s->prm.ru1 / s->prm.prn;
-  const double rflagx = (double)s->prm.implx, rflagcx = 0., rflagy = (double)s->prm.imply, rflagcy = 0.;
+  const double rflagx = (double)s->prm.implx, rflagcx = (double)s->prm.implcx, rflagy = (double)s->prm.imply,
+               rflagcy = (double)s->prm.implcy;
   memset(rr, 0, sizeof(double) * (size_t)s->ncell);
 #pragma omp parallel for schedule(static)
   for (int k = g->kz1; k <= g->kz2; k++)
@@ -759,12 +761,15 @@ void eo_density(eo_state *s, double alfxdt, double gamxdt, double rhoxdt) {
   eo_boundary_dens(s, rhb);
   /* implicit y diffusion, then the whole array is copied (density.f:96-100):
    * ghost cells take RS's, which nothing above writes but BOUNDARY_DENS */
-  if (s->prm.imply == 1) {
+  if (s->prm.imply == 1 && s->prm.implcy == 1) {
+    eo_inverseyd_new(s, alfxdt);
+    memcpy(dens, rs, sizeof(double) * (size_t)s->ncell);
+  } else if (s->prm.imply == 1) {
     eo_inverseyd(s, alfxdt);
     memcpy(dens, rs, sizeof(double) * (size_t)s->ncell);
   }
   /* implicit x diffusion (density.f:101-104) */
-  if (s->prm.implx == 1) {
+  if (s->prm.implx == 1 || s->prm.implcx == 1) {
     eo_inversexd(s, alfxdt);
     memcpy(dens, rs, sizeof(double) * (size_t)s->ncell);
   }
@@ -817,18 +822,20 @@ void eo_cyclic(const double *a, const double *b, const double *c, double alpha, 
   for (int i = 0; i < n; i++) x[i] = x[i] - fact * z[i];
 }
 
-/* INVERSEY (src/timeindeg.f:120-340), viscous part (implcy = 0: the
- * convective coefficients and right-hand-side terms are exact zeros),
- * Cartesian (rp = ru = 1), IMPLYDCMP = 0: v lines for i in [2, NX-1],
- * w lines for i in [2, NX-1] and k in [kbw, kew], u lines for i in [2, NX-2];
- * j periodic over [jy1, jy2].  REFRESHBC is a no-op on one rank with
- * non-periodic z. */
+/* INVERSEY (src/timeindeg.f:120-340), Cartesian (rp = ru = 1), IMPLYDCMP = 0:
+ * v lines for i in [2, NX-1], w lines for i in [2, NX-1] and k in [kbw, kew],
+ * u lines for i in [2, NX-2]; j periodic over [jy1, jy2].  rflagy = IMPLY
+ * scales the viscous coefficients, rflagcy = IMPLCY the convective ones: the
+ * v lines linearise about VO (and take the explicit half back on the right-
+ * hand side), the w and u lines about the provisional VS the v lines just
+ * produced.  REFRESHBC is a no-op on one rank with non-periodic z. */
 void eo_inversey(eo_state *s, double alfxdt) {
   const eo_grid *g = s->g;
-  const double coef = 0.5 * alfxdt, ru1 = s->prm.ru1, rflagy = 1.0;
+  const double coef = 0.5 * alfxdt, ru1 = s->prm.ru1;
+  const double rflagy = (double)s->prm.imply, rflagcy = (double)s->prm.implcy;
   const int n = g->jy2 - 1;
   double *us = s->us, *vs = s->vs, *ws = s->ws;
-  const double *tv = s->tv;
+  const double *tv = s->tv, *vo = s->vo;
   const double *bp = g->bp, *bu = g->bu, *bv = g->bv, *bw = g->bw;
 #pragma omp parallel
   {
@@ -842,11 +849,18 @@ void eo_inversey(eo_state *s, double alfxdt) {
           const int jj = j - 2;
           const double tvjp = 2. * A(tv, i, j + 1, k) + ru1, tvjm = 2. * A(tv, i, j, k) + ru1;
           ry[jj] = A(vs, i, j, k);
-          const double coefy = rflagy * coef * bv[j] / (1.0 * 1.0);
+          double coefy = rflagy * coef * bv[j] / (1.0 * 1.0);
           const double ayv = -coefy * bp[j] * tvjm, cyv = -coefy * bp[j + 1] * tvjp, byv = -ayv - cyv;
-          ay[jj] = ayv;
-          cy[jj] = cyv;
-          by[jj] = 1.0 + byv;
+          coefy = rflagcy * coef * bv[j] / 1.0;
+          const double ayc = -0.25 * coefy * (A(vo, i, j - 1, k) + A(vo, i, j, k)) * 2.0;
+          const double cyc = 0.25 * coefy * (A(vo, i, j + 1, k) + A(vo, i, j, k)) * 2.0;
+          const double byc = ayc + cyc;
+          ay[jj] = ayv + ayc;
+          cy[jj] = cyv + cyc;
+          by[jj] = 1.0 + byv + byc;
+          const double vyp = (A(vo, i, j + 1, k) + A(vo, i, j, k)) * 0.5;
+          const double vym = (A(vo, i, j, k) + A(vo, i, j - 1, k)) * 0.5;
+          ry[jj] = ry[jj] + coefy * (vyp * vyp - vym * vym);
         }
         eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
         for (int j = g->jbv; j <= g->jev; j++) A(vs, i, j, k) = x[j - 2];
@@ -862,11 +876,15 @@ void eo_inversey(eo_state *s, double alfxdt) {
           const double tvjm =
               0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i, j - 1, k + 1) + A(tv, i, j - 1, k)) + ru1;
           ry[jj] = A(ws, i, j, k);
-          const double coefy = rflagy * coef * bw[j] / (1.0 * 1.0);
+          double coefy = rflagy * coef * bw[j] / (1.0 * 1.0);
           const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
-          ay[jj] = ayv;
-          cy[jj] = cyv;
-          by[jj] = 1.0 + byv;
+          const double vzp = (A(vs, i, j, k + 1) + A(vs, i, j, k)) * 0.5;
+          const double vzm = (A(vs, i, j - 1, k + 1) + A(vs, i, j - 1, k)) * 0.5;
+          coefy = rflagcy * 0.5 * coef * bw[j] / 1.0;
+          const double ayc = -coefy * vzm, cyc = coefy * vzp, byc = ayc + cyc;
+          ay[jj] = ayv + ayc;
+          cy[jj] = cyv + cyc;
+          by[jj] = 1.0 + byv + byc;
         }
         eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
         for (int j = g->jy1; j <= g->jy2; j++) A(ws, i, j, k) = x[j - 2];
@@ -882,14 +900,56 @@ void eo_inversey(eo_state *s, double alfxdt) {
           const double tvjm =
               0.25 * (A(tv, i + 1, j, k) + A(tv, i, j, k) + A(tv, i + 1, j - 1, k) + A(tv, i, j - 1, k)) + ru1;
           ry[jj] = A(us, i, j, k);
-          const double coefy = rflagy * coef * bu[j] / (1.0 * 1.0);
+          double coefy = rflagy * coef * bu[j] / (1.0 * 1.0);
           const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
-          ay[jj] = ayv;
-          cy[jj] = cyv;
-          by[jj] = 1.0 + byv;
+          const double vxp = (A(vs, i + 1, j, k) + A(vs, i, j, k)) * 0.5;
+          const double vxm = (A(vs, i + 1, j - 1, k) + A(vs, i, j - 1, k)) * 0.5;
+          coefy = rflagcy * 0.5 * coef * bu[j] / 1.0;
+          const double ayc = -coefy * vxm, cyc = coefy * vxp, byc = ayc + cyc;
+          ay[jj] = ayv + ayc;
+          cy[jj] = cyv + cyc;
+          by[jj] = 1.0 + byv + byc;
         }
         eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
         for (int j = g->jy1; j <= g->jy2; j++) A(us, i, j, k) = x[j - 2];
+      }
+    free(ay); free(by); free(cy); free(ry); free(x); free(wk);
+  }
+}
+
+/* INVERSEYD_NEW (src/density.f:290-380), IMPLY = IMPLCY = 1: the y diffusion
+ * with the face diffusivities 0.5 (tv(j) + tv(j+/-1)) + ru1/prn and the
+ * convection by VO, k in [kbw, kew], i in [2, NX-1] */
+void eo_inverseyd_new(eo_state *s, double alfxdt) {
+  const eo_grid *g = s->g;
+  const double coef = 0.5 * alfxdt, kmol = s->prm.ru1 / s->prm.prn;
+  const double rflagy = (double)s->prm.imply, rflagcy = (double)s->prm.implcy;
+  const int n = g->jy2 - 1;
+  double *rs = s->rs;
+  const double *tv = s->tv, *vo = s->vo, *bp = g->bp, *bv = g->bv;
+#pragma omp parallel
+  {
+    double *ay = malloc(sizeof(double) * n), *by = malloc(sizeof(double) * n), *cy = malloc(sizeof(double) * n),
+           *ry = malloc(sizeof(double) * n), *x = malloc(sizeof(double) * n), *wk = malloc(sizeof(double) * 4 * n);
+#pragma omp for schedule(static) collapse(2)
+    for (int k = g->kbw; k <= g->kew; k++)
+      for (int i = 2; i <= NX - 1; i++) {
+        for (int j = g->jy1; j <= g->jy2; j++) {
+          const int jj = j - 2;
+          const double tvjp = 0.5 * (A(tv, i, j, k) + A(tv, i, j + 1, k)) + kmol;
+          const double tvjm = 0.5 * (A(tv, i, j, k) + A(tv, i, j - 1, k)) + kmol;
+          ry[jj] = A(rs, i, j, k);
+          double coefy = rflagy * coef * bp[j] / (1.0 * 1.0);
+          const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+          const double vzp = A(vo, i, j, k), vzm = A(vo, i, j - 1, k);
+          coefy = rflagcy * 0.5 * coef * bp[j] / 1.0;
+          const double ayc = -coefy * vzm, cyc = coefy * vzp, byc = ayc + cyc;
+          ay[jj] = ayv + ayc;
+          cy[jj] = cyv + cyc;
+          by[jj] = 1.0 + byv + byc;
+        }
+        eo_cyclic(ay, by, cy, cy[n - 1], ay[0], ry, x, n, wk);
+        for (int j = g->jy1; j <= g->jy2; j++) A(rs, i, j, k) = x[j - 2];
       }
     free(ay); free(by); free(cy); free(ry); free(x); free(wk);
   }
@@ -989,17 +1049,19 @@ void eo_inversex_walls(eo_state *s, double alfxdt) {
   eo_boundary(s, s->ub, s->vb, s->wb);
 }
 
-/* INVERSEX (src/timeindeg.f:344-690), viscous part (implcx = 0: the
- * convective coefficients and right-hand-side terms are exact zeros),
- * Cartesian (rp = ru = 1), IMPLXDCMP = 0: u lines for i in [2, NX-2], then
+/* INVERSEX (src/timeindeg.f:344-690), Cartesian (rp = ru = 1), rflagx =
+ * IMPLX and rflagcx = IMPLCX (the u lines linearised about UO, with the
+ * explicit flux back on the right-hand side; the v and w lines about the
+ * provisional US), IMPLXDCMP = 0: u lines for i in [2, NX-2], then
  * v lines (j in [jbv, jev]) and w lines (k in [kbw, kew]) for i in [2, NX-1];
  * tridag (src/numrec.f:783-802) on each.  REFRESHBC is a no-op on one rank
  * with non-periodic z. */
 void eo_inversex(eo_state *s, double alfxdt) {
   const eo_grid *g = s->g;
-  const double coef = 0.5 * alfxdt, ru1 = s->prm.ru1, rflagx = 1.0;
+  const double coef = 0.5 * alfxdt, ru1 = s->prm.ru1;
+  const double rflagx = (double)s->prm.implx, rflagcx = (double)s->prm.implcx;
   double *us = s->us, *vs = s->vs, *ws = s->ws;
-  const double *ub = s->ub, *vb = s->vb, *wb = s->wb, *tv = s->tv;
+  const double *ub = s->ub, *vb = s->vb, *wb = s->wb, *tv = s->tv, *uo = s->uo;
   const double *ap = g->ap, *au = g->au, *av = g->av, *aw = g->aw;
   xbc_tables t;
   x_tables(s, &t);
@@ -1018,11 +1080,19 @@ void eo_inversex(eo_state *s, double alfxdt) {
           const int ii = i - i1;
           const double tvip = 2. * A(tv, i + 1, j, k) + ru1, tvim = 2. * A(tv, i, j, k) + ru1;
           rx[ii] = A(us, i, j, k);
-          const double coefx = rflagx * coef * au[i];
+          double coefx = rflagx * coef * au[i];
           const double axv = -coefx * ap[i] * tvim, cxv = -coefx * ap[i + 1] * tvip, bxv = -axv - cxv;
-          ax[ii] = axv;
-          cx[ii] = cxv;
-          bx[ii] = 1.0 + bxv;
+          /* convective terms about UO (timeindeg.f:466-486) */
+          coefx = rflagcx * coef * au[i] / 1.0;
+          const double qxm = (A(uo, i, j, k) + A(uo, i - 1, j, k)) * 0.5;
+          const double qxp = (A(uo, i, j, k) + A(uo, i + 1, j, k)) * 0.5;
+          const double axc = -coefx * qxm, cxc = coefx * qxp, bxc = axc + cxc;
+          ax[ii] = axv + axc;
+          cx[ii] = cxv + cxc;
+          bx[ii] = 1.0 + bxv + bxc;
+          const double uxp = (A(uo, i + 1, j, k) + A(uo, i, j, k)) * 0.5;
+          const double uxm = (A(uo, i - 1, j, k) + A(uo, i, j, k)) * 0.5;
+          rx[ii] = rx[ii] + coefx * (qxp * uxp - qxm * uxm);
         }
         rx[0] = rx[0] - ax[0] * (A(us, i1 - 1, j, k) * t.rdir[0][0] + A(ub, i1 - 1, j, k) * t.rperb[0][0]);
         rx[n - 1] =
@@ -1042,11 +1112,16 @@ void eo_inversex(eo_state *s, double alfxdt) {
           const double tvim =
               0.25 * (A(tv, i, j + 1, k) + A(tv, i, j, k) + A(tv, i - 1, j + 1, k) + A(tv, i - 1, j, k)) + ru1;
           rx[ii] = A(vs, i, j, k);
-          const double coefx = rflagx * coef * av[i] / 1.0;
+          double coefx = rflagx * coef * av[i] / 1.0;
           const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
-          ax[ii] = axv;
-          cx[ii] = cxv;
-          bx[ii] = 1.0 + bxv;
+          /* convective terms about the provisional US (timeindeg.f:545-556) */
+          coefx = rflagcx * 0.5 * coef * av[i] / 1.0;
+          const double qyp = 1.0 * (A(us, i, j + 1, k) + A(us, i, j, k)) * 0.5;
+          const double qym = 1.0 * (A(us, i - 1, j + 1, k) + A(us, i - 1, j, k)) * 0.5;
+          const double axc = -coefx * qym, cxc = coefx * qyp, bxc = axc + cxc;
+          ax[ii] = axv + axc;
+          cx[ii] = cxv + cxc;
+          bx[ii] = 1.0 + bxv + bxc;
         }
         bx[0] = bx[0] + (t.bdirb[1][0] + t.bneub[1][0]) * ax[0];
         bx[n - 1] = bx[n - 1] + (t.bdirb[1][1] + t.bneub[1][1]) * cx[n - 1];
@@ -1069,11 +1144,16 @@ void eo_inversex(eo_state *s, double alfxdt) {
           const double tvim =
               0.25 * (A(tv, i, j, k + 1) + A(tv, i, j, k) + A(tv, i - 1, j, k + 1) + A(tv, i - 1, j, k)) + ru1;
           rx[ii] = A(ws, i, j, k);
-          const double coefx = rflagx * coef * aw[i] / 1.0;
+          double coefx = rflagx * coef * aw[i] / 1.0;
           const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
-          ax[ii] = axv;
-          cx[ii] = cxv;
-          bx[ii] = 1.0 + bxv;
+          /* convective terms about the provisional US (timeindeg.f:610-622) */
+          coefx = rflagcx * 0.5 * coef * aw[i] / 1.0;
+          const double qzp = 1.0 * (A(us, i, j, k + 1) + A(us, i, j, k)) * 0.5;
+          const double qzm = 1.0 * (A(us, i - 1, j, k + 1) + A(us, i - 1, j, k)) * 0.5;
+          const double axc = -coefx * qzm, cxc = coefx * qzp, bxc = axc + cxc;
+          ax[ii] = axv + axc;
+          cx[ii] = cxv + cxc;
+          bx[ii] = 1.0 + bxv + bxc;
         }
         bx[0] = bx[0] + (t.bdirb[2][0] + t.bneub[2][0]) * ax[0];
         bx[n - 1] = bx[n - 1] + (t.bdirb[2][1] + t.bneub[2][1]) * cx[n - 1];
@@ -1095,7 +1175,7 @@ void eo_inversex(eo_state *s, double alfxdt) {
  * the explicit right-hand side with IMPLX = 1, is not restored here) */
 void eo_inversexd(eo_state *s, double alfxdt) {
   const eo_grid *g = s->g;
-  const double coef = 0.5 * alfxdt, rflagx = 1.0, kmol = s->prm.ru1 / s->prm.prn;
+  const double coef = 0.5 * alfxdt, rflagx = (double)s->prm.implx, kmol = s->prm.ru1 / s->prm.prn;
   double *rs = s->rs;
   const double *rhb = s->rhb, *au = g->au, *aw = g->aw;
   xbc_tables t;

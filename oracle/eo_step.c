@@ -67,9 +67,10 @@ void eo_substep(eo_state *s, int is, double dtm1) {
   }
   /* Crank-Nicolson y, then x lines (:2582-2607; the IBM = 0 planes of UB
    * only without a body) */
-  if (s->prm.implx == 1 && !s->ib) eo_inversex_walls(s, alfxdt);
-  if (s->prm.imply == 1) eo_inversey(s, alfxdt);
-  if (s->prm.implx == 1) eo_inversex(s, alfxdt);
+  const int cx = s->prm.implx == 1 || s->prm.implcx == 1, cy = s->prm.imply == 1 || s->prm.implcy == 1;
+  if (cx && !s->ib) eo_inversex_walls(s, alfxdt);
+  if (cy) eo_inversey(s, alfxdt);
+  if (cx) eo_inversex(s, alfxdt);
   /* :2689-2704 */
   eo_boundary(s, s->us, s->vs, s->ws);
   eo_boundinout(s, s->us, s->vs, s->ws, s->uo, s->vo, s->wo, alfxdt, 1);
@@ -256,11 +257,12 @@ double eo_max_divergence(eo_state *s) {
 }
 
 /* CALCFL (src/timestep.f:2-78), Cartesian: CONST = 2, rp = 1, the implicit
- * flags RFLAGX = IMPLX, RFLAGY = IMPLY, the convective ones 0; returns CFLM
- * over the interior */
+ * flags RFLAGX = IMPLX, RFLAGY = IMPLY, RFLAGCX = IMPLCX, RFLAGCY = IMPLCY;
+ * returns CFLM over the interior */
 double eo_calcfl(eo_state *s) {
   const eo_grid *g = s->g;
-  const double cst = 2., rflagx = (double)s->prm.implx, rflagcx = 0., rflagcy = 0., rflagy = (double)s->prm.imply;
+  const double cst = 2., rflagx = (double)s->prm.implx, rflagcx = (double)s->prm.implcx,
+               rflagcy = (double)s->prm.implcy, rflagy = (double)s->prm.imply;
   const int nx = g->nx, ny = g->ny;
   double cflm = 0.;
   for (int k = g->kz1; k <= g->kz2; k++)

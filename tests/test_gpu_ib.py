@@ -114,11 +114,15 @@ def test_mixed_form_with_sphere(oracle, product):
     assert g.max_divergence() < 1e-10
 
 
-@pytest.mark.parametrize("imply,implx", [(1, 0), (0, 1), (1, 1)])
-def test_steps_with_moving_sphere_crank_nicolson(oracle, product, imply, implx):
-    # the C.N. steps with a body: the forcing from the explicit estimate UB
-    # before the line solves (momforc_mod2 / velinterior with impl = 1)
-    w = config.small(mx=32, ly=16, nz_=40, noise=0.2, re=2000.0, imply=imply, implx=implx)
+@pytest.mark.parametrize("imply,implx,implcx,implcy", [(1, 0, 0, 0), (0, 1, 0, 0), (1, 1, 0, 0), (0, 0, 1, 1),
+                                                      (1, 1, 1, 1)])
+def test_steps_with_moving_sphere_crank_nicolson(oracle, product, imply, implx, implcx, implcy):
+    # the C.N. steps with a body: with the viscous terms implicit the forcing
+    # from the explicit estimate UB before the line solves (momforc_mod2 /
+    # velinterior with impl = 1); with the convective terms alone the
+    # explicit forcing of US, then the line solves
+    w = config.small(mx=32, ly=16, nz_=40, noise=0.2, re=2000.0, imply=imply, implx=implx, implcx=implcx,
+                     implcy=implcy)
     vel = (0.0, 0.0, -1.0)
     o, ib, g = _pair(oracle, product, w, 3, vel, attach=True)
     f = _initial(o, w)

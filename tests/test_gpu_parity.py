@@ -274,9 +274,74 @@ def test_full_step_parity_implicit_x(oracle, product, imply):
     assert abs(g.cfl() - o.calcfl()) < 1e-11 * o.calcfl()
 
 
-@pytest.mark.parametrize("imply,implx", [(0, 0), (1, 0), (0, 1), (1, 1)])
-def test_cfl_and_extrema_bit_exact(oracle, product, imply, implx):
-    w = config.small(mx=20, ly=16, nz_=24, noise=0.3, re=500.0, imply=imply, implx=implx)
+_CONV = [(0, 0, 0, 1), (1, 0, 0, 1), (0, 0, 1, 0), (0, 1, 1, 0), (1, 1, 1, 1)]
+
+
+@pytest.mark.parametrize("imply,implx,implcx,implcy", _CONV)
+def test_line_solves_with_convection_bit_exact(oracle, product, imply, implx, implcx, implcy):
+    # IMPLCX / IMPLCY: the convective terms inside the same line solves,
+    # linearised about UO / VO and the provisional US / VS
+    w = config.small(mx=20, ly=16, nz_=24, noise=0.3, re=500.0, imply=imply, implx=implx, implcx=implcx,
+                     implcy=implcy)
+    o, g = make_pair(oracle, product, w)
+    alf, gam, rho = 2 / 15 * 1e-3, 5 / 12 * 1e-3, -17 / 60 * 1e-3
+    o.rhs_predictord(alf, gam, rho)
+    g.call("eddy_rhs_predictord", alf, gam, rho)
+    for n in ("us", "vs", "ws", "ua", "va", "wa"):
+        np.testing.assert_array_equal(g.download(n), o.get(n), err_msg="predictor " + n)
+    if imply or implcy:
+        o.inversey(alf)
+        g.call("eddy_inversey", alf)
+        for n in ("us", "vs", "ws"):
+            np.testing.assert_array_equal(g.download(n), o.get(n), err_msg="inversey " + n)
+    if implx or implcx:
+        o.inversex_walls(alf)
+        o.inversex(alf)
+        g.call("eddy_inversex", alf)
+        for n in ("us", "vs", "ws"):
+            np.testing.assert_array_equal(g.download(n), o.get(n), err_msg="inversex " + n)
+
+
+@pytest.mark.parametrize("imply,implx,implcx,implcy", _CONV)
+def test_density_with_convection_bit_exact(oracle, product, imply, implx, implcx, implcy):
+    # INVERSEYD_NEW when IMPLY and IMPLCY are both on; INVERSEXD with either x flag
+    w = config.small(mx=20, ly=16, nz_=24, noise=0.3, re=500.0, imply=imply, implx=implx, implcx=implcx,
+                     implcy=implcy)
+    o, g = make_pair(oracle, product, w)
+    alf, gam, rho = 2 / 15 * 1e-3, 5 / 12 * 1e-3, -17 / 60 * 1e-3
+    o.density(alf, gam, rho)
+    g.call("eddy_density", alf, gam, rho)
+    np.testing.assert_array_equal(g.download("dens"), o.get("dens"))
+
+
+@pytest.mark.parametrize("imply,implx,implcx,implcy", _CONV)
+def test_full_step_parity_implicit_convection(oracle, product, imply, implx, implcx, implcy):
+    w = config.small(mx=16, ly=16, nz_=24, noise=0.2, re=500.0, imply=imply, implx=implx, implcx=implcx,
+                     implcy=implcy)
+    o = oracle.OracleSolver(w)
+    f = config.initial_fields(w, o.grid.get("dens_bg")[: w.nx])
+    o.load_initial(f)
+    o.initialize()
+    g = product.Solver(w)
+    g.load_initial(f)
+    g.initialize()
+    scale = run_with_scale(o, 10)
+    g.step(10)
+    for n in ("uo", "vo", "wo", "dens", "tv"):
+        e = rel_err(g.download(n), o.get(n))
+        assert e < 1e-11, (n, e)
+    pg = g.download("p")
+    assert p_err(pg, o.get("p"), scale) < P_BAR
+    assert p_profile_err(pg, o.get("p"), scale) < P_PROFILE_BAR
+    assert g.max_divergence() < 1e-12
+    assert abs(g.cfl() - o.calcfl()) < 1e-11 * o.calcfl()
+
+
+@pytest.mark.parametrize("imply,implx,implcx,implcy", [(0, 0, 0, 0), (1, 0, 0, 0), (0, 1, 0, 0), (1, 1, 0, 0),
+                                                      (0, 0, 1, 0), (0, 0, 0, 1), (1, 1, 1, 1)])
+def test_cfl_and_extrema_bit_exact(oracle, product, imply, implx, implcx, implcy):
+    w = config.small(mx=20, ly=16, nz_=24, noise=0.3, re=500.0, imply=imply, implx=implx, implcx=implcx,
+                     implcy=implcy)
     o, g = make_pair(oracle, product, w)
     assert g.cfl() == o.calcfl() > 0
     for n in ("uo", "vo", "wo", "p", "dens", "tv"):

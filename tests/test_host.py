@@ -66,14 +66,16 @@ def test_create_fails_cleanly_without_valid_config(product):
         product.Solver(w)
     # the implicit x terms are built for slip walls on both x sides and the
     # plain FP64 form only: anything else is refused before any device work
-    for kw in ({"implx": 1, "itype": (60, 82, 500, 500, 305, 730)}, {"implx": 2}):
+    for kw in ({"implx": 1, "itype": (60, 82, 500, 500, 305, 730)}, {"implx": 2},
+               {"implcx": 1, "itype": (82, 60, 500, 500, 305, 730)}, {"implcx": -1}, {"implcy": 2}):
         w = config.small(mx=12, ly=8, nz_=16)
         for k, v in kw.items():
             setattr(w, k, v)
         with pytest.raises(product.EddyError):
             product.Solver(w)
-    with pytest.raises(product.EddyError):
-        product.Solver(config.small(mx=12, ly=8, nz_=16, implx=1), precision=product.MIXED)
+    for kw in ({"implx": 1}, {"implcx": 1}, {"implcy": 1}):
+        with pytest.raises(product.EddyError):
+            product.Solver(config.small(mx=12, ly=8, nz_=16, **kw), precision=product.MIXED)
 
 
 def test_download_checks_the_callers_buffer_before_copying(product):
