@@ -68,6 +68,9 @@ def parse():
                          "--deploy-steps steps against a plain FP64 run: nu_t error against the dynamic model and "
                          "the wake-centreline velocity; prints one JSON line")
     ap.add_argument("--deploy-steps", type=int, default=200)
+    ap.add_argument("--implicit", action="store_true",
+                    help="the plain FP64 step of the wake workload with the y viscous terms Crank-Nicolson "
+                         "(imply = 1, the reference input's setting) beside the explicit one; prints one JSON line")
     ap.add_argument("--grid", default=None,
                     help="NZ-2xNX-2xNY-2 of the wake workload, e.g. 64x384x256 (6.3M cells, fields larger "
                          "than L2, a few GB on the device) for ncu captures")
@@ -282,7 +285,7 @@ def timed_steps(g, steps, stream, torch, device):
     with the clocks sampled during the timed region."""
     g.sync()
     torch.cuda.synchronize()
-    g.profile_enable(0x7FFF)
+    g.profile_enable(0xFFFF)
     l0 = g.launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -490,6 +493,55 @@ def run_poisson(args):
     print(json.dumps({"poisson": out}), flush=True)
 
 
+# C.N. line solves, per launch (one velocity component's lines): R right-hand
+# side, W solution, R nu_t (the faces' viscosities) -- the bytes a one-pass
+# solve would move; the Thomas + Sherman-Morrison sweeps move more (their
+# multipliers and correction vector go through two scratch fields)
+CN_LINE_BYTES = 3 * 8
+
+
+def run_implicit(args):
+    """The plain FP64 step of the wake workload (the moving sphere) with the y
+    viscous terms Crank-Nicolson (imply = 1: INVERSEY on the three velocity
+    components, INVERSEYD on the density, the implicit pressure terms) and
+    the same step explicit, both timed on the device like the main bench."""
+    import numpy as np
+    import torch
+    import eddy_hybrid_b200 as eb
+    from eddy_hybrid_b200 import body as bd
+    from eddy_hybrid_b200 import config
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    out = {}
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    for name, imply in (("explicit", 0), ("imply_1", 1)):
+        w = workload(args.small, args.medium, args.grid)
+        w.imply = imply
+        xu = np.diff(w.faces()[0])
+        tri, nrm = bd.icosphere(bd.level_for_spacing(max(float(xu.min()), 0.004)))
+        g = eb.Solver(w, precision=eb.PLAIN_FP64)
+        if w.sphere:
+            g.set_body(tri, nrm, bd.body_velocity(w))
+        g.load_initial(config.initial_fields(w, g.metric("dens_bg")[: w.nx]))
+        g.initialize()
+        g.step(args.warmup)
+        st = torch.cuda.ExternalStream(g.stream, device=dev)
+        ms, prof, launches, clk = timed_steps(g, args.steps, st, torch, 0)
+        alg = dict(ALG_BYTES, cn_line_solve=CN_LINE_BYTES)
+        out[name] = {"ms_per_step": ms / args.steps, "value": w.ncell * args.steps / (ms / 1e3) / 1e6,
+                     "unit": UNIT, "launches": launches, "clocks": clk,
+                     "kernels": kernel_table(prof, args.steps, w.ncell, alg, hbm, FP64_OPS_PEAK),
+                     "max_div_u": g.max_divergence()}
+        g.close()
+        del g
+    print(json.dumps({"workload": workload(args.small, args.medium, args.grid).name, "form": "plain FP64",
+                      "steps": args.steps, "warmup": args.warmup, "hbm_peak_gbs": hbm, **out}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -498,6 +550,8 @@ def main():
         return run_deploy(args)
     if args.poisson:
         return run_poisson(args)
+    if args.implicit:
+        return run_implicit(args)
     rank, world, local, dist = dist_init(args.gpus)
     import numpy as np
     import torch

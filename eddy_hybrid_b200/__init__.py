@@ -482,14 +482,14 @@ class Solver:
     PROFILE_CATEGORIES = ["rhs_predictor", "boundary", "div_fft_fwd", "transform_fwd",
                           "z_line_solve", "transform_bwd", "fft_bwd", "correct",
                           "pressure_update", "density", "eddy_viscosity", "refine_residual",
-                          "precision_copy", "ib_regen", "ib_force"]
+                          "precision_copy", "ib_regen", "ib_force", "cn_line_solve"]
 
-    def profile_enable(self, mask: int = 0x7FFF):
+    def profile_enable(self, mask: int = 0xFFFF):
         self._check(lib().eddy_profile_enable(self.h, mask), "eddy_profile_enable")
 
     def profile_read(self) -> dict:
-        ms = (C.c_double * 15)()
-        n = (C.c_longlong * 15)()
+        ms = (C.c_double * len(self.PROFILE_CATEGORIES))()
+        n = (C.c_longlong * len(self.PROFILE_CATEGORIES))()
         self._check(lib().eddy_profile_read(self.h, ms, n), "eddy_profile_read")
         return {c: (ms[i], n[i]) for i, c in enumerate(self.PROFILE_CATEGORIES)}
 

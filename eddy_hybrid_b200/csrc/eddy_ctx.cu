@@ -809,11 +809,11 @@ static int substep_core(eddy_ctx *ctx, int is, double dt) {
   }
   // Crank-Nicolson y, then x lines (src/Eddy6.f:2596-2607)
   if (ctx->sc.imply == 1 || ctx->sc.implcy == 1) {
-    ProfScope ps(ctx, PROF_TRIDIAG);
+    ProfScope ps(ctx, PROF_CN_LINES);
     if ((rc = launch_inversey(ctx, alfxdt))) return rc;
   }
   if (ctx->sc.implx == 1 || ctx->sc.implcx == 1) {
-    ProfScope ps(ctx, PROF_TRIDIAG);
+    ProfScope ps(ctx, PROF_CN_LINES);
     if ((rc = launch_inversex(ctx, alfxdt))) return rc;
   }
   {

@@ -70,7 +70,7 @@ struct PoissonPlan {
 enum {
   PROF_RHS_PRED = 0, PROF_BC, PROF_DIV_FFT, PROF_GEMM_FWD, PROF_TRIDIAG, PROF_GEMM_BWD, PROF_FFT_BWD,
   PROF_CORRECT, PROF_PUPDATE, PROF_DENSITY, PROF_TURVIS, PROF_REFINE, PROF_CONVERT, PROF_IB_REGEN,
-  PROF_IB_FORCE, PROF_NCAT
+  PROF_IB_FORCE, PROF_CN_LINES, PROF_NCAT
 };
 
 struct TmaEntry {

@@ -25,12 +25,19 @@ namespace {
 // right-hand side.  fy = rflagy (IMPLY) scales the viscous coefficients, fc =
 // rflagcy (IMPLCY) the convective ones (timeindeg.f:150-312)
 struct RowV {  // v: viscosity 2 tv(j) and 2 tv(j+1) on the faces; convection about VO
-  const double *tv, *bv, *bp, *vo;
+  const double *__restrict__ tv, *__restrict__ bv, *__restrict__ bp, *__restrict__ vo;
   double coef, ru1, fy, fc;
   __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 2. * tv[fidx(d, i, j + 1, k)] + ru1, tvjm = 2. * tv[fidx(d, i, j, k)] + ru1;
     const double coefy = fy * coef * bv[j] / (1.0 * 1.0);
     const double ayv = -coefy * bp[j] * tvjm, cyv = -coefy * bp[j + 1] * tvjp, byv = -ayv - cyv;
+    if (fc == 0.) {  // the convective terms are signed zeros: the same sums without their loads
+      a = ayv;
+      c = cyv;
+      b = 1.0 + byv;
+      r = 0.;
+      return;
+    }
     const double vm = vo[fidx(d, i, j - 1, k)], v0 = vo[fidx(d, i, j, k)], vp = vo[fidx(d, i, j + 1, k)];
     const double coefc = fc * coef * bv[j] / 1.0;
     const double ayc = -0.25 * coefc * (vm + v0) * 2.0, cyc = 0.25 * coefc * (vp + v0) * 2.0, byc = ayc + cyc;
@@ -42,7 +49,7 @@ struct RowV {  // v: viscosity 2 tv(j) and 2 tv(j+1) on the faces; convection ab
   }
 };
 struct RowW {  // w: edge viscosity averaged over four cells; convection about the provisional VS
-  const double *tv, *bw, *bv, *vs;
+  const double *__restrict__ tv, *__restrict__ bw, *__restrict__ bv, *__restrict__ vs;
   double coef, ru1, fy, fc;
   __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 0.25 * (tv[fidx(d, i, j, k + 1)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k + 1)] +
@@ -51,6 +58,13 @@ struct RowW {  // w: edge viscosity averaged over four cells; convection about t
                                 tv[fidx(d, i, j - 1, k)]) + ru1;
     const double coefy = fy * coef * bw[j] / (1.0 * 1.0);
     const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+    if (fc == 0.) {
+      a = ayv;
+      c = cyv;
+      b = 1.0 + byv;
+      r = 0.;
+      return;
+    }
     const double vzp = (vs[fidx(d, i, j, k + 1)] + vs[fidx(d, i, j, k)]) * 0.5;
     const double vzm = (vs[fidx(d, i, j - 1, k + 1)] + vs[fidx(d, i, j - 1, k)]) * 0.5;
     const double coefc = fc * 0.5 * coef * bw[j] / 1.0;
@@ -62,7 +76,7 @@ struct RowW {  // w: edge viscosity averaged over four cells; convection about t
   }
 };
 struct RowU {  // u (timeindeg.f:290-312); convection about the provisional VS
-  const double *tv, *bu, *bv, *vs;
+  const double *__restrict__ tv, *__restrict__ bu, *__restrict__ bv, *__restrict__ vs;
   double coef, ru1, fy, fc;
   __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 0.25 * (tv[fidx(d, i + 1, j, k)] + tv[fidx(d, i, j, k)] + tv[fidx(d, i + 1, j + 1, k)] +
@@ -71,6 +85,13 @@ struct RowU {  // u (timeindeg.f:290-312); convection about the provisional VS
                                 tv[fidx(d, i, j - 1, k)]) + ru1;
     const double coefy = fy * coef * bu[j] / (1.0 * 1.0);
     const double ayv = -coefy * bv[j - 1] * tvjm, cyv = -coefy * bv[j] * tvjp, byv = -ayv - cyv;
+    if (fc == 0.) {
+      a = ayv;
+      c = cyv;
+      b = 1.0 + byv;
+      r = 0.;
+      return;
+    }
     const double vxp = (vs[fidx(d, i + 1, j, k)] + vs[fidx(d, i, j, k)]) * 0.5;
     const double vxm = (vs[fidx(d, i + 1, j - 1, k)] + vs[fidx(d, i, j - 1, k)]) * 0.5;
     const double coefc = fc * 0.5 * coef * bu[j] / 1.0;
@@ -82,7 +103,7 @@ struct RowU {  // u (timeindeg.f:290-312); convection about the provisional VS
   }
 };
 struct RowD {  // density (density.f:425-440): both faces take 0.5 (tv(j) + tv(j+1)) + ru1/prn
-  const double *tv, *bp;
+  const double *__restrict__ tv, *__restrict__ bp;
   double coef, kmol;
   __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k)]) + kmol;
@@ -95,7 +116,7 @@ struct RowD {  // density (density.f:425-440): both faces take 0.5 (tv(j) + tv(j
   }
 };
 struct RowDN {  // density, INVERSEYD_NEW (density.f:322-352): faces 0.5 (tv(j) + tv(j+/-1)) + ru1/prn, convection by VO
-  const double *tv, *bp, *bv, *vo;
+  const double *__restrict__ tv, *__restrict__ bp, *__restrict__ bv, *__restrict__ vo;
   double coef, kmol, fy, fc;
   __device__ void operator()(const Dims &d, int i, int j, int k, double &a, double &b, double &c, double &r) const {
     const double tvjp = 0.5 * (tv[fidx(d, i, j, k)] + tv[fidx(d, i, j + 1, k)]) + kmol;
@@ -113,23 +134,33 @@ struct RowDN {  // density, INVERSEYD_NEW (density.f:322-352): faces 0.5 (tv(j) 
 };
 
 // lines i in [i0, i0+ni), k in [k0, k0+nk); rows jy1..jy2 (n = jy2 - 1 >= 3);
-// x: right-hand side in, solution out (in place); gam, z: scratch fields
+// x: right-hand side in, solution out (in place); gam, z: scratch fields.
+// Each sweep loads the next row's operands before the current row's
+// dependent arithmetic (the loads do not depend on the recurrence), so every
+// thread keeps two rows of loads in flight.
 template <class Row>
-__global__ void __launch_bounds__(128) k_cyclic_lines(Dims d, Row row, int i0, int ni, int k0, int nk, double *x,
-                                                      double *gam, double *z) {
+__global__ void __launch_bounds__(128) k_cyclic_lines(Dims d, Row row, int i0, int ni, int k0, int nk,
+                                                      double *__restrict__ x, double *__restrict__ gam,
+                                                      double *__restrict__ z) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)ni * nk) return;
   const int i = i0 + (int)(t % ni), k = k0 + (int)(t / ni);
   const int n = d.jy2 - 1;
+  const long long q0 = fidx(d, i, d.jy1, k), sj = d.nx;
   // forward elimination of A' x = r and A' z = (gamma, 0, .., 0, alpha), A'
   // the matrix with b1' = b1 - gamma, bn' = bn - alpha beta / gamma
   double beta = 0., gamma = 1., bet = 1., cprev = 0., xp = 0., zp = 0.;
+  double a, b, c, dr;
+  row(d, i, d.jy1, k, a, b, c, dr);
+  double xr = x[q0];
   for (int r = 0; r < n; r++) {
-    const int j = d.jy1 + r;
-    const long long q = fidx(d, i, j, k);
-    double a, b, c, dr;
-    row(d, i, j, k, a, b, c, dr);
-    const double rr = x[q] + dr;
+    const long long q = q0 + sj * r;
+    double an = 0., bn = 1., cn = 0., drn = 0., xrn = 0.;
+    if (r + 1 < n) {
+      row(d, i, d.jy1 + r + 1, k, an, bn, cn, drn);
+      xrn = x[q + sj];
+    }
+    const double rr = xr + dr;
     if (r == 0) {
       beta = a;
       gamma = -b;
@@ -148,21 +179,31 @@ __global__ void __launch_bounds__(128) k_cyclic_lines(Dims d, Row row, int i0, i
     x[q] = xp;
     z[q] = zp;
     cprev = c;
+    a = an; b = bn; c = cn; dr = drn; xr = xrn;
   }
   // back substitution (the last row stands)
   const double xn = xp, zn = zp;
-  for (int r = n - 2; r >= 0; r--) {
-    const long long q = fidx(d, i, d.jy1 + r, k), qn = q + d.nx;
-    const double g = gam[qn];
-    xp = x[q] - g * xp;
-    zp = z[q] - g * zp;
-    x[q] = xp;
-    z[q] = zp;
+  if (n >= 2) {
+    long long q = q0 + sj * (n - 2);
+    double g = gam[q + sj], xq = x[q], zq = z[q];
+    for (int r = n - 2; r >= 0; r--, q -= sj) {
+      double gnx = 0., xnx = 0., znx = 0.;
+      if (r > 0) {
+        gnx = gam[q];
+        xnx = x[q - sj];
+        znx = z[q - sj];
+      }
+      xp = xq - g * xp;
+      zp = zq - g * zp;
+      x[q] = xp;
+      z[q] = zp;
+      g = gnx; xq = xnx; zq = znx;
+    }
   }
   // Sherman-Morrison correction for the two corner entries
   const double fact = (xp + beta * xn / gamma) / (1. + zp + beta * zn / gamma);
   for (int r = 0; r < n; r++) {
-    const long long q = fidx(d, i, d.jy1 + r, k);
+    const long long q = q0 + sj * r;
     x[q] = x[q] - fact * z[q];
   }
 }

@@ -305,9 +305,11 @@ int eddy_body_force_cv_reset(eddy_ctx *ctx);
  * 5 backward transform, 6 backward FFT, 7 CORRECT, 8 pressure update,
  * 9 density, 10 eddy viscosity, 11 refinement residual + forward FFT,
  * 12 FP64/FP32 copies (mixed form), 13 immersed-body regeneration, 14
- * immersed-body forcing.  eddy_profile_read synchronises, adds the window's
- * elapsed times per category to ms[15] / counts[15] (cumulative
- * since the mask was set) and starts a new window. */
+ * immersed-body forcing, 15 Crank-Nicolson line solves of the velocities
+ * (INVERSEY / INVERSEX; the density's run inside category 9).
+ * eddy_profile_read synchronises, adds the window's elapsed times per
+ * category to ms[16] / counts[16] (cumulative since the mask was set) and
+ * starts a new window. */
 int eddy_profile_enable(eddy_ctx *ctx, unsigned mask);
 int eddy_profile_read(eddy_ctx *ctx, double *ms, long long *counts);
 
