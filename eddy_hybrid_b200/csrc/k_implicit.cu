@@ -237,6 +237,13 @@ struct RowXU {  // u (timeindeg.f:441-486): viscosity 2 tv(i) and 2 tv(i+1); con
     const double tvip = 2. * tv[fidx(d, i + 1, j, k)] + ru1, tvim = 2. * tv[fidx(d, i, j, k)] + ru1;
     const double coefx = fx * coef * au[i];
     const double axv = -coefx * ap[i] * tvim, cxv = -coefx * ap[i + 1] * tvip, bxv = -axv - cxv;
+    if (fc == 0.) {  // the convective terms are signed zeros: the same sums without their loads
+      a = axv;
+      c = cxv;
+      b = 1.0 + bxv;
+      r = 0.;
+      return;
+    }
     const double um = uo[fidx(d, i - 1, j, k)], u0 = uo[fidx(d, i, j, k)], up = uo[fidx(d, i + 1, j, k)];
     const double coefc = fc * coef * au[i] / 1.0;
     const double qxm = (u0 + um) * 0.5, qxp = (u0 + up) * 0.5;
@@ -258,6 +265,13 @@ struct RowXV {  // v (timeindeg.f:528-560); convection about the provisional US
                                 tv[fidx(d, i - 1, j, k)]) + ru1;
     const double coefx = fx * coef * av[i] / 1.0;
     const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
+    if (fc == 0.) {  // the convective terms are signed zeros: the same sums without their loads
+      a = axv;
+      c = cxv;
+      b = 1.0 + bxv;
+      r = 0.;
+      return;
+    }
     const double coefc = fc * 0.5 * coef * av[i] / 1.0;
     const double qyp = 1.0 * (us[fidx(d, i, j + 1, k)] + us[fidx(d, i, j, k)]) * 0.5;
     const double qym = 1.0 * (us[fidx(d, i - 1, j + 1, k)] + us[fidx(d, i - 1, j, k)]) * 0.5;
@@ -278,6 +292,13 @@ struct RowXW {  // w (timeindeg.f:594-626); convection about the provisional US
                                 tv[fidx(d, i - 1, j, k)]) + ru1;
     const double coefx = fx * coef * aw[i] / 1.0;
     const double axv = -coefx * au[i - 1] * tvim, cxv = -coefx * au[i] * tvip, bxv = -axv - cxv;
+    if (fc == 0.) {  // the convective terms are signed zeros: the same sums without their loads
+      a = axv;
+      c = cxv;
+      b = 1.0 + bxv;
+      r = 0.;
+      return;
+    }
     const double coefc = fc * 0.5 * coef * aw[i] / 1.0;
     const double qzp = 1.0 * (us[fidx(d, i, j, k + 1)] + us[fidx(d, i, j, k)]) * 0.5;
     const double qzm = 1.0 * (us[fidx(d, i - 1, j, k + 1)] + us[fidx(d, i - 1, j, k)]) * 0.5;
