@@ -102,7 +102,7 @@ __global__ void k_to64(Dims d, int px, const float *__restrict__ b, double *__re
 // ---------------------------------------------------------------------------
 // RHS + PREDICTORD in FP32 (src/rhs.f:4-438, src/timeindeg.f:1041-1265) on the
 // TMA plane ring; same structure as the FP64 kernel.
-constexpr int TX = 32, TY = 8, NFLD = 9, KCHUNK = 32;  // uo vo wo tv p dens ua va wa
+constexpr int TX = 32, TY = 8, NFLD = 9, KCHUNK = 64;  // uo vo wo tv p dens ua va wa
 using Acc9 = RingAcc<TX, TY, NFLD, float>;
 
 struct MomAcc32 {
